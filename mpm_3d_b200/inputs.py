@@ -1,0 +1,293 @@
+"""Seeded synthetic inputs for the explicit MPM step, in mpm_3d's own formats.
+
+A ``Case`` holds everything one ExplicitUSL run needs: the CartesianLinear grid,
+the bodies (points with mass, volume, position, velocity, active flag, an
+IsotropicLinearElasticity material and an optional CartesianBox boundary),
+ContactHuang pairs, the gravity mode and the time step. ``write_case`` writes it
+as a mpm_3d ``.cfg`` plus one ``.points`` file per body, the formats the
+reference reads (``src/config/config.cpp:176-528``,
+``src/objects/points/default_points.cpp:104-193``); doubles are written with
+17 significant digits, so ``std::stod`` reads back the exact same values.
+
+Block layouts follow the reference examples (``examples/blockdrop2D/test2D.points``):
+2 points per cell per axis at the quarter points of each cell relative to the
+block origin, ``m = rho * (h/2)^D`` and ``V = (h/2)^D``.
+
+The named workloads:
+
+* ``block_drop_2d()``: 2D block drop, 20x20 grid on 1x1 m, 144 points,
+  E=1e5, nu=0.3, v=(0,-1), dt=1e-4, 2000 steps.
+* ``two_body_collision_3d(n_cells=128)``: two 0.25 m cubes colliding at
+  +-1 m/s in a 1 m cube, ContactHuang mu=0.4; 128^3 cells gives 262,144 points
+  per body; dt=2e-5, 1000 steps.
+* ``column_collapse_3d(scale=1)``: 0.5x0.5x0.75 m column on the floor of a
+  2x2x1 m domain at 256x256x128 cells (3,145,728 points), rho=1500,
+  +-1% h seeded jitter, dt=1e-5, 500 steps. ``scale`` divides the cell
+  counts for smaller parity cases.
+* ``block_drop_ensemble(count, seed)``: independent 3D block drops with
+  seeded grid size, block size/position, velocity and material, dt from each
+  instance's CFL limit.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+import os
+from typing import List, Optional, Sequence, Tuple
+
+import numpy as np
+
+__all__ = [
+    "Body",
+    "Contact",
+    "Case",
+    "block_points",
+    "block_drop_2d",
+    "two_body_collision_3d",
+    "column_collapse_3d",
+    "block_drop_ensemble",
+    "write_case",
+    "read_points_file",
+]
+
+
+@dataclasses.dataclass
+class Body:
+    """One DefaultBody: point arrays plus material and boundary settings."""
+
+    name: str
+    m: np.ndarray  # (n,) mass
+    v: np.ndarray  # (n,) volume
+    x: np.ndarray  # (n, 3) position (third column 0 in 2D)
+    x_t: np.ndarray  # (n, 3) velocity
+    active: np.ndarray  # (n,) int32
+    E: float = 1e5
+    nu: float = 0.3
+    material: bool = True
+    boundary: bool = True
+
+    @property
+    def n(self) -> int:
+        return int(self.m.shape[0])
+
+
+@dataclasses.dataclass
+class Contact:
+    """ContactHuang between bodies b1 and b2 with friction mu."""
+
+    b1: int
+    b2: int
+    mu: float
+
+
+@dataclasses.dataclass
+class Case:
+    name: str
+    dim: int
+    L: Tuple[float, ...]
+    N: Tuple[int, ...]
+    dt: float
+    steps: int
+    bodies: List[Body]
+    contacts: List[Contact] = dataclasses.field(default_factory=list)
+    cpdi: int = 1  # ExplicitUSL int-properties[0] (use_gimp)
+    contact_spec: int = 1  # ExplicitUSL int-properties[1] (1 = IMPLICIT)
+    gravity: Optional[Tuple[float, float, float]] = None  # None = DefaultDriver
+    seed: Optional[int] = None
+
+    @property
+    def h(self) -> Tuple[float, ...]:
+        return tuple(self.L[i] / self.N[i] for i in range(self.dim))
+
+    @property
+    def n_points(self) -> int:
+        return sum(b.n for b in self.bodies)
+
+    @property
+    def n_nodes(self) -> int:
+        out = 1
+        for i in range(self.dim):
+            out *= self.N[i] + 1
+        return out
+
+
+def block_points(lo: Sequence[float], counts: Sequence[int], h: Sequence[float], rho: float,
+                 velocity: Sequence[float], jitter: float = 0.0,
+                 rng: Optional[np.random.Generator] = None, name: str = "block",
+                 E: float = 1e5, nu: float = 0.3) -> Body:
+    """A block of 2 points per cell per axis starting at ``lo``.
+
+    ``counts[i]`` points along axis i at ``lo + (j + 1/2) * h/2``; ``jitter`` is a
+    fraction of ``h`` for a seeded uniform perturbation per axis.
+    """
+    dim = len(counts)
+    axes = [lo[i] + (np.arange(counts[i], dtype=np.float64) + 0.5) * (h[i] / 2.0) for i in range(dim)]
+    # last axis fastest, like examples/collision3D/test3D.points
+    grids = np.meshgrid(*axes, indexing="ij")
+    pos = np.stack([g.reshape(-1) for g in grids], axis=1)
+    n = pos.shape[0]
+    if jitter:
+        assert rng is not None
+        pos = pos + rng.uniform(-jitter, jitter, size=pos.shape) * np.asarray(h[:dim])
+    x = np.zeros((n, 3))
+    x[:, :dim] = pos
+    vol = 1.0
+    for i in range(dim):
+        vol *= h[i] / 2.0
+    xt = np.zeros((n, 3))
+    xt[:, :dim] = np.asarray(velocity[:dim], dtype=np.float64)
+    return Body(name=name, m=np.full(n, rho * vol), v=np.full(n, vol), x=x, x_t=xt,
+                active=np.ones(n, dtype=np.int32), E=E, nu=nu)
+
+
+def block_drop_2d() -> Case:
+    """2D block drop: 20x20 grid on 1x1 m, 0.3x0.3 m block centred at (0.5,0.6)."""
+    h = (0.05, 0.05)
+    body = block_points((0.35, 0.45), (12, 12), h, 1000.0, (0.0, -1.0), name="block", E=1e5, nu=0.3)
+    return Case(name="block_drop_2d", dim=2, L=(1.0, 1.0), N=(20, 20), dt=1e-4, steps=2000, bodies=[body])
+
+
+def two_body_collision_3d(n_cells: int = 128, steps: int = 1000, gravity=None, gap: Optional[float] = None,
+                          speed: float = 1.0, mu: float = 0.4) -> Case:
+    """Two 0.25 m cubes at (0.3,0.5,0.5) and (0.7,0.5,0.5) moving at +-1 m/s.
+
+    ``gap`` (metres) instead places the second cube that far from the first,
+    so that contact engages within the first steps.
+    """
+    h = (1.0 / n_cells,) * 3
+    per_axis = int(round(0.25 / (h[0] / 2.0)))
+    lo2 = 0.575 if gap is None else 0.425 + gap
+    a = block_points((0.175, 0.375, 0.375), (per_axis,) * 3, h, 1000.0, (speed, 0.0, 0.0), name="cube1", E=1e6,
+                     nu=0.3)
+    b = block_points((lo2, 0.375, 0.375), (per_axis,) * 3, h, 1000.0, (-speed, 0.0, 0.0), name="cube2", E=1e6, nu=0.3)
+    tag = "" if gap is None else "_touching"
+    return Case(name=f"two_body_collision_3d_{n_cells}{tag}", dim=3, L=(1.0, 1.0, 1.0), N=(n_cells,) * 3, dt=2e-5,
+                steps=steps, bodies=[a, b], contacts=[Contact(0, 1, mu)], gravity=gravity)
+
+
+def two_body_collision_2d(n_cells: int = 20, steps: int = 200, gap: float = 0.02, mu: float = 0.4) -> Case:
+    """2D analogue of the two-body collision, blocks already in contact range."""
+    h = (1.0 / n_cells,) * 2
+    per_axis = int(round(0.3 / (h[0] / 2.0)))
+    a = block_points((0.15, 0.35), (per_axis, per_axis), h, 1000.0, (1.0, 0.5), name="left", E=1e5, nu=0.3)
+    b = block_points((0.45 + gap, 0.3), (per_axis, per_axis), h, 1000.0, (-1.0, 0.0), name="right", E=1e5, nu=0.3)
+    return Case(name=f"two_body_collision_2d_{n_cells}", dim=2, L=(1.0, 1.0), N=(n_cells, n_cells), dt=1e-4,
+                steps=steps, bodies=[a, b], contacts=[Contact(0, 1, mu)])
+
+
+def column_collapse_3d(scale: int = 1, seed: int = 1002, steps: int = 500) -> Case:
+    """Column 0.5x0.5x0.75 m on the floor of a 2x2x1 m domain, rho=1500."""
+    N = (256 // scale, 256 // scale, 128 // scale)
+    h = (2.0 / N[0], 2.0 / N[1], 1.0 / N[2])
+    counts = tuple(int(round(s / (hh / 2.0))) for s, hh in zip((0.5, 0.5, 0.75), h))
+    rng = np.random.default_rng(seed)
+    body = block_points((0.75, 0.75, 0.0), counts, h, 1500.0, (0.0, 0.0, 0.0), jitter=0.01, rng=rng,
+                        name="column", E=1e6, nu=0.3)
+    return Case(name=f"column_collapse_3d_s{scale}", dim=3, L=(2.0, 2.0, 1.0), N=N, dt=1e-5, steps=steps,
+                bodies=[body], seed=seed)
+
+
+def _cfl_dt(h: float, E: float, nu: float, rho: float, vmax: float, courant: float = 0.3) -> float:
+    G = E / (2.0 * (1.0 + nu))
+    K = E / (3.0 * (1.0 - 2.0 * nu))
+    c = math.sqrt((K + 4.0 * G / 3.0) / rho)
+    return courant * h / (c + vmax)
+
+
+def block_drop_ensemble(count: int = 512, seed: int = 1003, n_range=(16, 96), steps: int = 500,
+                        side_range=(0.15, 0.4)) -> List[Case]:
+    """Independent 3D block drops drawn from ``seed``.
+
+    Per instance: N log-uniform in ``n_range`` (grid N^3 on a 1 m cube), a cube of
+    side uniform in ``side_range`` placed at least one cell from every wall,
+    velocity uniform in [-2,2]^3, E log-uniform in [1e4,1e7], nu uniform in
+    [0.2,0.45], rho=1000, DefaultDriver gravity, dt = 0.3 h / (c + |v|max).
+    """
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(count):
+        n = int(round(math.exp(rng.uniform(math.log(n_range[0]), math.log(n_range[1])))))
+        h = 1.0 / n
+        side = rng.uniform(*side_range)
+        per_axis = max(2, int(round(side / (h / 2.0))))
+        side = per_axis * h / 2.0
+        lo = [rng.uniform(h, 1.0 - h - side) for _ in range(3)]
+        vel = rng.uniform(-2.0, 2.0, size=3)
+        E = math.exp(rng.uniform(math.log(1e4), math.log(1e7)))
+        nu = rng.uniform(0.2, 0.45)
+        body = block_points(lo, (per_axis,) * 3, (h,) * 3, 1000.0, vel, name="block", E=E, nu=nu)
+        dt = _cfl_dt(h, E, nu, 1000.0, float(np.abs(vel).max()) * math.sqrt(3.0))
+        out.append(Case(name=f"ensemble_{seed}_{k}", dim=3, L=(1.0, 1.0, 1.0), N=(n, n, n), dt=dt,
+                        steps=steps, bodies=[body], seed=seed))
+    return out
+
+
+def _fmt(v: float) -> str:
+    return repr(float(v))
+
+
+def write_points_file(body: Body, path: str, dim: int) -> None:
+    """Writes a ``.points`` file: count, then ``m v x.. x_t.. active`` lines."""
+    cols = [body.m[:, None], body.v[:, None], body.x[:, :dim], body.x_t[:, :dim]]
+    arr = np.concatenate(cols, axis=1)
+    with open(path, "w") as f:
+        f.write(f"{body.n}\n")
+        for row, act in zip(arr, body.active):
+            f.write(" ".join(_fmt(v) for v in row) + f" {int(act)}\n")
+
+
+def read_points_file(path: str, dim: int) -> Tuple[np.ndarray, ...]:
+    """Reads a ``.points`` file; returns (m, v, x (n,3), x_t (n,3), active)."""
+    with open(path) as f:
+        n = int(f.readline())
+        data = np.loadtxt(f, ndmin=2)
+    if data.shape[0] != n:
+        raise ValueError(f"{path}: header says {n} points, found {data.shape[0]}")
+    if data.shape[1] != 3 + 2 * dim:
+        raise ValueError(f"{path}: expected {3 + 2 * dim} columns, found {data.shape[1]}")
+    x = np.zeros((n, 3))
+    xt = np.zeros((n, 3))
+    x[:, :dim] = data[:, 2:2 + dim]
+    xt[:, :dim] = data[:, 2 + dim:2 + 2 * dim]
+    return data[:, 0].copy(), data[:, 1].copy(), x, xt, data[:, -1].astype(np.int32)
+
+
+def write_case(case: Case, directory: str, solver_class: str = "ExplicitUSL", points_class: str = "DefaultPoints",
+               threads: Optional[int] = None) -> str:
+    """Writes ``<name>.cfg`` and the ``.points`` files; returns the cfg path."""
+    os.makedirs(directory, exist_ok=True)
+    lines = ["job", "{", f"    dt = {_fmt(case.dt)}", "    t = 0", f"    TYPE = {case.dim}"]
+    if threads is not None:
+        lines.append(f"    threads = {threads}")
+    lines += ["}", "", "serializer", "{", '    class = "DefaultVTK"', "    properties = {60}",
+              '    str-properties = {"output","save","case"}', "}", ""]
+    stop = case.dt * case.steps
+    if case.gravity is None:
+        lines += ["driver", "{", '    class = "DefaultDriver"', f"    properties = {{{_fmt(stop)}}}", "}", ""]
+    else:
+        g = ",".join(_fmt(v) for v in case.gravity[:case.dim])
+        lines += ["driver", "{", '    class = "UserDefinedGravityDriver"', f"    properties = {{{_fmt(stop)},{g}}}",
+                  "}", ""]
+    lines += ["solver", "{", f'    class = "{solver_class}"', f"    int-properties = {{{case.cpdi},{case.contact_spec}}}",
+              "}", ""]
+    lines += ["grid", "{", '    class = "CartesianLinear"',
+              "    properties = {" + ",".join(_fmt(case.L[i]) for i in range(case.dim)) + "}",
+              "    int-properties = {" + ",".join(str(case.N[i]) for i in range(case.dim)) + "}", "}", ""]
+    for bi, body in enumerate(case.bodies):
+        pfile = f"{case.name}_{bi}_{body.name}.points"
+        write_points_file(body, os.path.join(directory, pfile), case.dim)
+        lines += ["body", "{", '    class = "DefaultBody"', f'    name = "{body.name}"', f'    point-file = "{pfile}"',
+                  f'    point-class = "{points_class}"', '    node-class = "DefaultNodes"']
+        if body.material:
+            lines += ['    material-class = "IsotropicLinearElasticity"',
+                      f"    material-props = {{{_fmt(body.E)},{_fmt(body.nu)}}}"]
+        if body.boundary:
+            lines += ['    boundary-class = "CartesianBox"']
+        lines += ["}", ""]
+    for c in case.contacts:
+        lines += ["contact", "{", '    name = "contact"', '    class = "ContactHuang"', f"    properties = {{{_fmt(c.mu)}}}",
+                  f'    str-properties = {{"{case.bodies[c.b1].name}","{case.bodies[c.b2].name}"}}', "}", ""]
+    path = os.path.join(directory, f"{case.name}.cfg")
+    with open(path, "w") as f:
+        f.write("\n".join(lines) + "\n")
+    return path
