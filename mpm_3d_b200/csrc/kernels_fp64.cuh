@@ -1,0 +1,377 @@
+// FP64 kernels of the explicit step: map + scatter (P2G), active-block
+// compaction, grid update (contact, boundary, moveGrid) and gather + point
+// update (G2P, strain rate, density, stress).
+#pragma once
+
+#include "exact_map.cuh"
+#include "geom.cuh"
+#include "state.cuh"
+
+namespace mpmb200 {
+
+__device__ __forceinline__ double sym_at(const double* s6, int a, int b) {
+  // xx yy zz xy yz xz
+  if (a == b) return s6[a];
+  const int lo = a < b ? a : b, hi = a < b ? b : a;
+  if (lo == 0 && hi == 1) return s6[3];
+  if (lo == 1 && hi == 2) return s6[4];
+  return s6[5];
+}
+
+// Marks the node blocks covered by a point's window.
+template <int DIM>
+__device__ __forceinline__ void mark_blocks(const Geom& g, const PointMap& pm, uint32_t* flags) {
+  const int i0 = pm.ax[0].base >> g.bsh[0], i1 = (pm.ax[0].base + pm.ax[0].span - 1) >> g.bsh[0];
+  const int j0 = pm.ax[1].base >> g.bsh[1], j1 = (pm.ax[1].base + pm.ax[1].span - 1) >> g.bsh[1];
+  int k0 = 0, k1 = 0;
+  if (DIM == 3) {
+    k0 = pm.ax[2].base >> g.bsh[2];
+    k1 = (pm.ax[2].base + pm.ax[2].span - 1) >> g.bsh[2];
+  }
+  for (int k = k0; k <= k1; k++)
+    for (int j = j0; j <= j1; j++)
+      for (int i = i0; i <= i1; i++) flags[i + (int64_t)g.nb[0] * (j + (int64_t)g.nb[1] * k)] = 1u;
+}
+
+// P2G: mapPointsToNodes (explicit_usl.cpp:112-164) and, for the first body
+// of a contact, the normal accumulation of ContactHuang::generateRules
+// (contact_huang.cpp:91), one thread per point, FP64 atomics per window node.
+template <int DIM>
+__global__ void __launch_bounds__(256) k_p2g(Geom g, StepParams sp, PointsDev P, NodesAcc A, uint32_t* flags, int* err) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < P.n; p += stride) {
+    if (!P.active[p]) continue;
+    double x[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int d = 0; d < DIM; d++) x[d] = P.x[d][p];
+    PointMap pm;
+    const int st = build_map<DIM>(g, sp.cpdi, x, P.ext[p], pm, err);
+    if (st < 0) {
+      P.active[p] = 0;  // default_points.cpp:217-219
+      continue;
+    }
+    if (st == 0) continue;
+    mark_blocks<DIM>(g, pm, flags);
+    const double m = P.m[p];
+    const double vol = P.vol[p];
+    double mv[3], mb[3], vs[6];
+#pragma unroll
+    for (int d = 0; d < DIM; d++) {
+      mv[d] = m * P.v[d][p];
+      mb[d] = m * sp.grav[d];
+    }
+#pragma unroll
+    for (int c = 0; c < 6; c++) vs[c] = (DIM == 3 || c == 0 || c == 1 || c == 3) ? P.s[c][p] * vol : 0.0;
+    const AxisMap& X = pm.ax[0];
+    const AxisMap& Y = pm.ax[1];
+    const int span2 = (DIM == 3) ? pm.ax[2].span : 1;
+    for (int k2 = 0; k2 < span2; k2++) {
+      const double wz = (DIM == 3) ? pm.ax[2].W[k2] : 1.0;
+      const double gz = (DIM == 3) ? pm.ax[2].G[k2] : 0.0;
+      for (int k1 = 0; k1 < Y.span; k1++) {
+        for (int k0 = 0; k0 < X.span; k0++) {
+          const double wxy = X.W[k0] * Y.W[k1];
+          const double S = pm.sS * (wxy * wz);
+          double gr[3];
+          gr[0] = pm.sG * (X.G[k0] * Y.W[k1] * wz);
+          gr[1] = pm.sG * (X.W[k0] * Y.G[k1] * wz);
+          gr[2] = (DIM == 3) ? pm.sG * (wxy * gz) : 0.0;
+          const int64_t s = node_slot(g, X.base + k0, Y.base + k1, DIM == 3 ? pm.ax[2].base + k2 : 0);
+          atomicAdd(A.m + s, S * m);
+#pragma unroll
+          for (int d = 0; d < DIM; d++) {
+            atomicAdd(A.mx[d] + s, S * mv[d]);
+            double fi = 0.0;
+#pragma unroll
+            for (int e = 0; e < DIM; e++) fi += sym_at(vs, d, e) * gr[e];
+            atomicAdd(A.f[d] + s, S * mb[d] - fi);
+            if (A.nrm[0] != nullptr) atomicAdd(A.nrm[d] + s, gr[d] * m);
+          }
+        }
+      }
+    }
+  }
+}
+
+// Compacts the flagged node blocks into `list`, clears the flags and keeps
+// the per-block activity of this step in `was_active`.
+__global__ void k_compact(int64_t nblocks, uint32_t* flags, int64_t* list, unsigned long long* count,
+                          uint8_t* was_active) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const int lane = threadIdx.x & 31;
+  for (int64_t base = blockIdx.x * (int64_t)blockDim.x; base < nblocks; base += stride) {
+    const int64_t blk = base + threadIdx.x;
+    const bool on = blk < nblocks && flags[blk] != 0u;
+    if (blk < nblocks) {
+      was_active[blk] = on ? 1 : 0;
+      if (on) flags[blk] = 0u;
+    }
+    const unsigned mask = __ballot_sync(0xffffffffu, on);
+    if (mask == 0u) continue;
+    unsigned long long first = 0;
+    if (lane == 0) first = atomicAdd(count, (unsigned long long)__popc(mask));
+    first = __shfl_sync(0xffffffffu, first, 0);
+    if (on) list[first + __popc(mask & ((1u << lane) - 1u))] = blk;
+  }
+}
+
+// Grid update over the active node blocks: ContactHuang::generateRules
+// normalisation and applyRules (contact_huang.cpp:80-197), CartesianBox
+// (cartesian_box.cpp:73-85) and moveGrid (explicit_usl.cpp:233-264).
+// One thread per node; each node is owned by exactly one thread.
+template <int DIM>
+__global__ void __launch_bounds__(64) k_grid(Geom g, StepParams sp, GridBodies GB, ContactSet CS, const int64_t* list,
+                                             const unsigned long long* count) {
+  const int64_t cnt = (int64_t)*count;
+  const double dt = sp.dt;
+  for (int64_t e = blockIdx.x; e < cnt; e += gridDim.x) {
+    const int64_t blk = list[e];
+    const int li = threadIdx.x;
+    int i, j, k;
+    slot_ijk(g, blk, li, i, j, k);
+    if (i >= g.nn[0] || j >= g.nn[1] || k >= g.nn[2]) continue;
+    const int64_t s = blk * 64 + li;
+    for (int c = 0; c < CS.nc; c++) {
+      const NodesAcc& A1 = GB.acc[CS.b1[c]];
+      const NodesAcc& A2 = GB.acc[CS.b2[c]];
+      double n[3] = {0.0, 0.0, 0.0};
+      double nn = 0.0;
+#pragma unroll
+      for (int d = 0; d < DIM; d++) {
+        n[d] = A1.nrm[d][s];
+        nn += n[d] * n[d];
+      }
+      const double inv_norm = 1.0 / sqrt(nn);
+#pragma unroll
+      for (int d = 0; d < DIM; d++) n[d] *= inv_norm;
+      double fc[3] = {0.0, 0.0, 0.0};
+      const double m1 = A1.m[s], m2 = A2.m[s];
+      if (m1 > 0 && m2 > 0) {
+        double mv1[3], mv2[3], vcm[3];
+        double f1[3], f2[3];
+#pragma unroll
+        for (int d = 0; d < DIM; d++) {
+          f1[d] = A1.f[d][s];
+          f2[d] = A2.f[d][s];
+          if (sp.contact_spec == 1) {
+            mv1[d] = A1.mx[d][s] + dt * f1[d];
+            mv2[d] = A2.mx[d][s] + dt * f2[d];
+          } else {
+            mv1[d] = A1.mx[d][s];
+            mv2[d] = A2.mx[d][s];
+          }
+        }
+        const double inv_m12 = 1.0 / (m1 + m2);
+        const double inv_m1 = 1.0 / m1;
+        double test = 0.0;
+#pragma unroll
+        for (int d = 0; d < DIM; d++) {
+          vcm[d] = (mv1[d] + mv2[d]) * inv_m12;
+          test += (mv1[d] * inv_m1 - vcm[d]) * n[d];
+        }
+        if (test > 0) {
+          double vcm_n = 0.0, mv1_n = 0.0;
+#pragma unroll
+          for (int d = 0; d < DIM; d++) {
+            vcm_n += vcm[d] * n[d];
+            mv1_n += mv1[d] * n[d];
+          }
+          const double fn = m1 / dt * (vcm_n - mv1_n / m1);
+          const double m1dt = m1 / dt;
+          double s1[3], ss = 0.0;
+#pragma unroll
+          for (int d = 0; d < DIM; d++) {
+            s1[d] = m1dt * (vcm[d] - mv1[d] * inv_m1) - fn * n[d];
+            ss += s1[d] * s1[d];
+          }
+          const double ft = sqrt(ss);
+          if (ft != 0) {
+            const double inv = 1.0 / ft;
+#pragma unroll
+            for (int d = 0; d < DIM; d++) s1[d] *= inv;
+          }
+          const double a = (fn < 0.0) ? fn : 0.0;  // std::min(0.0, fn)
+          const double mufn = CS.mu[c] * fabs(fn);
+          const double b = (fabs(ft) < mufn) ? fabs(ft) : mufn;  // std::min(mu|fn|, |ft|)
+#pragma unroll
+          for (int d = 0; d < DIM; d++) {
+            fc[d] = a * n[d] + b * s1[d];
+            A1.f[d][s] = f1[d] + fc[d];
+            A2.f[d][s] = f2[d] - fc[d];
+          }
+        }
+      }
+      if (CS.normal_out[c] != nullptr) {
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+          CS.normal_out[c][3 * s + d] = (d < DIM) ? n[d] : 0.0;
+          CS.force_out[c][3 * s + d] = fc[d];
+        }
+      }
+    }
+    const bool on_face = (i == 0 || i == g.N[0] || j == 0 || j == g.N[1] || (DIM == 3 && (k == 0 || k == g.N[2])));
+    for (int b = 0; b < GB.nb; b++) {
+      const NodesAcc& A = GB.acc[b];
+      const NodesVel& V = GB.vel[b];
+      const double m = A.m[s];
+      double mx[3], f[3];
+#pragma unroll
+      for (int d = 0; d < DIM; d++) {
+        mx[d] = A.mx[d][s];
+        f[d] = A.f[d][s];
+      }
+      if (GB.has_boundary[b] && on_face) {
+#pragma unroll
+        for (int d = 0; d < DIM; d++) {
+          mx[d] = 0.0;
+          f[d] = 0.0;
+        }
+      }
+      double inv = 0.0;
+      if (m > 0) inv = 1.0 / m;
+#pragma unroll
+      for (int d = 0; d < DIM; d++) {
+        mx[d] = mx[d] + dt * f[d];
+        V.vt[d][s] = (m > 0) ? mx[d] * inv : 0.0;
+        V.dv[d][s] = (m > 0) ? (dt * f[d]) * inv : 0.0;
+      }
+      if (sp.keep_debug) {
+#pragma unroll
+        for (int d = 0; d < DIM; d++) {
+          A.mx[d][s] = mx[d];
+          A.f[d][s] = f[d];
+        }
+      } else {
+        A.m[s] = 0.0;
+#pragma unroll
+        for (int d = 0; d < DIM; d++) {
+          A.mx[d][s] = 0.0;
+          A.f[d][s] = 0.0;
+          if (A.nrm[0] != nullptr) A.nrm[d][s] = 0.0;
+        }
+      }
+    }
+  }
+}
+
+// Jaumann update of IsotropicLinearElasticity (isolin.cpp:62-74) on the 6
+// stored components. For symmetric T and W = -W^T, (T W)_ab = -(W T)_ba, so
+// W T - T W = (W T)_ab + (W T)_ba.
+template <int DIM>
+__device__ __forceinline__ void jaumann_update(const double L[3][3], double* s6, double G, double lambda, double dt) {
+  double D[3][3], W[3][3];
+#pragma unroll
+  for (int a = 0; a < 3; a++)
+#pragma unroll
+    for (int b = 0; b < 3; b++) {
+      D[a][b] = 0.5 * (L[a][b] + L[b][a]);
+      W[a][b] = 0.5 * (L[a][b] - L[b][a]);
+    }
+  const double trD = D[0][0] + D[1][1] + D[2][2];
+  const double T[3][3] = {{s6[0], s6[3], s6[5]}, {s6[3], s6[1], s6[4]}, {s6[5], s6[4], s6[2]}};
+  double WT[3][3];
+#pragma unroll
+  for (int a = 0; a < 3; a++)
+#pragma unroll
+    for (int b = 0; b < 3; b++) WT[a][b] = W[a][0] * T[0][b] + W[a][1] * T[1][b] + W[a][2] * T[2][b];
+  const double twoG = 2.0 * G;
+  const double ltr = lambda * trD;
+  const int ia[6] = {0, 1, 2, 0, 1, 0};
+  const int ib[6] = {0, 1, 2, 1, 2, 2};
+#pragma unroll
+  for (int c = 0; c < 6; c++) {
+    const int a = ia[c], b = ib[c];
+    const double rate = ((twoG * D[a][b] + (a == b ? ltr : 0.0)) + WT[a][b]) + WT[b][a];
+    s6[c] = s6[c] + dt * rate;
+  }
+}
+
+// G2P: movePoints (explicit_usl.cpp:266-300), calculateStrainRate
+// (302-330), updateDensity (332-345) and updateStress (347-355).
+template <int DIM>
+__global__ void __launch_bounds__(256) k_g2p(Geom g, StepParams sp, PointsDev P, NodesVel V, MaterialParams mat, int* err) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const double dt = sp.dt;
+  for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < P.n; p += stride) {
+    if (!P.active[p]) continue;
+    double x[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int d = 0; d < DIM; d++) x[d] = P.x[d][p];
+    PointMap pm;
+    const int st = build_map<DIM>(g, sp.cpdi, x, P.ext[p], pm, err);
+    double du[3] = {0.0, 0.0, 0.0}, dvel[3] = {0.0, 0.0, 0.0};
+    double L[3][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};
+    if (st > 0) {
+      const AxisMap& X = pm.ax[0];
+      const AxisMap& Y = pm.ax[1];
+      const int span2 = (DIM == 3) ? pm.ax[2].span : 1;
+      for (int k2 = 0; k2 < span2; k2++) {
+        const double wz = (DIM == 3) ? pm.ax[2].W[k2] : 1.0;
+        const double gz = (DIM == 3) ? pm.ax[2].G[k2] : 0.0;
+        for (int k1 = 0; k1 < Y.span; k1++) {
+          for (int k0 = 0; k0 < X.span; k0++) {
+            const double wxy = X.W[k0] * Y.W[k1];
+            const double S = pm.sS * (wxy * wz);
+            double gr[3];
+            gr[0] = pm.sG * (X.G[k0] * Y.W[k1] * wz);
+            gr[1] = pm.sG * (X.W[k0] * Y.G[k1] * wz);
+            gr[2] = (DIM == 3) ? pm.sG * (wxy * gz) : 0.0;
+            const int64_t s = node_slot(g, X.base + k0, Y.base + k1, DIM == 3 ? pm.ax[2].base + k2 : 0);
+            double vt[3];
+#pragma unroll
+            for (int d = 0; d < DIM; d++) {
+              vt[d] = V.vt[d][s];
+              du[d] += S * (dt * vt[d]);
+              dvel[d] += S * V.dv[d][s];
+            }
+#pragma unroll
+            for (int a = 0; a < DIM; a++)
+#pragma unroll
+              for (int b = 0; b < DIM; b++) L[a][b] += vt[a] * gr[b];
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int d = 0; d < DIM; d++) {
+      P.x[d][p] = x[d] + du[d];
+      P.u[d][p] = P.u[d][p] + du[d];
+      P.v[d][p] = P.v[d][p] + dvel[d];
+    }
+    P.vol[p] = P.vol[p] * exp(dt * (L[0][0] + L[1][1] + L[2][2]));
+    if (mat.has_material) {
+      double s6[6];
+#pragma unroll
+      for (int c = 0; c < 6; c++) s6[c] = P.s[c][p];
+      jaumann_update<DIM>(L, s6, mat.G, mat.lambda, dt);
+#pragma unroll
+      for (int c = 0; c < 6; c++) P.s[c][p] = s6[c];
+    }
+    if (P.L != nullptr) {
+#pragma unroll
+      for (int a = 0; a < 3; a++)
+#pragma unroll
+        for (int b = 0; b < 3; b++) P.L[9 * p + 3 * a + b] = L[a][b];
+    }
+  }
+}
+
+// Exact triplet export (mpmgpu_dump_map).
+template <int DIM>
+__global__ void k_export_map(Geom g, int cpdi, PointsDev P, int32_t* node_out, double* s_out, double* g_out) {
+  constexpr int cp = 1 << DIM;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < P.n; p += stride) {
+    const int64_t slot = p * cp * cp;
+    if (!P.active[p]) {
+      for (int k = 0; k < cp * cp; k++) node_out[slot + k] = -1;
+      continue;
+    }
+    double x[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int d = 0; d < DIM; d++) x[d] = P.x[d][p];
+    if (export_point<DIM>(g, cpdi, x, P.ext[p], node_out, s_out, g_out, slot) < 0) P.active[p] = 0;
+  }
+}
+
+}  // namespace mpmb200

@@ -1,0 +1,181 @@
+"""ctypes binding of the C ABI in include/mpm_b200.h, and ``GPUExplicitUSL``,
+the B200 replacement for mpm_3d's ExplicitUSL solver on a ``Case``.
+
+The binding loads ``mpm_3d_b200/lib/libmpm_b200.so`` and fails loudly when it
+is missing: there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Dict, Optional, Tuple
+
+import numpy as np
+
+from . import inputs
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libmpm_b200.so")
+
+MODES = {"fp64": 0, "fp64_deterministic": 1, "mixed": 2}
+POINT_FIELDS = {"x": (0, 3), "u": (1, 3), "x_t": (2, 3), "mx_t": (3, 3), "b": (4, 3), "L": (5, 9), "T": (6, 9),
+                "m": (7, 1), "v": (8, 1), "extent": (9, 1), "active": (10, 1)}
+NODE_FIELDS = {"m": (0, 1), "mx_t": (1, 3), "f": (2, 3), "x_t": (3, 3), "u": (4, 3), "diff_x_t": (5, 3)}
+CONTACT_FIELDS = {"normal": (0, 3), "force": (1, 3)}
+
+
+class MpmGpuError(RuntimeError):
+    pass
+
+
+class _Config(ctypes.Structure):
+    _fields_ = [("dim", ctypes.c_int), ("L", ctypes.c_double * 3), ("N", ctypes.c_int * 3), ("dt", ctypes.c_double),
+                ("cpdi_spec", ctypes.c_int), ("contact_spec", ctypes.c_int), ("mode", ctypes.c_int),
+                ("device", ctypes.c_int), ("keep_debug", ctypes.c_int)]
+
+
+class _BodyDesc(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int64), ("m", ctypes.c_void_p), ("v", ctypes.c_void_p), ("x", ctypes.c_void_p),
+                ("x_t", ctypes.c_void_p), ("active", ctypes.c_void_p), ("has_material", ctypes.c_int),
+                ("E", ctypes.c_double), ("nu", ctypes.c_double), ("has_boundary", ctypes.c_int)]
+
+
+_lib = None
+
+
+def load() -> ctypes.CDLL:
+    """Loads the CUDA library; raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with `python -m mpm_3d_b200.build` "
+                          "(there is no CPU fallback)")
+    lib = ctypes.CDLL(LIB_PATH)
+    vp = ctypes.c_void_p
+    lib.mpmgpu_status_string.restype = ctypes.c_char_p
+    lib.mpmgpu_status_string.argtypes = [ctypes.c_int]
+    lib.mpmgpu_last_error.restype = ctypes.c_char_p
+    lib.mpmgpu_last_error.argtypes = [vp]
+    lib.mpmgpu_create.argtypes = [ctypes.POINTER(_Config), ctypes.POINTER(vp)]
+    lib.mpmgpu_add_body.argtypes = [vp, ctypes.POINTER(_BodyDesc), ctypes.POINTER(ctypes.c_int)]
+    lib.mpmgpu_add_contact.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.POINTER(ctypes.c_int)]
+    lib.mpmgpu_set_gravity.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+    lib.mpmgpu_step.argtypes = [vp, ctypes.c_int]
+    lib.mpmgpu_synchronize.argtypes = [vp]
+    for fn in ("mpmgpu_download_points", "mpmgpu_download_nodes", "mpmgpu_download_contact"):
+        getattr(lib, fn).argtypes = [vp, ctypes.c_int, ctypes.c_int, vp]
+    lib.mpmgpu_dump_map.argtypes = [vp, ctypes.c_int, vp, vp, vp, vp, ctypes.POINTER(ctypes.c_int64)]
+    lib.mpmgpu_sizes.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)]
+    lib.mpmgpu_launch_count.restype = ctypes.c_int64
+    lib.mpmgpu_launch_count.argtypes = [vp]
+    lib.mpmgpu_destroy.argtypes = [vp]
+    _lib = lib
+    return lib
+
+
+def _ptr(a: np.ndarray) -> ctypes.c_void_p:
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+class GPUExplicitUSL:
+    """ExplicitUSL on the GPU for one ``inputs.Case`` (the Job's grid, bodies,
+    contacts and driver gravity), with the reference's step/frame surface:
+    ``step(n)`` advances n steps; ``points``/``nodes``/``contact`` read fields
+    in the reference's layout (AoS, original point order, reference node ids).
+    """
+
+    def __init__(self, case: inputs.Case, mode: str = "fp64", keep_debug: bool = False, device: int = 0):
+        self.lib = load()
+        self.case = case
+        cfg = _Config()
+        cfg.dim = case.dim
+        for d in range(3):
+            cfg.L[d] = case.L[d] if d < case.dim else 0.0
+            cfg.N[d] = case.N[d] if d < case.dim else 0
+        cfg.dt = case.dt
+        cfg.cpdi_spec = case.cpdi
+        cfg.contact_spec = case.contact_spec
+        cfg.mode = MODES[mode]
+        cfg.device = device
+        cfg.keep_debug = int(keep_debug)
+        h = ctypes.c_void_p()
+        self._check(self.lib.mpmgpu_create(ctypes.byref(cfg), ctypes.byref(h)), None)
+        self.h = h
+        for body in case.bodies:
+            arrs = dict(m=np.ascontiguousarray(body.m, np.float64), v=np.ascontiguousarray(body.v, np.float64),
+                        x=np.ascontiguousarray(body.x, np.float64), x_t=np.ascontiguousarray(body.x_t, np.float64),
+                        active=np.ascontiguousarray(body.active, np.int32))
+            desc = _BodyDesc(body.n, _ptr(arrs["m"]).value, _ptr(arrs["v"]).value, _ptr(arrs["x"]).value,
+                             _ptr(arrs["x_t"]).value, _ptr(arrs["active"]).value, int(body.material), body.E, body.nu,
+                             int(body.boundary))
+            bid = ctypes.c_int()
+            self._check(self.lib.mpmgpu_add_body(self.h, ctypes.byref(desc), ctypes.byref(bid)))
+        for c in case.contacts:
+            cid = ctypes.c_int()
+            self._check(self.lib.mpmgpu_add_contact(self.h, c.b1, c.b2, c.mu, ctypes.byref(cid)))
+        if case.gravity is not None:
+            g = (ctypes.c_double * 3)(*(list(case.gravity) + [0.0] * (3 - len(case.gravity))))
+            self._check(self.lib.mpmgpu_set_gravity(self.h, 1, g))
+        n_nodes = ctypes.c_int64()
+        self._check(self.lib.mpmgpu_sizes(self.h, 0, None, ctypes.byref(n_nodes)))
+        self.n_nodes = n_nodes.value
+
+    def _check(self, status: int, h=0):
+        if status != 0:
+            hh = self.h if h == 0 else h
+            msg = self.lib.mpmgpu_status_string(status).decode()
+            detail = self.lib.mpmgpu_last_error(hh).decode() if hh else ""
+            raise MpmGpuError(f"{msg}: {detail}")
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.mpmgpu_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def step(self, n: int = 1):
+        self._check(self.lib.mpmgpu_step(self.h, n))
+
+    def synchronize(self):
+        self._check(self.lib.mpmgpu_synchronize(self.h))
+
+    def launches(self) -> int:
+        return int(self.lib.mpmgpu_launch_count(self.h))
+
+    def points(self, b: int, name: str) -> np.ndarray:
+        fid, w = POINT_FIELDS[name]
+        out = np.zeros((self.case.bodies[b].n, w))
+        self._check(self.lib.mpmgpu_download_points(self.h, b, fid, _ptr(out)))
+        return out
+
+    def nodes(self, b: int, name: str) -> np.ndarray:
+        fid, w = NODE_FIELDS[name]
+        out = np.zeros((self.n_nodes, w))
+        self._check(self.lib.mpmgpu_download_nodes(self.h, b, fid, _ptr(out)))
+        return out
+
+    def contact(self, c: int, name: str) -> np.ndarray:
+        fid, w = CONTACT_FIELDS[name]
+        out = np.zeros((self.n_nodes, w))
+        self._check(self.lib.mpmgpu_download_contact(self.h, c, fid, _ptr(out)))
+        return out
+
+    def map(self, b: int) -> Tuple[np.ndarray, np.ndarray, np.ndarray, np.ndarray]:
+        """Exact S / gradS triplets of body b at the current positions, in the
+        reference's order: (node, point, S value, gradient (k,3))."""
+        cnt = ctypes.c_int64()
+        self._check(self.lib.mpmgpu_dump_map(self.h, b, None, None, None, None, ctypes.byref(cnt)))
+        n = cnt.value
+        node = np.zeros(n, np.int32)
+        pt = np.zeros(n, np.int32)
+        val = np.zeros(n)
+        grad = np.zeros((n, 3))
+        self._check(self.lib.mpmgpu_dump_map(self.h, b, _ptr(node), _ptr(pt), _ptr(val), _ptr(grad),
+                                             ctypes.byref(cnt)))
+        return node, pt, val, grad

@@ -56,11 +56,12 @@ class _JobBase:
         return getattr(self.lib, self._prefix + fname)
 
     def _field(self, fname, b, name, count, width):
-        out = np.zeros((count, width), dtype=np.float64)
+        # the C side writes `got` packed doubles per entry (got <= width)
+        out = np.zeros(count * width, dtype=np.float64)
         got = self._f(fname)(self.h, b, name.encode(), _ptr(out))
         if got < 0:
             raise KeyError(name)
-        return out[:, :got] if got != width else out
+        return out[:count * got].reshape(count, got).copy()
 
 
 class ReferenceJob(_JobBase):
