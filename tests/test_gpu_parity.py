@@ -2,16 +2,19 @@
 
 The oracle is the C restatement in oracle/mpm_oracle.c, which is bit-exact
 with the reference's own sources (tests/test_oracle.py pins it). Tolerance:
-max |gpu - oracle| / max |oracle| <= 1e-10 per field after every step; the
-S / gradS connectivity from mpmgpu_dump_map must be bit-identical.
+max |gpu - oracle| / max(max |oracle|, physical floor) <= 1e-10 per field
+after every step (util.field_floor); the S / gradS connectivity of
+mpmgpu_dump_map must be bit-identical for identical positions.
 """
+import copy
+
 import numpy as np
 import pytest
 
 import bridge
 from mpm_3d_b200 import inputs
 from mpm_3d_b200.native import GPUExplicitUSL
-from util import FP64_TOL, assert_close, bits_equal
+from util import FP64_TOL, assert_close, bits_equal, field_floor
 
 pytestmark = pytest.mark.gpu
 
@@ -43,25 +46,39 @@ def _wall_exit_2d():
     return c
 
 
+def _spinning_block_2d():
+    """Block drop with a rigid spin, so stress and velocity gradient are
+    physical from the first step (free fall alone leaves them at round-off)."""
+    c = inputs.block_drop_2d()
+    b = c.bodies[0]
+    cx = b.x[:, :2].mean(0)
+    b.x_t[:, 0] = -(b.x[:, 1] - cx[1]) * 20.0
+    b.x_t[:, 1] = (b.x[:, 0] - cx[0]) * 20.0 - 1.0
+    c.name = "spinning_block_2d"
+    return c
+
+
 CASES = {
     "wall_exit_2d": (_wall_exit_2d, 25),
     "block_drop_2d": (inputs.block_drop_2d, 120),
+    "spinning_block_2d": (_spinning_block_2d, 120),
     "block_drop_2d_cpdi_off": (_cpdi_off_2d, 40),
     "collision_2d": (lambda: inputs.two_body_collision_2d(20, steps=60), 60),
     "collision_3d_touching": (lambda: inputs.two_body_collision_3d(16, steps=15, gap=0.01), 15),
     "collision_3d_explicit": (_explicit_contact_3d, 8),
     "column_collapse_s16": (lambda: inputs.column_collapse_3d(scale=16, steps=15), 15),
-    "collision_3d_zero_gravity": (lambda: inputs.two_body_collision_3d(16, steps=8, gap=0.01, gravity=(0.0, 0.0, 0.0)), 8),
+    "collision_3d_zero_gravity": (lambda: inputs.two_body_collision_3d(16, steps=8, gap=0.01, gravity=(0.0, 0.0, 0.0)),
+                                  8),
 }
 
 
-def _ensure_oracle():
+@pytest.fixture(scope="module", autouse=True)
+def restated_lib():
     bridge.build_restated()
 
 
 @pytest.mark.parametrize("name", sorted(CASES))
 def test_step_parity(name):
-    _ensure_oracle()
     make, steps = CASES[name]
     case = make()
     ref = bridge.RestatedJob(case)
@@ -72,7 +89,8 @@ def test_step_parity(name):
         gpu.step(1)
         for b in range(len(case.bodies)):
             for f in POINT_FIELDS:
-                e = assert_close(gpu.points(b, f), ref.points(b, f), FP64_TOL, f"{name} step {s} body {b} point {f}")
+                e = assert_close(gpu.points(b, f), ref.points(b, f), FP64_TOL, f"{name} step {s} body {b} point {f}",
+                                 field_floor(case, f))
                 worst[f] = max(worst.get(f, 0.0), e)
             for f in NODE_FIELDS:
                 e = assert_close(gpu.nodes(b, f), ref.nodes(b, f), FP64_TOL, f"{name} step {s} body {b} node {f}")
@@ -88,23 +106,83 @@ def test_step_parity(name):
     print(name, {k: f"{v:.1e}" for k, v in worst.items()})
 
 
+def _assert_same_map(gpu, ref, b, what):
+    node, pt, val, grad = gpu.map(b)
+    rn, rp, rv = ref.map(b)
+    gn, gp, gg = ref.grad_map(b)
+    assert np.array_equal(node, rn) and np.array_equal(pt, rp), f"{what}: S connectivity differs"
+    assert bits_equal(val, rv), f"{what}: S values differ"
+    assert np.array_equal(node, gn) and np.array_equal(pt, gp), f"{what}: gradS connectivity differs"
+    assert bits_equal(grad, gg), f"{what}: gradS values differ"
+    return len(node)
+
+
+def _with_positions(case, gpu):
+    """A copy of the case whose points sit where the GPU has moved them
+    (volumes stay the initial ones: extent is never updated)."""
+    moved = copy.deepcopy(case)
+    for b, body in enumerate(moved.bodies):
+        body.x = gpu.points(b, "x").copy()
+        body.active = gpu.points(b, "active")[:, 0].astype(np.int32)
+    return moved
+
+
 @pytest.mark.parametrize("name", sorted(CASES))
 def test_map_bit_exact(name):
-    _ensure_oracle()
     make, steps = CASES[name]
     case = make()
-    ref = bridge.RestatedJob(case)
     gpu = GPUExplicitUSL(case, keep_debug=True)
-    for s in (0, min(steps, 5)):
-        if s:
-            ref.step(s)
-            gpu.step(s)
-        ref.build_map()
-        for b in range(len(case.bodies)):
-            node, pt, val, grad = gpu.map(b)
-            rn, rp, rv = ref.map(b)
-            gn, gp, gg = ref.grad_map(b)
-            assert np.array_equal(node, rn) and np.array_equal(pt, rp), f"{name}: S connectivity differs"
-            assert bits_equal(val, rv), f"{name}: S values differ"
-            assert np.array_equal(node, gn) and np.array_equal(pt, gp), f"{name}: gradS connectivity differs"
-            assert bits_equal(grad, gg), f"{name}: gradS values differ"
+    ref = bridge.RestatedJob(case)
+    ref.build_map()
+    for b in range(len(case.bodies)):
+        _assert_same_map(gpu, ref, b, f"{name} initial")
+    gpu.step(min(steps, 5))
+    moved = _with_positions(case, gpu)
+    ref2 = bridge.RestatedJob(moved)
+    ref2.build_map()
+    for b in range(len(case.bodies)):
+        _assert_same_map(gpu, ref2, b, f"{name} after steps")
+
+
+def _edge_case_2d(cpdi):
+    """Points on special positions of a 20x20 grid on 1x1 m: exactly on a
+    node (0/0 gradient of the point-sampled map), a hi corner exactly on the
+    upper wall (no element for that corner), a point exactly on the wall
+    (no element at all), a point outside (deactivated) and a near-wall point
+    whose corners leave the domain (point-sampled fallback)."""
+    h = 0.05
+    vol = (h / 2) ** 2
+    a = 0.5 * (0.5 * np.sqrt(vol))
+    x_corner_at_wall = 1.0 - a
+    while x_corner_at_wall + a < 1.0:
+        x_corner_at_wall = np.nextafter(x_corner_at_wall, 2.0)
+    while x_corner_at_wall + a > 1.0:
+        x_corner_at_wall = np.nextafter(x_corner_at_wall, 0.0)
+    pts = [
+        (0.25, 0.25),                 # on a node
+        (x_corner_at_wall, 0.4),      # hi corner exactly at x = L
+        (1.0, 0.6),                   # on the wall
+        (1.2, 0.3),                   # outside
+        (0.003, 0.7),                 # corners cross x = 0
+        (0.5 + 1e-17, 0.5),           # at a node within rounding
+        (0.3125, 0.4375),             # regular interior point
+    ]
+    x = np.zeros((len(pts), 3))
+    x[:, :2] = np.array(pts)
+    n = len(pts)
+    body = inputs.Body(name="edge", m=np.full(n, 1000 * vol), v=np.full(n, vol), x=x, x_t=np.zeros((n, 3)),
+                       active=np.ones(n, np.int32), E=1e5, nu=0.3)
+    return inputs.Case(name=f"edge_2d_cpdi{cpdi}", dim=2, L=(1.0, 1.0), N=(20, 20), dt=1e-4, steps=1,
+                       bodies=[body], cpdi=cpdi)
+
+
+@pytest.mark.parametrize("cpdi", [0, 1])
+def test_map_edge_positions(cpdi):
+    case = _edge_case_2d(cpdi)
+    gpu = GPUExplicitUSL(case, keep_debug=True)
+    ref = bridge.RestatedJob(case)
+    ref.build_map()
+    count = _assert_same_map(gpu, ref, 0, f"edge cpdi={cpdi}")
+    assert count > 0
+    assert np.array_equal(gpu.points(0, "active"), ref.points(0, "active"))
+    assert ref.points(0, "active")[3, 0] == 0

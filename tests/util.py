@@ -7,20 +7,28 @@ import numpy as np
 FP64_TOL = 1e-10
 
 
-def rel_err(got: np.ndarray, ref: np.ndarray) -> float:
+def rel_err(got: np.ndarray, ref: np.ndarray, floor: float = 0.0) -> float:
+    """max |got - ref| / max(max |ref|, floor).
+
+    ``floor`` is the field's physical scale for fields that can be pure
+    round-off in the reference (the stress and velocity gradient of a block
+    in free fall are ~1e-12 noise): differences far below that scale are
+    summation-order noise, not disagreement.
+    """
     got = np.asarray(got, dtype=np.float64)
     ref = np.asarray(ref, dtype=np.float64)
     if got.shape != ref.shape:
         raise AssertionError(f"shape {got.shape} != {ref.shape}")
     scale = float(np.max(np.abs(ref))) if ref.size else 0.0
+    scale = max(scale, floor)
     diff = float(np.max(np.abs(got - ref))) if ref.size else 0.0
     if scale == 0.0:
         return diff
     return diff / scale
 
 
-def assert_close(got, ref, tol, what):
-    e = rel_err(got, ref)
+def assert_close(got, ref, tol, what, floor: float = 0.0):
+    e = rel_err(got, ref, floor)
     assert e <= tol, f"{what}: relative error {e:.3e} > {tol:.1e}"
     return e
 
@@ -36,3 +44,14 @@ def bits_equal(a, b) -> bool:
     if not np.array_equal(na, nb):
         return False
     return bool(np.array_equal(a[~na].view(np.int64), b[~nb].view(np.int64)))
+
+
+def field_floor(case, field: str) -> float:
+    """Physical scale of a field for ``rel_err``: the velocity scale is the
+    largest initial speed (at least 1 m/s); the velocity-gradient scale is
+    that speed over a cell; the stress scale is one step of elastic stress
+    at that gradient (E * dt * v / h)."""
+    v0 = max(1.0, max(float(np.abs(b.x_t).max()) for b in case.bodies))
+    h = min(case.h)
+    E = max(b.E for b in case.bodies)
+    return {"L": v0 / h, "T": E * case.dt * v0 / h, "x_t": v0, "u": h, "x": min(case.L)}.get(field, 0.0)
