@@ -69,6 +69,8 @@ typedef struct {
   int device;       /* CUDA device ordinal */
   int keep_debug;   /* 1: keep L, nodal m/mx_t/f and contact forces
                        readable after each step (costs extra traffic) */
+  int sort_interval;/* steps between re-binning the points by cell
+                       (0 = default 32); results do not depend on it */
 } mpmgpu_config;
 
 /* One DefaultBody: its points (DefaultPoints::readFromFile columns,
@@ -170,6 +172,18 @@ mpmgpu_status mpmgpu_sizes(const mpmgpu_handle* h, int body, int64_t* n_points, 
 
 /* Number of kernel launches issued since creation (for launch accounting). */
 int64_t mpmgpu_launch_count(const mpmgpu_handle* h);
+
+/* The CUDA stream (cudaStream_t) all of the handle's work is queued on, so
+ * a caller can record its own events around mpmgpu_step. */
+void* mpmgpu_stream(const mpmgpu_handle* h);
+
+/* Per-stage device time accounting with CUDA events recorded on the
+ * handle's stream around every launch of a stage. enable != 0 starts (and
+ * resets) it, 0 stops it. Stages: 0 fused gather/scatter kernel, 1 grid
+ * update, 2 active-block compaction, 3 point re-binning. */
+mpmgpu_status mpmgpu_profile(mpmgpu_handle* h, int enable);
+/* Waits for the stream, then reports launches and total milliseconds of a stage. */
+mpmgpu_status mpmgpu_profile_read(mpmgpu_handle* h, int stage, int64_t* launches, double* total_ms);
 
 mpmgpu_status mpmgpu_destroy(mpmgpu_handle* h);
 

@@ -1,4 +1,14 @@
 // Host side of the C ABI declared in include/mpm_b200.h.
+//
+// One step on the device (FP64 form):
+//   compact   active node blocks flagged by the last scatter -> work list
+//   grid      body force, contact, boundary, moveGrid on the active blocks
+//   g2p2g     per bin of points: gather + point update (this step), map
+//             build + scatter at the new positions (next step)
+// plus, every sort_interval steps, a re-binning of the points. Before the
+// first step a scatter-only pass of the fused kernel builds the first
+// nodal sums.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -6,7 +16,9 @@
 #include <vector>
 
 #include "../../include/mpm_b200.h"
+#include "fused.cuh"
 #include "kernels_fp64.cuh"
+#include "sort.cuh"
 
 using namespace mpmb200;
 
@@ -14,12 +26,23 @@ namespace {
 
 struct BodyDev {
   int64_t n = 0;
-  PointsDev P{};
+  PointsDev P{};      // current storage order
+  PointsDev Palt{};   // second buffer for re-binning
   NodesAcc A{};
   NodesVel V{};
+  NodesAcc snap{};    // debug copies (m, mx, f) or null
   MaterialParams mat{};
   int has_boundary = 0;
   bool needs_normal = false;
+  // binning
+  int32_t* key = nullptr;
+  int32_t* rank = nullptr;
+  int32_t* cell_count = nullptr;  // nbins * cells_per_bin + 1
+  int32_t* bin_start = nullptr;   // nbins + 2
+  int32_t* work_bin = nullptr;
+  int32_t* work_start = nullptr;
+  int32_t* work_end = nullptr;
+  int32_t* nwork = nullptr;
 };
 
 }  // namespace
@@ -27,6 +50,8 @@ struct BodyDev {
 struct mpmgpu_handle {
   mpmgpu_config cfg{};
   Geom g{};
+  MapConst mc{};
+  BinGeom bg{};
   StepParams sp{};
   cudaStream_t stream = nullptr;
   std::vector<BodyDev> bodies;
@@ -36,11 +61,23 @@ struct mpmgpu_handle {
   unsigned long long* count = nullptr;
   uint8_t* was_active = nullptr;
   int* err = nullptr;
+  unsigned long long* drift = nullptr;
   std::vector<void*> allocs;
   std::string last_error;
   int64_t launches = 0;
   int sm_count = 148;
   bool stepped = false;
+  bool primed = false;
+  int steps_since_sort = 0;
+  int sort_interval = 32;
+  int fused_blocks = 0;
+  // per-stage event timing (mpmgpu_profile)
+  static constexpr int kStages = 4;
+  bool profiling = false;
+  std::vector<cudaEvent_t> event_pool;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending[kStages];
+  int64_t stage_launches[kStages] = {0, 0, 0, 0};
+  double stage_ms[kStages] = {0.0, 0.0, 0.0, 0.0};
 };
 
 namespace {
@@ -50,31 +87,30 @@ mpmgpu_status fail(mpmgpu_handle* h, mpmgpu_status s, const std::string& msg) {
   return s;
 }
 
-#define CUDA_TRY(h, expr)                                                                               \
-  do {                                                                                                  \
-    cudaError_t e_ = (expr);                                                                            \
+#define CUDA_TRY(h, expr)                                                                                     \
+  do {                                                                                                        \
+    cudaError_t e_ = (expr);                                                                                  \
     if (e_ != cudaSuccess) return fail((h), MPMGPU_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(e_)); \
   } while (0)
 
+#define TRY(expr)                   \
+  do {                              \
+    mpmgpu_status s_ = (expr);      \
+    if (s_ != MPMGPU_OK) return s_; \
+  } while (0)
+
 template <typename T>
-mpmgpu_status dev_alloc(mpmgpu_handle* h, T** p, size_t count, bool zero = true) {
+mpmgpu_status dev_alloc(mpmgpu_handle* h, T** p, size_t count) {
   void* q = nullptr;
-  cudaError_t e = cudaMalloc(&q, count * sizeof(T) > 0 ? count * sizeof(T) : 1);
+  const size_t bytes = std::max<size_t>(count * sizeof(T), 16);
+  cudaError_t e = cudaMalloc(&q, bytes);
   if (e != cudaSuccess) return fail(h, MPMGPU_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
   h->allocs.push_back(q);
-  if (zero) {
-    e = cudaMemsetAsync(q, 0, count * sizeof(T), h->stream);
-    if (e != cudaSuccess) return fail(h, MPMGPU_ERR_CUDA, std::string("cudaMemset: ") + cudaGetErrorString(e));
-  }
+  e = cudaMemsetAsync(q, 0, bytes, h->stream);
+  if (e != cudaSuccess) return fail(h, MPMGPU_ERR_CUDA, std::string("cudaMemset: ") + cudaGetErrorString(e));
   *p = static_cast<T*>(q);
   return MPMGPU_OK;
 }
-
-#define TRY(expr)                       \
-  do {                                  \
-    mpmgpu_status s_ = (expr);          \
-    if (s_ != MPMGPU_OK) return s_;     \
-  } while (0)
 
 int grid_blocks(const mpmgpu_handle* h, int64_t work, int threads) {
   int64_t b = (work + threads - 1) / threads;
@@ -91,23 +127,198 @@ mpmgpu_status check_launch(mpmgpu_handle* h, const char* what) {
   return MPMGPU_OK;
 }
 
-// Host copy of a strided upload: column d of an AoS array of width w.
+// Stage timing: records a start event before and a stop event after the
+// stage's launches when profiling is on.
+struct StageTimer {
+  mpmgpu_handle* h;
+  int stage;
+  cudaEvent_t start = nullptr;
+  StageTimer(mpmgpu_handle* hh, int s) : h(hh), stage(s) {
+    if (!h->profiling) return;
+    start = take_event();
+    cudaEventRecord(start, h->stream);
+  }
+  ~StageTimer() {
+    if (!h->profiling || !start) return;
+    cudaEvent_t stop = take_event();
+    cudaEventRecord(stop, h->stream);
+    h->pending[stage].push_back({start, stop});
+  }
+  cudaEvent_t take_event() {
+    cudaEvent_t e = nullptr;
+    if (!h->event_pool.empty()) {
+      e = h->event_pool.back();
+      h->event_pool.pop_back();
+    } else {
+      cudaEventCreate(&e);
+    }
+    return e;
+  }
+};
+
 std::vector<double> column(const double* aos, int64_t n, int w, int d) {
   std::vector<double> out((size_t)n);
   for (int64_t i = 0; i < n; i++) out[(size_t)i] = aos[i * w + d];
   return out;
 }
 
-mpmgpu_status upload(mpmgpu_handle* h, double* dst, const std::vector<double>& src) {
-  CUDA_TRY(h, cudaMemcpyAsync(dst, src.data(), src.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+template <typename T>
+mpmgpu_status upload(mpmgpu_handle* h, T* dst, const std::vector<T>& src) {
+  if (src.empty()) return MPMGPU_OK;
+  CUDA_TRY(h, cudaMemcpyAsync(dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice, h->stream));
   CUDA_TRY(h, cudaStreamSynchronize(h->stream));
   return MPMGPU_OK;
 }
 
-mpmgpu_status download(mpmgpu_handle* h, std::vector<double>& dst, const double* src, size_t n) {
+template <typename T>
+mpmgpu_status download(mpmgpu_handle* h, std::vector<T>& dst, const T* src, size_t n) {
   dst.resize(n);
-  CUDA_TRY(h, cudaMemcpyAsync(dst.data(), src, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  if (n == 0) return MPMGPU_OK;
+  CUDA_TRY(h, cudaMemcpyAsync(dst.data(), src, n * sizeof(T), cudaMemcpyDeviceToHost, h->stream));
   CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  return MPMGPU_OK;
+}
+
+mpmgpu_status alloc_points(mpmgpu_handle* h, PointsDev& P, int64_t n, bool with_L) {
+  P.n = n;
+  for (int d = 0; d < 3; d++) {
+    TRY(dev_alloc(h, &P.x[d], (size_t)n));
+    TRY(dev_alloc(h, &P.v[d], (size_t)n));
+    TRY(dev_alloc(h, &P.u[d], (size_t)n));
+  }
+  for (int c = 0; c < 6; c++) TRY(dev_alloc(h, &P.s[c], (size_t)n));
+  TRY(dev_alloc(h, &P.vol, (size_t)n));
+  TRY(dev_alloc(h, &P.m, (size_t)n));
+  TRY(dev_alloc(h, &P.ext, (size_t)n));
+  TRY(dev_alloc(h, &P.active, (size_t)n));
+  TRY(dev_alloc(h, &P.pid, (size_t)n));
+  P.L = nullptr;
+  if (with_L) TRY(dev_alloc(h, &P.L, (size_t)n * 9));
+  return MPMGPU_OK;
+}
+
+PointArrays point_arrays(const PointsDev& P) {
+  PointArrays a{};
+  a.nf = 0;
+  for (int d = 0; d < 3; d++) a.f[a.nf++] = P.x[d];
+  for (int d = 0; d < 3; d++) a.f[a.nf++] = P.v[d];
+  for (int d = 0; d < 3; d++) a.f[a.nf++] = P.u[d];
+  for (int c = 0; c < 6; c++) a.f[a.nf++] = P.s[c];
+  a.f[a.nf++] = P.vol;
+  a.f[a.nf++] = P.m;
+  a.f[a.nf++] = P.ext;
+  a.ni = 0;
+  a.i[a.ni++] = P.active;
+  a.i[a.ni++] = P.pid;
+  a.L9 = P.L;
+  return a;
+}
+
+// Re-bins the points of one body (counting sort by bin, rank-major within
+// bins) and rebuilds the work list of non-empty bins.
+template <int DIM>
+mpmgpu_status sort_body(mpmgpu_handle* h, BodyDev& B) {
+  cudaStream_t st = h->stream;
+  const BinGeom& bg = h->bg;
+  const int64_t ncells = (int64_t)bg.nbins * bg.cells_per_bin + 1;
+  CUDA_TRY(h, cudaMemsetAsync(B.cell_count, 0, ncells * sizeof(int32_t), st));
+  CUDA_TRY(h, cudaMemsetAsync(B.nwork, 0, sizeof(int32_t), st));
+  if (B.n > 0) {
+    k_sort_count<DIM><<<grid_blocks(h, B.n, 256), 256, 0, st>>>(h->g, bg, B.P, B.key, B.rank, B.cell_count);
+    TRY(check_launch(h, "k_sort_count"));
+  }
+  k_bin_totals<<<(bg.nbins + 1 + 255) / 256, 256, 0, st>>>(bg, B.cell_count, B.bin_start);
+  TRY(check_launch(h, "k_bin_totals"));
+  k_scan_small<<<1, 1024, 0, st>>>(B.bin_start, bg.nbins + 1, B.bin_start + bg.nbins + 1);
+  TRY(check_launch(h, "k_scan_small"));
+  if (B.n > 0) {
+    k_sort_scatter<<<grid_blocks(h, B.n, 256), 256, 0, st>>>(bg, B.n, B.key, B.rank, B.cell_count, B.bin_start,
+                                                             point_arrays(B.P), point_arrays(B.Palt));
+    TRY(check_launch(h, "k_sort_scatter"));
+    std::swap(B.P, B.Palt);
+  }
+  k_bin_work<<<(bg.nbins + 255) / 256, 256, 0, st>>>(bg, B.bin_start, B.work_bin, B.work_start, B.work_end, B.nwork);
+  TRY(check_launch(h, "k_bin_work"));
+  return MPMGPU_OK;
+}
+
+template <int DIM, int BB, bool NORMAL>
+mpmgpu_status launch_fused(mpmgpu_handle* h, BodyDev& B, int do_g2p, int do_p2g) {
+  FusedParams fp{};
+  fp.g = h->g;
+  fp.mc = h->mc;
+  fp.bg = h->bg;
+  fp.sp = h->sp;
+  fp.mat = B.mat;
+  fp.P = B.P;
+  fp.V = B.V;
+  fp.A = B.A;
+  fp.work_bin = B.work_bin;
+  fp.work_start = B.work_start;
+  fp.work_end = B.work_end;
+  fp.nwork = B.nwork;
+  fp.flags = h->flags;
+  fp.err = h->err;
+  fp.drift = h->drift;
+  fp.do_g2p = do_g2p;
+  fp.do_p2g = do_p2g;
+  const size_t smem = fused_smem_bytes<DIM, BB>(NORMAL);
+  static bool configured = false;
+  if (!configured) {
+    CUDA_TRY(h, cudaFuncSetAttribute(k_g2p2g<DIM, BB, NORMAL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    configured = true;
+  }
+  int per_sm = 0;
+  CUDA_TRY(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_g2p2g<DIM, BB, NORMAL>, 256, smem));
+  const int blocks = std::max(1, per_sm) * h->sm_count;
+  StageTimer timer(h, 0);
+  k_g2p2g<DIM, BB, NORMAL><<<blocks, 256, smem, h->stream>>>(fp);
+  return check_launch(h, "k_g2p2g");
+}
+
+template <int DIM>
+mpmgpu_status fused(mpmgpu_handle* h, BodyDev& B, int do_g2p, int do_p2g) {
+  constexpr int BB = DIM == 3 ? 4 : 8;
+  if (B.needs_normal) return launch_fused<DIM, BB, true>(h, B, do_g2p, do_p2g);
+  return launch_fused<DIM, BB, false>(h, B, do_g2p, do_p2g);
+}
+
+template <int DIM>
+mpmgpu_status step_once(mpmgpu_handle* h) {
+  const Geom& g = h->g;
+  cudaStream_t st = h->stream;
+  if (!h->primed) {
+    for (BodyDev& B : h->bodies) TRY(sort_body<DIM>(h, B));
+    for (BodyDev& B : h->bodies) TRY(fused<DIM>(h, B, 0, 1));
+    h->primed = true;
+    h->steps_since_sort = 0;
+  }
+  GridBodies GB{};
+  GB.nb = (int)h->bodies.size();
+  for (size_t b = 0; b < h->bodies.size(); b++) {
+    GB.acc[b] = h->bodies[b].A;
+    GB.vel[b] = h->bodies[b].V;
+    GB.snap[b] = h->bodies[b].snap;
+    GB.has_boundary[b] = h->bodies[b].has_boundary;
+  }
+  {
+    StageTimer timer(h, 2);
+    CUDA_TRY(h, cudaMemsetAsync(h->count, 0, sizeof(unsigned long long), st));
+    k_compact<<<grid_blocks(h, g.nblocks, 256), 256, 0, st>>>(g.nblocks, h->flags, h->list, h->count, h->was_active);
+    TRY(check_launch(h, "k_compact"));
+  }
+  {
+    StageTimer timer(h, 1);
+    const int gb = (int)std::min<int64_t>(std::max<int64_t>(g.nblocks, 1), (int64_t)h->sm_count * 32);
+    k_grid<DIM><<<gb, 64, 0, st>>>(g, h->sp, GB, h->cs, h->list, h->count);
+    TRY(check_launch(h, "k_grid"));
+  }
+  for (BodyDev& B : h->bodies) TRY(fused<DIM>(h, B, 1, 1));
+  if (++h->steps_since_sort >= h->sort_interval) {
+    StageTimer timer(h, 3);
+    for (BodyDev& B : h->bodies) TRY(sort_body<DIM>(h, B));
+    h->steps_since_sort = 0;
+  }
   return MPMGPU_OK;
 }
 
@@ -138,10 +349,12 @@ mpmgpu_status mpmgpu_create(const mpmgpu_config* cfg, mpmgpu_handle** out) {
   if (cfg->cpdi_spec != 0 && cfg->cpdi_spec != 1) return MPMGPU_ERR_ARG;
   if (cfg->contact_spec != 0 && cfg->contact_spec != 1) return MPMGPU_ERR_ARG;
   if (cfg->mode != MPMGPU_MODE_FP64) return MPMGPU_ERR_UNSUPPORTED;
+  if (cfg->sort_interval < 0) return MPMGPU_ERR_ARG;
   for (int d = 0; d < cfg->dim; d++)
     if (cfg->N[d] < 1 || !(cfg->L[d] > 0)) return MPMGPU_ERR_ARG;
   mpmgpu_handle* h = new mpmgpu_handle();
   h->cfg = *cfg;
+  h->sort_interval = cfg->sort_interval > 0 ? cfg->sort_interval : 32;
   cudaError_t e = cudaSetDevice(cfg->device);
   if (e != cudaSuccess) {
     delete h;
@@ -164,11 +377,15 @@ mpmgpu_status mpmgpu_create(const mpmgpu_config* cfg, mpmgpu_handle** out) {
       g.h[d] = cfg->L[d] / cfg->N[d];  // cartesian.cpp:40
       g.nn[d] = cfg->N[d] + 1;
       g.nnodes *= g.nn[d];
+      h->mc.NL[d] = (double)cfg->N[d] / cfg->L[d];
+      h->mc.invh[d] = 1.0 / g.h[d];
     } else {
       g.L[d] = 0.0;
       g.N[d] = 0;
       g.h[d] = 0.0;
       g.nn[d] = 1;
+      h->mc.NL[d] = 0.0;
+      h->mc.invh[d] = 0.0;
     }
   }
   if (cfg->dim == 3) {
@@ -184,6 +401,15 @@ mpmgpu_status mpmgpu_create(const mpmgpu_config* cfg, mpmgpu_handle** out) {
     g.nblocks *= g.nb[d];
   }
   g.nslots = g.nblocks * 64;
+  BinGeom& bg = h->bg;
+  bg.B = cfg->dim == 3 ? 4 : 8;
+  bg.cells_per_bin = cfg->dim == 3 ? 64 : 64;
+  bg.nbx = (g.N[0] + bg.B - 1) / bg.B;
+  bg.nby = (g.N[1] + bg.B - 1) / bg.B;
+  bg.nbz = cfg->dim == 3 ? (g.N[2] + bg.B - 1) / bg.B : 1;
+  bg.nbins = bg.nbx * bg.nby * bg.nbz;
+  bg.T = bg.B + 3;
+  bg.tile_nodes = cfg->dim == 3 ? bg.T * bg.T * bg.T : bg.T * bg.T;
   h->sp.dt = cfg->dt;
   h->sp.cpdi = cfg->cpdi_spec;
   h->sp.contact_spec = cfg->contact_spec;
@@ -193,9 +419,9 @@ mpmgpu_status mpmgpu_create(const mpmgpu_config* cfg, mpmgpu_handle** out) {
   h->sp.grav[cfg->dim == 2 ? 1 : 2] = -9.81;
   mpmgpu_status s = MPMGPU_OK;
   if ((s = dev_alloc(h, &h->flags, (size_t)g.nblocks)) != MPMGPU_OK ||
-      (s = dev_alloc(h, &h->list, (size_t)g.nblocks)) != MPMGPU_OK ||
-      (s = dev_alloc(h, &h->count, 1)) != MPMGPU_OK || (s = dev_alloc(h, &h->was_active, (size_t)g.nblocks)) != MPMGPU_OK ||
-      (s = dev_alloc(h, &h->err, 1)) != MPMGPU_OK) {
+      (s = dev_alloc(h, &h->list, (size_t)g.nblocks)) != MPMGPU_OK || (s = dev_alloc(h, &h->count, 1)) != MPMGPU_OK ||
+      (s = dev_alloc(h, &h->was_active, (size_t)g.nblocks)) != MPMGPU_OK || (s = dev_alloc(h, &h->err, 1)) != MPMGPU_OK ||
+      (s = dev_alloc(h, &h->drift, 1)) != MPMGPU_OK) {
     mpmgpu_destroy(h);
     return s;
   }
@@ -207,25 +433,15 @@ mpmgpu_status mpmgpu_add_body(mpmgpu_handle* h, const mpmgpu_body_desc* desc, in
   if (!h || !desc) return MPMGPU_ERR_ARG;
   if (h->stepped) return fail(h, MPMGPU_ERR_STATE, "bodies must be added before the first step");
   if ((int)h->bodies.size() >= kMaxBodies) return fail(h, MPMGPU_ERR_UNSUPPORTED, "too many bodies");
-  if (desc->n < 0 || (desc->n > 0 && (!desc->m || !desc->v || !desc->x || !desc->x_t)))
-    return fail(h, MPMGPU_ERR_ARG, "body arrays missing");
+  if (desc->n < 0 || desc->n > (int64_t)INT32_MAX / 2 ||
+      (desc->n > 0 && (!desc->m || !desc->v || !desc->x || !desc->x_t)))
+    return fail(h, MPMGPU_ERR_ARG, "body arrays missing or too many points");
   const int D = h->g.dim;
   const int64_t n = desc->n;
   BodyDev B;
   B.n = n;
-  B.P.n = n;
-  for (int d = 0; d < 3; d++) {
-    TRY(dev_alloc(h, &B.P.x[d], (size_t)n));
-    TRY(dev_alloc(h, &B.P.v[d], (size_t)n));
-    TRY(dev_alloc(h, &B.P.u[d], (size_t)n));
-  }
-  for (int c = 0; c < 6; c++) TRY(dev_alloc(h, &B.P.s[c], (size_t)n));
-  TRY(dev_alloc(h, &B.P.vol, (size_t)n));
-  TRY(dev_alloc(h, &B.P.m, (size_t)n));
-  TRY(dev_alloc(h, &B.P.ext, (size_t)n));
-  TRY(dev_alloc(h, &B.P.active, (size_t)n));
-  B.P.L = nullptr;
-  if (h->cfg.keep_debug) TRY(dev_alloc(h, &B.P.L, (size_t)n * 9));
+  TRY(alloc_points(h, B.P, n, h->cfg.keep_debug != 0));
+  TRY(alloc_points(h, B.Palt, n, h->cfg.keep_debug != 0));
   if (n > 0) {
     for (int d = 0; d < D; d++) {
       TRY(upload(h, B.P.x[d], column(desc->x, n, 3, d)));
@@ -238,11 +454,13 @@ mpmgpu_status mpmgpu_add_body(mpmgpu_handle* h, const mpmgpu_body_desc* desc, in
     // extent, default_points.cpp:49-57 (computed once, never updated)
     for (int64_t i = 0; i < n; i++) tmp[(size_t)i] = (D == 2) ? 0.5 * std::sqrt(desc->v[i]) : 0.5 * std::cbrt(desc->v[i]);
     TRY(upload(h, B.P.ext, tmp));
-    std::vector<int32_t> act((size_t)n, 1);
-    if (desc->active)
-      for (int64_t i = 0; i < n; i++) act[(size_t)i] = desc->active[i] != 0 ? 1 : 0;
-    CUDA_TRY(h, cudaMemcpyAsync(B.P.active, act.data(), act.size() * sizeof(int32_t), cudaMemcpyHostToDevice, h->stream));
-    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    std::vector<int32_t> act((size_t)n, 1), pid((size_t)n);
+    for (int64_t i = 0; i < n; i++) {
+      if (desc->active) act[(size_t)i] = desc->active[i] != 0 ? 1 : 0;
+      pid[(size_t)i] = (int32_t)i;
+    }
+    TRY(upload(h, B.P.active, act));
+    TRY(upload(h, B.P.pid, pid));
   }
   const size_t ns = (size_t)h->g.nslots;
   TRY(dev_alloc(h, &B.A.m, ns));
@@ -253,6 +471,23 @@ mpmgpu_status mpmgpu_add_body(mpmgpu_handle* h, const mpmgpu_body_desc* desc, in
     TRY(dev_alloc(h, &B.V.dv[d], ns));
     B.A.nrm[d] = nullptr;
   }
+  if (h->cfg.keep_debug) {
+    TRY(dev_alloc(h, &B.snap.m, ns));
+    for (int d = 0; d < 3; d++) {
+      TRY(dev_alloc(h, &B.snap.mx[d], ns));
+      TRY(dev_alloc(h, &B.snap.f[d], ns));
+      B.snap.nrm[d] = nullptr;
+    }
+  }
+  const BinGeom& bg = h->bg;
+  TRY(dev_alloc(h, &B.key, (size_t)n));
+  TRY(dev_alloc(h, &B.rank, (size_t)n));
+  TRY(dev_alloc(h, &B.cell_count, (size_t)bg.nbins * bg.cells_per_bin + 1));
+  TRY(dev_alloc(h, &B.bin_start, (size_t)bg.nbins + 2));
+  TRY(dev_alloc(h, &B.work_bin, (size_t)bg.nbins));
+  TRY(dev_alloc(h, &B.work_start, (size_t)bg.nbins));
+  TRY(dev_alloc(h, &B.work_end, (size_t)bg.nbins));
+  TRY(dev_alloc(h, &B.nwork, 1));
   B.mat.has_material = desc->has_material;
   if (desc->has_material) {
     // isolin.cpp:34-38
@@ -297,6 +532,7 @@ mpmgpu_status mpmgpu_add_contact(mpmgpu_handle* h, int body1, int body2, double 
 
 mpmgpu_status mpmgpu_set_gravity(mpmgpu_handle* h, int use_vector, const double g[3]) {
   if (!h) return MPMGPU_ERR_ARG;
+  if (h->stepped) return fail(h, MPMGPU_ERR_STATE, "gravity must be set before the first step");
   for (int d = 0; d < 3; d++) h->sp.grav[d] = 0.0;
   if (use_vector) {
     if (!g) return fail(h, MPMGPU_ERR_ARG, "gravity vector missing");
@@ -307,65 +543,9 @@ mpmgpu_status mpmgpu_set_gravity(mpmgpu_handle* h, int use_vector, const double 
   return MPMGPU_OK;
 }
 
-}  // extern "C"
-
-namespace {
-
-template <int DIM>
-mpmgpu_status step_once(mpmgpu_handle* h) {
-  const Geom& g = h->g;
-  cudaStream_t st = h->stream;
-  GridBodies GB{};
-  GB.nb = (int)h->bodies.size();
-  if (h->cfg.keep_debug) {
-    // Debug form: nodal arrays are zeroed in full each step so downloads of
-    // untouched nodes read zero, as the reference's full-grid arrays do.
-    const size_t bytes = (size_t)g.nslots * sizeof(double);
-    for (BodyDev& B : h->bodies) {
-      CUDA_TRY(h, cudaMemsetAsync(B.A.m, 0, bytes, st));
-      for (int d = 0; d < 3; d++) {
-        CUDA_TRY(h, cudaMemsetAsync(B.A.mx[d], 0, bytes, st));
-        CUDA_TRY(h, cudaMemsetAsync(B.A.f[d], 0, bytes, st));
-        CUDA_TRY(h, cudaMemsetAsync(B.V.vt[d], 0, bytes, st));
-        CUDA_TRY(h, cudaMemsetAsync(B.V.dv[d], 0, bytes, st));
-        if (B.A.nrm[d]) CUDA_TRY(h, cudaMemsetAsync(B.A.nrm[d], 0, bytes, st));
-      }
-    }
-    for (int c = 0; c < h->cs.nc; c++) {
-      CUDA_TRY(h, cudaMemsetAsync(h->cs.force_out[c], 0, 3 * bytes, st));
-      // untouched nodes have a 0/0 normal in the reference (contact_huang.cpp:93-96)
-    }
-  }
-  for (size_t b = 0; b < h->bodies.size(); b++) {
-    BodyDev& B = h->bodies[b];
-    GB.acc[b] = B.A;
-    GB.vel[b] = B.V;
-    GB.has_boundary[b] = B.has_boundary;
-    if (B.n == 0) continue;
-    k_p2g<DIM><<<grid_blocks(h, B.n, 256), 256, 0, st>>>(g, h->sp, B.P, B.A, h->flags, h->err);
-    TRY(check_launch(h, "k_p2g"));
-  }
-  CUDA_TRY(h, cudaMemsetAsync(h->count, 0, sizeof(unsigned long long), st));
-  k_compact<<<grid_blocks(h, g.nblocks, 256), 256, 0, st>>>(g.nblocks, h->flags, h->list, h->count, h->was_active);
-  TRY(check_launch(h, "k_compact"));
-  const int gb = (int)std::min<int64_t>(g.nblocks, (int64_t)h->sm_count * 32);
-  k_grid<DIM><<<gb, 64, 0, st>>>(g, h->sp, GB, h->cs, h->list, h->count);
-  TRY(check_launch(h, "k_grid"));
-  for (size_t b = 0; b < h->bodies.size(); b++) {
-    BodyDev& B = h->bodies[b];
-    if (B.n == 0) continue;
-    k_g2p<DIM><<<grid_blocks(h, B.n, 256), 256, 0, st>>>(g, h->sp, B.P, B.V, B.mat, h->err);
-    TRY(check_launch(h, "k_g2p"));
-  }
-  return MPMGPU_OK;
-}
-
-}  // namespace
-
-extern "C" {
-
 mpmgpu_status mpmgpu_step(mpmgpu_handle* h, int nsteps) {
   if (!h || nsteps < 0) return MPMGPU_ERR_ARG;
+  if (h->bodies.empty()) return fail(h, MPMGPU_ERR_STATE, "no bodies");
   h->stepped = true;
   for (int s = 0; s < nsteps; s++) {
     mpmgpu_status r = (h->g.dim == 3) ? step_once<3>(h) : step_once<2>(h);
@@ -393,24 +573,63 @@ mpmgpu_status mpmgpu_sizes(const mpmgpu_handle* h, int body, int64_t* n_points, 
 
 int64_t mpmgpu_launch_count(const mpmgpu_handle* h) { return h ? h->launches : 0; }
 
+void* mpmgpu_stream(const mpmgpu_handle* h) { return h ? (void*)h->stream : nullptr; }
+
+mpmgpu_status mpmgpu_profile(mpmgpu_handle* h, int enable) {
+  if (!h) return MPMGPU_ERR_ARG;
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  for (int s = 0; s < mpmgpu_handle::kStages; s++) {
+    for (auto& pr : h->pending[s]) {
+      h->event_pool.push_back(pr.first);
+      h->event_pool.push_back(pr.second);
+    }
+    h->pending[s].clear();
+    h->stage_launches[s] = 0;
+    h->stage_ms[s] = 0.0;
+  }
+  h->profiling = enable != 0;
+  return MPMGPU_OK;
+}
+
+mpmgpu_status mpmgpu_profile_read(mpmgpu_handle* h, int stage, int64_t* launches, double* total_ms) {
+  if (!h || stage < 0 || stage >= mpmgpu_handle::kStages) return MPMGPU_ERR_ARG;
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  for (int s = 0; s < mpmgpu_handle::kStages; s++) {
+    for (auto& pr : h->pending[s]) {
+      float ms = 0.0f;
+      CUDA_TRY(h, cudaEventElapsedTime(&ms, pr.first, pr.second));
+      h->stage_ms[s] += ms;
+      h->stage_launches[s]++;
+      h->event_pool.push_back(pr.first);
+      h->event_pool.push_back(pr.second);
+    }
+    h->pending[s].clear();
+  }
+  if (launches) *launches = h->stage_launches[stage];
+  if (total_ms) *total_ms = h->stage_ms[stage];
+  return MPMGPU_OK;
+}
+
 mpmgpu_status mpmgpu_download_points(mpmgpu_handle* h, int body, int field, double* out) {
   if (!h || !out || body < 0 || body >= (int)h->bodies.size()) return MPMGPU_ERR_ARG;
   TRY(mpmgpu_synchronize(h));
   BodyDev& B = h->bodies[(size_t)body];
   const int64_t n = B.n;
   const int D = h->g.dim;
+  std::vector<int32_t> pid;
+  TRY(download(h, pid, B.P.pid, (size_t)n));
   std::vector<double> tmp;
   auto vec3 = [&](double* const* arr) -> mpmgpu_status {
     for (int64_t i = 0; i < 3 * n; i++) out[i] = 0.0;
     for (int d = 0; d < D; d++) {
       TRY(download(h, tmp, arr[d], (size_t)n));
-      for (int64_t i = 0; i < n; i++) out[3 * i + d] = tmp[(size_t)i];
+      for (int64_t i = 0; i < n; i++) out[3 * (int64_t)pid[(size_t)i] + d] = tmp[(size_t)i];
     }
     return MPMGPU_OK;
   };
   auto scal = [&](const double* arr) -> mpmgpu_status {
     TRY(download(h, tmp, arr, (size_t)n));
-    std::memcpy(out, tmp.data(), sizeof(double) * (size_t)n);
+    for (int64_t i = 0; i < n; i++) out[pid[(size_t)i]] = tmp[(size_t)i];
     return MPMGPU_OK;
   };
   switch (field) {
@@ -422,8 +641,10 @@ mpmgpu_status mpmgpu_download_points(mpmgpu_handle* h, int body, int field, doub
       std::vector<double> m;
       TRY(download(h, m, B.P.m, (size_t)n));
       // movePoints: mx_t = m * x_t (explicit_usl.cpp:295-297)
-      for (int64_t i = 0; i < n; i++)
-        for (int d = 0; d < D; d++) out[3 * i + d] = m[(size_t)i] * out[3 * i + d];
+      for (int64_t i = 0; i < n; i++) {
+        const int64_t q = pid[(size_t)i];
+        for (int d = 0; d < D; d++) out[3 * q + d] = m[(size_t)i] * out[3 * q + d];
+      }
       return MPMGPU_OK;
     }
     case MPMGPU_P_B:
@@ -433,23 +654,26 @@ mpmgpu_status mpmgpu_download_points(mpmgpu_handle* h, int body, int field, doub
     case MPMGPU_P_L:
       if (!B.P.L) return fail(h, MPMGPU_ERR_STATE, "L is kept only with keep_debug");
       TRY(download(h, tmp, B.P.L, (size_t)n * 9));
-      std::memcpy(out, tmp.data(), sizeof(double) * 9 * (size_t)n);
+      for (int64_t i = 0; i < n; i++)
+        for (int k = 0; k < 9; k++) out[9 * (int64_t)pid[(size_t)i] + k] = tmp[(size_t)(9 * i + k)];
       return MPMGPU_OK;
     case MPMGPU_P_T: {
       static const int idx[9] = {0, 3, 5, 3, 1, 4, 5, 4, 2};
       std::vector<std::vector<double>> s(6);
       for (int c = 0; c < 6; c++) TRY(download(h, s[(size_t)c], B.P.s[c], (size_t)n));
       for (int64_t i = 0; i < n; i++)
-        for (int k = 0; k < 9; k++) out[9 * i + k] = s[(size_t)idx[k]][(size_t)i];
+        for (int k = 0; k < 9; k++) out[9 * (int64_t)pid[(size_t)i] + k] = s[(size_t)idx[k]][(size_t)i];
       return MPMGPU_OK;
     }
     case MPMGPU_P_M: return scal(B.P.m);
     case MPMGPU_P_V: return scal(B.P.vol);
     case MPMGPU_P_EXTENT: return scal(B.P.ext);
     case MPMGPU_P_ACTIVE: {
-      std::vector<int32_t> a((size_t)n);
-      CUDA_TRY(h, cudaMemcpy(a.data(), B.P.active, sizeof(int32_t) * (size_t)n, cudaMemcpyDeviceToHost));
-      for (int64_t i = 0; i < n; i++) out[i] = a[(size_t)i];
+      std::vector<int32_t> a;
+      TRY(download(h, a, B.P.active, (size_t)n));
+      // 2 = left the domain at the last move: still active until the next
+      // map build deactivates it, as in the reference
+      for (int64_t i = 0; i < n; i++) out[pid[(size_t)i]] = a[(size_t)i] != 0 ? 1.0 : 0.0;
       return MPMGPU_OK;
     }
   }
@@ -460,13 +684,12 @@ mpmgpu_status mpmgpu_download_points(mpmgpu_handle* h, int body, int field, doub
 
 namespace {
 
-// Copies a block-linear nodal array (width-component SoA) to reference node
-// order; nodes of blocks that were not active in the last step read zero.
-mpmgpu_status nodes_to_ref(mpmgpu_handle* h, double* const* arr, int comps, int width, double* out, bool mask_inactive,
-                           double fill) {
+// Copies a block-linear nodal array (comps SoA components) to reference node
+// order; nodes of blocks that were not active in the last step read `fill`.
+mpmgpu_status nodes_to_ref(mpmgpu_handle* h, double* const* arr, int comps, int width, double* out, double fill) {
   const Geom& g = h->g;
-  std::vector<uint8_t> act((size_t)g.nblocks, 1);
-  if (mask_inactive) CUDA_TRY(h, cudaMemcpy(act.data(), h->was_active, (size_t)g.nblocks, cudaMemcpyDeviceToHost));
+  std::vector<uint8_t> act;
+  TRY(download(h, act, h->was_active, (size_t)g.nblocks));
   for (int64_t i = 0; i < g.nnodes * width; i++) out[i] = 0.0;
   std::vector<double> tmp;
   for (int d = 0; d < comps; d++) {
@@ -491,21 +714,25 @@ mpmgpu_status mpmgpu_download_nodes(mpmgpu_handle* h, int body, int field, doubl
   TRY(mpmgpu_synchronize(h));
   BodyDev& B = h->bodies[(size_t)body];
   const int D = h->g.dim;
-  const bool dbg = h->cfg.keep_debug != 0;
+  const bool dbg = B.snap.m != nullptr;
+  if (!h->primed) {
+    for (int64_t i = 0; i < h->g.nnodes * (field == MPMGPU_N_M ? 1 : 3); i++) out[i] = 0.0;
+    return MPMGPU_OK;
+  }
   switch (field) {
     case MPMGPU_N_M:
       if (!dbg) return fail(h, MPMGPU_ERR_STATE, "nodal m is kept only with keep_debug");
-      return nodes_to_ref(h, &B.A.m, 1, 1, out, false, 0.0);
+      return nodes_to_ref(h, &B.snap.m, 1, 1, out, 0.0);
     case MPMGPU_N_MX_T:
       if (!dbg) return fail(h, MPMGPU_ERR_STATE, "nodal mx_t is kept only with keep_debug");
-      return nodes_to_ref(h, B.A.mx, D, 3, out, false, 0.0);
+      return nodes_to_ref(h, B.snap.mx, D, 3, out, 0.0);
     case MPMGPU_N_F:
       if (!dbg) return fail(h, MPMGPU_ERR_STATE, "nodal f is kept only with keep_debug");
-      return nodes_to_ref(h, B.A.f, D, 3, out, false, 0.0);
-    case MPMGPU_N_X_T: return nodes_to_ref(h, B.V.vt, D, 3, out, !dbg, 0.0);
-    case MPMGPU_N_DIFF_X_T: return nodes_to_ref(h, B.V.dv, D, 3, out, !dbg, 0.0);
+      return nodes_to_ref(h, B.snap.f, D, 3, out, 0.0);
+    case MPMGPU_N_X_T: return nodes_to_ref(h, B.V.vt, D, 3, out, 0.0);
+    case MPMGPU_N_DIFF_X_T: return nodes_to_ref(h, B.V.dv, D, 3, out, 0.0);
     case MPMGPU_N_U: {
-      TRY(nodes_to_ref(h, B.V.vt, D, 3, out, !dbg, 0.0));
+      TRY(nodes_to_ref(h, B.V.vt, D, 3, out, 0.0));
       // moveGrid: u = dt * x_t (explicit_usl.cpp:252)
       for (int64_t i = 0; i < 3 * h->g.nnodes; i++) out[i] = h->sp.dt * out[i];
       return MPMGPU_OK;
@@ -517,21 +744,21 @@ mpmgpu_status mpmgpu_download_nodes(mpmgpu_handle* h, int body, int field, doubl
 mpmgpu_status mpmgpu_download_contact(mpmgpu_handle* h, int contact, int field, double* out) {
   if (!h || !out || contact < 0 || contact >= h->cs.nc) return MPMGPU_ERR_ARG;
   if (!h->cfg.keep_debug) return fail(h, MPMGPU_ERR_STATE, "contact fields are kept only with keep_debug");
+  if (field != MPMGPU_C_NORMAL && field != MPMGPU_C_FORCE) return fail(h, MPMGPU_ERR_ARG, "unknown contact field");
   TRY(mpmgpu_synchronize(h));
   const Geom& g = h->g;
   double* src = (field == MPMGPU_C_NORMAL) ? h->cs.normal_out[contact] : h->cs.force_out[contact];
-  if (field != MPMGPU_C_NORMAL && field != MPMGPU_C_FORCE) return fail(h, MPMGPU_ERR_ARG, "unknown contact field");
   std::vector<double> tmp;
   TRY(download(h, tmp, src, 3 * (size_t)g.nslots));
-  std::vector<uint8_t> act((size_t)g.nblocks, 1);
-  CUDA_TRY(h, cudaMemcpy(act.data(), h->was_active, (size_t)g.nblocks, cudaMemcpyDeviceToHost));
+  std::vector<uint8_t> act;
+  TRY(download(h, act, h->was_active, (size_t)g.nblocks));
   const double nan = std::nan("");
   for (int k = 0; k < g.nn[2]; k++)
     for (int j = 0; j < g.nn[1]; j++)
       for (int i = 0; i < g.nn[0]; i++) {
         const int64_t id = i + (int64_t)g.nn[0] * (j + (int64_t)g.nn[1] * k);
         const int64_t s = node_slot(g, i, j, k);
-        const bool on = act[(size_t)node_block(g, i, j, k)] != 0;
+        const bool on = h->primed && act[(size_t)node_block(g, i, j, k)] != 0;
         for (int d = 0; d < 3; d++) {
           double v = tmp[(size_t)(3 * s + d)];
           // the reference normalises every node's normal; a zero normal gives 0 * (1/0)
@@ -593,6 +820,12 @@ mpmgpu_status mpmgpu_dump_map(mpmgpu_handle* h, int body, int32_t* node, int32_t
 mpmgpu_status mpmgpu_destroy(mpmgpu_handle* h) {
   if (!h) return MPMGPU_OK;
   if (h->stream) cudaStreamSynchronize(h->stream);
+  for (int s = 0; s < mpmgpu_handle::kStages; s++)
+    for (auto& pr : h->pending[s]) {
+      cudaEventDestroy(pr.first);
+      cudaEventDestroy(pr.second);
+    }
+  for (cudaEvent_t e : h->event_pool) cudaEventDestroy(e);
   for (void* p : h->allocs) cudaFree(p);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;

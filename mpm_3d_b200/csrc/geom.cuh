@@ -99,28 +99,43 @@ __device__ __forceinline__ int axis_element(const Geom& g, int d, double c) {
   return (int)floor(__dmul_rn(__ddiv_rn(c, g.L[d]), (double)g.N[d]));
 }
 
-// Hat value 1 - |(c - h*idx)/h| of cartesian.cpp:292-295.
-__device__ __forceinline__ double hat(const Geom& g, int d, double c, int idx) {
-  const double xn = __dmul_rn(g.h[d], (double)idx);
-  const double r = __ddiv_rn(__dsub_rn(c, xn), g.h[d]);
-  return __dsub_rn(1.0, fabs(r));
+// Per-grid constants of the fast map.
+struct MapConst {
+  double NL[3];    // N / L: element index scale
+  double invh[3];  // 1 / h
+};
+
+// Element index floor(x / L * N) without a division: the product x * (N/L)
+// differs from the reference's two roundings by a few ulps, which can only
+// change the floor when the value is within that distance of an integer; in
+// that band the exact two-rounding form decides.
+__device__ __forceinline__ int axis_element_fast(const Geom& g, const MapConst& mc, int d, double c) {
+  const double t = c * mc.NL[d];
+  const double f = floor(t);
+  if (t - f < 1e-9 || (f + 1.0) - t < 1e-9) return axis_element(g, d, c);
+  return (int)f;
 }
 
-// Builds the separable map of one point, following the decisions of
-// DefaultPoints::generateMap (default_points.cpp:211-236).
-// Returns -1 if the point is outside the domain (the caller deactivates it),
-// 0 if it has no triplets (whichElement fails), 1 otherwise.
+// Builds the separable map of one point with the decisions of
+// DefaultPoints::generateMap (default_points.cpp:211-236): corner-sampled
+// unless a corner leaves the closed domain, no triplets for a corner (or
+// point) without an element, deactivation outside the domain. Hat values are
+// computed as (c - x_n) * (1/h), a different rounding of the reference's
+// (c - x_n) / h; the element indices, and so the connectivity, are exact
+// (axis_element_fast). Triplet-exact values come from exact_map.cuh.
+// Returns -1 outside the domain (caller deactivates), 0 without triplets,
+// 1 otherwise.
 template <int DIM>
-__device__ __forceinline__ int build_map(const Geom& g, int cpdi_spec, const double* x, double extent, PointMap& pm,
-                                         int* err) {
+__device__ __forceinline__ int build_map_fast(const Geom& g, const MapConst& mc, int cpdi_spec, const double* x,
+                                              double extent, PointMap& pm, int* err) {
   if (!in_domain<DIM>(g, x)) return -1;
   int cpdi = cpdi_spec;
-  const double a = __dmul_rn(0.5, extent);
+  const double a = 0.5 * extent;
   double clo[3], chi[3];
 #pragma unroll
   for (int d = 0; d < DIM; d++) {
-    clo[d] = __dadd_rn(x[d], __dmul_rn(a, -1.0));
-    chi[d] = __dadd_rn(x[d], __dmul_rn(a, 1.0));
+    clo[d] = x[d] - a;
+    chi[d] = x[d] + a;
   }
   if (cpdi == 1) {
 #pragma unroll
@@ -128,57 +143,68 @@ __device__ __forceinline__ int build_map(const Geom& g, int cpdi_spec, const dou
       if (!(clo[d] <= g.L[d] && clo[d] >= 0.0) || !(chi[d] <= g.L[d] && chi[d] >= 0.0)) cpdi = 0;
   }
   if (cpdi == 1) {
-    // whichElement accepts x < L only; a hi corner exactly at L has no
-    // element and contributes nothing (cartesian.cpp:228-230, 284-286).
 #pragma unroll
     for (int d = 0; d < DIM; d++) {
       AxisMap& A = pm.ax[d];
-      const int elo = axis_element(g, d, clo[d]);
+      const int elo = axis_element_fast(g, mc, d, clo[d]);
       const bool hi_ok = chi[d] < g.L[d];
-      const int ehi = hi_ok ? axis_element(g, d, chi[d]) : elo;
-      if (elo >= g.N[d] || (hi_ok && ehi >= g.N[d])) atomicOr(err, kErrElemAlias);
+      const int ehi = hi_ok ? axis_element_fast(g, mc, d, chi[d]) : elo;
+      if (elo >= g.N[d] || (hi_ok && ehi >= g.N[d])) {
+        // element index rounded up to N for x < L: flagged, and no nodal
+        // contributions (its nodes would lie outside the grid)
+        atomicOr(err, kErrElemAlias);
+        return 0;
+      }
       const int delta = ehi - elo;
       if (delta > 1 || delta < 0) atomicOr(err, kErrWideSpan);
       A.base = elo;
       A.span = 2 + (hi_ok && delta == 1 ? 1 : 0);
-      const double wl0 = hat(g, d, clo[d], elo), wl1 = hat(g, d, clo[d], elo + 1);
-      A.W[0] = wl0;
-      A.W[1] = wl1;
-      A.W[2] = 0.0;
-      A.G[0] = -wl0;
-      A.G[1] = -wl1;
-      A.G[2] = 0.0;
+      const double rl = (clo[d] - g.h[d] * (double)elo) * mc.invh[d];
+      const double wl0 = 1.0 - fabs(rl), wl1 = 1.0 - fabs(rl - 1.0);
+      double wh0 = 0.0, wh1 = 0.0;
       if (hi_ok) {
-        const double wh0 = hat(g, d, chi[d], ehi), wh1 = hat(g, d, chi[d], ehi + 1);
-        const int o = (delta == 1) ? 1 : 0;
-        A.W[o] += wh0;
-        A.W[o + 1] += wh1;
-        A.G[o] += wh0;
-        A.G[o + 1] += wh1;
+        const double rh = (chi[d] - g.h[d] * (double)ehi) * mc.invh[d];
+        wh0 = 1.0 - fabs(rh);
+        wh1 = 1.0 - fabs(rh - 1.0);
+      }
+      if (delta == 1) {
+        A.W[0] = wl0;
+        A.W[1] = wl1 + wh0;
+        A.W[2] = wh1;
+        A.G[0] = -wl0;
+        A.G[1] = wh0 - wl1;
+        A.G[2] = wh1;
+      } else {
+        A.W[0] = wl0 + wh0;
+        A.W[1] = wl1 + wh1;
+        A.W[2] = 0.0;
+        A.G[0] = wh0 - wl0;
+        A.G[1] = wh1 - wl1;
+        A.G[2] = 0.0;
       }
     }
     pm.sS = 1.0 / (double)g.cp;
     pm.sG = 1.0 / ((g.cp * 0.5) * extent);
     return 1;
   }
-  // CPDI_OFF: plain hat functions at x, evaluateBasisFnValue/Gradient.
 #pragma unroll
   for (int d = 0; d < DIM; d++)
     if (!(x[d] < g.L[d] && x[d] >= 0.0)) return 0;
 #pragma unroll
   for (int d = 0; d < DIM; d++) {
     AxisMap& A = pm.ax[d];
-    const int e = axis_element(g, d, x[d]);
-    if (e >= g.N[d]) atomicOr(err, kErrElemAlias);
+    const int e = axis_element_fast(g, mc, d, x[d]);
+    if (e >= g.N[d]) {
+      atomicOr(err, kErrElemAlias);
+      return 0;
+    }
     A.base = e;
     A.span = 2;
 #pragma unroll
     for (int o = 0; o < 2; o++) {
-      const double xn = __dmul_rn(g.h[d], (double)(e + o));
-      const double r = __ddiv_rn(__dsub_rn(x[d], xn), g.h[d]);
-      A.W[o] = __dsub_rn(1.0, fabs(r));
-      // -sign(r)/h, NaN at r == 0 and 0 for |r| >= 1, as cartesian.cpp:329-332
-      A.G[o] = (fabs(r) >= 1.0) ? 0.0 : -(r / fabs(r)) / g.h[d];
+      const double r = (x[d] - g.h[d] * (double)(e + o)) * mc.invh[d];
+      A.W[o] = 1.0 - fabs(r);
+      A.G[o] = (fabs(r) >= 1.0) ? 0.0 : -(r / fabs(r)) * mc.invh[d];
     }
     A.W[2] = 0.0;
     A.G[2] = 0.0;

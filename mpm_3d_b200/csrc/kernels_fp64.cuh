@@ -1,6 +1,6 @@
-// FP64 kernels of the explicit step: map + scatter (P2G), active-block
-// compaction, grid update (contact, boundary, moveGrid) and gather + point
-// update (G2P, strain rate, density, stress).
+// FP64 kernels of the explicit step around the fused gather/scatter kernel:
+// active-block compaction, grid update (contact, boundary, moveGrid), the
+// Jaumann stress update and the exact triplet export.
 #pragma once
 
 #include "exact_map.cuh"
@@ -31,66 +31,6 @@ __device__ __forceinline__ void mark_blocks(const Geom& g, const PointMap& pm, u
   for (int k = k0; k <= k1; k++)
     for (int j = j0; j <= j1; j++)
       for (int i = i0; i <= i1; i++) flags[i + (int64_t)g.nb[0] * (j + (int64_t)g.nb[1] * k)] = 1u;
-}
-
-// P2G: mapPointsToNodes (explicit_usl.cpp:112-164) and, for the first body
-// of a contact, the normal accumulation of ContactHuang::generateRules
-// (contact_huang.cpp:91), one thread per point, FP64 atomics per window node.
-template <int DIM>
-__global__ void __launch_bounds__(256) k_p2g(Geom g, StepParams sp, PointsDev P, NodesAcc A, uint32_t* flags, int* err) {
-  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < P.n; p += stride) {
-    if (!P.active[p]) continue;
-    double x[3] = {0.0, 0.0, 0.0};
-#pragma unroll
-    for (int d = 0; d < DIM; d++) x[d] = P.x[d][p];
-    PointMap pm;
-    const int st = build_map<DIM>(g, sp.cpdi, x, P.ext[p], pm, err);
-    if (st < 0) {
-      P.active[p] = 0;  // default_points.cpp:217-219
-      continue;
-    }
-    if (st == 0) continue;
-    mark_blocks<DIM>(g, pm, flags);
-    const double m = P.m[p];
-    const double vol = P.vol[p];
-    double mv[3], mb[3], vs[6];
-#pragma unroll
-    for (int d = 0; d < DIM; d++) {
-      mv[d] = m * P.v[d][p];
-      mb[d] = m * sp.grav[d];
-    }
-#pragma unroll
-    for (int c = 0; c < 6; c++) vs[c] = (DIM == 3 || c == 0 || c == 1 || c == 3) ? P.s[c][p] * vol : 0.0;
-    const AxisMap& X = pm.ax[0];
-    const AxisMap& Y = pm.ax[1];
-    const int span2 = (DIM == 3) ? pm.ax[2].span : 1;
-    for (int k2 = 0; k2 < span2; k2++) {
-      const double wz = (DIM == 3) ? pm.ax[2].W[k2] : 1.0;
-      const double gz = (DIM == 3) ? pm.ax[2].G[k2] : 0.0;
-      for (int k1 = 0; k1 < Y.span; k1++) {
-        for (int k0 = 0; k0 < X.span; k0++) {
-          const double wxy = X.W[k0] * Y.W[k1];
-          const double S = pm.sS * (wxy * wz);
-          double gr[3];
-          gr[0] = pm.sG * (X.G[k0] * Y.W[k1] * wz);
-          gr[1] = pm.sG * (X.W[k0] * Y.G[k1] * wz);
-          gr[2] = (DIM == 3) ? pm.sG * (wxy * gz) : 0.0;
-          const int64_t s = node_slot(g, X.base + k0, Y.base + k1, DIM == 3 ? pm.ax[2].base + k2 : 0);
-          atomicAdd(A.m + s, S * m);
-#pragma unroll
-          for (int d = 0; d < DIM; d++) {
-            atomicAdd(A.mx[d] + s, S * mv[d]);
-            double fi = 0.0;
-#pragma unroll
-            for (int e = 0; e < DIM; e++) fi += sym_at(vs, d, e) * gr[e];
-            atomicAdd(A.f[d] + s, S * mb[d] - fi);
-            if (A.nrm[0] != nullptr) atomicAdd(A.nrm[d] + s, gr[d] * m);
-          }
-        }
-      }
-    }
-  }
 }
 
 // Compacts the flagged node blocks into `list`, clears the flags and keeps
@@ -131,6 +71,15 @@ __global__ void __launch_bounds__(64) k_grid(Geom g, StepParams sp, GridBodies G
     slot_ijk(g, blk, li, i, j, k);
     if (i >= g.nn[0] || j >= g.nn[1] || k >= g.nn[2]) continue;
     const int64_t s = blk * 64 + li;
+    // the scatter leaves out the body force; S * (m b) summed over points is
+    // the nodal mass times g (explicit_usl.cpp:150-154, b uniform)
+    for (int b = 0; b < GB.nb; b++) {
+      const NodesAcc& A = GB.acc[b];
+      const double m = A.m[s];
+#pragma unroll
+      for (int d = 0; d < DIM; d++)
+        if (sp.grav[d] != 0.0) A.f[d][s] = A.f[d][s] + m * sp.grav[d];
+    }
     for (int c = 0; c < CS.nc; c++) {
       const NodesAcc& A1 = GB.acc[CS.b1[c]];
       const NodesAcc& A2 = GB.acc[CS.b2[c]];
@@ -235,20 +184,22 @@ __global__ void __launch_bounds__(64) k_grid(Geom g, StepParams sp, GridBodies G
         V.vt[d][s] = (m > 0) ? mx[d] * inv : 0.0;
         V.dv[d][s] = (m > 0) ? (dt * f[d]) * inv : 0.0;
       }
-      if (sp.keep_debug) {
+      const NodesAcc& Sn = GB.snap[b];
+      if (Sn.m != nullptr) {
+        Sn.m[s] = m;
 #pragma unroll
         for (int d = 0; d < DIM; d++) {
-          A.mx[d][s] = mx[d];
-          A.f[d][s] = f[d];
+          Sn.mx[d][s] = mx[d];
+          Sn.f[d][s] = f[d];
         }
-      } else {
-        A.m[s] = 0.0;
+      }
+      // the next step's scatter accumulates into zeroed arrays
+      A.m[s] = 0.0;
 #pragma unroll
-        for (int d = 0; d < DIM; d++) {
-          A.mx[d][s] = 0.0;
-          A.f[d][s] = 0.0;
-          if (A.nrm[0] != nullptr) A.nrm[d][s] = 0.0;
-        }
+      for (int d = 0; d < DIM; d++) {
+        A.mx[d][s] = 0.0;
+        A.f[d][s] = 0.0;
+        if (A.nrm[0] != nullptr) A.nrm[d][s] = 0.0;
       }
     }
   }
@@ -286,83 +237,15 @@ __device__ __forceinline__ void jaumann_update(const double L[3][3], double* s6,
   }
 }
 
-// G2P: movePoints (explicit_usl.cpp:266-300), calculateStrainRate
-// (302-330), updateDensity (332-345) and updateStress (347-355).
-template <int DIM>
-__global__ void __launch_bounds__(256) k_g2p(Geom g, StepParams sp, PointsDev P, NodesVel V, MaterialParams mat, int* err) {
-  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  const double dt = sp.dt;
-  for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < P.n; p += stride) {
-    if (!P.active[p]) continue;
-    double x[3] = {0.0, 0.0, 0.0};
-#pragma unroll
-    for (int d = 0; d < DIM; d++) x[d] = P.x[d][p];
-    PointMap pm;
-    const int st = build_map<DIM>(g, sp.cpdi, x, P.ext[p], pm, err);
-    double du[3] = {0.0, 0.0, 0.0}, dvel[3] = {0.0, 0.0, 0.0};
-    double L[3][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};
-    if (st > 0) {
-      const AxisMap& X = pm.ax[0];
-      const AxisMap& Y = pm.ax[1];
-      const int span2 = (DIM == 3) ? pm.ax[2].span : 1;
-      for (int k2 = 0; k2 < span2; k2++) {
-        const double wz = (DIM == 3) ? pm.ax[2].W[k2] : 1.0;
-        const double gz = (DIM == 3) ? pm.ax[2].G[k2] : 0.0;
-        for (int k1 = 0; k1 < Y.span; k1++) {
-          for (int k0 = 0; k0 < X.span; k0++) {
-            const double wxy = X.W[k0] * Y.W[k1];
-            const double S = pm.sS * (wxy * wz);
-            double gr[3];
-            gr[0] = pm.sG * (X.G[k0] * Y.W[k1] * wz);
-            gr[1] = pm.sG * (X.W[k0] * Y.G[k1] * wz);
-            gr[2] = (DIM == 3) ? pm.sG * (wxy * gz) : 0.0;
-            const int64_t s = node_slot(g, X.base + k0, Y.base + k1, DIM == 3 ? pm.ax[2].base + k2 : 0);
-            double vt[3];
-#pragma unroll
-            for (int d = 0; d < DIM; d++) {
-              vt[d] = V.vt[d][s];
-              du[d] += S * (dt * vt[d]);
-              dvel[d] += S * V.dv[d][s];
-            }
-#pragma unroll
-            for (int a = 0; a < DIM; a++)
-#pragma unroll
-              for (int b = 0; b < DIM; b++) L[a][b] += vt[a] * gr[b];
-          }
-        }
-      }
-    }
-#pragma unroll
-    for (int d = 0; d < DIM; d++) {
-      P.x[d][p] = x[d] + du[d];
-      P.u[d][p] = P.u[d][p] + du[d];
-      P.v[d][p] = P.v[d][p] + dvel[d];
-    }
-    P.vol[p] = P.vol[p] * exp(dt * (L[0][0] + L[1][1] + L[2][2]));
-    if (mat.has_material) {
-      double s6[6];
-#pragma unroll
-      for (int c = 0; c < 6; c++) s6[c] = P.s[c][p];
-      jaumann_update<DIM>(L, s6, mat.G, mat.lambda, dt);
-#pragma unroll
-      for (int c = 0; c < 6; c++) P.s[c][p] = s6[c];
-    }
-    if (P.L != nullptr) {
-#pragma unroll
-      for (int a = 0; a < 3; a++)
-#pragma unroll
-        for (int b = 0; b < 3; b++) P.L[9 * p + 3 * a + b] = L[a][b];
-    }
-  }
-}
-
 // Exact triplet export (mpmgpu_dump_map).
 template <int DIM>
 __global__ void k_export_map(Geom g, int cpdi, PointsDev P, int32_t* node_out, double* s_out, double* g_out) {
   constexpr int cp = 1 << DIM;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < P.n; p += stride) {
-    const int64_t slot = p * cp * cp;
+    // slots in original point order (P.pid), so the host reads triplets in
+    // the reference's point-major order whatever the storage order
+    const int64_t slot = (int64_t)P.pid[p] * cp * cp;
     if (!P.active[p]) {
       for (int k = 0; k < cp * cp; k++) node_out[slot + k] = -1;
       continue;

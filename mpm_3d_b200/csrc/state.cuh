@@ -19,7 +19,9 @@ struct PointsDev {
   double* vol;
   double* m;
   double* ext;      // extent, default_points.cpp:40-57
-  int32_t* active;
+  int32_t* active;   // 1 active, 0 inactive, 2 left the domain at the last
+                     // move (inactive from the next map build on)
+  int32_t* pid;      // original index of the point
   double* L;        // 9 per point when debug output is kept, else null
 };
 
@@ -43,6 +45,7 @@ struct GridBodies {
   int nb;
   NodesAcc acc[kMaxBodies];
   NodesVel vel[kMaxBodies];
+  NodesAcc snap[kMaxBodies];  // debug copies of m, mx_t, f after the update (or null)
   int has_boundary[kMaxBodies];
 };
 

@@ -31,7 +31,7 @@ class MpmGpuError(RuntimeError):
 class _Config(ctypes.Structure):
     _fields_ = [("dim", ctypes.c_int), ("L", ctypes.c_double * 3), ("N", ctypes.c_int * 3), ("dt", ctypes.c_double),
                 ("cpdi_spec", ctypes.c_int), ("contact_spec", ctypes.c_int), ("mode", ctypes.c_int),
-                ("device", ctypes.c_int), ("keep_debug", ctypes.c_int)]
+                ("device", ctypes.c_int), ("keep_debug", ctypes.c_int), ("sort_interval", ctypes.c_int)]
 
 
 class _BodyDesc(ctypes.Structure):
@@ -69,6 +69,10 @@ def load() -> ctypes.CDLL:
     lib.mpmgpu_sizes.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)]
     lib.mpmgpu_launch_count.restype = ctypes.c_int64
     lib.mpmgpu_launch_count.argtypes = [vp]
+    lib.mpmgpu_stream.restype = vp
+    lib.mpmgpu_stream.argtypes = [vp]
+    lib.mpmgpu_profile.argtypes = [vp, ctypes.c_int]
+    lib.mpmgpu_profile_read.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_double)]
     lib.mpmgpu_destroy.argtypes = [vp]
     _lib = lib
     return lib
@@ -85,7 +89,8 @@ class GPUExplicitUSL:
     in the reference's layout (AoS, original point order, reference node ids).
     """
 
-    def __init__(self, case: inputs.Case, mode: str = "fp64", keep_debug: bool = False, device: int = 0):
+    def __init__(self, case: inputs.Case, mode: str = "fp64", keep_debug: bool = False, device: int = 0,
+                 sort_interval: int = 0):
         self.lib = load()
         self.case = case
         cfg = _Config()
@@ -99,6 +104,7 @@ class GPUExplicitUSL:
         cfg.mode = MODES[mode]
         cfg.device = device
         cfg.keep_debug = int(keep_debug)
+        cfg.sort_interval = int(sort_interval)
         h = ctypes.c_void_p()
         self._check(self.lib.mpmgpu_create(ctypes.byref(cfg), ctypes.byref(h)), None)
         self.h = h
@@ -147,6 +153,26 @@ class GPUExplicitUSL:
 
     def launches(self) -> int:
         return int(self.lib.mpmgpu_launch_count(self.h))
+
+    def stream(self) -> int:
+        """The cudaStream_t (as an integer) the solver queues its work on."""
+        return int(self.lib.mpmgpu_stream(self.h) or 0)
+
+    STAGES = {"g2p2g": 0, "grid": 1, "compact": 2, "rebin": 3}
+
+    def profile(self, enable: bool = True):
+        """Starts (and resets) or stops per-stage CUDA-event timing."""
+        self._check(self.lib.mpmgpu_profile(self.h, int(enable)))
+
+    def profile_read(self) -> Dict[str, Tuple[int, float]]:
+        """Per stage: (launches, total device milliseconds)."""
+        out = {}
+        for name, sid in self.STAGES.items():
+            n = ctypes.c_int64()
+            ms = ctypes.c_double()
+            self._check(self.lib.mpmgpu_profile_read(self.h, sid, ctypes.byref(n), ctypes.byref(ms)))
+            out[name] = (int(n.value), float(ms.value))
+        return out
 
     def points(self, b: int, name: str) -> np.ndarray:
         fid, w = POINT_FIELDS[name]
