@@ -89,7 +89,7 @@ class ClockSampler:
         os.close(fd)
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.QUERY}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
@@ -173,13 +173,37 @@ def cpu_reference_run(case, steps: int, warmup: int, threads: int):
     d = tempfile.mkdtemp()
     cfg = inputs.write_case(case, d, solver_class="ThreadPoolExplicitUSL", points_class="ThreadPoolPoints",
                             threads=threads)
-    job = bridge.ReferenceJob(cfg, build="timing")
-    job.step(warmup)
-    t0 = time.perf_counter()
-    job.step(steps)
-    dt = (time.perf_counter() - t0) / steps
-    job.close()
+    with quiet_stdout():  # the reference reports its set-up on stdout
+        job = bridge.ReferenceJob(cfg, build="timing")
+        job.step(warmup)
+        t0 = time.perf_counter()
+        job.step(steps)
+        dt = (time.perf_counter() - t0) / steps
+        job.close()
     return dt
+
+
+class quiet_stdout:
+    """Sends file descriptor 1 to /dev/null (C and C++ output included), so
+    the benchmark's JSON line stays the only line on stdout."""
+
+    def __enter__(self):
+        import ctypes
+
+        self.libc = ctypes.CDLL(None)
+        sys.stdout.flush()
+        self.libc.fflush(None)
+        self.saved = os.dup(1)
+        devnull = os.open(os.devnull, os.O_WRONLY)
+        os.dup2(devnull, 1)
+        os.close(devnull)
+        return self
+
+    def __exit__(self, *exc):
+        sys.stdout.flush()
+        self.libc.fflush(None)
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
 
 
 def run_reference_arm(args, rank, world):
@@ -332,8 +356,8 @@ def run_e2e(case, steps: int, device: int):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=0, help="timed steps (default: the workload's own step count)")
+    ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--workload", default="collision", choices=["collision", "column"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--ref-steps", type=int, default=4, help="steps of the CPU reference sample")
@@ -342,6 +366,8 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.steps <= 0:
+        args.steps = make_workload(args.workload).steps
     rank, world, local = dist_setup(args.gpus)
     try:
         if args.impl == "reference":

@@ -87,6 +87,9 @@ typedef struct {
   int has_material;     /* 0: no Material (stress never updated) */
   double E, nu;
   int has_boundary;     /* 0: no Boundary */
+  const double* u;      /* 3n initial displacements (AoS) or NULL (zero) */
+  const double* T;      /* 9n initial Cauchy stresses (row-major, symmetric)
+                           or NULL (zero) */
 } mpmgpu_body_desc;
 
 typedef struct mpmgpu_handle mpmgpu_handle;
@@ -141,7 +144,10 @@ mpmgpu_status mpmgpu_add_contact(mpmgpu_handle* h, int body1, int body2, double 
 
 /* Gravity as the driver applies it (Driver::generateGravity/applyGravity):
  * use_vector 0 = DefaultDriver (-9.81 along y in 2D, z in 3D,
- * default_driver.cpp:90-105), 1 = UserDefinedGravityDriver vector g. */
+ * default_driver.cpp:90-105), 1 = UserDefinedGravityDriver vector g. May be
+ * called between steps; the new body force enters the next step's nodal
+ * forces, as points->b set at the end of a step does in the reference
+ * (explicit_usl.cpp:80-81). */
 mpmgpu_status mpmgpu_set_gravity(mpmgpu_handle* h, int use_vector, const double g[3]);
 
 /* Replaces nsteps calls of ExplicitUSL::step (explicit_usl.cpp:48-87).

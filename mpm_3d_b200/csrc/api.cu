@@ -269,10 +269,10 @@ mpmgpu_status launch_fused(mpmgpu_handle* h, BodyDev& B, int do_g2p, int do_p2g)
     configured = true;
   }
   int per_sm = 0;
-  CUDA_TRY(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_g2p2g<DIM, BB, NORMAL>, 256, smem));
+  CUDA_TRY(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_g2p2g<DIM, BB, NORMAL>, kFusedThreads, smem));
   const int blocks = std::max(1, per_sm) * h->sm_count;
   StageTimer timer(h, 0);
-  k_g2p2g<DIM, BB, NORMAL><<<blocks, 256, smem, h->stream>>>(fp);
+  k_g2p2g<DIM, BB, NORMAL><<<blocks, kFusedThreads, smem, h->stream>>>(fp);
   return check_launch(h, "k_g2p2g");
 }
 
@@ -454,6 +454,13 @@ mpmgpu_status mpmgpu_add_body(mpmgpu_handle* h, const mpmgpu_body_desc* desc, in
     // extent, default_points.cpp:49-57 (computed once, never updated)
     for (int64_t i = 0; i < n; i++) tmp[(size_t)i] = (D == 2) ? 0.5 * std::sqrt(desc->v[i]) : 0.5 * std::cbrt(desc->v[i]);
     TRY(upload(h, B.P.ext, tmp));
+    if (desc->u)
+      for (int d = 0; d < D; d++) TRY(upload(h, B.P.u[d], column(desc->u, n, 3, d)));
+    if (desc->T) {
+      // stored as xx yy zz xy yz xz (row-major 9 -> symmetric 6)
+      static const int idx[6] = {0, 4, 8, 1, 5, 2};
+      for (int c = 0; c < 6; c++) TRY(upload(h, B.P.s[c], column(desc->T, n, 9, idx[c])));
+    }
     std::vector<int32_t> act((size_t)n, 1), pid((size_t)n);
     for (int64_t i = 0; i < n; i++) {
       if (desc->active) act[(size_t)i] = desc->active[i] != 0 ? 1 : 0;
@@ -532,7 +539,6 @@ mpmgpu_status mpmgpu_add_contact(mpmgpu_handle* h, int body1, int body2, double 
 
 mpmgpu_status mpmgpu_set_gravity(mpmgpu_handle* h, int use_vector, const double g[3]) {
   if (!h) return MPMGPU_ERR_ARG;
-  if (h->stepped) return fail(h, MPMGPU_ERR_STATE, "gravity must be set before the first step");
   for (int d = 0; d < 3; d++) h->sp.grav[d] = 0.0;
   if (use_vector) {
     if (!g) return fail(h, MPMGPU_ERR_ARG, "gravity vector missing");

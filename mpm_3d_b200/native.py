@@ -15,7 +15,8 @@ import numpy as np
 from . import inputs
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "lib", "libmpm_b200.so")
+# MPM_B200_LIB selects another build of the same library (e.g. a tuning variant)
+LIB_PATH = os.environ.get("MPM_B200_LIB", os.path.join(HERE, "lib", "libmpm_b200.so"))
 
 MODES = {"fp64": 0, "fp64_deterministic": 1, "mixed": 2}
 POINT_FIELDS = {"x": (0, 3), "u": (1, 3), "x_t": (2, 3), "mx_t": (3, 3), "b": (4, 3), "L": (5, 9), "T": (6, 9),
@@ -37,7 +38,8 @@ class _Config(ctypes.Structure):
 class _BodyDesc(ctypes.Structure):
     _fields_ = [("n", ctypes.c_int64), ("m", ctypes.c_void_p), ("v", ctypes.c_void_p), ("x", ctypes.c_void_p),
                 ("x_t", ctypes.c_void_p), ("active", ctypes.c_void_p), ("has_material", ctypes.c_int),
-                ("E", ctypes.c_double), ("nu", ctypes.c_double), ("has_boundary", ctypes.c_int)]
+                ("E", ctypes.c_double), ("nu", ctypes.c_double), ("has_boundary", ctypes.c_int),
+                ("u", ctypes.c_void_p), ("T", ctypes.c_void_p)]
 
 
 _lib = None
@@ -114,7 +116,7 @@ class GPUExplicitUSL:
                         active=np.ascontiguousarray(body.active, np.int32))
             desc = _BodyDesc(body.n, _ptr(arrs["m"]).value, _ptr(arrs["v"]).value, _ptr(arrs["x"]).value,
                              _ptr(arrs["x_t"]).value, _ptr(arrs["active"]).value, int(body.material), body.E, body.nu,
-                             int(body.boundary))
+                             int(body.boundary), None, None)
             bid = ctypes.c_int()
             self._check(self.lib.mpmgpu_add_body(self.h, ctypes.byref(desc), ctypes.byref(bid)))
         for c in case.contacts:

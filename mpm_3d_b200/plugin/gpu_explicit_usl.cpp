@@ -1,0 +1,233 @@
+// GPUExplicitUSL: mpm_3d Solver plugin over the C ABI of include/mpm_b200.h.
+// Compiled inside the reference tree; it uses only the
+// reference's public object interface.
+#include "gpu_explicit_usl.hpp"
+
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <iostream>
+#include <vector>
+
+#include "objects/bodies/bodies.hpp"
+#include "objects/boundaries/boundaries.hpp"
+#include "objects/contacts/contacts.hpp"
+#include "objects/grids/grids.hpp"
+#include "objects/materials/materials.hpp"
+#include "objects/points/points.hpp"
+
+namespace {
+
+[[noreturn]] void unsupported(const std::string& what) {
+  std::cerr << "GPUExplicitUSL: " << what << std::endl;
+  exit(0);
+}
+
+}  // namespace
+
+GPUExplicitUSL::~GPUExplicitUSL() {
+  if (handle) mpmgpu_destroy(handle);
+}
+
+void GPUExplicitUSL::check(mpmgpu_status s, const char* what) {
+  if (s == MPMGPU_OK) return;
+  std::cerr << "GPUExplicitUSL: " << what << ": " << mpmgpu_status_string(s) << " ("
+            << mpmgpu_last_error(handle) << ")" << std::endl;
+  exit(0);
+}
+
+// explicit_usl.cpp:25-44, plus the optional write-back interval.
+void GPUExplicitUSL::init(Job* job) {
+  if (int_props.size() >= 1) cpdi_spec = int_props[0];
+  if (int_props.size() >= 2) contact_spec = int_props[1];
+  if (int_props.size() >= 3) writeback_interval = int_props[2];
+  printf("Solver properties (cpdi_spec = %i, contact_spec = %i, writeback = %i).\n", cpdi_spec, contact_spec,
+         writeback_interval);
+  std::cout << "Solver Initialized." << std::endl;
+}
+
+// Device set-up on the first step: Job::init runs solver->init before the
+// grid and bodies exist (job.hpp:90-102).
+void GPUExplicitUSL::setUp(Job* job) {
+  CartesianLinear* grid = dynamic_cast<CartesianLinear*>(job->grid.get());
+  if (!grid) unsupported("grid class " + job->grid->object_name + " (CartesianLinear only)");
+  if (job->JOB_TYPE != Job::JOB_2D && job->JOB_TYPE != Job::JOB_3D)
+    unsupported("job TYPE " + std::to_string(job->JOB_TYPE) + " (2 or 3 only)");
+  const int dim = job->grid->GRID_DIM;
+  mpmgpu_config cfg = {};
+  cfg.dim = dim;
+  for (int d = 0; d < dim; d++) {
+    cfg.L[d] = grid->Lx(d);
+    cfg.N[d] = grid->Nx(d);
+  }
+  cfg.dt = job->dt;
+  cfg.cpdi_spec = cpdi_spec;
+  cfg.contact_spec = contact_spec;
+  cfg.mode = MPMGPU_MODE_FP64;
+  cfg.device = 0;
+  cfg.keep_debug = 1;  // node and contact fields are written in frames
+  cfg.sort_interval = 0;
+  check(mpmgpu_create(&cfg, &handle), "mpmgpu_create");
+
+  gpu_body.assign(job->bodies.size(), -1);
+  for (size_t b = 0; b < job->bodies.size(); b++) {
+    if (job->activeBodies[b] == 0) continue;
+    Body* body = job->bodies[b].get();
+    if (!dynamic_cast<DefaultPoints*>(body->points.get()))
+      unsupported("point class " + body->points->object_name + " (DefaultPoints only)");
+    Points* pts = body->points.get();
+    const int n = pts->x.size();
+    std::vector<double> x(3 * (size_t)n), xt(3 * (size_t)n), u(3 * (size_t)n), T(9 * (size_t)n);
+    std::vector<int32_t> active((size_t)n);
+    for (int i = 0; i < n; i++) {
+      for (int j = 0; j < 3; j++) {
+        x[3 * i + j] = pts->x(i, j);
+        xt[3 * i + j] = pts->x_t(i, j);
+        u[3 * i + j] = pts->u(i, j);
+      }
+      for (int k = 0; k < 9; k++) T[9 * i + k] = pts->T[i][k];
+      active[i] = pts->active(i);
+    }
+    mpmgpu_body_desc desc = {};
+    desc.n = n;
+    desc.m = pts->m.data();
+    desc.v = pts->v.data();
+    desc.x = x.data();
+    desc.x_t = xt.data();
+    desc.active = active.data();
+    desc.u = u.data();
+    desc.T = T.data();
+    if (body->activeMaterial) {
+      IsotropicLinearElasticity* mat = dynamic_cast<IsotropicLinearElasticity*>(body->material.get());
+      if (!mat) unsupported("material class " + body->material->object_name);
+      desc.has_material = 1;
+      desc.E = mat->E;
+      desc.nu = mat->nu;
+    }
+    if (body->activeBoundary) {
+      if (!dynamic_cast<CartesianBox*>(body->boundary.get()))
+        unsupported("boundary class " + body->boundary->object_name);
+      desc.has_boundary = 1;
+    }
+    int id = -1;
+    check(mpmgpu_add_body(handle, &desc, &id), "mpmgpu_add_body");
+    gpu_body[b] = id;
+  }
+  for (size_t c = 0; c < job->contacts.size(); c++) {
+    if (job->activeContacts[c] == 0) continue;
+    ContactHuang* ch = dynamic_cast<ContactHuang*>(job->contacts[c].get());
+    if (!ch) unsupported("contact class " + job->contacts[c]->object_name);
+    const int b1 = gpu_body[ch->bodyIDs[0]], b2 = gpu_body[ch->bodyIDs[1]];
+    if (b1 < 0 || b2 < 0) unsupported("contact between inactive bodies");
+    check(mpmgpu_add_contact(handle, b1, b2, ch->mu_f, nullptr), "mpmgpu_add_contact");
+  }
+  // the driver has applied gravity to every point before the loop
+  // (default_driver.cpp:58-60): take it from the points
+  for (size_t b = 0; b < job->bodies.size(); b++) {
+    if (gpu_body[b] < 0 || job->bodies[b]->points->b.size() == 0) continue;
+    for (int d = 0; d < 3; d++) gravity[d] = job->bodies[b]->points->b(0, d);
+    break;
+  }
+  check(mpmgpu_set_gravity(handle, 1, gravity), "mpmgpu_set_gravity");
+  const std::string& sname = job->serializer->object_name;
+  if ((sname == "DefaultVTK" || sname == "MinimalVTK") && !job->serializer->fp64_props.empty())
+    sample_rate = job->serializer->fp64_props[0];
+}
+
+// DefaultVTK::writeFrame writes when (t - t0) >= frames / rate or on its
+// first call (default_vtk.cpp:121-124); the driver calls it right after
+// step() with the same t (default_driver.cpp:65-80).
+bool GPUExplicitUSL::frameDue(Job* job) {
+  if (writeback_interval > 0) return steps % writeback_interval == 0;
+  if (!(sample_rate > 0)) return true;
+  if ((job->t - job->t0) >= (frames / sample_rate) || frames == 0) {
+    frames++;
+    return true;
+  }
+  return false;
+}
+
+// ExplicitUSL::step (explicit_usl.cpp:48-87) on the GPU.
+void GPUExplicitUSL::step(Job* job) {
+  if (!handle) setUp(job);
+  check(mpmgpu_step(handle, 1), "mpmgpu_step");
+  steps++;
+  // explicit_usl.cpp:80-81: the driver sets the next step's body force
+  job->driver->generateGravity(job);
+  job->driver->applyGravity(job);
+  for (size_t b = 0; b < job->bodies.size(); b++) {
+    if (gpu_body[b] < 0 || job->bodies[b]->points->b.size() == 0) continue;
+    double g[3];
+    for (int d = 0; d < 3; d++) g[d] = job->bodies[b]->points->b(0, d);
+    if (g[0] != gravity[0] || g[1] != gravity[1] || g[2] != gravity[2]) {
+      for (int d = 0; d < 3; d++) gravity[d] = g[d];
+      check(mpmgpu_set_gravity(handle, 1, gravity), "mpmgpu_set_gravity");
+    }
+    break;
+  }
+  if (frameDue(job)) writeBack(job);
+}
+
+void GPUExplicitUSL::writeBack(Job* job) {
+  check(mpmgpu_synchronize(handle), "mpmgpu_synchronize");
+  for (size_t b = 0; b < job->bodies.size(); b++) {
+    const int id = gpu_body[b];
+    if (id < 0) continue;
+    Points* pts = job->bodies[b]->points.get();
+    Nodes* nds = job->bodies[b]->nodes.get();
+    const int n = pts->x.size();
+    std::vector<double> buf(9 * (size_t)n);
+    auto vec3 = [&](int field, KinematicVectorArray& arr) {
+      check(mpmgpu_download_points(handle, id, field, buf.data()), "mpmgpu_download_points");
+      for (int i = 0; i < n; i++)
+        for (int j = 0; j < 3; j++) arr(i, j) = buf[3 * i + j];
+    };
+    vec3(MPMGPU_P_X, pts->x);
+    vec3(MPMGPU_P_U, pts->u);
+    vec3(MPMGPU_P_X_T, pts->x_t);
+    vec3(MPMGPU_P_MX_T, pts->mx_t);
+    check(mpmgpu_download_points(handle, id, MPMGPU_P_L, buf.data()), "mpmgpu_download_points");
+    for (int i = 0; i < n; i++)
+      for (int k = 0; k < 9; k++) pts->L[i][k] = buf[9 * i + k];
+    check(mpmgpu_download_points(handle, id, MPMGPU_P_T, buf.data()), "mpmgpu_download_points");
+    for (int i = 0; i < n; i++)
+      for (int k = 0; k < 9; k++) pts->T[i][k] = buf[9 * i + k];
+    check(mpmgpu_download_points(handle, id, MPMGPU_P_V, buf.data()), "mpmgpu_download_points");
+    for (int i = 0; i < n; i++) pts->v(i) = buf[i];
+    check(mpmgpu_download_points(handle, id, MPMGPU_P_ACTIVE, buf.data()), "mpmgpu_download_points");
+    for (int i = 0; i < n; i++) pts->active(i) = (int)buf[i];
+
+    const int nn = nds->x.size();
+    std::vector<double> nb(3 * (size_t)nn);
+    auto nvec3 = [&](int field, KinematicVectorArray& arr) {
+      check(mpmgpu_download_nodes(handle, id, field, nb.data()), "mpmgpu_download_nodes");
+      for (int i = 0; i < nn; i++)
+        for (int j = 0; j < 3; j++) arr(i, j) = nb[3 * i + j];
+    };
+    check(mpmgpu_download_nodes(handle, id, MPMGPU_N_M, nb.data()), "mpmgpu_download_nodes");
+    for (int i = 0; i < nn; i++) nds->m(i) = nb[i];
+    nvec3(MPMGPU_N_MX_T, nds->mx_t);
+    nvec3(MPMGPU_N_F, nds->f);
+    nvec3(MPMGPU_N_X_T, nds->x_t);
+    nvec3(MPMGPU_N_U, nds->u);
+    nvec3(MPMGPU_N_DIFF_X_T, nds->diff_x_t);
+  }
+  int gc = 0;
+  for (size_t c = 0; c < job->contacts.size(); c++) {
+    if (job->activeContacts[c] == 0) continue;
+    ContactHuang* ch = dynamic_cast<ContactHuang*>(job->contacts[c].get());
+    const int nn = ch->contact_normal.size();
+    std::vector<double> nb(3 * (size_t)nn);
+    check(mpmgpu_download_contact(handle, gc, MPMGPU_C_NORMAL, nb.data()), "mpmgpu_download_contact");
+    for (int i = 0; i < nn; i++)
+      for (int j = 0; j < 3; j++) ch->contact_normal(i, j) = nb[3 * i + j];
+    check(mpmgpu_download_contact(handle, gc, MPMGPU_C_FORCE, nb.data()), "mpmgpu_download_contact");
+    for (int i = 0; i < nn; i++)
+      for (int j = 0; j < 3; j++) ch->contact_force(i, j) = nb[3 * i + j];
+    gc++;
+  }
+}
+
+// As ExplicitUSL (explicit_usl.cpp:91-99): not implemented in the reference.
+std::string GPUExplicitUSL::saveState(Job* job, Serializer* serializer, std::string filepath) { return "err"; }
+int GPUExplicitUSL::loadState(Job* job, Serializer* serializer, std::string fullpath) { return 0; }
