@@ -44,6 +44,12 @@
 #include "objects/points/points.hpp"
 #include "objects/solvers/solvers.hpp"
 
+#ifdef MPM_WITH_GPU_PLUGIN
+// Drop-in check: the GPU solver plugin registered next to ExplicitUSL, as a
+// maintainer would add it to src/registry/registry.cpp.
+#include "gpu_explicit_usl.hpp"
+#endif
+
 namespace {
 
 class NullSerializer : public Serializer {
@@ -144,6 +150,9 @@ Registry<Solver>::Registry() {
   object["ExplicitUSL"] = &make<Solver, ExplicitUSL>;
   object["ParallelExplicitUSL"] = &make<Solver, ParallelExplicitUSL>;
   object["ThreadPoolExplicitUSL"] = &make<Solver, ThreadPoolExplicitUSL>;
+#ifdef MPM_WITH_GPU_PLUGIN
+  object["GPUExplicitUSL"] = &make<Solver, GPUExplicitUSL>;
+#endif
 }
 template <>
 Registry<Grid>::Registry() {

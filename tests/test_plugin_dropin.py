@@ -1,0 +1,58 @@
+"""Drop-in check of the GPUExplicitUSL Solver plugin.
+
+The reference's own Configurator, Job, DefaultBody/DefaultPoints/DefaultNodes,
+material, boundary and contact objects (compiled from its sources by
+oracle/Makefile) run the same .cfg twice: once with
+`solver { class = "ExplicitUSL" }` and once with `class = "GPUExplicitUSL"`
+(mpm_3d_b200/plugin, registered next to it as a maintainer would). The GPU
+run's host arrays, written back by the plugin, must match the reference
+solver within the FP64 parity tolerance.
+"""
+import tempfile
+
+import pytest
+
+import bridge
+from mpm_3d_b200 import inputs
+from util import FP64_TOL, assert_close, field_floor
+
+needs_gpu_harness = pytest.mark.skipif(not bridge.available("libmpmref_gpu.so"),
+                                       reason="oracle/_ref/libmpmref_gpu.so not built (needs the reference tree)")
+
+
+@needs_gpu_harness
+def test_plugin_configures_from_a_reference_config():
+    """Config parsing and Job::init with the plugin need no GPU: device set-up
+    is deferred to the first step."""
+    case = inputs.block_drop_2d()
+    cfg = inputs.write_case(case, tempfile.mkdtemp(), solver_class="GPUExplicitUSL")
+    job = bridge.ReferenceJob(cfg, build="gpu")
+    assert job.nbodies == 1 and job.n_points(0) == 144
+
+
+CASES = {
+    "block_drop_2d": (inputs.block_drop_2d, 30),
+    "collision_2d": (lambda: inputs.two_body_collision_2d(20, steps=20), 20),
+    "collision_3d_touching": (lambda: inputs.two_body_collision_3d(16, steps=8, gap=0.01), 8),
+}
+
+
+@needs_gpu_harness
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_dropin_matches_reference_solver(name):
+    make, steps = CASES[name]
+    case = make()
+    ref = bridge.ReferenceJob(inputs.write_case(case, tempfile.mkdtemp()), build="parity")
+    gpu = bridge.ReferenceJob(inputs.write_case(case, tempfile.mkdtemp(), solver_class="GPUExplicitUSL"), build="gpu")
+    for s in range(steps):
+        ref.step(1)
+        gpu.step(1)
+        for b in range(len(case.bodies)):
+            for f in ("x", "u", "x_t", "mx_t", "T", "L", "v", "active", "b"):
+                assert_close(gpu.points(b, f), ref.points(b, f), FP64_TOL, f"{name} step {s} point {f}",
+                             field_floor(case, f))
+            for f in ("m", "mx_t", "f", "x_t", "u", "diff_x_t"):
+                assert_close(gpu.nodes(b, f), ref.nodes(b, f), FP64_TOL, f"{name} step {s} node {f}")
+        for c in range(len(case.contacts)):
+            assert_close(gpu.contact(c, "force"), ref.contact(c, "force"), FP64_TOL, f"{name} step {s} contact")
