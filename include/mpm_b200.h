@@ -173,6 +173,31 @@ mpmgpu_status mpmgpu_download_contact(mpmgpu_handle* h, int contact, int field, 
 mpmgpu_status mpmgpu_dump_map(mpmgpu_handle* h, int body, int32_t* node, int32_t* point, double* s_val,
                               double* grad, int64_t* count);
 
+/* No counterpart in the reference: an allocation-free form of
+ * mpmgpu_dump_map for callers that cannot allocate device memory when they
+ * need the map, e.g. code running while a CUDA stream is being captured into
+ * a graph, a host framework that owns all device memory through its own
+ * pool, or a real-time loop that forbids cudaMalloc/cudaFree after set-up.
+ *
+ * Writes the same triplets as mpmgpu_dump_map, in the same reference order,
+ * into caller-provided DEVICE arrays: d_node[k], d_point[k] (int32),
+ * d_s[k] and d_grad[3k..3k+2] (double), k < capacity. *count receives the
+ * number of triplets; if it exceeds capacity the call writes the first
+ * `capacity` triplets and returns MPMGPU_ERR_ARG.
+ *
+ * Scratch lives in one static device array of the library (20 MiB, held by
+ * every GPU that loads the library until the process exits), so the call
+ * allocates nothing, but it serves at most 524,288 triplet slots: points x
+ * 4^dim (8,192 points in 3D, 32,768 in 2D); larger bodies are rejected with
+ * MPMGPU_ERR_ARG. The first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress); make that first call before any stream
+ * capture. Every call reuses the same array: calls that overlap on the GPU
+ * (from two handles or threads at once) race and must be serialised by the
+ * caller. Returns after the triplets are written (synchronises the handle's
+ * stream). */
+mpmgpu_status mpmgpu_dump_map_noalloc(mpmgpu_handle* h, int body, int32_t* d_node, int32_t* d_point, double* d_s,
+                                      double* d_grad, int64_t capacity, int64_t* count);
+
 /* Number of points of body b and nodes of the grid. */
 mpmgpu_status mpmgpu_sizes(const mpmgpu_handle* h, int body, int64_t* n_points, int64_t* n_nodes);
 

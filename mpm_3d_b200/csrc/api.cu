@@ -839,3 +839,150 @@ mpmgpu_status mpmgpu_destroy(mpmgpu_handle* h) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free map export (mpmgpu_dump_map_noalloc).
+//
+// For callers that must not allocate device memory when they read the map
+// (graph capture, caller-owned memory pools, real-time loops): the slot
+// buffers that mpmgpu_dump_map takes from cudaMalloc live here in one static
+// device array, and the compaction to the reference's triplet order runs on
+// the device into the caller's arrays. Nothing is allocated on the host or
+// the device by the call.
+// ---------------------------------------------------------------------------
+#include <mutex>
+
+namespace {
+
+// Slots served per call: points x 4^dim triplets of k_export_map.
+constexpr int64_t kNoAllocSlots = (int64_t)1 << 19;
+constexpr int64_t kNoAllocBlocks = kNoAllocSlots / 1024;
+// Carved into: node ids (int32), slot positions (int32), block offsets
+// (int32, +1 total), S values (double), gradients (3 doubles).
+constexpr size_t kNoAllocOffNode = 0;
+constexpr size_t kNoAllocOffPos = kNoAllocOffNode + 4 * kNoAllocSlots;
+constexpr size_t kNoAllocOffBlk = kNoAllocOffPos + 4 * kNoAllocSlots;
+constexpr size_t kNoAllocOffS = kNoAllocOffBlk + 256 * ((4 * (kNoAllocBlocks + 1) + 255) / 256);
+constexpr size_t kNoAllocOffGrad = kNoAllocOffS + 8 * kNoAllocSlots;
+constexpr size_t kNoAllocBytes = kNoAllocOffGrad + 24 * kNoAllocSlots;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+unsigned char* g_noalloc_base[kNoAllocMaxDevices] = {};
+
+// Device address of the scratch array on `device`, looked up once per device
+// with that device current (in host code the symbol is only a stand-in).
+mpmgpu_status noalloc_scratch(mpmgpu_handle* h, int device, unsigned char** out) {
+  if (device < 0 || device >= kNoAllocMaxDevices) return fail(h, MPMGPU_ERR_ARG, "device ordinal out of range");
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (g_noalloc_base[device] == nullptr) {
+    int current = 0;
+    CUDA_TRY(h, cudaGetDevice(&current));
+    if (current != device) CUDA_TRY(h, cudaSetDevice(device));
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (current != device) CUDA_TRY(h, cudaSetDevice(current));
+    if (e != cudaSuccess)
+      return fail(h, MPMGPU_ERR_CUDA, std::string("cudaGetSymbolAddress(map scratch): ") + cudaGetErrorString(e));
+    g_noalloc_base[device] = static_cast<unsigned char*>(p);
+  }
+  *out = g_noalloc_base[device];
+  return MPMGPU_OK;
+}
+
+// Exclusive scan, per 1024-slot block, of the "slot holds a triplet" flags;
+// block totals go to blk[blockIdx.x].
+__global__ void k_noalloc_slot_scan(const int32_t* node, int64_t nslots, int32_t* pos, int32_t* blk) {
+  __shared__ int32_t warp_sums[32];
+  const int64_t i = blockIdx.x * 1024LL + threadIdx.x;
+  const int flag = (i < nslots && node[i] >= 0) ? 1 : 0;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  int incl = flag;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  if (lane == 31) warp_sums[wid] = incl;
+  __syncthreads();
+  if (wid == 0) {
+    int ws = warp_sums[lane];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, ws, o);
+      if (lane >= o) ws += y;
+    }
+    warp_sums[lane] = ws;
+  }
+  __syncthreads();
+  const int before = wid > 0 ? warp_sums[wid - 1] : 0;
+  if (i < nslots) pos[i] = before + incl - flag;
+  if (threadIdx.x == 1023) blk[blockIdx.x] = before + incl;
+}
+
+// Writes the occupied slots, in slot order, to the caller's device arrays.
+__global__ void k_noalloc_compact(const int32_t* node, const double* s, const double* grad, const int32_t* pos,
+                                  const int32_t* blk, int64_t nslots, int per_point, int32_t* d_node, int32_t* d_point,
+                                  double* d_s, double* d_grad, int64_t capacity) {
+  const int64_t i = blockIdx.x * 1024LL + threadIdx.x;
+  if (i >= nslots || node[i] < 0) return;
+  const int64_t k = (int64_t)blk[blockIdx.x] + pos[i];
+  if (k >= capacity) return;
+  d_node[k] = node[i];
+  d_point[k] = (int32_t)(i / per_point);
+  d_s[k] = s[i];
+  for (int c = 0; c < 3; c++) d_grad[3 * k + c] = grad[3 * i + c];
+}
+
+}  // namespace
+
+extern "C" mpmgpu_status mpmgpu_dump_map_noalloc(mpmgpu_handle* h, int body, int32_t* d_node, int32_t* d_point,
+                                                  double* d_s, double* d_grad, int64_t capacity, int64_t* count) {
+  if (!h || !count || body < 0 || body >= (int)h->bodies.size()) return MPMGPU_ERR_ARG;
+  if (capacity < 0 || (capacity > 0 && (!d_node || !d_point || !d_s || !d_grad)))
+    return fail(h, MPMGPU_ERR_ARG, "output arrays missing");
+  BodyDev& B = h->bodies[(size_t)body];
+  const int per_point = h->g.cp * h->g.cp;
+  const int64_t nslots = B.n * per_point;
+  if (nslots > kNoAllocSlots)
+    return fail(h, MPMGPU_ERR_ARG,
+                "mpmgpu_dump_map_noalloc: body has " + std::to_string(B.n) + " points x " + std::to_string(per_point) +
+                    " triplet slots = " + std::to_string(nslots) + " slots, above the static scratch limit of " +
+                    std::to_string(kNoAllocSlots));
+  unsigned char* base = nullptr;
+  TRY(noalloc_scratch(h, h->cfg.device, &base));
+  int32_t* node = reinterpret_cast<int32_t*>(base + kNoAllocOffNode);
+  int32_t* pos = reinterpret_cast<int32_t*>(base + kNoAllocOffPos);
+  int32_t* blk = reinterpret_cast<int32_t*>(base + kNoAllocOffBlk);
+  double* s = reinterpret_cast<double*>(base + kNoAllocOffS);
+  double* grad = reinterpret_cast<double*>(base + kNoAllocOffGrad);
+  cudaStream_t st = h->stream;
+  // every slot read below is written first by this call: nothing carries over
+  if (B.n > 0) {
+    if (h->g.dim == 3)
+      k_export_map<3><<<grid_blocks(h, B.n, 128), 128, 0, st>>>(h->g, h->sp.cpdi, B.P, node, s, grad);
+    else
+      k_export_map<2><<<grid_blocks(h, B.n, 128), 128, 0, st>>>(h->g, h->sp.cpdi, B.P, node, s, grad);
+    TRY(check_launch(h, "k_export_map"));
+  }
+  const int nblk = (int)((nslots + 1023) / 1024);
+  if (nblk > 0) {
+    k_noalloc_slot_scan<<<nblk, 1024, 0, st>>>(node, nslots, pos, blk);
+    TRY(check_launch(h, "k_noalloc_slot_scan"));
+  }
+  k_scan_small<<<1, 1024, 0, st>>>(blk, nblk, blk + nblk);
+  TRY(check_launch(h, "k_scan_small"));
+  if (nblk > 0 && capacity > 0) {
+    k_noalloc_compact<<<nblk, 1024, 0, st>>>(node, s, grad, pos, blk, nslots, per_point, d_node, d_point, d_s, d_grad,
+                                             capacity);
+    TRY(check_launch(h, "k_noalloc_compact"));
+  }
+  int32_t total = 0;
+  CUDA_TRY(h, cudaMemcpyAsync(&total, blk + nblk, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(h, cudaStreamSynchronize(st));
+  *count = total;
+  if (total > capacity) return fail(h, MPMGPU_ERR_ARG, "capacity below the triplet count");
+  return MPMGPU_OK;
+}

@@ -68,6 +68,8 @@ def load() -> ctypes.CDLL:
     for fn in ("mpmgpu_download_points", "mpmgpu_download_nodes", "mpmgpu_download_contact"):
         getattr(lib, fn).argtypes = [vp, ctypes.c_int, ctypes.c_int, vp]
     lib.mpmgpu_dump_map.argtypes = [vp, ctypes.c_int, vp, vp, vp, vp, ctypes.POINTER(ctypes.c_int64)]
+    lib.mpmgpu_dump_map_noalloc.argtypes = [vp, ctypes.c_int, vp, vp, vp, vp, ctypes.c_int64,
+                                            ctypes.POINTER(ctypes.c_int64)]
     lib.mpmgpu_sizes.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)]
     lib.mpmgpu_launch_count.restype = ctypes.c_int64
     lib.mpmgpu_launch_count.argtypes = [vp]
@@ -207,3 +209,11 @@ class GPUExplicitUSL:
         self._check(self.lib.mpmgpu_dump_map(self.h, b, _ptr(node), _ptr(pt), _ptr(val), _ptr(grad),
                                              ctypes.byref(cnt)))
         return node, pt, val, grad
+
+    def map_noalloc(self, b: int, d_node: int, d_point: int, d_s: int, d_grad: int, capacity: int) -> int:
+        """Allocation-free triplet export into caller-owned device arrays
+        (integer device addresses); returns the triplet count."""
+        cnt = ctypes.c_int64()
+        self._check(self.lib.mpmgpu_dump_map_noalloc(self.h, b, d_node, d_point, d_s, d_grad, capacity,
+                                                     ctypes.byref(cnt)))
+        return cnt.value
