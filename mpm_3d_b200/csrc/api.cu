@@ -179,19 +179,23 @@ mpmgpu_status download(mpmgpu_handle* h, std::vector<T>& dst, const T* src, size
   return MPMGPU_OK;
 }
 
+// Point arrays hold n entries plus 8 of padding: the fused kernel's bulk
+// copies round their windows out to 16-byte boundaries and may read up to 3
+// entries past the last point.
 mpmgpu_status alloc_points(mpmgpu_handle* h, PointsDev& P, int64_t n, bool with_L) {
   P.n = n;
+  const size_t na = (size_t)n + 8;
   for (int d = 0; d < 3; d++) {
-    TRY(dev_alloc(h, &P.x[d], (size_t)n));
-    TRY(dev_alloc(h, &P.v[d], (size_t)n));
-    TRY(dev_alloc(h, &P.u[d], (size_t)n));
+    TRY(dev_alloc(h, &P.x[d], na));
+    TRY(dev_alloc(h, &P.v[d], na));
+    TRY(dev_alloc(h, &P.u[d], na));
   }
-  for (int c = 0; c < 6; c++) TRY(dev_alloc(h, &P.s[c], (size_t)n));
-  TRY(dev_alloc(h, &P.vol, (size_t)n));
-  TRY(dev_alloc(h, &P.m, (size_t)n));
-  TRY(dev_alloc(h, &P.ext, (size_t)n));
-  TRY(dev_alloc(h, &P.active, (size_t)n));
-  TRY(dev_alloc(h, &P.pid, (size_t)n));
+  for (int c = 0; c < 6; c++) TRY(dev_alloc(h, &P.s[c], na));
+  TRY(dev_alloc(h, &P.vol, na));
+  TRY(dev_alloc(h, &P.m, na));
+  TRY(dev_alloc(h, &P.ext, na));
+  TRY(dev_alloc(h, &P.active, na));
+  TRY(dev_alloc(h, &P.pid, na));
   P.L = nullptr;
   if (with_L) TRY(dev_alloc(h, &P.L, (size_t)n * 9));
   return MPMGPU_OK;
@@ -237,7 +241,8 @@ mpmgpu_status sort_body(mpmgpu_handle* h, BodyDev& B) {
     TRY(check_launch(h, "k_sort_scatter"));
     std::swap(B.P, B.Palt);
   }
-  k_bin_work<<<(bg.nbins + 255) / 256, 256, 0, st>>>(bg, B.bin_start, B.work_bin, B.work_start, B.work_end, B.nwork);
+  k_bin_work<<<(bg.nbins + 255) / 256, 256, 0, st>>>(bg, B.bin_start, kCap, B.work_bin, B.work_start, B.work_end,
+                                                      B.nwork);
   TRY(check_launch(h, "k_bin_work"));
   return MPMGPU_OK;
 }
@@ -491,9 +496,10 @@ mpmgpu_status mpmgpu_add_body(mpmgpu_handle* h, const mpmgpu_body_desc* desc, in
   TRY(dev_alloc(h, &B.rank, (size_t)n));
   TRY(dev_alloc(h, &B.cell_count, (size_t)bg.nbins * bg.cells_per_bin + 1));
   TRY(dev_alloc(h, &B.bin_start, (size_t)bg.nbins + 2));
-  TRY(dev_alloc(h, &B.work_bin, (size_t)bg.nbins));
-  TRY(dev_alloc(h, &B.work_start, (size_t)bg.nbins));
-  TRY(dev_alloc(h, &B.work_end, (size_t)bg.nbins));
+  const size_t max_items = (size_t)bg.nbins + (size_t)n / kCap + 1;
+  TRY(dev_alloc(h, &B.work_bin, max_items));
+  TRY(dev_alloc(h, &B.work_start, max_items));
+  TRY(dev_alloc(h, &B.work_end, max_items));
   TRY(dev_alloc(h, &B.nwork, 1));
   B.mat.has_material = desc->has_material;
   if (desc->has_material) {

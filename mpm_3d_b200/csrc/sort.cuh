@@ -159,22 +159,21 @@ __global__ void k_sort_scatter(BinGeom bg, int64_t n, const int32_t* key, const 
   }
 }
 
-// Work list of non-empty bins: bin id and [start, end) of its points.
-__global__ void k_bin_work(BinGeom bg, const int32_t* bin_start, int32_t* work_bin, int32_t* work_start,
+// Work list: every non-empty bin split into items of at most `cap` points:
+// bin id and [start, end) of the item's points. At most
+// nonempty_bins + n / cap items.
+__global__ void k_bin_work(BinGeom bg, const int32_t* bin_start, int cap, int32_t* work_bin, int32_t* work_start,
                            int32_t* work_end, int32_t* nwork) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
-  const int lane = threadIdx.x & 31;
-  const bool on = b < bg.nbins && bin_start[b + 1] > bin_start[b];
-  const unsigned mask = __ballot_sync(0xffffffffu, on);
-  if (mask == 0u) return;
-  int first = 0;
-  if (lane == 0) first = atomicAdd(nwork, __popc(mask));
-  first = __shfl_sync(0xffffffffu, first, 0);
-  if (on) {
-    const int w = first + __popc(mask & ((1u << lane) - 1u));
-    work_bin[w] = b;
-    work_start[w] = bin_start[b];
-    work_end[w] = bin_start[b + 1];
+  if (b >= bg.nbins) return;
+  const int s = bin_start[b], e = bin_start[b + 1];
+  if (e <= s) return;
+  const int items = (e - s + cap - 1) / cap;
+  const int first = atomicAdd(nwork, items);
+  for (int i = 0; i < items; i++) {
+    work_bin[first + i] = b;
+    work_start[first + i] = s + i * cap;
+    work_end[first + i] = min(e, s + (i + 1) * cap);
   }
 }
 
