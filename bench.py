@@ -275,9 +275,9 @@ def run_ours(args, rank, world, local):
     bpp = bytes_per_point_step(active_ratio)
     g_launches, g_ms = prof["g2p2g"]
     per_launch_ms = g_ms / max(1, g_launches)
-    # one fused launch per body per step processes that body's points; the
+    # the fused launches of a step together process every point once; the
     # algorithmic bytes of a launch are its points times bytes per point-step
-    points_per_launch = n / len(case.bodies)
+    points_per_launch = n * args.steps / max(1, g_launches)
     achieved_gbs = points_per_launch * bpp / (per_launch_ms * 1e-3) / 1e9
     peak, peak_kind = peaks()
     sim.close()

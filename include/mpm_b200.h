@@ -48,10 +48,11 @@ typedef enum {
 typedef enum {
   /* FP64 throughout; nodal sums use atomics (order varies run to run). */
   MPMGPU_MODE_FP64 = 0,
-  /* FP64 throughout; nodal sums in a fixed order: bit-reproducible. */
+  /* FP64 throughout; nodal sums in a fixed order: bit-reproducible
+   * (not available in this build: MPMGPU_ERR_UNSUPPORTED). */
   MPMGPU_MODE_FP64_DETERMINISTIC = 1,
-  /* FP32 particle state, shape functions and stress; FP64 nodal mass and
-   * momentum sums, nodal division and contact projection. */
+  /* FP32 particle state, shape functions and stress; FP64 nodal mass,
+   * momentum and force sums, nodal division and contact projection. */
   MPMGPU_MODE_MIXED = 2
 } mpmgpu_mode;
 
@@ -208,6 +209,11 @@ int64_t mpmgpu_launch_count(const mpmgpu_handle* h);
  * a caller can record its own events around mpmgpu_step. */
 void* mpmgpu_stream(const mpmgpu_handle* h);
 
+/* Nodes with mass (counted per body) in the last step's grid update, and
+ * the number of point visits that found a point outside its bin's staged
+ * tile since creation (drift between re-binnings). Synchronises. */
+mpmgpu_status mpmgpu_active_nodes(mpmgpu_handle* h, int64_t* nodes, int64_t* drifted);
+
 /* Per-stage device time accounting with CUDA events recorded on the
  * handle's stream around every launch of a stage. enable != 0 starts (and
  * resets) it, 0 stops it. Stages: 0 fused gather/scatter kernel, 1 grid
@@ -217,6 +223,100 @@ mpmgpu_status mpmgpu_profile(mpmgpu_handle* h, int enable);
 mpmgpu_status mpmgpu_profile_read(mpmgpu_handle* h, int stage, int64_t* launches, double* total_ms);
 
 mpmgpu_status mpmgpu_destroy(mpmgpu_handle* h);
+
+/* ------------------------------------------------------------------------
+ * Batch: many independent jobs advanced together.
+ *
+ * No counterpart in the reference, which runs one Job per process
+ * (main.cpp:60-106). A batch holds jobs of one dimension and one arithmetic
+ * form, each with its own grid, bodies, contacts, dt and step count; every
+ * mpmgpu_batch_step advances all jobs that still have steps, with one
+ * launch per stage for the whole batch (the step and the re-binning are
+ * replayed from CUDA graphs). Jobs may be added while others run: they join
+ * at the next step boundary; a job that has run its steps stops advancing
+ * and stays readable until it is removed. Each job computes exactly what a
+ * single-job handle with the same inputs computes (up to the order of the
+ * nodal sums).
+ * ---------------------------------------------------------------------- */
+
+typedef struct mpmgpu_batch mpmgpu_batch;
+
+typedef struct {
+  int dim;             /* 2 or 3 for every job of the batch */
+  int mode;            /* MPMGPU_MODE_FP64 or MPMGPU_MODE_MIXED */
+  int device;          /* CUDA device ordinal */
+  int sort_interval;   /* steps between re-binnings (0 = default 32) */
+  int points_per_item; /* points per CTA work item: 0 = default (512);
+                          3D: 256 or 512 (FP64), 256, 512 or 1024 (mixed);
+                          see mpmgpu_batch_autotune */
+  int no_graph;        /* 1: launch stage by stage instead of graph replay */
+  int keep_debug;      /* as mpmgpu_config.keep_debug */
+} mpmgpu_batch_config;
+
+/* One ContactHuang pair of a job (bodies are indices within the job). */
+typedef struct {
+  int body1, body2;
+  double mu;
+} mpmgpu_contact_desc;
+
+/* One job: grid / dt / cpdi_spec / contact_spec from `grid` (its mode,
+ * device, keep_debug and sort_interval are the batch's), its bodies and
+ * contacts, the driver gravity (as mpmgpu_set_gravity) and its step count. */
+typedef struct {
+  const mpmgpu_config* grid;
+  int nbodies;
+  const mpmgpu_body_desc* bodies;
+  int ncontacts;
+  const mpmgpu_contact_desc* contacts;
+  int gravity_vector;   /* 0 = DefaultDriver, 1 = the vector below */
+  double gravity[3];
+  int64_t steps;
+} mpmgpu_job_desc;
+
+mpmgpu_status mpmgpu_batch_create(const mpmgpu_batch_config* cfg, mpmgpu_batch** out);
+const char* mpmgpu_batch_last_error(const mpmgpu_batch* b);
+
+/* Device bytes the job will hold once added (for admission control). */
+mpmgpu_status mpmgpu_batch_footprint(const mpmgpu_batch* b, const mpmgpu_job_desc* job, int64_t* bytes);
+
+/* Copies the job's arrays to the device; the job joins at the next step. */
+mpmgpu_status mpmgpu_batch_add_job(mpmgpu_batch* b, const mpmgpu_job_desc* job, int* job_id);
+
+/* nsteps steps of every job that still has steps (asynchronous). */
+mpmgpu_status mpmgpu_batch_step(mpmgpu_batch* b, int nsteps);
+mpmgpu_status mpmgpu_batch_synchronize(mpmgpu_batch* b);
+
+/* Steps done and left of a job (host bookkeeping; no synchronisation). */
+mpmgpu_status mpmgpu_batch_job_state(const mpmgpu_batch* b, int job, int64_t* steps_done, int64_t* steps_left);
+mpmgpu_status mpmgpu_batch_sizes(const mpmgpu_batch* b, int job, int body, int64_t* n_points, int64_t* n_nodes);
+
+/* As mpmgpu_download_points, for body `body` of job `job`. */
+mpmgpu_status mpmgpu_batch_download_points(mpmgpu_batch* b, int job, int body, int field, double* out);
+
+/* Frees the job's device memory; it leaves the batch at the next step. */
+mpmgpu_status mpmgpu_batch_remove_job(mpmgpu_batch* b, int job);
+
+/* Jobs and points still stepping, and device bytes held by the batch. */
+mpmgpu_status mpmgpu_batch_counts(const mpmgpu_batch* b, int* live_jobs, int64_t* live_points, int64_t* bytes_in_use);
+
+/* Times `steps` steps of the current jobs for every available
+ * points-per-item choice (restoring the state after each trial) and keeps
+ * the fastest; the jobs' state after the call is the state before it. */
+mpmgpu_status mpmgpu_batch_autotune(mpmgpu_batch* b, int steps, int* points_per_item);
+int mpmgpu_batch_points_per_item(const mpmgpu_batch* b);
+
+/* As mpmgpu_active_nodes, over every job of the batch. */
+mpmgpu_status mpmgpu_batch_active_nodes(mpmgpu_batch* b, int64_t* nodes, int64_t* drifted);
+
+/* Per-stage event timing, as mpmgpu_profile (launches stage by stage while
+ * enabled). */
+mpmgpu_status mpmgpu_batch_profile(mpmgpu_batch* b, int enable);
+mpmgpu_status mpmgpu_batch_profile_read(mpmgpu_batch* b, int stage, int64_t* launches, double* total_ms);
+
+void* mpmgpu_batch_stream(const mpmgpu_batch* b);
+/* Kernel launches issued (a graph replay counts its kernels). */
+int64_t mpmgpu_batch_launch_count(const mpmgpu_batch* b);
+mpmgpu_status mpmgpu_batch_destroy(mpmgpu_batch* b);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,1487 @@
+// Host side of the step engine: a batch of independent jobs (each one the
+// reference's Job: a CartesianLinear grid, its DefaultBodies and
+// ContactHuang pairs) advanced together, one launch per stage for the whole
+// batch:
+//
+//   compact   active node blocks flagged by the last scatter -> work list
+//   grid      body force, contact, boundary, moveGrid on the active blocks
+//   g2p2g     per bin of points: gather + point update (this step), map
+//             build + scatter at the new positions (next step)
+//
+// plus, every sort_interval steps and whenever jobs join or leave, a
+// re-binning of every body's points. A job that joins is binned and primed
+// (a scatter-only pass of its bodies builds its first nodal sums) at the
+// next step boundary while the others keep their state; a job that has run
+// its steps stops advancing and keeps its state readable until removed.
+//
+// Kernels read sizes and per-job / per-body parameters from device tables,
+// so the step and the re-binning are captured once in CUDA graphs and stay
+// valid while jobs come and go (they are re-captured only when a capacity
+// grows). The single-job C ABI (mpmgpu_handle) is a batch of one job.
+#pragma once
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/mpm_b200.h"
+#include "fused.cuh"
+#include "kernels_fp64.cuh"
+#include "sort.cuh"
+
+namespace mpmb200 {
+
+#define MPM_CUDA_TRY(expr)                                                                            \
+  do {                                                                                                \
+    cudaError_t e_ = (expr);                                                                          \
+    if (e_ != cudaSuccess) return fail(MPMGPU_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+#define MPM_TRY(expr)               \
+  do {                              \
+    mpmgpu_status s_ = (expr);      \
+    if (s_ != MPMGPU_OK) return s_; \
+  } while (0)
+
+// Stages of the per-stage event profile.
+enum { kStageFused = 0, kStageGrid = 1, kStageCompact = 2, kStageRebin = 3, kStages = 4 };
+
+// Grid geometry of a job from its config (CartesianLinear::init,
+// cartesian.cpp:24-67) and the node-block / bin layouts.
+inline void make_geometry(const mpmgpu_config& cfg, Geom& g, MapConst& mc, BinGeom& bg) {
+  g = Geom{};
+  mc = MapConst{};
+  bg = BinGeom{};
+  g.dim = cfg.dim;
+  g.cp = 1 << cfg.dim;
+  g.nnodes = 1;
+  for (int d = 0; d < 3; d++) {
+    if (d < cfg.dim) {
+      g.L[d] = cfg.L[d];
+      g.N[d] = cfg.N[d];
+      g.h[d] = cfg.L[d] / cfg.N[d];  // cartesian.cpp:40
+      g.nn[d] = cfg.N[d] + 1;
+      g.nnodes *= g.nn[d];
+      mc.NL[d] = (double)cfg.N[d] / cfg.L[d];
+      mc.invh[d] = 1.0 / g.h[d];
+    } else {
+      g.nn[d] = 1;
+    }
+    mc.Lf[d] = (float)g.L[d];
+    mc.hf[d] = (float)g.h[d];
+    mc.NLf[d] = (float)mc.NL[d];
+    mc.invhf[d] = (float)mc.invh[d];
+  }
+  if (cfg.dim == 3) {
+    g.bsh[0] = g.bsh[1] = g.bsh[2] = 2;
+  } else {
+    g.bsh[0] = g.bsh[1] = 3;
+    g.bsh[2] = 0;
+  }
+  g.nblocks = 1;
+  for (int d = 0; d < 3; d++) {
+    const int ext = 1 << g.bsh[d];
+    g.nb[d] = (g.nn[d] + ext - 1) / ext;
+    g.nblocks *= g.nb[d];
+  }
+  g.nslots = g.nblocks * 64;
+  bg.B = cfg.dim == 3 ? 4 : 8;
+  bg.cells_per_bin = 64;
+  bg.nbx = (g.N[0] + bg.B - 1) / bg.B;
+  bg.nby = (g.N[1] + bg.B - 1) / bg.B;
+  bg.nbz = cfg.dim == 3 ? (g.N[2] + bg.B - 1) / bg.B : 1;
+  bg.nbins = bg.nbx * bg.nby * bg.nbz;
+  bg.T = bg.B + 3;
+  bg.tile_nodes = cfg.dim == 3 ? bg.T * bg.T * bg.T : bg.T * bg.T;
+}
+
+// IsotropicLinearElasticity constants, isolin.cpp:34-38.
+inline MaterialParams make_material(int has_material, double E, double nu) {
+  MaterialParams m{};
+  m.has_material = has_material;
+  if (has_material) {
+    const double G = E / (2.0 * (1.0 + nu));
+    const double K = E / (3.0 * (1.0 - 2 * nu));
+    m.G = G;
+    m.lambda = K - 2.0 * G / 3.0;
+  }
+  return m;
+}
+
+// Extent of a point, default_points.cpp:49-57 (computed once, never updated).
+inline double point_extent(int dim, double vol) { return dim == 2 ? 0.5 * std::sqrt(vol) : 0.5 * std::cbrt(vol); }
+
+// Particles per work item (CTA) available for each dimension and precision.
+inline bool cap_available(int dim, bool mixed, int cap) {
+  if (dim == 3) return mixed ? (cap == 256 || cap == 512 || cap == 1024) : (cap == 256 || cap == 512);
+  return cap == 512;
+}
+
+// Device bytes a job will hold: points (two buffers), nodal arrays, binning
+// and its share of the batch's scratch.
+inline int64_t job_footprint(const mpmgpu_config& cfg, bool mixed, bool keep_debug, int nbodies, const int64_t* npts,
+                             int ncontacts) {
+  Geom g;
+  MapConst mc;
+  BinGeom bg;
+  make_geometry(cfg, g, mc, bg);
+  const int64_t ps = mixed ? 4 : 8;
+  int64_t bytes = 0;
+  for (int b = 0; b < nbodies; b++) {
+    const int64_t n = npts[b] + 8;
+    bytes += 2 * n * (18 * ps + 8);             // two point buffers
+    if (keep_debug && !mixed) bytes += 2 * n * 72;
+    bytes += g.nslots * 8 * (7 + 6);            // accumulators + velocities
+    bytes += n * 8;                              // sort key + rank
+    bytes += ((int64_t)bg.nbins * bg.cells_per_bin + 1) * 4 + ((int64_t)bg.nbins + 2) * 4;
+    bytes += ((int64_t)bg.nbins + n / 256 + 1) * 16;
+    if (keep_debug) bytes += g.nslots * 8 * 7;
+  }
+  bytes += (int64_t)ncontacts * g.nslots * 8 * (3 + (keep_debug ? 6 : 0));
+  bytes += g.nblocks * (4 + 8 + 1 + 4);
+  return bytes;
+}
+
+// Type-independent interface of a batch (the C ABI holds this).
+class BatchBase {
+ public:
+  virtual ~BatchBase() = default;
+  std::string last_error;
+  mpmgpu_status fail(mpmgpu_status s, const std::string& msg) {
+    last_error = msg;
+    return s;
+  }
+  virtual int dim() const = 0;
+  virtual bool mixed() const = 0;
+  virtual cudaStream_t stream() const = 0;
+  virtual int64_t launches() const = 0;
+  virtual mpmgpu_status new_job(const mpmgpu_config& cfg, int64_t steps, int* job) = 0;
+  virtual mpmgpu_status add_body(int job, const mpmgpu_body_desc& desc, int* body) = 0;
+  virtual mpmgpu_status add_contact(int job, int b1, int b2, double mu, int* contact) = 0;
+  virtual mpmgpu_status set_gravity(int job, int use_vector, const double* g) = 0;
+  virtual mpmgpu_status admit(int job) = 0;
+  virtual mpmgpu_status step(int nsteps) = 0;
+  virtual mpmgpu_status synchronize() = 0;
+  virtual mpmgpu_status remove_job(int job) = 0;
+  virtual mpmgpu_status job_state(int job, int64_t* done, int64_t* left) const = 0;
+  virtual mpmgpu_status download_points(int job, int body, int field, double* out) = 0;
+  virtual mpmgpu_status download_nodes(int job, int body, int field, double* out) = 0;
+  virtual mpmgpu_status download_contact(int job, int contact, int field, double* out) = 0;
+  virtual mpmgpu_status sizes(int job, int body, int64_t* n_points, int64_t* n_nodes) const = 0;
+  virtual mpmgpu_status profile(int enable) = 0;
+  virtual mpmgpu_status profile_read(int stage, int64_t* launches, double* ms) = 0;
+  virtual mpmgpu_status autotune(int steps, int* best_cap) = 0;
+  virtual int64_t memory_in_use() const = 0;
+  virtual void counts(int* live_jobs, int64_t* live_points) const = 0;
+  virtual int points_per_item() const = 0;
+  virtual mpmgpu_status active_nodes(int64_t* nodes, int64_t* drifted) = 0;
+  // FP64 map export support (single-job handle)
+  virtual mpmgpu_status body_points_fp64(int job, int body, PointsDev* P, Geom* g, int* cpdi) = 0;
+  virtual int device() const = 0;
+};
+
+template <typename PT>
+class Batch : public BatchBase {
+ public:
+  struct HBody {
+    int64_t n = 0;
+    PointsT<PT> P{}, Palt{};
+    NodesAcc A{}, snap{};
+    NodesVel V{};
+    MaterialParams mat{};
+    int has_boundary = 0;
+    int needs_normal = 0;
+    int prime = 1;
+    std::vector<void*> allocs;
+  };
+  struct HJob {
+    mpmgpu_config cfg{};
+    Geom g{};
+    MapConst mc{};
+    BinGeom bg{};
+    StepParams sp{};
+    std::vector<HBody> bodies;
+    int nc = 0;
+    int cb1[kMaxContacts] = {}, cb2[kMaxContacts] = {};
+    double mu[kMaxContacts] = {};
+    double* normal_out[kMaxContacts] = {};
+    double* force_out[kMaxContacts] = {};
+    std::vector<void*> allocs;
+    int64_t block_off = -1;
+    int64_t steps_done = 0, steps_left = 0;
+    bool admitted = false;   // asked to join
+    bool in_tables = false;  // part of the stepped set
+    bool finished = false;
+    bool removed = false;
+    bool primed = false;     // has had its first scatter
+    int64_t bytes = 0;
+  };
+
+  Batch(int dim, int device, int sort_interval, int cap, int use_graph, int keep_debug)
+      : dim_(dim), device_(device), keep_debug_(keep_debug != 0), use_graph_(use_graph != 0) {
+    sort_interval_ = sort_interval > 0 ? sort_interval : 32;
+    cap_ = cap;
+  }
+
+  mpmgpu_status init() {
+    MPM_CUDA_TRY(cudaSetDevice(device_));
+    MPM_CUDA_TRY(cudaDeviceGetAttribute(&sm_count_, cudaDevAttrMultiProcessorCount, device_));
+    MPM_CUDA_TRY(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    if (cap_ == 0) cap_ = default_cap();
+    if (!cap_available(dim_, mixed(), cap_))
+      return fail(MPMGPU_ERR_ARG, "points_per_item " + std::to_string(cap_) + " not available for this form");
+    MPM_TRY(alloc_raw(&hdr_, 1, scratch_allocs_));
+    MPM_TRY(alloc_raw(&count_, 1, scratch_allocs_));
+    MPM_TRY(alloc_raw(&err_, 1, scratch_allocs_));
+    MPM_TRY(alloc_raw(&drift_, 1, scratch_allocs_));
+    MPM_TRY(alloc_raw(&nwork_, 1, scratch_allocs_));
+    MPM_TRY(alloc_raw(&active_nodes_, 1, scratch_allocs_));
+    return MPMGPU_OK;
+  }
+
+  ~Batch() override {
+    if (stream_) cudaStreamSynchronize(stream_);
+    drop_graphs();
+    for (int s = 0; s < kStages; s++)
+      for (auto& pr : pending_[s]) {
+        cudaEventDestroy(pr.first);
+        cudaEventDestroy(pr.second);
+      }
+    for (cudaEvent_t e : event_pool_) cudaEventDestroy(e);
+    for (auto& j : jobs_) free_job(j);
+    for (void* p : scratch_allocs_) cudaFree(p);
+    for (void* p : cap_allocs_) cudaFree(p);
+    if (stream_) cudaStreamDestroy(stream_);
+  }
+
+  int dim() const override { return dim_; }
+  bool mixed() const override { return sizeof(PT) == 4; }
+  cudaStream_t stream() const override { return stream_; }
+  int64_t launches() const override { return launches_; }
+  int points_per_item() const override { return cap_; }
+
+  // Nodes with mass (per body) in the last step's grid update, and points
+  // found outside their bin's tile since the batch was created.
+  mpmgpu_status active_nodes(int64_t* nodes, int64_t* drifted) override {
+    MPM_CUDA_TRY(cudaStreamSynchronize(stream_));
+    unsigned long long a = 0, d = 0;
+    MPM_CUDA_TRY(cudaMemcpy(&a, active_nodes_, sizeof(a), cudaMemcpyDeviceToHost));
+    MPM_CUDA_TRY(cudaMemcpy(&d, drift_, sizeof(d), cudaMemcpyDeviceToHost));
+    if (nodes) *nodes = (int64_t)a;
+    if (drifted) *drifted = (int64_t)d;
+    return MPMGPU_OK;
+  }
+  int device() const override { return device_; }
+
+  mpmgpu_status new_job(const mpmgpu_config& cfg, int64_t steps, int* job) override {
+    if (cfg.dim != dim_) return fail(MPMGPU_ERR_ARG, "job dimension differs from the batch's");
+    if (!(cfg.dt > 0)) return fail(MPMGPU_ERR_ARG, "dt must be positive");
+    if (cfg.cpdi_spec != 0 && cfg.cpdi_spec != 1) return fail(MPMGPU_ERR_ARG, "cpdi_spec must be 0 or 1");
+    if (cfg.contact_spec != 0 && cfg.contact_spec != 1) return fail(MPMGPU_ERR_ARG, "contact_spec must be 0 or 1");
+    for (int d = 0; d < cfg.dim; d++)
+      if (cfg.N[d] < 1 || !(cfg.L[d] > 0)) return fail(MPMGPU_ERR_ARG, "grid sizes must be positive");
+    if (steps < 0) return fail(MPMGPU_ERR_ARG, "negative step count");
+    HJob j;
+    j.cfg = cfg;
+    make_geometry(cfg, j.g, j.mc, j.bg);
+    j.sp.dt = cfg.dt;
+    j.sp.cpdi = cfg.cpdi_spec;
+    j.sp.contact_spec = cfg.contact_spec;
+    j.sp.keep_debug = keep_debug_ ? 1 : 0;
+    // DefaultDriver gravity until set otherwise (default_driver.cpp:90-105)
+    j.sp.grav[cfg.dim == 2 ? 1 : 2] = -9.81;
+    j.steps_left = steps;
+    jobs_.push_back(std::move(j));
+    *job = (int)jobs_.size() - 1;
+    return MPMGPU_OK;
+  }
+
+  mpmgpu_status add_body(int job, const mpmgpu_body_desc& desc, int* body) override {
+    HJob* j;
+    MPM_TRY(editable_job(job, &j));
+    if ((int)j->bodies.size() >= kMaxBodies) return fail(MPMGPU_ERR_UNSUPPORTED, "too many bodies in a job");
+    if (desc.n < 0 || desc.n > (int64_t)INT32_MAX / 2 || (desc.n > 0 && (!desc.m || !desc.v || !desc.x || !desc.x_t)))
+      return fail(MPMGPU_ERR_ARG, "body arrays missing or too many points");
+    const int D = dim_;
+    const int64_t n = desc.n;
+    HBody B;
+    B.n = n;
+    MPM_TRY(alloc_points(B.P, n, B.allocs, j->bytes));
+    MPM_TRY(alloc_points(B.Palt, n, B.allocs, j->bytes));
+    if (n > 0) {
+      std::vector<PT> tmp((size_t)n);
+      auto col = [&](const double* aos, int w, int d) {
+        for (int64_t i = 0; i < n; i++) tmp[(size_t)i] = (PT)aos[i * w + d];
+      };
+      for (int d = 0; d < D; d++) {
+        col(desc.x, 3, d);
+        MPM_TRY(upload(B.P.x[d], tmp));
+        col(desc.x_t, 3, d);
+        MPM_TRY(upload(B.P.v[d], tmp));
+      }
+      col(desc.m, 1, 0);
+      MPM_TRY(upload(B.P.m, tmp));
+      col(desc.v, 1, 0);
+      MPM_TRY(upload(B.P.vol, tmp));
+      for (int64_t i = 0; i < n; i++) tmp[(size_t)i] = (PT)point_extent(D, desc.v[i]);
+      MPM_TRY(upload(B.P.ext, tmp));
+      if (desc.u)
+        for (int d = 0; d < D; d++) {
+          col(desc.u, 3, d);
+          MPM_TRY(upload(B.P.u[d], tmp));
+        }
+      if (desc.T) {
+        // stored as xx yy zz xy yz xz (row-major 9 -> symmetric 6)
+        static const int idx[6] = {0, 4, 8, 1, 5, 2};
+        for (int c = 0; c < 6; c++) {
+          col(desc.T, 9, idx[c]);
+          MPM_TRY(upload(B.P.s[c], tmp));
+        }
+      }
+      std::vector<int32_t> act((size_t)n, 1), pid((size_t)n);
+      for (int64_t i = 0; i < n; i++) {
+        if (desc.active) act[(size_t)i] = desc.active[i] != 0 ? 1 : 0;
+        pid[(size_t)i] = (int32_t)i;
+      }
+      MPM_TRY(upload(B.P.active, act));
+      MPM_TRY(upload(B.P.pid, pid));
+    }
+    const size_t ns = (size_t)j->g.nslots;
+    MPM_TRY(alloc_dev(&B.A.m, ns, B.allocs, j->bytes));
+    for (int d = 0; d < 3; d++) {
+      MPM_TRY(alloc_dev(&B.A.mx[d], ns, B.allocs, j->bytes));
+      MPM_TRY(alloc_dev(&B.A.f[d], ns, B.allocs, j->bytes));
+      MPM_TRY(alloc_dev(&B.V.vt[d], ns, B.allocs, j->bytes));
+      MPM_TRY(alloc_dev(&B.V.dv[d], ns, B.allocs, j->bytes));
+    }
+    if (keep_debug_) {
+      MPM_TRY(alloc_dev(&B.snap.m, ns, B.allocs, j->bytes));
+      for (int d = 0; d < 3; d++) {
+        MPM_TRY(alloc_dev(&B.snap.mx[d], ns, B.allocs, j->bytes));
+        MPM_TRY(alloc_dev(&B.snap.f[d], ns, B.allocs, j->bytes));
+      }
+    }
+    B.mat = make_material(desc.has_material, desc.E, desc.nu);
+    B.has_boundary = desc.has_boundary;
+    j->bodies.push_back(std::move(B));
+    if (body) *body = (int)j->bodies.size() - 1;
+    return MPMGPU_OK;
+  }
+
+  mpmgpu_status add_contact(int job, int b1, int b2, double mu, int* contact) override {
+    HJob* j;
+    MPM_TRY(editable_job(job, &j));
+    const int nb = (int)j->bodies.size();
+    if (b1 < 0 || b2 < 0 || b1 >= nb || b2 >= nb || b1 == b2) return fail(MPMGPU_ERR_ARG, "contact bodies out of range");
+    if (j->nc >= kMaxContacts) return fail(MPMGPU_ERR_UNSUPPORTED, "too many contacts");
+    HBody& B1 = j->bodies[(size_t)b1];
+    const size_t ns = (size_t)j->g.nslots;
+    if (!B1.needs_normal) {
+      for (int d = 0; d < 3; d++) MPM_TRY(alloc_dev(&B1.A.nrm[d], ns, B1.allocs, j->bytes));
+      B1.needs_normal = 1;
+    }
+    const int c = j->nc;
+    j->cb1[c] = b1;
+    j->cb2[c] = b2;
+    j->mu[c] = mu;
+    if (keep_debug_) {
+      MPM_TRY(alloc_dev(&j->normal_out[c], 3 * ns, j->allocs, j->bytes));
+      MPM_TRY(alloc_dev(&j->force_out[c], 3 * ns, j->allocs, j->bytes));
+    }
+    j->nc++;
+    if (contact) *contact = c;
+    return MPMGPU_OK;
+  }
+
+  mpmgpu_status set_gravity(int job, int use_vector, const double* gv) override {
+    HJob* j;
+    MPM_TRY(live_job(job, &j));
+    double g3[3] = {0.0, 0.0, 0.0};
+    if (use_vector) {
+      if (!gv) return fail(MPMGPU_ERR_ARG, "gravity vector missing");
+      for (int d = 0; d < dim_; d++) g3[d] = gv[d];
+    } else {
+      g3[dim_ == 2 ? 1 : 2] = -9.81;
+    }
+    for (int d = 0; d < 3; d++) j->sp.grav[d] = g3[d];
+    tables_dirty_ = true;
+    return MPMGPU_OK;
+  }
+
+  mpmgpu_status admit(int job) override {
+    HJob* j;
+    MPM_TRY(editable_job(job, &j));
+    if (j->bodies.empty()) return fail(MPMGPU_ERR_STATE, "job has no bodies");
+    j->admitted = true;
+    membership_dirty_ = true;
+    return MPMGPU_OK;
+  }
+
+  mpmgpu_status step(int nsteps) override {
+    if (nsteps < 0) return fail(MPMGPU_ERR_ARG, "negative step count");
+    for (int s = 0; s < nsteps; s++) {
+      MPM_TRY(commit());
+      if (live_jobs_ == 0) break;
+      MPM_TRY(launch_step());
+      steps_since_sort_++;
+      bool finished_any = false;
+      for (auto& j : jobs_) {
+        if (!j.in_tables) continue;
+        j.steps_done++;
+        if (--j.steps_left <= 0) {
+          j.finished = true;
+          finished_any = true;
+        }
+      }
+      if (finished_any) membership_dirty_ = true;
+      if (steps_since_sort_ >= sort_interval_ && !membership_dirty_) MPM_TRY(launch_sort());
+    }
+    return MPMGPU_OK;
+  }
+
+  mpmgpu_status synchronize() override {
+    MPM_CUDA_TRY(cudaStreamSynchronize(stream_));
+    int flag = 0;
+    MPM_CUDA_TRY(cudaMemcpy(&flag, err_, sizeof(int), cudaMemcpyDeviceToHost));
+    if (flag & kErrWideSpan) return fail(MPMGPU_ERR_DEVICE, "point corners span more than two cells (extent > cell size)");
+    if (flag & kErrElemAlias) return fail(MPMGPU_ERR_DEVICE, "point within rounding of the upper domain face");
+    if (flag & kErrWaitTimeout) return fail(MPMGPU_ERR_DEVICE, "a bulk copy did not complete within the wait limit");
+    return MPMGPU_OK;
+  }
+
+  mpmgpu_status remove_job(int job) override {
+    if (job < 0 || job >= (int)jobs_.size() || jobs_[(size_t)job].removed) return fail(MPMGPU_ERR_ARG, "no such job");
+    MPM_CUDA_TRY(cudaStreamSynchronize(stream_));
+    HJob& j = jobs_[(size_t)job];
+    if (j.in_tables) membership_dirty_ = true;
+    j.finished = true;
+    j.admitted = false;
+    if (j.block_off >= 0 && j.in_tables) {
+      // the next compaction must not see its blocks
+      MPM_CUDA_TRY(cudaMemsetAsync(flags_ + j.block_off, 0, sizeof(uint32_t) * j.g.nblocks, stream_));
+    }
+    MPM_CUDA_TRY(cudaStreamSynchronize(stream_));
+    free_job(j);
+    j.removed = true;
+    return MPMGPU_OK;
+  }
+
+  mpmgpu_status job_state(int job, int64_t* done, int64_t* left) const override {
+    if (job < 0 || job >= (int)jobs_.size()) return MPMGPU_ERR_ARG;
+    const HJob& j = jobs_[(size_t)job];
+    if (done) *done = j.steps_done;
+    if (left) *left = j.finished ? 0 : j.steps_left;
+    return MPMGPU_OK;
+  }
+
+  mpmgpu_status sizes(int job, int body, int64_t* n_points, int64_t* n_nodes) const override {
+    if (job < 0 || job >= (int)jobs_.size()) return MPMGPU_ERR_ARG;
+    const HJob& j = jobs_[(size_t)job];
+    if (body < 0 || body >= (int)j.bodies.size()) return MPMGPU_ERR_ARG;
+    if (n_points) *n_points = j.bodies[(size_t)body].n;
+    if (n_nodes) *n_nodes = j.g.nnodes;
+    return MPMGPU_OK;
+  }
+
+  mpmgpu_status body_points_fp64(int job, int body, PointsDev* P, Geom* g, int* cpdi) override {
+    if (mixed()) return fail(MPMGPU_ERR_UNSUPPORTED, "map export needs the FP64 form");
+    if (job < 0 || job >= (int)jobs_.size()) return fail(MPMGPU_ERR_ARG, "no such job");
+    HJob& j = jobs_[(size_t)job];
+    if (body < 0 || body >= (int)j.bodies.size()) return fail(MPMGPU_ERR_ARG, "no such body");
+    std::memcpy(P, &j.bodies[(size_t)body].P, sizeof(PointsDev));
+    *g = j.g;
+    *cpdi = j.sp.cpdi;
+    return MPMGPU_OK;
+  }
+
+  int64_t memory_in_use() const override {
+    int64_t b = scratch_bytes_;
+    for (const auto& j : jobs_)
+      if (!j.removed) b += j.bytes;
+    return b;
+  }
+
+  void counts(int* live_jobs, int64_t* live_points) const override {
+    int lj = 0;
+    int64_t lp = 0;
+    for (const auto& j : jobs_)
+      if (j.admitted && !j.finished && !j.removed) {
+        lj++;
+        for (const auto& b : j.bodies) lp += b.n;
+      }
+    if (live_jobs) *live_jobs = lj;
+    if (live_points) *live_points = lp;
+  }
+
+  // ---- downloads (reference layout, original point order) ----
+
+  mpmgpu_status download_points(int job, int body, int field, double* out) override {
+    HJob* j;
+    HBody* B;
+    MPM_TRY(readable_body(job, body, &j, &B));
+    MPM_TRY(synchronize());
+    const int64_t n = B->n;
+    const int D = dim_;
+    std::vector<int32_t> pid;
+    MPM_TRY(download(pid, B->P.pid, (size_t)n));
+    std::vector<PT> tmp;
+    auto vec3 = [&](PT* const* arr) -> mpmgpu_status {
+      for (int64_t i = 0; i < 3 * n; i++) out[i] = 0.0;
+      for (int d = 0; d < D; d++) {
+        MPM_TRY(download(tmp, arr[d], (size_t)n));
+        for (int64_t i = 0; i < n; i++) out[3 * (int64_t)pid[(size_t)i] + d] = (double)tmp[(size_t)i];
+      }
+      return MPMGPU_OK;
+    };
+    auto scal = [&](const PT* arr) -> mpmgpu_status {
+      MPM_TRY(download(tmp, arr, (size_t)n));
+      for (int64_t i = 0; i < n; i++) out[pid[(size_t)i]] = (double)tmp[(size_t)i];
+      return MPMGPU_OK;
+    };
+    switch (field) {
+      case MPMGPU_P_X: return vec3(B->P.x);
+      case MPMGPU_P_U: return vec3(B->P.u);
+      case MPMGPU_P_X_T: return vec3(B->P.v);
+      case MPMGPU_P_MX_T: {
+        MPM_TRY(vec3(B->P.v));
+        std::vector<PT> m;
+        MPM_TRY(download(m, B->P.m, (size_t)n));
+        // movePoints: mx_t = m * x_t (explicit_usl.cpp:295-297)
+        for (int64_t i = 0; i < n; i++) {
+          const int64_t q = pid[(size_t)i];
+          for (int d = 0; d < D; d++) out[3 * q + d] = (double)m[(size_t)i] * out[3 * q + d];
+        }
+        return MPMGPU_OK;
+      }
+      case MPMGPU_P_B:
+        for (int64_t i = 0; i < n; i++)
+          for (int d = 0; d < 3; d++) out[3 * i + d] = j->sp.grav[d];
+        return MPMGPU_OK;
+      case MPMGPU_P_L: {
+        if (!B->P.L) return fail(MPMGPU_ERR_STATE, "L is kept only with keep_debug in the FP64 form");
+        std::vector<double> L;
+        MPM_TRY(download(L, B->P.L, (size_t)n * 9));
+        for (int64_t i = 0; i < n; i++)
+          for (int k = 0; k < 9; k++) out[9 * (int64_t)pid[(size_t)i] + k] = L[(size_t)(9 * i + k)];
+        return MPMGPU_OK;
+      }
+      case MPMGPU_P_T: {
+        static const int idx[9] = {0, 3, 5, 3, 1, 4, 5, 4, 2};
+        std::vector<std::vector<PT>> s(6);
+        for (int c = 0; c < 6; c++) MPM_TRY(download(s[(size_t)c], B->P.s[c], (size_t)n));
+        for (int64_t i = 0; i < n; i++)
+          for (int k = 0; k < 9; k++) out[9 * (int64_t)pid[(size_t)i] + k] = (double)s[(size_t)idx[k]][(size_t)i];
+        return MPMGPU_OK;
+      }
+      case MPMGPU_P_M: return scal(B->P.m);
+      case MPMGPU_P_V: return scal(B->P.vol);
+      case MPMGPU_P_EXTENT: return scal(B->P.ext);
+      case MPMGPU_P_ACTIVE: {
+        std::vector<int32_t> a;
+        MPM_TRY(download(a, B->P.active, (size_t)n));
+        // 2 = left the domain at the last move: still active until the next
+        // map build deactivates it, as in the reference
+        for (int64_t i = 0; i < n; i++) out[pid[(size_t)i]] = a[(size_t)i] != 0 ? 1.0 : 0.0;
+        return MPMGPU_OK;
+      }
+    }
+    return fail(MPMGPU_ERR_ARG, "unknown point field");
+  }
+
+  mpmgpu_status download_nodes(int job, int body, int field, double* out) override {
+    HJob* j;
+    HBody* B;
+    MPM_TRY(readable_body(job, body, &j, &B));
+    MPM_TRY(synchronize());
+    const int D = dim_;
+    const bool dbg = B->snap.m != nullptr;
+    if (!j->primed || j->block_off < 0) {
+      for (int64_t i = 0; i < j->g.nnodes * (field == MPMGPU_N_M ? 1 : 3); i++) out[i] = 0.0;
+      return MPMGPU_OK;
+    }
+    switch (field) {
+      case MPMGPU_N_M:
+        if (!dbg) return fail(MPMGPU_ERR_STATE, "nodal m is kept only with keep_debug");
+        return nodes_to_ref(*j, &B->snap.m, 1, 1, out);
+      case MPMGPU_N_MX_T:
+        if (!dbg) return fail(MPMGPU_ERR_STATE, "nodal mx_t is kept only with keep_debug");
+        return nodes_to_ref(*j, B->snap.mx, D, 3, out);
+      case MPMGPU_N_F:
+        if (!dbg) return fail(MPMGPU_ERR_STATE, "nodal f is kept only with keep_debug");
+        return nodes_to_ref(*j, B->snap.f, D, 3, out);
+      case MPMGPU_N_X_T: return nodes_to_ref(*j, B->V.vt, D, 3, out);
+      case MPMGPU_N_DIFF_X_T: return nodes_to_ref(*j, B->V.dv, D, 3, out);
+      case MPMGPU_N_U: {
+        MPM_TRY(nodes_to_ref(*j, B->V.vt, D, 3, out));
+        // moveGrid: u = dt * x_t (explicit_usl.cpp:252)
+        for (int64_t i = 0; i < 3 * j->g.nnodes; i++) out[i] = j->sp.dt * out[i];
+        return MPMGPU_OK;
+      }
+    }
+    return fail(MPMGPU_ERR_ARG, "unknown node field");
+  }
+
+  mpmgpu_status download_contact(int job, int contact, int field, double* out) override {
+    if (job < 0 || job >= (int)jobs_.size() || jobs_[(size_t)job].removed) return fail(MPMGPU_ERR_ARG, "no such job");
+    HJob& j = jobs_[(size_t)job];
+    if (contact < 0 || contact >= j.nc) return fail(MPMGPU_ERR_ARG, "no such contact");
+    if (!keep_debug_) return fail(MPMGPU_ERR_STATE, "contact fields are kept only with keep_debug");
+    if (field != MPMGPU_C_NORMAL && field != MPMGPU_C_FORCE) return fail(MPMGPU_ERR_ARG, "unknown contact field");
+    MPM_TRY(synchronize());
+    const Geom& g = j.g;
+    double* src = (field == MPMGPU_C_NORMAL) ? j.normal_out[contact] : j.force_out[contact];
+    std::vector<double> tmp;
+    MPM_TRY(download(tmp, src, 3 * (size_t)g.nslots));
+    std::vector<uint8_t> act((size_t)g.nblocks, 0);
+    if (j.block_off >= 0) MPM_TRY(download(act, was_active_ + j.block_off, (size_t)g.nblocks));
+    const double nan = std::nan("");
+    for (int k = 0; k < g.nn[2]; k++)
+      for (int jj = 0; jj < g.nn[1]; jj++)
+        for (int i = 0; i < g.nn[0]; i++) {
+          const int64_t id = i + (int64_t)g.nn[0] * (jj + (int64_t)g.nn[1] * k);
+          const int64_t s = node_slot(g, i, jj, k);
+          const bool on = j.primed && act[(size_t)node_block(g, i, jj, k)] != 0;
+          for (int d = 0; d < 3; d++) {
+            double v = tmp[(size_t)(3 * s + d)];
+            // the reference normalises every node's normal; a zero normal gives 0 * (1/0)
+            if (!on) v = (field == MPMGPU_C_NORMAL) ? (d < g.dim ? nan : 0.0) : 0.0;
+            out[3 * id + d] = v;
+          }
+        }
+    return MPMGPU_OK;
+  }
+
+  // ---- profiling ----
+
+  mpmgpu_status profile(int enable) override {
+    MPM_CUDA_TRY(cudaStreamSynchronize(stream_));
+    for (int s = 0; s < kStages; s++) {
+      for (auto& pr : pending_[s]) {
+        event_pool_.push_back(pr.first);
+        event_pool_.push_back(pr.second);
+      }
+      pending_[s].clear();
+      stage_launches_[s] = 0;
+      stage_ms_[s] = 0.0;
+    }
+    profiling_ = enable != 0;
+    return MPMGPU_OK;
+  }
+
+  mpmgpu_status profile_read(int stage, int64_t* launches, double* total_ms) override {
+    if (stage < 0 || stage >= kStages) return fail(MPMGPU_ERR_ARG, "no such stage");
+    MPM_CUDA_TRY(cudaStreamSynchronize(stream_));
+    for (int s = 0; s < kStages; s++) {
+      for (auto& pr : pending_[s]) {
+        float ms = 0.0f;
+        MPM_CUDA_TRY(cudaEventElapsedTime(&ms, pr.first, pr.second));
+        stage_ms_[s] += ms;
+        stage_launches_[s]++;
+        event_pool_.push_back(pr.first);
+        event_pool_.push_back(pr.second);
+      }
+      pending_[s].clear();
+    }
+    if (launches) *launches = stage_launches_[stage];
+    if (total_ms) *total_ms = stage_ms_[stage];
+    return MPMGPU_OK;
+  }
+
+  // ---- autotuning ----
+
+  // Times `steps` steps of the current jobs with every available
+  // points-per-item choice, restoring the state after each trial, and keeps
+  // the fastest. The simulation state after the call is the state before it.
+  mpmgpu_status autotune(int steps, int* best_cap) override {
+    if (steps < 1) return fail(MPMGPU_ERR_ARG, "autotune needs at least one step");
+    MPM_TRY(commit());
+    if (live_jobs_ == 0) return fail(MPMGPU_ERR_STATE, "no jobs to tune on");
+    MPM_TRY(snapshot_save());
+    const int caps[3] = {256, 512, 1024};
+    const int original = cap_;
+    int best = original;
+    float best_ms = 1e30f;
+    cudaEvent_t e0, e1;
+    MPM_CUDA_TRY(cudaEventCreate(&e0));
+    MPM_CUDA_TRY(cudaEventCreate(&e1));
+    mpmgpu_status st = MPMGPU_OK;
+    for (int ci = 0; ci < 3 && st == MPMGPU_OK; ci++) {
+      if (!cap_available(dim_, mixed(), caps[ci])) continue;
+      cap_ = caps[ci];
+      drop_graphs();
+      st = launch_sort();   // work items depend on the item size
+      for (int w = 0; w < 2 && st == MPMGPU_OK; w++) st = launch_step();
+      if (st != MPMGPU_OK) break;
+      cudaEventRecord(e0, stream_);
+      for (int s = 0; s < steps && st == MPMGPU_OK; s++) st = launch_step();
+      cudaEventRecord(e1, stream_);
+      if (cudaEventSynchronize(e1) != cudaSuccess) st = fail(MPMGPU_ERR_CUDA, "autotune timing failed");
+      float ms = 0.0f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (st == MPMGPU_OK && ms < best_ms) {
+        best_ms = ms;
+        best = caps[ci];
+      }
+      if (st == MPMGPU_OK) st = snapshot_restore();
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cap_ = (st == MPMGPU_OK) ? best : original;
+    drop_graphs();
+    snapshot_free();
+    MPM_TRY(st);
+    MPM_TRY(launch_sort());
+    if (best_cap) *best_cap = cap_;
+    return MPMGPU_OK;
+  }
+
+ private:
+  // ---- allocation helpers ----
+
+  template <typename T>
+  mpmgpu_status alloc_raw(T** p, size_t count, std::vector<void*>& owner) {
+    void* q = nullptr;
+    const size_t bytes = std::max<size_t>(count * sizeof(T), 16);
+    cudaError_t e = cudaMalloc(&q, bytes);
+    if (e != cudaSuccess) return fail(MPMGPU_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    owner.push_back(q);
+    e = cudaMemsetAsync(q, 0, bytes, stream_);
+    if (e != cudaSuccess) return fail(MPMGPU_ERR_CUDA, std::string("cudaMemset: ") + cudaGetErrorString(e));
+    *p = static_cast<T*>(q);
+    scratch_bytes_ += (int64_t)bytes;
+    return MPMGPU_OK;
+  }
+
+  template <typename T>
+  mpmgpu_status alloc_dev(T** p, size_t count, std::vector<void*>& owner, int64_t& bytes) {
+    void* q = nullptr;
+    const size_t nb = std::max<size_t>(count * sizeof(T), 16);
+    cudaError_t e = cudaMalloc(&q, nb);
+    if (e != cudaSuccess) return fail(MPMGPU_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    owner.push_back(q);
+    e = cudaMemsetAsync(q, 0, nb, stream_);
+    if (e != cudaSuccess) return fail(MPMGPU_ERR_CUDA, std::string("cudaMemset: ") + cudaGetErrorString(e));
+    *p = static_cast<T*>(q);
+    bytes += (int64_t)nb;
+    return MPMGPU_OK;
+  }
+
+  // Point arrays hold n entries plus 8 of padding: the fused kernel's bulk
+  // copies round their windows out to 16-byte boundaries and may read up to
+  // 3 entries past the last point.
+  mpmgpu_status alloc_points(PointsT<PT>& P, int64_t n, std::vector<void*>& owner, int64_t& bytes) {
+    P = PointsT<PT>{};
+    P.n = n;
+    const size_t na = (size_t)n + 8;
+    for (int d = 0; d < 3; d++) {
+      MPM_TRY(alloc_dev(&P.x[d], na, owner, bytes));
+      MPM_TRY(alloc_dev(&P.v[d], na, owner, bytes));
+      MPM_TRY(alloc_dev(&P.u[d], na, owner, bytes));
+    }
+    for (int c = 0; c < 6; c++) MPM_TRY(alloc_dev(&P.s[c], na, owner, bytes));
+    MPM_TRY(alloc_dev(&P.vol, na, owner, bytes));
+    MPM_TRY(alloc_dev(&P.m, na, owner, bytes));
+    MPM_TRY(alloc_dev(&P.ext, na, owner, bytes));
+    MPM_TRY(alloc_dev(&P.active, na, owner, bytes));
+    MPM_TRY(alloc_dev(&P.pid, na, owner, bytes));
+    P.L = nullptr;
+    if (keep_debug_ && !mixed()) MPM_TRY(alloc_dev(&P.L, (size_t)n * 9, owner, bytes));
+    return MPMGPU_OK;
+  }
+
+  void free_job(HJob& j) {
+    for (auto& b : j.bodies) {
+      for (void* p : b.allocs) cudaFree(p);
+      b.allocs.clear();
+    }
+    for (void* p : j.allocs) cudaFree(p);
+    j.allocs.clear();
+    j.bytes = 0;
+  }
+
+  template <typename T>
+  mpmgpu_status upload(T* dst, const std::vector<T>& src) {
+    if (src.empty()) return MPMGPU_OK;
+    MPM_CUDA_TRY(cudaMemcpyAsync(dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice, stream_));
+    MPM_CUDA_TRY(cudaStreamSynchronize(stream_));
+    return MPMGPU_OK;
+  }
+
+  template <typename T>
+  mpmgpu_status download(std::vector<T>& dst, const T* src, size_t n) {
+    dst.resize(n);
+    if (n == 0) return MPMGPU_OK;
+    MPM_CUDA_TRY(cudaMemcpyAsync(dst.data(), src, n * sizeof(T), cudaMemcpyDeviceToHost, stream_));
+    MPM_CUDA_TRY(cudaStreamSynchronize(stream_));
+    return MPMGPU_OK;
+  }
+
+  mpmgpu_status editable_job(int job, HJob** out) {
+    if (job < 0 || job >= (int)jobs_.size() || jobs_[(size_t)job].removed) return fail(MPMGPU_ERR_ARG, "no such job");
+    HJob& j = jobs_[(size_t)job];
+    if (j.admitted) return fail(MPMGPU_ERR_STATE, "bodies and contacts must be added before the job starts");
+    *out = &j;
+    return MPMGPU_OK;
+  }
+
+  mpmgpu_status live_job(int job, HJob** out) {
+    if (job < 0 || job >= (int)jobs_.size() || jobs_[(size_t)job].removed) return fail(MPMGPU_ERR_ARG, "no such job");
+    *out = &jobs_[(size_t)job];
+    return MPMGPU_OK;
+  }
+
+  mpmgpu_status readable_body(int job, int body, HJob** j, HBody** b) {
+    MPM_TRY(live_job(job, j));
+    if (body < 0 || body >= (int)(*j)->bodies.size()) return fail(MPMGPU_ERR_ARG, "no such body");
+    *b = &(*j)->bodies[(size_t)body];
+    return MPMGPU_OK;
+  }
+
+  int default_cap() const { return 512; }
+
+  // Copies a block-linear nodal array (comps SoA components) to reference
+  // node order; nodes of blocks that were not active in the last step read 0.
+  mpmgpu_status nodes_to_ref(HJob& j, double* const* arr, int comps, int width, double* out) {
+    const Geom& g = j.g;
+    std::vector<uint8_t> act;
+    MPM_TRY(download(act, was_active_ + j.block_off, (size_t)g.nblocks));
+    for (int64_t i = 0; i < g.nnodes * width; i++) out[i] = 0.0;
+    std::vector<double> tmp;
+    for (int d = 0; d < comps; d++) {
+      MPM_TRY(download(tmp, arr[d], (size_t)g.nslots));
+      for (int k = 0; k < g.nn[2]; k++)
+        for (int jj = 0; jj < g.nn[1]; jj++)
+          for (int i = 0; i < g.nn[0]; i++) {
+            const int64_t id = i + (int64_t)g.nn[0] * (jj + (int64_t)g.nn[1] * k);
+            const bool on = act[(size_t)node_block(g, i, jj, k)] != 0;
+            out[id * width + d] = on ? tmp[(size_t)node_slot(g, i, jj, k)] : 0.0;
+          }
+    }
+    return MPMGPU_OK;
+  }
+
+  // ---- block space (first-fit ranges, stable for a job's lifetime) ----
+
+  int64_t block_alloc(int64_t len) {
+    for (size_t i = 0; i < free_.size(); i++) {
+      if (free_[i].second >= len) {
+        const int64_t off = free_[i].first;
+        free_[i].first += len;
+        free_[i].second -= len;
+        if (free_[i].second == 0) free_.erase(free_.begin() + (long)i);
+        return off;
+      }
+    }
+    // grow at the end (merging a free tail)
+    int64_t off = block_end_;
+    if (!free_.empty() && free_.back().first + free_.back().second == block_end_) {
+      off = free_.back().first;
+      free_.pop_back();
+    }
+    block_end_ = off + len;
+    return off;
+  }
+
+  void block_free(int64_t off, int64_t len) {
+    free_.push_back({off, len});
+    std::sort(free_.begin(), free_.end());
+    std::vector<std::pair<int64_t, int64_t>> merged;
+    for (auto& r : free_) {
+      if (!merged.empty() && merged.back().first + merged.back().second == r.first)
+        merged.back().second += r.second;
+      else
+        merged.push_back(r);
+    }
+    free_ = merged;
+  }
+
+  // Grows a device array to at least `need` elements (doubling), keeping
+  // the first `keep` elements; invalidates the graphs.
+  template <typename T>
+  mpmgpu_status grow(T** p, int64_t* cap, int64_t need, int64_t keep) {
+    if (need <= *cap) return MPMGPU_OK;
+    const int64_t ncap = std::max<int64_t>(need, std::max<int64_t>(2 * *cap, 1024));
+    void* q = nullptr;
+    cudaError_t e = cudaMalloc(&q, (size_t)ncap * sizeof(T));
+    if (e != cudaSuccess) return fail(MPMGPU_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    MPM_CUDA_TRY(cudaMemsetAsync(q, 0, (size_t)ncap * sizeof(T), stream_));
+    if (*p != nullptr) {
+      if (keep > 0) MPM_CUDA_TRY(cudaMemcpyAsync(q, *p, (size_t)keep * sizeof(T), cudaMemcpyDeviceToDevice, stream_));
+      MPM_CUDA_TRY(cudaStreamSynchronize(stream_));
+      auto it = std::find(cap_allocs_.begin(), cap_allocs_.end(), (void*)*p);
+      if (it != cap_allocs_.end()) cap_allocs_.erase(it);
+      cudaFree(*p);
+      scratch_bytes_ -= *cap * (int64_t)sizeof(T);
+    }
+    cap_allocs_.push_back(q);
+    scratch_bytes_ += ncap * (int64_t)sizeof(T);
+    *p = static_cast<T*>(q);
+    *cap = ncap;
+    drop_graphs();
+    return MPMGPU_OK;
+  }
+
+  // ---- membership: tables, binning, priming ----
+
+  // Applies joins and leaves at a step boundary: block ranges, tables,
+  // re-binning of every body and the first scatter of joining bodies.
+  mpmgpu_status commit() {
+    if (!membership_dirty_ && !tables_dirty_) return MPMGPU_OK;
+    const bool membership = membership_dirty_;
+    if (membership) {
+      for (auto& j : jobs_) {
+        const bool want = j.admitted && !j.finished && !j.removed && j.steps_left > 0;
+        if (j.admitted && !j.finished && j.steps_left <= 0) j.finished = true;
+        if (want && !j.in_tables) {
+          j.block_off = block_alloc(j.g.nblocks);
+          j.in_tables = true;
+        } else if (!want && j.in_tables) {
+          j.in_tables = false;
+          // its flags were set by its last scatter: clear them so no later
+          // compaction lists its blocks
+          MPM_CUDA_TRY(cudaMemsetAsync(flags_ + j.block_off, 0, sizeof(uint32_t) * j.g.nblocks, stream_));
+          block_free(j.block_off, j.g.nblocks);
+          j.block_off = j.removed ? -1 : j.block_off;
+        }
+      }
+    }
+    // table contents
+    std::vector<InstDev> insts;
+    std::vector<GridBody> gbodies;
+    std::vector<BodyCtx<PT>> ctx;
+    std::vector<int64_t> point_end, bin_end;
+    std::vector<int32_t> item_off;
+    int64_t points = 0, bins = 0, cells = 0, items = 0;
+    live_jobs_ = 0;
+    bool any_prime = false;
+    for (auto& j : jobs_) {
+      if (!j.in_tables) continue;
+      InstDev I{};
+      I.g = j.g;
+      I.sp = j.sp;
+      I.nb = (int)j.bodies.size();
+      I.body0 = (int)ctx.size();
+      I.nc = j.nc;
+      for (int c = 0; c < j.nc; c++) {
+        I.cb1[c] = j.cb1[c];
+        I.cb2[c] = j.cb2[c];
+        I.mu[c] = j.mu[c];
+        I.normal_out[c] = j.normal_out[c];
+        I.force_out[c] = j.force_out[c];
+      }
+      I.block_off = j.block_off;
+      insts.push_back(I);
+      for (auto& b : j.bodies) {
+        GridBody G{};
+        G.A = b.A;
+        G.V = b.V;
+        G.snap = b.snap;
+        G.has_boundary = b.has_boundary;
+        gbodies.push_back(G);
+        BodyCtx<PT> c{};
+        c.g = j.g;
+        c.mc = j.mc;
+        c.bg = j.bg;
+        c.sp = j.sp;
+        c.mat = b.mat;
+        c.P = b.P;
+        c.V = b.V;
+        c.A = b.A;
+        c.flags = flags_ + j.block_off;   // rebased after growth below
+        c.needs_normal = b.needs_normal;
+        c.prime = b.prime;
+        any_prime = any_prime || b.prime;
+        c.Palt = b.Palt;
+        c.point_off = points;
+        c.bin_off = bins;
+        c.cell_off = cells;
+        c.inst = (int)insts.size() - 1;
+        points += b.n;
+        bins += j.bg.nbins + 1;
+        cells += (int64_t)j.bg.nbins * j.bg.cells_per_bin + 1;
+        item_off.push_back((int32_t)items);
+        items += j.bg.nbins + b.n / 256 + 1;
+        point_end.push_back(points);
+        bin_end.push_back(bins);
+        ctx.push_back(c);
+      }
+      live_jobs_++;
+    }
+    // capacities
+    const int64_t nb = (int64_t)ctx.size(), ni = (int64_t)insts.size();
+    MPM_TRY(grow(&insts_d_, &cap_insts_, std::max<int64_t>(ni, 1), 0));
+    MPM_TRY(grow(&gbodies_d_, &cap_bodies_g_, std::max<int64_t>(nb, 1), 0));
+    MPM_TRY(grow(&ctx_d_, &cap_bodies_c_, std::max<int64_t>(nb, 1), 0));
+    MPM_TRY(grow(&point_end_d_, &cap_bodies_p_, std::max<int64_t>(nb, 1), 0));
+    MPM_TRY(grow(&bin_end_d_, &cap_bodies_b_, std::max<int64_t>(nb, 1), 0));
+    const int64_t old_blocks = cap_blocks_;
+    MPM_TRY(grow(&flags_, &cap_blocks_, std::max<int64_t>(block_end_, 1), old_blocks));
+    int64_t tmp_cap = old_blocks;
+    MPM_TRY(grow(&was_active_, &tmp_cap, cap_blocks_, old_blocks));
+    tmp_cap = old_blocks;
+    MPM_TRY(grow(&blk_inst_, &tmp_cap, cap_blocks_, 0));
+    tmp_cap = old_blocks;
+    MPM_TRY(grow(&list_, &tmp_cap, cap_blocks_, 0));
+    MPM_TRY(grow(&key_, &cap_points_k_, std::max<int64_t>(points, 1), 0));
+    MPM_TRY(grow(&rank_, &cap_points_r_, std::max<int64_t>(points, 1), 0));
+    MPM_TRY(grow(&cell_count_, &cap_cells_, std::max<int64_t>(cells, 1), 0));
+    MPM_TRY(grow(&bin_scan_, &cap_bins_, bins + 2, 0));
+    MPM_TRY(grow(&chunk_sum_, &cap_chunks_, cap_bins_ / kScanChunk + 2, 0));
+    MPM_TRY(grow(&item_off_d_, &cap_bodies_i_, std::max<int64_t>(nb, 1), 0));
+    MPM_TRY(grow(&nwork_body_, &cap_bodies_w_, std::max<int64_t>(nb, 1), 0));
+    MPM_TRY(grow(&work_end_body_, &cap_bodies_e_, std::max<int64_t>(nb, 1), 0));
+    MPM_TRY(grow(&work_bin_, &cap_items_n_, std::max<int64_t>(items, 1), 0));
+    MPM_TRY(grow(&work_start_, &cap_items_s_, std::max<int64_t>(items, 1), 0));
+    MPM_TRY(grow(&work_end_, &cap_items_e_, std::max<int64_t>(items, 1), 0));
+    for (size_t b = 0; b < ctx.size(); b++) ctx[b].flags = flags_ + insts[(size_t)ctx[b].inst].block_off;
+    ctx_host_ = ctx;
+    single_mode_ = ctx.size() <= 4;
+    any_plain_ = any_normal_ = false;
+    for (const auto& c : ctx) (c.needs_normal ? any_normal_ : any_plain_) = true;
+    drop_graphs();   // one-body launches carry the table entries in their arguments
+    // block -> job slot map: rebuilt for the whole space (holes -1)
+    std::vector<int32_t> bi((size_t)cap_blocks_, -1);
+    for (size_t s = 0; s < insts.size(); s++)
+      for (int64_t k = 0; k < insts[s].g.nblocks; k++) bi[(size_t)(insts[s].block_off + k)] = (int32_t)s;
+    BatchHdr hdr{};
+    hdr.points = points;
+    hdr.bins = bins;
+    hdr.cells = cells;
+    hdr.blocks = block_end_;
+    hdr.nbodies = (int)nb;
+    hdr.ninst = (int)ni;
+    // the device tables change only between steps (stream order)
+    MPM_TRY(upload_async(insts_d_, insts));
+    MPM_TRY(upload_async(gbodies_d_, gbodies));
+    MPM_TRY(upload_async(ctx_d_, ctx));
+    MPM_TRY(upload_async(point_end_d_, point_end));
+    MPM_TRY(upload_async(bin_end_d_, bin_end));
+    MPM_TRY(upload_async(item_off_d_, item_off));
+    MPM_TRY(upload_async(blk_inst_, bi));
+    MPM_CUDA_TRY(cudaMemcpyAsync(hdr_, &hdr, sizeof(hdr), cudaMemcpyHostToDevice, stream_));
+    MPM_CUDA_TRY(cudaStreamSynchronize(stream_));  // host vectors go out of scope
+    hdr_host_ = hdr;
+    tables_dirty_ = false;
+    membership_dirty_ = false;
+    if (membership && live_jobs_ > 0) {
+      MPM_TRY(launch_sort());
+      if (any_prime) MPM_TRY(prime());
+    }
+    return MPMGPU_OK;
+  }
+
+  template <typename T>
+  mpmgpu_status upload_async(T* dst, const std::vector<T>& src) {
+    if (src.empty()) return MPMGPU_OK;
+    MPM_CUDA_TRY(cudaMemcpyAsync(dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice, stream_));
+    return MPMGPU_OK;
+  }
+
+  // First scatter of joining bodies (their nodal sums for the first step).
+  mpmgpu_status prime() {
+    MPM_TRY(launch_fused(1));
+    // clear the prime flags in the host mirrors and the device table
+    for (auto& j : jobs_) {
+      if (!j.in_tables) continue;
+      j.primed = true;
+      for (auto& b : j.bodies) b.prime = 0;
+    }
+    for (auto& c : ctx_host_) c.prime = 0;
+    MPM_TRY(launch_clear_prime());
+    return MPMGPU_OK;
+  }
+
+  // ---- launches ----
+
+  mpmgpu_status check_launch(const char* what) {
+    launches_++;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(MPMGPU_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+    return MPMGPU_OK;
+  }
+
+  struct StageTimer {
+    Batch* b;
+    int stage;
+    cudaEvent_t start = nullptr;
+    StageTimer(Batch* bb, int s) : b(bb), stage(s) {
+      if (!b->profiling_) return;
+      start = b->take_event();
+      cudaEventRecord(start, b->stream_);
+    }
+    ~StageTimer() {
+      if (!b->profiling_ || !start) return;
+      cudaEvent_t stop = b->take_event();
+      cudaEventRecord(stop, b->stream_);
+      b->pending_[stage].push_back({start, stop});
+    }
+  };
+  cudaEvent_t take_event() {
+    cudaEvent_t e = nullptr;
+    if (!event_pool_.empty()) {
+      e = event_pool_.back();
+      event_pool_.pop_back();
+    } else {
+      cudaEventCreate(&e);
+    }
+    return e;
+  }
+
+  int stride_blocks(int threads) const { return sm_count_ * (2048 / threads); }
+
+  template <int DIM, int CAP, bool NORMAL, bool SINGLE>
+  mpmgpu_status launch_fused_k(int prime_pass, int one_body) {
+    FusedLaunch<PT> fl{};
+    if (SINGLE) fl.one = ctx_host_[(size_t)one_body];
+    fl.one_body = SINGLE ? one_body : -1;
+    fl.bodies = ctx_d_;
+    fl.item_off = item_off_d_;
+    fl.nwork_body = nwork_body_;
+    fl.work_end_body = work_end_body_;
+    fl.nbodies_cap = (int)ctx_host_.size();
+    fl.work_bin = work_bin_;
+    fl.work_start = work_start_;
+    fl.work_end = work_end_;
+    fl.nwork = nwork_;
+    fl.err = err_;
+    fl.drift = drift_;
+    fl.prime_pass = prime_pass;
+    constexpr size_t smem = fused_smem_bytes<DIM, PT, CAP>();
+    auto kern = k_g2p2g<DIM, PT, CAP, NORMAL, SINGLE>;
+    // resident CTAs per SM, looked up once per kernel (before any capture)
+    int& per_sm = fused_per_sm_[(CAP == 256 ? 0 : (CAP == 512 ? 1 : 2)) * 4 + (NORMAL ? 2 : 0) + (SINGLE ? 1 : 0)];
+    if (per_sm == 0) {
+      MPM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      MPM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kFusedThreads, smem));
+      if (per_sm < 1) return fail(MPMGPU_ERR_CUDA, "fused kernel does not fit on an SM");
+    }
+    const int blocks = per_sm * sm_count_;
+    StageTimer timer(this, kStageFused);
+    kern<<<blocks, kFusedThreads, smem, stream_>>>(fl);
+    return check_launch("k_g2p2g");
+  }
+
+  // One launch per body for small batches at the default item size (the
+  // body's parameters then sit in the constant bank), else one launch per
+  // kind of body (with or without the contact normal) over the table.
+  template <int DIM, int CAP>
+  mpmgpu_status launch_fused_t(int prime_pass) {
+    if constexpr (CAP == 512) {
+      if (single_mode_) {
+        for (size_t b = 0; b < ctx_host_.size(); b++) {
+          if (prime_pass && !ctx_host_[b].prime) continue;
+          if (ctx_host_[b].needs_normal)
+            MPM_TRY((launch_fused_k<DIM, CAP, true, true>(prime_pass, (int)b)));
+          else
+            MPM_TRY((launch_fused_k<DIM, CAP, false, true>(prime_pass, (int)b)));
+        }
+        return MPMGPU_OK;
+      }
+    }
+    if (any_plain_) MPM_TRY((launch_fused_k<DIM, CAP, false, false>(prime_pass, -1)));
+    if (any_normal_) MPM_TRY((launch_fused_k<DIM, CAP, true, false>(prime_pass, -1)));
+    return MPMGPU_OK;
+  }
+
+  mpmgpu_status launch_fused(int prime_pass) {
+    if (dim_ == 3) {
+      if (cap_ == 256) return launch_fused_t<3, 256>(prime_pass);
+      if constexpr (sizeof(PT) == 4) {
+        if (cap_ == 1024) return launch_fused_t<3, 1024>(prime_pass);
+      }
+      return launch_fused_t<3, 512>(prime_pass);
+    }
+    return launch_fused_t<2, 512>(prime_pass);
+  }
+
+  mpmgpu_status launch_clear_prime() {
+    k_clear_prime<PT><<<1, 256, 0, stream_>>>(hdr_, ctx_d_);
+    return check_launch("k_clear_prime");
+  }
+
+  mpmgpu_status launch_step_direct() {
+    {
+      StageTimer timer(this, kStageCompact);
+      MPM_CUDA_TRY(cudaMemsetAsync(count_, 0, sizeof(unsigned long long), stream_));
+      k_compact<<<stride_blocks(256), 256, 0, stream_>>>(hdr_, flags_, list_, count_, was_active_, active_nodes_);
+      MPM_TRY(check_launch("k_compact"));
+    }
+    {
+      StageTimer timer(this, kStageGrid);
+      const int gb = sm_count_ * 32;
+      if (dim_ == 3)
+        k_grid<3><<<gb, 64, 0, stream_>>>(insts_d_, gbodies_d_, blk_inst_, list_, count_, active_nodes_);
+      else
+        k_grid<2><<<gb, 64, 0, stream_>>>(insts_d_, gbodies_d_, blk_inst_, list_, count_, active_nodes_);
+      MPM_TRY(check_launch("k_grid"));
+    }
+    return launch_fused(0);
+  }
+
+  template <int DIM>
+  mpmgpu_status launch_sort_direct_t() {
+    const int sb = stride_blocks(256);
+    k_sort_clear<<<sb, 256, 0, stream_>>>(hdr_, cell_count_, nwork_body_);
+    MPM_TRY(check_launch("k_sort_clear"));
+    k_sort_count<DIM, PT><<<sb, 256, 0, stream_>>>(hdr_, ctx_d_, point_end_d_, key_, rank_, cell_count_);
+    MPM_TRY(check_launch("k_sort_count"));
+    k_bin_totals<PT><<<sb, 256, 0, stream_>>>(hdr_, ctx_d_, bin_end_d_, cell_count_, bin_scan_);
+    MPM_TRY(check_launch("k_bin_totals"));
+    const int chunks = (int)((cap_bins_ + kScanChunk - 1) / kScanChunk);
+    k_scan_blocks<<<chunks, kScanChunk, 0, stream_>>>(hdr_, bin_scan_, chunk_sum_);
+    MPM_TRY(check_launch("k_scan_blocks"));
+    k_scan_small<<<1, 1024, 0, stream_>>>(chunk_sum_, chunks, nullptr);
+    MPM_TRY(check_launch("k_scan_small"));
+    k_scan_add<<<chunks, kScanChunk, 0, stream_>>>(hdr_, bin_scan_, chunk_sum_);
+    MPM_TRY(check_launch("k_scan_add"));
+    k_sort_scatter<DIM, PT><<<sb, 256, 0, stream_>>>(hdr_, ctx_d_, point_end_d_, key_, rank_, cell_count_, bin_scan_);
+    MPM_TRY(check_launch("k_sort_scatter"));
+    k_sort_flip<PT><<<std::max(1, (hdr_host_.nbodies + 255) / 256 + 1), 256, 0, stream_>>>(hdr_, ctx_d_);
+    MPM_TRY(check_launch("k_sort_flip"));
+    k_bin_work<PT><<<sb, 256, 0, stream_>>>(hdr_, ctx_d_, bin_end_d_, bin_scan_, item_off_d_, cap_, work_bin_,
+                                            work_start_, work_end_, nwork_body_);
+    MPM_TRY(check_launch("k_bin_work"));
+    k_work_prefix<<<1, 1024, 0, stream_>>>(hdr_, nwork_body_, work_end_body_, nwork_);
+    MPM_TRY(check_launch("k_work_prefix"));
+    return MPMGPU_OK;
+  }
+
+  mpmgpu_status launch_sort_direct() {
+    StageTimer timer(this, kStageRebin);
+    return dim_ == 3 ? launch_sort_direct_t<3>() : launch_sort_direct_t<2>();
+  }
+
+  // Host mirrors of the point buffers follow the device-side swap.
+  void flip_mirrors() {
+    for (auto& j : jobs_) {
+      if (!j.in_tables) continue;
+      for (auto& b : j.bodies) std::swap(b.P, b.Palt);
+    }
+    for (auto& c : ctx_host_) std::swap(c.P, c.Palt);
+    flip_ ^= 1;
+  }
+
+  // Captures `body` into graph `g` on first use; launches it.
+  template <typename F>
+  mpmgpu_status run_graph(cudaGraphExec_t& g, bool& warm, int kernels, F&& body) {
+    // the first run of a launch sequence is direct (it also sets kernel
+    // attributes, which cannot happen inside a capture); later runs replay
+    // the captured graph
+    if (!use_graph_ || profiling_ || !warm) {
+      warm = true;
+      return body();
+    }
+    if (g == nullptr) {
+      cudaGraph_t graph = nullptr;
+      MPM_CUDA_TRY(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+      const int64_t before = launches_;
+      mpmgpu_status st = body();
+      cudaError_t e = cudaStreamEndCapture(stream_, &graph);
+      launches_ = before;
+      if (st != MPMGPU_OK) {
+        if (graph) cudaGraphDestroy(graph);
+        return st;
+      }
+      if (e != cudaSuccess) return fail(MPMGPU_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+      e = cudaGraphInstantiate(&g, graph, 0);
+      cudaGraphDestroy(graph);
+      if (e != cudaSuccess) return fail(MPMGPU_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+    }
+    MPM_CUDA_TRY(cudaGraphLaunch(g, stream_));
+    launches_ += kernels;
+    return MPMGPU_OK;
+  }
+
+  void drop_graphs() {
+    for (int i = 0; i < 2; i++) {
+      if (g_step_[i]) cudaGraphExecDestroy(g_step_[i]);
+      g_step_[i] = nullptr;
+      step_warm_[i] = false;
+    }
+    if (g_sort_) cudaGraphExecDestroy(g_sort_);
+    g_sort_ = nullptr;
+    sort_warm_ = false;
+  }
+
+  // The step graph depends on which point buffer is current (one-body
+  // launches carry the pointers): one graph per buffer parity.
+  mpmgpu_status launch_step() {
+    const int kernels = 2 + (single_mode_ && cap_ == 512 ? (int)ctx_host_.size() : (any_plain_ ? 1 : 0) + (any_normal_ ? 1 : 0));
+    return run_graph(g_step_[flip_], step_warm_[flip_], kernels, [&] { return launch_step_direct(); });
+  }
+
+  mpmgpu_status launch_sort() {
+    MPM_TRY(run_graph(g_sort_, sort_warm_, 10, [&] { return launch_sort_direct(); }));
+    flip_mirrors();
+    steps_since_sort_ = 0;
+    return MPMGPU_OK;
+  }
+
+  // ---- autotune snapshots ----
+
+  std::vector<std::pair<void*, std::pair<void*, size_t>>> snap_;  // (saved copy, (live array, bytes))
+
+  mpmgpu_status snap_one(void* live, size_t bytes) {
+    if (!live || bytes == 0) return MPMGPU_OK;
+    void* q = nullptr;
+    cudaError_t e = cudaMalloc(&q, bytes);
+    if (e != cudaSuccess) return fail(MPMGPU_ERR_NOMEM, "autotune snapshot: out of device memory");
+    MPM_CUDA_TRY(cudaMemcpyAsync(q, live, bytes, cudaMemcpyDeviceToDevice, stream_));
+    snap_.push_back({q, {live, bytes}});
+    return MPMGPU_OK;
+  }
+
+  mpmgpu_status snapshot_save() {
+    snapshot_free();
+    for (auto& j : jobs_) {
+      if (!j.in_tables) continue;
+      const size_t ns = (size_t)j.g.nslots * sizeof(double);
+      for (auto& b : j.bodies) {
+        const size_t np = (size_t)(b.n + 8) * sizeof(PT), ni = (size_t)(b.n + 8) * sizeof(int32_t);
+        // point buffers by role: the restore writes into whichever buffer
+        // is current then (the trials re-bin and swap them)
+        for (int d = 0; d < 3; d++) {
+          MPM_TRY(snap_one(b.P.x[d], np));
+          MPM_TRY(snap_one(b.P.v[d], np));
+          MPM_TRY(snap_one(b.P.u[d], np));
+        }
+        for (int c = 0; c < 6; c++) MPM_TRY(snap_one(b.P.s[c], np));
+        MPM_TRY(snap_one(b.P.vol, np));
+        MPM_TRY(snap_one(b.P.m, np));
+        MPM_TRY(snap_one(b.P.ext, np));
+        MPM_TRY(snap_one(b.P.active, ni));
+        MPM_TRY(snap_one(b.P.pid, ni));
+        if (b.P.L) MPM_TRY(snap_one(b.P.L, (size_t)b.n * 9 * sizeof(double)));
+        MPM_TRY(snap_one(b.A.m, ns));
+        for (int d = 0; d < 3; d++) {
+          MPM_TRY(snap_one(b.A.mx[d], ns));
+          MPM_TRY(snap_one(b.A.f[d], ns));
+          MPM_TRY(snap_one(b.A.nrm[d], ns));
+          MPM_TRY(snap_one(b.V.vt[d], ns));
+          MPM_TRY(snap_one(b.V.dv[d], ns));
+        }
+      }
+    }
+    MPM_TRY(snap_one(flags_, (size_t)cap_blocks_ * sizeof(uint32_t)));
+    MPM_TRY(snap_one(was_active_, (size_t)cap_blocks_));
+    snap_pbuf_.clear();
+    for (auto& j : jobs_)
+      for (auto& b : j.bodies) snap_pbuf_.push_back(b.P.x[0]);
+    MPM_CUDA_TRY(cudaStreamSynchronize(stream_));
+    return MPMGPU_OK;
+  }
+
+  mpmgpu_status snapshot_restore() {
+    // after the trial the current buffer may be the other one: restore the
+    // saved point arrays into the buffer that was current at the save
+    size_t k = 0;
+    for (auto& j : jobs_)
+      for (auto& b : j.bodies) {
+        if (k < snap_pbuf_.size() && b.P.x[0] != snap_pbuf_[k]) std::swap(b.P, b.Palt);
+        k++;
+      }
+    for (auto& s : snap_)
+      MPM_CUDA_TRY(cudaMemcpyAsync(s.second.first, s.first, s.second.second, cudaMemcpyDeviceToDevice, stream_));
+    // the table's point pointers must match the mirrors again
+    tables_dirty_ = true;
+    const bool m = membership_dirty_;
+    MPM_TRY(commit());
+    membership_dirty_ = m;
+    MPM_CUDA_TRY(cudaStreamSynchronize(stream_));
+    return MPMGPU_OK;
+  }
+
+  void snapshot_free() {
+    for (auto& s : snap_) cudaFree(s.first);
+    snap_.clear();
+  }
+  std::vector<void*> snap_pbuf_;
+
+  // ---- state ----
+  int dim_;
+  int device_;
+  bool keep_debug_;
+  bool use_graph_;
+  int sort_interval_ = 32;
+  int cap_ = 512;
+  int sm_count_ = 148;
+  int fused_per_sm_[12] = {};
+  std::vector<BodyCtx<PT>> ctx_host_;   // host copy of the body table
+  bool single_mode_ = false;
+  bool any_plain_ = false, any_normal_ = false;
+  int flip_ = 0;                        // point buffers swapped an odd number of times
+  cudaStream_t stream_ = nullptr;
+  std::vector<HJob> jobs_;
+  int live_jobs_ = 0;
+  bool membership_dirty_ = false;
+  bool tables_dirty_ = false;
+  int steps_since_sort_ = 0;
+  int64_t launches_ = 0;
+  int64_t scratch_bytes_ = 0;
+  std::vector<void*> scratch_allocs_;
+  std::vector<void*> cap_allocs_;
+  // block space
+  std::vector<std::pair<int64_t, int64_t>> free_;
+  int64_t block_end_ = 0;
+  // device tables and scratch
+  BatchHdr* hdr_ = nullptr;
+  BatchHdr hdr_host_{};
+  unsigned long long* count_ = nullptr;
+  int* err_ = nullptr;
+  unsigned long long* drift_ = nullptr;
+  int32_t* nwork_ = nullptr;
+  unsigned long long* active_nodes_ = nullptr;
+  InstDev* insts_d_ = nullptr;
+  int64_t cap_insts_ = 0;
+  GridBody* gbodies_d_ = nullptr;
+  int64_t cap_bodies_g_ = 0;
+  BodyCtx<PT>* ctx_d_ = nullptr;
+  int64_t cap_bodies_c_ = 0;
+  int64_t* point_end_d_ = nullptr;
+  int64_t cap_bodies_p_ = 0;
+  int64_t* bin_end_d_ = nullptr;
+  int64_t cap_bodies_b_ = 0;
+  uint32_t* flags_ = nullptr;
+  int64_t cap_blocks_ = 0;
+  uint8_t* was_active_ = nullptr;
+  int32_t* blk_inst_ = nullptr;
+  int64_t* list_ = nullptr;
+  int32_t* key_ = nullptr;
+  int64_t cap_points_k_ = 0;
+  int32_t* rank_ = nullptr;
+  int64_t cap_points_r_ = 0;
+  int32_t* cell_count_ = nullptr;
+  int64_t cap_cells_ = 0;
+  int32_t* bin_scan_ = nullptr;
+  int64_t cap_bins_ = 0;
+  int32_t* chunk_sum_ = nullptr;
+  int64_t cap_chunks_ = 0;
+  int32_t* item_off_d_ = nullptr;
+  int64_t cap_bodies_i_ = 0;
+  int32_t* nwork_body_ = nullptr;
+  int64_t cap_bodies_w_ = 0;
+  int32_t* work_end_body_ = nullptr;
+  int64_t cap_bodies_e_ = 0;
+  int32_t* work_bin_ = nullptr;
+  int64_t cap_items_n_ = 0;
+  int32_t* work_start_ = nullptr;
+  int64_t cap_items_s_ = 0;
+  int32_t* work_end_ = nullptr;
+  int64_t cap_items_e_ = 0;
+  cudaGraphExec_t g_step_[2] = {nullptr, nullptr};
+  cudaGraphExec_t g_sort_ = nullptr;
+  bool step_warm_[2] = {false, false};
+  bool sort_warm_ = false;
+  // profiling
+  bool profiling_ = false;
+  std::vector<cudaEvent_t> event_pool_;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending_[kStages];
+  int64_t stage_launches_[kStages] = {0, 0, 0, 0};
+  double stage_ms_[kStages] = {0.0, 0.0, 0.0, 0.0};
+};
+
+}  // namespace mpmb200

@@ -58,12 +58,14 @@ __host__ __device__ __forceinline__ void slot_ijk(const Geom& g, int64_t blk, in
 }
 
 // One axis of a point's shape-function window: nodes base..base+span-1 with
-// summed hat values W and signed sums G.
-struct AxisMap {
+// summed hat values W and signed sums G (R: double for the FP64 form, float
+// for the mixed form).
+template <typename R>
+struct AxisMapT {
   int base;
   int span;
-  double W[3];
-  double G[3];
+  R W[3];
+  R G[3];
 };
 
 // The S / gradS rows of one point in separable form. For the corner-sampled
@@ -78,11 +80,14 @@ struct AxisMap {
 // with W and G the per-axis sums of hat values (G signed by the corner side).
 // Point-sampled (CPDI_OFF) rows have the same form with W = hat values at x,
 // G = -sign(r)/h (cartesian.cpp:307-357), sS = sG = 1.
-struct PointMap {
-  AxisMap ax[3];
-  double sS;
-  double sG;
+template <typename R>
+struct PointMapT {
+  AxisMapT<R> ax[3];
+  R sS;
+  R sG;
 };
+using AxisMap = AxisMapT<double>;
+using PointMap = PointMapT<double>;
 
 // inDomain, cartesian.cpp:245-253 (closed interval).
 template <int DIM>
@@ -103,6 +108,10 @@ __device__ __forceinline__ int axis_element(const Geom& g, int d, double c) {
 struct MapConst {
   double NL[3];    // N / L: element index scale
   double invh[3];  // 1 / h
+  float Lf[3];     // single-precision copies for the mixed form
+  float hf[3];
+  float NLf[3];
+  float invhf[3];
 };
 
 // Element index floor(x / L * N) without a division: the product x * (N/L)
@@ -212,6 +221,109 @@ __device__ __forceinline__ int build_map_fast(const Geom& g, const MapConst& mc,
   pm.sS = 1.0;
   pm.sG = 1.0;
   return 1;
+}
+
+// Single-precision map of the mixed form: the same decisions as
+// build_map_fast in float arithmetic. The element index comes from
+// floor(x * N/L) clamped into the grid (no exact fallback: the mixed form
+// is compared with the FP64 form by tolerance, not bit for bit).
+__device__ __forceinline__ int axis_element_f32(const Geom& g, const MapConst& mc, int d, float c) {
+  int e = (int)floorf(c * mc.NLf[d]);
+  e = e < 0 ? 0 : e;
+  return e >= g.N[d] ? g.N[d] - 1 : e;
+}
+
+template <int DIM>
+__device__ __forceinline__ int build_map_f32(const Geom& g, const MapConst& mc, int cpdi_spec, const float* x,
+                                             float extent, PointMapT<float>& pm, int* err) {
+#pragma unroll
+  for (int d = 0; d < DIM; d++)
+    if (!(x[d] <= mc.Lf[d] && x[d] >= 0.0f)) return -1;
+  int cpdi = cpdi_spec;
+  const float a = 0.5f * extent;
+  float clo[3], chi[3];
+#pragma unroll
+  for (int d = 0; d < DIM; d++) {
+    clo[d] = x[d] - a;
+    chi[d] = x[d] + a;
+  }
+  if (cpdi == 1) {
+#pragma unroll
+    for (int d = 0; d < DIM; d++)
+      if (!(clo[d] <= mc.Lf[d] && clo[d] >= 0.0f) || !(chi[d] <= mc.Lf[d] && chi[d] >= 0.0f)) cpdi = 0;
+  }
+  if (cpdi == 1) {
+#pragma unroll
+    for (int d = 0; d < DIM; d++) {
+      AxisMapT<float>& A = pm.ax[d];
+      const int elo = axis_element_f32(g, mc, d, clo[d]);
+      const bool hi_ok = chi[d] < mc.Lf[d];
+      const int ehi = hi_ok ? axis_element_f32(g, mc, d, chi[d]) : elo;
+      const int delta = ehi - elo;
+      if (delta > 1 || delta < 0) atomicOr(err, kErrWideSpan);
+      A.base = elo;
+      A.span = 2 + (hi_ok && delta == 1 ? 1 : 0);
+      const float rl = (clo[d] - mc.hf[d] * (float)elo) * mc.invhf[d];
+      const float wl0 = 1.0f - fabsf(rl), wl1 = 1.0f - fabsf(rl - 1.0f);
+      float wh0 = 0.0f, wh1 = 0.0f;
+      if (hi_ok) {
+        const float rh = (chi[d] - mc.hf[d] * (float)ehi) * mc.invhf[d];
+        wh0 = 1.0f - fabsf(rh);
+        wh1 = 1.0f - fabsf(rh - 1.0f);
+      }
+      if (delta == 1) {
+        A.W[0] = wl0;
+        A.W[1] = wl1 + wh0;
+        A.W[2] = wh1;
+        A.G[0] = -wl0;
+        A.G[1] = wh0 - wl1;
+        A.G[2] = wh1;
+      } else {
+        A.W[0] = wl0 + wh0;
+        A.W[1] = wl1 + wh1;
+        A.W[2] = 0.0f;
+        A.G[0] = wh0 - wl0;
+        A.G[1] = wh1 - wl1;
+        A.G[2] = 0.0f;
+      }
+    }
+    pm.sS = 1.0f / (float)g.cp;
+    pm.sG = 1.0f / (((float)g.cp * 0.5f) * extent);
+    return 1;
+  }
+#pragma unroll
+  for (int d = 0; d < DIM; d++)
+    if (!(x[d] < mc.Lf[d] && x[d] >= 0.0f)) return 0;
+#pragma unroll
+  for (int d = 0; d < DIM; d++) {
+    AxisMapT<float>& A = pm.ax[d];
+    const int e = axis_element_f32(g, mc, d, x[d]);
+    A.base = e;
+    A.span = 2;
+#pragma unroll
+    for (int o = 0; o < 2; o++) {
+      const float r = (x[d] - mc.hf[d] * (float)(e + o)) * mc.invhf[d];
+      A.W[o] = 1.0f - fabsf(r);
+      A.G[o] = (fabsf(r) >= 1.0f) ? 0.0f : -(r / fabsf(r)) * mc.invhf[d];
+    }
+    A.W[2] = 0.0f;
+    A.G[2] = 0.0f;
+  }
+  pm.sS = 1.0f;
+  pm.sG = 1.0f;
+  return 1;
+}
+
+// One map builder per point precision.
+template <int DIM>
+__device__ __forceinline__ int build_map(const Geom& g, const MapConst& mc, int cpdi, const double* x, double ext,
+                                         PointMapT<double>& pm, int* err) {
+  return build_map_fast<DIM>(g, mc, cpdi, x, ext, pm, err);
+}
+template <int DIM>
+__device__ __forceinline__ int build_map(const Geom& g, const MapConst& mc, int cpdi, const float* x, float ext,
+                                         PointMapT<float>& pm, int* err) {
+  return build_map_f32<DIM>(g, mc, cpdi, x, ext, pm, err);
 }
 
 }  // namespace mpmb200

@@ -1,6 +1,7 @@
-// FP64 kernels of the explicit step around the fused gather/scatter kernel:
-// active-block compaction, grid update (contact, boundary, moveGrid), the
-// Jaumann stress update and the exact triplet export.
+// Kernels of the explicit step around the fused gather/scatter kernel (all
+// nodal work is FP64 in every form): active-block compaction, grid update
+// (contact, boundary, moveGrid), the Jaumann stress update and the exact
+// triplet export.
 #pragma once
 
 #include "exact_map.cuh"
@@ -19,8 +20,8 @@ __device__ __forceinline__ double sym_at(const double* s6, int a, int b) {
 }
 
 // Marks the node blocks covered by a point's window.
-template <int DIM>
-__device__ __forceinline__ void mark_blocks(const Geom& g, const PointMap& pm, uint32_t* flags) {
+template <int DIM, typename R>
+__device__ __forceinline__ void mark_blocks(const Geom& g, const PointMapT<R>& pm, uint32_t* flags) {
   const int i0 = pm.ax[0].base >> g.bsh[0], i1 = (pm.ax[0].base + pm.ax[0].span - 1) >> g.bsh[0];
   const int j0 = pm.ax[1].base >> g.bsh[1], j1 = (pm.ax[1].base + pm.ax[1].span - 1) >> g.bsh[1];
   int k0 = 0, k1 = 0;
@@ -33,10 +34,13 @@ __device__ __forceinline__ void mark_blocks(const Geom& g, const PointMap& pm, u
       for (int i = i0; i <= i1; i++) flags[i + (int64_t)g.nb[0] * (j + (int64_t)g.nb[1] * k)] = 1u;
 }
 
-// Compacts the flagged node blocks into `list`, clears the flags and keeps
-// the per-block activity of this step in `was_active`.
-__global__ void k_compact(int64_t nblocks, uint32_t* flags, int64_t* list, unsigned long long* count,
-                          uint8_t* was_active) {
+// Compacts the flagged node blocks of the batch's block space into `list`,
+// clears the flags and keeps the per-block activity of this step in
+// `was_active`.
+__global__ void k_compact(const BatchHdr* hdr, uint32_t* flags, int64_t* list, unsigned long long* count,
+                          uint8_t* was_active, unsigned long long* active_nodes) {
+  const int64_t nblocks = hdr->blocks;
+  if (blockIdx.x == 0 && threadIdx.x == 0) *active_nodes = 0;   // counted by this step's grid update
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   const int lane = threadIdx.x & 31;
   for (int64_t base = blockIdx.x * (int64_t)blockDim.x; base < nblocks; base += stride) {
@@ -55,34 +59,50 @@ __global__ void k_compact(int64_t nblocks, uint32_t* flags, int64_t* list, unsig
   }
 }
 
-// Grid update over the active node blocks: ContactHuang::generateRules
-// normalisation and applyRules (contact_huang.cpp:80-197), CartesianBox
-// (cartesian_box.cpp:73-85) and moveGrid (explicit_usl.cpp:233-264).
-// One thread per node; each node is owned by exactly one thread.
+// Grid update over the active node blocks of every job in the batch:
+// ContactHuang::generateRules normalisation and applyRules
+// (contact_huang.cpp:80-197), CartesianBox (cartesian_box.cpp:73-85) and
+// moveGrid (explicit_usl.cpp:233-264). One CTA of 64 threads per block, one
+// thread per node; each node is owned by exactly one thread.
 template <int DIM>
-__global__ void __launch_bounds__(64) k_grid(Geom g, StepParams sp, GridBodies GB, ContactSet CS, const int64_t* list,
-                                             const unsigned long long* count) {
+__global__ void __launch_bounds__(64) k_grid(const InstDev* insts, const GridBody* bodies, const int32_t* blk_inst,
+                                             const int64_t* list, const unsigned long long* count,
+                                             unsigned long long* active_nodes) {
   const int64_t cnt = (int64_t)*count;
-  const double dt = sp.dt;
   for (int64_t e = blockIdx.x; e < cnt; e += gridDim.x) {
-    const int64_t blk = list[e];
+    const int64_t gblk = list[e];
+    const InstDev& I = insts[blk_inst[gblk]];
+    const Geom& g = I.g;
+    const StepParams& sp = I.sp;
+    const double dt = sp.dt;
+    const GridBody* GB = bodies + I.body0;
+    const int64_t blk = gblk - I.block_off;
     const int li = threadIdx.x;
     int i, j, k;
     slot_ijk(g, blk, li, i, j, k);
-    if (i >= g.nn[0] || j >= g.nn[1] || k >= g.nn[2]) continue;
+    const bool inside = i < g.nn[0] && j < g.nn[1] && k < g.nn[2];
     const int64_t s = blk * 64 + li;
+    {
+      // nodes with mass, per body (the grid term of the step's traffic)
+      int cnt = 0;
+      if (inside)
+        for (int b = 0; b < I.nb; b++) cnt += GB[b].A.m[s] > 0.0 ? 1 : 0;
+      cnt = __reduce_add_sync(0xffffffffu, cnt);
+      if ((threadIdx.x & 31) == 0 && cnt > 0) atomicAdd(active_nodes, (unsigned long long)cnt);
+    }
+    if (!inside) continue;
     // the scatter leaves out the body force; S * (m b) summed over points is
     // the nodal mass times g (explicit_usl.cpp:150-154, b uniform)
-    for (int b = 0; b < GB.nb; b++) {
-      const NodesAcc& A = GB.acc[b];
+    for (int b = 0; b < I.nb; b++) {
+      const NodesAcc& A = GB[b].A;
       const double m = A.m[s];
 #pragma unroll
       for (int d = 0; d < DIM; d++)
         if (sp.grav[d] != 0.0) A.f[d][s] = A.f[d][s] + m * sp.grav[d];
     }
-    for (int c = 0; c < CS.nc; c++) {
-      const NodesAcc& A1 = GB.acc[CS.b1[c]];
-      const NodesAcc& A2 = GB.acc[CS.b2[c]];
+    for (int c = 0; c < I.nc; c++) {
+      const NodesAcc& A1 = GB[I.cb1[c]].A;
+      const NodesAcc& A2 = GB[I.cb2[c]].A;
       double n[3] = {0.0, 0.0, 0.0};
       double nn = 0.0;
 #pragma unroll
@@ -140,7 +160,7 @@ __global__ void __launch_bounds__(64) k_grid(Geom g, StepParams sp, GridBodies G
             for (int d = 0; d < DIM; d++) s1[d] *= inv;
           }
           const double a = (fn < 0.0) ? fn : 0.0;  // std::min(0.0, fn)
-          const double mufn = CS.mu[c] * fabs(fn);
+          const double mufn = I.mu[c] * fabs(fn);
           const double b = (fabs(ft) < mufn) ? fabs(ft) : mufn;  // std::min(mu|fn|, |ft|)
 #pragma unroll
           for (int d = 0; d < DIM; d++) {
@@ -150,18 +170,18 @@ __global__ void __launch_bounds__(64) k_grid(Geom g, StepParams sp, GridBodies G
           }
         }
       }
-      if (CS.normal_out[c] != nullptr) {
+      if (I.normal_out[c] != nullptr) {
 #pragma unroll
         for (int d = 0; d < 3; d++) {
-          CS.normal_out[c][3 * s + d] = (d < DIM) ? n[d] : 0.0;
-          CS.force_out[c][3 * s + d] = fc[d];
+          I.normal_out[c][3 * s + d] = (d < DIM) ? n[d] : 0.0;
+          I.force_out[c][3 * s + d] = fc[d];
         }
       }
     }
     const bool on_face = (i == 0 || i == g.N[0] || j == 0 || j == g.N[1] || (DIM == 3 && (k == 0 || k == g.N[2])));
-    for (int b = 0; b < GB.nb; b++) {
-      const NodesAcc& A = GB.acc[b];
-      const NodesVel& V = GB.vel[b];
+    for (int b = 0; b < I.nb; b++) {
+      const NodesAcc& A = GB[b].A;
+      const NodesVel& V = GB[b].V;
       const double m = A.m[s];
       double mx[3], f[3];
 #pragma unroll
@@ -169,7 +189,7 @@ __global__ void __launch_bounds__(64) k_grid(Geom g, StepParams sp, GridBodies G
         mx[d] = A.mx[d][s];
         f[d] = A.f[d][s];
       }
-      if (GB.has_boundary[b] && on_face) {
+      if (GB[b].has_boundary && on_face) {
 #pragma unroll
         for (int d = 0; d < DIM; d++) {
           mx[d] = 0.0;
@@ -184,7 +204,7 @@ __global__ void __launch_bounds__(64) k_grid(Geom g, StepParams sp, GridBodies G
         V.vt[d][s] = (m > 0) ? mx[d] * inv : 0.0;
         V.dv[d][s] = (m > 0) ? (dt * f[d]) * inv : 0.0;
       }
-      const NodesAcc& Sn = GB.snap[b];
+      const NodesAcc& Sn = GB[b].snap;
       if (Sn.m != nullptr) {
         Sn.m[s] = m;
 #pragma unroll
@@ -208,31 +228,31 @@ __global__ void __launch_bounds__(64) k_grid(Geom g, StepParams sp, GridBodies G
 // Jaumann update of IsotropicLinearElasticity (isolin.cpp:62-74) on the 6
 // stored components. For symmetric T and W = -W^T, (T W)_ab = -(W T)_ba, so
 // W T - T W = (W T)_ab + (W T)_ba.
-template <int DIM>
-__device__ __forceinline__ void jaumann_update(const double L[3][3], double* s6, double G, double lambda, double dt) {
-  double D[3][3], W[3][3];
+template <int DIM, typename R>
+__device__ __forceinline__ void jaumann_update(const R L[3][3], R* s6, R G, R lambda, R dt) {
+  R D[3][3], W[3][3];
 #pragma unroll
   for (int a = 0; a < 3; a++)
 #pragma unroll
     for (int b = 0; b < 3; b++) {
-      D[a][b] = 0.5 * (L[a][b] + L[b][a]);
-      W[a][b] = 0.5 * (L[a][b] - L[b][a]);
+      D[a][b] = R(0.5) * (L[a][b] + L[b][a]);
+      W[a][b] = R(0.5) * (L[a][b] - L[b][a]);
     }
-  const double trD = D[0][0] + D[1][1] + D[2][2];
-  const double T[3][3] = {{s6[0], s6[3], s6[5]}, {s6[3], s6[1], s6[4]}, {s6[5], s6[4], s6[2]}};
-  double WT[3][3];
+  const R trD = D[0][0] + D[1][1] + D[2][2];
+  const R T[3][3] = {{s6[0], s6[3], s6[5]}, {s6[3], s6[1], s6[4]}, {s6[5], s6[4], s6[2]}};
+  R WT[3][3];
 #pragma unroll
   for (int a = 0; a < 3; a++)
 #pragma unroll
     for (int b = 0; b < 3; b++) WT[a][b] = W[a][0] * T[0][b] + W[a][1] * T[1][b] + W[a][2] * T[2][b];
-  const double twoG = 2.0 * G;
-  const double ltr = lambda * trD;
+  const R twoG = R(2.0) * G;
+  const R ltr = lambda * trD;
   const int ia[6] = {0, 1, 2, 0, 1, 0};
   const int ib[6] = {0, 1, 2, 1, 2, 2};
 #pragma unroll
   for (int c = 0; c < 6; c++) {
     const int a = ia[c], b = ib[c];
-    const double rate = ((twoG * D[a][b] + (a == b ? ltr : 0.0)) + WT[a][b]) + WT[b][a];
+    const R rate = ((twoG * D[a][b] + (a == b ? ltr : R(0.0))) + WT[a][b]) + WT[b][a];
     s6[c] = s6[c] + dt * rate;
   }
 }

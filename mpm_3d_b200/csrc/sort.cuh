@@ -1,18 +1,23 @@
-// Binning of points for the fused gather/scatter kernel.
+// Binning of points for the fused gather/scatter kernel, for every body of a
+// batch in one set of launches.
 //
 // Points are kept grouped by bin: a block of B^dim cells (4x4x4 in 3D, 8x8
 // in 2D). Within a bin they are laid out rank-major: first the first point
 // of every cell (in cell order), then the second point of every cell, and so
 // on. A warp of consecutive points therefore covers distinct cells, so the
-// points of one warp never add into the same node at the same time in the
+// points of one warp rarely add into the same node at the same time in the
 // shared-memory tile (same-address atomics serialise).
 //
-// The sort is a counting sort in three passes (count + rank, bin offsets,
-// scatter); it is only run when points have drifted out of their bin's tile,
-// because the fused kernel stays correct (slower) for drifted points.
+// The sort is a counting sort over the batch's concatenated point space
+// (count + rank, per-bin totals, one exclusive scan over all bodies' bins,
+// scatter), then the work list of (body, bin, point range) items. It runs
+// when jobs join or leave the batch and every sort_interval steps, because
+// the fused kernel stays correct (slower) for points that drifted out of
+// their bin's tile.
 #pragma once
 
 #include "geom.cuh"
+#include "state.cuh"
 
 namespace mpmb200 {
 
@@ -26,12 +31,48 @@ struct BinGeom {
   int tile_nodes;    // T^dim
 };
 
+// Per-body table entry. The first part (up to Palt) is what the fused
+// kernel stages in shared memory for a work item.
+template <typename PT>
+struct BodyCtx {
+  Geom g;
+  MapConst mc;
+  BinGeom bg;
+  StepParams sp;
+  MaterialParams mat;
+  PointsT<PT> P;        // current storage order
+  NodesVel V;
+  NodesAcc A;
+  uint32_t* flags;      // node-block flags of the body's job (its first block)
+  int needs_normal;     // accumulate the contact normal (first body of a contact)
+  int prime;            // 1 until the body's first scatter has run
+  // sort side
+  PointsT<PT> Palt;     // second buffer; swapped with P after a sort
+  int64_t point_off;    // first point in the batch's point space
+  int64_t bin_off;      // first entry in the batch's bin arrays (nbins + 1 per body)
+  int64_t cell_off;     // first cell counter (nbins * cells_per_bin + 1 per body)
+  int inst;
+};
+
+// Index of the entry whose [end[b-1], end[b]) range holds i (end: inclusive
+// prefix sums, n entries).
+template <typename I>
+__device__ __forceinline__ int find_range(const I* end, int n, int64_t i) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (end[mid] > i) hi = mid;
+    else lo = mid + 1;
+  }
+  return lo;
+}
+
 // Cell of a point for binning, clamped into the grid.
-template <int DIM>
-__device__ __forceinline__ void point_cell(const Geom& g, const double* x, int* c) {
+template <int DIM, typename PT>
+__device__ __forceinline__ void point_cell(const Geom& g, const PT* x, int* c) {
 #pragma unroll
   for (int d = 0; d < DIM; d++) {
-    int v = (int)floor(x[d] * (g.N[d] / g.L[d]));
+    int v = (int)floor((double)x[d] * (g.N[d] / g.L[d]));
     v = v < 0 ? 0 : (v >= g.N[d] ? g.N[d] - 1 : v);
     c[d] = v;
   }
@@ -45,46 +86,67 @@ __device__ __forceinline__ void bin_of(const BinGeom& bg, const int* c, int* bin
   *local = lx + bg.B * (ly + bg.B * lz);
 }
 
-// Pass 1: key (bin * cells_per_bin + local cell) and rank within the cell.
-// Inactive points go to the trailing key nbins * cells_per_bin.
-template <int DIM>
-__global__ void k_sort_count(Geom g, BinGeom bg, PointsDev P, int32_t* key, int32_t* rank, int32_t* cell_count) {
+// Pass 0: clears the cell counters and the per-body work-item counts.
+__global__ void k_sort_clear(const BatchHdr* hdr, int32_t* cell_count, int32_t* nwork_body) {
+  const int64_t n = hdr->cells;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < P.n; p += stride) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += stride) cell_count[i] = 0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < hdr->nbodies; i += stride) nwork_body[i] = 0;
+}
+
+// Pass 1: key (bin * cells_per_bin + local cell, local to the body) and rank
+// within the cell. Inactive points go to the trailing key nbins * cells_per_bin.
+template <int DIM, typename PT>
+__global__ void k_sort_count(const BatchHdr* hdr, const BodyCtx<PT>* bodies, const int64_t* point_end, int32_t* key,
+                             int32_t* rank, int32_t* cell_count) {
+  const int64_t total = hdr->points;
+  const int nb = hdr->nbodies;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < total; q += stride) {
+    const BodyCtx<PT>& B = bodies[find_range(point_end, nb, q)];
+    const int64_t p = q - B.point_off;
     int k;
-    if (P.active[p] == 0) {
-      k = bg.nbins * bg.cells_per_bin;
+    if (B.P.active[p] == 0) {
+      k = B.bg.nbins * B.bg.cells_per_bin;
     } else {
-      double xp[3] = {0.0, 0.0, 0.0};
+      PT xp[3] = {PT(0), PT(0), PT(0)};
 #pragma unroll
-      for (int d = 0; d < DIM; d++) xp[d] = P.x[d][p];
+      for (int d = 0; d < DIM; d++) xp[d] = B.P.x[d][p];
       int c[3] = {0, 0, 0};
-      point_cell<DIM>(g, xp, c);
+      point_cell<DIM>(B.g, xp, c);
       int b, l;
-      bin_of<DIM>(bg, c, &b, &l);
-      k = b * bg.cells_per_bin + l;
+      bin_of<DIM>(B.bg, c, &b, &l);
+      k = b * B.bg.cells_per_bin + l;
     }
-    key[p] = k;
-    rank[p] = atomicAdd(cell_count + k, 1);
+    key[q] = k;
+    rank[q] = atomicAdd(cell_count + B.cell_off + k, 1);
   }
 }
 
-// Pass 2a: per-bin point counts (one thread per bin, sums its cells). The
-// trailing inactive bin is bin index nbins.
-__global__ void k_bin_totals(BinGeom bg, const int32_t* cell_count, int32_t* bin_total) {
-  const int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b > bg.nbins) return;
-  int s = 0;
-  if (b < bg.nbins) {
-    for (int l = 0; l < bg.cells_per_bin; l++) s += cell_count[b * bg.cells_per_bin + l];
-  } else {
-    s = cell_count[bg.nbins * bg.cells_per_bin];
+// Pass 2: per-bin point counts (one thread per bin entry, summing its
+// cells); entry nbins of a body counts its inactive points.
+template <typename PT>
+__global__ void k_bin_totals(const BatchHdr* hdr, const BodyCtx<PT>* bodies, const int64_t* bin_end,
+                             const int32_t* cell_count, int32_t* bin_total) {
+  const int64_t total = hdr->bins;
+  const int nb = hdr->nbodies;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += stride) {
+    const BodyCtx<PT>& B = bodies[find_range(bin_end, nb, i)];
+    const int lb = (int)(i - B.bin_off);
+    const int32_t* cc = cell_count + B.cell_off;
+    int s = 0;
+    if (lb < B.bg.nbins) {
+      for (int l = 0; l < B.bg.cells_per_bin; l++) s += cc[lb * B.bg.cells_per_bin + l];
+    } else {
+      s = cc[B.bg.nbins * B.bg.cells_per_bin];
+    }
+    bin_total[i] = s;
   }
-  bin_total[b] = s;
 }
 
-// Exclusive scan of n int32 values in place, one CTA of 1024 threads,
-// in chunks (the bin count is at most a few hundred thousand).
+// Exclusive scan of n int32 values in place, one CTA of 1024 threads, in
+// chunks (for short arrays: the block sums of k_scan_blocks).
 __global__ void k_scan_small(int32_t* v, int n, int32_t* total) {
   __shared__ int32_t warp_sums[32];
   __shared__ int32_t carry;
@@ -121,29 +183,75 @@ __global__ void k_scan_small(int32_t* v, int n, int32_t* total) {
   if (threadIdx.x == 0 && total) *total = carry;
 }
 
-// Pass 3: destination of each point inside its bin (rank-major order) and
-// the permutation copy of every per-point array.
-struct PointArrays {
-  double* f[24];   // double arrays (x, v, u, s, vol, m, ext, ...)
-  int nf;
-  int32_t* i[4];   // int arrays (active, pid)
-  int ni;
-  double* L9;      // 9 doubles per point (debug velocity gradient) or null
-};
+// Multi-CTA exclusive scan of hdr->bins values: each CTA of 1024 threads
+// scans its chunk in place and writes the chunk total; k_scan_small scans
+// the totals; k_scan_add adds them back.
+constexpr int kScanChunk = 1024;
 
-__global__ void k_sort_scatter(BinGeom bg, int64_t n, const int32_t* key, const int32_t* rank, const int32_t* cell_count,
-                               const int32_t* bin_start, PointArrays src, PointArrays dst) {
+__device__ __forceinline__ int block_exclusive_scan_1024(int x, int* total) {
+  __shared__ int32_t warp_sums[32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  int incl = x;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  if (lane == 31) warp_sums[wid] = incl;
+  __syncthreads();
+  if (wid == 0) {
+    int ws = warp_sums[lane];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, ws, o);
+      if (lane >= o) ws += y;
+    }
+    warp_sums[lane] = ws;
+  }
+  __syncthreads();
+  *total = warp_sums[31];
+  return (wid > 0 ? warp_sums[wid - 1] : 0) + incl - x;
+}
+
+__global__ void __launch_bounds__(kScanChunk) k_scan_blocks(const BatchHdr* hdr, int32_t* v, int32_t* chunk_sum) {
+  const int64_t n = hdr->bins;
+  const int64_t i = blockIdx.x * (int64_t)kScanChunk + threadIdx.x;
+  const int x = i < n ? v[i] : 0;
+  int tot = 0;
+  const int ex = block_exclusive_scan_1024(x, &tot);
+  if (i < n) v[i] = ex;
+  if (threadIdx.x == 0) chunk_sum[blockIdx.x] = tot;
+}
+
+__global__ void __launch_bounds__(kScanChunk) k_scan_add(const BatchHdr* hdr, int32_t* v, const int32_t* chunk_sum) {
+  const int64_t n = hdr->bins;
+  const int64_t i = blockIdx.x * (int64_t)kScanChunk + threadIdx.x;
+  if (i < n) v[i] += chunk_sum[blockIdx.x];
+}
+
+// Pass 3: destination of each point inside its bin (rank-major order) and
+// the permutation copy of every per-point array into the second buffer.
+template <int DIM, typename PT>
+__global__ void k_sort_scatter(const BatchHdr* hdr, const BodyCtx<PT>* bodies, const int64_t* point_end,
+                               const int32_t* key, const int32_t* rank, const int32_t* cell_count,
+                               const int32_t* bin_scan) {
+  const int64_t total = hdr->points;
+  const int nb = hdr->nbodies;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n; p += stride) {
-    const int k = key[p];
-    const int r = rank[p];
-    const int b = k / bg.cells_per_bin;
-    int64_t pos = bin_start[b];
-    if (b < bg.nbins) {
-      const int l = k - b * bg.cells_per_bin;
-      const int32_t* cc = cell_count + (int64_t)b * bg.cells_per_bin;
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < total; q += stride) {
+    const BodyCtx<PT>& B = bodies[find_range(point_end, nb, q)];
+    const int64_t p = q - B.point_off;
+    const int k = key[q];
+    const int r = rank[q];
+    const int cpb = B.bg.cells_per_bin;
+    const int b = k / cpb;
+    const int32_t* bs = bin_scan + B.bin_off;
+    int64_t pos = bs[b] - bs[0];
+    if (b < B.bg.nbins) {
+      const int l = k - b * cpb;
+      const int32_t* cc = cell_count + B.cell_off + (int64_t)b * cpb;
       int below = 0, same_level = 0;
-      for (int c = 0; c < bg.cells_per_bin; c++) {
+      for (int c = 0; c < cpb; c++) {
         const int cnt = cc[c];
         below += cnt < r ? cnt : r;
         same_level += (c < l && cnt > r) ? 1 : 0;
@@ -152,29 +260,92 @@ __global__ void k_sort_scatter(BinGeom bg, int64_t n, const int32_t* key, const 
     } else {
       pos += r;
     }
-    for (int a = 0; a < src.nf; a++) dst.f[a][pos] = src.f[a][p];
-    for (int a = 0; a < src.ni; a++) dst.i[a][pos] = src.i[a][p];
-    if (src.L9 != nullptr)
-      for (int a = 0; a < 9; a++) dst.L9[9 * pos + a] = src.L9[9 * p + a];
+    const PointsT<PT>& S = B.P;
+    const PointsT<PT>& D = B.Palt;
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      D.x[d][pos] = S.x[d][p];
+      D.v[d][pos] = S.v[d][p];
+      D.u[d][pos] = S.u[d][p];
+    }
+#pragma unroll
+    for (int c = 0; c < 6; c++) D.s[c][pos] = S.s[c][p];
+    D.vol[pos] = S.vol[p];
+    D.m[pos] = S.m[p];
+    D.ext[pos] = S.ext[p];
+    D.active[pos] = S.active[p];
+    D.pid[pos] = S.pid[p];
+    if (S.L != nullptr)
+      for (int a = 0; a < 9; a++) D.L[9 * pos + a] = S.L[9 * p + a];
   }
 }
 
-// Work list: every non-empty bin split into items of at most `cap` points:
-// bin id and [start, end) of the item's points. At most
-// nonempty_bins + n / cap items.
-__global__ void k_bin_work(BinGeom bg, const int32_t* bin_start, int cap, int32_t* work_bin, int32_t* work_start,
-                           int32_t* work_end, int32_t* nwork) {
-  const int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= bg.nbins) return;
-  const int s = bin_start[b], e = bin_start[b + 1];
-  if (e <= s) return;
-  const int items = (e - s + cap - 1) / cap;
-  const int first = atomicAdd(nwork, items);
-  for (int i = 0; i < items; i++) {
-    work_bin[first + i] = b;
-    work_start[first + i] = s + i * cap;
-    work_end[first + i] = min(e, s + (i + 1) * cap);
+// Swaps the two point buffers of every body after the scatter.
+template <typename PT>
+__global__ void k_sort_flip(const BatchHdr* hdr, BodyCtx<PT>* bodies) {
+  const int nb = hdr->nbodies;
+  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) {
+    const PointsT<PT> t = bodies[b].P;
+    bodies[b].P = bodies[b].Palt;
+    bodies[b].Palt = t;
   }
+}
+
+// Clears the prime flags of every body after the priming scatter.
+template <typename PT>
+__global__ void k_clear_prime(const BatchHdr* hdr, BodyCtx<PT>* bodies) {
+  for (int b = threadIdx.x; b < hdr->nbodies; b += blockDim.x) bodies[b].prime = 0;
+}
+
+// Work list: every non-empty bin of every body split into items of at most
+// `cap` points: bin and [start, end) of the item's points (local to the
+// body). Each body's items fill its own range starting at item_off[body]
+// (room for nbins + n / cap + 1 items), so that a launch over one body
+// reads a contiguous range and CTAs share its items evenly.
+template <typename PT>
+__global__ void k_bin_work(const BatchHdr* hdr, const BodyCtx<PT>* bodies, const int64_t* bin_end,
+                           const int32_t* bin_scan, const int32_t* item_off, int cap, int32_t* work_bin,
+                           int32_t* work_start, int32_t* work_end, int32_t* nwork_body) {
+  const int64_t total = hdr->bins;
+  const int nb = hdr->nbodies;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += stride) {
+    const int bi = find_range(bin_end, nb, i);
+    const BodyCtx<PT>& B = bodies[bi];
+    const int lb = (int)(i - B.bin_off);
+    if (lb >= B.bg.nbins) continue;
+    const int32_t base = bin_scan[B.bin_off];
+    const int s = bin_scan[i] - base, e = bin_scan[i + 1] - base;
+    if (e <= s) continue;
+    const int items = (e - s + cap - 1) / cap;
+    const int first = item_off[bi] + atomicAdd(nwork_body + bi, items);
+    for (int k = 0; k < items; k++) {
+      work_bin[first + k] = lb;
+      work_start[first + k] = s + k * cap;
+      work_end[first + k] = min(e, s + (k + 1) * cap);
+    }
+  }
+}
+
+// Inclusive prefix of the per-body item counts (work_end_body[b]) and the
+// total (one CTA; bodies are at most a few thousand).
+__global__ void k_work_prefix(const BatchHdr* hdr, const int32_t* nwork_body, int32_t* work_end_body,
+                              int32_t* nwork) {
+  __shared__ int32_t carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  const int nb = hdr->nbodies;
+  for (int base = 0; base < nb; base += blockDim.x) {
+    const int i = base + threadIdx.x;
+    const int x = i < nb ? nwork_body[i] : 0;
+    int tot = 0;
+    const int ex = block_exclusive_scan_1024(x, &tot);
+    if (i < nb) work_end_body[i] = carry + ex + x;
+    __syncthreads();
+    if (threadIdx.x == 0) carry += tot;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *nwork = carry;
 }
 
 }  // namespace mpmb200

@@ -1,29 +1,33 @@
-// Device-side state of one explicit MPM job: point arrays (SoA, FP64),
-// nodal accumulators and nodal velocities (block-linear, FP64).
+// Device-side state of a batch of explicit MPM jobs: point arrays (SoA, FP64
+// or FP32), nodal accumulators and nodal velocities (block-linear, FP64
+// always), and the per-job / per-body tables the kernels read.
 #pragma once
 
 #include "geom.cuh"
 
 namespace mpmb200 {
 
-// Points of one body, structure of arrays. The Cauchy stress is stored as
-// its 6 independent components (xx, yy, zz, xy, yz, xz): the reference's
-// update (isolin.cpp:62-74) keeps T exactly symmetric when it starts
-// symmetric, so the 9-component form carries no extra information.
-struct PointsDev {
+// Points of one body, structure of arrays, in the point precision PT
+// (double for the FP64 form, float for the mixed form). The Cauchy stress is
+// stored as its 6 independent components (xx, yy, zz, xy, yz, xz): the
+// reference's update (isolin.cpp:62-74) keeps T exactly symmetric when it
+// starts symmetric, so the 9-component form carries no extra information.
+template <typename PT>
+struct PointsT {
   int64_t n;
-  double* x[3];
-  double* v[3];     // x_t
-  double* u[3];
-  double* s[6];     // stress xx yy zz xy yz xz
-  double* vol;
-  double* m;
-  double* ext;      // extent, default_points.cpp:40-57
+  PT* x[3];
+  PT* v[3];     // x_t
+  PT* u[3];
+  PT* s[6];     // stress xx yy zz xy yz xz
+  PT* vol;
+  PT* m;
+  PT* ext;      // extent, default_points.cpp:40-57
   int32_t* active;   // 1 active, 0 inactive, 2 left the domain at the last
                      // move (inactive from the next map build on)
   int32_t* pid;      // original index of the point
-  double* L;        // 9 per point when debug output is kept, else null
+  double* L;         // 9 per point when debug output is kept (FP64 form), else null
 };
+using PointsDev = PointsT<double>;
 
 // Nodal accumulators of one body (the values mapPointsToNodes builds,
 // explicit_usl.cpp:112-164): mass, momentum and force.
@@ -41,23 +45,6 @@ struct NodesVel {
   double* dv[3];
 };
 
-struct GridBodies {
-  int nb;
-  NodesAcc acc[kMaxBodies];
-  NodesVel vel[kMaxBodies];
-  NodesAcc snap[kMaxBodies];  // debug copies of m, mx_t, f after the update (or null)
-  int has_boundary[kMaxBodies];
-};
-
-struct ContactSet {
-  int nc;
-  int b1[kMaxContacts];
-  int b2[kMaxContacts];
-  double mu[kMaxContacts];
-  double* normal_out[kMaxContacts];  // 3 * nslots or null (debug)
-  double* force_out[kMaxContacts];   // 3 * nslots or null (debug)
-};
-
 struct StepParams {
   double dt;
   double grav[3];
@@ -70,6 +57,42 @@ struct MaterialParams {
   int has_material;
   double G;
   double lambda;
+};
+
+// One job (the reference's Job: one grid, its bodies and contacts). Bodies
+// body0 .. body0+nb-1 of the body tables belong to it; contact body indices
+// are local to the job.
+struct InstDev {
+  Geom g;
+  StepParams sp;
+  int nb;
+  int body0;
+  int nc;
+  int cb1[kMaxContacts];
+  int cb2[kMaxContacts];
+  double mu[kMaxContacts];
+  double* normal_out[kMaxContacts];  // 3 * nslots or null (debug)
+  double* force_out[kMaxContacts];   // 3 * nslots or null (debug)
+  int64_t block_off;                 // first node block of the job in the batch's block space
+};
+
+// What the grid update needs of a body.
+struct GridBody {
+  NodesAcc A;
+  NodesVel V;
+  NodesAcc snap;     // debug copies of m, mx_t, f after the update (or null)
+  int has_boundary;
+};
+
+// Sizes of the batch's index spaces, read by the kernels on the device so
+// that captured graphs stay valid while jobs come and go.
+struct BatchHdr {
+  int64_t points;   // sum of body point counts (sort space)
+  int64_t bins;     // sum of (nbins + 1) over bodies
+  int64_t cells;    // sum of (nbins * cells_per_bin + 1) over bodies
+  int64_t blocks;   // node-block space (jobs' ranges and free holes)
+  int nbodies;
+  int ninst;
 };
 
 }  // namespace mpmb200

@@ -35,11 +35,27 @@ class _Config(ctypes.Structure):
                 ("device", ctypes.c_int), ("keep_debug", ctypes.c_int), ("sort_interval", ctypes.c_int)]
 
 
+class _BatchConfig(ctypes.Structure):
+    _fields_ = [("dim", ctypes.c_int), ("mode", ctypes.c_int), ("device", ctypes.c_int),
+                ("sort_interval", ctypes.c_int), ("points_per_item", ctypes.c_int), ("no_graph", ctypes.c_int),
+                ("keep_debug", ctypes.c_int)]
+
+
+class _ContactDesc(ctypes.Structure):
+    _fields_ = [("body1", ctypes.c_int), ("body2", ctypes.c_int), ("mu", ctypes.c_double)]
+
+
 class _BodyDesc(ctypes.Structure):
     _fields_ = [("n", ctypes.c_int64), ("m", ctypes.c_void_p), ("v", ctypes.c_void_p), ("x", ctypes.c_void_p),
                 ("x_t", ctypes.c_void_p), ("active", ctypes.c_void_p), ("has_material", ctypes.c_int),
                 ("E", ctypes.c_double), ("nu", ctypes.c_double), ("has_boundary", ctypes.c_int),
                 ("u", ctypes.c_void_p), ("T", ctypes.c_void_p)]
+
+
+class _JobDesc(ctypes.Structure):
+    _fields_ = [("grid", ctypes.POINTER(_Config)), ("nbodies", ctypes.c_int), ("bodies", ctypes.POINTER(_BodyDesc)),
+                ("ncontacts", ctypes.c_int), ("contacts", ctypes.POINTER(_ContactDesc)),
+                ("gravity_vector", ctypes.c_int), ("gravity", ctypes.c_double * 3), ("steps", ctypes.c_int64)]
 
 
 _lib = None
@@ -78,6 +94,30 @@ def load() -> ctypes.CDLL:
     lib.mpmgpu_profile.argtypes = [vp, ctypes.c_int]
     lib.mpmgpu_profile_read.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_double)]
     lib.mpmgpu_destroy.argtypes = [vp]
+    i64p = ctypes.POINTER(ctypes.c_int64)
+    lib.mpmgpu_batch_create.argtypes = [ctypes.POINTER(_BatchConfig), ctypes.POINTER(vp)]
+    lib.mpmgpu_batch_last_error.restype = ctypes.c_char_p
+    lib.mpmgpu_batch_last_error.argtypes = [vp]
+    lib.mpmgpu_batch_footprint.argtypes = [vp, ctypes.POINTER(_JobDesc), i64p]
+    lib.mpmgpu_batch_add_job.argtypes = [vp, ctypes.POINTER(_JobDesc), ctypes.POINTER(ctypes.c_int)]
+    lib.mpmgpu_batch_step.argtypes = [vp, ctypes.c_int]
+    lib.mpmgpu_batch_synchronize.argtypes = [vp]
+    lib.mpmgpu_batch_job_state.argtypes = [vp, ctypes.c_int, i64p, i64p]
+    lib.mpmgpu_batch_sizes.argtypes = [vp, ctypes.c_int, ctypes.c_int, i64p, i64p]
+    lib.mpmgpu_batch_download_points.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp]
+    lib.mpmgpu_batch_remove_job.argtypes = [vp, ctypes.c_int]
+    lib.mpmgpu_batch_counts.argtypes = [vp, ctypes.POINTER(ctypes.c_int), i64p, i64p]
+    lib.mpmgpu_batch_autotune.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+    lib.mpmgpu_batch_points_per_item.argtypes = [vp]
+    lib.mpmgpu_batch_active_nodes.argtypes = [vp, i64p, i64p]
+    lib.mpmgpu_active_nodes.argtypes = [vp, i64p, i64p]
+    lib.mpmgpu_batch_profile.argtypes = [vp, ctypes.c_int]
+    lib.mpmgpu_batch_profile_read.argtypes = [vp, ctypes.c_int, i64p, ctypes.POINTER(ctypes.c_double)]
+    lib.mpmgpu_batch_stream.restype = vp
+    lib.mpmgpu_batch_stream.argtypes = [vp]
+    lib.mpmgpu_batch_launch_count.restype = ctypes.c_int64
+    lib.mpmgpu_batch_launch_count.argtypes = [vp]
+    lib.mpmgpu_batch_destroy.argtypes = [vp]
     _lib = lib
     return lib
 
@@ -164,6 +204,13 @@ class GPUExplicitUSL:
 
     STAGES = {"g2p2g": 0, "grid": 1, "compact": 2, "rebin": 3}
 
+    def active_nodes(self) -> Tuple[int, int]:
+        """(nodes with mass in the last step, per body; drifted point visits)."""
+        a = ctypes.c_int64()
+        d = ctypes.c_int64()
+        self._check(self.lib.mpmgpu_active_nodes(self.h, ctypes.byref(a), ctypes.byref(d)))
+        return int(a.value), int(d.value)
+
     def profile(self, enable: bool = True):
         """Starts (and resets) or stops per-stage CUDA-event timing."""
         self._check(self.lib.mpmgpu_profile(self.h, int(enable)))
@@ -217,3 +264,162 @@ class GPUExplicitUSL:
         self._check(self.lib.mpmgpu_dump_map_noalloc(self.h, b, d_node, d_point, d_s, d_grad, capacity,
                                                      ctypes.byref(cnt)))
         return cnt.value
+
+
+def _case_config(case: inputs.Case, mode: str = "fp64") -> _Config:
+    cfg = _Config()
+    cfg.dim = case.dim
+    for d in range(3):
+        cfg.L[d] = case.L[d] if d < case.dim else 0.0
+        cfg.N[d] = case.N[d] if d < case.dim else 0
+    cfg.dt = case.dt
+    cfg.cpdi_spec = case.cpdi
+    cfg.contact_spec = case.contact_spec
+    cfg.mode = MODES[mode]
+    return cfg
+
+
+class GPUBatch:
+    """Many independent ``inputs.Case`` jobs stepped together on one GPU
+    (``mpmgpu_batch_*``): one launch per stage for all jobs, the step replayed
+    from a CUDA graph. Jobs may be added while others run; each runs its own
+    step count and then stops advancing until removed.
+    """
+
+    def __init__(self, dim: int = 3, mode: str = "mixed", device: int = 0, sort_interval: int = 0,
+                 points_per_item: int = 0, graph: bool = True, keep_debug: bool = False):
+        self.lib = load()
+        cfg = _BatchConfig(dim, MODES[mode], device, sort_interval, points_per_item, 0 if graph else 1,
+                           int(keep_debug))
+        h = ctypes.c_void_p()
+        st = self.lib.mpmgpu_batch_create(ctypes.byref(cfg), ctypes.byref(h))
+        if st != 0:
+            raise MpmGpuError(f"{self.lib.mpmgpu_status_string(st).decode()}: batch create")
+        self.h = h
+        self.dim = dim
+        self.cases: Dict[int, inputs.Case] = {}
+
+    def _check(self, status: int):
+        if status != 0:
+            msg = self.lib.mpmgpu_status_string(status).decode()
+            raise MpmGpuError(f"{msg}: {self.lib.mpmgpu_batch_last_error(self.h).decode()}")
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.mpmgpu_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _job_desc(self, case: inputs.Case, steps: Optional[int]):
+        keep = []
+        cfg = _case_config(case)
+        bodies = (_BodyDesc * len(case.bodies))()
+        for i, body in enumerate(case.bodies):
+            arrs = dict(m=np.ascontiguousarray(body.m, np.float64), v=np.ascontiguousarray(body.v, np.float64),
+                        x=np.ascontiguousarray(body.x, np.float64), x_t=np.ascontiguousarray(body.x_t, np.float64),
+                        active=np.ascontiguousarray(body.active, np.int32))
+            keep.append(arrs)
+            bodies[i] = _BodyDesc(body.n, _ptr(arrs["m"]).value, _ptr(arrs["v"]).value, _ptr(arrs["x"]).value,
+                                  _ptr(arrs["x_t"]).value, _ptr(arrs["active"]).value, int(body.material), body.E,
+                                  body.nu, int(body.boundary), None, None)
+        contacts = (_ContactDesc * max(1, len(case.contacts)))()
+        for i, c in enumerate(case.contacts):
+            contacts[i] = _ContactDesc(c.b1, c.b2, c.mu)
+        desc = _JobDesc()
+        desc.grid = ctypes.pointer(cfg)
+        desc.nbodies = len(case.bodies)
+        desc.bodies = bodies
+        desc.ncontacts = len(case.contacts)
+        desc.contacts = contacts
+        if case.gravity is not None:
+            desc.gravity_vector = 1
+            g = list(case.gravity) + [0.0] * (3 - len(case.gravity))
+            for d in range(3):
+                desc.gravity[d] = g[d]
+        desc.steps = int(case.steps if steps is None else steps)
+        keep += [cfg, bodies, contacts]
+        return desc, keep
+
+    def footprint(self, case: inputs.Case, steps: Optional[int] = None) -> int:
+        desc, _keep = self._job_desc(case, steps)
+        out = ctypes.c_int64()
+        self._check(self.lib.mpmgpu_batch_footprint(self.h, ctypes.byref(desc), ctypes.byref(out)))
+        return int(out.value)
+
+    def add(self, case: inputs.Case, steps: Optional[int] = None) -> int:
+        """Adds a job (runs ``steps``, default ``case.steps``); returns its id."""
+        desc, _keep = self._job_desc(case, steps)
+        jid = ctypes.c_int()
+        self._check(self.lib.mpmgpu_batch_add_job(self.h, ctypes.byref(desc), ctypes.byref(jid)))
+        self.cases[jid.value] = case
+        return jid.value
+
+    def step(self, n: int = 1):
+        self._check(self.lib.mpmgpu_batch_step(self.h, n))
+
+    def synchronize(self):
+        self._check(self.lib.mpmgpu_batch_synchronize(self.h))
+
+    def state(self, job: int) -> Tuple[int, int]:
+        done = ctypes.c_int64()
+        left = ctypes.c_int64()
+        self._check(self.lib.mpmgpu_batch_job_state(self.h, job, ctypes.byref(done), ctypes.byref(left)))
+        return int(done.value), int(left.value)
+
+    def points(self, job: int, b: int, name: str) -> np.ndarray:
+        fid, w = POINT_FIELDS[name]
+        out = np.zeros((self.cases[job].bodies[b].n, w))
+        self._check(self.lib.mpmgpu_batch_download_points(self.h, job, b, fid, _ptr(out)))
+        return out
+
+    def remove(self, job: int):
+        self._check(self.lib.mpmgpu_batch_remove_job(self.h, job))
+        self.cases.pop(job, None)
+
+    def counts(self) -> Tuple[int, int, int]:
+        """(jobs still stepping, their points, device bytes held)."""
+        j = ctypes.c_int()
+        p = ctypes.c_int64()
+        b = ctypes.c_int64()
+        self._check(self.lib.mpmgpu_batch_counts(self.h, ctypes.byref(j), ctypes.byref(p), ctypes.byref(b)))
+        return int(j.value), int(p.value), int(b.value)
+
+    def autotune(self, steps: int = 5) -> int:
+        cap = ctypes.c_int()
+        self._check(self.lib.mpmgpu_batch_autotune(self.h, steps, ctypes.byref(cap)))
+        return int(cap.value)
+
+    def points_per_item(self) -> int:
+        return int(self.lib.mpmgpu_batch_points_per_item(self.h))
+
+    def active_nodes(self) -> Tuple[int, int]:
+        """(nodes with mass in the last step, per body; drifted point visits)."""
+        a = ctypes.c_int64()
+        d = ctypes.c_int64()
+        self._check(self.lib.mpmgpu_batch_active_nodes(self.h, ctypes.byref(a), ctypes.byref(d)))
+        return int(a.value), int(d.value)
+
+    STAGES = GPUExplicitUSL.STAGES
+
+    def profile(self, enable: bool = True):
+        self._check(self.lib.mpmgpu_batch_profile(self.h, int(enable)))
+
+    def profile_read(self) -> Dict[str, Tuple[int, float]]:
+        out = {}
+        for name, sid in self.STAGES.items():
+            n = ctypes.c_int64()
+            ms = ctypes.c_double()
+            self._check(self.lib.mpmgpu_batch_profile_read(self.h, sid, ctypes.byref(n), ctypes.byref(ms)))
+            out[name] = (int(n.value), float(ms.value))
+        return out
+
+    def stream(self) -> int:
+        return int(self.lib.mpmgpu_batch_stream(self.h) or 0)
+
+    def launches(self) -> int:
+        return int(self.lib.mpmgpu_batch_launch_count(self.h))
