@@ -1037,6 +1037,8 @@ class Batch : public BatchBase {
     MPM_TRY(grow(&work_bin_, &cap_items_n_, std::max<int64_t>(items, 1), 0));
     MPM_TRY(grow(&work_start_, &cap_items_s_, std::max<int64_t>(items, 1), 0));
     MPM_TRY(grow(&work_end_, &cap_items_e_, std::max<int64_t>(items, 1), 0));
+    MPM_TRY(grow(&flat_body_, &cap_items_fb_, std::max<int64_t>(items, 1), 0));
+    MPM_TRY(grow(&flat_item_, &cap_items_fi_, std::max<int64_t>(items, 1), 0));
     for (size_t b = 0; b < ctx.size(); b++) ctx[b].flags = flags_ + insts[(size_t)ctx[b].inst].block_off;
     ctx_host_ = ctx;
     single_mode_ = ctx.size() <= 4;
@@ -1142,6 +1144,8 @@ class Batch : public BatchBase {
     fl.item_off = item_off_d_;
     fl.nwork_body = nwork_body_;
     fl.work_end_body = work_end_body_;
+    fl.flat_body = flat_body_;
+    fl.flat_item = flat_item_;
     fl.nbodies_cap = (int)ctx_host_.size();
     fl.work_bin = work_bin_;
     fl.work_start = work_start_;
@@ -1247,6 +1251,9 @@ class Batch : public BatchBase {
     MPM_TRY(check_launch("k_bin_work"));
     k_work_prefix<<<1, 1024, 0, stream_>>>(hdr_, nwork_body_, work_end_body_, nwork_);
     MPM_TRY(check_launch("k_work_prefix"));
+    k_work_flat<<<sb, 256, 0, stream_>>>(hdr_, item_off_d_, nwork_body_, work_end_body_, nwork_, flat_body_,
+                                         flat_item_);
+    MPM_TRY(check_launch("k_work_flat"));
     return MPMGPU_OK;
   }
 
@@ -1315,7 +1322,7 @@ class Batch : public BatchBase {
   }
 
   mpmgpu_status launch_sort() {
-    MPM_TRY(run_graph(g_sort_, sort_warm_, 10, [&] { return launch_sort_direct(); }));
+    MPM_TRY(run_graph(g_sort_, sort_warm_, 11, [&] { return launch_sort_direct(); }));
     flip_mirrors();
     steps_since_sort_ = 0;
     return MPMGPU_OK;
@@ -1460,6 +1467,10 @@ class Batch : public BatchBase {
   int64_t cap_bins_ = 0;
   int32_t* chunk_sum_ = nullptr;
   int64_t cap_chunks_ = 0;
+  int32_t* flat_body_ = nullptr;
+  int64_t cap_items_fb_ = 0;
+  int32_t* flat_item_ = nullptr;
+  int64_t cap_items_fi_ = 0;
   int32_t* item_off_d_ = nullptr;
   int64_t cap_bodies_i_ = 0;
   int32_t* nwork_body_ = nullptr;

@@ -52,6 +52,8 @@ struct FusedLaunch {
   const int32_t* item_off;       // first item of each body's range
   const int32_t* nwork_body;     // items of each body
   const int32_t* work_end_body;  // inclusive prefix of nwork_body
+  const int32_t* flat_body;      // flat index -> body (launches over every body)
+  const int32_t* flat_item;      // flat index -> item
   const int32_t* work_bin;
   const int32_t* work_start;
   const int32_t* work_end;
@@ -85,16 +87,20 @@ __host__ __device__ constexpr int fused_bin() {
   return DIM == 3 ? 4 : 8;
 }
 
-// Shared memory layout: mbarrier | body table entry | points [kNF][row] |
-// active [row] | tile [10][TN] doubles | touched [TN].
+// Shared memory layout: mbarriers (points, table entry slots 0 and 1) |
+// body table entries [2] | points [kNF][row] | active [row] | tile [10][TN]
+// doubles | touched [TN].
 template <typename PT>
 __host__ __device__ constexpr size_t ctx_bytes() {
   return (offsetof(BodyCtx<PT>, Palt) + 15) / 16 * 16;
 }
-constexpr size_t kOffCtx = 16;
+constexpr size_t kOffCtx = 32;
+static_assert(ctx_bytes<double>() % 16 == 0 && ctx_bytes<float>() % 16 == 0, "bulk copies move 16-byte multiples");
+static_assert(sizeof(BodyCtx<double>) % 16 == 0 && sizeof(BodyCtx<float>) % 16 == 0,
+              "table entries start on 16-byte boundaries");
 template <typename PT, int CAP>
 __host__ __device__ constexpr size_t off_pts() {
-  return kOffCtx + ctx_bytes<PT>();
+  return kOffCtx + 2 * ctx_bytes<PT>();
 }
 template <typename PT, int CAP>
 __host__ __device__ constexpr size_t off_act() {
@@ -483,10 +489,13 @@ __global__ void __launch_bounds__(MPMB200_FUSED_THREADS, MPMB200_FUSED_MIN_CTAS)
   constexpr int TN = fused_tile_nodes<DIM, B>();
   constexpr int ROW = cap_row<CAP>();
   constexpr int AL = 16 / (int)sizeof(PT);   // elements per 16 bytes
+  constexpr uint32_t kCtxBytes = (uint32_t)ctx_bytes<PT>();
   extern __shared__ __align__(128) unsigned char smem[];
-  uint64_t* bar = reinterpret_cast<uint64_t*>(smem);
-  BodyCtx<PT>& sc = *reinterpret_cast<BodyCtx<PT>*>(smem + kOffCtx);
-  const BodyCtx<PT>& c = SINGLE ? fl.one : sc;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem);          // point arrays
+  uint64_t* bar_ctx = reinterpret_cast<uint64_t*>(smem + 8);  // table entry slots 0, 1
+  // slot i holds the first ctx_bytes of a table entry (the fields up to
+  // Palt); it is addressed by bytes, not as an array of whole entries
+  auto slot_ctx = [&](int i) { return reinterpret_cast<BodyCtx<PT>*>(smem + kOffCtx + (size_t)i * kCtxBytes); };
   PT* pts = reinterpret_cast<PT*>(smem + off_pts<PT, CAP>());
   int32_t* act = reinterpret_cast<int32_t*>(smem + off_act<PT, CAP>());
   double* tile = reinterpret_cast<double*>(smem + off_tile<PT, CAP>());  // phase 2: NACC FP64 values
@@ -495,27 +504,52 @@ __global__ void __launch_bounds__(MPMB200_FUSED_THREADS, MPMB200_FUSED_MIN_CTAS)
 
   if (threadIdx.x == 0) {
     mbar_init(bar, 1);
+    mbar_init(bar_ctx, 1);
+    mbar_init(bar_ctx + 1, 1);
     mbar_init_fence();
   }
   __syncthreads();
   uint32_t parity = 0;
   const int nwork = SINGLE ? fl.nwork_body[fl.one_body] : *fl.nwork;
-  for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
-    int body, item;
+  // launches over every body: the table entry of each work item arrives by
+  // a bulk copy issued one item ahead (slot k & 1 for the CTA's k-th item)
+  if (!SINGLE && threadIdx.x == 0 && (int)blockIdx.x < nwork) {
+    mbar_arrive_expect_tx(bar_ctx, kCtxBytes);
+    bulk_copy_g2s(slot_ctx(0), fl.bodies + fl.flat_body[blockIdx.x], kCtxBytes, bar_ctx);
+  }
+  int k = 0;
+  for (int w = blockIdx.x; w < nwork; w += gridDim.x, k++) {
+    int item;
     if (SINGLE) {
-      body = fl.one_body;
-      item = fl.item_off[body] + w;
+      item = fl.item_off[fl.one_body] + w;
     } else {
-      // the body whose items hold flat index w (every thread finds the same)
-      body = find_range(fl.work_end_body, fl.nbodies_cap, w);
-      item = fl.item_off[body] + (w - (fl.work_end_body[body] - fl.nwork_body[body]));
+      item = fl.flat_item[w];
+      const int slot = k & 1;
+      const bool ahead = w + (int)gridDim.x < nwork;
+      if (threadIdx.x == 0 && ahead) {
+        // the other slot was last read by the previous item (all threads
+        // passed its closing barrier)
+        fence_async_shared();
+        mbar_arrive_expect_tx(bar_ctx + (slot ^ 1), kCtxBytes);
+        bulk_copy_g2s(slot_ctx(slot ^ 1), fl.bodies + fl.flat_body[w + gridDim.x], kCtxBytes, bar_ctx + (slot ^ 1));
+      }
+      const bool got = mbar_wait_bounded(bar_ctx + slot, (uint32_t)((k >> 1) & 1), fl.err);
+      if (__syncthreads_or(got ? 0 : 1)) {
+        // let the copies in flight land before leaving
+        if (threadIdx.x == 0) {
+          if (!got) mbar_wait_bounded(bar_ctx + slot, (uint32_t)((k >> 1) & 1), fl.err);
+          if (ahead) mbar_wait_bounded(bar_ctx + (slot ^ 1), (uint32_t)(((k + 1) >> 1) & 1), fl.err);
+        }
+        return;
+      }
+    }
+    const BodyCtx<PT>& c = SINGLE ? fl.one : *slot_ctx(k & 1);
+    if (!SINGLE) {
       // items of the other kind (contact normal or not) belong to the other launch
-      if ((fl.bodies[body].needs_normal != 0) != NORMAL) continue;
-      // stage the body's table entry
-      const uint4* src = reinterpret_cast<const uint4*>(fl.bodies + body);
-      uint4* dst = reinterpret_cast<uint4*>(&sc);
-      for (int i = threadIdx.x; i < (int)(ctx_bytes<PT>() / 16); i += blockDim.x) dst[i] = src[i];
-      __syncthreads();
+      if ((c.needs_normal != 0) != NORMAL) {
+        __syncthreads();
+        continue;
+      }
     }
     const int prime = c.prime;
     if (fl.prime_pass && !prime) {

@@ -34,7 +34,7 @@ struct BinGeom {
 // Per-body table entry. The first part (up to Palt) is what the fused
 // kernel stages in shared memory for a work item.
 template <typename PT>
-struct BodyCtx {
+struct alignas(16) BodyCtx {
   Geom g;
   MapConst mc;
   BinGeom bg;
@@ -317,12 +317,14 @@ __global__ void k_bin_work(const BatchHdr* hdr, const BodyCtx<PT>* bodies, const
     const int32_t base = bin_scan[B.bin_off];
     const int s = bin_scan[i] - base, e = bin_scan[i + 1] - base;
     if (e <= s) continue;
+    // split evenly: a bin of 1.2 cap points becomes two items of 0.6 cap
     const int items = (e - s + cap - 1) / cap;
     const int first = item_off[bi] + atomicAdd(nwork_body + bi, items);
+    const int cnt = e - s;
     for (int k = 0; k < items; k++) {
       work_bin[first + k] = lb;
-      work_start[first + k] = s + k * cap;
-      work_end[first + k] = min(e, s + (k + 1) * cap);
+      work_start[first + k] = s + (int)((int64_t)cnt * k / items);
+      work_end[first + k] = s + (int)((int64_t)cnt * (k + 1) / items);
     }
   }
 }
@@ -346,6 +348,20 @@ __global__ void k_work_prefix(const BatchHdr* hdr, const int32_t* nwork_body, in
     __syncthreads();
   }
   if (threadIdx.x == 0) *nwork = carry;
+}
+
+// Flat work list for launches over every body: flat index w -> (body, item),
+// body-major, so that consecutive CTAs take consecutive items.
+__global__ void k_work_flat(const BatchHdr* hdr, const int32_t* item_off, const int32_t* nwork_body,
+                            const int32_t* work_end_body, const int32_t* nwork, int32_t* flat_body,
+                            int32_t* flat_item) {
+  const int total = *nwork;
+  const int nb = hdr->nbodies;
+  for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < total; w += gridDim.x * blockDim.x) {
+    const int b = find_range(work_end_body, nb, w);
+    flat_body[w] = b;
+    flat_item[w] = item_off[b] + (w - (work_end_body[b] - nwork_body[b]));
+  }
 }
 
 }  // namespace mpmb200

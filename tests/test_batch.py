@@ -99,6 +99,22 @@ def test_remove_and_reuse_block_ranges():
     batch.close()
 
 
+def test_table_launch_with_many_items_per_cta():
+    """More than four bodies: one launch over the body table, and more work
+    items than CTAs, so every CTA walks several items (its table-entry
+    slots alternate)."""
+    col = inputs.column_collapse_3d(scale=2, steps=6)
+    tiny = inputs.block_drop_ensemble(count=4, seed=5, n_range=(8, 10), steps=6)
+    cases = [col] + tiny
+    batch = GPUBatch(dim=3, mode="fp64")
+    jobs = [batch.add(c) for c in cases]
+    batch.step(6)
+    batch.synchronize()
+    for j, c in zip(jobs, cases):
+        _compare(c, _from_batch(batch, j, c), _solo(c, c.steps), FP64_TOL, c.name)
+    batch.close()
+
+
 def test_graph_replay_matches_direct_launches():
     cases = _cases()[:3]
     runs = []
