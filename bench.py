@@ -2,25 +2,34 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME] [--impl ours|reference]
 
-Prints one JSON line. A "step" is one ExplicitUSL time step over the whole
-workload (map build, P2G, contact, boundary, grid update, G2P, stress) with
-the point and grid state resident in HBM; ``value`` is whole-job
+Prints one JSON line. A "step" is one ExplicitUSL time step of every job of
+the workload (map build, P2G, contact, boundary, grid update, G2P, stress)
+with the point and grid state resident in HBM; ``value`` is whole-job
 particle-steps per second from CUDA events on the solver's stream, ``e2e``
 is the same metric through the C ABI from host buffers (upload, K steps,
 download of the final point state, all inside the timed region).
 
 Workloads (seeded synthetic inputs, mpm_3d_b200.inputs):
-  collision  two 0.25 m cubes colliding, 128^3 grid, 524,288 points, ContactHuang
-  column     column collapse, 256x256x128 grid, 3,145,728 points
+  ensemble   (default) 512 independent 3D block drops (grids 16^3..96^3,
+             16.75 M points, seed 1003) in one batch, mixed form (FP32 point
+             state, FP64 nodal sums), one launch per stage replayed from a
+             CUDA graph, points per CTA chosen by the autotuner. Reported
+             beside it: the same batch in FP64, the plain FP64 path (one
+             handle per job, jobs one after another) and the mixed form's
+             error against FP64 on every 8th job.
+  collision  two 0.25 m cubes colliding, 128^3 grid, 524,288 points, ContactHuang (FP64)
+  column     column collapse, 256x256x128 grid, 3,145,728 points (FP64)
 
-With N > 1 (torchrun) every rank runs an independent replica of the
-workload (the single-instance step does not shard); ``value`` sums the
-points of all ranks over the slowest rank's time.
+With N > 1 (torchrun) every rank runs its own copy of the workload (the
+ensemble with seed 1003 + rank; the single jobs as replicas): no data
+crosses ranks; ``value`` sums the points of all ranks over the slowest
+rank's time.
 
 ``--impl reference`` times the reference solver's own CPU code
 (ThreadPoolExplicitUSL + ThreadPoolPoints, compiled from its sources into
 oracle/_ref/libmpmref_timing.so) on all host threads, on a bounded sample of
-steps of the same workload.
+the same workload (for the ensemble: 16 of its jobs, every 32nd, a few steps
+each, one after another).
 """
 from __future__ import annotations
 
@@ -56,20 +65,43 @@ def peaks():
         return 6650.0, "fallback"
 
 
-def make_workload(name: str):
+ENSEMBLE_JOBS = 512
+ENSEMBLE_SEED = 1003
+
+
+def make_workload(name: str, rank: int = 0):
     if name == "collision":
         return inputs.two_body_collision_3d(128)
     if name == "column":
         return inputs.column_collapse_3d(1)
+    if name == "ensemble":
+        return inputs.block_drop_ensemble(ENSEMBLE_JOBS, seed=ENSEMBLE_SEED + rank)
     raise SystemExit(f"unknown workload {name}")
 
 
-def bytes_per_point_step(active_nodes_per_point: float) -> float:
-    """Algorithmic bytes per particle-step of the FP64 form: point state read
+def bytes_per_point_step(active_nodes_per_point: float, mixed: bool = False) -> float:
+    """Algorithmic bytes per particle-step. FP64 form: point state read
     (x, v, m, V, sigma(6), u, extent, active = 148 B) and written (x, v, V,
-    sigma, u = 128 B), plus the grid term 112 B per active node per body
-    (m, momentum, force accumulated and read once)."""
-    return 276.0 + 112.0 * active_nodes_per_point
+    sigma, u = 128 B); mixed form: the same fields in FP32 (76 B read, 64 B
+    written). Plus the grid term 112 B per active node per body (m,
+    momentum, force accumulated and read once, FP64 in both forms)."""
+    return (140.0 if mixed else 276.0) + 112.0 * active_nodes_per_point
+
+
+def field_floor(case, field: str) -> float:
+    """Physical scale of a field for relative errors (velocity: largest
+    initial speed, at least 1 m/s; stress: one step of elastic stress at
+    that speed over a cell; position: the domain)."""
+    v0 = max(1.0, max(float(np.abs(b.x_t).max()) for b in case.bodies))
+    h = min(case.h)
+    E = max(b.E for b in case.bodies)
+    return {"T": E * case.dt * v0 / h, "x_t": v0, "x": min(case.L)}.get(field, 0.0)
+
+
+def rel_err(got, ref, floor: float) -> float:
+    scale = max(float(np.max(np.abs(ref))) if ref.size else 0.0, floor)
+    diff = float(np.max(np.abs(got - ref))) if ref.size else 0.0
+    return diff / scale if scale > 0 else diff
 
 
 class ClockSampler:
@@ -209,6 +241,22 @@ class quiet_stdout:
 def run_reference_arm(args, rank, world):
     if rank != 0:
         return
+    if args.workload == "ensemble":
+        cases = make_workload("ensemble")
+        steps = max(1, min(args.steps, args.ref_steps))
+        cpu = cpu_ensemble_sample(cases, steps)
+        value = cpu["value"]
+        line = {
+            "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": steps, "warmup": 1, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": f"synthetic (block_drop_ensemble seed {ENSEMBLE_SEED})",
+            "config": {"workload": f"ensemble{ENSEMBLE_JOBS}", "jobs": len(cases),
+                       "points": sum(c.n_points for c in cases)},
+            "cpu_baseline": cpu,
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }
+        print(json.dumps(line), flush=True)
+        return
     case = make_workload(args.workload)
     threads = os.cpu_count() or 1
     steps = max(1, min(args.steps, args.ref_steps))
@@ -228,7 +276,56 @@ def run_reference_arm(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
-def run_ours(args, rank, world, local):
+def timed_steps(sim, steps: int, flush_buf=None):
+    """Times `steps` single steps with CUDA events on the solver's stream
+    (L2 flushed before each when `flush_buf` is given); returns per-step ms,
+    kernel launches in the timed region and the clock record."""
+    import torch
+
+    stream = torch.cuda.ExternalStream(sim.stream())
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    stops = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    sim.synchronize()
+    torch.cuda.synchronize()
+    launches0 = sim.launches()
+    with ClockSampler(torch.cuda.current_device()) as clocks:
+        for k in range(steps):
+            if flush_buf is not None:
+                with torch.cuda.stream(stream):
+                    flush_buf.fill_(float(k))
+            starts[k].record(stream)
+            sim.step(1)
+            stops[k].record(stream)
+        sim.synchronize()
+        torch.cuda.synchronize()
+    launches = sim.launches() - launches0
+    return [starts[k].elapsed_time(stops[k]) for k in range(steps)], launches, clocks.summary()
+
+
+def profile_pass(sim, steps: int):
+    """Per-stage device time over `steps` steps (stage by stage launches)."""
+    sim.profile(True)
+    sim.step(steps)
+    prof = sim.profile_read()
+    sim.profile(False)
+    return prof
+
+
+def roofline(points: int, steps: int, prof, active_ratio: float, mixed: bool):
+    peak, peak_kind = peaks()
+    bpp = bytes_per_point_step(active_ratio, mixed)
+    g_launches, g_ms = prof["g2p2g"]
+    per_launch_ms = g_ms / max(1, g_launches)
+    # the fused launches of a step together process every point once; the
+    # algorithmic bytes of a launch are its points times bytes per point-step
+    points_per_launch = points * steps / max(1, g_launches)
+    achieved_gbs = points_per_launch * bpp / (per_launch_ms * 1e-3) / 1e9
+    return {"bound": "hbm", "kernel": "k_g2p2g", "achieved": achieved_gbs, "peak": peak, "unit": "GB/s",
+            "frac": achieved_gbs / peak, "peak_kind": peak_kind, "traffic": None, "bytes_per_point_step": bpp,
+            "launch_ms": per_launch_ms, "points_per_launch": points_per_launch}
+
+
+def run_single(args, rank, world, local):
     import torch
 
     from mpm_3d_b200.native import GPUExplicitUSL
@@ -240,49 +337,23 @@ def run_ours(args, rank, world, local):
     flush_l2 = state_bytes < 2 * L2_BYTES
     flush_buf = torch.empty(4 * L2_BYTES // 4, dtype=torch.float32, device="cuda") if flush_l2 else None
 
-    sim = GPUExplicitUSL(case, device=local)
-    stream = torch.cuda.ExternalStream(sim.stream())
+    sim = GPUExplicitUSL(case, device=local, mode=args.form)
     sim.step(args.warmup)
-    sim.synchronize()
-    sim.profile(True)
-    launches0 = sim.launches()
-    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    stops = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    torch.cuda.synchronize()
     barrier(world)
-    with ClockSampler(local) as clocks:
-        for k in range(args.steps):
-            if flush_l2:
-                with torch.cuda.stream(stream):
-                    flush_buf.fill_(float(k))
-            starts[k].record(stream)
-            sim.step(1)
-            stops[k].record(stream)
-        sim.synchronize()
-        torch.cuda.synchronize()
+    step_ms, launches, clk = timed_steps(sim, args.steps, flush_buf)
     barrier(world)
-    step_ms = [starts[k].elapsed_time(stops[k]) for k in range(args.steps)]
-    prof = sim.profile_read()
-    launches = sim.launches() - launches0
-    sim.profile(False)
     total_ms = sum(step_ms)
     total_ms_max = max_over_ranks(total_ms, world)
     points_all = sum_over_ranks(float(n), world)
     value = points_all * args.steps / (total_ms_max * 1e-3)
-
-    # active nodes per point (grid term of the algorithmic bytes)
-    active_ratio = active_nodes_ratio(sim, case)
-    bpp = bytes_per_point_step(active_ratio)
-    g_launches, g_ms = prof["g2p2g"]
-    per_launch_ms = g_ms / max(1, g_launches)
-    # the fused launches of a step together process every point once; the
-    # algorithmic bytes of a launch are its points times bytes per point-step
-    points_per_launch = n * args.steps / max(1, g_launches)
-    achieved_gbs = points_per_launch * bpp / (per_launch_ms * 1e-3) / 1e9
-    peak, peak_kind = peaks()
+    prof_steps = min(10, args.steps)
+    prof = profile_pass(sim, prof_steps)
+    active, _drift = sim.active_nodes()
+    active_ratio = active / max(1, n)
+    roof = roofline(n, prof_steps, prof, active_ratio, args.form == "mixed")
     sim.close()
 
-    e2e = run_e2e(case, args.steps, local) if rank == 0 and not args.no_e2e else None
+    e2e = run_e2e(case, args.steps, local, args.form) if rank == 0 and not args.no_e2e else None
     cpu = None
     if rank == 0 and not args.no_cpu:
         try:
@@ -296,19 +367,16 @@ def run_ours(args, rank, world, local):
             cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": f"unavailable: {exc}"}
     if rank != 0:
         return
-    clk = clocks.summary()
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": total_ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64", "data": "synthetic (seeded mpm_3d_b200.inputs)",
+        "dtype": "f32+f64" if args.form == "mixed" else "f64", "data": "synthetic (seeded mpm_3d_b200.inputs)",
         "config": {"workload": args.workload, "points": n, "bodies": len(case.bodies), "grid": list(case.N),
-                   "dt": case.dt, "form": "fp64", "parallelism": f"replicas{world}",
+                   "dt": case.dt, "form": args.form, "parallelism": f"replicas{world}",
                    "l2": "flushed between steps" if flush_l2 else "inputs larger than L2",
                    "active_nodes_per_point": round(active_ratio, 4)},
-        "roofline": {"bound": "hbm", "kernel": "k_g2p2g", "achieved": achieved_gbs, "peak": peak, "unit": "GB/s",
-                     "frac": achieved_gbs / peak, "peak_kind": peak_kind, "traffic": None,
-                     "bytes_per_point_step": bpp, "launch_ms": per_launch_ms},
-        "stage_ms_per_step": {k: v[1] / args.steps for k, v in prof.items()},
+        "roofline": roof,
+        "stage_ms_per_step": {k: v[1] / prof_steps for k, v in prof.items()},
         "gpu_launches": launches,
         "clocks": clk,
         "e2e": e2e,
@@ -317,18 +385,162 @@ def run_ours(args, rank, world, local):
     print(json.dumps(line), flush=True)
 
 
-def active_nodes_ratio(sim, case) -> float:
-    """Active nodes (m > 0) per point, counted per body after the last step."""
-    from mpm_3d_b200.native import GPUExplicitUSL  # noqa: F401
-
-    tot = 0
-    for b in range(len(case.bodies)):
-        xt = sim.nodes(b, "x_t")
-        tot += int(np.count_nonzero(np.any(xt != 0.0, axis=1)))
-    return tot / max(1, case.n_points)
+def ensemble_sample(cases, every: int = 8):
+    return list(range(0, len(cases), every))
 
 
-def run_e2e(case, steps: int, device: int):
+def run_batch(cases, mode: str, args, device: int, sample_ids):
+    """One batch of every job: autotune, warm-up, K timed steps (graph
+    replay), a profiled pass; returns figures and the final x, x_t, T of the
+    sampled jobs."""
+    from mpm_3d_b200.native import GPUBatch
+
+    b = GPUBatch(dim=3, mode=mode, device=device)
+    jobs = [b.add(c) for c in cases]
+    cap = b.autotune(steps=8)
+    si = b.sort_interval()
+    b.step(args.warmup)
+    step_ms, launches, clk = timed_steps(b, args.steps)
+    prof_steps = 3
+    prof = profile_pass(b, prof_steps)
+    active, drift = b.active_nodes()
+    fields = {i: {f: b.points(jobs[i], 0, f) for f in ("x", "x_t", "T")} for i in sample_ids}
+    steps_done = b.state(jobs[0])[0]
+    b.close()
+    return {"step_ms": step_ms, "launches": launches, "clocks": clk, "prof": prof, "prof_steps": prof_steps,
+            "active": active, "drift": drift, "cap": cap, "sort_interval": si, "fields": fields,
+            "steps_done": steps_done}
+
+
+def plain_fp64(cases, steps: int, device: int):
+    """The plain FP64 path: one single-job handle per job, the jobs one
+    after another; per job 3 warm-up steps, then `steps` steps timed with
+    CUDA events (set-up and teardown outside the timed regions)."""
+    import torch
+
+    from mpm_3d_b200.native import GPUExplicitUSL
+
+    total_ms = 0.0
+    points = 0
+    for c in cases:
+        sim = GPUExplicitUSL(c, device=device)
+        sim.step(3)
+        stream = torch.cuda.ExternalStream(sim.stream())
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        sim.synchronize()
+        e0.record(stream)
+        sim.step(steps)
+        e1.record(stream)
+        sim.synchronize()
+        total_ms += e0.elapsed_time(e1)
+        points += c.n_points
+        sim.close()
+    return points * steps / (total_ms * 1e-3), total_ms
+
+
+def run_ensemble(args, rank, world, local):
+    import torch
+
+    torch.cuda.set_device(local)
+    cases = make_workload("ensemble", rank)
+    n = sum(c.n_points for c in cases)
+    sample_ids = ensemble_sample(cases)
+    barrier(world)
+    fp64 = run_batch(cases, "fp64", args, local, sample_ids)
+    mixed = run_batch(cases, "mixed", args, local, sample_ids)
+    barrier(world)
+    total_ms = sum(mixed["step_ms"])
+    total_ms_max = max_over_ranks(total_ms, world)
+    points_all = sum_over_ranks(float(n), world)
+    value = points_all * args.steps / (total_ms_max * 1e-3)
+    fp64_value = n * args.steps / (sum(fp64["step_ms"]) * 1e-3)
+    # the mixed form's error against FP64 after the same steps, per field
+    errs = {f: 0.0 for f in ("x", "x_t", "T")}
+    for i in sample_ids:
+        for f in errs:
+            errs[f] = max(errs[f], rel_err(mixed["fields"][i][f], fp64["fields"][i][f], field_floor(cases[i], f)))
+    active_ratio = mixed["active"] / max(1, n)
+    roof = roofline(n, mixed["prof_steps"], mixed["prof"], active_ratio, True)
+    plain_value, plain_ms = plain_fp64(cases, args.plain_steps, local) if not args.no_plain else (None, None)
+    e2e = (run_e2e_batch(cases, args.steps, local, mixed["cap"], mixed["sort_interval"])
+           if rank == 0 and not args.no_e2e else None)
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        try:
+            cpu = cpu_ensemble_sample(cases, args.ref_steps)
+        except Exception as exc:  # the oracle build may be absent
+            cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": f"unavailable: {exc}"}
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": total_ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32+f64", "data": f"synthetic (mpm_3d_b200.inputs.block_drop_ensemble, seed {ENSEMBLE_SEED}+rank)",
+        "config": {"workload": f"ensemble{ENSEMBLE_JOBS}", "jobs": len(cases), "points": n,
+                   "grids": "N^3, N log-uniform in [16,96]", "form": "mixed (FP32 points, FP64 nodal sums)",
+                   "points_per_item": mixed["cap"], "sort_interval": mixed["sort_interval"], "graph": True,
+                   "parallelism": f"independent{world}",
+                   "l2": "inputs larger than L2", "active_nodes_per_point": round(active_ratio, 4)},
+        "batched_fp64": {"value": fp64_value, "unit": UNIT, "points_per_item": fp64["cap"],
+                         "sort_interval": fp64["sort_interval"]},
+        "plain_fp64": {"value": plain_value, "unit": UNIT, "steps_per_job": args.plain_steps,
+                       "how": "one mpmgpu_handle per job, jobs in sequence, CUDA events around each job's steps"},
+        "vs_plain_fp64": (value / plain_value) if plain_value else None,
+        "mixed_rel_err_vs_fp64": {**errs, "jobs_compared": len(sample_ids), "after_steps": mixed["steps_done"]},
+        "roofline": roof,
+        "stage_ms_per_step": {k: v[1] / mixed["prof_steps"] for k, v in mixed["prof"].items()},
+        "gpu_launches": mixed["launches"],
+        "clocks": mixed["clocks"],
+        "e2e": e2e,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_e2e_batch(cases, steps: int, device: int, cap: int, sort_interval: int):
+    """The ensemble through the C ABI from host buffers: batch creation and
+    upload of every job, `steps` steps, download of every point's x, x_t and
+    stress, teardown, all on the wall clock."""
+    import torch
+
+    from mpm_3d_b200.native import GPUBatch
+
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    b = GPUBatch(dim=3, mode="mixed", device=device, points_per_item=cap, sort_interval=sort_interval)
+    jobs = [b.add(c) for c in cases]
+    b.step(steps)
+    d2h = 0
+    for j in jobs:
+        for f in ("x", "x_t", "T"):
+            d2h += b.points(j, 0, f).nbytes
+    b.close()
+    dt = time.perf_counter() - t0
+    n = sum(c.n_points for c in cases)
+    h2d = sum(b_.n * (8 + 8 + 24 + 24 + 4) for c in cases for b_ in c.bodies)
+    return {"value": n * steps / dt, "unit": UNIT, "h2d_bytes_per_step": h2d // steps, "d2h_bytes_per_step": d2h // steps,
+            "steps": steps, "seconds": dt}
+
+
+def cpu_ensemble_sample(cases, steps: int):
+    """The reference's ThreadPoolExplicitUSL on 16 of the jobs (every 32nd),
+    one after another, `steps` steps each after one warm-up step."""
+    threads = os.cpu_count() or 1
+    ids = list(range(0, len(cases), max(1, len(cases) // 16)))[:16]
+    pts = 0
+    sec = 0.0
+    for i in ids:
+        dt = cpu_reference_run(cases[i], steps, 1, threads)
+        sec += dt * steps
+        pts += cases[i].n_points * steps
+    return {"value": pts / sec, "unit": UNIT, "cores": threads, "kind": "reference",
+            "sample": f"jobs {ids[0]}..{ids[-1]} step {ids[1] - ids[0] if len(ids) > 1 else 1} "
+                      f"({len(ids)} jobs, {sum(cases[i].n_points for i in ids)} points), {steps} steps each after 1 "
+                      f"warm-up, in sequence, ThreadPoolExplicitUSL+ThreadPoolPoints, threads={threads}"}
+
+
+def run_e2e(case, steps: int, device: int, form: str = "fp64"):
     """Same metric through the C ABI from host buffers: create + upload,
     `steps` steps, download of every point's x, x_t and stress, destroy."""
     import torch
@@ -337,7 +549,7 @@ def run_e2e(case, steps: int, device: int):
 
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    sim = GPUExplicitUSL(case, device=device)
+    sim = GPUExplicitUSL(case, device=device, mode=form)
     sim.step(steps)
     outs = []
     for b in range(len(case.bodies)):
@@ -358,7 +570,10 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=0, help="timed steps (default: the workload's own step count)")
     ap.add_argument("--warmup", type=int, default=10)
-    ap.add_argument("--workload", default="collision", choices=["collision", "column"])
+    ap.add_argument("--workload", default="ensemble", choices=["ensemble", "collision", "column"])
+    ap.add_argument("--form", default="fp64", choices=["fp64", "mixed"], help="form of the single-job workloads")
+    ap.add_argument("--plain-steps", type=int, default=10, help="timed steps per job of the plain FP64 path")
+    ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--ref-steps", type=int, default=4, help="steps of the CPU reference sample")
     ap.add_argument("--no-cpu", action="store_true")
@@ -367,13 +582,15 @@ def main():
     if args.warmup < 3:
         args.warmup = 3
     if args.steps <= 0:
-        args.steps = make_workload(args.workload).steps
+        args.steps = 100 if args.workload == "ensemble" else make_workload(args.workload).steps
     rank, world, local = dist_setup(args.gpus)
     try:
         if args.impl == "reference":
             run_reference_arm(args, rank, world)
+        elif args.workload == "ensemble":
+            run_ensemble(args, rank, world, local)
         else:
-            run_ours(args, rank, world, local)
+            run_single(args, rank, world, local)
     finally:
         if world > 1:
             import torch.distributed as dist

@@ -299,11 +299,14 @@ mpmgpu_status mpmgpu_batch_remove_job(mpmgpu_batch* b, int job);
 /* Jobs and points still stepping, and device bytes held by the batch. */
 mpmgpu_status mpmgpu_batch_counts(const mpmgpu_batch* b, int* live_jobs, int64_t* live_points, int64_t* bytes_in_use);
 
-/* Times `steps` steps of the current jobs for every available
- * points-per-item choice (restoring the state after each trial) and keeps
- * the fastest; the jobs' state after the call is the state before it. */
+/* Tunes the launch shape on the current jobs: times `steps` steps for every
+ * available points-per-item choice, then 32 steps for each re-binning
+ * interval (4, 8, 16, 32), restoring the jobs' state after each trial, and
+ * keeps the fastest of each. The jobs' state after the call is the state
+ * before it. */
 mpmgpu_status mpmgpu_batch_autotune(mpmgpu_batch* b, int steps, int* points_per_item);
 int mpmgpu_batch_points_per_item(const mpmgpu_batch* b);
+int mpmgpu_batch_sort_interval(const mpmgpu_batch* b);
 
 /* As mpmgpu_active_nodes, over every job of the batch. */
 mpmgpu_status mpmgpu_batch_active_nodes(mpmgpu_batch* b, int64_t* nodes, int64_t* drifted);

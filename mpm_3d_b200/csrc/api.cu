@@ -376,6 +376,8 @@ mpmgpu_status mpmgpu_batch_profile_read(mpmgpu_batch* b, int stage, int64_t* lau
 
 int mpmgpu_batch_points_per_item(const mpmgpu_batch* b) { return b ? b->b->points_per_item() : 0; }
 
+int mpmgpu_batch_sort_interval(const mpmgpu_batch* b) { return b ? b->b->sort_interval() : 0; }
+
 mpmgpu_status mpmgpu_batch_active_nodes(mpmgpu_batch* b, int64_t* nodes, int64_t* drifted) {
   if (!b) return MPMGPU_ERR_ARG;
   return b->b->active_nodes(nodes, drifted);

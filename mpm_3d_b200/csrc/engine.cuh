@@ -178,6 +178,7 @@ class BatchBase {
   virtual int64_t memory_in_use() const = 0;
   virtual void counts(int* live_jobs, int64_t* live_points) const = 0;
   virtual int points_per_item() const = 0;
+  virtual int sort_interval() const = 0;
   virtual mpmgpu_status active_nodes(int64_t* nodes, int64_t* drifted) = 0;
   // FP64 map export support (single-job handle)
   virtual mpmgpu_status body_points_fp64(int job, int body, PointsDev* P, Geom* g, int* cpdi) = 0;
@@ -319,6 +320,11 @@ class Batch : public BatchBase {
       };
       for (int d = 0; d < D; d++) {
         col(desc.x, 3, d);
+        if constexpr (sizeof(PT) == 4) {
+          // the mixed form stores x0 = x - u and uses x = x0 + u
+          if (desc.u)
+            for (int64_t i = 0; i < n; i++) tmp[(size_t)i] = (PT)(desc.x[3 * i + d] - desc.u[3 * i + d]);
+        }
         MPM_TRY(upload(B.P.x[d], tmp));
         col(desc.x_t, 3, d);
         MPM_TRY(upload(B.P.v[d], tmp));
@@ -543,7 +549,19 @@ class Batch : public BatchBase {
       return MPMGPU_OK;
     };
     switch (field) {
-      case MPMGPU_P_X: return vec3(B->P.x);
+      case MPMGPU_P_X:
+        if constexpr (sizeof(PT) == 4) {
+          // the mixed form keeps x0 in the x arrays: x = x0 + u (in FP32)
+          std::vector<PT> u;
+          for (int64_t i = 0; i < 3 * n; i++) out[i] = 0.0;
+          for (int d = 0; d < D; d++) {
+            MPM_TRY(download(tmp, B->P.x[d], (size_t)n));
+            MPM_TRY(download(u, B->P.u[d], (size_t)n));
+            for (int64_t i = 0; i < n; i++) out[3 * (int64_t)pid[(size_t)i] + d] = (double)(tmp[(size_t)i] + u[(size_t)i]);
+          }
+          return MPMGPU_OK;
+        }
+        return vec3(B->P.x);
       case MPMGPU_P_U: return vec3(B->P.u);
       case MPMGPU_P_X_T: return vec3(B->P.v);
       case MPMGPU_P_MX_T: {
@@ -693,44 +711,69 @@ class Batch : public BatchBase {
 
   // ---- autotuning ----
 
-  // Times `steps` steps of the current jobs with every available
-  // points-per-item choice, restoring the state after each trial, and keeps
-  // the fastest. The simulation state after the call is the state before it.
+  // Tunes the launch shape on the current jobs, restoring their state after
+  // every trial (the state after the call is the state before it): first
+  // the points per work item (each available choice timed over `steps`
+  // steps), then the re-binning interval (4, 8, 16, 32 steps, each timed
+  // over 32 steps with its re-binnings), keeping the fastest of each.
   mpmgpu_status autotune(int steps, int* best_cap) override {
     if (steps < 1) return fail(MPMGPU_ERR_ARG, "autotune needs at least one step");
     MPM_TRY(commit());
     if (live_jobs_ == 0) return fail(MPMGPU_ERR_STATE, "no jobs to tune on");
     MPM_TRY(snapshot_save());
-    const int caps[3] = {256, 512, 1024};
-    const int original = cap_;
-    int best = original;
-    float best_ms = 1e30f;
+    const int original_cap = cap_, original_si = sort_interval_;
     cudaEvent_t e0, e1;
     MPM_CUDA_TRY(cudaEventCreate(&e0));
     MPM_CUDA_TRY(cudaEventCreate(&e1));
+    // one trial: re-bin, 2 warm-up steps, `n` timed steps re-binning every
+    // `si` steps; the state is restored afterwards
+    auto trial = [&](int n, int si, float* ms) -> mpmgpu_status {
+      drop_graphs();
+      MPM_TRY(launch_sort());   // work items depend on the item size
+      for (int w = 0; w < 2; w++) MPM_TRY(launch_step());
+      cudaEventRecord(e0, stream_);
+      int since = 0;
+      for (int k = 0; k < n; k++) {
+        MPM_TRY(launch_step());
+        if (++since >= si) {
+          MPM_TRY(launch_sort());
+          since = 0;
+        }
+      }
+      cudaEventRecord(e1, stream_);
+      if (cudaEventSynchronize(e1) != cudaSuccess) return fail(MPMGPU_ERR_CUDA, "autotune timing failed");
+      cudaEventElapsedTime(ms, e0, e1);
+      return snapshot_restore();
+    };
     mpmgpu_status st = MPMGPU_OK;
+    int best_c = original_cap, best_si = original_si;
+    float best_ms = 1e30f;
+    const int caps[3] = {256, 512, 1024};
     for (int ci = 0; ci < 3 && st == MPMGPU_OK; ci++) {
       if (!cap_available(dim_, mixed(), caps[ci])) continue;
       cap_ = caps[ci];
-      drop_graphs();
-      st = launch_sort();   // work items depend on the item size
-      for (int w = 0; w < 2 && st == MPMGPU_OK; w++) st = launch_step();
-      if (st != MPMGPU_OK) break;
-      cudaEventRecord(e0, stream_);
-      for (int s = 0; s < steps && st == MPMGPU_OK; s++) st = launch_step();
-      cudaEventRecord(e1, stream_);
-      if (cudaEventSynchronize(e1) != cudaSuccess) st = fail(MPMGPU_ERR_CUDA, "autotune timing failed");
       float ms = 0.0f;
-      cudaEventElapsedTime(&ms, e0, e1);
+      st = trial(steps, 1 << 30, &ms);
       if (st == MPMGPU_OK && ms < best_ms) {
         best_ms = ms;
-        best = caps[ci];
+        best_c = caps[ci];
       }
-      if (st == MPMGPU_OK) st = snapshot_restore();
+    }
+    cap_ = best_c;
+    best_ms = 1e30f;
+    const int intervals[4] = {4, 8, 16, 32};
+    for (int k = 0; k < 4 && st == MPMGPU_OK; k++) {
+      float ms = 0.0f;
+      st = trial(32, intervals[k], &ms);
+      if (st == MPMGPU_OK && ms < best_ms) {
+        best_ms = ms;
+        best_si = intervals[k];
+      }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    cap_ = (st == MPMGPU_OK) ? best : original;
+    cap_ = (st == MPMGPU_OK) ? best_c : original_cap;
+    sort_interval_ = (st == MPMGPU_OK) ? best_si : original_si;
     drop_graphs();
     snapshot_free();
     MPM_TRY(st);
@@ -738,6 +781,8 @@ class Batch : public BatchBase {
     if (best_cap) *best_cap = cap_;
     return MPMGPU_OK;
   }
+
+  int sort_interval() const override { return sort_interval_; }
 
  private:
   // ---- allocation helpers ----

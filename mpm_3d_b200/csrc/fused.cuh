@@ -126,15 +126,24 @@ __host__ __device__ constexpr size_t fused_smem_bytes() {
 #endif
 constexpr int kFusedThreads = MPMB200_FUSED_THREADS;
 
+// Entry k (0..2) of a 3-array without indexing it by a variable (which
+// would move the array to local memory).
+template <typename R>
+__device__ __forceinline__ R sel3(const R* a, int k) {
+  return k == 0 ? a[0] : (k == 1 ? a[1] : a[2]);
+}
+
 // Visits the window nodes of a point map: f(k0, k1, k2). Spans are 2 or 3
-// per axis; the first two offsets of every axis are unconditional.
+// per axis; the first two offsets of every axis are unconditional. Only the
+// innermost axis is unrolled: the general windows are the rarer path, and a
+// fully unrolled 3x3x3 visit inflates the kernel's instruction footprint.
 template <int DIM, typename R, typename F>
 __device__ __forceinline__ void for_window(const PointMapT<R>& pm, F&& f) {
   constexpr int K2 = DIM == 3 ? 3 : 1;
-#pragma unroll
+#pragma unroll 1
   for (int k2 = 0; k2 < K2; k2++) {
     if (DIM == 3 && k2 == 2 && pm.ax[2].span < 3) break;
-#pragma unroll
+#pragma unroll 1
     for (int k1 = 0; k1 < 3; k1++) {
       if (k1 == 2 && pm.ax[1].span < 3) break;
 #pragma unroll
@@ -213,7 +222,8 @@ __device__ __forceinline__ GatherSum<R> gather_regular(const PointMapT<R>& pm, c
 // Gather over any window (three-node spans, nodes outside the tile).
 template <int DIM, int T, int TN, typename PT, typename R>
 __device__ __forceinline__ GatherSum<R> gather_general(const BodyCtx<PT>& c, unsigned long long* drift,
-                                                       const PointMapT<R>& pm, const int* o, const R* tvel) {
+                                                       const PointMapT<R>& pm, const int* o, const R* tvel,
+                                                       const double* vref) {
   GatherSum<R> gs;
   const Geom& g = c.g;
   const bool in_tile = window_in_tile<DIM>(pm, o, T);
@@ -221,14 +231,15 @@ __device__ __forceinline__ GatherSum<R> gather_general(const BodyCtx<PT>& c, uns
   const int t0 = (pm.ax[0].base - o[0]) + T * ((pm.ax[1].base - o[1]) + (DIM == 3 ? T * (pm.ax[2].base - o[2]) : 0));
   const R sS = pm.sS, sG = pm.sG;
   for_window<DIM>(pm, [&](int k0, int k1, int k2) {
-    const R wz = DIM == 3 ? pm.ax[2].W[k2] : R(1);
-    const R gz = DIM == 3 ? pm.ax[2].G[k2] : R(0);
-    const R W12 = pm.ax[1].W[k1] * wz;
+    const R wz = DIM == 3 ? sel3(pm.ax[2].W, k2) : R(1);
+    const R gz = DIM == 3 ? sel3(pm.ax[2].G, k2) : R(0);
+    const R w1 = sel3(pm.ax[1].W, k1), g1 = sel3(pm.ax[1].G, k1);
+    const R W12 = w1 * wz;
     const R S = sS * pm.ax[0].W[k0] * W12;
     const R gr0 = sG * pm.ax[0].G[k0] * W12;
     const R gw0 = sG * pm.ax[0].W[k0];
-    const R gr1 = gw0 * (pm.ax[1].G[k1] * wz);
-    const R gr2 = gw0 * (pm.ax[1].W[k1] * gz);
+    const R gr1 = gw0 * (g1 * wz);
+    const R gr2 = gw0 * (w1 * gz);
     R vt[3] = {R(0), R(0), R(0)}, dv[3] = {R(0), R(0), R(0)};
     if (in_tile) {
       const int t = t0 + k0 + T * (k1 + T * k2);
@@ -241,7 +252,7 @@ __device__ __forceinline__ GatherSum<R> gather_general(const BodyCtx<PT>& c, uns
       const int64_t s = node_slot(g, pm.ax[0].base + k0, pm.ax[1].base + k1, DIM == 3 ? pm.ax[2].base + k2 : 0);
 #pragma unroll
       for (int d = 0; d < DIM; d++) {
-        vt[d] = (R)c.V.vt[d][s];
+        vt[d] = (R)(c.V.vt[d][s] - vref[d]);
         dv[d] = (R)c.V.dv[d][s];
       }
     }
@@ -257,18 +268,39 @@ __device__ __forceinline__ GatherSum<R> gather_general(const BodyCtx<PT>& c, uns
   return gs;
 }
 
+// Position of a staged point. The FP64 form stores x and updates it as the
+// reference does (x += S^T u). The mixed form stores the initial position
+// x0 in the x arrays and derives x = x0 + u from the displacement u, which
+// the reference updates by the same increment (explicit_usl.cpp:279-280),
+// so x0 + u is x in exact arithmetic; in FP32 it avoids accumulating a
+// rounding of x at every step (x is large next to its increments, u is
+// not), and x0 is never written.
+template <typename PT, int ROW>
+__device__ __forceinline__ PT staged_pos(const PT* sp, int d) {
+  if constexpr (sizeof(PT) == 8) return sp[(kFx + d) * ROW];
+  else return sp[(kFx + d) * ROW] + sp[(kFu + d) * ROW];
+}
+
 // Phase 1 for one point: gather, movePoints / calculateStrainRate /
 // updateDensity / updateStress (explicit_usl.cpp:266-355). `sp` points at the
 // point's column in the staged arrays (stride ROW).
+//
+// The staged nodal velocities are relative to `vref` (zero in the FP64
+// form; in the mixed form the velocity of the work item's first point,
+// subtracted in FP64 before the conversion to FP32). Since the shape
+// functions sum to one and their gradients to zero, S^T v = vref +
+// S^T (v - vref) and the velocity gradient is that of v - vref: the same
+// values in exact arithmetic, without the cancellation of a common
+// translation against the velocity differences in FP32.
 template <int DIM, int T, int TN, int ROW, typename PT>
 __device__ __forceinline__ void gather_update(const BodyCtx<PT>& c, int* err, unsigned long long* drift, int64_t p,
-                                              PT* sp, const int* o, const PT* tvel) {
+                                              PT* sp, const int* o, const PT* tvel, const double* vref) {
   using R = PT;
   const PointsT<PT>& P = c.P;
   const R dt = (R)c.sp.dt;
   R x[3] = {R(0), R(0), R(0)};
 #pragma unroll
-  for (int d = 0; d < DIM; d++) x[d] = sp[(kFx + d) * ROW];
+  for (int d = 0; d < DIM; d++) x[d] = staged_pos<PT, ROW>(sp, d);
   PointMapT<R> pm;
   const int st = build_map<DIM>(c.g, c.mc, c.sp.cpdi, x, sp[kFext * ROW], pm, err);
   GatherSum<R> gs;
@@ -276,20 +308,28 @@ __device__ __forceinline__ void gather_update(const BodyCtx<PT>& c, int* err, un
     if (regular_window<DIM>(pm, o, T))
       gs = gather_regular<DIM, T, TN>(pm, o, tvel);
     else
-      gs = gather_general<DIM, T, TN>(c, drift, pm, o, tvel);
+      gs = gather_general<DIM, T, TN>(c, drift, pm, o, tvel, vref);
+    if constexpr (sizeof(PT) == 4) {
+#pragma unroll
+      for (int d = 0; d < DIM; d++) gs.du[d] += (R)vref[d];
+    }
   }
   // movePoints: u_node = dt * x_t_node; x += S^T u, u += S^T u,
   // x_t += S^T diff_x_t (explicit_usl.cpp:279-292)
 #pragma unroll
   for (int d = 0; d < DIM; d++) {
     const R dx = dt * gs.du[d];
-    const R xn = x[d] + dx;
     const R vn = sp[(kFv + d) * ROW] + gs.dv[d];
-    sp[(kFx + d) * ROW] = xn;
+    const R un = sp[(kFu + d) * ROW] + dx;
+    if constexpr (sizeof(PT) == 8) {
+      const R xn = x[d] + dx;
+      sp[(kFx + d) * ROW] = xn;
+      P.x[d][p] = xn;
+    }
     sp[(kFv + d) * ROW] = vn;
-    P.x[d][p] = xn;
+    sp[(kFu + d) * ROW] = un;
     P.v[d][p] = vn;
-    P.u[d][p] = sp[(kFu + d) * ROW] + dx;
+    P.u[d][p] = un;
   }
   const R vol = sp[kFvol * ROW] * exp(dt * (gs.L[0][0] + gs.L[1][1] + gs.L[2][2]));
   sp[kFvol * ROW] = vol;
@@ -409,12 +449,13 @@ __device__ __forceinline__ void scatter_general(const BodyCtx<PT>& c, unsigned l
   const int t0 = (pm.ax[0].base - o[0]) + T * ((pm.ax[1].base - o[1]) + (DIM == 3 ? T * (pm.ax[2].base - o[2]) : 0));
   const R sS = pm.sS, sG = pm.sG;
   for_window<DIM>(pm, [&](int k0, int k1, int k2) {
-    const R wz = DIM == 3 ? pm.ax[2].W[k2] : R(1);
-    const R gz = DIM == 3 ? pm.ax[2].G[k2] : R(0);
-    const R W12 = pm.ax[1].W[k1] * wz;
+    const R wz = DIM == 3 ? sel3(pm.ax[2].W, k2) : R(1);
+    const R gz = DIM == 3 ? sel3(pm.ax[2].G, k2) : R(0);
+    const R w1 = sel3(pm.ax[1].W, k1), g1 = sel3(pm.ax[1].G, k1);
+    const R W12 = w1 * wz;
     const R S = sS * pm.ax[0].W[k0] * W12;
     const R gw0 = sG * pm.ax[0].W[k0];
-    const R gr[3] = {sG * pm.ax[0].G[k0] * W12, gw0 * (pm.ax[1].G[k1] * wz), gw0 * (pm.ax[1].W[k1] * gz)};
+    const R gr[3] = {sG * pm.ax[0].G[k0] * W12, gw0 * (g1 * wz), gw0 * (w1 * gz)};
     NodeVals<DIM, NORMAL, R> nv;
     nv.v[0] = S * q.m;
 #pragma unroll
@@ -451,7 +492,7 @@ __device__ __forceinline__ void map_scatter(const BodyCtx<PT>& c, int* err, unsi
   using R = PT;
   R x[3] = {R(0), R(0), R(0)};
 #pragma unroll
-  for (int d = 0; d < DIM; d++) x[d] = sp[(kFx + d) * ROW];
+  for (int d = 0; d < DIM; d++) x[d] = staged_pos<PT, ROW>(sp, d);
   PointMapT<R> pm;
   const int st = build_map<DIM>(c.g, c.mc, c.sp.cpdi, x, sp[kFext * ROW], pm, err);
   if (st < 0) {
@@ -499,7 +540,13 @@ __global__ void __launch_bounds__(MPMB200_FUSED_THREADS, MPMB200_FUSED_MIN_CTAS)
   PT* pts = reinterpret_cast<PT*>(smem + off_pts<PT, CAP>());
   int32_t* act = reinterpret_cast<int32_t*>(smem + off_act<PT, CAP>());
   double* tile = reinterpret_cast<double*>(smem + off_tile<PT, CAP>());  // phase 2: NACC FP64 values
-  PT* tvel = reinterpret_cast<PT*>(tile);                                 // phase 1: vt0..2 dv0..2
+  // phase 1: nodal vt0..2 dv0..2 as loaded (FP64), and in the point
+  // precision relative to the reference velocity (the same array in the
+  // FP64 form; behind the FP64 copy in the mixed form)
+  double* tv64 = tile;
+  PT* tvel = sizeof(PT) == 8 ? reinterpret_cast<PT*>(tile) : reinterpret_cast<PT*>(tile + 6 * TN);
+  static_assert(sizeof(PT) == 8 || 6 * TN * (sizeof(double) + sizeof(PT)) <= 10 * TN * sizeof(double),
+                "the mixed form's velocity tiles fit in the accumulation tile");
   uint8_t* touched = reinterpret_cast<uint8_t*>(tile + 10 * TN);
 
   if (threadIdx.x == 0) {
@@ -590,8 +637,8 @@ __global__ void __launch_bounds__(MPMB200_FUSED_THREADS, MPMB200_FUSED_MIN_CTAS)
         const int64_t s = node_slot(g, i, j, k);
 #pragma unroll
         for (int d = 0; d < DIM; d++) {
-          tvel[d * TN + t] = (PT)c.V.vt[d][s];
-          tvel[(3 + d) * TN + t] = (PT)c.V.dv[d][s];
+          tv64[d * TN + t] = c.V.vt[d][s];
+          tv64[(3 + d) * TN + t] = c.V.dv[d][s];
         }
       }
     }
@@ -602,6 +649,23 @@ __global__ void __launch_bounds__(MPMB200_FUSED_THREADS, MPMB200_FUSED_MIN_CTAS)
       return;
     }
     parity ^= 1u;
+    double vref[3] = {0.0, 0.0, 0.0};
+    if constexpr (sizeof(PT) == 4) {
+      if (do_g2p) {
+        // reference velocity: the item's first point (any value is exact;
+        // one close to the item's velocities keeps the differences small)
+#pragma unroll
+        for (int d = 0; d < DIM; d++) vref[d] = (double)pts[(kFv + d) * ROW + offp];
+        for (int t = threadIdx.x; t < TN; t += blockDim.x) {
+#pragma unroll
+          for (int d = 0; d < DIM; d++) {
+            tvel[d * TN + t] = (PT)(tv64[d * TN + t] - vref[d]);
+            tvel[(3 + d) * TN + t] = (PT)tv64[(3 + d) * TN + t];
+          }
+        }
+        __syncthreads();
+      }
+    }
     if (do_g2p) {
       for (int j = threadIdx.x; j < n; j += blockDim.x) {
         const int64_t p = pstart + j;
@@ -613,7 +677,7 @@ __global__ void __launch_bounds__(MPMB200_FUSED_THREADS, MPMB200_FUSED_MIN_CTAS)
           act[off4 + j] = 0;
           continue;
         }
-        gather_update<DIM, T, TN, ROW>(c, fl.err, fl.drift, p, pts + offp + j, o, tvel);
+        gather_update<DIM, T, TN, ROW>(c, fl.err, fl.drift, p, pts + offp + j, o, tvel, vref);
       }
       __syncthreads();
     }

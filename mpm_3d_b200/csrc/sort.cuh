@@ -111,7 +111,11 @@ __global__ void k_sort_count(const BatchHdr* hdr, const BodyCtx<PT>* bodies, con
     } else {
       PT xp[3] = {PT(0), PT(0), PT(0)};
 #pragma unroll
-      for (int d = 0; d < DIM; d++) xp[d] = B.P.x[d][p];
+      for (int d = 0; d < DIM; d++) {
+        // the mixed form keeps x0 in the x arrays and x = x0 + u
+        if constexpr (sizeof(PT) == 8) xp[d] = B.P.x[d][p];
+        else xp[d] = B.P.x[d][p] + B.P.u[d][p];
+      }
       int c[3] = {0, 0, 0};
       point_cell<DIM>(B.g, xp, c);
       int b, l;

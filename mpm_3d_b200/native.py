@@ -109,6 +109,7 @@ def load() -> ctypes.CDLL:
     lib.mpmgpu_batch_counts.argtypes = [vp, ctypes.POINTER(ctypes.c_int), i64p, i64p]
     lib.mpmgpu_batch_autotune.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
     lib.mpmgpu_batch_points_per_item.argtypes = [vp]
+    lib.mpmgpu_batch_sort_interval.argtypes = [vp]
     lib.mpmgpu_batch_active_nodes.argtypes = [vp, i64p, i64p]
     lib.mpmgpu_active_nodes.argtypes = [vp, i64p, i64p]
     lib.mpmgpu_batch_profile.argtypes = [vp, ctypes.c_int]
@@ -396,6 +397,9 @@ class GPUBatch:
 
     def points_per_item(self) -> int:
         return int(self.lib.mpmgpu_batch_points_per_item(self.h))
+
+    def sort_interval(self) -> int:
+        return int(self.lib.mpmgpu_batch_sort_interval(self.h))
 
     def active_nodes(self) -> Tuple[int, int]:
         """(nodes with mass in the last step, per body; drifted point visits)."""
