@@ -321,6 +321,49 @@ void* mpmgpu_batch_stream(const mpmgpu_batch* b);
 int64_t mpmgpu_batch_launch_count(const mpmgpu_batch* b);
 mpmgpu_status mpmgpu_batch_destroy(mpmgpu_batch* b);
 
+/* ------------------------------------------------------------------------
+ * Server: continuous batching of simulation requests.
+ *
+ * No counterpart in the reference. A server owns one batch and a device
+ * memory budget. mpmgpu_server_submit admits a request (one job) at once if
+ * its footprint (mpmgpu_batch_footprint) fits the budget left by the
+ * requests still running, or while nothing runs; otherwise it returns
+ * MPMGPU_ERR_STATE and the caller keeps the request queued and retries
+ * after the next advance. Admitted requests join the running batch at the
+ * next step boundary and step together with it; a request that has run its
+ * steps has its final point state (x, u, x_t, T, v, active) copied to host
+ * memory and its device memory released. Each request computes what it
+ * would compute alone (up to the order of the nodal sums).
+ * ---------------------------------------------------------------------- */
+
+typedef struct mpmgpu_server mpmgpu_server;
+
+mpmgpu_status mpmgpu_server_create(const mpmgpu_batch_config* cfg, int64_t budget_bytes, mpmgpu_server** out);
+const char* mpmgpu_server_last_error(const mpmgpu_server* s);
+/* Device bytes the request will reserve from the budget while it runs. */
+mpmgpu_status mpmgpu_server_footprint(const mpmgpu_server* s, const mpmgpu_job_desc* job, int64_t* bytes);
+mpmgpu_status mpmgpu_server_submit(mpmgpu_server* s, const mpmgpu_job_desc* job, int* request_id);
+/* `steps` steps of every running request, then collection of the finished
+ * ones (synchronises when a request finishes). */
+mpmgpu_status mpmgpu_server_advance(mpmgpu_server* s, int steps);
+/* Ids of requests finished since the last poll (at most max_ids); returns
+ * their number. */
+int mpmgpu_server_poll(mpmgpu_server* s, int* ids, int max_ids);
+/* State (1 running, 2 finished, 3 released), admission and completion
+ * times on mpmgpu_server_clock, points and steps of a request. */
+mpmgpu_status mpmgpu_server_request(const mpmgpu_server* s, int id, int* state, double* t_admit, double* t_done,
+                                    int64_t* points, int64_t* steps);
+/* A finished request's final point field (MPMGPU_P_X, _U, _X_T, _T, _V or
+ * _ACTIVE) of one body, in the layout of mpmgpu_download_points. */
+mpmgpu_status mpmgpu_server_result(mpmgpu_server* s, int id, int body, int field, double* out);
+/* Frees a finished request's host copy of its results. */
+mpmgpu_status mpmgpu_server_release(mpmgpu_server* s, int id);
+mpmgpu_status mpmgpu_server_stats(const mpmgpu_server* s, int* running, int64_t* reserved_bytes, int64_t* live_points,
+                                  int64_t* particle_steps_done);
+/* Seconds since the server was created (steady clock). */
+double mpmgpu_server_clock(const mpmgpu_server* s);
+mpmgpu_status mpmgpu_server_destroy(mpmgpu_server* s);
+
 #ifdef __cplusplus
 }
 #endif

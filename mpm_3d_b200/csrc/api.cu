@@ -11,6 +11,7 @@
 
 #include "../../include/mpm_b200.h"
 #include "engine.cuh"
+#include "server.cuh"
 
 using namespace mpmb200;
 
@@ -27,6 +28,10 @@ struct mpmgpu_batch {
   mpmgpu_batch_config cfg{};
   std::unique_ptr<BatchBase> b;
   std::string last_error;
+};
+
+struct mpmgpu_server {
+  std::unique_ptr<Server> s;
 };
 
 namespace {
@@ -389,6 +394,80 @@ int64_t mpmgpu_batch_launch_count(const mpmgpu_batch* b) { return b ? b->b->laun
 
 mpmgpu_status mpmgpu_batch_destroy(mpmgpu_batch* b) {
   delete b;
+  return MPMGPU_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Server
+// ---------------------------------------------------------------------------
+
+mpmgpu_status mpmgpu_server_create(const mpmgpu_batch_config* cfg, int64_t budget_bytes, mpmgpu_server** out) {
+  if (!cfg || !out || budget_bytes <= 0) return MPMGPU_ERR_ARG;
+  *out = nullptr;
+  if (cfg->dim != 2 && cfg->dim != 3) return MPMGPU_ERR_UNSUPPORTED;
+  if (cfg->mode != MPMGPU_MODE_FP64 && cfg->mode != MPMGPU_MODE_MIXED) return MPMGPU_ERR_UNSUPPORTED;
+  if (cfg->points_per_item != 0 && !cap_available(cfg->dim, cfg->mode == MPMGPU_MODE_MIXED, cfg->points_per_item))
+    return MPMGPU_ERR_UNSUPPORTED;
+  mpmgpu_status st = MPMGPU_OK;
+  std::string msg;
+  auto b = make_batch(cfg->dim, cfg->mode, cfg->device, cfg->sort_interval, cfg->points_per_item, !cfg->no_graph,
+                      cfg->keep_debug, &st, &msg);
+  if (st != MPMGPU_OK) return st;
+  auto srv = std::make_unique<mpmgpu_server>();
+  srv->s = std::make_unique<Server>(std::move(b), cfg->mode == MPMGPU_MODE_MIXED, cfg->keep_debug != 0, budget_bytes);
+  *out = srv.release();
+  return MPMGPU_OK;
+}
+
+const char* mpmgpu_server_last_error(const mpmgpu_server* s) { return s ? s->s->last_error.c_str() : ""; }
+
+mpmgpu_status mpmgpu_server_footprint(const mpmgpu_server* s, const mpmgpu_job_desc* job, int64_t* bytes) {
+  if (!s || !job || !bytes) return MPMGPU_ERR_ARG;
+  return s->s->footprint(*job, bytes);
+}
+
+mpmgpu_status mpmgpu_server_submit(mpmgpu_server* s, const mpmgpu_job_desc* job, int* request_id) {
+  if (!s || !job || !request_id) return MPMGPU_ERR_ARG;
+  return s->s->submit(*job, request_id);
+}
+
+mpmgpu_status mpmgpu_server_advance(mpmgpu_server* s, int steps) {
+  if (!s) return MPMGPU_ERR_ARG;
+  return s->s->advance(steps);
+}
+
+int mpmgpu_server_poll(mpmgpu_server* s, int* ids, int max_ids) {
+  if (!s || !ids || max_ids <= 0) return 0;
+  return s->s->poll(ids, max_ids);
+}
+
+mpmgpu_status mpmgpu_server_request(const mpmgpu_server* s, int id, int* state, double* t_admit, double* t_done,
+                                    int64_t* points, int64_t* steps) {
+  if (!s) return MPMGPU_ERR_ARG;
+  return s->s->request(id, state, t_admit, t_done, points, steps);
+}
+
+mpmgpu_status mpmgpu_server_result(mpmgpu_server* s, int id, int body, int field, double* out) {
+  if (!s) return MPMGPU_ERR_ARG;
+  return s->s->result(id, body, field, out);
+}
+
+mpmgpu_status mpmgpu_server_release(mpmgpu_server* s, int id) {
+  if (!s) return MPMGPU_ERR_ARG;
+  return s->s->release(id);
+}
+
+mpmgpu_status mpmgpu_server_stats(const mpmgpu_server* s, int* running, int64_t* reserved_bytes, int64_t* live_points,
+                                  int64_t* particle_steps_done) {
+  if (!s) return MPMGPU_ERR_ARG;
+  s->s->stats(running, reserved_bytes, live_points, particle_steps_done);
+  return MPMGPU_OK;
+}
+
+double mpmgpu_server_clock(const mpmgpu_server* s) { return s ? s->s->clock() : 0.0; }
+
+mpmgpu_status mpmgpu_server_destroy(mpmgpu_server* s) {
+  delete s;
   return MPMGPU_OK;
 }
 

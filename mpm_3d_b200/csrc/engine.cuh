@@ -213,6 +213,8 @@ class Batch : public BatchBase {
     double* force_out[kMaxContacts] = {};
     std::vector<void*> allocs;
     int64_t block_off = -1;
+    int slot = -1;           // stable index in the job table while stepped
+    bool fill_pending = false;  // its block range still maps to another slot
     int64_t steps_done = 0, steps_left = 0;
     bool admitted = false;   // asked to join
     bool in_tables = false;  // part of the stepped set
@@ -232,6 +234,19 @@ class Batch : public BatchBase {
     MPM_CUDA_TRY(cudaSetDevice(device_));
     MPM_CUDA_TRY(cudaDeviceGetAttribute(&sm_count_, cudaDevAttrMultiProcessorCount, device_));
     MPM_CUDA_TRY(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    MPM_CUDA_TRY(cudaStreamCreateWithFlags(&copy_stream_, cudaStreamNonBlocking));
+    MPM_CUDA_TRY(cudaEventCreateWithFlags(&upload_ev_, cudaEventDisableTiming));
+    {
+      // jobs' arrays come from a stream-ordered pool that keeps freed memory
+      // for the next job (no device-wide synchronisation per job)
+      cudaMemPoolProps props{};
+      props.allocType = cudaMemAllocationTypePinned;
+      props.location.type = cudaMemLocationTypeDevice;
+      props.location.id = device_;
+      MPM_CUDA_TRY(cudaMemPoolCreate(&pool_, &props));
+      uint64_t keep = UINT64_MAX;
+      MPM_CUDA_TRY(cudaMemPoolSetAttribute(pool_, cudaMemPoolAttrReleaseThreshold, &keep));
+    }
     if (cap_ == 0) cap_ = default_cap();
     if (!cap_available(dim_, mixed(), cap_))
       return fail(MPMGPU_ERR_ARG, "points_per_item " + std::to_string(cap_) + " not available for this form");
@@ -246,6 +261,7 @@ class Batch : public BatchBase {
 
   ~Batch() override {
     if (stream_) cudaStreamSynchronize(stream_);
+    if (copy_stream_) cudaStreamSynchronize(copy_stream_);
     drop_graphs();
     for (int s = 0; s < kStages; s++)
       for (auto& pr : pending_[s]) {
@@ -254,8 +270,13 @@ class Batch : public BatchBase {
       }
     for (cudaEvent_t e : event_pool_) cudaEventDestroy(e);
     for (auto& j : jobs_) free_job(j);
+    if (stream_) cudaStreamSynchronize(stream_);
     for (void* p : scratch_allocs_) cudaFree(p);
     for (void* p : cap_allocs_) cudaFree(p);
+    if (pool_) cudaMemPoolDestroy(pool_);
+    if (stage_) cudaFreeHost(stage_);
+    if (upload_ev_) cudaEventDestroy(upload_ev_);
+    if (copy_stream_) cudaStreamDestroy(copy_stream_);
     if (stream_) cudaStreamDestroy(stream_);
   }
 
@@ -311,6 +332,7 @@ class Batch : public BatchBase {
     const int64_t n = desc.n;
     HBody B;
     B.n = n;
+    MPM_TRY(stage_reserve((size_t)n * (18 * sizeof(PT) + 8) + 64 * 256));
     MPM_TRY(alloc_points(B.P, n, B.allocs, j->bytes));
     MPM_TRY(alloc_points(B.Palt, n, B.allocs, j->bytes));
     if (n > 0) {
@@ -373,6 +395,7 @@ class Batch : public BatchBase {
     }
     B.mat = make_material(desc.has_material, desc.E, desc.nu);
     B.has_boundary = desc.has_boundary;
+    MPM_TRY(finish_uploads());
     j->bodies.push_back(std::move(B));
     if (body) *body = (int)j->bodies.size() - 1;
     return MPMGPU_OK;
@@ -399,6 +422,7 @@ class Batch : public BatchBase {
       MPM_TRY(alloc_dev(&j->force_out[c], 3 * ns, j->allocs, j->bytes));
     }
     j->nc++;
+    MPM_TRY(finish_uploads());
     if (contact) *contact = c;
     return MPMGPU_OK;
   }
@@ -461,7 +485,6 @@ class Batch : public BatchBase {
 
   mpmgpu_status remove_job(int job) override {
     if (job < 0 || job >= (int)jobs_.size() || jobs_[(size_t)job].removed) return fail(MPMGPU_ERR_ARG, "no such job");
-    MPM_CUDA_TRY(cudaStreamSynchronize(stream_));
     HJob& j = jobs_[(size_t)job];
     if (j.in_tables) membership_dirty_ = true;
     j.finished = true;
@@ -470,7 +493,9 @@ class Batch : public BatchBase {
       // the next compaction must not see its blocks
       MPM_CUDA_TRY(cudaMemsetAsync(flags_ + j.block_off, 0, sizeof(uint32_t) * j.g.nblocks, stream_));
     }
-    MPM_CUDA_TRY(cudaStreamSynchronize(stream_));
+    // stream-ordered: the arrays return to the pool after the queued work;
+    // the job leaves the device tables at the next step boundary, before
+    // any later launch
     free_job(j);
     j.removed = true;
     return MPMGPU_OK;
@@ -802,13 +827,15 @@ class Batch : public BatchBase {
   }
 
   template <typename T>
+  // A job's array from the pool, zeroed, ordered on the copy stream (the
+  // compute stream waits for it in finish_uploads).
   mpmgpu_status alloc_dev(T** p, size_t count, std::vector<void*>& owner, int64_t& bytes) {
     void* q = nullptr;
     const size_t nb = std::max<size_t>(count * sizeof(T), 16);
-    cudaError_t e = cudaMalloc(&q, nb);
-    if (e != cudaSuccess) return fail(MPMGPU_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    cudaError_t e = cudaMallocFromPoolAsync(&q, nb, pool_, copy_stream_);
+    if (e != cudaSuccess) return fail(MPMGPU_ERR_NOMEM, std::string("cudaMallocFromPoolAsync: ") + cudaGetErrorString(e));
     owner.push_back(q);
-    e = cudaMemsetAsync(q, 0, nb, stream_);
+    e = cudaMemsetAsync(q, 0, nb, copy_stream_);
     if (e != cudaSuccess) return fail(MPMGPU_ERR_CUDA, std::string("cudaMemset: ") + cudaGetErrorString(e));
     *p = static_cast<T*>(q);
     bytes += (int64_t)nb;
@@ -838,21 +865,56 @@ class Batch : public BatchBase {
     return MPMGPU_OK;
   }
 
+  // Returns a job's arrays to the pool after the work already queued on the
+  // compute stream.
   void free_job(HJob& j) {
     for (auto& b : j.bodies) {
-      for (void* p : b.allocs) cudaFree(p);
+      for (void* p : b.allocs) cudaFreeAsync(p, stream_);
       b.allocs.clear();
     }
-    for (void* p : j.allocs) cudaFree(p);
+    for (void* p : j.allocs) cudaFreeAsync(p, stream_);
     j.allocs.clear();
     j.bytes = 0;
+  }
+
+  // Uploads go through a pinned staging buffer on the copy stream, so they
+  // overlap the steps already queued on the compute stream.
+  mpmgpu_status stage_reserve(size_t bytes) {
+    MPM_CUDA_TRY(cudaStreamSynchronize(copy_stream_));  // the staging buffer is free again
+    stage_used_ = 0;
+    if (bytes <= stage_cap_) return MPMGPU_OK;
+    if (stage_) cudaFreeHost(stage_);
+    stage_ = nullptr;
+    stage_cap_ = 0;
+    const size_t cap = std::max<size_t>(bytes, (size_t)64 << 20);
+    MPM_CUDA_TRY(cudaHostAlloc(&stage_, cap, cudaHostAllocDefault));
+    stage_cap_ = cap;
+    return MPMGPU_OK;
   }
 
   template <typename T>
   mpmgpu_status upload(T* dst, const std::vector<T>& src) {
     if (src.empty()) return MPMGPU_OK;
-    MPM_CUDA_TRY(cudaMemcpyAsync(dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice, stream_));
-    MPM_CUDA_TRY(cudaStreamSynchronize(stream_));
+    const size_t bytes = src.size() * sizeof(T);
+    if (stage_used_ + bytes > stage_cap_) {
+      // more than reserved: this copy goes through the pageable path
+      MPM_CUDA_TRY(cudaMemcpyAsync(dst, src.data(), bytes, cudaMemcpyHostToDevice, copy_stream_));
+      MPM_CUDA_TRY(cudaStreamSynchronize(copy_stream_));
+      return MPMGPU_OK;
+    }
+    unsigned char* h = static_cast<unsigned char*>(stage_) + stage_used_;
+    std::memcpy(h, src.data(), bytes);
+    stage_used_ += (bytes + 255) / 256 * 256;
+    MPM_CUDA_TRY(cudaMemcpyAsync(dst, h, bytes, cudaMemcpyHostToDevice, copy_stream_));
+    return MPMGPU_OK;
+  }
+
+  // Orders the compute stream after the allocations and copies queued on
+  // the copy stream, and waits for them (the staging buffer is reused).
+  mpmgpu_status finish_uploads() {
+    MPM_CUDA_TRY(cudaEventRecord(upload_ev_, copy_stream_));
+    MPM_CUDA_TRY(cudaStreamWaitEvent(stream_, upload_ev_, 0));
+    MPM_CUDA_TRY(cudaStreamSynchronize(copy_stream_));
     return MPMGPU_OK;
   }
 
@@ -983,19 +1045,29 @@ class Batch : public BatchBase {
         if (j.admitted && !j.finished && j.steps_left <= 0) j.finished = true;
         if (want && !j.in_tables) {
           j.block_off = block_alloc(j.g.nblocks);
+          if (!free_slots_.empty()) {
+            j.slot = free_slots_.back();
+            free_slots_.pop_back();
+          } else {
+            j.slot = next_slot_++;
+          }
+          j.fill_pending = true;
           j.in_tables = true;
         } else if (!want && j.in_tables) {
           j.in_tables = false;
           // its flags were set by its last scatter: clear them so no later
-          // compaction lists its blocks
+          // compaction lists its blocks (its stale block -> slot entries are
+          // then never read)
           MPM_CUDA_TRY(cudaMemsetAsync(flags_ + j.block_off, 0, sizeof(uint32_t) * j.g.nblocks, stream_));
           block_free(j.block_off, j.g.nblocks);
+          free_slots_.push_back(j.slot);
+          j.slot = -1;
           j.block_off = j.removed ? -1 : j.block_off;
         }
       }
     }
-    // table contents
-    std::vector<InstDev> insts;
+    // table contents (the job table by stable slot, unused slots empty)
+    std::vector<InstDev> insts((size_t)std::max(next_slot_, 1), InstDev{});
     std::vector<GridBody> gbodies;
     std::vector<BodyCtx<PT>> ctx;
     std::vector<int64_t> point_end, bin_end;
@@ -1019,7 +1091,7 @@ class Batch : public BatchBase {
         I.force_out[c] = j.force_out[c];
       }
       I.block_off = j.block_off;
-      insts.push_back(I);
+      insts[(size_t)j.slot] = I;
       for (auto& b : j.bodies) {
         GridBody G{};
         G.A = b.A;
@@ -1044,7 +1116,7 @@ class Batch : public BatchBase {
         c.point_off = points;
         c.bin_off = bins;
         c.cell_off = cells;
-        c.inst = (int)insts.size() - 1;
+        c.inst = j.slot;
         points += b.n;
         bins += j.bg.nbins + 1;
         cells += (int64_t)j.bg.nbins * j.bg.cells_per_bin + 1;
@@ -1068,7 +1140,7 @@ class Batch : public BatchBase {
     int64_t tmp_cap = old_blocks;
     MPM_TRY(grow(&was_active_, &tmp_cap, cap_blocks_, old_blocks));
     tmp_cap = old_blocks;
-    MPM_TRY(grow(&blk_inst_, &tmp_cap, cap_blocks_, 0));
+    MPM_TRY(grow(&blk_inst_, &tmp_cap, cap_blocks_, old_blocks));
     tmp_cap = old_blocks;
     MPM_TRY(grow(&list_, &tmp_cap, cap_blocks_, 0));
     MPM_TRY(grow(&key_, &cap_points_k_, std::max<int64_t>(points, 1), 0));
@@ -1090,10 +1162,15 @@ class Batch : public BatchBase {
     any_plain_ = any_normal_ = false;
     for (const auto& c : ctx) (c.needs_normal ? any_normal_ : any_plain_) = true;
     drop_graphs();   // one-body launches carry the table entries in their arguments
-    // block -> job slot map: rebuilt for the whole space (holes -1)
-    std::vector<int32_t> bi((size_t)cap_blocks_, -1);
-    for (size_t s = 0; s < insts.size(); s++)
-      for (int64_t k = 0; k < insts[s].g.nblocks; k++) bi[(size_t)(insts[s].block_off + k)] = (int32_t)s;
+    // block -> job slot map: only the ranges of joining jobs change
+    for (auto& j : jobs_) {
+      if (!j.in_tables || !j.fill_pending) continue;
+      const int64_t nbk = j.g.nblocks;
+      k_fill_i32<<<(int)std::min<int64_t>((nbk + 255) / 256, 4096), 256, 0, stream_>>>(blk_inst_ + j.block_off, nbk,
+                                                                                        j.slot);
+      MPM_TRY(check_launch("k_fill_i32"));
+      j.fill_pending = false;
+    }
     BatchHdr hdr{};
     hdr.points = points;
     hdr.bins = bins;
@@ -1108,7 +1185,6 @@ class Batch : public BatchBase {
     MPM_TRY(upload_async(point_end_d_, point_end));
     MPM_TRY(upload_async(bin_end_d_, bin_end));
     MPM_TRY(upload_async(item_off_d_, item_off));
-    MPM_TRY(upload_async(blk_inst_, bi));
     MPM_CUDA_TRY(cudaMemcpyAsync(hdr_, &hdr, sizeof(hdr), cudaMemcpyHostToDevice, stream_));
     MPM_CUDA_TRY(cudaStreamSynchronize(stream_));  // host vectors go out of scope
     hdr_host_ = hdr;
@@ -1462,6 +1538,11 @@ class Batch : public BatchBase {
   int cap_ = 512;
   int sm_count_ = 148;
   int fused_per_sm_[12] = {};
+  cudaStream_t copy_stream_ = nullptr;
+  cudaEvent_t upload_ev_ = nullptr;
+  cudaMemPool_t pool_ = nullptr;
+  void* stage_ = nullptr;
+  size_t stage_cap_ = 0, stage_used_ = 0;
   std::vector<BodyCtx<PT>> ctx_host_;   // host copy of the body table
   bool single_mode_ = false;
   bool any_plain_ = false, any_normal_ = false;
@@ -1476,6 +1557,9 @@ class Batch : public BatchBase {
   int64_t scratch_bytes_ = 0;
   std::vector<void*> scratch_allocs_;
   std::vector<void*> cap_allocs_;
+  // job slots
+  std::vector<int> free_slots_;
+  int next_slot_ = 0;
   // block space
   std::vector<std::pair<int64_t, int64_t>> free_;
   int64_t block_end_ = 0;

@@ -34,6 +34,11 @@ __device__ __forceinline__ void mark_blocks(const Geom& g, const PointMapT<R>& p
       for (int i = i0; i <= i1; i++) flags[i + (int64_t)g.nb[0] * (j + (int64_t)g.nb[1] * k)] = 1u;
 }
 
+// Sets n int32 values to v.
+__global__ void k_fill_i32(int32_t* p, int64_t n, int32_t v) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) p[i] = v;
+}
+
 // Compacts the flagged node blocks of the batch's block space into `list`,
 // clears the flags and keeps the per-block activity of this step in
 // `was_active`.

@@ -46,6 +46,9 @@ __all__ = [
     "two_body_collision_3d",
     "column_collapse_3d",
     "block_drop_ensemble",
+    "RequestSpec",
+    "serving_stream",
+    "serving_case",
     "write_case",
     "read_points_file",
 ]
@@ -207,19 +210,71 @@ def block_drop_ensemble(count: int = 512, seed: int = 1003, n_range=(16, 96), st
     out = []
     for k in range(count):
         n = int(round(math.exp(rng.uniform(math.log(n_range[0]), math.log(n_range[1])))))
-        h = 1.0 / n
-        side = rng.uniform(*side_range)
-        per_axis = max(2, int(round(side / (h / 2.0))))
-        side = per_axis * h / 2.0
-        lo = [rng.uniform(h, 1.0 - h - side) for _ in range(3)]
-        vel = rng.uniform(-2.0, 2.0, size=3)
-        E = math.exp(rng.uniform(math.log(1e4), math.log(1e7)))
-        nu = rng.uniform(0.2, 0.45)
-        body = block_points(lo, (per_axis,) * 3, (h,) * 3, 1000.0, vel, name="block", E=E, nu=nu)
-        dt = _cfl_dt(h, E, nu, 1000.0, float(np.abs(vel).max()) * math.sqrt(3.0))
-        out.append(Case(name=f"ensemble_{seed}_{k}", dim=3, L=(1.0, 1.0, 1.0), N=(n, n, n), dt=dt,
-                        steps=steps, bodies=[body], seed=seed))
+        out.append(_block_drop(rng, n, steps, side_range, f"ensemble_{seed}_{k}", seed))
     return out
+
+
+def _block_drop(rng: np.random.Generator, n: int, steps: int, side_range, name: str, seed: int) -> Case:
+    """One block drop on an n^3 grid with the remaining draws from ``rng``."""
+    h = 1.0 / n
+    side = rng.uniform(*side_range)
+    per_axis = max(2, int(round(side / (h / 2.0))))
+    side = per_axis * h / 2.0
+    lo = [rng.uniform(h, 1.0 - h - side) for _ in range(3)]
+    vel = rng.uniform(-2.0, 2.0, size=3)
+    E = math.exp(rng.uniform(math.log(1e4), math.log(1e7)))
+    nu = rng.uniform(0.2, 0.45)
+    body = block_points(lo, (per_axis,) * 3, (h,) * 3, 1000.0, vel, name="block", E=E, nu=nu)
+    dt = _cfl_dt(h, E, nu, 1000.0, float(np.abs(vel).max()) * math.sqrt(3.0))
+    return Case(name=name, dim=3, L=(1.0, 1.0, 1.0), N=(n, n, n), dt=dt, steps=steps, bodies=[body], seed=seed)
+
+
+@dataclasses.dataclass
+class RequestSpec:
+    """One request of a serving stream: its arrival time and the draws that
+    make its case (``serving_case``); the arrays are built only when needed."""
+
+    index: int
+    arrival: float
+    kind: str      # "block" or "contact"
+    n: int
+    steps: int
+    mu: float
+    seed: int
+
+
+def serving_stream(rate: float = 100.0, duration: float = 60.0, seed: int = 1004, n_range=(16, 128),
+                   steps_range=(200, 5000), contact_frac: float = 0.1) -> List[RequestSpec]:
+    """Poisson arrivals at ``rate`` per second for ``duration`` seconds. Each
+    request is a 3D block drop drawn like ``block_drop_ensemble`` with N
+    log-uniform in ``n_range`` and a step count log-uniform in
+    ``steps_range``; a fraction ``contact_frac`` are instead two-body
+    ContactHuang collisions laid out like ``two_body_collision_3d`` at the
+    drawn N (mu uniform in [0.1, 0.6], dt scaled with the cell size)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    t = 0.0
+    while True:
+        t += float(rng.exponential(1.0 / rate))
+        if t >= duration:
+            break
+        kind = "contact" if rng.random() < contact_frac else "block"
+        n = int(round(math.exp(rng.uniform(math.log(n_range[0]), math.log(n_range[1])))))
+        steps = int(round(math.exp(rng.uniform(math.log(steps_range[0]), math.log(steps_range[1])))))
+        mu = float(rng.uniform(0.1, 0.6))
+        out.append(RequestSpec(len(out), t, kind, n, steps, mu, int(rng.integers(0, 2**31 - 1))))
+    return out
+
+
+def serving_case(spec: RequestSpec) -> Case:
+    """The case of a serving request (deterministic in the spec)."""
+    if spec.kind == "contact":
+        c = two_body_collision_3d(spec.n, steps=spec.steps, mu=spec.mu)
+        c.dt = 2e-5 * 128.0 / spec.n
+        c.name = f"request_{spec.index}_contact"
+        return c
+    rng = np.random.default_rng(spec.seed)
+    return _block_drop(rng, spec.n, spec.steps, (0.15, 0.4), f"request_{spec.index}", spec.seed)
 
 
 def _fmt(v: float) -> str:

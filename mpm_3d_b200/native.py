@@ -119,6 +119,22 @@ def load() -> ctypes.CDLL:
     lib.mpmgpu_batch_launch_count.restype = ctypes.c_int64
     lib.mpmgpu_batch_launch_count.argtypes = [vp]
     lib.mpmgpu_batch_destroy.argtypes = [vp]
+    lib.mpmgpu_server_create.argtypes = [ctypes.POINTER(_BatchConfig), ctypes.c_int64, ctypes.POINTER(vp)]
+    lib.mpmgpu_server_last_error.restype = ctypes.c_char_p
+    lib.mpmgpu_server_last_error.argtypes = [vp]
+    lib.mpmgpu_server_submit.argtypes = [vp, ctypes.POINTER(_JobDesc), ctypes.POINTER(ctypes.c_int)]
+    lib.mpmgpu_server_footprint.argtypes = [vp, ctypes.POINTER(_JobDesc), i64p]
+    lib.mpmgpu_server_advance.argtypes = [vp, ctypes.c_int]
+    lib.mpmgpu_server_poll.restype = ctypes.c_int
+    lib.mpmgpu_server_poll.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.c_int]
+    lib.mpmgpu_server_request.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                          ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double), i64p, i64p]
+    lib.mpmgpu_server_result.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp]
+    lib.mpmgpu_server_release.argtypes = [vp, ctypes.c_int]
+    lib.mpmgpu_server_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_int), i64p, i64p, i64p]
+    lib.mpmgpu_server_clock.restype = ctypes.c_double
+    lib.mpmgpu_server_clock.argtypes = [vp]
+    lib.mpmgpu_server_destroy.argtypes = [vp]
     _lib = lib
     return lib
 
@@ -280,6 +296,38 @@ def _case_config(case: inputs.Case, mode: str = "fp64") -> _Config:
     return cfg
 
 
+def job_desc(case: inputs.Case, steps: Optional[int] = None):
+    """mpmgpu_job_desc of a case, and the arrays it points at (keep them alive)."""
+    keep = []
+    cfg = _case_config(case)
+    bodies = (_BodyDesc * len(case.bodies))()
+    for i, body in enumerate(case.bodies):
+        arrs = dict(m=np.ascontiguousarray(body.m, np.float64), v=np.ascontiguousarray(body.v, np.float64),
+                    x=np.ascontiguousarray(body.x, np.float64), x_t=np.ascontiguousarray(body.x_t, np.float64),
+                    active=np.ascontiguousarray(body.active, np.int32))
+        keep.append(arrs)
+        bodies[i] = _BodyDesc(body.n, _ptr(arrs["m"]).value, _ptr(arrs["v"]).value, _ptr(arrs["x"]).value,
+                              _ptr(arrs["x_t"]).value, _ptr(arrs["active"]).value, int(body.material), body.E,
+                              body.nu, int(body.boundary), None, None)
+    contacts = (_ContactDesc * max(1, len(case.contacts)))()
+    for i, c in enumerate(case.contacts):
+        contacts[i] = _ContactDesc(c.b1, c.b2, c.mu)
+    desc = _JobDesc()
+    desc.grid = ctypes.pointer(cfg)
+    desc.nbodies = len(case.bodies)
+    desc.bodies = bodies
+    desc.ncontacts = len(case.contacts)
+    desc.contacts = contacts
+    if case.gravity is not None:
+        desc.gravity_vector = 1
+        g = list(case.gravity) + [0.0] * (3 - len(case.gravity))
+        for d in range(3):
+            desc.gravity[d] = g[d]
+    desc.steps = int(case.steps if steps is None else steps)
+    keep += [cfg, bodies, contacts]
+    return desc, keep
+
+
 class GPUBatch:
     """Many independent ``inputs.Case`` jobs stepped together on one GPU
     (``mpmgpu_batch_*``): one launch per stage for all jobs, the step replayed
@@ -317,34 +365,7 @@ class GPUBatch:
             pass
 
     def _job_desc(self, case: inputs.Case, steps: Optional[int]):
-        keep = []
-        cfg = _case_config(case)
-        bodies = (_BodyDesc * len(case.bodies))()
-        for i, body in enumerate(case.bodies):
-            arrs = dict(m=np.ascontiguousarray(body.m, np.float64), v=np.ascontiguousarray(body.v, np.float64),
-                        x=np.ascontiguousarray(body.x, np.float64), x_t=np.ascontiguousarray(body.x_t, np.float64),
-                        active=np.ascontiguousarray(body.active, np.int32))
-            keep.append(arrs)
-            bodies[i] = _BodyDesc(body.n, _ptr(arrs["m"]).value, _ptr(arrs["v"]).value, _ptr(arrs["x"]).value,
-                                  _ptr(arrs["x_t"]).value, _ptr(arrs["active"]).value, int(body.material), body.E,
-                                  body.nu, int(body.boundary), None, None)
-        contacts = (_ContactDesc * max(1, len(case.contacts)))()
-        for i, c in enumerate(case.contacts):
-            contacts[i] = _ContactDesc(c.b1, c.b2, c.mu)
-        desc = _JobDesc()
-        desc.grid = ctypes.pointer(cfg)
-        desc.nbodies = len(case.bodies)
-        desc.bodies = bodies
-        desc.ncontacts = len(case.contacts)
-        desc.contacts = contacts
-        if case.gravity is not None:
-            desc.gravity_vector = 1
-            g = list(case.gravity) + [0.0] * (3 - len(case.gravity))
-            for d in range(3):
-                desc.gravity[d] = g[d]
-        desc.steps = int(case.steps if steps is None else steps)
-        keep += [cfg, bodies, contacts]
-        return desc, keep
+        return job_desc(case, steps)
 
     def footprint(self, case: inputs.Case, steps: Optional[int] = None) -> int:
         desc, _keep = self._job_desc(case, steps)
@@ -427,3 +448,98 @@ class GPUBatch:
 
     def launches(self) -> int:
         return int(self.lib.mpmgpu_batch_launch_count(self.h))
+
+
+STATUS_STATE = 5
+
+
+class GPUServer:
+    """Continuous batching of simulation requests (``mpmgpu_server_*``):
+    ``submit`` admits a case at once if its device footprint fits the budget
+    left by the running requests (else returns None: keep it queued and retry
+    after ``advance``); ``advance(k)`` steps everything running k steps and
+    collects the requests that have run their steps."""
+
+    def __init__(self, budget_bytes: int, dim: int = 3, mode: str = "mixed", device: int = 0, sort_interval: int = 0,
+                 points_per_item: int = 0, graph: bool = True):
+        self.lib = load()
+        cfg = _BatchConfig(dim, MODES[mode], device, sort_interval, points_per_item, 0 if graph else 1, 0)
+        h = ctypes.c_void_p()
+        st = self.lib.mpmgpu_server_create(ctypes.byref(cfg), int(budget_bytes), ctypes.byref(h))
+        if st != 0:
+            raise MpmGpuError(f"{self.lib.mpmgpu_status_string(st).decode()}: server create")
+        self.h = h
+        self.cases: Dict[int, inputs.Case] = {}
+
+    def _check(self, status: int):
+        if status != 0:
+            msg = self.lib.mpmgpu_status_string(status).decode()
+            raise MpmGpuError(f"{msg}: {self.lib.mpmgpu_server_last_error(self.h).decode()}")
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.mpmgpu_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def footprint(self, case: inputs.Case, steps: Optional[int] = None) -> int:
+        desc, _keep = job_desc(case, steps)
+        out = ctypes.c_int64()
+        self._check(self.lib.mpmgpu_server_footprint(self.h, ctypes.byref(desc), ctypes.byref(out)))
+        return int(out.value)
+
+    def submit(self, case: inputs.Case, steps: Optional[int] = None) -> Optional[int]:
+        desc, _keep = job_desc(case, steps)
+        rid = ctypes.c_int()
+        st = self.lib.mpmgpu_server_submit(self.h, ctypes.byref(desc), ctypes.byref(rid))
+        if st == STATUS_STATE:
+            return None
+        self._check(st)
+        self.cases[rid.value] = case
+        return rid.value
+
+    def advance(self, steps: int):
+        self._check(self.lib.mpmgpu_server_advance(self.h, steps))
+
+    def poll(self, max_ids: int = 4096):
+        ids = (ctypes.c_int * max_ids)()
+        k = self.lib.mpmgpu_server_poll(self.h, ids, max_ids)
+        return [ids[i] for i in range(k)]
+
+    def request(self, rid: int) -> Dict[str, float]:
+        st = ctypes.c_int()
+        ta = ctypes.c_double()
+        td = ctypes.c_double()
+        pts = ctypes.c_int64()
+        steps = ctypes.c_int64()
+        self._check(self.lib.mpmgpu_server_request(self.h, rid, ctypes.byref(st), ctypes.byref(ta), ctypes.byref(td),
+                                                   ctypes.byref(pts), ctypes.byref(steps)))
+        return {"state": st.value, "t_admit": ta.value, "t_done": td.value, "points": pts.value, "steps": steps.value}
+
+    def result(self, rid: int, b: int, name: str) -> np.ndarray:
+        fid, w = POINT_FIELDS[name]
+        out = np.zeros((self.cases[rid].bodies[b].n, w))
+        self._check(self.lib.mpmgpu_server_result(self.h, rid, b, fid, _ptr(out)))
+        return out
+
+    def release(self, rid: int):
+        self._check(self.lib.mpmgpu_server_release(self.h, rid))
+        self.cases.pop(rid, None)
+
+    def stats(self) -> Dict[str, int]:
+        r = ctypes.c_int()
+        res = ctypes.c_int64()
+        lp = ctypes.c_int64()
+        done = ctypes.c_int64()
+        self._check(self.lib.mpmgpu_server_stats(self.h, ctypes.byref(r), ctypes.byref(res), ctypes.byref(lp),
+                                                 ctypes.byref(done)))
+        return {"running": r.value, "reserved_bytes": res.value, "live_points": lp.value,
+                "particle_steps_done": done.value}
+
+    def clock(self) -> float:
+        return float(self.lib.mpmgpu_server_clock(self.h))
