@@ -19,6 +19,13 @@ Workloads (seeded synthetic inputs, mpm_3d_b200.inputs):
              error against FP64 on every 8th job.
   collision  two 0.25 m cubes colliding, 128^3 grid, 524,288 points, ContactHuang (FP64)
   column     column collapse, 256x256x128 grid, 3,145,728 points (FP64)
+  serving    Poisson request stream at 100/s (block drops with N in [16,128],
+             200..5000 steps, 10 % two-body ContactHuang), admitted under a
+             150 GB budget into one continuously batched mixed-form server;
+             ``value`` is the particle-steps/s of the completed requests over
+             the makespan, with p50/p99 time to completion. The ensemble
+             line carries the same figures for the first --serve-seconds of
+             the stream.
 
 With N > 1 (torchrun) every rank runs its own copy of the workload (the
 ensemble with seed 1003 + rank; the single jobs as replicas): no data
@@ -67,6 +74,12 @@ def peaks():
 
 ENSEMBLE_JOBS = 512
 ENSEMBLE_SEED = 1003
+
+# DRAM bytes (read + write) per point of one k_g2p2g launch, from ncu
+# captures (profiles/k_g2p2g_ensemble96_mixed.md: the first 96 jobs of the
+# ensemble, scaled to a launch by its points; profiles/k_g2p2g_column_fp64.md:
+# the full column). None where no capture exists.
+TRAFFIC_BYTES_PER_POINT = {("ensemble", "mixed"): 155.6, ("column", "fp64"): 303.4}
 
 
 def make_workload(name: str, rank: int = 0):
@@ -241,8 +254,12 @@ class quiet_stdout:
 def run_reference_arm(args, rank, world):
     if rank != 0:
         return
-    if args.workload == "ensemble":
-        cases = make_workload("ensemble")
+    if args.workload in ("ensemble", "serving"):
+        if args.workload == "serving":
+            specs = inputs.serving_stream(rate=100.0, duration=args.serve_seconds, seed=1004)
+            cases = [inputs.serving_case(sp) for sp in specs[::max(1, len(specs) // 16)][:16]]
+        else:
+            cases = make_workload("ensemble")
         steps = max(1, min(args.steps, args.ref_steps))
         cpu = cpu_ensemble_sample(cases, steps)
         value = cpu["value"]
@@ -250,8 +267,8 @@ def run_reference_arm(args, rank, world):
             "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": steps, "warmup": 1, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": f"synthetic (block_drop_ensemble seed {ENSEMBLE_SEED})",
-            "config": {"workload": f"ensemble{ENSEMBLE_JOBS}", "jobs": len(cases),
-                       "points": sum(c.n_points for c in cases)},
+            "config": {"workload": args.workload if args.workload == "serving" else f"ensemble{ENSEMBLE_JOBS}",
+                       "jobs": len(cases), "points": sum(c.n_points for c in cases)},
             "cpu_baseline": cpu,
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         }
@@ -311,7 +328,7 @@ def profile_pass(sim, steps: int):
     return prof
 
 
-def roofline(points: int, steps: int, prof, active_ratio: float, mixed: bool):
+def roofline(points: int, steps: int, prof, active_ratio: float, mixed: bool, traffic_key=None):
     peak, peak_kind = peaks()
     bpp = bytes_per_point_step(active_ratio, mixed)
     g_launches, g_ms = prof["g2p2g"]
@@ -320,9 +337,12 @@ def roofline(points: int, steps: int, prof, active_ratio: float, mixed: bool):
     # algorithmic bytes of a launch are its points times bytes per point-step
     points_per_launch = points * steps / max(1, g_launches)
     achieved_gbs = points_per_launch * bpp / (per_launch_ms * 1e-3) / 1e9
+    tb = TRAFFIC_BYTES_PER_POINT.get(traffic_key)
     return {"bound": "hbm", "kernel": "k_g2p2g", "achieved": achieved_gbs, "peak": peak, "unit": "GB/s",
-            "frac": achieved_gbs / peak, "peak_kind": peak_kind, "traffic": None, "bytes_per_point_step": bpp,
-            "launch_ms": per_launch_ms, "points_per_launch": points_per_launch}
+            "frac": achieved_gbs / peak, "peak_kind": peak_kind,
+            "traffic": tb * points_per_launch if tb else None,
+            "traffic_source": "ncu dram__bytes per point x points per launch" if tb else None,
+            "bytes_per_point_step": bpp, "launch_ms": per_launch_ms, "points_per_launch": points_per_launch}
 
 
 def run_single(args, rank, world, local):
@@ -350,7 +370,7 @@ def run_single(args, rank, world, local):
     prof = profile_pass(sim, prof_steps)
     active, _drift = sim.active_nodes()
     active_ratio = active / max(1, n)
-    roof = roofline(n, prof_steps, prof, active_ratio, args.form == "mixed")
+    roof = roofline(n, prof_steps, prof, active_ratio, args.form == "mixed", (args.workload, args.form))
     sim.close()
 
     e2e = run_e2e(case, args.steps, local, args.form) if rank == 0 and not args.no_e2e else None
@@ -444,25 +464,28 @@ def run_ensemble(args, rank, world, local):
 
     torch.cuda.set_device(local)
     cases = make_workload("ensemble", rank)
+    if args.jobs > 0:
+        cases = cases[:args.jobs]
     n = sum(c.n_points for c in cases)
     sample_ids = ensemble_sample(cases)
     barrier(world)
-    fp64 = run_batch(cases, "fp64", args, local, sample_ids)
+    fp64 = run_batch(cases, "fp64", args, local, sample_ids) if not args.only_mixed else None
     mixed = run_batch(cases, "mixed", args, local, sample_ids)
     barrier(world)
     total_ms = sum(mixed["step_ms"])
     total_ms_max = max_over_ranks(total_ms, world)
     points_all = sum_over_ranks(float(n), world)
     value = points_all * args.steps / (total_ms_max * 1e-3)
-    fp64_value = n * args.steps / (sum(fp64["step_ms"]) * 1e-3)
+    fp64_value = n * args.steps / (sum(fp64["step_ms"]) * 1e-3) if fp64 else None
     # the mixed form's error against FP64 after the same steps, per field
-    errs = {f: 0.0 for f in ("x", "x_t", "T")}
-    for i in sample_ids:
+    errs = {f: (0.0 if fp64 else None) for f in ("x", "x_t", "T")}
+    for i in (sample_ids if fp64 else []):
         for f in errs:
             errs[f] = max(errs[f], rel_err(mixed["fields"][i][f], fp64["fields"][i][f], field_floor(cases[i], f)))
     active_ratio = mixed["active"] / max(1, n)
-    roof = roofline(n, mixed["prof_steps"], mixed["prof"], active_ratio, True)
+    roof = roofline(n, mixed["prof_steps"], mixed["prof"], active_ratio, True, ("ensemble", "mixed"))
     plain_value, plain_ms = plain_fp64(cases, args.plain_steps, local) if not args.no_plain else (None, None)
+    serving = run_serving(args.serve_seconds, local, mixed["sort_interval"]) if args.serve_seconds > 0 else None
     e2e = (run_e2e_batch(cases, args.steps, local, mixed["cap"], mixed["sort_interval"])
            if rank == 0 and not args.no_e2e else None)
     cpu = None
@@ -477,23 +500,63 @@ def run_ensemble(args, rank, world, local):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": total_ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32+f64", "data": f"synthetic (mpm_3d_b200.inputs.block_drop_ensemble, seed {ENSEMBLE_SEED}+rank)",
-        "config": {"workload": f"ensemble{ENSEMBLE_JOBS}", "jobs": len(cases), "points": n,
+        "config": {"workload": f"ensemble{ENSEMBLE_JOBS}" + (f"[:{args.jobs}]" if args.jobs > 0 else ""),
+                   "jobs": len(cases), "points": n,
                    "grids": "N^3, N log-uniform in [16,96]", "form": "mixed (FP32 points, FP64 nodal sums)",
                    "points_per_item": mixed["cap"], "sort_interval": mixed["sort_interval"], "graph": True,
                    "parallelism": f"independent{world}",
                    "l2": "inputs larger than L2", "active_nodes_per_point": round(active_ratio, 4)},
-        "batched_fp64": {"value": fp64_value, "unit": UNIT, "points_per_item": fp64["cap"],
-                         "sort_interval": fp64["sort_interval"]},
+        "batched_fp64": ({"value": fp64_value, "unit": UNIT, "points_per_item": fp64["cap"],
+                          "sort_interval": fp64["sort_interval"]} if fp64 else None),
         "plain_fp64": {"value": plain_value, "unit": UNIT, "steps_per_job": args.plain_steps,
                        "how": "one mpmgpu_handle per job, jobs in sequence, CUDA events around each job's steps"},
         "vs_plain_fp64": (value / plain_value) if plain_value else None,
-        "mixed_rel_err_vs_fp64": {**errs, "jobs_compared": len(sample_ids), "after_steps": mixed["steps_done"]},
+        "mixed_rel_err_vs_fp64": {**errs, "jobs_compared": len(sample_ids), "after_steps": mixed["steps_done"],
+                                  "norm": "max|mixed - fp64| / max(max|fp64|, field scale) per job, worst job"},
+        "serving": serving,
         "roofline": roof,
         "stage_ms_per_step": {k: v[1] / mixed["prof_steps"] for k, v in mixed["prof"].items()},
         "gpu_launches": mixed["launches"],
         "clocks": mixed["clocks"],
         "e2e": e2e,
         "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_serving(seconds: float, device: int, sort_interval: int = 8, round_steps: int = 20):
+    """The serving stream for `seconds` of arrivals (seed 1004) until every
+    request has completed; p50/p99 time to completion and throughput."""
+    from mpm_3d_b200.native import GPUServer
+    from mpm_3d_b200.serving import run_stream
+
+    specs = inputs.serving_stream(rate=100.0, duration=seconds, seed=1004)
+    srv = GPUServer(budget_bytes=150 * 10**9, mode="mixed", device=device, sort_interval=sort_interval)
+    rep = run_stream(srv, specs, round_steps=round_steps)
+    srv.close()
+    out = rep.summary()
+    out.update({"arrivals_s": seconds, "rate_per_s": 100.0, "budget_bytes": 150 * 10**9, "round_steps": round_steps,
+                "form": "mixed"})
+    return out
+
+
+def run_serving_workload(args, rank, world, local):
+    import torch
+
+    torch.cuda.set_device(local)
+    rep = run_serving(args.serve_seconds, local)
+    rep_max = max_over_ranks(rep["makespan_s"], world)
+    steps_all = sum_over_ranks(float(rep["particle_steps"]), world)
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": steps_all / rep_max, "unit": UNIT, "n_gpus": world, "steps": None,
+        "warmup": 0, "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32+f64", "data": "synthetic (mpm_3d_b200.inputs.serving_stream, seed 1004)",
+        "config": {"workload": "serving", "arrivals_s": args.serve_seconds, "rate_per_s": 100.0,
+                   "budget_bytes": 150 * 10**9, "form": "mixed", "parallelism": f"independent{world}"},
+        "serving": rep,
+        "gpu_launches": None,
     }
     print(json.dumps(line), flush=True)
 
@@ -570,10 +633,14 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=0, help="timed steps (default: the workload's own step count)")
     ap.add_argument("--warmup", type=int, default=10)
-    ap.add_argument("--workload", default="ensemble", choices=["ensemble", "collision", "column"])
+    ap.add_argument("--workload", default="ensemble", choices=["ensemble", "collision", "column", "serving"])
     ap.add_argument("--form", default="fp64", choices=["fp64", "mixed"], help="form of the single-job workloads")
     ap.add_argument("--plain-steps", type=int, default=10, help="timed steps per job of the plain FP64 path")
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--jobs", type=int, default=0, help="ensemble: only the first JOBS jobs (profiling cases)")
+    ap.add_argument("--only-mixed", action="store_true", help="ensemble: skip the FP64 batch")
+    ap.add_argument("--serve-seconds", type=float, default=-1.0,
+                    help="seconds of request arrivals of the serving stream (default 3 with the ensemble, 60 alone)")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--ref-steps", type=int, default=4, help="steps of the CPU reference sample")
     ap.add_argument("--no-cpu", action="store_true")
@@ -581,14 +648,18 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.serve_seconds < 0:
+        args.serve_seconds = 60.0 if args.workload == "serving" else 3.0
     if args.steps <= 0:
-        args.steps = 100 if args.workload == "ensemble" else make_workload(args.workload).steps
+        args.steps = 100 if args.workload in ("ensemble", "serving") else make_workload(args.workload).steps
     rank, world, local = dist_setup(args.gpus)
     try:
         if args.impl == "reference":
             run_reference_arm(args, rank, world)
         elif args.workload == "ensemble":
             run_ensemble(args, rank, world, local)
+        elif args.workload == "serving":
+            run_serving_workload(args, rank, world, local)
         else:
             run_single(args, rank, world, local)
     finally:
