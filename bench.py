@@ -168,7 +168,9 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def dist_setup(n_gpus: int):
+def dist_setup(n_gpus: int, backend: str = "nccl"):
+    """Rank, world size and local rank from the torchrun environment; joins
+    the process group (NCCL between GPUs; gloo for the host-side tests)."""
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -176,8 +178,14 @@ def dist_setup(n_gpus: int):
         import torch.distributed as dist
         from datetime import timedelta
 
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+        dist.init_process_group(backend, timeout=timedelta(seconds=120))
     return rank, world, local
+
+
+def _reduce_device():
+    import torch.distributed as dist
+
+    return "cpu" if dist.get_backend() == "gloo" else "cuda"
 
 
 def barrier(world):
@@ -193,7 +201,7 @@ def max_over_ranks(value: float, world: int) -> float:
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    t = torch.tensor([value], dtype=torch.float64, device=_reduce_device())
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -204,7 +212,7 @@ def sum_over_ranks(value: float, world: int) -> float:
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    t = torch.tensor([value], dtype=torch.float64, device=_reduce_device())
     dist.all_reduce(t, op=dist.ReduceOp.SUM)
     return float(t.item())
 
