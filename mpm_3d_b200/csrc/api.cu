@@ -74,8 +74,9 @@ mpmgpu_status check_launch(mpmgpu_handle* h, const char* what) {
 std::unique_ptr<BatchBase> make_batch(int dim, int mode, int device, int sort_interval, int cap, int use_graph,
                                       int keep_debug, mpmgpu_status* st, std::string* msg) {
   std::unique_ptr<BatchBase> b;
-  if (mode == MPMGPU_MODE_FP64) {
-    auto p = std::make_unique<Batch<double>>(dim, device, sort_interval, cap, use_graph, keep_debug);
+  if (mode == MPMGPU_MODE_FP64 || mode == MPMGPU_MODE_FP64_DETERMINISTIC) {
+    auto p = std::make_unique<Batch<double>>(dim, device, sort_interval, cap, use_graph, keep_debug,
+                                             mode == MPMGPU_MODE_FP64_DETERMINISTIC);
     *st = p->init();
     *msg = p->last_error;
     b = std::move(p);
@@ -124,7 +125,8 @@ mpmgpu_status mpmgpu_create(const mpmgpu_config* cfg, mpmgpu_handle** out) {
   if (!(cfg->dt > 0)) return MPMGPU_ERR_ARG;
   if (cfg->cpdi_spec != 0 && cfg->cpdi_spec != 1) return MPMGPU_ERR_ARG;
   if (cfg->contact_spec != 0 && cfg->contact_spec != 1) return MPMGPU_ERR_ARG;
-  if (cfg->mode != MPMGPU_MODE_FP64 && cfg->mode != MPMGPU_MODE_MIXED) return MPMGPU_ERR_UNSUPPORTED;
+  if (cfg->mode != MPMGPU_MODE_FP64 && cfg->mode != MPMGPU_MODE_MIXED && cfg->mode != MPMGPU_MODE_FP64_DETERMINISTIC)
+    return MPMGPU_ERR_UNSUPPORTED;
   if (cfg->sort_interval < 0) return MPMGPU_ERR_ARG;
   for (int d = 0; d < cfg->dim; d++)
     if (cfg->N[d] < 1 || !(cfg->L[d] > 0)) return MPMGPU_ERR_ARG;
@@ -279,7 +281,8 @@ mpmgpu_status mpmgpu_batch_create(const mpmgpu_batch_config* cfg, mpmgpu_batch**
   if (!cfg || !out) return MPMGPU_ERR_ARG;
   *out = nullptr;
   if (cfg->dim != 2 && cfg->dim != 3) return MPMGPU_ERR_UNSUPPORTED;
-  if (cfg->mode != MPMGPU_MODE_FP64 && cfg->mode != MPMGPU_MODE_MIXED) return MPMGPU_ERR_UNSUPPORTED;
+  if (cfg->mode != MPMGPU_MODE_FP64 && cfg->mode != MPMGPU_MODE_MIXED && cfg->mode != MPMGPU_MODE_FP64_DETERMINISTIC)
+    return MPMGPU_ERR_UNSUPPORTED;
   if (cfg->sort_interval < 0 || cfg->points_per_item < 0) return MPMGPU_ERR_ARG;
   if (cfg->points_per_item != 0 && !cap_available(cfg->dim, cfg->mode == MPMGPU_MODE_MIXED, cfg->points_per_item))
     return MPMGPU_ERR_UNSUPPORTED;

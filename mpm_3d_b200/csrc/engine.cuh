@@ -192,6 +192,7 @@ class Batch : public BatchBase {
     int64_t n = 0;
     PointsT<PT> P{}, Palt{};
     NodesAcc A{}, snap{};
+    NodesAcc Ar{};   // deterministic form: level-1 sums
     NodesVel V{};
     MaterialParams mat{};
     int has_boundary = 0;
@@ -224,8 +225,8 @@ class Batch : public BatchBase {
     int64_t bytes = 0;
   };
 
-  Batch(int dim, int device, int sort_interval, int cap, int use_graph, int keep_debug)
-      : dim_(dim), device_(device), keep_debug_(keep_debug != 0), use_graph_(use_graph != 0) {
+  Batch(int dim, int device, int sort_interval, int cap, int use_graph, int keep_debug, bool det = false)
+      : dim_(dim), device_(device), keep_debug_(keep_debug != 0), use_graph_(use_graph != 0), det_(det) {
     sort_interval_ = sort_interval > 0 ? sort_interval : 32;
     cap_ = cap;
   }
@@ -248,8 +249,9 @@ class Batch : public BatchBase {
       MPM_CUDA_TRY(cudaMemPoolSetAttribute(pool_, cudaMemPoolAttrReleaseThreshold, &keep));
     }
     if (cap_ == 0) cap_ = default_cap();
-    if (!cap_available(dim_, mixed(), cap_))
+    if (!cap_available(dim_, mixed(), cap_) || (det_ && cap_ != default_cap()))
       return fail(MPMGPU_ERR_ARG, "points_per_item " + std::to_string(cap_) + " not available for this form");
+    if (det_ && mixed()) return fail(MPMGPU_ERR_UNSUPPORTED, "the deterministic form is FP64");
     MPM_TRY(alloc_raw(&hdr_, 1, scratch_allocs_));
     MPM_TRY(alloc_raw(&count_, 1, scratch_allocs_));
     MPM_TRY(alloc_raw(&err_, 1, scratch_allocs_));
@@ -379,6 +381,13 @@ class Batch : public BatchBase {
       MPM_TRY(upload(B.P.pid, pid));
     }
     const size_t ns = (size_t)j->g.nslots;
+    if (det_) {
+      MPM_TRY(alloc_dev(&B.Ar.m, ns, B.allocs, j->bytes));
+      for (int d = 0; d < 3; d++) {
+        MPM_TRY(alloc_dev(&B.Ar.mx[d], ns, B.allocs, j->bytes));
+        MPM_TRY(alloc_dev(&B.Ar.f[d], ns, B.allocs, j->bytes));
+      }
+    }
     MPM_TRY(alloc_dev(&B.A.m, ns, B.allocs, j->bytes));
     for (int d = 0; d < 3; d++) {
       MPM_TRY(alloc_dev(&B.A.mx[d], ns, B.allocs, j->bytes));
@@ -411,6 +420,8 @@ class Batch : public BatchBase {
     const size_t ns = (size_t)j->g.nslots;
     if (!B1.needs_normal) {
       for (int d = 0; d < 3; d++) MPM_TRY(alloc_dev(&B1.A.nrm[d], ns, B1.allocs, j->bytes));
+      if (det_)
+        for (int d = 0; d < 3; d++) MPM_TRY(alloc_dev(&B1.Ar.nrm[d], ns, B1.allocs, j->bytes));
       B1.needs_normal = 1;
     }
     const int c = j->nc;
@@ -775,7 +786,7 @@ class Batch : public BatchBase {
     float best_ms = 1e30f;
     const int caps[3] = {256, 512, 1024};
     for (int ci = 0; ci < 3 && st == MPMGPU_OK; ci++) {
-      if (!cap_available(dim_, mixed(), caps[ci])) continue;
+      if (!cap_available(dim_, mixed(), caps[ci]) || (det_ && caps[ci] != default_cap())) continue;
       cap_ = caps[ci];
       float ms = 0.0f;
       st = trial(steps, 1 << 30, &ms);
@@ -948,7 +959,7 @@ class Batch : public BatchBase {
     return MPMGPU_OK;
   }
 
-  int default_cap() const { return 512; }
+  int default_cap() const { return det_ && dim_ == 3 ? 256 : 512; }
 
   // Copies a block-linear nodal array (comps SoA components) to reference
   // node order; nodes of blocks that were not active in the last step read 0.
@@ -1095,6 +1106,7 @@ class Batch : public BatchBase {
       for (auto& b : j.bodies) {
         GridBody G{};
         G.A = b.A;
+        G.Ar = b.Ar;
         G.V = b.V;
         G.snap = b.snap;
         G.has_boundary = b.has_boundary;
@@ -1108,6 +1120,7 @@ class Batch : public BatchBase {
         c.P = b.P;
         c.V = b.V;
         c.A = b.A;
+        c.Ar = b.Ar;
         c.flags = flags_ + j.block_off;   // rebased after growth below
         c.needs_normal = b.needs_normal;
         c.prime = b.prime;
@@ -1149,6 +1162,7 @@ class Batch : public BatchBase {
     MPM_TRY(grow(&bin_scan_, &cap_bins_, bins + 2, 0));
     MPM_TRY(grow(&chunk_sum_, &cap_chunks_, cap_bins_ / kScanChunk + 2, 0));
     MPM_TRY(grow(&item_off_d_, &cap_bodies_i_, std::max<int64_t>(nb, 1), 0));
+    if (det_) MPM_TRY(grow(&bounds_, &cap_bounds_, std::max<int64_t>(4 * nb, 4), 0));
     MPM_TRY(grow(&nwork_body_, &cap_bodies_w_, std::max<int64_t>(nb, 1), 0));
     MPM_TRY(grow(&work_end_body_, &cap_bodies_e_, std::max<int64_t>(nb, 1), 0));
     MPM_TRY(grow(&work_bin_, &cap_items_n_, std::max<int64_t>(items, 1), 0));
@@ -1206,7 +1220,8 @@ class Batch : public BatchBase {
 
   // First scatter of joining bodies (their nodal sums for the first step).
   mpmgpu_status prime() {
-    MPM_TRY(launch_fused(1));
+    if (det_) MPM_TRY(launch_bounds());
+    MPM_TRY(launch_fused(1, det_ ? 2 : 3));
     // clear the prime flags in the host mirrors and the device table
     for (auto& j : jobs_) {
       if (!j.in_tables) continue;
@@ -1256,8 +1271,8 @@ class Batch : public BatchBase {
 
   int stride_blocks(int threads) const { return sm_count_ * (2048 / threads); }
 
-  template <int DIM, int CAP, bool NORMAL, bool SINGLE>
-  mpmgpu_status launch_fused_k(int prime_pass, int one_body) {
+  template <int DIM, int CAP, bool NORMAL, bool SINGLE, bool DET>
+  mpmgpu_status launch_fused_k(int prime_pass, int phases, int one_body) {
     FusedLaunch<PT> fl{};
     if (SINGLE) fl.one = ctx_host_[(size_t)one_body];
     fl.one_body = SINGLE ? one_body : -1;
@@ -1275,10 +1290,13 @@ class Batch : public BatchBase {
     fl.err = err_;
     fl.drift = drift_;
     fl.prime_pass = prime_pass;
-    constexpr size_t smem = fused_smem_bytes<DIM, PT, CAP>();
-    auto kern = k_g2p2g<DIM, PT, CAP, NORMAL, SINGLE>;
+    fl.phases = phases;
+    fl.bounds = bounds_;
+    constexpr size_t smem = fused_smem_bytes<DIM, PT, CAP, DET>();
+    auto kern = k_g2p2g<DIM, PT, CAP, NORMAL, SINGLE, DET>;
     // resident CTAs per SM, looked up once per kernel (before any capture)
-    int& per_sm = fused_per_sm_[(CAP == 256 ? 0 : (CAP == 512 ? 1 : 2)) * 4 + (NORMAL ? 2 : 0) + (SINGLE ? 1 : 0)];
+    int& per_sm = fused_per_sm_[((CAP == 256 ? 0 : (CAP == 512 ? 1 : 2)) * 4 + (NORMAL ? 2 : 0) + (SINGLE ? 1 : 0)) * 2 +
+                                (DET ? 1 : 0)];
     if (per_sm == 0) {
       MPM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
       MPM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kFusedThreads, smem));
@@ -1293,34 +1311,56 @@ class Batch : public BatchBase {
   // One launch per body for small batches at the default item size (the
   // body's parameters then sit in the constant bank), else one launch per
   // kind of body (with or without the contact normal) over the table.
-  template <int DIM, int CAP>
-  mpmgpu_status launch_fused_t(int prime_pass) {
+  template <int DIM, int CAP, bool DET>
+  mpmgpu_status launch_fused_t(int prime_pass, int phases) {
     if constexpr (CAP == 512) {
       if (single_mode_) {
         for (size_t b = 0; b < ctx_host_.size(); b++) {
           if (prime_pass && !ctx_host_[b].prime) continue;
           if (ctx_host_[b].needs_normal)
-            MPM_TRY((launch_fused_k<DIM, CAP, true, true>(prime_pass, (int)b)));
+            MPM_TRY((launch_fused_k<DIM, CAP, true, true, DET>(prime_pass, phases, (int)b)));
           else
-            MPM_TRY((launch_fused_k<DIM, CAP, false, true>(prime_pass, (int)b)));
+            MPM_TRY((launch_fused_k<DIM, CAP, false, true, DET>(prime_pass, phases, (int)b)));
         }
         return MPMGPU_OK;
       }
     }
-    if (any_plain_) MPM_TRY((launch_fused_k<DIM, CAP, false, false>(prime_pass, -1)));
-    if (any_normal_) MPM_TRY((launch_fused_k<DIM, CAP, true, false>(prime_pass, -1)));
+    if (any_plain_) MPM_TRY((launch_fused_k<DIM, CAP, false, false, DET>(prime_pass, phases, -1)));
+    if (any_normal_) MPM_TRY((launch_fused_k<DIM, CAP, true, false, DET>(prime_pass, phases, -1)));
     return MPMGPU_OK;
   }
 
-  mpmgpu_status launch_fused(int prime_pass) {
-    if (dim_ == 3) {
-      if (cap_ == 256) return launch_fused_t<3, 256>(prime_pass);
-      if constexpr (sizeof(PT) == 4) {
-        if (cap_ == 1024) return launch_fused_t<3, 1024>(prime_pass);
+  mpmgpu_status launch_fused(int prime_pass, int phases) {
+    if constexpr (sizeof(PT) == 8) {
+      if (det_) {
+        // the deterministic form: 256 points per item in 3D (two tile levels)
+        if (dim_ == 3) return launch_fused_t<3, 256, true>(prime_pass, phases);
+        return launch_fused_t<2, 512, true>(prime_pass, phases);
       }
-      return launch_fused_t<3, 512>(prime_pass);
     }
-    return launch_fused_t<2, 512>(prime_pass);
+    if (dim_ == 3) {
+      if (cap_ == 256) return launch_fused_t<3, 256, false>(prime_pass, phases);
+      if constexpr (sizeof(PT) == 4) {
+        if (cap_ == 1024) return launch_fused_t<3, 1024, false>(prime_pass, phases);
+      }
+      return launch_fused_t<3, 512, false>(prime_pass, phases);
+    }
+    return launch_fused_t<2, 512, false>(prime_pass, phases);
+  }
+
+  // Deterministic form: per-body bounds of the nodal contributions from the
+  // updated point state (before the scatter that uses them).
+  mpmgpu_status launch_bounds() {
+    if constexpr (sizeof(PT) == 8) {
+      MPM_CUDA_TRY(cudaMemsetAsync(bounds_, 0, sizeof(unsigned long long) * 4 * std::max<size_t>(ctx_host_.size(), 1),
+                                   stream_));
+      if (dim_ == 3)
+        k_det_bounds<3><<<stride_blocks(256), 256, 0, stream_>>>(hdr_, ctx_d_, point_end_d_, bounds_);
+      else
+        k_det_bounds<2><<<stride_blocks(256), 256, 0, stream_>>>(hdr_, ctx_d_, point_end_d_, bounds_);
+      return check_launch("k_det_bounds");
+    }
+    return MPMGPU_OK;
   }
 
   mpmgpu_status launch_clear_prime() {
@@ -1344,7 +1384,13 @@ class Batch : public BatchBase {
         k_grid<2><<<gb, 64, 0, stream_>>>(insts_d_, gbodies_d_, blk_inst_, list_, count_, active_nodes_);
       MPM_TRY(check_launch("k_grid"));
     }
-    return launch_fused(0);
+    if (det_) {
+      // update, bounds from the new state, then the scatter
+      MPM_TRY(launch_fused(0, 1));
+      MPM_TRY(launch_bounds());
+      return launch_fused(0, 2);
+    }
+    return launch_fused(0, 3);
   }
 
   template <int DIM>
@@ -1395,7 +1441,7 @@ class Batch : public BatchBase {
 
   // Captures `body` into graph `g` on first use; launches it.
   template <typename F>
-  mpmgpu_status run_graph(cudaGraphExec_t& g, bool& warm, int kernels, F&& body) {
+  mpmgpu_status run_graph(cudaGraphExec_t& g, bool& warm, int& kernels, F&& body) {
     // the first run of a launch sequence is direct (it also sets kernel
     // attributes, which cannot happen inside a capture); later runs replay
     // the captured graph
@@ -1409,6 +1455,7 @@ class Batch : public BatchBase {
       const int64_t before = launches_;
       mpmgpu_status st = body();
       cudaError_t e = cudaStreamEndCapture(stream_, &graph);
+      kernels = (int)(launches_ - before);   // kernels the graph replays
       launches_ = before;
       if (st != MPMGPU_OK) {
         if (graph) cudaGraphDestroy(graph);
@@ -1438,12 +1485,11 @@ class Batch : public BatchBase {
   // The step graph depends on which point buffer is current (one-body
   // launches carry the pointers): one graph per buffer parity.
   mpmgpu_status launch_step() {
-    const int kernels = 2 + (single_mode_ && cap_ == 512 ? (int)ctx_host_.size() : (any_plain_ ? 1 : 0) + (any_normal_ ? 1 : 0));
-    return run_graph(g_step_[flip_], step_warm_[flip_], kernels, [&] { return launch_step_direct(); });
+    return run_graph(g_step_[flip_], step_warm_[flip_], g_step_k_[flip_], [&] { return launch_step_direct(); });
   }
 
   mpmgpu_status launch_sort() {
-    MPM_TRY(run_graph(g_sort_, sort_warm_, 11, [&] { return launch_sort_direct(); }));
+    MPM_TRY(run_graph(g_sort_, sort_warm_, g_sort_k_, [&] { return launch_sort_direct(); }));
     flip_mirrors();
     steps_since_sort_ = 0;
     return MPMGPU_OK;
@@ -1534,10 +1580,11 @@ class Batch : public BatchBase {
   int device_;
   bool keep_debug_;
   bool use_graph_;
+  bool det_ = false;   // deterministic form: two-level exact nodal sums
   int sort_interval_ = 32;
   int cap_ = 512;
   int sm_count_ = 148;
-  int fused_per_sm_[12] = {};
+  int fused_per_sm_[24] = {};
   cudaStream_t copy_stream_ = nullptr;
   cudaEvent_t upload_ev_ = nullptr;
   cudaMemPool_t pool_ = nullptr;
@@ -1600,6 +1647,8 @@ class Batch : public BatchBase {
   int64_t cap_items_fb_ = 0;
   int32_t* flat_item_ = nullptr;
   int64_t cap_items_fi_ = 0;
+  unsigned long long* bounds_ = nullptr;   // deterministic form: 4 per body
+  int64_t cap_bounds_ = 0;
   int32_t* item_off_d_ = nullptr;
   int64_t cap_bodies_i_ = 0;
   int32_t* nwork_body_ = nullptr;
@@ -1613,6 +1662,8 @@ class Batch : public BatchBase {
   int32_t* work_end_ = nullptr;
   int64_t cap_items_e_ = 0;
   cudaGraphExec_t g_step_[2] = {nullptr, nullptr};
+  int g_step_k_[2] = {0, 0};
+  int g_sort_k_ = 0;
   cudaGraphExec_t g_sort_ = nullptr;
   bool step_warm_[2] = {false, false};
   bool sort_warm_ = false;

@@ -62,6 +62,8 @@ struct FusedLaunch {
   int* err;
   unsigned long long* drift;
   int prime_pass;   // 1: only bodies still to prime, scatter only
+  int phases;       // 1: gather + point update, 2: map + scatter, 3: both
+  const unsigned long long* bounds;  // deterministic form: 4 per body (k_det_bounds)
 };
 
 // Staged point arrays: x0..2 v0..2 u0..2 s0..5 vol m ext, then active.
@@ -89,7 +91,7 @@ __host__ __device__ constexpr int fused_bin() {
 
 // Shared memory layout: mbarriers (points, table entry slots 0 and 1) |
 // body table entries [2] | points [kNF][row] | active [row] | tile [10][TN]
-// doubles | touched [TN].
+// doubles (two such levels in the deterministic form) | touched [TN].
 template <typename PT>
 __host__ __device__ constexpr size_t ctx_bytes() {
   return (offsetof(BodyCtx<PT>, Palt) + 15) / 16 * 16;
@@ -110,9 +112,10 @@ template <typename PT, int CAP>
 __host__ __device__ constexpr size_t off_tile() {
   return off_act<PT, CAP>() + sizeof(int32_t) * cap_row<CAP>();
 }
-template <int DIM, typename PT, int CAP>
+// Accumulator tile levels: 1, or 2 in the deterministic form.
+template <int DIM, typename PT, int CAP, bool DET>
 __host__ __device__ constexpr size_t fused_smem_bytes() {
-  return off_tile<PT, CAP>() + sizeof(double) * 10 * fused_tile_nodes<DIM, fused_bin<DIM>()>() +
+  return off_tile<PT, CAP>() + sizeof(double) * (DET ? 20 : 10) * fused_tile_nodes<DIM, fused_bin<DIM>()>() +
          fused_tile_nodes<DIM, fused_bin<DIM>()>();
 }
 
@@ -292,7 +295,7 @@ __device__ __forceinline__ PT staged_pos(const PT* sp, int d) {
 // S^T (v - vref) and the velocity gradient is that of v - vref: the same
 // values in exact arithmetic, without the cancellation of a common
 // translation against the velocity differences in FP32.
-template <int DIM, int T, int TN, int ROW, typename PT>
+template <int DIM, int T, int TN, int ROW, bool DET, typename PT>
 __device__ __forceinline__ void gather_update(const BodyCtx<PT>& c, int* err, unsigned long long* drift, int64_t p,
                                               PT* sp, const int* o, const PT* tvel, const double* vref) {
   using R = PT;
@@ -305,7 +308,10 @@ __device__ __forceinline__ void gather_update(const BodyCtx<PT>& c, int* err, un
   const int st = build_map<DIM>(c.g, c.mc, c.sp.cpdi, x, sp[kFext * ROW], pm, err);
   GatherSum<R> gs;
   if (st > 0) {
-    if (regular_window<DIM>(pm, o, T))
+    // the deterministic form takes one arithmetic for every window: the
+    // straight-line path rounds differently, and whether a window qualifies
+    // depends on the binning
+    if (!DET && regular_window<DIM>(pm, o, T))
       gs = gather_regular<DIM, T, TN>(pm, o, tvel);
     else
       gs = gather_general<DIM, T, TN>(c, drift, pm, o, tvel, vref);
@@ -369,10 +375,22 @@ __device__ __forceinline__ constexpr int tile_field(int i) {
 // Adds one node's values to the shared FP64 tile (shared-memory FP64
 // atomics). Issuing the compare-and-swap steps of all values together was
 // measured slower than the plain atomics (register pressure).
-template <int DIM, bool NORMAL, int TN, typename R>
-__device__ __forceinline__ void tile_add_node(double* tacc, int t, const NodeVals<DIM, NORMAL, R>& nv) {
+template <int DIM, bool NORMAL, int TN, bool DET, typename R>
+__device__ __forceinline__ void tile_add_node(double* tacc, int t, const NodeVals<DIM, NORMAL, R>& nv,
+                                              const Split2* ks) {
 #pragma unroll
-  for (int i = 0; i < NodeVals<DIM, NORMAL, R>::K; i++) atomicAdd(tacc + tile_field<DIM>(i) * TN + t, (double)nv.v[i]);
+  for (int i = 0; i < NodeVals<DIM, NORMAL, R>::K; i++) {
+    if constexpr (DET) {
+      // deterministic form: two exactly summed levels (second tile behind the first)
+      const int cls = i == 0 ? 0 : (i <= DIM ? 1 : (i <= 2 * DIM ? 2 : 3));
+      double q0, q1;
+      presplit((double)nv.v[i], ks[cls], q0, q1);
+      atomicAdd(tacc + tile_field<DIM>(i) * TN + t, q0);
+      atomicAdd(tacc + (10 + tile_field<DIM>(i)) * TN + t, q1);
+    } else {
+      atomicAdd(tacc + tile_field<DIM>(i) * TN + t, (double)nv.v[i]);
+    }
+  }
 }
 
 // Per-point scatter sources: m, m x_t and V sigma (symmetric 3x3).
@@ -386,9 +404,9 @@ struct ScatterSrc {
 // Scatter over a regular (2^dim-node, in-tile) window. The nodal force
 // -V sigma . grad S is evaluated per row of the window as
 // -(G0 A + W0 B) with A, B the row factors of the separable gradient.
-template <int DIM, int T, int TN, bool NORMAL, typename R>
+template <int DIM, int T, int TN, bool NORMAL, bool DET, typename R>
 __device__ __forceinline__ void scatter_regular(const PointMapT<R>& pm, const int* o, const ScatterSrc<R>& q,
-                                                double* tacc, uint8_t* touched) {
+                                                double* tacc, uint8_t* touched, const Split2* ks) {
   const int t0 = (pm.ax[0].base - o[0]) + T * ((pm.ax[1].base - o[1]) + (DIM == 3 ? T * (pm.ax[2].base - o[2]) : 0));
   const R W0s[2] = {pm.sS * pm.ax[0].W[0], pm.sS * pm.ax[0].W[1]};
   const R G0g[2] = {pm.sG * pm.ax[0].G[0], pm.sG * pm.ax[0].G[1]};
@@ -428,7 +446,7 @@ __device__ __forceinline__ void scatter_regular(const PointMapT<R>& pm, const in
 #pragma unroll
           for (int d = 0; d < DIM; d++) nv.v[1 + 2 * DIM + d] = gr[d] * q.m;
         }
-        tile_add_node<DIM, NORMAL, TN>(tacc, t, nv);
+        tile_add_node<DIM, NORMAL, TN, DET>(tacc, t, nv, ks);
       }
     }
   }
@@ -436,10 +454,10 @@ __device__ __forceinline__ void scatter_regular(const PointMapT<R>& pm, const in
 
 // Scatter over any window (three-node spans, nodes outside the tile, which
 // go straight to the global accumulators).
-template <int DIM, int T, int TN, bool NORMAL, typename PT, typename R>
+template <int DIM, int T, int TN, bool NORMAL, bool DET, typename PT, typename R>
 __device__ __forceinline__ void scatter_general(const BodyCtx<PT>& c, unsigned long long* drift,
                                                 const PointMapT<R>& pm, const int* o, const ScatterSrc<R>& q,
-                                                double* tacc, uint8_t* touched) {
+                                                double* tacc, uint8_t* touched, const Split2* ks) {
   const Geom& g = c.g;
   const bool in_tile = window_in_tile<DIM>(pm, o, T);
   if (!in_tile) {
@@ -469,15 +487,26 @@ __device__ __forceinline__ void scatter_general(const BodyCtx<PT>& c, unsigned l
     if (in_tile) {
       const int t = t0 + k0 + T * (k1 + T * k2);
       touched[t] = 1;
-      tile_add_node<DIM, NORMAL, TN>(tacc, t, nv);
+      tile_add_node<DIM, NORMAL, TN, DET>(tacc, t, nv, ks);
     } else {
       const int64_t s = node_slot(g, pm.ax[0].base + k0, pm.ax[1].base + k1, DIM == 3 ? pm.ax[2].base + k2 : 0);
-      atomicAdd(c.A.m + s, (double)nv.v[0]);
+      // global accumulator of value i (m, mx, f, normal order of NodeVals)
+      auto gadd = [&](double* a0, double* a1, int cls, double v) {
+        if constexpr (DET) {
+          double q0, q1;
+          presplit(v, ks[cls], q0, q1);
+          atomicAdd(a0 + s, q0);
+          atomicAdd(a1 + s, q1);
+        } else {
+          atomicAdd(a0 + s, v);
+        }
+      };
+      gadd(c.A.m, c.Ar.m, 0, (double)nv.v[0]);
 #pragma unroll
       for (int d = 0; d < DIM; d++) {
-        atomicAdd(c.A.mx[d] + s, (double)nv.v[1 + d]);
-        atomicAdd(c.A.f[d] + s, (double)nv.v[1 + DIM + d]);
-        if constexpr (NORMAL) atomicAdd(c.A.nrm[d] + s, (double)nv.v[1 + 2 * DIM + d]);
+        gadd(c.A.mx[d], c.Ar.mx[d], 1, (double)nv.v[1 + d]);
+        gadd(c.A.f[d], c.Ar.f[d], 2, (double)nv.v[1 + DIM + d]);
+        if constexpr (NORMAL) gadd(c.A.nrm[d], c.Ar.nrm[d], 3, (double)nv.v[1 + 2 * DIM + d]);
       }
     }
   });
@@ -486,9 +515,10 @@ __device__ __forceinline__ void scatter_general(const BodyCtx<PT>& c, unsigned l
 // Phase 2 for one point: map build and scatter of mapPointsToNodes
 // (explicit_usl.cpp:112-164) and the contact normal of
 // ContactHuang::generateRules (contact_huang.cpp:91).
-template <int DIM, int T, int TN, int ROW, bool NORMAL, typename PT>
+template <int DIM, int T, int TN, int ROW, bool NORMAL, bool DET, typename PT>
 __device__ __forceinline__ void map_scatter(const BodyCtx<PT>& c, int* err, unsigned long long* drift, int64_t p,
-                                            const PT* sp, const int* o, int do_g2p, double* tacc, uint8_t* touched) {
+                                            const PT* sp, const int* o, int stepping, double* tacc, uint8_t* touched,
+                                            const Split2* ks) {
   using R = PT;
   R x[3] = {R(0), R(0), R(0)};
 #pragma unroll
@@ -498,7 +528,7 @@ __device__ __forceinline__ void map_scatter(const BodyCtx<PT>& c, int* err, unsi
   if (st < 0) {
     // outside the domain: inactive from the next map build on
     // (default_points.cpp:217-219); before the first step, at once
-    c.P.active[p] = do_g2p ? 2 : 0;
+    c.P.active[p] = stepping ? 2 : 0;
     return;
   }
   if (st == 0) return;
@@ -516,15 +546,17 @@ __device__ __forceinline__ void map_scatter(const BodyCtx<PT>& c, int* err, unsi
   for (int a = 0; a < 3; a++)
 #pragma unroll
     for (int b = 0; b < 3; b++) q.V3[a][b] = V3[a][b];
-  if (regular_window<DIM>(pm, o, T))
-    scatter_regular<DIM, T, TN, NORMAL>(pm, o, q, tacc, touched);
+  if (!DET && regular_window<DIM>(pm, o, T))
+    scatter_regular<DIM, T, TN, NORMAL, DET>(pm, o, q, tacc, touched, ks);
   else
-    scatter_general<DIM, T, TN, NORMAL>(c, drift, pm, o, q, tacc, touched);
+    scatter_general<DIM, T, TN, NORMAL, DET>(c, drift, pm, o, q, tacc, touched, ks);
 }
 
-template <int DIM, typename PT, int CAP, bool NORMAL, bool SINGLE>
+template <int DIM, typename PT, int CAP, bool NORMAL, bool SINGLE, bool DET>
 __global__ void __launch_bounds__(MPMB200_FUSED_THREADS, MPMB200_FUSED_MIN_CTAS)
     k_g2p2g(const __grid_constant__ FusedLaunch<PT> fl) {
+  static_assert(!DET || sizeof(PT) == 8, "the deterministic form is FP64");
+  __shared__ Split2 ksplit[4];   // deterministic form: per-field split of the item's body
   constexpr int B = fused_bin<DIM>();
   constexpr int T = B + 3;
   constexpr int TN = fused_tile_nodes<DIM, B>();
@@ -547,7 +579,8 @@ __global__ void __launch_bounds__(MPMB200_FUSED_THREADS, MPMB200_FUSED_MIN_CTAS)
   PT* tvel = sizeof(PT) == 8 ? reinterpret_cast<PT*>(tile) : reinterpret_cast<PT*>(tile + 6 * TN);
   static_assert(sizeof(PT) == 8 || 6 * TN * (sizeof(double) + sizeof(PT)) <= 10 * TN * sizeof(double),
                 "the mixed form's velocity tiles fit in the accumulation tile");
-  uint8_t* touched = reinterpret_cast<uint8_t*>(tile + 10 * TN);
+  // after the accumulator levels (two in the deterministic form)
+  uint8_t* touched = reinterpret_cast<uint8_t*>(tile + (DET ? 20 : 10) * TN);
 
   if (threadIdx.x == 0) {
     mbar_init(bar, 1);
@@ -566,10 +599,12 @@ __global__ void __launch_bounds__(MPMB200_FUSED_THREADS, MPMB200_FUSED_MIN_CTAS)
   }
   int k = 0;
   for (int w = blockIdx.x; w < nwork; w += gridDim.x, k++) {
-    int item;
+    int item, body_of_item;
     if (SINGLE) {
+      body_of_item = fl.one_body;
       item = fl.item_off[fl.one_body] + w;
     } else {
+      body_of_item = fl.flat_body[w];
       item = fl.flat_item[w];
       const int slot = k & 1;
       const bool ahead = w + (int)gridDim.x < nwork;
@@ -603,7 +638,8 @@ __global__ void __launch_bounds__(MPMB200_FUSED_THREADS, MPMB200_FUSED_MIN_CTAS)
       __syncthreads();   // every thread has read the staged entry
       continue;
     }
-    const int do_g2p = prime ? 0 : 1;
+    const int do_g2p = (prime || !(fl.phases & 1)) ? 0 : 1;
+    const bool do_p2g = (fl.phases & 2) != 0;
     const PointsT<PT>& P = c.P;
     const Geom& g = c.g;
     const int bin = fl.work_bin[item];
@@ -677,30 +713,54 @@ __global__ void __launch_bounds__(MPMB200_FUSED_THREADS, MPMB200_FUSED_MIN_CTAS)
           act[off4 + j] = 0;
           continue;
         }
-        gather_update<DIM, T, TN, ROW>(c, fl.err, fl.drift, p, pts + offp + j, o, tvel, vref);
+        gather_update<DIM, T, TN, ROW, DET>(c, fl.err, fl.drift, p, pts + offp + j, o, tvel, vref);
       }
       __syncthreads();
     }
-    constexpr int NACC = fused_nacc(NORMAL);
-    for (int t = threadIdx.x; t < NACC * TN; t += blockDim.x) tile[t] = 0.0;
-    for (int t = threadIdx.x; t < TN; t += blockDim.x) touched[t] = 0;
-    __syncthreads();
-    for (int j = threadIdx.x; j < n; j += blockDim.x) {
-      if (act[off4 + j] != 1) continue;
-      map_scatter<DIM, T, TN, ROW, NORMAL>(c, fl.err, fl.drift, pstart + j, pts + offp + j, o, do_g2p, tile, touched);
-    }
-    __syncthreads();
-    for (int t = threadIdx.x; t < TN; t += blockDim.x) {
-      if (!touched[t]) continue;
-      const int i = o[0] + t % T, j = o[1] + (t / T) % T, k = DIM == 3 ? o[2] + t / (T * T) : 0;
-      const int64_t s = node_slot(g, i, j, k);
-      c.flags[node_block(g, i, j, k)] = 1u;
-      atomicAdd(c.A.m + s, tile[t]);
+    if (do_p2g) {
+      constexpr int NACC = fused_nacc(NORMAL);
+      for (int t = threadIdx.x; t < NACC * TN; t += blockDim.x) tile[t] = 0.0;
+      if constexpr (DET) {
+        for (int t = threadIdx.x; t < NACC * TN; t += blockDim.x) tile[10 * TN + t] = 0.0;
+        if (threadIdx.x < 4) {
+          // split of each field from the body's bounds (k_det_bounds)
+          const unsigned long long* bb = fl.bounds + 4 * (SINGLE ? fl.one_body : body_of_item);
+          ksplit[threadIdx.x] = make_split(__longlong_as_double((long long)bb[threadIdx.x]), P.n);
+        }
+      }
+      for (int t = threadIdx.x; t < TN; t += blockDim.x) touched[t] = 0;
+      __syncthreads();
+      for (int j = threadIdx.x; j < n; j += blockDim.x) {
+        if (act[off4 + j] != 1) continue;
+        // a point found outside the domain here is at a regular step's map
+        // build (inactive from the next step on: state 2), or at the priming
+        // map build before the first step (inactive at once)
+        map_scatter<DIM, T, TN, ROW, NORMAL, DET>(c, fl.err, fl.drift, pstart + j, pts + offp + j, o, prime ? 0 : 1,
+                                                   tile, touched, ksplit);
+      }
+      __syncthreads();
+      for (int t = threadIdx.x; t < TN; t += blockDim.x) {
+        if (!touched[t]) continue;
+        const int i = o[0] + t % T, j = o[1] + (t / T) % T, k = DIM == 3 ? o[2] + t / (T * T) : 0;
+        const int64_t s = node_slot(g, i, j, k);
+        c.flags[node_block(g, i, j, k)] = 1u;
+        atomicAdd(c.A.m + s, tile[t]);
 #pragma unroll
-      for (int d = 0; d < DIM; d++) {
-        atomicAdd(c.A.mx[d] + s, tile[(1 + d) * TN + t]);
-        atomicAdd(c.A.f[d] + s, tile[(4 + d) * TN + t]);
-        if (NORMAL) atomicAdd(c.A.nrm[d] + s, tile[(7 + d) * TN + t]);
+        for (int d = 0; d < DIM; d++) {
+          atomicAdd(c.A.mx[d] + s, tile[(1 + d) * TN + t]);
+          atomicAdd(c.A.f[d] + s, tile[(4 + d) * TN + t]);
+          if (NORMAL) atomicAdd(c.A.nrm[d] + s, tile[(7 + d) * TN + t]);
+        }
+        if constexpr (DET) {
+          const double* t1 = tile + 10 * TN;
+          atomicAdd(c.Ar.m + s, t1[t]);
+#pragma unroll
+          for (int d = 0; d < DIM; d++) {
+            atomicAdd(c.Ar.mx[d] + s, t1[(1 + d) * TN + t]);
+            atomicAdd(c.Ar.f[d] + s, t1[(4 + d) * TN + t]);
+            if (NORMAL) atomicAdd(c.Ar.nrm[d] + s, t1[(7 + d) * TN + t]);
+          }
+        }
       }
     }
     __syncthreads();

@@ -96,6 +96,27 @@ __global__ void __launch_bounds__(64) k_grid(const InstDev* insts, const GridBod
       if ((threadIdx.x & 31) == 0 && cnt > 0) atomicAdd(active_nodes, (unsigned long long)cnt);
     }
     if (!inside) continue;
+    if (GB[0].Ar.m != nullptr) {
+      // deterministic form: each nodal value arrived as two exactly summed
+      // parts (level 0 in A, level 1 in Ar); one fixed rounding joins them
+      for (int b = 0; b < I.nb; b++) {
+        const NodesAcc& A = GB[b].A;
+        const NodesAcc& R = GB[b].Ar;
+        A.m[s] = A.m[s] + R.m[s];
+        R.m[s] = 0.0;
+#pragma unroll
+        for (int d = 0; d < DIM; d++) {
+          A.mx[d][s] = A.mx[d][s] + R.mx[d][s];
+          A.f[d][s] = A.f[d][s] + R.f[d][s];
+          R.mx[d][s] = 0.0;
+          R.f[d][s] = 0.0;
+          if (A.nrm[0] != nullptr) {
+            A.nrm[d][s] = A.nrm[d][s] + R.nrm[d][s];
+            R.nrm[d][s] = 0.0;
+          }
+        }
+      }
+    }
     // the scatter leaves out the body force; S * (m b) summed over points is
     // the nodal mass times g (explicit_usl.cpp:150-154, b uniform)
     for (int b = 0; b < I.nb; b++) {
@@ -260,6 +281,38 @@ __device__ __forceinline__ void jaumann_update(const R L[3][3], R* s6, R G, R la
     const R rate = ((twoG * D[a][b] + (a == b ? ltr : R(0.0))) + WT[a][b]) + WT[b][a];
     s6[c] = s6[c] + dt * rate;
   }
+}
+
+// Order-independent nodal sums of the deterministic form (pre-rounded
+// two-level summation after Demmel and Nguyen, "Fast reproducible
+// floating-point summation", ARITH 2013). With M bounding every partial sum
+// of |contributions| to a node (n contributions of at most maxc each), a
+// contribution x splits exactly into q0 + q1 + e: q0 is x rounded to a
+// multiple of 2^(E0-52) with 2^E0 > 2M, q1 the remainder rounded to a
+// multiple of 2^(E1-52) with E1 = E0 - 52 + L, 2^L > 2n, and |e| <
+// 2^(E1-53). Sums of q0 (of q1) stay below 2^E0 (2^E1) in any order, so
+// every addition is exact and the two sums are the same bits whatever the
+// order; the nodal value is level0 + level1 rounded once.
+struct Split2 {
+  double s0;  // 1.5 * 2^E0
+  double s1;  // 1.5 * 2^E1
+};
+
+__device__ __forceinline__ Split2 make_split(double maxc, int64_t n) {
+  Split2 k{0.0, 0.0};
+  if (!(maxc > 0.0) || n < 1) return k;  // all contributions are zero
+  const int L = ilogb((double)n) + 2;
+  const int E0 = ilogb(maxc) + L + 1;
+  const int E1 = E0 - 52 + L;
+  k.s0 = ldexp(1.5, E0);
+  k.s1 = ldexp(1.5, E1);
+  return k;
+}
+
+__device__ __forceinline__ void presplit(double x, const Split2& k, double& q0, double& q1) {
+  q0 = __dsub_rn(__dadd_rn(k.s0, x), k.s0);
+  const double r = __dsub_rn(x, q0);
+  q1 = __dsub_rn(__dadd_rn(k.s1, r), k.s1);
 }
 
 // Exact triplet export (mpmgpu_dump_map).

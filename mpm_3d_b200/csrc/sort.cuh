@@ -43,6 +43,7 @@ struct alignas(16) BodyCtx {
   PointsT<PT> P;        // current storage order
   NodesVel V;
   NodesAcc A;
+  NodesAcc Ar;          // deterministic form: level-1 (remainder) sums, else null
   uint32_t* flags;      // node-block flags of the body's job (its first block)
   int needs_normal;     // accumulate the contact normal (first body of a contact)
   int prime;            // 1 until the body's first scatter has run
@@ -292,6 +293,42 @@ __global__ void k_sort_flip(const BatchHdr* hdr, BodyCtx<PT>* bodies) {
     const PointsT<PT> t = bodies[b].P;
     bodies[b].P = bodies[b].Palt;
     bodies[b].Palt = t;
+  }
+}
+
+// Bounds of the contributions of each body's points to one node, for the
+// deterministic form's two-level split (make_split): bounds[4 b + k] (the
+// bits of a non-negative double, so that an integer maximum orders them,
+// and a maximum is the same whatever the order) for k = 0 mass (S m <= m),
+// 1 momentum (m max_d |v_d|), 2 internal force (V 3 max|sigma| max|grad S|),
+// 3 contact normal (m max|grad S|), with |grad S| <= max(2 / extent, 1 / h):
+// 2 / extent for the corner-sampled map (sG times at most 2 x 2 x 2), 1 / h
+// point-sampled.
+template <int DIM>
+__global__ void k_det_bounds(const BatchHdr* hdr, const BodyCtx<double>* bodies, const int64_t* point_end,
+                             unsigned long long* bounds) {
+  const int64_t total = hdr->points;
+  const int nb = hdr->nbodies;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < total; q += stride) {
+    const int b = find_range(point_end, nb, q);
+    const BodyCtx<double>& B = bodies[b];
+    const int64_t p = q - B.point_off;
+    if (B.P.active[p] == 0) continue;
+    double hmin = B.g.h[0];
+#pragma unroll
+    for (int d = 1; d < DIM; d++) hmin = fmin(hmin, B.g.h[d]);
+    const double gmax = fmax(2.0 / B.P.ext[p], 1.0 / hmin);
+    const double m = B.P.m[p];
+    double vmax = 0.0;
+#pragma unroll
+    for (int d = 0; d < DIM; d++) vmax = fmax(vmax, fabs(B.P.v[d][p]));
+    double smax = 0.0;
+#pragma unroll
+    for (int c = 0; c < 6; c++) smax = fmax(smax, fabs(B.P.s[c][p]));
+    const double c4[4] = {m, m * vmax, B.P.vol[p] * 3.0 * smax * gmax, m * gmax};
+#pragma unroll
+    for (int k = 0; k < 4; k++) atomicMax(bounds + 4 * b + k, (unsigned long long)__double_as_longlong(c4[k]));
   }
 }
 

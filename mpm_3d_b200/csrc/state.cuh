@@ -79,6 +79,7 @@ struct InstDev {
 // What the grid update needs of a body.
 struct GridBody {
   NodesAcc A;
+  NodesAcc Ar;       // deterministic form: level-1 (remainder) sums, else null
   NodesVel V;
   NodesAcc snap;     // debug copies of m, mx_t, f after the update (or null)
   int has_boundary;

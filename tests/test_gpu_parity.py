@@ -77,11 +77,11 @@ def restated_lib():
     bridge.build_restated()
 
 
-def _step_parity(name, sort_interval=0):
+def _step_parity(name, sort_interval=0, mode="fp64"):
     make, steps = CASES[name]
     case = make()
     ref = bridge.RestatedJob(case)
-    gpu = GPUExplicitUSL(case, keep_debug=True, sort_interval=sort_interval)
+    gpu = GPUExplicitUSL(case, keep_debug=True, sort_interval=sort_interval, mode=mode)
     worst = {}
     for s in range(steps):
         ref.step(1)
