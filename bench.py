@@ -642,7 +642,7 @@ def main():
     ap.add_argument("--steps", type=int, default=0, help="timed steps (default: the workload's own step count)")
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--workload", default="ensemble", choices=["ensemble", "collision", "column", "serving"])
-    ap.add_argument("--form", default="fp64", choices=["fp64", "mixed"], help="form of the single-job workloads")
+    ap.add_argument("--form", default="fp64", choices=["fp64", "mixed", "fp64_deterministic"], help="form of the single-job workloads")
     ap.add_argument("--plain-steps", type=int, default=10, help="timed steps per job of the plain FP64 path")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--jobs", type=int, default=0, help="ensemble: only the first JOBS jobs (profiling cases)")
