@@ -119,15 +119,18 @@ __host__ __device__ constexpr size_t fused_smem_bytes() {
          fused_tile_nodes<DIM, fused_bin<DIM>()>();
 }
 
-// Threads per CTA and minimum resident CTAs per SM of the fused kernel
-// (2 CTAs of 256 threads: 128 registers per thread).
-#ifndef MPMB200_FUSED_THREADS
-#define MPMB200_FUSED_THREADS 256
-#endif
-#ifndef MPMB200_FUSED_MIN_CTAS
-#define MPMB200_FUSED_MIN_CTAS 2
-#endif
-constexpr int kFusedThreads = MPMB200_FUSED_THREADS;
+// Threads per CTA and the resident CTAs per SM the register budget is sized
+// for (128 registers per thread either way): items of 256 points run on
+// 128-thread CTAs, four per SM, so that a barrier waits on fewer warps;
+// larger items on 256-thread CTAs, two per SM.
+template <int CAP>
+__host__ __device__ constexpr int fused_threads() {
+  return CAP <= 256 ? 128 : 256;
+}
+template <int CAP>
+__host__ __device__ constexpr int fused_min_ctas() {
+  return CAP <= 256 ? 4 : 2;
+}
 
 // Entry k (0..2) of a 3-array without indexing it by a variable (which
 // would move the array to local memory).
@@ -553,7 +556,7 @@ __device__ __forceinline__ void map_scatter(const BodyCtx<PT>& c, int* err, unsi
 }
 
 template <int DIM, typename PT, int CAP, bool NORMAL, bool SINGLE, bool DET>
-__global__ void __launch_bounds__(MPMB200_FUSED_THREADS, MPMB200_FUSED_MIN_CTAS)
+__global__ void __launch_bounds__(fused_threads<CAP>(), fused_min_ctas<CAP>())
     k_g2p2g(const __grid_constant__ FusedLaunch<PT> fl) {
   static_assert(!DET || sizeof(PT) == 8, "the deterministic form is FP64");
   __shared__ Split2 ksplit[4];   // deterministic form: per-field split of the item's body
