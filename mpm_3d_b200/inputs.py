@@ -308,8 +308,10 @@ def read_points_file(path: str, dim: int) -> Tuple[np.ndarray, ...]:
 
 
 def write_case(case: Case, directory: str, solver_class: str = "ExplicitUSL", points_class: str = "DefaultPoints",
-               threads: Optional[int] = None) -> str:
-    """Writes ``<name>.cfg`` and the ``.points`` files; returns the cfg path."""
+               threads: Optional[int] = None, solver_extra: Sequence[int] = ()) -> str:
+    """Writes ``<name>.cfg`` and the ``.points`` files; returns the cfg path.
+    ``solver_extra`` appends solver int-properties (the GPU solver's
+    write-back interval and form)."""
     os.makedirs(directory, exist_ok=True)
     lines = ["job", "{", f"    dt = {_fmt(case.dt)}", "    t = 0", f"    TYPE = {case.dim}"]
     if threads is not None:
@@ -323,8 +325,8 @@ def write_case(case: Case, directory: str, solver_class: str = "ExplicitUSL", po
         g = ",".join(_fmt(v) for v in case.gravity[:case.dim])
         lines += ["driver", "{", '    class = "UserDefinedGravityDriver"', f"    properties = {{{_fmt(stop)},{g}}}",
                   "}", ""]
-    lines += ["solver", "{", f'    class = "{solver_class}"', f"    int-properties = {{{case.cpdi},{case.contact_spec}}}",
-              "}", ""]
+    sprops = ",".join(str(v) for v in [case.cpdi, case.contact_spec, *solver_extra])
+    lines += ["solver", "{", f'    class = "{solver_class}"', f"    int-properties = {{{sprops}}}", "}", ""]
     lines += ["grid", "{", '    class = "CartesianLinear"',
               "    properties = {" + ",".join(_fmt(case.L[i]) for i in range(case.dim)) + "}",
               "    int-properties = {" + ",".join(str(case.N[i]) for i in range(case.dim)) + "}", "}", ""]

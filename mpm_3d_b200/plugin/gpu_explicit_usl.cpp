@@ -36,13 +36,19 @@ void GPUExplicitUSL::check(mpmgpu_status s, const char* what) {
   exit(0);
 }
 
-// explicit_usl.cpp:25-44, plus the optional write-back interval.
+// explicit_usl.cpp:25-44, plus the optional write-back interval and form
+// (0 FP64, 1 deterministic FP64, 2 mixed FP32/FP64; mpmgpu_mode).
 void GPUExplicitUSL::init(Job* job) {
   if (int_props.size() >= 1) cpdi_spec = int_props[0];
   if (int_props.size() >= 2) contact_spec = int_props[1];
   if (int_props.size() >= 3) writeback_interval = int_props[2];
-  printf("Solver properties (cpdi_spec = %i, contact_spec = %i, writeback = %i).\n", cpdi_spec, contact_spec,
-         writeback_interval);
+  if (int_props.size() >= 4) mode = int_props[3];
+  if (mode < 0 || mode > 2) {
+    std::cerr << "GPUExplicitUSL: form " << mode << " is not 0 (FP64), 1 (deterministic) or 2 (mixed)." << std::endl;
+    exit(0);
+  }
+  printf("Solver properties (cpdi_spec = %i, contact_spec = %i, writeback = %i, form = %i).\n", cpdi_spec,
+         contact_spec, writeback_interval, mode);
   std::cout << "Solver Initialized." << std::endl;
 }
 
@@ -63,7 +69,7 @@ void GPUExplicitUSL::setUp(Job* job) {
   cfg.dt = job->dt;
   cfg.cpdi_spec = cpdi_spec;
   cfg.contact_spec = contact_spec;
-  cfg.mode = MPMGPU_MODE_FP64;
+  cfg.mode = mode;
   cfg.device = 0;
   cfg.keep_debug = 1;  // node and contact fields are written in frames
   cfg.sort_interval = 0;
@@ -186,9 +192,12 @@ void GPUExplicitUSL::writeBack(Job* job) {
     vec3(MPMGPU_P_U, pts->u);
     vec3(MPMGPU_P_X_T, pts->x_t);
     vec3(MPMGPU_P_MX_T, pts->mx_t);
-    check(mpmgpu_download_points(handle, id, MPMGPU_P_L, buf.data()), "mpmgpu_download_points");
-    for (int i = 0; i < n; i++)
-      for (int k = 0; k < 9; k++) pts->L[i][k] = buf[9 * i + k];
+    if (mode != MPMGPU_MODE_MIXED) {
+      // the velocity gradient is kept on the device in the FP64 forms only
+      check(mpmgpu_download_points(handle, id, MPMGPU_P_L, buf.data()), "mpmgpu_download_points");
+      for (int i = 0; i < n; i++)
+        for (int k = 0; k < 9; k++) pts->L[i][k] = buf[9 * i + k];
+    }
     check(mpmgpu_download_points(handle, id, MPMGPU_P_T, buf.data()), "mpmgpu_download_points");
     for (int i = 0; i < n; i++)
       for (int k = 0; k < 9; k++) pts->T[i][k] = buf[9 * i + k];

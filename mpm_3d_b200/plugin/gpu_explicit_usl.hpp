@@ -34,6 +34,7 @@ class GPUExplicitUSL : public Solver {
   int cpdi_spec = 1;
   int contact_spec = Contact::IMPLICIT;
   int writeback_interval = 0;
+  int mode = 0;  // mpmgpu_mode: 0 FP64, 1 deterministic FP64, 2 mixed
 
   void init(Job* job) override;
   void step(Job* job) override;

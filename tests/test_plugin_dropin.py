@@ -56,3 +56,20 @@ def test_dropin_matches_reference_solver(name):
                 assert_close(gpu.nodes(b, f), ref.nodes(b, f), FP64_TOL, f"{name} step {s} node {f}")
         for c in range(len(case.contacts)):
             assert_close(gpu.contact(c, "force"), ref.contact(c, "force"), FP64_TOL, f"{name} step {s} contact")
+
+
+@needs_gpu_harness
+@pytest.mark.gpu
+@pytest.mark.parametrize("form,tol", [(1, FP64_TOL), (2, 1e-4)])
+def test_dropin_forms_from_the_config(form, tol):
+    """The form is the fourth solver int-property: 1 deterministic FP64
+    (same tolerance as FP64), 2 mixed FP32/FP64 (1e-4)."""
+    case = inputs.two_body_collision_3d(16, steps=8, gap=0.01)
+    ref = bridge.ReferenceJob(inputs.write_case(case, tempfile.mkdtemp()), build="parity")
+    gpu = bridge.ReferenceJob(inputs.write_case(case, tempfile.mkdtemp(), solver_class="GPUExplicitUSL",
+                                                solver_extra=(0, form)), build="gpu")
+    ref.step(8)
+    gpu.step(8)
+    for b in range(len(case.bodies)):
+        for f in ("x", "u", "x_t", "T", "v"):
+            assert_close(gpu.points(b, f), ref.points(b, f), tol, f"form {form} point {f}", field_floor(case, f))
