@@ -17,6 +17,7 @@ Workloads (seeded synthetic inputs, mpm_3d_b200.inputs):
              beside it: the same batch in FP64, the plain FP64 path (one
              handle per job, jobs one after another) and the mixed form's
              error against FP64 on every 8th job.
+  blockdrop2d  the 2D block drop, 20x20 grid, 144 points, 2000 steps (CPU-sized)
   collision  two 0.25 m cubes colliding, 128^3 grid, 524,288 points, ContactHuang (FP64)
   column     column collapse, 256x256x128 grid, 3,145,728 points (FP64)
   serving    Poisson request stream at 100/s (block drops with N in [16,128],
@@ -89,6 +90,8 @@ def make_workload(name: str, rank: int = 0):
         return inputs.column_collapse_3d(1)
     if name == "ensemble":
         return inputs.block_drop_ensemble(ENSEMBLE_JOBS, seed=ENSEMBLE_SEED + rank)
+    if name == "blockdrop2d":
+        return inputs.block_drop_2d()
     raise SystemExit(f"unknown workload {name}")
 
 
@@ -269,11 +272,11 @@ def run_reference_arm(args, rank, world):
         else:
             cases = make_workload("ensemble")
         steps = max(1, min(args.steps, args.ref_steps))
-        cpu = cpu_ensemble_sample(cases, steps)
+        cpu = cpu_ensemble_sample(cases, steps, args.warmup)
         value = cpu["value"]
         line = {
             "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": steps, "warmup": 1, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+            "steps": steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": f"synthetic (block_drop_ensemble seed {ENSEMBLE_SEED})",
             "config": {"workload": args.workload if args.workload == "serving" else f"ensemble{ENSEMBLE_JOBS}",
                        "jobs": len(cases), "points": sum(c.n_points for c in cases)},
@@ -594,20 +597,20 @@ def run_e2e_batch(cases, steps: int, device: int, cap: int, sort_interval: int):
             "steps": steps, "seconds": dt}
 
 
-def cpu_ensemble_sample(cases, steps: int):
+def cpu_ensemble_sample(cases, steps: int, warmup: int = 1):
     """The reference's ThreadPoolExplicitUSL on 16 of the jobs (every 32nd),
-    one after another, `steps` steps each after one warm-up step."""
+    one after another, `steps` steps each after `warmup` warm-up steps."""
     threads = os.cpu_count() or 1
     ids = list(range(0, len(cases), max(1, len(cases) // 16)))[:16]
     pts = 0
     sec = 0.0
     for i in ids:
-        dt = cpu_reference_run(cases[i], steps, 1, threads)
+        dt = cpu_reference_run(cases[i], steps, warmup, threads)
         sec += dt * steps
         pts += cases[i].n_points * steps
     return {"value": pts / sec, "unit": UNIT, "cores": threads, "kind": "reference",
             "sample": f"jobs {ids[0]}..{ids[-1]} step {ids[1] - ids[0] if len(ids) > 1 else 1} "
-                      f"({len(ids)} jobs, {sum(cases[i].n_points for i in ids)} points), {steps} steps each after 1 "
+                      f"({len(ids)} jobs, {sum(cases[i].n_points for i in ids)} points), {steps} steps each after {warmup} "
                       f"warm-up, in sequence, ThreadPoolExplicitUSL+ThreadPoolPoints, threads={threads}"}
 
 
@@ -641,7 +644,8 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=0, help="timed steps (default: the workload's own step count)")
     ap.add_argument("--warmup", type=int, default=10)
-    ap.add_argument("--workload", default="ensemble", choices=["ensemble", "collision", "column", "serving"])
+    ap.add_argument("--workload", default="ensemble",
+                    choices=["ensemble", "collision", "column", "serving", "blockdrop2d"])
     ap.add_argument("--form", default="fp64", choices=["fp64", "mixed", "fp64_deterministic"], help="form of the single-job workloads")
     ap.add_argument("--plain-steps", type=int, default=10, help="timed steps per job of the plain FP64 path")
     ap.add_argument("--no-plain", action="store_true")
