@@ -309,26 +309,51 @@ __global__ void k_det_bounds(const BatchHdr* hdr, const BodyCtx<double>* bodies,
                              unsigned long long* bounds) {
   const int64_t total = hdr->points;
   const int nb = hdr->nbodies;
-  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < total; q += stride) {
-    const int b = find_range(point_end, nb, q);
-    const BodyCtx<double>& B = bodies[b];
-    const int64_t p = q - B.point_off;
-    if (B.P.active[p] == 0) continue;
-    double hmin = B.g.h[0];
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  // a warp takes 32 consecutive points (mostly of one body) per round, so
+  // that one atomic per field and warp carries the warp's maximum
+  for (int64_t base = ((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5) * 32; base < total;
+       base += warps * 32) {
+    const int64_t q = base + lane;
+    int b = -1;
+    double c4[4] = {0.0, 0.0, 0.0, 0.0};
+    if (q < total) {
+      b = find_range(point_end, nb, q);
+      const BodyCtx<double>& B = bodies[b];
+      const int64_t p = q - B.point_off;
+      if (B.P.active[p] != 0) {
+        double hmin = B.g.h[0];
 #pragma unroll
-    for (int d = 1; d < DIM; d++) hmin = fmin(hmin, B.g.h[d]);
-    const double gmax = fmax(2.0 / B.P.ext[p], 1.0 / hmin);
-    const double m = B.P.m[p];
-    double vmax = 0.0;
+        for (int d = 1; d < DIM; d++) hmin = fmin(hmin, B.g.h[d]);
+        const double gmax = fmax(2.0 / B.P.ext[p], 1.0 / hmin);
+        const double m = B.P.m[p];
+        double vmax = 0.0;
 #pragma unroll
-    for (int d = 0; d < DIM; d++) vmax = fmax(vmax, fabs(B.P.v[d][p]));
-    double smax = 0.0;
+        for (int d = 0; d < DIM; d++) vmax = fmax(vmax, fabs(B.P.v[d][p]));
+        double smax = 0.0;
 #pragma unroll
-    for (int c = 0; c < 6; c++) smax = fmax(smax, fabs(B.P.s[c][p]));
-    const double c4[4] = {m, m * vmax, B.P.vol[p] * 3.0 * smax * gmax, m * gmax};
+        for (int c = 0; c < 6; c++) smax = fmax(smax, fabs(B.P.s[c][p]));
+        c4[0] = m;
+        c4[1] = m * vmax;
+        c4[2] = B.P.vol[p] * 3.0 * smax * gmax;
+        c4[3] = m * gmax;
+      }
+    }
+    const int b0 = __shfl_sync(0xffffffffu, b, 0);
+    const bool same = b == b0;
 #pragma unroll
-    for (int k = 0; k < 4; k++) atomicMax(bounds + 4 * b + k, (unsigned long long)__double_as_longlong(c4[k]));
+    for (int k = 0; k < 4; k++) {
+      // non-negative doubles order like their bit patterns
+      unsigned long long v = same ? (unsigned long long)__double_as_longlong(c4[k]) : 0ull;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long w = __shfl_xor_sync(0xffffffffu, v, o);
+        v = w > v ? w : v;
+      }
+      if (lane == 0 && b0 >= 0) atomicMax(bounds + 4 * b0 + k, v);
+      if (!same && b >= 0) atomicMax(bounds + 4 * b + k, (unsigned long long)__double_as_longlong(c4[k]));
+    }
   }
 }
 
