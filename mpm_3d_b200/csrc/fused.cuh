@@ -178,35 +178,46 @@ struct GatherSum {
   R L[3][3] = {{R(0), R(0), R(0)}, {R(0), R(0), R(0)}, {R(0), R(0), R(0)}};
 };
 
-// The common window: two nodes per axis, inside the staged tile.
+// Span bits of a window: bit d set when axis d spans three nodes.
 template <int DIM, typename R>
-__device__ __forceinline__ bool regular_window(const PointMapT<R>& pm, const int* o, int T) {
-  bool r = true;
+__device__ __forceinline__ int span_bits(const PointMapT<R>& pm) {
+  int b = 0;
 #pragma unroll
-  for (int d = 0; d < DIM; d++) r = r && pm.ax[d].span == 2 && pm.ax[d].base >= o[d] && pm.ax[d].base + 2 <= o[d] + T;
-  return r;
+  for (int d = 0; d < DIM; d++) b |= (pm.ax[d].span == 3 ? 1 : 0) << d;
+  return b;
 }
 
-// Gather over a regular (2^dim-node, in-tile) window: straight-line code.
-template <int DIM, int T, int TN, typename R>
-__device__ __forceinline__ GatherSum<R> gather_regular(const PointMapT<R>& pm, const int* o, const R* tvel) {
+// Gather over a box of K0 x K1 (x K2) nodes from the window's base, all
+// inside the staged tile: straight-line code. A warp runs the box of the
+// union of its lanes' spans, so lanes whose window is narrower along an
+// axis skip that axis' third node (their W and G there are zero anyway).
+template <int DIM, int T, int TN, int K0, int K1, int K2, typename R>
+__device__ __forceinline__ GatherSum<R> gather_box(const PointMapT<R>& pm, const int* o, const R* tvel) {
   GatherSum<R> gs;
   const int t0 = (pm.ax[0].base - o[0]) + T * ((pm.ax[1].base - o[1]) + (DIM == 3 ? T * (pm.ax[2].base - o[2]) : 0));
-  const R W0s[2] = {pm.sS * pm.ax[0].W[0], pm.sS * pm.ax[0].W[1]};
-  const R G0g[2] = {pm.sG * pm.ax[0].G[0], pm.sG * pm.ax[0].G[1]};
-  const R W0g[2] = {pm.sG * pm.ax[0].W[0], pm.sG * pm.ax[0].W[1]};
-  constexpr int K2 = DIM == 3 ? 2 : 1;
+  R W0s[3], G0g[3], W0g[3];
 #pragma unroll
-  for (int k2 = 0; k2 < K2; k2++) {
+  for (int k = 0; k < K0; k++) {
+    W0s[k] = pm.sS * pm.ax[0].W[k];
+    G0g[k] = pm.sG * pm.ax[0].G[k];
+    W0g[k] = pm.sG * pm.ax[0].W[k];
+  }
+  const bool third0 = pm.ax[0].span == 3, third1 = pm.ax[1].span == 3, third2 = DIM == 3 && pm.ax[2].span == 3;
+  constexpr int KZ = DIM == 3 ? K2 : 1;
+#pragma unroll
+  for (int k2 = 0; k2 < KZ; k2++) {
+    if (k2 == 2 && !third2) continue;
     const R wz = DIM == 3 ? pm.ax[2].W[k2] : R(1);
     const R gz = DIM == 3 ? pm.ax[2].G[k2] : R(0);
 #pragma unroll
-    for (int k1 = 0; k1 < 2; k1++) {
+    for (int k1 = 0; k1 < K1; k1++) {
+      if (k1 == 2 && !third1) continue;
       const R W12 = pm.ax[1].W[k1] * wz;
       const R G1W2 = pm.ax[1].G[k1] * wz;
       const R W1G2 = pm.ax[1].W[k1] * gz;
 #pragma unroll
-      for (int k0 = 0; k0 < 2; k0++) {
+      for (int k0 = 0; k0 < K0; k0++) {
+        if (k0 == 2 && !third0) continue;
         const int t = t0 + k0 + T * (k1 + T * k2);
         const R S = W0s[k0] * W12;
         const R gr0 = G0g[k0] * W12, gr1 = W0g[k0] * G1W2, gr2 = W0g[k0] * W1G2;
@@ -223,6 +234,29 @@ __device__ __forceinline__ GatherSum<R> gather_regular(const PointMapT<R>& pm, c
     }
   }
   return gs;
+}
+
+template <int DIM, int T, int TN, typename R>
+__device__ __forceinline__ GatherSum<R> gather_box_any(const PointMapT<R>& pm, const int* o, const R* tvel, int mask) {
+  if constexpr (DIM == 3) {
+    switch (mask) {
+      case 0: return gather_box<DIM, T, TN, 2, 2, 2>(pm, o, tvel);
+      case 1: return gather_box<DIM, T, TN, 3, 2, 2>(pm, o, tvel);
+      case 2: return gather_box<DIM, T, TN, 2, 3, 2>(pm, o, tvel);
+      case 3: return gather_box<DIM, T, TN, 3, 3, 2>(pm, o, tvel);
+      case 4: return gather_box<DIM, T, TN, 2, 2, 3>(pm, o, tvel);
+      case 5: return gather_box<DIM, T, TN, 3, 2, 3>(pm, o, tvel);
+      case 6: return gather_box<DIM, T, TN, 2, 3, 3>(pm, o, tvel);
+      default: return gather_box<DIM, T, TN, 3, 3, 3>(pm, o, tvel);
+    }
+  } else {
+    switch (mask & 3) {
+      case 0: return gather_box<DIM, T, TN, 2, 2, 2>(pm, o, tvel);
+      case 1: return gather_box<DIM, T, TN, 3, 2, 2>(pm, o, tvel);
+      case 2: return gather_box<DIM, T, TN, 2, 3, 2>(pm, o, tvel);
+      default: return gather_box<DIM, T, TN, 3, 3, 2>(pm, o, tvel);
+    }
+  }
 }
 
 // Gather over any window (three-node spans, nodes outside the tile).
@@ -311,11 +345,15 @@ __device__ __forceinline__ void gather_update(const BodyCtx<PT>& c, int* err, un
   const int st = build_map<DIM>(c.g, c.mc, c.sp.cpdi, x, sp[kFext * ROW], pm, err);
   GatherSum<R> gs;
   if (st > 0) {
-    // the deterministic form takes one arithmetic for every window: the
-    // straight-line path rounds differently, and whether a window qualifies
-    // depends on the binning
-    if (!DET && regular_window<DIM>(pm, o, T))
-      gs = gather_regular<DIM, T, TN>(pm, o, tvel);
+    // windows inside the tile take the straight-line box of the union of
+    // the warp's spans; the deterministic form takes one arithmetic for
+    // every window (the straight-line path rounds differently, and whether
+    // a window is inside the tile depends on the binning)
+    const bool in = !DET && window_in_tile<DIM>(pm, o, T);
+    const unsigned am = __activemask();
+    const unsigned inm = __ballot_sync(am, in);
+    if (in)
+      gs = gather_box_any<DIM, T, TN>(pm, o, tvel, __reduce_or_sync(inm, span_bits<DIM>(pm)));
     else
       gs = gather_general<DIM, T, TN>(c, drift, pm, o, tvel, vref);
     if constexpr (sizeof(PT) == 4) {
@@ -404,23 +442,30 @@ struct ScatterSrc {
   R V3[3][3];
 };
 
-// Scatter over a regular (2^dim-node, in-tile) window. The nodal force
-// -V sigma . grad S is evaluated per row of the window as
-// -(G0 A + W0 B) with A, B the row factors of the separable gradient.
-template <int DIM, int T, int TN, bool NORMAL, bool DET, typename R>
-__device__ __forceinline__ void scatter_regular(const PointMapT<R>& pm, const int* o, const ScatterSrc<R>& q,
-                                                double* tacc, uint8_t* touched, const Split2* ks) {
+// Scatter over a box of K0 x K1 (x K2) nodes inside the tile (as
+// gather_box). The nodal force -V sigma . grad S is evaluated per row of the
+// box as -(G0 A + W0 B) with A, B the row factors of the separable gradient.
+template <int DIM, int T, int TN, bool NORMAL, bool DET, int K0, int K1, int K2, typename R>
+__device__ __forceinline__ void scatter_box(const PointMapT<R>& pm, const int* o, const ScatterSrc<R>& q,
+                                            double* tacc, uint8_t* touched, const Split2* ks) {
   const int t0 = (pm.ax[0].base - o[0]) + T * ((pm.ax[1].base - o[1]) + (DIM == 3 ? T * (pm.ax[2].base - o[2]) : 0));
-  const R W0s[2] = {pm.sS * pm.ax[0].W[0], pm.sS * pm.ax[0].W[1]};
-  const R G0g[2] = {pm.sG * pm.ax[0].G[0], pm.sG * pm.ax[0].G[1]};
-  const R W0g[2] = {pm.sG * pm.ax[0].W[0], pm.sG * pm.ax[0].W[1]};
-  constexpr int K2 = DIM == 3 ? 2 : 1;
+  R W0s[3], G0g[3], W0g[3];
 #pragma unroll
-  for (int k2 = 0; k2 < K2; k2++) {
+  for (int k = 0; k < K0; k++) {
+    W0s[k] = pm.sS * pm.ax[0].W[k];
+    G0g[k] = pm.sG * pm.ax[0].G[k];
+    W0g[k] = pm.sG * pm.ax[0].W[k];
+  }
+  const bool third0 = pm.ax[0].span == 3, third1 = pm.ax[1].span == 3, third2 = DIM == 3 && pm.ax[2].span == 3;
+  constexpr int KZ = DIM == 3 ? K2 : 1;
+#pragma unroll
+  for (int k2 = 0; k2 < KZ; k2++) {
+    if (k2 == 2 && !third2) continue;
     const R wz = DIM == 3 ? pm.ax[2].W[k2] : R(1);
     const R gz = DIM == 3 ? pm.ax[2].G[k2] : R(0);
 #pragma unroll
-    for (int k1 = 0; k1 < 2; k1++) {
+    for (int k1 = 0; k1 < K1; k1++) {
+      if (k1 == 2 && !third1) continue;
       const R W12 = pm.ax[1].W[k1] * wz;
       const R G1W2 = pm.ax[1].G[k1] * wz;
       const R W1G2 = pm.ax[1].W[k1] * gz;
@@ -434,7 +479,8 @@ __device__ __forceinline__ void scatter_regular(const PointMapT<R>& pm, const in
         if (DIM == 3) Bf[d] += q.V3[d][2] * W1G2;
       }
 #pragma unroll
-      for (int k0 = 0; k0 < 2; k0++) {
+      for (int k0 = 0; k0 < K0; k0++) {
+        if (k0 == 2 && !third0) continue;
         const int t = t0 + k0 + T * (k1 + T * k2);
         touched[t] = 1;
         NodeVals<DIM, NORMAL, R> nv;
@@ -451,6 +497,30 @@ __device__ __forceinline__ void scatter_regular(const PointMapT<R>& pm, const in
         }
         tile_add_node<DIM, NORMAL, TN, DET>(tacc, t, nv, ks);
       }
+    }
+  }
+}
+
+template <int DIM, int T, int TN, bool NORMAL, bool DET, typename R>
+__device__ __forceinline__ void scatter_box_any(const PointMapT<R>& pm, const int* o, const ScatterSrc<R>& q,
+                                                double* tacc, uint8_t* touched, const Split2* ks, int mask) {
+  if constexpr (DIM == 3) {
+    switch (mask) {
+      case 0: return scatter_box<DIM, T, TN, NORMAL, DET, 2, 2, 2>(pm, o, q, tacc, touched, ks);
+      case 1: return scatter_box<DIM, T, TN, NORMAL, DET, 3, 2, 2>(pm, o, q, tacc, touched, ks);
+      case 2: return scatter_box<DIM, T, TN, NORMAL, DET, 2, 3, 2>(pm, o, q, tacc, touched, ks);
+      case 3: return scatter_box<DIM, T, TN, NORMAL, DET, 3, 3, 2>(pm, o, q, tacc, touched, ks);
+      case 4: return scatter_box<DIM, T, TN, NORMAL, DET, 2, 2, 3>(pm, o, q, tacc, touched, ks);
+      case 5: return scatter_box<DIM, T, TN, NORMAL, DET, 3, 2, 3>(pm, o, q, tacc, touched, ks);
+      case 6: return scatter_box<DIM, T, TN, NORMAL, DET, 2, 3, 3>(pm, o, q, tacc, touched, ks);
+      default: return scatter_box<DIM, T, TN, NORMAL, DET, 3, 3, 3>(pm, o, q, tacc, touched, ks);
+    }
+  } else {
+    switch (mask & 3) {
+      case 0: return scatter_box<DIM, T, TN, NORMAL, DET, 2, 2, 2>(pm, o, q, tacc, touched, ks);
+      case 1: return scatter_box<DIM, T, TN, NORMAL, DET, 3, 2, 2>(pm, o, q, tacc, touched, ks);
+      case 2: return scatter_box<DIM, T, TN, NORMAL, DET, 2, 3, 2>(pm, o, q, tacc, touched, ks);
+      default: return scatter_box<DIM, T, TN, NORMAL, DET, 3, 3, 2>(pm, o, q, tacc, touched, ks);
     }
   }
 }
@@ -549,8 +619,13 @@ __device__ __forceinline__ void map_scatter(const BodyCtx<PT>& c, int* err, unsi
   for (int a = 0; a < 3; a++)
 #pragma unroll
     for (int b = 0; b < 3; b++) q.V3[a][b] = V3[a][b];
-  if (!DET && regular_window<DIM>(pm, o, T))
-    scatter_regular<DIM, T, TN, NORMAL, DET>(pm, o, q, tacc, touched, ks);
+  // as in gather_update: the union box of the warp for windows inside the
+  // tile, the general path otherwise (and always in the deterministic form)
+  const bool in = !DET && window_in_tile<DIM>(pm, o, T);
+  const unsigned am = __activemask();
+  const unsigned inm = __ballot_sync(am, in);
+  if (in)
+    scatter_box_any<DIM, T, TN, NORMAL, DET>(pm, o, q, tacc, touched, ks, __reduce_or_sync(inm, span_bits<DIM>(pm)));
   else
     scatter_general<DIM, T, TN, NORMAL, DET>(c, drift, pm, o, q, tacc, touched, ks);
 }
