@@ -79,9 +79,33 @@ __host__ __device__ constexpr int cap_row() {
 // Number of accumulated values per node: m, mx (3), f (3), contact normal (3).
 __host__ __device__ constexpr int fused_nacc(bool normal) { return normal ? 10 : 7; }
 
+// Slots of the node tile (T = B + 3 nodes per axis). In 3D the x-rows of
+// four consecutive z planes share one y row of 4T slots: slot = x + 4T y +
+// T (z mod 4) + 4T^2 (z div 4). A warp's lanes sit in distinct cells, x
+// fastest: the 16 lanes of a half-warp (4 x 4 cells of one z plane) read
+// and add at x + 4T y, which with 4T = 28 = 12 (mod 16) falls on 16
+// distinct 8-byte bank pairs (rows of T = 7 slots put lanes two rows apart
+// on the same banks). Slots with z >= T stay unused. 2D: x + T y.
+template <int DIM, int T>
+struct TileLayout {
+  static constexpr int ZG = DIM == 3 ? 4 : 1;       // z planes per row
+  static constexpr int RL = ZG * T;                 // slots per y row
+  static constexpr int PG = RL * T;                 // slots per group of ZG planes
+  static constexpr int N = DIM == 3 ? PG * ((T + ZG - 1) / ZG) : T * T;
+  __host__ __device__ static constexpr int zoff(int z) { return DIM == 3 ? T * (z % ZG) + PG * (z / ZG) : 0; }
+  __host__ __device__ static constexpr int slot(int x, int y, int z) { return x + RL * y + zoff(z); }
+  // node of slot t (relative to the tile origin); false for unused slots
+  __device__ static bool node(int t, int& x, int& y, int& z) {
+    x = t % T;
+    y = (t / RL) % T;
+    z = DIM == 3 ? (t / T) % ZG + ZG * (t / PG) : 0;
+    return z < (DIM == 3 ? T : 1);
+  }
+};
+
 template <int DIM, int B>
 __host__ __device__ constexpr int fused_tile_nodes() {
-  return DIM == 3 ? (B + 3) * (B + 3) * (B + 3) : (B + 3) * (B + 3);
+  return TileLayout<DIM, B + 3>::N;
 }
 
 template <int DIM>
@@ -194,7 +218,9 @@ __device__ __forceinline__ int span_bits(const PointMapT<R>& pm) {
 template <int DIM, int T, int TN, int K0, int K1, int K2, typename R>
 __device__ __forceinline__ GatherSum<R> gather_box(const PointMapT<R>& pm, const int* o, const R* tvel) {
   GatherSum<R> gs;
-  const int t0 = (pm.ax[0].base - o[0]) + T * ((pm.ax[1].base - o[1]) + (DIM == 3 ? T * (pm.ax[2].base - o[2]) : 0));
+  using TL = TileLayout<DIM, T>;
+  const int txy = (pm.ax[0].base - o[0]) + TL::RL * (pm.ax[1].base - o[1]);
+  const int bz = DIM == 3 ? pm.ax[2].base - o[2] : 0;
   R W0s[3], G0g[3], W0g[3];
 #pragma unroll
   for (int k = 0; k < K0; k++) {
@@ -218,7 +244,7 @@ __device__ __forceinline__ GatherSum<R> gather_box(const PointMapT<R>& pm, const
 #pragma unroll
       for (int k0 = 0; k0 < K0; k0++) {
         if (k0 == 2 && !third0) continue;
-        const int t = t0 + k0 + T * (k1 + T * k2);
+        const int t = txy + k0 + TL::RL * k1 + TL::zoff(bz + k2);
         const R S = W0s[k0] * W12;
         const R gr0 = G0g[k0] * W12, gr1 = W0g[k0] * G1W2, gr2 = W0g[k0] * W1G2;
 #pragma unroll
@@ -268,7 +294,9 @@ __device__ __forceinline__ GatherSum<R> gather_general(const BodyCtx<PT>& c, uns
   const Geom& g = c.g;
   const bool in_tile = window_in_tile<DIM>(pm, o, T);
   if (!in_tile) atomicAdd(drift, 1ull);
-  const int t0 = (pm.ax[0].base - o[0]) + T * ((pm.ax[1].base - o[1]) + (DIM == 3 ? T * (pm.ax[2].base - o[2]) : 0));
+  using TL = TileLayout<DIM, T>;
+  const int txy = (pm.ax[0].base - o[0]) + TL::RL * (pm.ax[1].base - o[1]);
+  const int bz = DIM == 3 ? pm.ax[2].base - o[2] : 0;
   const R sS = pm.sS, sG = pm.sG;
   for_window<DIM>(pm, [&](int k0, int k1, int k2) {
     const R wz = DIM == 3 ? sel3(pm.ax[2].W, k2) : R(1);
@@ -282,7 +310,7 @@ __device__ __forceinline__ GatherSum<R> gather_general(const BodyCtx<PT>& c, uns
     const R gr2 = gw0 * (w1 * gz);
     R vt[3] = {R(0), R(0), R(0)}, dv[3] = {R(0), R(0), R(0)};
     if (in_tile) {
-      const int t = t0 + k0 + T * (k1 + T * k2);
+      const int t = txy + k0 + TL::RL * k1 + TL::zoff(bz + k2);
 #pragma unroll
       for (int d = 0; d < DIM; d++) {
         vt[d] = tvel[d * TN + t];
@@ -448,7 +476,9 @@ struct ScatterSrc {
 template <int DIM, int T, int TN, bool NORMAL, bool DET, int K0, int K1, int K2, typename R>
 __device__ __forceinline__ void scatter_box(const PointMapT<R>& pm, const int* o, const ScatterSrc<R>& q,
                                             double* tacc, uint8_t* touched, const Split2* ks) {
-  const int t0 = (pm.ax[0].base - o[0]) + T * ((pm.ax[1].base - o[1]) + (DIM == 3 ? T * (pm.ax[2].base - o[2]) : 0));
+  using TL = TileLayout<DIM, T>;
+  const int txy = (pm.ax[0].base - o[0]) + TL::RL * (pm.ax[1].base - o[1]);
+  const int bz = DIM == 3 ? pm.ax[2].base - o[2] : 0;
   R W0s[3], G0g[3], W0g[3];
 #pragma unroll
   for (int k = 0; k < K0; k++) {
@@ -481,7 +511,7 @@ __device__ __forceinline__ void scatter_box(const PointMapT<R>& pm, const int* o
 #pragma unroll
       for (int k0 = 0; k0 < K0; k0++) {
         if (k0 == 2 && !third0) continue;
-        const int t = t0 + k0 + T * (k1 + T * k2);
+        const int t = txy + k0 + TL::RL * k1 + TL::zoff(bz + k2);
         touched[t] = 1;
         NodeVals<DIM, NORMAL, R> nv;
         nv.v[0] = W0s[k0] * mrow;
@@ -537,7 +567,9 @@ __device__ __forceinline__ void scatter_general(const BodyCtx<PT>& c, unsigned l
     atomicAdd(drift, 1ull);
     mark_blocks<DIM>(g, pm, c.flags);
   }
-  const int t0 = (pm.ax[0].base - o[0]) + T * ((pm.ax[1].base - o[1]) + (DIM == 3 ? T * (pm.ax[2].base - o[2]) : 0));
+  using TL = TileLayout<DIM, T>;
+  const int txy = (pm.ax[0].base - o[0]) + TL::RL * (pm.ax[1].base - o[1]);
+  const int bz = DIM == 3 ? pm.ax[2].base - o[2] : 0;
   const R sS = pm.sS, sG = pm.sG;
   for_window<DIM>(pm, [&](int k0, int k1, int k2) {
     const R wz = DIM == 3 ? sel3(pm.ax[2].W, k2) : R(1);
@@ -558,7 +590,7 @@ __device__ __forceinline__ void scatter_general(const BodyCtx<PT>& c, unsigned l
       if constexpr (NORMAL) nv.v[1 + 2 * DIM + d] = gr[d] * q.m;
     }
     if (in_tile) {
-      const int t = t0 + k0 + T * (k1 + T * k2);
+      const int t = txy + k0 + TL::RL * k1 + TL::zoff(bz + k2);
       touched[t] = 1;
       tile_add_node<DIM, NORMAL, TN, DET>(tacc, t, nv, ks);
     } else {
@@ -746,7 +778,9 @@ __global__ void __launch_bounds__(fused_threads<CAP>(), fused_min_ctas<CAP>())
     }
     if (do_g2p) {
       for (int t = threadIdx.x; t < TN; t += blockDim.x) {
-        const int i = o[0] + t % T, j = o[1] + (t / T) % T, k = DIM == 3 ? o[2] + t / (T * T) : 0;
+        int tx, ty, tz;
+        if (!TileLayout<DIM, T>::node(t, tx, ty, tz)) continue;
+        const int i = o[0] + tx, j = o[1] + ty, k = o[2] + tz;
         if (i < 0 || j < 0 || k < 0 || i >= g.nn[0] || j >= g.nn[1] || k >= g.nn[2]) continue;
         const int64_t s = node_slot(g, i, j, k);
 #pragma unroll
@@ -819,7 +853,9 @@ __global__ void __launch_bounds__(fused_threads<CAP>(), fused_min_ctas<CAP>())
       __syncthreads();
       for (int t = threadIdx.x; t < TN; t += blockDim.x) {
         if (!touched[t]) continue;
-        const int i = o[0] + t % T, j = o[1] + (t / T) % T, k = DIM == 3 ? o[2] + t / (T * T) : 0;
+        int tx, ty, tz;
+        TileLayout<DIM, T>::node(t, tx, ty, tz);
+        const int i = o[0] + tx, j = o[1] + ty, k = o[2] + tz;
         const int64_t s = node_slot(g, i, j, k);
         c.flags[node_block(g, i, j, k)] = 1u;
         atomicAdd(c.A.m + s, tile[t]);
