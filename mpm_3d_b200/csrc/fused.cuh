@@ -221,15 +221,10 @@ __device__ __forceinline__ GatherSum<R> gather_box(const PointMapT<R>& pm, const
   using TL = TileLayout<DIM, T>;
   const int txy = (pm.ax[0].base - o[0]) + TL::RL * (pm.ax[1].base - o[1]);
   const int bz = DIM == 3 ? pm.ax[2].base - o[2] : 0;
-  R W0s[3], G0g[3], W0g[3];
-#pragma unroll
-  for (int k = 0; k < K0; k++) {
-    W0s[k] = pm.sS * pm.ax[0].W[k];
-    G0g[k] = pm.sG * pm.ax[0].G[k];
-    W0g[k] = pm.sG * pm.ax[0].W[k];
-  }
   const bool third0 = pm.ax[0].span == 3, third1 = pm.ax[1].span == 3, third2 = DIM == 3 && pm.ax[2].span == 3;
   constexpr int KZ = DIM == 3 ? K2 : 1;
+  // sums over the unscaled separable products; the map's scales (sS on
+  // values, sG on gradients) are applied once at the end
 #pragma unroll
   for (int k2 = 0; k2 < KZ; k2++) {
     if (k2 == 2 && !third2) continue;
@@ -245,8 +240,9 @@ __device__ __forceinline__ GatherSum<R> gather_box(const PointMapT<R>& pm, const
       for (int k0 = 0; k0 < K0; k0++) {
         if (k0 == 2 && !third0) continue;
         const int t = txy + k0 + TL::RL * k1 + TL::zoff(bz + k2);
-        const R S = W0s[k0] * W12;
-        const R gr0 = G0g[k0] * W12, gr1 = W0g[k0] * G1W2, gr2 = W0g[k0] * W1G2;
+        const R w0 = pm.ax[0].W[k0];
+        const R S = w0 * W12;
+        const R gr0 = pm.ax[0].G[k0] * W12, gr1 = w0 * G1W2, gr2 = w0 * W1G2;
 #pragma unroll
         for (int d = 0; d < DIM; d++) {
           const R vt = tvel[d * TN + t];
@@ -258,6 +254,13 @@ __device__ __forceinline__ GatherSum<R> gather_box(const PointMapT<R>& pm, const
         }
       }
     }
+  }
+#pragma unroll
+  for (int d = 0; d < DIM; d++) {
+    gs.du[d] *= pm.sS;
+    gs.dv[d] *= pm.sS;
+#pragma unroll
+    for (int b = 0; b < DIM; b++) gs.L[d][b] *= pm.sG;
   }
   return gs;
 }
@@ -479,15 +482,19 @@ __device__ __forceinline__ void scatter_box(const PointMapT<R>& pm, const int* o
   using TL = TileLayout<DIM, T>;
   const int txy = (pm.ax[0].base - o[0]) + TL::RL * (pm.ax[1].base - o[1]);
   const int bz = DIM == 3 ? pm.ax[2].base - o[2] : 0;
-  R W0s[3], G0g[3], W0g[3];
-#pragma unroll
-  for (int k = 0; k < K0; k++) {
-    W0s[k] = pm.sS * pm.ax[0].W[k];
-    G0g[k] = pm.sG * pm.ax[0].G[k];
-    W0g[k] = pm.sG * pm.ax[0].W[k];
-  }
   const bool third0 = pm.ax[0].span == 3, third1 = pm.ax[1].span == 3, third2 = DIM == 3 && pm.ax[2].span == 3;
   constexpr int KZ = DIM == 3 ? K2 : 1;
+  // the map's scales go into the point's sources once (sS on m and m x_t,
+  // sG on V sigma and on m for the normal), the node loop uses the
+  // unscaled axis factors
+  const R sm = pm.sS * q.m, gm = pm.sG * q.m;
+  R smv[3], sV[3][3];
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    smv[a] = pm.sS * q.mv[a];
+#pragma unroll
+    for (int b = 0; b < 3; b++) sV[a][b] = pm.sG * q.V3[a][b];
+  }
 #pragma unroll
   for (int k2 = 0; k2 < KZ; k2++) {
     if (k2 == 2 && !third2) continue;
@@ -499,31 +506,32 @@ __device__ __forceinline__ void scatter_box(const PointMapT<R>& pm, const int* o
       const R W12 = pm.ax[1].W[k1] * wz;
       const R G1W2 = pm.ax[1].G[k1] * wz;
       const R W1G2 = pm.ax[1].W[k1] * gz;
-      const R mrow = q.m * W12;
+      const R mrow = sm * W12;
       R mvrow[3], A[3], Bf[3];
 #pragma unroll
       for (int d = 0; d < DIM; d++) {
-        mvrow[d] = q.mv[d] * W12;
-        A[d] = q.V3[d][0] * W12;
-        Bf[d] = q.V3[d][1] * G1W2;
-        if (DIM == 3) Bf[d] += q.V3[d][2] * W1G2;
+        mvrow[d] = smv[d] * W12;
+        A[d] = sV[d][0] * W12;
+        Bf[d] = sV[d][1] * G1W2;
+        if (DIM == 3) Bf[d] += sV[d][2] * W1G2;
       }
 #pragma unroll
       for (int k0 = 0; k0 < K0; k0++) {
         if (k0 == 2 && !third0) continue;
         const int t = txy + k0 + TL::RL * k1 + TL::zoff(bz + k2);
         touched[t] = 1;
+        const R w0 = pm.ax[0].W[k0], g0 = pm.ax[0].G[k0];
         NodeVals<DIM, NORMAL, R> nv;
-        nv.v[0] = W0s[k0] * mrow;
+        nv.v[0] = w0 * mrow;
 #pragma unroll
         for (int d = 0; d < DIM; d++) {
-          nv.v[1 + d] = W0s[k0] * mvrow[d];
-          nv.v[1 + DIM + d] = -(G0g[k0] * A[d] + W0g[k0] * Bf[d]);
+          nv.v[1 + d] = w0 * mvrow[d];
+          nv.v[1 + DIM + d] = -(g0 * A[d] + w0 * Bf[d]);
         }
         if constexpr (NORMAL) {
-          const R gr[3] = {G0g[k0] * W12, W0g[k0] * G1W2, W0g[k0] * W1G2};
+          const R gr[3] = {g0 * W12, w0 * G1W2, w0 * W1G2};
 #pragma unroll
-          for (int d = 0; d < DIM; d++) nv.v[1 + 2 * DIM + d] = gr[d] * q.m;
+          for (int d = 0; d < DIM; d++) nv.v[1 + 2 * DIM + d] = gr[d] * gm;
         }
         tile_add_node<DIM, NORMAL, TN, DET>(tacc, t, nv, ks);
       }
