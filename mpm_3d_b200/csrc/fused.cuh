@@ -14,9 +14,9 @@
 //      copy;
 //   2. the tile is cleared, every point builds its map at the new position
 //      and adds its contributions with FP64 shared-memory atomics (points of
-//      one warp lie in distinct cells: few same-address conflicts). Windows
-//      of two nodes per axis inside the tile (the common case) take a
-//      straight-line path with the force evaluated per window row;
+//      one warp have distinct window bases: no same-address conflicts).
+//      Windows inside the tile take a straight-line node box, the union of
+//      the warp's window shapes, with the force evaluated per box row;
 //   3. the tile is added into the global nodal accumulators, one global
 //      atomic per touched node and value.
 // No phase waits on DRAM latency per point: the point state arrives in bulk

@@ -2,11 +2,17 @@
 // batch in one set of launches.
 //
 // Points are kept grouped by bin: a block of B^dim cells (4x4x4 in 3D, 8x8
-// in 2D). Within a bin they are laid out rank-major: first the first point
-// of every cell (in cell order), then the second point of every cell, and so
-// on. A warp of consecutive points therefore covers distinct cells, so the
-// points of one warp rarely add into the same node at the same time in the
-// shared-memory tile (same-address atomics serialise).
+// in 2D). A point's cell here is the cell of its shape-function window's
+// base node (the cell of the lower corner, x - extent/2), not the cell that
+// contains x: the kernels visit a window as offsets from its base, so two
+// points with the same base add into the same tile nodes in the same
+// instruction, while points with distinct bases never collide. (Binning by
+// the containing cell puts the two points of a cell along an axis on bases
+// k-1 and k whenever the lower corner of one crosses a node, and neighbours
+// then share bases.) Within a bin points are laid out rank-major: first the
+// first point of every cell (in cell order), then the second point of every
+// cell, and so on, so a warp of consecutive points covers distinct bases and
+// its shared-memory atomics do not serialise on equal addresses.
 //
 // The sort is a counting sort over the batch's concatenated point space
 // (count + rank, per-bin totals, one exclusive scan over all bodies' bins,
@@ -68,12 +74,15 @@ __device__ __forceinline__ int find_range(const I* end, int n, int64_t i) {
   return lo;
 }
 
-// Cell of a point for binning, clamped into the grid.
+// Cell of a point for binning: the cell of its window's base, x - a with a
+// half the point's extent (the lower corner of build_map), clamped into the
+// grid. Windows then span base .. base+2, inside the bin's node tile (which
+// starts one node below the bin) with one node to spare below.
 template <int DIM, typename PT>
-__device__ __forceinline__ void point_cell(const Geom& g, const PT* x, int* c) {
+__device__ __forceinline__ void point_cell(const Geom& g, const PT* x, double a, int* c) {
 #pragma unroll
   for (int d = 0; d < DIM; d++) {
-    int v = (int)floor((double)x[d] * (g.N[d] / g.L[d]));
+    int v = (int)floor(((double)x[d] - a) * (g.N[d] / g.L[d]));
     v = v < 0 ? 0 : (v >= g.N[d] ? g.N[d] - 1 : v);
     c[d] = v;
   }
@@ -118,7 +127,7 @@ __global__ void k_sort_count(const BatchHdr* hdr, const BodyCtx<PT>* bodies, con
         else xp[d] = B.P.x[d][p] + B.P.u[d][p];
       }
       int c[3] = {0, 0, 0};
-      point_cell<DIM>(B.g, xp, c);
+      point_cell<DIM>(B.g, xp, 0.5 * (double)B.P.ext[p], c);
       int b, l;
       bin_of<DIM>(B.bg, c, &b, &l);
       k = b * B.bg.cells_per_bin + l;
