@@ -265,11 +265,74 @@ __device__ __forceinline__ GatherSum<R> gather_box(const PointMapT<R>& pm, const
   return gs;
 }
 
+// Gather over the union box of a warp with a three-node span on some axis:
+// rolled loops over the y and z offsets (bounds from the warp's union mask),
+// the x offsets unrolled, lanes skipping the third node of an axis they do
+// not span. One compact loop for every such shape keeps the kernel's
+// instruction footprint small (warps of different shapes run side by side).
+template <int DIM, int T, int TN, typename R>
+__device__ __forceinline__ GatherSum<R> gather_rolled(const PointMapT<R>& pm, const int* o, const R* tvel, int mask) {
+  using TL = TileLayout<DIM, T>;
+  GatherSum<R> gs;
+  const int txy = (pm.ax[0].base - o[0]) + TL::RL * (pm.ax[1].base - o[1]);
+  const int bz = DIM == 3 ? pm.ax[2].base - o[2] : 0;
+  const bool third0 = pm.ax[0].span == 3, third1 = pm.ax[1].span == 3, third2 = DIM == 3 && pm.ax[2].span == 3;
+  const int K1 = 2 + ((mask >> 1) & 1), K2 = DIM == 3 ? 2 + ((mask >> 2) & 1) : 1;
+  const bool wide0 = (mask & 1) != 0;
+#pragma unroll 1
+  for (int k2 = 0; k2 < K2; k2++) {
+    const bool on2 = k2 < 2 || third2;
+    const R wz = DIM == 3 ? sel3(pm.ax[2].W, k2) : R(1);
+    const R gz = DIM == 3 ? sel3(pm.ax[2].G, k2) : R(0);
+    const int zo = TL::zoff(bz + k2);
+#pragma unroll 1
+    for (int k1 = 0; k1 < K1; k1++) {
+      if (!on2 || (k1 == 2 && !third1)) continue;
+      const R w1 = sel3(pm.ax[1].W, k1);
+      const R W12 = w1 * wz;
+      const R G1W2 = sel3(pm.ax[1].G, k1) * wz;
+      const R W1G2 = w1 * gz;
+      const int trow = txy + TL::RL * k1 + zo;
+#pragma unroll
+      for (int k0 = 0; k0 < 3; k0++) {
+        if (k0 == 2 && !(wide0 && third0)) break;
+        const int t = trow + k0;
+        const R w0 = pm.ax[0].W[k0];
+        const R S = w0 * W12;
+        const R gr0 = pm.ax[0].G[k0] * W12, gr1 = w0 * G1W2, gr2 = w0 * W1G2;
+#pragma unroll
+        for (int d = 0; d < DIM; d++) {
+          const R vt = tvel[d * TN + t];
+          gs.du[d] += S * vt;
+          gs.dv[d] += S * tvel[(3 + d) * TN + t];
+          gs.L[d][0] += vt * gr0;
+          gs.L[d][1] += vt * gr1;
+          if (DIM == 3) gs.L[d][2] += vt * gr2;
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int d = 0; d < DIM; d++) {
+    gs.du[d] *= pm.sS;
+    gs.dv[d] *= pm.sS;
+#pragma unroll
+    for (int b = 0; b < DIM; b++) gs.L[d][b] *= pm.sG;
+  }
+  return gs;
+}
+
+// The warp's union box: straight-line code for two nodes per axis; other
+// shapes through the rolled loop in FP32 (the mixed form), and through one
+// straight-line instantiation per shape in FP64, where the rolled loop's
+// extra registers cost more than the larger code.
 template <int DIM, int T, int TN, typename R>
 __device__ __forceinline__ GatherSum<R> gather_box_any(const PointMapT<R>& pm, const int* o, const R* tvel, int mask) {
-  if constexpr (DIM == 3) {
+  if (mask == 0) return gather_box<DIM, T, TN, 2, 2, 2>(pm, o, tvel);
+  if constexpr (sizeof(R) == 4) {
+    return gather_rolled<DIM, T, TN>(pm, o, tvel, mask);
+  } else if constexpr (DIM == 3) {
     switch (mask) {
-      case 0: return gather_box<DIM, T, TN, 2, 2, 2>(pm, o, tvel);
       case 1: return gather_box<DIM, T, TN, 3, 2, 2>(pm, o, tvel);
       case 2: return gather_box<DIM, T, TN, 2, 3, 2>(pm, o, tvel);
       case 3: return gather_box<DIM, T, TN, 3, 3, 2>(pm, o, tvel);
@@ -280,7 +343,6 @@ __device__ __forceinline__ GatherSum<R> gather_box_any(const PointMapT<R>& pm, c
     }
   } else {
     switch (mask & 3) {
-      case 0: return gather_box<DIM, T, TN, 2, 2, 2>(pm, o, tvel);
       case 1: return gather_box<DIM, T, TN, 3, 2, 2>(pm, o, tvel);
       case 2: return gather_box<DIM, T, TN, 2, 3, 2>(pm, o, tvel);
       default: return gather_box<DIM, T, TN, 3, 3, 2>(pm, o, tvel);
@@ -539,12 +601,80 @@ __device__ __forceinline__ void scatter_box(const PointMapT<R>& pm, const int* o
   }
 }
 
+// Scatter over the union box of a warp with a three-node span on some axis
+// (as gather_rolled).
+template <int DIM, int T, int TN, bool NORMAL, bool DET, typename R>
+__device__ __forceinline__ void scatter_rolled(const PointMapT<R>& pm, const int* o, const ScatterSrc<R>& q,
+                                               double* tacc, uint8_t* touched, const Split2* ks, int mask) {
+  using TL = TileLayout<DIM, T>;
+  const int txy = (pm.ax[0].base - o[0]) + TL::RL * (pm.ax[1].base - o[1]);
+  const int bz = DIM == 3 ? pm.ax[2].base - o[2] : 0;
+  const bool third0 = pm.ax[0].span == 3, third1 = pm.ax[1].span == 3, third2 = DIM == 3 && pm.ax[2].span == 3;
+  const int K1 = 2 + ((mask >> 1) & 1), K2 = DIM == 3 ? 2 + ((mask >> 2) & 1) : 1;
+  const bool wide0 = (mask & 1) != 0;
+  const R sm = pm.sS * q.m, gm = pm.sG * q.m;
+  R smv[3], sV[3][3];
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    smv[a] = pm.sS * q.mv[a];
+#pragma unroll
+    for (int b = 0; b < 3; b++) sV[a][b] = pm.sG * q.V3[a][b];
+  }
+#pragma unroll 1
+  for (int k2 = 0; k2 < K2; k2++) {
+    const bool on2 = k2 < 2 || third2;
+    const R wz = DIM == 3 ? sel3(pm.ax[2].W, k2) : R(1);
+    const R gz = DIM == 3 ? sel3(pm.ax[2].G, k2) : R(0);
+    const int zo = TL::zoff(bz + k2);
+#pragma unroll 1
+    for (int k1 = 0; k1 < K1; k1++) {
+      if (!on2 || (k1 == 2 && !third1)) continue;
+      const R w1 = sel3(pm.ax[1].W, k1);
+      const R W12 = w1 * wz;
+      const R G1W2 = sel3(pm.ax[1].G, k1) * wz;
+      const R W1G2 = w1 * gz;
+      const R mrow = sm * W12;
+      R mvrow[3], A[3], Bf[3];
+#pragma unroll
+      for (int d = 0; d < DIM; d++) {
+        mvrow[d] = smv[d] * W12;
+        A[d] = sV[d][0] * W12;
+        Bf[d] = sV[d][1] * G1W2;
+        if (DIM == 3) Bf[d] += sV[d][2] * W1G2;
+      }
+      const int trow = txy + TL::RL * k1 + zo;
+#pragma unroll
+      for (int k0 = 0; k0 < 3; k0++) {
+        if (k0 == 2 && !(wide0 && third0)) break;
+        const int t = trow + k0;
+        touched[t] = 1;
+        const R w0 = pm.ax[0].W[k0], g0 = pm.ax[0].G[k0];
+        NodeVals<DIM, NORMAL, R> nv;
+        nv.v[0] = w0 * mrow;
+#pragma unroll
+        for (int d = 0; d < DIM; d++) {
+          nv.v[1 + d] = w0 * mvrow[d];
+          nv.v[1 + DIM + d] = -(g0 * A[d] + w0 * Bf[d]);
+        }
+        if constexpr (NORMAL) {
+          const R gr[3] = {g0 * W12, w0 * G1W2, w0 * W1G2};
+#pragma unroll
+          for (int d = 0; d < DIM; d++) nv.v[1 + 2 * DIM + d] = gr[d] * gm;
+        }
+        tile_add_node<DIM, NORMAL, TN, DET>(tacc, t, nv, ks);
+      }
+    }
+  }
+}
+
 template <int DIM, int T, int TN, bool NORMAL, bool DET, typename R>
 __device__ __forceinline__ void scatter_box_any(const PointMapT<R>& pm, const int* o, const ScatterSrc<R>& q,
                                                 double* tacc, uint8_t* touched, const Split2* ks, int mask) {
-  if constexpr (DIM == 3) {
+  if (mask == 0) return scatter_box<DIM, T, TN, NORMAL, DET, 2, 2, 2>(pm, o, q, tacc, touched, ks);
+  if constexpr (sizeof(R) == 4) {
+    scatter_rolled<DIM, T, TN, NORMAL, DET>(pm, o, q, tacc, touched, ks, mask);
+  } else if constexpr (DIM == 3) {
     switch (mask) {
-      case 0: return scatter_box<DIM, T, TN, NORMAL, DET, 2, 2, 2>(pm, o, q, tacc, touched, ks);
       case 1: return scatter_box<DIM, T, TN, NORMAL, DET, 3, 2, 2>(pm, o, q, tacc, touched, ks);
       case 2: return scatter_box<DIM, T, TN, NORMAL, DET, 2, 3, 2>(pm, o, q, tacc, touched, ks);
       case 3: return scatter_box<DIM, T, TN, NORMAL, DET, 3, 3, 2>(pm, o, q, tacc, touched, ks);
@@ -555,7 +685,6 @@ __device__ __forceinline__ void scatter_box_any(const PointMapT<R>& pm, const in
     }
   } else {
     switch (mask & 3) {
-      case 0: return scatter_box<DIM, T, TN, NORMAL, DET, 2, 2, 2>(pm, o, q, tacc, touched, ks);
       case 1: return scatter_box<DIM, T, TN, NORMAL, DET, 3, 2, 2>(pm, o, q, tacc, touched, ks);
       case 2: return scatter_box<DIM, T, TN, NORMAL, DET, 2, 3, 2>(pm, o, q, tacc, touched, ks);
       default: return scatter_box<DIM, T, TN, NORMAL, DET, 3, 3, 2>(pm, o, q, tacc, touched, ks);
