@@ -136,8 +136,8 @@ inline int64_t job_footprint(const mpmgpu_config& cfg, bool mixed, bool keep_deb
     bytes += 2 * n * (18 * ps + 8);             // two point buffers
     if (keep_debug && !mixed) bytes += 2 * n * 72;
     bytes += g.nslots * 8 * (7 + 6);            // accumulators + velocities
-    bytes += n * 8;                              // sort key + rank
-    bytes += ((int64_t)bg.nbins * bg.cells_per_bin + 1) * 4 + ((int64_t)bg.nbins + 2) * 4;
+    bytes += n * 10;                             // sort key, rank, class rank
+    bytes += ((int64_t)bg.nbins * bg.cells_per_bin + 1) * 12 + ((int64_t)bg.nbins + 2) * 4;
     bytes += ((int64_t)bg.nbins + n / 256 + 1) * 16;
     if (keep_debug) bytes += g.nslots * 8 * 7;
   }
@@ -1159,6 +1159,8 @@ class Batch : public BatchBase {
     MPM_TRY(grow(&key_, &cap_points_k_, std::max<int64_t>(points, 1), 0));
     MPM_TRY(grow(&rank_, &cap_points_r_, std::max<int64_t>(points, 1), 0));
     MPM_TRY(grow(&cell_count_, &cap_cells_, std::max<int64_t>(cells, 1), 0));
+    MPM_TRY(grow(&cell_hist_, &cap_cells_h_, std::max<int64_t>(cells, 1), 0));
+    MPM_TRY(grow(&crank_, &cap_points_c_, std::max<int64_t>(points, 1), 0));
     MPM_TRY(grow(&bin_scan_, &cap_bins_, bins + 2, 0));
     MPM_TRY(grow(&chunk_sum_, &cap_chunks_, cap_bins_ / kScanChunk + 2, 0));
     MPM_TRY(grow(&item_off_d_, &cap_bodies_i_, std::max<int64_t>(nb, 1), 0));
@@ -1396,9 +1398,10 @@ class Batch : public BatchBase {
   template <int DIM>
   mpmgpu_status launch_sort_direct_t() {
     const int sb = stride_blocks(256);
-    k_sort_clear<<<sb, 256, 0, stream_>>>(hdr_, cell_count_, nwork_body_);
+    k_sort_clear<<<sb, 256, 0, stream_>>>(hdr_, cell_count_, cell_hist_, nwork_body_);
     MPM_TRY(check_launch("k_sort_clear"));
-    k_sort_count<DIM, PT><<<sb, 256, 0, stream_>>>(hdr_, ctx_d_, point_end_d_, key_, rank_, cell_count_);
+    k_sort_count<DIM, PT><<<sb, 256, 0, stream_>>>(hdr_, ctx_d_, point_end_d_, key_, rank_, cell_count_, cell_hist_,
+                                                   crank_);
     MPM_TRY(check_launch("k_sort_count"));
     k_bin_totals<PT><<<sb, 256, 0, stream_>>>(hdr_, ctx_d_, bin_end_d_, cell_count_, bin_scan_);
     MPM_TRY(check_launch("k_bin_totals"));
@@ -1409,7 +1412,8 @@ class Batch : public BatchBase {
     MPM_TRY(check_launch("k_scan_small"));
     k_scan_add<<<chunks, kScanChunk, 0, stream_>>>(hdr_, bin_scan_, chunk_sum_);
     MPM_TRY(check_launch("k_scan_add"));
-    k_sort_scatter<DIM, PT><<<sb, 256, 0, stream_>>>(hdr_, ctx_d_, point_end_d_, key_, rank_, cell_count_, bin_scan_);
+    k_sort_scatter<DIM, PT><<<sb, 256, 0, stream_>>>(hdr_, ctx_d_, point_end_d_, key_, rank_, cell_count_, cell_hist_,
+                                                     crank_, bin_scan_);
     MPM_TRY(check_launch("k_sort_scatter"));
     k_sort_flip<PT><<<std::max(1, (hdr_host_.nbodies + 255) / 256 + 1), 256, 0, stream_>>>(hdr_, ctx_d_);
     MPM_TRY(check_launch("k_sort_flip"));
@@ -1639,6 +1643,10 @@ class Batch : public BatchBase {
   int64_t cap_points_r_ = 0;
   int32_t* cell_count_ = nullptr;
   int64_t cap_cells_ = 0;
+  unsigned long long* cell_hist_ = nullptr;   // per cell: 8 class counts of 8 bits
+  int64_t cap_cells_h_ = 0;
+  int16_t* crank_ = nullptr;                  // per point: class << 8 | rank in class
+  int64_t cap_points_c_ = 0;
   int32_t* bin_scan_ = nullptr;
   int64_t cap_bins_ = 0;
   int32_t* chunk_sum_ = nullptr;

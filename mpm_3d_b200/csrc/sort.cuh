@@ -12,7 +12,12 @@
 // then share bases.) Within a bin points are laid out rank-major: first the
 // first point of every cell (in cell order), then the second point of every
 // cell, and so on, so a warp of consecutive points covers distinct bases and
-// its shared-memory atomics do not serialise on equal addresses.
+// its shared-memory atomics do not serialise on equal addresses. Within a
+// cell, points are ranked by window class (the axes along which the window
+// spans three nodes) before arrival order: in the regular layouts of a few
+// points per cell the r-th point of every cell then has the same window
+// shape, and a warp's node box (the union of its lanes' shapes) is its
+// lanes' own.
 //
 // The sort is a counting sort over the batch's concatenated point space
 // (count + rank, per-bin totals, one exclusive scan over all bodies' bins,
@@ -78,14 +83,21 @@ __device__ __forceinline__ int find_range(const I* end, int n, int64_t i) {
 // half the point's extent (the lower corner of build_map), clamped into the
 // grid. Windows then span base .. base+2, inside the bin's node tile (which
 // starts one node below the bin) with one node to spare below.
+// Also returns the point's window class: bit d set when the upper corner
+// x + a lies in a later element than the lower one (a three-node span).
 template <int DIM, typename PT>
-__device__ __forceinline__ void point_cell(const Geom& g, const PT* x, double a, int* c) {
+__device__ __forceinline__ int point_cell(const Geom& g, const PT* x, double a, int* c) {
+  int cls = 0;
 #pragma unroll
   for (int d = 0; d < DIM; d++) {
-    int v = (int)floor(((double)x[d] - a) * (g.N[d] / g.L[d]));
+    const double nl = g.N[d] / g.L[d];
+    const double lo = floor(((double)x[d] - a) * nl);
+    cls |= (floor(((double)x[d] + a) * nl) != lo ? 1 : 0) << d;
+    int v = (int)lo;
     v = v < 0 ? 0 : (v >= g.N[d] ? g.N[d] - 1 : v);
     c[d] = v;
   }
+  return cls;
 }
 
 template <int DIM>
@@ -96,19 +108,28 @@ __device__ __forceinline__ void bin_of(const BinGeom& bg, const int* c, int* bin
   *local = lx + bg.B * (ly + bg.B * lz);
 }
 
-// Pass 0: clears the cell counters and the per-body work-item counts.
-__global__ void k_sort_clear(const BatchHdr* hdr, int32_t* cell_count, int32_t* nwork_body) {
+// Pass 0: clears the cell counters, the cells' class histograms and the
+// per-body work-item counts.
+__global__ void k_sort_clear(const BatchHdr* hdr, int32_t* cell_count, unsigned long long* cell_hist,
+                             int32_t* nwork_body) {
   const int64_t n = hdr->cells;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += stride) cell_count[i] = 0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += stride) {
+    cell_count[i] = 0;
+    cell_hist[i] = 0ull;
+  }
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < hdr->nbodies; i += stride) nwork_body[i] = 0;
 }
 
 // Pass 1: key (bin * cells_per_bin + local cell, local to the body) and rank
-// within the cell. Inactive points go to the trailing key nbins * cells_per_bin.
+// within the cell (arrival order). Inactive points go to the trailing key
+// nbins * cells_per_bin. Active points also count in their cell's class
+// histogram, eight 8-bit counts in one 64-bit word, and keep their class and
+// their arrival rank within the class (crank = class << 8 | rank, the rank
+// saturated at 255).
 template <int DIM, typename PT>
 __global__ void k_sort_count(const BatchHdr* hdr, const BodyCtx<PT>* bodies, const int64_t* point_end, int32_t* key,
-                             int32_t* rank, int32_t* cell_count) {
+                             int32_t* rank, int32_t* cell_count, unsigned long long* cell_hist, int16_t* crank) {
   const int64_t total = hdr->points;
   const int nb = hdr->nbodies;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
@@ -127,10 +148,13 @@ __global__ void k_sort_count(const BatchHdr* hdr, const BodyCtx<PT>* bodies, con
         else xp[d] = B.P.x[d][p] + B.P.u[d][p];
       }
       int c[3] = {0, 0, 0};
-      point_cell<DIM>(B.g, xp, 0.5 * (double)B.P.ext[p], c);
+      const int cls = point_cell<DIM>(B.g, xp, 0.5 * (double)B.P.ext[p], c);
       int b, l;
       bin_of<DIM>(B.bg, c, &b, &l);
       k = b * B.bg.cells_per_bin + l;
+      const unsigned long long old = atomicAdd(cell_hist + B.cell_off + k, 1ull << (8 * cls));
+      const int rc = (int)((old >> (8 * cls)) & 0xffull);
+      crank[q] = (int16_t)((cls << 8) | rc);
     }
     key[q] = k;
     rank[q] = atomicAdd(cell_count + B.cell_off + k, 1);
@@ -245,10 +269,16 @@ __global__ void __launch_bounds__(kScanChunk) k_scan_add(const BatchHdr* hdr, in
 
 // Pass 3: destination of each point inside its bin (rank-major order) and
 // the permutation copy of every per-point array into the second buffer.
+// The rank of a point within its cell is its class-order rank (points of
+// lower classes first, then the class's arrival rank) when the cell's class
+// histogram is exact, i.e. its counts sum to the cell's count (a class of
+// 256 or more points in one cell would have carried into the next count);
+// otherwise every point of that cell keeps its arrival rank. Either way the
+// ranks of a cell are a permutation of 0 .. count-1.
 template <int DIM, typename PT>
 __global__ void k_sort_scatter(const BatchHdr* hdr, const BodyCtx<PT>* bodies, const int64_t* point_end,
                                const int32_t* key, const int32_t* rank, const int32_t* cell_count,
-                               const int32_t* bin_scan) {
+                               const unsigned long long* cell_hist, const int16_t* crank, const int32_t* bin_scan) {
   const int64_t total = hdr->points;
   const int nb = hdr->nbodies;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
@@ -256,7 +286,7 @@ __global__ void k_sort_scatter(const BatchHdr* hdr, const BodyCtx<PT>* bodies, c
     const BodyCtx<PT>& B = bodies[find_range(point_end, nb, q)];
     const int64_t p = q - B.point_off;
     const int k = key[q];
-    const int r = rank[q];
+    int r = rank[q];
     const int cpb = B.bg.cells_per_bin;
     const int b = k / cpb;
     const int32_t* bs = bin_scan + B.bin_off;
@@ -264,6 +294,17 @@ __global__ void k_sort_scatter(const BatchHdr* hdr, const BodyCtx<PT>* bodies, c
     if (b < B.bg.nbins) {
       const int l = k - b * cpb;
       const int32_t* cc = cell_count + B.cell_off + (int64_t)b * cpb;
+      const unsigned long long h = cell_hist[B.cell_off + k];
+      const int cr = crank[q];
+      const int cls = cr >> 8;
+      int sum = 0, lower = 0;
+#pragma unroll
+      for (int j = 0; j < 8; j++) {
+        const int f = (int)((h >> (8 * j)) & 0xffull);
+        sum += f;
+        lower += j < cls ? f : 0;
+      }
+      if (sum == cc[l]) r = lower + (cr & 0xff);
       int below = 0, same_level = 0;
       for (int c = 0; c < cpb; c++) {
         const int cnt = cc[c];
