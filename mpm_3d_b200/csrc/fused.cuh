@@ -322,32 +322,12 @@ __device__ __forceinline__ GatherSum<R> gather_rolled(const PointMapT<R>& pm, co
   return gs;
 }
 
-// The warp's union box: straight-line code for two nodes per axis; other
-// shapes through the rolled loop in FP32 (the mixed form), and through one
-// straight-line instantiation per shape in FP64, where the rolled loop's
-// extra registers cost more than the larger code.
+// The warp's union box: straight-line code for two nodes per axis (the
+// regular layouts' common shape), the rolled loop for every other shape.
 template <int DIM, int T, int TN, typename R>
 __device__ __forceinline__ GatherSum<R> gather_box_any(const PointMapT<R>& pm, const int* o, const R* tvel, int mask) {
   if (mask == 0) return gather_box<DIM, T, TN, 2, 2, 2>(pm, o, tvel);
-  if constexpr (sizeof(R) == 4) {
-    return gather_rolled<DIM, T, TN>(pm, o, tvel, mask);
-  } else if constexpr (DIM == 3) {
-    switch (mask) {
-      case 1: return gather_box<DIM, T, TN, 3, 2, 2>(pm, o, tvel);
-      case 2: return gather_box<DIM, T, TN, 2, 3, 2>(pm, o, tvel);
-      case 3: return gather_box<DIM, T, TN, 3, 3, 2>(pm, o, tvel);
-      case 4: return gather_box<DIM, T, TN, 2, 2, 3>(pm, o, tvel);
-      case 5: return gather_box<DIM, T, TN, 3, 2, 3>(pm, o, tvel);
-      case 6: return gather_box<DIM, T, TN, 2, 3, 3>(pm, o, tvel);
-      default: return gather_box<DIM, T, TN, 3, 3, 3>(pm, o, tvel);
-    }
-  } else {
-    switch (mask & 3) {
-      case 1: return gather_box<DIM, T, TN, 3, 2, 2>(pm, o, tvel);
-      case 2: return gather_box<DIM, T, TN, 2, 3, 2>(pm, o, tvel);
-      default: return gather_box<DIM, T, TN, 3, 3, 2>(pm, o, tvel);
-    }
-  }
+  return gather_rolled<DIM, T, TN>(pm, o, tvel, mask);
 }
 
 // Gather over any window (three-node spans, nodes outside the tile).
@@ -671,25 +651,7 @@ template <int DIM, int T, int TN, bool NORMAL, bool DET, typename R>
 __device__ __forceinline__ void scatter_box_any(const PointMapT<R>& pm, const int* o, const ScatterSrc<R>& q,
                                                 double* tacc, uint8_t* touched, const Split2* ks, int mask) {
   if (mask == 0) return scatter_box<DIM, T, TN, NORMAL, DET, 2, 2, 2>(pm, o, q, tacc, touched, ks);
-  if constexpr (sizeof(R) == 4) {
-    scatter_rolled<DIM, T, TN, NORMAL, DET>(pm, o, q, tacc, touched, ks, mask);
-  } else if constexpr (DIM == 3) {
-    switch (mask) {
-      case 1: return scatter_box<DIM, T, TN, NORMAL, DET, 3, 2, 2>(pm, o, q, tacc, touched, ks);
-      case 2: return scatter_box<DIM, T, TN, NORMAL, DET, 2, 3, 2>(pm, o, q, tacc, touched, ks);
-      case 3: return scatter_box<DIM, T, TN, NORMAL, DET, 3, 3, 2>(pm, o, q, tacc, touched, ks);
-      case 4: return scatter_box<DIM, T, TN, NORMAL, DET, 2, 2, 3>(pm, o, q, tacc, touched, ks);
-      case 5: return scatter_box<DIM, T, TN, NORMAL, DET, 3, 2, 3>(pm, o, q, tacc, touched, ks);
-      case 6: return scatter_box<DIM, T, TN, NORMAL, DET, 2, 3, 3>(pm, o, q, tacc, touched, ks);
-      default: return scatter_box<DIM, T, TN, NORMAL, DET, 3, 3, 3>(pm, o, q, tacc, touched, ks);
-    }
-  } else {
-    switch (mask & 3) {
-      case 1: return scatter_box<DIM, T, TN, NORMAL, DET, 3, 2, 2>(pm, o, q, tacc, touched, ks);
-      case 2: return scatter_box<DIM, T, TN, NORMAL, DET, 2, 3, 2>(pm, o, q, tacc, touched, ks);
-      default: return scatter_box<DIM, T, TN, NORMAL, DET, 3, 3, 2>(pm, o, q, tacc, touched, ks);
-    }
-  }
+  scatter_rolled<DIM, T, TN, NORMAL, DET>(pm, o, q, tacc, touched, ks, mask);
 }
 
 // Scatter over any window (three-node spans, nodes outside the tile, which
