@@ -497,7 +497,9 @@ def run_ensemble(args, rank, world, local):
     roof = roofline(n, mixed["prof_steps"], mixed["prof"], active_ratio, True, ("ensemble", "mixed"))
     plain_value, plain_ms = plain_fp64(cases, args.plain_steps, local) if not args.no_plain else (None, None)
     serving = run_serving(args.serve_seconds, local, mixed["sort_interval"]) if args.serve_seconds > 0 else None
-    e2e = (run_e2e_batch(cases, args.steps, local, mixed["cap"], mixed["sort_interval"])
+    # end to end: every job runs its own step count (the workload's 500
+    # steps), as a user runs the ensemble
+    e2e = (run_e2e_batch(cases, max(c.steps for c in cases), local, mixed["cap"], mixed["sort_interval"])
            if rank == 0 and not args.no_e2e else None)
     cpu = None
     if rank == 0 and not args.no_cpu:
@@ -574,8 +576,9 @@ def run_serving_workload(args, rank, world, local):
 
 def run_e2e_batch(cases, steps: int, device: int, cap: int, sort_interval: int):
     """The ensemble through the C ABI from host buffers: batch creation and
-    upload of every job, `steps` steps, download of every point's x, x_t and
-    stress, teardown, all on the wall clock."""
+    upload of every job, `steps` steps (each job stops at its own count),
+    download of every point's x, x_t and stress, teardown, all on the wall
+    clock."""
     import torch
 
     from mpm_3d_b200.native import GPUBatch
@@ -585,15 +588,16 @@ def run_e2e_batch(cases, steps: int, device: int, cap: int, sort_interval: int):
     b = GPUBatch(dim=3, mode="mixed", device=device, points_per_item=cap, sort_interval=sort_interval)
     jobs = [b.add(c) for c in cases]
     b.step(steps)
+    b.synchronize()
     d2h = 0
     for j in jobs:
         for f in ("x", "x_t", "T"):
             d2h += b.points(j, 0, f).nbytes
     b.close()
     dt = time.perf_counter() - t0
-    n = sum(c.n_points for c in cases)
+    psteps = sum(c.n_points * min(c.steps, steps) for c in cases)
     h2d = sum(b_.n * (8 + 8 + 24 + 24 + 4) for c in cases for b_ in c.bodies)
-    return {"value": n * steps / dt, "unit": UNIT, "h2d_bytes_per_step": h2d // steps, "d2h_bytes_per_step": d2h // steps,
+    return {"value": psteps / dt, "unit": UNIT, "h2d_bytes_per_step": h2d // steps, "d2h_bytes_per_step": d2h // steps,
             "steps": steps, "seconds": dt}
 
 

@@ -781,13 +781,9 @@ __global__ void __launch_bounds__(fused_threads<CAP>(), fused_min_ctas<CAP>())
   PT* pts = reinterpret_cast<PT*>(smem + off_pts<PT, CAP>());
   int32_t* act = reinterpret_cast<int32_t*>(smem + off_act<PT, CAP>());
   double* tile = reinterpret_cast<double*>(smem + off_tile<PT, CAP>());  // phase 2: NACC FP64 values
-  // phase 1: nodal vt0..2 dv0..2 as loaded (FP64), and in the point
-  // precision relative to the reference velocity (the same array in the
-  // FP64 form; behind the FP64 copy in the mixed form)
-  double* tv64 = tile;
-  PT* tvel = sizeof(PT) == 8 ? reinterpret_cast<PT*>(tile) : reinterpret_cast<PT*>(tile + 6 * TN);
-  static_assert(sizeof(PT) == 8 || 6 * TN * (sizeof(double) + sizeof(PT)) <= 10 * TN * sizeof(double),
-                "the mixed form's velocity tiles fit in the accumulation tile");
+  // phase 1: nodal vt0..2 dv0..2 in the point precision (relative to the
+  // reference velocity in the mixed form), in the accumulator tile's space
+  PT* tvel = reinterpret_cast<PT*>(tile);
   // after the accumulator levels (two in the deterministic form)
   uint8_t* touched = reinterpret_cast<uint8_t*>(tile + (DET ? 20 : 10) * TN);
 
@@ -875,17 +871,63 @@ __global__ void __launch_bounds__(fused_threads<CAP>(), fused_min_ctas<CAP>())
       o[1] = (r % c.bg.nby) * B - 1;
       o[2] = DIM == 3 ? (r / c.bg.nby) * B - 1 : 0;
     }
+    // reference velocity of the mixed form: the item's first point (any
+    // value is exact; one close to the item's velocities keeps the
+    // differences small), read here from global memory (the same value the
+    // staged copy receives)
+    double vref[3] = {0.0, 0.0, 0.0};
     if (do_g2p) {
-      for (int t = threadIdx.x; t < TN; t += blockDim.x) {
-        int tx, ty, tz;
-        if (!TileLayout<DIM, T>::node(t, tx, ty, tz)) continue;
-        const int i = o[0] + tx, j = o[1] + ty, k = o[2] + tz;
-        if (i < 0 || j < 0 || k < 0 || i >= g.nn[0] || j >= g.nn[1] || k >= g.nn[2]) continue;
-        const int64_t s = node_slot(g, i, j, k);
+      if constexpr (sizeof(PT) == 4) {
 #pragma unroll
-        for (int d = 0; d < DIM; d++) {
-          tv64[d * TN + t] = c.V.vt[d][s];
-          tv64[(3 + d) * TN + t] = c.V.dv[d][s];
+        for (int d = 0; d < DIM; d++) vref[d] = (double)P.v[d][pstart];
+      }
+      // nodal velocities of the tile
+      if constexpr (sizeof(PT) == 8) {
+        for (int t = threadIdx.x; t < TN; t += blockDim.x) {
+          int tx, ty, tz;
+          if (!TileLayout<DIM, T>::node(t, tx, ty, tz)) continue;
+          const int i = o[0] + tx, j = o[1] + ty, k = o[2] + tz;
+          if (i < 0 || j < 0 || k < 0 || i >= g.nn[0] || j >= g.nn[1] || k >= g.nn[2]) continue;
+          const int64_t s = node_slot(g, i, j, k);
+#pragma unroll
+          for (int d = 0; d < DIM; d++) {
+            tvel[d * TN + t] = c.V.vt[d][s];
+            tvel[(3 + d) * TN + t] = c.V.dv[d][s];
+          }
+        }
+      } else {
+        // mixed form: every thread issues all its loads before its first
+        // shared-memory store (one memory latency per item) and stores the
+        // values in FP32, relative to vref
+        constexpr int NT = fused_threads<CAP>();
+        constexpr int ITER = (TN + NT - 1) / NT;
+        double vv[ITER][2 * DIM];
+        int tt[ITER];
+#pragma unroll
+        for (int it = 0; it < ITER; it++) {
+          const int t = (int)threadIdx.x + it * NT;
+          tt[it] = -1;
+          int tx, ty, tz;
+          if (t >= TN || !TileLayout<DIM, T>::node(t, tx, ty, tz)) continue;
+          const int i = o[0] + tx, j = o[1] + ty, k = o[2] + tz;
+          if (i < 0 || j < 0 || k < 0 || i >= g.nn[0] || j >= g.nn[1] || k >= g.nn[2]) continue;
+          const int64_t s = node_slot(g, i, j, k);
+          tt[it] = t;
+#pragma unroll
+          for (int d = 0; d < DIM; d++) {
+            vv[it][d] = c.V.vt[d][s];
+            vv[it][DIM + d] = c.V.dv[d][s];
+          }
+        }
+#pragma unroll
+        for (int it = 0; it < ITER; it++) {
+          const int t = tt[it];
+          if (t < 0) continue;
+#pragma unroll
+          for (int d = 0; d < DIM; d++) {
+            tvel[d * TN + t] = (PT)(vv[it][d] - vref[d]);
+            tvel[(3 + d) * TN + t] = (PT)vv[it][DIM + d];
+          }
         }
       }
     }
@@ -896,23 +938,6 @@ __global__ void __launch_bounds__(fused_threads<CAP>(), fused_min_ctas<CAP>())
       return;
     }
     parity ^= 1u;
-    double vref[3] = {0.0, 0.0, 0.0};
-    if constexpr (sizeof(PT) == 4) {
-      if (do_g2p) {
-        // reference velocity: the item's first point (any value is exact;
-        // one close to the item's velocities keeps the differences small)
-#pragma unroll
-        for (int d = 0; d < DIM; d++) vref[d] = (double)pts[(kFv + d) * ROW + offp];
-        for (int t = threadIdx.x; t < TN; t += blockDim.x) {
-#pragma unroll
-          for (int d = 0; d < DIM; d++) {
-            tvel[d * TN + t] = (PT)(tv64[d * TN + t] - vref[d]);
-            tvel[(3 + d) * TN + t] = (PT)tv64[(3 + d) * TN + t];
-          }
-        }
-        __syncthreads();
-      }
-    }
     if (do_g2p) {
       for (int j = threadIdx.x; j < n; j += blockDim.x) {
         const int64_t p = pstart + j;
