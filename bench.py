@@ -80,7 +80,7 @@ ENSEMBLE_SEED = 1003
 # captures (profiles/k_g2p2g_ensemble96_mixed.md: the first 96 jobs of the
 # ensemble, scaled to a launch by its points; profiles/k_g2p2g_column_fp64.md:
 # the full column). None where no capture exists.
-TRAFFIC_BYTES_PER_POINT = {("ensemble", "mixed"): 155.6, ("column", "fp64"): 303.4}
+TRAFFIC_BYTES_PER_POINT = {("ensemble", "mixed"): 159.9, ("column", "fp64"): 305.3}
 
 
 def make_workload(name: str, rank: int = 0):
