@@ -896,37 +896,41 @@ __global__ void __launch_bounds__(fused_threads<CAP>(), fused_min_ctas<CAP>())
           }
         }
       } else {
-        // mixed form: every thread issues all its loads before its first
-        // shared-memory store (one memory latency per item) and stores the
-        // values in FP32, relative to vref
+        // mixed form: every thread issues the loads of up to two nodes
+        // before its first shared-memory store (one or two memory latencies
+        // per item) and stores the values in FP32, relative to vref
         constexpr int NT = fused_threads<CAP>();
         constexpr int ITER = (TN + NT - 1) / NT;
-        double vv[ITER][2 * DIM];
-        int tt[ITER];
+        constexpr int CH = ITER > 2 ? 2 : ITER;   // nodes per thread in flight (registers)
+#pragma unroll 1
+        for (int it0 = 0; it0 < ITER; it0 += CH) {
+          double vv[CH][2 * DIM];
+          int tt[CH];
 #pragma unroll
-        for (int it = 0; it < ITER; it++) {
-          const int t = (int)threadIdx.x + it * NT;
-          tt[it] = -1;
-          int tx, ty, tz;
-          if (t >= TN || !TileLayout<DIM, T>::node(t, tx, ty, tz)) continue;
-          const int i = o[0] + tx, j = o[1] + ty, k = o[2] + tz;
-          if (i < 0 || j < 0 || k < 0 || i >= g.nn[0] || j >= g.nn[1] || k >= g.nn[2]) continue;
-          const int64_t s = node_slot(g, i, j, k);
-          tt[it] = t;
+          for (int ic = 0; ic < CH; ic++) {
+            const int t = (int)threadIdx.x + (it0 + ic) * NT;
+            tt[ic] = -1;
+            int tx, ty, tz;
+            if (t >= TN || !TileLayout<DIM, T>::node(t, tx, ty, tz)) continue;
+            const int i = o[0] + tx, j = o[1] + ty, k = o[2] + tz;
+            if (i < 0 || j < 0 || k < 0 || i >= g.nn[0] || j >= g.nn[1] || k >= g.nn[2]) continue;
+            const int64_t s = node_slot(g, i, j, k);
+            tt[ic] = t;
 #pragma unroll
-          for (int d = 0; d < DIM; d++) {
-            vv[it][d] = c.V.vt[d][s];
-            vv[it][DIM + d] = c.V.dv[d][s];
+            for (int d = 0; d < DIM; d++) {
+              vv[ic][d] = c.V.vt[d][s];
+              vv[ic][DIM + d] = c.V.dv[d][s];
+            }
           }
-        }
 #pragma unroll
-        for (int it = 0; it < ITER; it++) {
-          const int t = tt[it];
-          if (t < 0) continue;
+          for (int ic = 0; ic < CH; ic++) {
+            const int t = tt[ic];
+            if (t < 0) continue;
 #pragma unroll
-          for (int d = 0; d < DIM; d++) {
-            tvel[d * TN + t] = (PT)(vv[it][d] - vref[d]);
-            tvel[(3 + d) * TN + t] = (PT)vv[it][DIM + d];
+            for (int d = 0; d < DIM; d++) {
+              tvel[d * TN + t] = (PT)(vv[ic][d] - vref[d]);
+              tvel[(3 + d) * TN + t] = (PT)vv[ic][DIM + d];
+            }
           }
         }
       }
