@@ -58,7 +58,30 @@ def _spinning_block_2d():
     return c
 
 
+def _dense_cells_3d():
+    """A regular block plus two crowded cells of an 8^3 grid: 600 points of
+    one window class in one cell (more than the 255 a class count of the
+    binning's per-cell histogram holds, so that cell keeps arrival order; its
+    bin also exceeds one work item) and 400 points spread over all classes
+    in another."""
+    rng = np.random.default_rng(11)
+    h = 1.0 / 8
+    block = inputs.block_points((2 * h, 2 * h, 2 * h), (6, 6, 6), (h, h, h), 1000.0, (0.3, -0.2, 0.1),
+                                name="block", E=1e5, nu=0.3)
+    vol = h ** 3 / 8
+    one_class = np.array([5, 5, 5]) * h + rng.uniform(0.2, 0.8, size=(600, 3)) * h
+    all_classes = np.array([5, 2, 5]) * h + rng.uniform(0.01, 0.99, size=(400, 3)) * h
+    x = np.vstack([block.x, one_class, all_classes])
+    n = x.shape[0]
+    x_t = np.vstack([block.x_t, rng.uniform(-0.2, 0.2, size=(1000, 3))])
+    body = inputs.Body(name="dense", m=np.full(n, 1000 * vol), v=np.full(n, vol), x=x, x_t=x_t,
+                       active=np.ones(n, np.int32), E=1e5, nu=0.3)
+    return inputs.Case(name="dense_cells_3d", dim=3, L=(1.0, 1.0, 1.0), N=(8, 8, 8), dt=1e-4, steps=10,
+                       bodies=[body])
+
+
 CASES = {
+    "dense_cells_3d": (_dense_cells_3d, 10),
     "wall_exit_2d": (_wall_exit_2d, 25),
     "block_drop_2d": (inputs.block_drop_2d, 120),
     "spinning_block_2d": (_spinning_block_2d, 120),
@@ -110,7 +133,7 @@ def test_step_parity(name):
     _step_parity(name)
 
 
-@pytest.mark.parametrize("name", ["collision_3d_touching", "wall_exit_2d", "spinning_block_2d"])
+@pytest.mark.parametrize("name", ["collision_3d_touching", "wall_exit_2d", "spinning_block_2d", "dense_cells_3d"])
 def test_step_parity_frequent_rebinning(name):
     """Re-binning every 2 steps permutes the point storage; results must not
     change (downloads come back in the original point order)."""
