@@ -338,19 +338,26 @@ mpmgpu_status mpmgpu_batch_destroy(mpmgpu_batch* b);
 
 typedef struct mpmgpu_server mpmgpu_server;
 
+/* cfg->points_per_item = 0 selects 256 for the 3D mixed form (many small
+ * jobs run fastest with small work items) and the batch default otherwise. */
 mpmgpu_status mpmgpu_server_create(const mpmgpu_batch_config* cfg, int64_t budget_bytes, mpmgpu_server** out);
 const char* mpmgpu_server_last_error(const mpmgpu_server* s);
 /* Device bytes the request will reserve from the budget while it runs. */
 mpmgpu_status mpmgpu_server_footprint(const mpmgpu_server* s, const mpmgpu_job_desc* job, int64_t* bytes);
 mpmgpu_status mpmgpu_server_submit(mpmgpu_server* s, const mpmgpu_job_desc* job, int* request_id);
-/* `steps` steps of every running request, then collection of the finished
- * ones (synchronises when a request finishes). */
+/* Queues `steps` steps of every running request. A request that runs its
+ * last step here has its point state copied to pinned host memory and its
+ * device memory released, both in stream order, without waiting; it is
+ * reported finished by the next advance, which converts the copies while the
+ * device runs that call's steps (advance waits for the previous call's
+ * copies, never for the steps it queues). */
 mpmgpu_status mpmgpu_server_advance(mpmgpu_server* s, int steps);
 /* Ids of requests finished since the last poll (at most max_ids); returns
  * their number. */
 int mpmgpu_server_poll(mpmgpu_server* s, int* ids, int max_ids);
-/* State (1 running, 2 finished, 3 released), admission and completion
- * times on mpmgpu_server_clock, points and steps of a request. */
+/* State (1 running, 4 being copied out, 2 finished, 3 released),
+ * admission and completion times on mpmgpu_server_clock, points and steps
+ * of a request. */
 mpmgpu_status mpmgpu_server_request(const mpmgpu_server* s, int id, int* state, double* t_admit, double* t_done,
                                     int64_t* points, int64_t* steps);
 /* A finished request's final point field (MPMGPU_P_X, _U, _X_T, _T, _V or

@@ -413,8 +413,13 @@ mpmgpu_status mpmgpu_server_create(const mpmgpu_batch_config* cfg, int64_t budge
     return MPMGPU_ERR_UNSUPPORTED;
   mpmgpu_status st = MPMGPU_OK;
   std::string msg;
-  auto b = make_batch(cfg->dim, cfg->mode, cfg->device, cfg->sort_interval, cfg->points_per_item, !cfg->no_graph,
-                      cfg->keep_debug, &st, &msg);
+  // a stream of requests is a batch of many small jobs: in 3D the mixed form
+  // runs them fastest with 256-point work items (the autotuner's choice on
+  // the block-drop ensemble), unless the caller picks the size
+  const int cap = cfg->points_per_item != 0 ? cfg->points_per_item
+                                            : (cfg->dim == 3 && cfg->mode == MPMGPU_MODE_MIXED ? 256 : 0);
+  auto b = make_batch(cfg->dim, cfg->mode, cfg->device, cfg->sort_interval, cap, !cfg->no_graph, cfg->keep_debug, &st,
+                      &msg);
   if (st != MPMGPU_OK) return st;
   auto srv = std::make_unique<mpmgpu_server>();
   srv->s = std::make_unique<Server>(std::move(b), cfg->mode == MPMGPU_MODE_MIXED, cfg->keep_debug != 0, budget_bytes);

@@ -169,6 +169,16 @@ class BatchBase {
   virtual mpmgpu_status remove_job(int job) = 0;
   virtual mpmgpu_status job_state(int job, int64_t* done, int64_t* left) const = 0;
   virtual mpmgpu_status download_points(int job, int body, int field, double* out) = 0;
+  // Raw point state of a body copied to host memory in stream order, i.e.
+  // as it stands after the work queued so far (without waiting): x, u, x_t
+  // (3 arrays each), stress (6) and V in the point precision, then active
+  // and pid (int32). `host` is pinned and holds snapshot_bytes(n).
+  virtual size_t snapshot_bytes(int64_t n) const = 0;
+  virtual mpmgpu_status snapshot_body(int job, int body, void* host) = 0;
+  // The fields of a completed snapshot in reference point order, as
+  // download_points gives them (x, u, x_t: 3 per point; T: 9; V; active).
+  virtual void snapshot_fields(const void* host, int64_t n, double* x, double* u, double* x_t, double* T, double* v,
+                               double* active) const = 0;
   virtual mpmgpu_status download_nodes(int job, int body, int field, double* out) = 0;
   virtual mpmgpu_status download_contact(int job, int contact, int field, double* out) = 0;
   virtual mpmgpu_status sizes(int job, int body, int64_t* n_points, int64_t* n_nodes) const = 0;
@@ -644,6 +654,52 @@ class Batch : public BatchBase {
       }
     }
     return fail(MPMGPU_ERR_ARG, "unknown point field");
+  }
+
+  size_t snapshot_bytes(int64_t n) const override { return (size_t)n * (16 * sizeof(PT) + 2 * sizeof(int32_t)); }
+
+  mpmgpu_status snapshot_body(int job, int body, void* host) override {
+    HJob* j;
+    HBody* B;
+    MPM_TRY(readable_body(job, body, &j, &B));
+    const size_t n = (size_t)B->n;
+    if (n == 0) return MPMGPU_OK;
+    PT* h = static_cast<PT*>(host);
+    const PT* src[16] = {B->P.x[0], B->P.x[1], B->P.x[2], B->P.u[0], B->P.u[1], B->P.u[2], B->P.v[0], B->P.v[1],
+                         B->P.v[2], B->P.s[0], B->P.s[1], B->P.s[2], B->P.s[3], B->P.s[4], B->P.s[5], B->P.vol};
+    for (int a = 0; a < 16; a++) {
+      // x, u and x_t exist for the grid's axes only
+      if (a < 9 && a % 3 >= dim_) continue;
+      MPM_CUDA_TRY(cudaMemcpyAsync(h + a * n, src[a], n * sizeof(PT), cudaMemcpyDeviceToHost, stream_));
+    }
+    int32_t* hi = reinterpret_cast<int32_t*>(h + 16 * n);
+    MPM_CUDA_TRY(cudaMemcpyAsync(hi, B->P.active, n * sizeof(int32_t), cudaMemcpyDeviceToHost, stream_));
+    MPM_CUDA_TRY(cudaMemcpyAsync(hi + n, B->P.pid, n * sizeof(int32_t), cudaMemcpyDeviceToHost, stream_));
+    return MPMGPU_OK;
+  }
+
+  void snapshot_fields(const void* host, int64_t n64, double* x, double* u, double* x_t, double* T, double* v,
+                       double* active) const override {
+    const size_t n = (size_t)n64;
+    const PT* h = static_cast<const PT*>(host);
+    const int32_t* act = reinterpret_cast<const int32_t*>(h + 16 * n);
+    const int32_t* pid = act + n;
+    static const int idx[9] = {0, 3, 5, 3, 1, 4, 5, 4, 2};
+    for (size_t i = 0; i < n; i++) {
+      const size_t q = (size_t)pid[i];
+      for (int d = 0; d < 3; d++) {
+        const bool on = d < dim_;
+        // the mixed form keeps x0 in the x arrays: x = x0 + u (in FP32)
+        const PT xv = on ? (sizeof(PT) == 4 ? (PT)(h[d * n + i] + h[(3 + d) * n + i]) : h[d * n + i]) : PT(0);
+        x[3 * q + d] = on ? (double)xv : 0.0;
+        u[3 * q + d] = on ? (double)h[(3 + d) * n + i] : 0.0;
+        x_t[3 * q + d] = on ? (double)h[(6 + d) * n + i] : 0.0;
+      }
+      for (int k = 0; k < 9; k++) T[9 * q + k] = (double)h[(9 + idx[k]) * n + i];
+      v[q] = (double)h[15 * n + i];
+      // 2 = left the domain at the last move: still active, as download_points
+      active[q] = act[i] != 0 ? 1.0 : 0.0;
+    }
   }
 
   mpmgpu_status download_nodes(int job, int body, int field, double* out) override {

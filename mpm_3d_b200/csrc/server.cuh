@@ -5,6 +5,13 @@
 // copied to host memory and their device memory released, so that queued
 // requests can take its place.
 //
+// Collection never stalls the device: the round in which a request runs
+// its last step is followed, in stream order, by copies of its point
+// arrays into pinned host memory and by the release of its device memory;
+// the host converts those copies during the next advance, while the device
+// runs the next round. A request is reported finished once its copies are
+// converted (at most one round after its last step).
+//
 // The caller owns the queue and the clock of arrivals: submit() either
 // admits a request at once or answers that it does not fit now (the caller
 // keeps it and retries after the next advance()).
@@ -12,6 +19,7 @@
 
 #include <chrono>
 #include <deque>
+#include <map>
 #include <memory>
 #include <string>
 #include <vector>
@@ -28,7 +36,7 @@ class Server {
   };
   struct Request {
     int job = -1;
-    int state = 0;  // 1 running, 2 done, 3 released
+    int state = 0;  // 1 running, 4 copying out, 2 done, 3 released
     int64_t footprint = 0;
     int64_t points = 0;
     int64_t steps = 0;
@@ -39,6 +47,14 @@ class Server {
   Server(std::unique_ptr<BatchBase> b, bool mixed, bool keep_debug, int64_t budget)
       : batch_(std::move(b)), mixed_(mixed), keep_debug_(keep_debug), budget_(budget),
         t0_(std::chrono::steady_clock::now()) {}
+
+  ~Server() {
+    batch_->synchronize();
+    for (auto& p : pending_) cudaEventDestroy(p.ev);
+    for (cudaEvent_t e : events_) cudaEventDestroy(e);
+    for (auto& kv : pinned_) cudaFreeHost(kv.second);
+    for (auto& kv : pinned_size_) cudaFreeHost(kv.first);
+  }
 
   std::string last_error;
   mpmgpu_status fail(mpmgpu_status s, const std::string& m) {
@@ -100,39 +116,29 @@ class Server {
     return MPMGPU_OK;
   }
 
-  // `steps` steps of every running request, then collection of the ones
-  // that have run all their steps (results to host memory, device memory
-  // released).
+  // `steps` steps of every running request. Requests that run their last
+  // step in this call are copied out and released in stream order; those
+  // copied out by earlier calls are converted to host results and reported
+  // (they were queued before this call's steps, so their copies complete
+  // while the device runs them).
   mpmgpu_status advance(int steps) {
     if (steps < 0) return fail(MPMGPU_ERR_ARG, "negative step count");
+    std::vector<Pending> earlier;
+    earlier.swap(pending_);
     mpmgpu_status st = batch_->step(steps);
     if (st != MPMGPU_OK) return fail(st, batch_->last_error);
-    bool any = false;
-    for (auto& r : reqs_) {
-      if (r.state != 1) continue;
-      int64_t done = 0, left = 0;
-      batch_->job_state(r.job, &done, &left);
-      if (left == 0) any = true;
-    }
-    if (!any) return MPMGPU_OK;
-    st = batch_->synchronize();
-    if (st != MPMGPU_OK) return fail(st, batch_->last_error);
-    const double now = clock();
     for (int id = 0; id < (int)reqs_.size(); id++) {
       Request& r = reqs_[(size_t)id];
       if (r.state != 1) continue;
       int64_t done = 0, left = 0;
       batch_->job_state(r.job, &done, &left);
       if (left != 0) continue;
-      st = collect(r);
+      st = copy_out(id);
       if (st != MPMGPU_OK) return st;
-      batch_->remove_job(r.job);
-      r.state = 2;
-      r.t_done = now;
-      running_--;
-      reserved_ -= r.footprint;
-      points_done_ += r.points * r.steps;
-      finished_.push_back(id);
+    }
+    for (auto& p : earlier) {
+      st = finish(p);
+      if (st != MPMGPU_OK) return st;
     }
     return MPMGPU_OK;
   }
@@ -200,30 +206,99 @@ class Server {
   BatchBase* batch() { return batch_.get(); }
 
  private:
-  mpmgpu_status collect(Request& r) {
+  struct Pending {
+    int id = -1;
+    cudaEvent_t ev = nullptr;
+    std::vector<std::pair<void*, int64_t>> bodies;  // pinned snapshot, points
+  };
+
+  // Pinned host buffers for the snapshots, reused by size.
+  mpmgpu_status pinned_get(size_t bytes, void** out) {
+    auto it = pinned_.lower_bound(bytes);
+    if (it != pinned_.end()) {
+      *out = it->second;
+      pinned_size_[it->second] = it->first;
+      pinned_.erase(it);
+      return MPMGPU_OK;
+    }
+    const size_t cap = std::max<size_t>(bytes, (size_t)1 << 20);
+    void* h = nullptr;
+    cudaError_t e = cudaHostAlloc(&h, cap, cudaHostAllocDefault);
+    if (e != cudaSuccess) return fail(MPMGPU_ERR_CUDA, std::string("cudaHostAlloc: ") + cudaGetErrorString(e));
+    pinned_size_[h] = cap;
+    *out = h;
+    return MPMGPU_OK;
+  }
+  void pinned_put(void* h) {
+    auto it = pinned_size_.find(h);
+    pinned_.emplace(it->second, h);
+    pinned_size_.erase(it);
+  }
+
+  // Queues the copies of a finished request's bodies and its release; the
+  // request leaves the budget now (its memory returns to the pool after
+  // the copies, in stream order).
+  mpmgpu_status copy_out(int id) {
+    Request& r = reqs_[(size_t)id];
+    Pending p;
+    p.id = id;
     int64_t npts = 0;
     for (int b = 0;; b++) {
       if (batch_->sizes(r.job, b, &npts, nullptr) != MPMGPU_OK) break;
-      Result res;
-      res.n = npts;
-      res.x.resize((size_t)(3 * npts));
-      res.u.resize((size_t)(3 * npts));
-      res.x_t.resize((size_t)(3 * npts));
-      res.T.resize((size_t)(9 * npts));
-      res.v.resize((size_t)npts);
-      res.active.resize((size_t)npts);
-      mpmgpu_status st = MPMGPU_OK;
-      if (npts > 0) {
-        if (st == MPMGPU_OK) st = batch_->download_points(r.job, b, MPMGPU_P_X, res.x.data());
-        if (st == MPMGPU_OK) st = batch_->download_points(r.job, b, MPMGPU_P_U, res.u.data());
-        if (st == MPMGPU_OK) st = batch_->download_points(r.job, b, MPMGPU_P_X_T, res.x_t.data());
-        if (st == MPMGPU_OK) st = batch_->download_points(r.job, b, MPMGPU_P_T, res.T.data());
-        if (st == MPMGPU_OK) st = batch_->download_points(r.job, b, MPMGPU_P_V, res.v.data());
-        if (st == MPMGPU_OK) st = batch_->download_points(r.job, b, MPMGPU_P_ACTIVE, res.active.data());
+      void* h = nullptr;
+      mpmgpu_status st = pinned_get(std::max<size_t>(batch_->snapshot_bytes(npts), 1), &h);
+      if (st == MPMGPU_OK) st = batch_->snapshot_body(r.job, b, h);
+      if (st != MPMGPU_OK) {
+        if (h) pinned_put(h);
+        for (auto& hb : p.bodies) pinned_put(hb.first);
+        return fail(st, batch_->last_error);
       }
-      if (st != MPMGPU_OK) return fail(st, batch_->last_error);
+      p.bodies.emplace_back(h, npts);
+    }
+    if (events_.empty()) {
+      cudaEvent_t e = nullptr;
+      cudaError_t ce = cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+      if (ce != cudaSuccess) return fail(MPMGPU_ERR_CUDA, std::string("cudaEventCreate: ") + cudaGetErrorString(ce));
+      events_.push_back(e);
+    }
+    p.ev = events_.back();
+    events_.pop_back();
+    cudaError_t ce = cudaEventRecord(p.ev, batch_->stream());
+    if (ce != cudaSuccess) return fail(MPMGPU_ERR_CUDA, std::string("cudaEventRecord: ") + cudaGetErrorString(ce));
+    batch_->remove_job(r.job);
+    r.state = 4;
+    running_--;
+    reserved_ -= r.footprint;
+    points_done_ += r.points * r.steps;
+    pending_.push_back(std::move(p));
+    return MPMGPU_OK;
+  }
+
+  // Waits for a request's copies, converts them and reports it finished.
+  mpmgpu_status finish(Pending& p) {
+    cudaError_t ce = cudaEventSynchronize(p.ev);
+    events_.push_back(p.ev);
+    if (ce != cudaSuccess) return fail(MPMGPU_ERR_CUDA, std::string("snapshot copy: ") + cudaGetErrorString(ce));
+    Request& r = reqs_[(size_t)p.id];
+    for (auto& hb : p.bodies) {
+      Result res;
+      const int64_t n = hb.second;
+      res.n = n;
+      res.x.assign((size_t)(3 * n), 0.0);
+      res.u.assign((size_t)(3 * n), 0.0);
+      res.x_t.assign((size_t)(3 * n), 0.0);
+      res.T.assign((size_t)(9 * n), 0.0);
+      res.v.assign((size_t)n, 0.0);
+      res.active.assign((size_t)n, 0.0);
+      if (n > 0)
+        batch_->snapshot_fields(hb.first, n, res.x.data(), res.u.data(), res.x_t.data(), res.T.data(), res.v.data(),
+                                res.active.data());
+      pinned_put(hb.first);
       r.bodies.push_back(std::move(res));
     }
+    r.state = 2;
+    r.t_done = clock();
+    finished_.push_back(p.id);
     return MPMGPU_OK;
   }
 
@@ -237,6 +312,10 @@ class Server {
   int running_ = 0;
   int64_t reserved_ = 0;
   int64_t points_done_ = 0;
+  std::vector<Pending> pending_;
+  std::vector<cudaEvent_t> events_;
+  std::multimap<size_t, void*> pinned_;        // free pinned buffers by size
+  std::map<void*, size_t> pinned_size_;        // pinned buffers in use
 };
 
 }  // namespace mpmb200
