@@ -1350,7 +1350,7 @@ class Batch : public BatchBase {
     fl.prime_pass = prime_pass;
     fl.phases = phases;
     fl.bounds = bounds_;
-    constexpr size_t smem = fused_smem_bytes<DIM, PT, CAP, DET>();
+    constexpr size_t smem = fused_smem_bytes<DIM, PT, CAP, NORMAL, DET>();
     auto kern = k_g2p2g<DIM, PT, CAP, NORMAL, SINGLE, DET>;
     // resident CTAs per SM, looked up once per kernel (before any capture)
     int& per_sm = fused_per_sm_[((CAP == 256 ? 0 : (CAP == 512 ? 1 : 2)) * 4 + (NORMAL ? 2 : 0) + (SINGLE ? 1 : 0)) * 2 +

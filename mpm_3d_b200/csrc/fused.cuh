@@ -136,11 +136,30 @@ template <typename PT, int CAP>
 __host__ __device__ constexpr size_t off_tile() {
   return off_act<PT, CAP>() + sizeof(int32_t) * cap_row<CAP>();
 }
-// Accumulator tile levels: 1, or 2 in the deterministic form.
-template <int DIM, typename PT, int CAP, bool DET>
+// The mixed form without contact normals keeps its FP32 velocity tile apart
+// from its 7 accumulator rows (the bytes of 10 rows in all), so that a
+// point can scatter while others still gather; the other kernels keep the
+// velocity tile in the accumulator tile's space.
+template <typename PT, bool NORMAL, bool DET>
+__host__ __device__ constexpr bool split_tiles() {
+  return sizeof(PT) == 4 && !NORMAL && !DET;
+}
+// Accumulator tile levels: 1, or 2 in the deterministic form; then the
+// touched flags; then the separate velocity tile where there is one.
+template <int DIM, typename PT, int CAP, bool NORMAL, bool DET>
+__host__ __device__ constexpr size_t off_touched() {
+  return off_tile<PT, CAP>() +
+         sizeof(double) * (DET ? 20 : (split_tiles<PT, NORMAL, DET>() ? 7 : 10)) * fused_tile_nodes<DIM, fused_bin<DIM>()>();
+}
+template <int DIM, typename PT, int CAP, bool NORMAL, bool DET>
+__host__ __device__ constexpr size_t off_tvel() {
+  return (off_touched<DIM, PT, CAP, NORMAL, DET>() + fused_tile_nodes<DIM, fused_bin<DIM>()>() + 15) / 16 * 16;
+}
+template <int DIM, typename PT, int CAP, bool NORMAL, bool DET>
 __host__ __device__ constexpr size_t fused_smem_bytes() {
-  return off_tile<PT, CAP>() + sizeof(double) * (DET ? 20 : 10) * fused_tile_nodes<DIM, fused_bin<DIM>()>() +
-         fused_tile_nodes<DIM, fused_bin<DIM>()>();
+  return split_tiles<PT, NORMAL, DET>()
+             ? off_tvel<DIM, PT, CAP, NORMAL, DET>() + sizeof(PT) * 6 * fused_tile_nodes<DIM, fused_bin<DIM>()>()
+             : off_touched<DIM, PT, CAP, NORMAL, DET>() + fused_tile_nodes<DIM, fused_bin<DIM>()>();
 }
 
 // Threads per CTA and the resident CTAs per SM the register budget is sized
@@ -761,6 +780,39 @@ __device__ __forceinline__ void map_scatter(const BodyCtx<PT>& c, int* err, unsi
     scatter_general<DIM, T, TN, NORMAL, DET>(c, drift, pm, o, q, tacc, touched, ks);
 }
 
+// Phase 3: adds the touched nodes of the tile into the body's global
+// accumulators (one global atomic per node and value) and flags their node
+// blocks for the grid update.
+template <int DIM, int T, int TN, bool NORMAL, bool DET, typename PT>
+__device__ __forceinline__ void flush_tile(const BodyCtx<PT>& c, const Geom& g, const int* o, const double* tile,
+                                           const uint8_t* touched) {
+  for (int t = threadIdx.x; t < TN; t += blockDim.x) {
+    if (!touched[t]) continue;
+    int tx, ty, tz;
+    TileLayout<DIM, T>::node(t, tx, ty, tz);
+    const int i = o[0] + tx, j = o[1] + ty, k = o[2] + tz;
+    const int64_t s = node_slot(g, i, j, k);
+    c.flags[node_block(g, i, j, k)] = 1u;
+    atomicAdd(c.A.m + s, tile[t]);
+#pragma unroll
+    for (int d = 0; d < DIM; d++) {
+      atomicAdd(c.A.mx[d] + s, tile[(1 + d) * TN + t]);
+      atomicAdd(c.A.f[d] + s, tile[(4 + d) * TN + t]);
+      if (NORMAL) atomicAdd(c.A.nrm[d] + s, tile[(7 + d) * TN + t]);
+    }
+    if constexpr (DET) {
+      const double* t1 = tile + 10 * TN;
+      atomicAdd(c.Ar.m + s, t1[t]);
+#pragma unroll
+      for (int d = 0; d < DIM; d++) {
+        atomicAdd(c.Ar.mx[d] + s, t1[(1 + d) * TN + t]);
+        atomicAdd(c.Ar.f[d] + s, t1[(4 + d) * TN + t]);
+        if (NORMAL) atomicAdd(c.Ar.nrm[d] + s, t1[(7 + d) * TN + t]);
+      }
+    }
+  }
+}
+
 template <int DIM, typename PT, int CAP, bool NORMAL, bool SINGLE, bool DET>
 __global__ void __launch_bounds__(fused_threads<CAP>(), fused_min_ctas<CAP>())
     k_g2p2g(const __grid_constant__ FusedLaunch<PT> fl) {
@@ -783,9 +835,10 @@ __global__ void __launch_bounds__(fused_threads<CAP>(), fused_min_ctas<CAP>())
   double* tile = reinterpret_cast<double*>(smem + off_tile<PT, CAP>());  // phase 2: NACC FP64 values
   // phase 1: nodal vt0..2 dv0..2 in the point precision (relative to the
   // reference velocity in the mixed form), in the accumulator tile's space
-  PT* tvel = reinterpret_cast<PT*>(tile);
+  constexpr bool SPLIT = split_tiles<PT, NORMAL, DET>();
+  PT* tvel = SPLIT ? reinterpret_cast<PT*>(smem + off_tvel<DIM, PT, CAP, NORMAL, DET>()) : reinterpret_cast<PT*>(tile);
   // after the accumulator levels (two in the deterministic form)
-  uint8_t* touched = reinterpret_cast<uint8_t*>(tile + (DET ? 20 : 10) * TN);
+  uint8_t* touched = smem + off_touched<DIM, PT, CAP, NORMAL, DET>();
 
   if (threadIdx.x == 0) {
     mbar_init(bar, 1);
@@ -935,6 +988,13 @@ __global__ void __launch_bounds__(fused_threads<CAP>(), fused_min_ctas<CAP>())
         }
       }
     }
+    if constexpr (SPLIT) {
+      // the accumulators are cleared while the point arrays arrive
+      if (do_p2g) {
+        for (int t = threadIdx.x; t < 7 * TN; t += blockDim.x) tile[t] = 0.0;
+        for (int t = threadIdx.x; t < TN; t += blockDim.x) touched[t] = 0;
+      }
+    }
     const bool arrived = mbar_wait_bounded(bar, parity, fl.err);
     // one decision for the whole CTA (also the barrier after the tile loads)
     if (__syncthreads_or(arrived ? 0 : 1)) {
@@ -942,6 +1002,33 @@ __global__ void __launch_bounds__(fused_threads<CAP>(), fused_min_ctas<CAP>())
       return;
     }
     parity ^= 1u;
+    if constexpr (SPLIT) {
+      // each thread takes its points through gather, update, map and
+      // scatter in one go
+      for (int j = threadIdx.x; j < n; j += blockDim.x) {
+        const int64_t p = pstart + j;
+        const int a = act[off4 + j];
+        if (a == 0) continue;
+        if (do_g2p) {
+          if (a == 2) {
+            // left the domain at the last move; generateMap deactivates it now
+            P.active[p] = 0;
+            act[off4 + j] = 0;
+            continue;
+          }
+          gather_update<DIM, T, TN, ROW, DET>(c, fl.err, fl.drift, p, pts + offp + j, o, tvel, vref);
+        }
+        if (do_p2g && a == 1)
+          map_scatter<DIM, T, TN, ROW, NORMAL, DET>(c, fl.err, fl.drift, p, pts + offp + j, o, prime ? 0 : 1, tile,
+                                                     touched, ksplit);
+      }
+      if (do_p2g) {
+        __syncthreads();
+        flush_tile<DIM, T, TN, NORMAL, DET>(c, g, o, tile, touched);
+      }
+      __syncthreads();
+      continue;
+    }
     if (do_g2p) {
       for (int j = threadIdx.x; j < n; j += blockDim.x) {
         const int64_t p = pstart + j;
@@ -979,31 +1066,7 @@ __global__ void __launch_bounds__(fused_threads<CAP>(), fused_min_ctas<CAP>())
                                                    tile, touched, ksplit);
       }
       __syncthreads();
-      for (int t = threadIdx.x; t < TN; t += blockDim.x) {
-        if (!touched[t]) continue;
-        int tx, ty, tz;
-        TileLayout<DIM, T>::node(t, tx, ty, tz);
-        const int i = o[0] + tx, j = o[1] + ty, k = o[2] + tz;
-        const int64_t s = node_slot(g, i, j, k);
-        c.flags[node_block(g, i, j, k)] = 1u;
-        atomicAdd(c.A.m + s, tile[t]);
-#pragma unroll
-        for (int d = 0; d < DIM; d++) {
-          atomicAdd(c.A.mx[d] + s, tile[(1 + d) * TN + t]);
-          atomicAdd(c.A.f[d] + s, tile[(4 + d) * TN + t]);
-          if (NORMAL) atomicAdd(c.A.nrm[d] + s, tile[(7 + d) * TN + t]);
-        }
-        if constexpr (DET) {
-          const double* t1 = tile + 10 * TN;
-          atomicAdd(c.Ar.m + s, t1[t]);
-#pragma unroll
-          for (int d = 0; d < DIM; d++) {
-            atomicAdd(c.Ar.mx[d] + s, t1[(1 + d) * TN + t]);
-            atomicAdd(c.Ar.f[d] + s, t1[(4 + d) * TN + t]);
-            if (NORMAL) atomicAdd(c.Ar.nrm[d] + s, t1[(7 + d) * TN + t]);
-          }
-        }
-      }
+      flush_tile<DIM, T, TN, NORMAL, DET>(c, g, o, tile, touched);
     }
     __syncthreads();
   }
