@@ -506,8 +506,8 @@ __device__ __forceinline__ constexpr int tile_field(int i) {
 }
 
 // Adds one node's values to the shared FP64 tile (shared-memory FP64
-// atomics). Issuing the compare-and-swap steps of all values together was
-// measured slower than the plain atomics (register pressure).
+// atomics). A hand-written variant that interleaved compare-and-swap loops
+// over all of a node's values was measured slower (register pressure).
 template <int DIM, bool NORMAL, int TN, bool DET, typename R>
 __device__ __forceinline__ void tile_add_node(double* tacc, int t, const NodeVals<DIM, NORMAL, R>& nv,
                                               const Split2* ks) {
