@@ -133,7 +133,7 @@ inline int64_t job_footprint(const mpmgpu_config& cfg, bool mixed, bool keep_deb
   int64_t bytes = 0;
   for (int b = 0; b < nbodies; b++) {
     const int64_t n = npts[b] + 8;
-    bytes += 2 * n * (18 * ps + 8);             // two point buffers
+    bytes += 2 * n * (18 * ps + 8) + 64 * 256;  // two point buffers (+ alignment of the arrays)
     if (keep_debug && !mixed) bytes += 2 * n * 72;
     bytes += g.nslots * 8 * (7 + 6);            // accumulators + velocities
     bytes += n * 10;                             // sort key, rank, class rank
@@ -345,8 +345,35 @@ class Batch : public BatchBase {
     HBody B;
     B.n = n;
     MPM_TRY(stage_reserve((size_t)n * (18 * sizeof(PT) + 8) + 64 * 256));
-    MPM_TRY(alloc_points(B.P, n, B.allocs, j->bytes));
-    MPM_TRY(alloc_points(B.Palt, n, B.allocs, j->bytes));
+    const size_t ns = (size_t)j->g.nslots;
+    // both point buffers and the nodal arrays of the body
+    MPM_TRY(alloc_arena(
+        [&](Arena& a) {
+          layout_points(a, B.P, n);
+          layout_points(a, B.Palt, n);
+          if (det_) {
+            carve(a, &B.Ar.m, ns);
+            for (int d = 0; d < 3; d++) {
+              carve(a, &B.Ar.mx[d], ns);
+              carve(a, &B.Ar.f[d], ns);
+            }
+          }
+          carve(a, &B.A.m, ns);
+          for (int d = 0; d < 3; d++) {
+            carve(a, &B.A.mx[d], ns);
+            carve(a, &B.A.f[d], ns);
+            carve(a, &B.V.vt[d], ns);
+            carve(a, &B.V.dv[d], ns);
+          }
+          if (keep_debug_) {
+            carve(a, &B.snap.m, ns);
+            for (int d = 0; d < 3; d++) {
+              carve(a, &B.snap.mx[d], ns);
+              carve(a, &B.snap.f[d], ns);
+            }
+          }
+        },
+        B.allocs, j->bytes));
     if (n > 0) {
       std::vector<PT> tmp((size_t)n);
       auto col = [&](const double* aos, int w, int d) {
@@ -389,28 +416,6 @@ class Batch : public BatchBase {
       }
       MPM_TRY(upload(B.P.active, act));
       MPM_TRY(upload(B.P.pid, pid));
-    }
-    const size_t ns = (size_t)j->g.nslots;
-    if (det_) {
-      MPM_TRY(alloc_dev(&B.Ar.m, ns, B.allocs, j->bytes));
-      for (int d = 0; d < 3; d++) {
-        MPM_TRY(alloc_dev(&B.Ar.mx[d], ns, B.allocs, j->bytes));
-        MPM_TRY(alloc_dev(&B.Ar.f[d], ns, B.allocs, j->bytes));
-      }
-    }
-    MPM_TRY(alloc_dev(&B.A.m, ns, B.allocs, j->bytes));
-    for (int d = 0; d < 3; d++) {
-      MPM_TRY(alloc_dev(&B.A.mx[d], ns, B.allocs, j->bytes));
-      MPM_TRY(alloc_dev(&B.A.f[d], ns, B.allocs, j->bytes));
-      MPM_TRY(alloc_dev(&B.V.vt[d], ns, B.allocs, j->bytes));
-      MPM_TRY(alloc_dev(&B.V.dv[d], ns, B.allocs, j->bytes));
-    }
-    if (keep_debug_) {
-      MPM_TRY(alloc_dev(&B.snap.m, ns, B.allocs, j->bytes));
-      for (int d = 0; d < 3; d++) {
-        MPM_TRY(alloc_dev(&B.snap.mx[d], ns, B.allocs, j->bytes));
-        MPM_TRY(alloc_dev(&B.snap.f[d], ns, B.allocs, j->bytes));
-      }
     }
     B.mat = make_material(desc.has_material, desc.E, desc.nu);
     B.has_boundary = desc.has_boundary;
@@ -909,27 +914,58 @@ class Batch : public BatchBase {
     return MPMGPU_OK;
   }
 
+  // A body's arrays are carved out of one pool allocation: one allocation,
+  // one clear and one release per body instead of one per array. The first
+  // pass of a layout only sums the sizes (base null), the second hands out
+  // 256-byte aligned sub-arrays.
+  struct Arena {
+    unsigned char* base = nullptr;
+    size_t used = 0;
+  };
+  template <typename T>
+  static void carve(Arena& a, T** p, size_t count) {
+    const size_t nb = (std::max<size_t>(count * sizeof(T), 16) + 255) / 256 * 256;
+    *p = a.base ? reinterpret_cast<T*>(a.base + a.used) : nullptr;
+    a.used += nb;
+  }
+  template <typename F>
+  mpmgpu_status alloc_arena(F&& layout, std::vector<void*>& owner, int64_t& bytes) {
+    Arena a;
+    layout(a);
+    const size_t total = std::max<size_t>(a.used, 256);
+    void* q = nullptr;
+    cudaError_t e = cudaMallocFromPoolAsync(&q, total, pool_, copy_stream_);
+    if (e != cudaSuccess) return fail(MPMGPU_ERR_NOMEM, std::string("cudaMallocFromPoolAsync: ") + cudaGetErrorString(e));
+    owner.push_back(q);
+    e = cudaMemsetAsync(q, 0, total, copy_stream_);
+    if (e != cudaSuccess) return fail(MPMGPU_ERR_CUDA, std::string("cudaMemset: ") + cudaGetErrorString(e));
+    Arena b;
+    b.base = static_cast<unsigned char*>(q);
+    layout(b);
+    bytes += (int64_t)total;
+    return MPMGPU_OK;
+  }
+
   // Point arrays hold n entries plus 8 of padding: the fused kernel's bulk
   // copies round their windows out to 16-byte boundaries and may read up to
   // 3 entries past the last point.
-  mpmgpu_status alloc_points(PointsT<PT>& P, int64_t n, std::vector<void*>& owner, int64_t& bytes) {
+  void layout_points(Arena& a, PointsT<PT>& P, int64_t n) {
     P = PointsT<PT>{};
     P.n = n;
     const size_t na = (size_t)n + 8;
     for (int d = 0; d < 3; d++) {
-      MPM_TRY(alloc_dev(&P.x[d], na, owner, bytes));
-      MPM_TRY(alloc_dev(&P.v[d], na, owner, bytes));
-      MPM_TRY(alloc_dev(&P.u[d], na, owner, bytes));
+      carve(a, &P.x[d], na);
+      carve(a, &P.v[d], na);
+      carve(a, &P.u[d], na);
     }
-    for (int c = 0; c < 6; c++) MPM_TRY(alloc_dev(&P.s[c], na, owner, bytes));
-    MPM_TRY(alloc_dev(&P.vol, na, owner, bytes));
-    MPM_TRY(alloc_dev(&P.m, na, owner, bytes));
-    MPM_TRY(alloc_dev(&P.ext, na, owner, bytes));
-    MPM_TRY(alloc_dev(&P.active, na, owner, bytes));
-    MPM_TRY(alloc_dev(&P.pid, na, owner, bytes));
+    for (int c = 0; c < 6; c++) carve(a, &P.s[c], na);
+    carve(a, &P.vol, na);
+    carve(a, &P.m, na);
+    carve(a, &P.ext, na);
+    carve(a, &P.active, na);
+    carve(a, &P.pid, na);
     P.L = nullptr;
-    if (keep_debug_ && !mixed()) MPM_TRY(alloc_dev(&P.L, (size_t)n * 9, owner, bytes));
-    return MPMGPU_OK;
+    if (keep_debug_ && !mixed()) carve(a, &P.L, (size_t)n * 9);
   }
 
   // Returns a job's arrays to the pool after the work already queued on the
