@@ -287,6 +287,7 @@ class Batch : public BatchBase {
     for (void* p : cap_allocs_) cudaFree(p);
     if (pool_) cudaMemPoolDestroy(pool_);
     if (stage_) cudaFreeHost(stage_);
+    if (dl_stage_) cudaFreeHost(dl_stage_);
     if (upload_ev_) cudaEventDestroy(upload_ev_);
     if (copy_stream_) cudaStreamDestroy(copy_stream_);
     if (stream_) cudaStreamDestroy(stream_);
@@ -580,81 +581,107 @@ class Batch : public BatchBase {
     HJob* j;
     HBody* B;
     MPM_TRY(readable_body(job, body, &j, &B));
-    MPM_TRY(synchronize());
     const int64_t n = B->n;
+    const size_t nz = (size_t)n;
     const int D = dim_;
-    std::vector<int32_t> pid;
-    MPM_TRY(download(pid, B->P.pid, (size_t)n));
-    std::vector<PT> tmp;
-    auto vec3 = [&](PT* const* arr) -> mpmgpu_status {
+    if (field == MPMGPU_P_B) {
+      MPM_TRY(synchronize());
+      for (int64_t i = 0; i < n; i++)
+        for (int d = 0; d < 3; d++) out[3 * i + d] = j->sp.grav[d];
+      return MPMGPU_OK;
+    }
+    if (field == MPMGPU_P_L && !B->P.L) return fail(MPMGPU_ERR_STATE, "L is kept only with keep_debug in the FP64 form");
+    // the point ids and the arrays of the field, copied with one wait
+    std::vector<std::pair<const void*, size_t>> items;
+    items.emplace_back(B->P.pid, nz * sizeof(int32_t));
+    const size_t np = nz * sizeof(PT);
+    switch (field) {
+      case MPMGPU_P_X:
+        for (int d = 0; d < D; d++) items.emplace_back(B->P.x[d], np);
+        if constexpr (sizeof(PT) == 4)
+          for (int d = 0; d < D; d++) items.emplace_back(B->P.u[d], np);
+        break;
+      case MPMGPU_P_U:
+        for (int d = 0; d < D; d++) items.emplace_back(B->P.u[d], np);
+        break;
+      case MPMGPU_P_X_T:
+        for (int d = 0; d < D; d++) items.emplace_back(B->P.v[d], np);
+        break;
+      case MPMGPU_P_MX_T:
+        for (int d = 0; d < D; d++) items.emplace_back(B->P.v[d], np);
+        items.emplace_back(B->P.m, np);
+        break;
+      case MPMGPU_P_L: items.emplace_back(B->P.L, nz * 9 * sizeof(double)); break;
+      case MPMGPU_P_T:
+        for (int c = 0; c < 6; c++) items.emplace_back(B->P.s[c], np);
+        break;
+      case MPMGPU_P_M: items.emplace_back(B->P.m, np); break;
+      case MPMGPU_P_V: items.emplace_back(B->P.vol, np); break;
+      case MPMGPU_P_EXTENT: items.emplace_back(B->P.ext, np); break;
+      case MPMGPU_P_ACTIVE: items.emplace_back(B->P.active, nz * sizeof(int32_t)); break;
+      default: return fail(MPMGPU_ERR_ARG, "unknown point field");
+    }
+    std::vector<const unsigned char*> h;
+    MPM_TRY(fetch(items, h));
+    const int32_t* pid = reinterpret_cast<const int32_t*>(h[0]);
+    auto arr = [&](size_t k) { return reinterpret_cast<const PT*>(h[k]); };
+    auto vec3 = [&](size_t first) {
       for (int64_t i = 0; i < 3 * n; i++) out[i] = 0.0;
       for (int d = 0; d < D; d++) {
-        MPM_TRY(download(tmp, arr[d], (size_t)n));
-        for (int64_t i = 0; i < n; i++) out[3 * (int64_t)pid[(size_t)i] + d] = (double)tmp[(size_t)i];
+        const PT* a = arr(first + (size_t)d);
+        for (size_t i = 0; i < nz; i++) out[3 * (int64_t)pid[i] + d] = (double)a[i];
       }
-      return MPMGPU_OK;
-    };
-    auto scal = [&](const PT* arr) -> mpmgpu_status {
-      MPM_TRY(download(tmp, arr, (size_t)n));
-      for (int64_t i = 0; i < n; i++) out[pid[(size_t)i]] = (double)tmp[(size_t)i];
-      return MPMGPU_OK;
     };
     switch (field) {
       case MPMGPU_P_X:
         if constexpr (sizeof(PT) == 4) {
           // the mixed form keeps x0 in the x arrays: x = x0 + u (in FP32)
-          std::vector<PT> u;
           for (int64_t i = 0; i < 3 * n; i++) out[i] = 0.0;
           for (int d = 0; d < D; d++) {
-            MPM_TRY(download(tmp, B->P.x[d], (size_t)n));
-            MPM_TRY(download(u, B->P.u[d], (size_t)n));
-            for (int64_t i = 0; i < n; i++) out[3 * (int64_t)pid[(size_t)i] + d] = (double)(tmp[(size_t)i] + u[(size_t)i]);
+            const PT* x0 = arr(1 + (size_t)d);
+            const PT* u = arr(1 + (size_t)(D + d));
+            for (size_t i = 0; i < nz; i++) out[3 * (int64_t)pid[i] + d] = (double)(x0[i] + u[i]);
           }
-          return MPMGPU_OK;
+        } else {
+          vec3(1);
         }
-        return vec3(B->P.x);
-      case MPMGPU_P_U: return vec3(B->P.u);
-      case MPMGPU_P_X_T: return vec3(B->P.v);
+        return MPMGPU_OK;
+      case MPMGPU_P_U:
+      case MPMGPU_P_X_T: vec3(1); return MPMGPU_OK;
       case MPMGPU_P_MX_T: {
-        MPM_TRY(vec3(B->P.v));
-        std::vector<PT> m;
-        MPM_TRY(download(m, B->P.m, (size_t)n));
+        vec3(1);
+        const PT* m = arr(1 + (size_t)D);
         // movePoints: mx_t = m * x_t (explicit_usl.cpp:295-297)
-        for (int64_t i = 0; i < n; i++) {
-          const int64_t q = pid[(size_t)i];
-          for (int d = 0; d < D; d++) out[3 * q + d] = (double)m[(size_t)i] * out[3 * q + d];
+        for (size_t i = 0; i < nz; i++) {
+          const int64_t q = pid[i];
+          for (int d = 0; d < D; d++) out[3 * q + d] = (double)m[i] * out[3 * q + d];
         }
         return MPMGPU_OK;
       }
-      case MPMGPU_P_B:
-        for (int64_t i = 0; i < n; i++)
-          for (int d = 0; d < 3; d++) out[3 * i + d] = j->sp.grav[d];
-        return MPMGPU_OK;
       case MPMGPU_P_L: {
-        if (!B->P.L) return fail(MPMGPU_ERR_STATE, "L is kept only with keep_debug in the FP64 form");
-        std::vector<double> L;
-        MPM_TRY(download(L, B->P.L, (size_t)n * 9));
-        for (int64_t i = 0; i < n; i++)
-          for (int k = 0; k < 9; k++) out[9 * (int64_t)pid[(size_t)i] + k] = L[(size_t)(9 * i + k)];
+        const double* L = reinterpret_cast<const double*>(h[1]);
+        for (size_t i = 0; i < nz; i++)
+          for (int k = 0; k < 9; k++) out[9 * (int64_t)pid[i] + k] = L[9 * i + (size_t)k];
         return MPMGPU_OK;
       }
       case MPMGPU_P_T: {
         static const int idx[9] = {0, 3, 5, 3, 1, 4, 5, 4, 2};
-        std::vector<std::vector<PT>> s(6);
-        for (int c = 0; c < 6; c++) MPM_TRY(download(s[(size_t)c], B->P.s[c], (size_t)n));
-        for (int64_t i = 0; i < n; i++)
-          for (int k = 0; k < 9; k++) out[9 * (int64_t)pid[(size_t)i] + k] = (double)s[(size_t)idx[k]][(size_t)i];
+        for (size_t i = 0; i < nz; i++)
+          for (int k = 0; k < 9; k++) out[9 * (int64_t)pid[i] + k] = (double)arr(1 + (size_t)idx[k])[i];
         return MPMGPU_OK;
       }
-      case MPMGPU_P_M: return scal(B->P.m);
-      case MPMGPU_P_V: return scal(B->P.vol);
-      case MPMGPU_P_EXTENT: return scal(B->P.ext);
+      case MPMGPU_P_M:
+      case MPMGPU_P_V:
+      case MPMGPU_P_EXTENT: {
+        const PT* a = arr(1);
+        for (size_t i = 0; i < nz; i++) out[pid[i]] = (double)a[i];
+        return MPMGPU_OK;
+      }
       case MPMGPU_P_ACTIVE: {
-        std::vector<int32_t> a;
-        MPM_TRY(download(a, B->P.active, (size_t)n));
+        const int32_t* a = reinterpret_cast<const int32_t*>(h[1]);
         // 2 = left the domain at the last move: still active until the next
         // map build deactivates it, as in the reference
-        for (int64_t i = 0; i < n; i++) out[pid[(size_t)i]] = a[(size_t)i] != 0 ? 1.0 : 0.0;
+        for (size_t i = 0; i < nz; i++) out[pid[i]] = a[i] != 0 ? 1.0 : 0.0;
         return MPMGPU_OK;
       }
     }
@@ -1018,6 +1045,39 @@ class Batch : public BatchBase {
     MPM_CUDA_TRY(cudaEventRecord(upload_ev_, copy_stream_));
     MPM_CUDA_TRY(cudaStreamWaitEvent(stream_, upload_ev_, 0));
     MPM_CUDA_TRY(cudaStreamSynchronize(copy_stream_));
+    return MPMGPU_OK;
+  }
+
+  // Copies device arrays to pinned staging on the compute stream (after the
+  // queued work) and waits once; checks the kernels' error flag like
+  // synchronize(). h[k] points at item k's bytes until the next fetch.
+  mpmgpu_status fetch(const std::vector<std::pair<const void*, size_t>>& items, std::vector<const unsigned char*>& h) {
+    size_t total = 256;   // error flag first
+    for (auto& it : items) total += (it.second + 255) / 256 * 256;
+    if (total > dl_cap_) {
+      MPM_CUDA_TRY(cudaStreamSynchronize(stream_));
+      if (dl_stage_) cudaFreeHost(dl_stage_);
+      dl_stage_ = nullptr;
+      dl_cap_ = 0;
+      const size_t cap = std::max<size_t>(total, (size_t)16 << 20);
+      MPM_CUDA_TRY(cudaHostAlloc(&dl_stage_, cap, cudaHostAllocDefault));
+      dl_cap_ = cap;
+    }
+    unsigned char* base = static_cast<unsigned char*>(dl_stage_);
+    MPM_CUDA_TRY(cudaMemcpyAsync(base, err_, sizeof(int), cudaMemcpyDeviceToHost, stream_));
+    size_t off = 256;
+    h.clear();
+    for (auto& it : items) {
+      if (it.second > 0) MPM_CUDA_TRY(cudaMemcpyAsync(base + off, it.first, it.second, cudaMemcpyDeviceToHost, stream_));
+      h.push_back(base + off);
+      off += (it.second + 255) / 256 * 256;
+    }
+    MPM_CUDA_TRY(cudaStreamSynchronize(stream_));
+    int flag = 0;
+    std::memcpy(&flag, base, sizeof(int));
+    if (flag & kErrWideSpan) return fail(MPMGPU_ERR_DEVICE, "point corners span more than two cells (extent > cell size)");
+    if (flag & kErrElemAlias) return fail(MPMGPU_ERR_DEVICE, "point within rounding of the upper domain face");
+    if (flag & kErrWaitTimeout) return fail(MPMGPU_ERR_DEVICE, "a bulk copy did not complete within the wait limit");
     return MPMGPU_OK;
   }
 
@@ -1735,6 +1795,8 @@ class Batch : public BatchBase {
   int64_t cap_points_r_ = 0;
   int32_t* cell_count_ = nullptr;
   int64_t cap_cells_ = 0;
+  void* dl_stage_ = nullptr;   // pinned staging of downloads
+  size_t dl_cap_ = 0;
   unsigned long long* cell_hist_ = nullptr;   // per cell: 8 class counts of 8 bits
   int64_t cap_cells_h_ = 0;
   int16_t* crank_ = nullptr;                  // per point: class << 8 | rank in class
