@@ -1453,12 +1453,12 @@ class Batch : public BatchBase {
                                 (DET ? 1 : 0)];
     if (per_sm == 0) {
       MPM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      MPM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, fused_threads<CAP>(), smem));
+      MPM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, fused_threads<PT, CAP>(), smem));
       if (per_sm < 1) return fail(MPMGPU_ERR_CUDA, "fused kernel does not fit on an SM");
     }
     const int blocks = per_sm * sm_count_;
     StageTimer timer(this, kStageFused);
-    kern<<<blocks, fused_threads<CAP>(), smem, stream_>>>(fl);
+    kern<<<blocks, fused_threads<PT, CAP>(), smem, stream_>>>(fl);
     return check_launch("k_g2p2g");
   }
 

@@ -163,16 +163,17 @@ __host__ __device__ constexpr size_t fused_smem_bytes() {
 }
 
 // Threads per CTA and the resident CTAs per SM the register budget is sized
-// for (128 registers per thread either way): items of 256 points run on
-// 128-thread CTAs, four per SM, so that a barrier waits on fewer warps;
-// larger items on 256-thread CTAs, two per SM.
-template <int CAP>
+// for (128 registers per thread either way): the mixed form runs 256-point
+// items on 128-thread CTAs, four per SM, so that a barrier waits on fewer
+// warps; larger items, and every FP64 item, run on 256-thread CTAs, two per
+// SM (one point per thread for 256-point items: measured faster in FP64).
+template <typename PT, int CAP>
 __host__ __device__ constexpr int fused_threads() {
-  return CAP <= 256 ? 128 : 256;
+  return sizeof(PT) == 4 && CAP <= 256 ? 128 : 256;
 }
-template <int CAP>
+template <typename PT, int CAP>
 __host__ __device__ constexpr int fused_min_ctas() {
-  return CAP <= 256 ? 4 : 2;
+  return sizeof(PT) == 4 && CAP <= 256 ? 4 : 2;
 }
 
 // Entry k (0..2) of a 3-array without indexing it by a variable (which
@@ -814,7 +815,7 @@ __device__ __forceinline__ void flush_tile(const BodyCtx<PT>& c, const Geom& g, 
 }
 
 template <int DIM, typename PT, int CAP, bool NORMAL, bool SINGLE, bool DET>
-__global__ void __launch_bounds__(fused_threads<CAP>(), fused_min_ctas<CAP>())
+__global__ void __launch_bounds__(fused_threads<PT, CAP>(), fused_min_ctas<PT, CAP>())
     k_g2p2g(const __grid_constant__ FusedLaunch<PT> fl) {
   static_assert(!DET || sizeof(PT) == 8, "the deterministic form is FP64");
   __shared__ Split2 ksplit[4];   // deterministic form: per-field split of the item's body
@@ -952,7 +953,7 @@ __global__ void __launch_bounds__(fused_threads<CAP>(), fused_min_ctas<CAP>())
         // mixed form: every thread issues the loads of up to two nodes
         // before its first shared-memory store (one or two memory latencies
         // per item) and stores the values in FP32, relative to vref
-        constexpr int NT = fused_threads<CAP>();
+        constexpr int NT = fused_threads<PT, CAP>();
         constexpr int ITER = (TN + NT - 1) / NT;
         constexpr int CH = ITER > 2 ? 2 : ITER;   // nodes per thread in flight (registers)
 #pragma unroll 1
