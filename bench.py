@@ -585,20 +585,28 @@ def run_e2e_batch(cases, steps: int, device: int, cap: int, sort_interval: int):
 
     torch.cuda.synchronize()
     t0 = time.perf_counter()
+    phases = {}
     b = GPUBatch(dim=3, mode="mixed", device=device, points_per_item=cap, sort_interval=sort_interval)
     jobs = [b.add(c) for c in cases]
+    t1 = time.perf_counter()
+    phases["create_upload_s"] = t1 - t0
     b.step(steps)
     b.synchronize()
+    t2 = time.perf_counter()
+    phases["steps_s"] = t2 - t1
     d2h = 0
     for j in jobs:
         for f in ("x", "x_t", "T"):
             d2h += b.points(j, 0, f).nbytes
+    t3 = time.perf_counter()
+    phases["download_s"] = t3 - t2
     b.close()
     dt = time.perf_counter() - t0
+    phases["teardown_s"] = dt - (t3 - t0)
     psteps = sum(c.n_points * min(c.steps, steps) for c in cases)
     h2d = sum(b_.n * (8 + 8 + 24 + 24 + 4) for c in cases for b_ in c.bodies)
     return {"value": psteps / dt, "unit": UNIT, "h2d_bytes_per_step": h2d // steps, "d2h_bytes_per_step": d2h // steps,
-            "steps": steps, "seconds": dt}
+            "steps": steps, "seconds": dt, "phases": {k: round(v, 3) for k, v in phases.items()}}
 
 
 def cpu_ensemble_sample(cases, steps: int, warmup: int = 1):
