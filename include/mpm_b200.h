@@ -76,8 +76,9 @@ typedef struct {
 
 /* One DefaultBody: its points (DefaultPoints::readFromFile columns,
  * default_points.cpp:150-174), IsotropicLinearElasticity E and nu
- * (isolin.cpp:26-46) and whether a CartesianBox boundary is attached
- * (cartesian_box.cpp:23-60). */
+ * (isolin.cpp:26-46) and its boundary: CartesianBox (cartesian_box.cpp),
+ * CartesianSmoothBox (cartesian_smooth_box.cpp) or CartesianFrictionalBox
+ * (cartesian_frictional_box.cpp, friction mu_f from its fp64 property). */
 typedef struct {
   int64_t n;            /* number of points */
   const double* m;      /* n masses */
@@ -87,10 +88,12 @@ typedef struct {
   const int32_t* active;/* n flags (nonzero = active); NULL = all active */
   int has_material;     /* 0: no Material (stress never updated) */
   double E, nu;
-  int has_boundary;     /* 0: no Boundary */
+  int has_boundary;     /* 0: no Boundary, 1: CartesianBox, 2: CartesianSmoothBox,
+                           3: CartesianFrictionalBox */
   const double* u;      /* 3n initial displacements (AoS) or NULL (zero) */
   const double* T;      /* 9n initial Cauchy stresses (row-major, symmetric)
                            or NULL (zero) */
+  double boundary_mu;   /* CartesianFrictionalBox mu_f (boundary-props[0]) */
 } mpmgpu_body_desc;
 
 typedef struct mpmgpu_handle mpmgpu_handle;

@@ -205,7 +205,8 @@ class Batch : public BatchBase {
     NodesAcc Ar{};   // deterministic form: level-1 sums
     NodesVel V{};
     MaterialParams mat{};
-    int has_boundary = 0;
+    int has_boundary = 0;   // boundary kind (mpmgpu_body_desc.has_boundary)
+    double mu_f = 0.0;
     int needs_normal = 0;
     int prime = 1;
     std::vector<void*> allocs;
@@ -341,6 +342,7 @@ class Batch : public BatchBase {
     if ((int)j->bodies.size() >= kMaxBodies) return fail(MPMGPU_ERR_UNSUPPORTED, "too many bodies in a job");
     if (desc.n < 0 || desc.n > (int64_t)INT32_MAX / 2 || (desc.n > 0 && (!desc.m || !desc.v || !desc.x || !desc.x_t)))
       return fail(MPMGPU_ERR_ARG, "body arrays missing or too many points");
+    if (desc.has_boundary < 0 || desc.has_boundary > 3) return fail(MPMGPU_ERR_ARG, "unknown boundary kind");
     const int D = dim_;
     const int64_t n = desc.n;
     HBody B;
@@ -420,6 +422,7 @@ class Batch : public BatchBase {
     }
     B.mat = make_material(desc.has_material, desc.E, desc.nu);
     B.has_boundary = desc.has_boundary;
+    B.mu_f = desc.boundary_mu;
     MPM_TRY(finish_uploads());
     j->bodies.push_back(std::move(B));
     if (body) *body = (int)j->bodies.size() - 1;
@@ -1262,6 +1265,7 @@ class Batch : public BatchBase {
         G.V = b.V;
         G.snap = b.snap;
         G.has_boundary = b.has_boundary;
+        G.mu_f = b.mu_f;
         gbodies.push_back(G);
         BodyCtx<PT> c{};
         c.g = j.g;

@@ -126,6 +126,13 @@ __global__ void __launch_bounds__(64) k_grid(const InstDev* insts, const GridBod
       for (int d = 0; d < DIM; d++)
         if (sp.grav[d] != 0.0) A.f[d][s] = A.f[d][s] + m * sp.grav[d];
     }
+    // CartesianFrictionalBox reads the nodal force before contact
+    // (bcNodalForce: S (m b) - gradS (V T), cartesian_frictional_box.cpp:86-108)
+    double fpre[kMaxBodies][3];
+    for (int b = 0; b < I.nb; b++)
+      if (GB[b].has_boundary == 3)
+#pragma unroll
+        for (int d = 0; d < DIM; d++) fpre[b][d] = GB[b].A.f[d][s];
     for (int c = 0; c < I.nc; c++) {
       const NodesAcc& A1 = GB[I.cb1[c]].A;
       const NodesAcc& A2 = GB[I.cb2[c]].A;
@@ -215,11 +222,65 @@ __global__ void __launch_bounds__(64) k_grid(const InstDev* insts, const GridBod
         mx[d] = A.mx[d][s];
         f[d] = A.f[d][s];
       }
-      if (GB[b].has_boundary && on_face) {
+      const int kind = GB[b].has_boundary;
+      if (kind == 1 && on_face) {
+        // CartesianBox (cartesian_box.cpp:73-85): every component of a node
+        // on any wall
 #pragma unroll
         for (int d = 0; d < DIM; d++) {
           mx[d] = 0.0;
           f[d] = 0.0;
+        }
+      } else if (kind == 2 && on_face) {
+        // CartesianSmoothBox (cartesian_smooth_box.cpp:69-83): the
+        // wall-normal components only
+#pragma unroll
+        for (int d = 0; d < DIM; d++) {
+          const int c = d == 0 ? i : (d == 1 ? j : k);
+          if (c == 0 || c == g.N[d]) {
+            mx[d] = 0.0;
+            f[d] = 0.0;
+          }
+        }
+      } else if (kind == 3 && on_face) {
+        // CartesianFrictionalBox (cartesian_frictional_box.cpp:94-143): the
+        // closing momentum of each wall component gives the normal force,
+        // the component is zeroed, and friction of at most mu_f times the
+        // normal force opposes the remaining motion (interior nodes: no
+        // normal force, no change)
+        double dmom[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+        for (int d = 0; d < DIM; d++) {
+          const int c = d == 0 ? i : (d == 1 ? j : k);
+          const double closing = mx[d] + dt * fpre[b][d];
+          if (c == 0) {
+            dmom[d] = -((closing < 0.0) ? closing : 0.0);   // -std::min(0.0, .)
+            mx[d] = 0.0;
+            f[d] = 0.0;
+          } else if (c == g.N[d]) {
+            dmom[d] = -((0.0 < closing) ? closing : 0.0);   // -std::max(0.0, .)
+            mx[d] = 0.0;
+            f[d] = 0.0;
+          }
+        }
+        double nn = 0.0;
+#pragma unroll
+        for (int d = 0; d < DIM; d++) nn += dmom[d] * dmom[d];
+        const double f_normal = sqrt(nn) / dt;
+        double mm = 0.0;
+#pragma unroll
+        for (int d = 0; d < DIM; d++) {
+          dmom[d] = mx[d] + dt * f[d];
+          mm += dmom[d] * dmom[d];
+        }
+        const double nrm = sqrt(mm);
+        if (nrm > 0) {
+          const double a = nrm / dt, bnd = f_normal * GB[b].mu_f;
+          const double cf = (bnd < a) ? bnd : a;   // std::min(|dm| / dt, f_normal mu_f)
+          // vector / scalar multiplies by the reciprocal (mpm_vector.hpp:609-615)
+          const double inv = 1.0 / nrm;
+#pragma unroll
+          for (int d = 0; d < DIM; d++) f[d] = f[d] - (cf * dmom[d]) * inv;
         }
       }
       double inv = 0.0;

@@ -82,7 +82,8 @@ struct GridBody {
   NodesAcc Ar;       // deterministic form: level-1 (remainder) sums, else null
   NodesVel V;
   NodesAcc snap;     // debug copies of m, mx_t, f after the update (or null)
-  int has_boundary;
+  int has_boundary;  // 0 none, 1 CartesianBox, 2 CartesianSmoothBox, 3 CartesianFrictionalBox
+  double mu_f;       // CartesianFrictionalBox friction
 };
 
 // Sizes of the batch's index spaces, read by the kernels on the device so

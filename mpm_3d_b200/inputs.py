@@ -2,7 +2,8 @@
 
 A ``Case`` holds everything one ExplicitUSL run needs: the CartesianLinear grid,
 the bodies (points with mass, volume, position, velocity, active flag, an
-IsotropicLinearElasticity material and an optional CartesianBox boundary),
+IsotropicLinearElasticity material and an optional CartesianBox, CartesianSmoothBox
+or CartesianFrictionalBox boundary),
 ContactHuang pairs, the gravity mode and the time step. ``write_case`` writes it
 as a mpm_3d ``.cfg`` plus one ``.points`` file per body, the formats the
 reference reads (``src/config/config.cpp:176-528``,
@@ -33,7 +34,7 @@ from __future__ import annotations
 import dataclasses
 import math
 import os
-from typing import List, Optional, Sequence, Tuple
+from typing import List, Optional, Sequence, Tuple, Union
 
 import numpy as np
 
@@ -67,11 +68,35 @@ class Body:
     E: float = 1e5
     nu: float = 0.3
     material: bool = True
-    boundary: bool = True
+    # True or "CartesianBox", "CartesianSmoothBox", "CartesianFrictionalBox";
+    # False: no boundary
+    boundary: Union[bool, str] = True
+    boundary_mu: float = 0.0   # CartesianFrictionalBox friction (boundary-props {mu_f})
 
     @property
     def n(self) -> int:
         return int(self.m.shape[0])
+
+
+BOUNDARY_CLASSES = ("CartesianBox", "CartesianSmoothBox", "CartesianFrictionalBox")
+
+
+def boundary_class(body: "Body") -> Optional[str]:
+    """The boundary class name of a body, or None."""
+    if body.boundary is True:
+        return "CartesianBox"
+    if not body.boundary:
+        return None
+    if body.boundary not in BOUNDARY_CLASSES:
+        raise ValueError(f"unknown boundary class {body.boundary!r}")
+    return str(body.boundary)
+
+
+def boundary_kind(body: "Body") -> int:
+    """The C ABI's boundary code: 0 none, 1 CartesianBox, 2 CartesianSmoothBox,
+    3 CartesianFrictionalBox."""
+    cls = boundary_class(body)
+    return 0 if cls is None else 1 + BOUNDARY_CLASSES.index(cls)
 
 
 @dataclasses.dataclass
@@ -148,6 +173,25 @@ def block_drop_2d() -> Case:
     h = (0.05, 0.05)
     body = block_points((0.35, 0.45), (12, 12), h, 1000.0, (0.0, -1.0), name="block", E=1e5, nu=0.3)
     return Case(name="block_drop_2d", dim=2, L=(1.0, 1.0), N=(20, 20), dt=1e-4, steps=2000, bodies=[body])
+
+
+def sliding_block(dim: int = 2, boundary: str = "CartesianFrictionalBox", mu: float = 0.3, n_cells: int = 16,
+                  steps: int = 200) -> Case:
+    """A block resting on the floor (and against the x = 0 wall) of an n^dim
+    grid on a 1 m box, thrown along x and pressed into the floor, with the
+    given boundary class (and its friction mu for CartesianFrictionalBox):
+    the walls' nodes carry mass, so the boundary rules act from the first
+    step."""
+    h = tuple([1.0 / n_cells] * dim)
+    counts = tuple([2 * (n_cells // 4)] * dim)
+    lo = tuple([0.0] * dim)
+    vel = (2.0, -1.0) if dim == 2 else (2.0, 0.5, -1.0)
+    body = block_points(lo, counts, h, 1000.0, vel, name="block", E=1e5, nu=0.3)
+    body.boundary = boundary
+    body.boundary_mu = mu
+    name = f"sliding_block_{dim}d_{boundary}"
+    return Case(name=name, dim=dim, L=tuple([1.0] * dim), N=tuple([n_cells] * dim), dt=1e-4, steps=steps,
+                bodies=[body])
 
 
 def two_body_collision_3d(n_cells: int = 128, steps: int = 1000, gravity=None, gap: Optional[float] = None,
@@ -338,8 +382,11 @@ def write_case(case: Case, directory: str, solver_class: str = "ExplicitUSL", po
         if body.material:
             lines += ['    material-class = "IsotropicLinearElasticity"',
                       f"    material-props = {{{_fmt(body.E)},{_fmt(body.nu)}}}"]
-        if body.boundary:
-            lines += ['    boundary-class = "CartesianBox"']
+        cls = boundary_class(body)
+        if cls is not None:
+            lines += [f'    boundary-class = "{cls}"']
+            if cls == "CartesianFrictionalBox":
+                lines += [f"    boundary-props = {{{_fmt(body.boundary_mu)}}}"]
         lines += ["}", ""]
     for c in case.contacts:
         lines += ["contact", "{", '    name = "contact"', '    class = "ContactHuang"', f"    properties = {{{_fmt(c.mu)}}}",

@@ -111,9 +111,17 @@ void GPUExplicitUSL::setUp(Job* job) {
       desc.nu = mat->nu;
     }
     if (body->activeBoundary) {
-      if (!dynamic_cast<CartesianBox*>(body->boundary.get()))
-        unsupported("boundary class " + body->boundary->object_name);
-      desc.has_boundary = 1;
+      Boundary* bc = body->boundary.get();
+      if (dynamic_cast<CartesianBox*>(bc)) {
+        desc.has_boundary = 1;
+      } else if (dynamic_cast<CartesianSmoothBox*>(bc)) {
+        desc.has_boundary = 2;
+      } else if (CartesianFrictionalBox* fb = dynamic_cast<CartesianFrictionalBox*>(bc)) {
+        desc.has_boundary = 3;
+        desc.boundary_mu = fb->mu_f;   // set by CartesianFrictionalBox::init from boundary-props
+      } else {
+        unsupported("boundary class " + bc->object_name);
+      }
     }
     int id = -1;
     check(mpmgpu_add_body(handle, &desc, &id), "mpmgpu_add_body");

@@ -36,8 +36,11 @@ typedef struct {
   int *active;
   /* nodes: 3 per node unless noted */
   double *nx, *nu, *nx_t, *nmx_t, *nf, *ndiff, *nm /* 1 per node */;
-  double *bc_mask;       /* CartesianBox bcNodalMask, 3 per node */
-  int has_material, has_boundary;
+  double *bc_mask;       /* the boundary's bcNodalMask, 3 per node */
+  double *bc_force;      /* CartesianFrictionalBox bcNodalForce, 3 per node */
+  double mu_f;           /* CartesianFrictionalBox friction */
+  int has_material;
+  int has_boundary;      /* 0 none, 1 CartesianBox, 2 CartesianSmoothBox, 3 CartesianFrictionalBox */
   double E, nu_, G, K, lambda;
   /* COO triplets of the last map build */
   int nnz, gnnz, cap;
@@ -404,33 +407,108 @@ static void contact_apply(oc_job* J, oc_contact* C) {
   }
 }
 
-/* CartesianBox::init mask, cartesian_box.cpp:29-55 */
+/* Boundary masks: CartesianBox::init (cartesian_box.cpp:29-55) locks every
+ * component of a node on any wall; CartesianSmoothBox::init
+ * (cartesian_smooth_box.cpp:23-59) locks the wall-normal components;
+ * CartesianFrictionalBox::init (cartesian_frictional_box.cpp:21-84) marks
+ * lower (-1) and upper (1) walls per component and 2 for the other
+ * components of a node on a wall. */
 static void boundary_init(oc_job* J, oc_body* B) {
   double Lmax[3] = {0, 0, 0};
   for (int i = 0; i < J->node_count; i++)
     for (int pos = 0; pos < J->dim; pos++)
       if (B->nx[3 * (size_t)i + pos] > Lmax[pos]) Lmax[pos] = B->nx[3 * (size_t)i + pos];
   for (int i = 0; i < J->node_count; i++) {
-    for (int d = 0; d < 3; d++) B->bc_mask[3 * (size_t)i + d] = 0;
-    for (int pos = 0; pos < J->dim; pos++) {
-      double xv = B->nx[3 * (size_t)i + pos];
-      if (xv == 0 || xv == Lmax[pos]) {
-        for (int d = 0; d < J->dim; d++) B->bc_mask[3 * (size_t)i + d] = 1;
-        break;
+    double* mk = B->bc_mask + 3 * (size_t)i;
+    const double* xn = B->nx + 3 * (size_t)i;
+    for (int d = 0; d < 3; d++) mk[d] = 0;
+    if (B->has_boundary == 1) {
+      for (int pos = 0; pos < J->dim; pos++) {
+        if (xn[pos] == 0 || xn[pos] == Lmax[pos]) {
+          for (int d = 0; d < J->dim; d++) mk[d] = 1;
+          break;
+        }
       }
+    } else if (B->has_boundary == 2) {
+      for (int pos = 0; pos < J->dim; pos++)
+        if (xn[pos] == 0 || xn[pos] == Lmax[pos]) mk[pos] = 1;
+    } else if (B->has_boundary == 3) {
+      int is_edge = 0;
+      for (int pos = 0; pos < J->dim; pos++) {
+        if (xn[pos] == 0) {
+          mk[pos] = -1;
+          is_edge = 1;
+        } else if (xn[pos] == Lmax[pos]) {
+          mk[pos] = 1;
+          is_edge = 1;
+        }
+      }
+      for (int pos = 0; pos < J->dim; pos++)
+        if (is_edge && mk[pos] != 1 && mk[pos] != -1) mk[pos] = 2;
     }
   }
 }
 
-/* CartesianBox::applyRules, cartesian_box.cpp:73-85 */
+/* std::min / std::max as the reference calls them */
+static double std_min(double a, double b) { return (b < a) ? b : a; }
+static double std_max(double a, double b) { return (a < b) ? b : a; }
+
+static double vec_norm(const double* v, int dim) {
+  double s = 0.0;
+  for (int d = 0; d < dim; d++) s += v[d] * v[d];
+  return sqrt(s);
+}
+
+/* CartesianBox::applyRules (cartesian_box.cpp:73-85) and
+ * CartesianSmoothBox::applyRules (cartesian_smooth_box.cpp:69-83): locked
+ * components of x_t, mx_t and f are zeroed. CartesianFrictionalBox::applyRules
+ * (cartesian_frictional_box.cpp:94-143): the closing momentum of a wall
+ * component (from the body force and stress divergence, bcNodalForce) gives
+ * a normal force, the component is zeroed, and a friction force of at most
+ * mu_f times the normal force opposes the remaining motion. */
 static void boundary_apply(oc_job* J, oc_body* B) {
-  for (int i = 0; i < J->node_count; i++)
-    for (int pos = 0; pos < J->dim; pos++)
-      if (B->bc_mask[3 * (size_t)i + pos] == 1) {
-        B->nx_t[3 * (size_t)i + pos] = 0;
-        B->nmx_t[3 * (size_t)i + pos] = 0;
-        B->nf[3 * (size_t)i + pos] = 0;
+  const int dim = J->dim;
+  const double dt = J->dt;
+  for (int i = 0; i < J->node_count; i++) {
+    const double* mk = B->bc_mask + 3 * (size_t)i;
+    double* xt = B->nx_t + 3 * (size_t)i;
+    double* mx = B->nmx_t + 3 * (size_t)i;
+    double* f = B->nf + 3 * (size_t)i;
+    if (B->has_boundary != 3) {
+      for (int pos = 0; pos < dim; pos++)
+        if (mk[pos] == 1) {
+          xt[pos] = 0;
+          mx[pos] = 0;
+          f[pos] = 0;
+        }
+      continue;
+    }
+    const double* bf = B->bc_force + 3 * (size_t)i;
+    double dmom[3] = {0, 0, 0};
+    for (int pos = 0; pos < dim; pos++) {
+      if (mk[pos] == -1) {
+        dmom[pos] = -std_min(0.0, mx[pos] + dt * bf[pos]);
+        xt[pos] = 0;
+        mx[pos] = 0;
+        f[pos] = 0;
+      } else if (mk[pos] == 1) {
+        dmom[pos] = -std_max(0.0, mx[pos] + dt * bf[pos]);
+        xt[pos] = 0;
+        mx[pos] = 0;
+        f[pos] = 0;
+      } else {
+        dmom[pos] = 0;
       }
+    }
+    const double f_normal = vec_norm(dmom, dim) / dt;
+    for (int pos = 0; pos < dim; pos++) dmom[pos] = mx[pos] + dt * f[pos];
+    if (vec_norm(dmom, dim) > 0) {
+      const double c = std_min(vec_norm(dmom, dim) / dt, f_normal * B->mu_f);
+      /* vector / scalar multiplies by the reciprocal (mpm_vector.hpp:609-615) */
+      const double inv = 1.0 / vec_norm(dmom, dim);
+      for (int pos = 0; pos < dim; pos++) f[pos] -= (c * dmom[pos]) * inv;
+    }
+  }
 }
 
 /* moveGrid, explicit_usl.cpp:233-264 */
@@ -581,12 +659,14 @@ void* oc_create(int dim, const double* L, const int* N, double dt, int cpdi_spec
 }
 
 /* Adds a body: n points with m, v (volume), x and x_t (3 per point, AoS),
- * active flags. Material E, nu (has_material), CartesianBox (has_boundary).
+ * active flags. Material E, nu (has_material); boundary kind (has_boundary: 0 none,
+ * 1 CartesianBox, 2 CartesianSmoothBox, 3 CartesianFrictionalBox with mu_f =
+ * boundary_mu).
  * Mirrors DefaultBody::init (default_body.cpp:24-40), DefaultPoints::init
  * (default_points.cpp:35-57), DefaultNodes::init (default_nodes.cpp:29-63),
  * IsotropicLinearElasticity::init (isolin.cpp:34-38). */
 int oc_add_body(void* hp, int n, const double* m, const double* v, const double* x, const double* x_t,
-                const int* active, int has_material, double E, double nu, int has_boundary) {
+                const int* active, int has_material, double E, double nu, int has_boundary, double boundary_mu) {
   oc_job* J = (oc_job*)hp;
   if (J->nbodies >= OC_MAX_BODIES) return -1;
   oc_body* B = &J->bodies[J->nbodies];
@@ -613,6 +693,7 @@ int oc_add_body(void* hp, int n, const double* m, const double* v, const double*
   B->ndiff = (double*)calloc(3 * N, sizeof(double));
   B->nm = (double*)calloc(N, sizeof(double));
   B->bc_mask = (double*)calloc(3 * N, sizeof(double));
+  B->bc_force = (double*)calloc(3 * N, sizeof(double));
   for (int p = 0; p < n; p++) {
     B->m[p] = m[p];
     B->v[p] = v[p];
@@ -627,6 +708,7 @@ int oc_add_body(void* hp, int n, const double* m, const double* v, const double*
   for (size_t i = 0; i < N; i++) node_position(J, (int)i, B->nx + 3 * i);
   B->has_material = has_material;
   B->has_boundary = has_boundary;
+  B->mu_f = boundary_mu;
   B->E = E;
   B->nu_ = nu;
   B->G = E / (2.0 * (1.0 + nu));
@@ -666,6 +748,12 @@ int oc_step(void* hp, int nsteps) {
     for (int b = 0; b < J->nbodies; b++)
       if (generate_map(J, &J->bodies[b]) != 0) return -1;
     for (int b = 0; b < J->nbodies; b++) map_points_to_nodes(J, &J->bodies[b]);
+    /* CartesianFrictionalBox::generateRules/applyRules recompute
+     * S (m b) - gradS (V T) with the operations of mapPointsToNodes
+     * (cartesian_frictional_box.cpp:86-108): the nodal force before contact */
+    for (int b = 0; b < J->nbodies; b++)
+      if (J->bodies[b].has_boundary == 3)
+        memcpy(J->bodies[b].bc_force, J->bodies[b].nf, 3 * (size_t)J->node_count * sizeof(double));
     for (int c = 0; c < J->ncontacts; c++) contact_generate(J, &J->contacts[c]);
     for (int c = 0; c < J->ncontacts; c++) contact_apply(J, &J->contacts[c]);
     for (int b = 0; b < J->nbodies; b++)
@@ -762,7 +850,7 @@ void oc_destroy(void* hp) {
     free(B->x); free(B->u); free(B->x_t); free(B->mx_t); free(B->b);
     free(B->L); free(B->T); free(B->m); free(B->v); free(B->v0);
     free(B->extent); free(B->active); free(B->nx); free(B->nu); free(B->nx_t);
-    free(B->nmx_t); free(B->nf); free(B->ndiff); free(B->nm); free(B->bc_mask);
+    free(B->nmx_t); free(B->nf); free(B->ndiff); free(B->nm); free(B->bc_mask); free(B->bc_force);
     free(B->S_i); free(B->S_j); free(B->S_v); free(B->G_i); free(B->G_j); free(B->G_v);
   }
   for (int c = 0; c < J->ncontacts; c++) {

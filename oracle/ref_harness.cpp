@@ -182,6 +182,8 @@ Registry<Material>::Registry() {
 template <>
 Registry<Boundary>::Registry() {
   object["CartesianBox"] = &make<Boundary, CartesianBox>;
+  object["CartesianSmoothBox"] = &make<Boundary, CartesianSmoothBox>;
+  object["CartesianFrictionalBox"] = &make<Boundary, CartesianFrictionalBox>;
 }
 
 namespace {

@@ -82,6 +82,12 @@ def _dense_cells_3d():
 
 CASES = {
     "dense_cells_3d": (_dense_cells_3d, 10),
+    "sliding_2d_smooth_box": (lambda: inputs.sliding_block(2, "CartesianSmoothBox", n_cells=16, steps=60), 60),
+    "sliding_2d_frictional_box": (lambda: inputs.sliding_block(2, "CartesianFrictionalBox", mu=0.3, n_cells=16,
+                                                               steps=60), 60),
+    "sliding_3d_smooth_box": (lambda: inputs.sliding_block(3, "CartesianSmoothBox", n_cells=12, steps=30), 30),
+    "sliding_3d_frictional_box": (lambda: inputs.sliding_block(3, "CartesianFrictionalBox", mu=0.3, n_cells=12,
+                                                               steps=30), 30),
     "wall_exit_2d": (_wall_exit_2d, 25),
     "block_drop_2d": (inputs.block_drop_2d, 120),
     "spinning_block_2d": (_spinning_block_2d, 120),

@@ -98,3 +98,22 @@ def test_restated_matches_reference_wall_exit():
         for f in POINT_FIELDS:
             assert bits_equal(job.points(0, f), ref.points(0, f)), f"step {s} point {f}"
     assert ref.points(0, "active").sum() < case.bodies[0].n
+
+
+@needs_ref
+@pytest.mark.parametrize("dim,boundary", [(2, "CartesianSmoothBox"), (2, "CartesianFrictionalBox"),
+                                          (3, "CartesianSmoothBox"), (3, "CartesianFrictionalBox")])
+def test_restated_matches_reference_boundaries(dim, boundary):
+    """A block sliding along the floor with the smooth (slip) and the
+    frictional box: restatement == reference every step."""
+    case = inputs.sliding_block(dim, boundary, mu=0.3, n_cells=8 if dim == 3 else 16, steps=15)
+    d = tempfile.mkdtemp()
+    ref = bridge.ReferenceJob(inputs.write_case(case, d))
+    job = bridge.RestatedJob(case)
+    for s in range(case.steps):
+        ref.step(1)
+        job.step(1)
+        for f in POINT_FIELDS:
+            assert bits_equal(job.points(0, f), ref.points(0, f)), f"{boundary} step {s} point {f}"
+        for f in NODE_FIELDS:
+            assert bits_equal(job.nodes(0, f), ref.nodes(0, f)), f"{boundary} step {s} node {f}"

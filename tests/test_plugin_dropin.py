@@ -34,6 +34,9 @@ CASES = {
     "block_drop_2d": (inputs.block_drop_2d, 30),
     "collision_2d": (lambda: inputs.two_body_collision_2d(20, steps=20), 20),
     "collision_3d_touching": (lambda: inputs.two_body_collision_3d(16, steps=8, gap=0.01), 8),
+    "sliding_2d_frictional_box": (lambda: inputs.sliding_block(2, "CartesianFrictionalBox", mu=0.3, n_cells=16,
+                                                               steps=20), 20),
+    "sliding_3d_smooth_box": (lambda: inputs.sliding_block(3, "CartesianSmoothBox", n_cells=12, steps=10), 10),
 }
 
 
