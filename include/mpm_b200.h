@@ -146,6 +146,12 @@ mpmgpu_status mpmgpu_add_body(mpmgpu_handle* h, const mpmgpu_body_desc* desc, in
 /* Replaces ContactHuang::init (contact_huang.cpp:24-75). */
 mpmgpu_status mpmgpu_add_contact(mpmgpu_handle* h, int body1, int body2, double mu_f, int* contact_id);
 
+/* Replaces ContactHuang_ReflectedBoundary::init
+ * (contact_huang_reflected_boundary.cpp:25-84): ContactHuang whose normal
+ * loses its components normal to the walls of the box at nodes where body1
+ * has mass (generateRules, 90-114). */
+mpmgpu_status mpmgpu_add_contact_reflected(mpmgpu_handle* h, int body1, int body2, double mu_f, int* contact_id);
+
 /* Gravity as the driver applies it (Driver::generateGravity/applyGravity):
  * use_vector 0 = DefaultDriver (-9.81 along y in 2D, z in 3D,
  * default_driver.cpp:90-105), 1 = UserDefinedGravityDriver vector g. May be
@@ -256,10 +262,12 @@ typedef struct {
   int keep_debug;      /* as mpmgpu_config.keep_debug */
 } mpmgpu_batch_config;
 
-/* One ContactHuang pair of a job (bodies are indices within the job). */
+/* One ContactHuang pair of a job (bodies are indices within the job);
+ * reflected = 1 for ContactHuang_ReflectedBoundary. */
 typedef struct {
   int body1, body2;
   double mu;
+  int reflected;
 } mpmgpu_contact_desc;
 
 /* One job: grid / dt / cpdi_spec / contact_spec from `grid` (its mode,

@@ -154,6 +154,12 @@ mpmgpu_status mpmgpu_add_contact(mpmgpu_handle* h, int body1, int body2, double 
   return h->b->add_contact(h->job, body1, body2, mu_f, contact_id);
 }
 
+mpmgpu_status mpmgpu_add_contact_reflected(mpmgpu_handle* h, int body1, int body2, double mu_f, int* contact_id) {
+  if (!h) return MPMGPU_ERR_ARG;
+  if (h->started) return hfail(h, MPMGPU_ERR_STATE, "contacts must be added before the first step");
+  return h->b->add_contact(h->job, body1, body2, mu_f, contact_id, 1);
+}
+
 mpmgpu_status mpmgpu_set_gravity(mpmgpu_handle* h, int use_vector, const double g[3]) {
   if (!h) return MPMGPU_ERR_ARG;
   return h->b->set_gravity(h->job, use_vector, g);
@@ -317,7 +323,8 @@ mpmgpu_status mpmgpu_batch_add_job(mpmgpu_batch* b, const mpmgpu_job_desc* job, 
   mpmgpu_status st = MPMGPU_OK;
   for (int i = 0; i < job->nbodies && st == MPMGPU_OK; i++) st = b->b->add_body(id, job->bodies[i], nullptr);
   for (int c = 0; c < job->ncontacts && st == MPMGPU_OK; c++)
-    st = b->b->add_contact(id, job->contacts[c].body1, job->contacts[c].body2, job->contacts[c].mu, nullptr);
+    st = b->b->add_contact(id, job->contacts[c].body1, job->contacts[c].body2, job->contacts[c].mu, nullptr,
+                           job->contacts[c].reflected);
   if (st == MPMGPU_OK) st = b->b->set_gravity(id, job->gravity_vector, job->gravity);
   if (st == MPMGPU_OK) st = b->b->admit(id);
   if (st != MPMGPU_OK) {

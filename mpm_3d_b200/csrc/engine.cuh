@@ -161,7 +161,7 @@ class BatchBase {
   virtual int64_t launches() const = 0;
   virtual mpmgpu_status new_job(const mpmgpu_config& cfg, int64_t steps, int* job) = 0;
   virtual mpmgpu_status add_body(int job, const mpmgpu_body_desc& desc, int* body) = 0;
-  virtual mpmgpu_status add_contact(int job, int b1, int b2, double mu, int* contact) = 0;
+  virtual mpmgpu_status add_contact(int job, int b1, int b2, double mu, int* contact, int reflected = 0) = 0;
   virtual mpmgpu_status set_gravity(int job, int use_vector, const double* g) = 0;
   virtual mpmgpu_status admit(int job) = 0;
   virtual mpmgpu_status step(int nsteps) = 0;
@@ -221,6 +221,7 @@ class Batch : public BatchBase {
     int nc = 0;
     int cb1[kMaxContacts] = {}, cb2[kMaxContacts] = {};
     double mu[kMaxContacts] = {};
+    int reflected[kMaxContacts] = {};
     double* normal_out[kMaxContacts] = {};
     double* force_out[kMaxContacts] = {};
     std::vector<void*> allocs;
@@ -429,7 +430,7 @@ class Batch : public BatchBase {
     return MPMGPU_OK;
   }
 
-  mpmgpu_status add_contact(int job, int b1, int b2, double mu, int* contact) override {
+  mpmgpu_status add_contact(int job, int b1, int b2, double mu, int* contact, int reflected = 0) override {
     HJob* j;
     MPM_TRY(editable_job(job, &j));
     const int nb = (int)j->bodies.size();
@@ -447,6 +448,7 @@ class Batch : public BatchBase {
     j->cb1[c] = b1;
     j->cb2[c] = b2;
     j->mu[c] = mu;
+    j->reflected[c] = reflected != 0 ? 1 : 0;
     if (keep_debug_) {
       MPM_TRY(alloc_dev(&j->normal_out[c], 3 * ns, j->allocs, j->bytes));
       MPM_TRY(alloc_dev(&j->force_out[c], 3 * ns, j->allocs, j->bytes));
@@ -1253,6 +1255,7 @@ class Batch : public BatchBase {
         I.cb1[c] = j.cb1[c];
         I.cb2[c] = j.cb2[c];
         I.mu[c] = j.mu[c];
+        I.reflected[c] = j.reflected[c];
         I.normal_out[c] = j.normal_out[c];
         I.force_out[c] = j.force_out[c];
       }

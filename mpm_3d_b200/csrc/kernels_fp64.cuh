@@ -143,11 +143,27 @@ __global__ void __launch_bounds__(64) k_grid(const InstDev* insts, const GridBod
         n[d] = A1.nrm[d][s];
         nn += n[d] * n[d];
       }
-      const double inv_norm = 1.0 / sqrt(nn);
-#pragma unroll
-      for (int d = 0; d < DIM; d++) n[d] *= inv_norm;
-      double fc[3] = {0.0, 0.0, 0.0};
       const double m1 = A1.m[s], m2 = A2.m[s];
+      if (!I.reflected[c]) {
+        const double inv_norm = 1.0 / sqrt(nn);
+#pragma unroll
+        for (int d = 0; d < DIM; d++) n[d] *= inv_norm;
+      } else if (m1 > 0) {
+        // ContactHuang_ReflectedBoundary (contact_huang_reflected_boundary.cpp:
+        // 90-114): the components normal to a wall of the box are dropped
+        // before the normalisation, at nodes where body 1 has mass
+        nn = 0.0;
+#pragma unroll
+        for (int d = 0; d < DIM; d++) {
+          const int cd = d == 0 ? i : (d == 1 ? j : k);
+          if (cd == 0 || cd == g.N[d]) n[d] = 0.0;
+          nn += n[d] * n[d];
+        }
+        const double inv_norm = 1.0 / sqrt(nn);
+#pragma unroll
+        for (int d = 0; d < DIM; d++) n[d] *= inv_norm;
+      }
+      double fc[3] = {0.0, 0.0, 0.0};
       if (m1 > 0 && m2 > 0) {
         double mv1[3], mv2[3], vcm[3];
         double f1[3], f2[3];

@@ -94,7 +94,8 @@ class Server {
     mpmgpu_status st = batch_->new_job(cfg, d.steps, &job);
     for (int b = 0; b < d.nbodies && st == MPMGPU_OK; b++) st = batch_->add_body(job, d.bodies[b], nullptr);
     for (int c = 0; c < d.ncontacts && st == MPMGPU_OK; c++)
-      st = batch_->add_contact(job, d.contacts[c].body1, d.contacts[c].body2, d.contacts[c].mu, nullptr);
+      st = batch_->add_contact(job, d.contacts[c].body1, d.contacts[c].body2, d.contacts[c].mu, nullptr,
+                               d.contacts[c].reflected);
     if (st == MPMGPU_OK) st = batch_->set_gravity(job, d.gravity_vector, d.gravity);
     if (st == MPMGPU_OK) st = batch_->admit(job);
     if (st != MPMGPU_OK) {

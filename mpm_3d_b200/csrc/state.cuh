@@ -71,6 +71,7 @@ struct InstDev {
   int cb1[kMaxContacts];
   int cb2[kMaxContacts];
   double mu[kMaxContacts];
+  int reflected[kMaxContacts];       // ContactHuang_ReflectedBoundary normals
   double* normal_out[kMaxContacts];  // 3 * nslots or null (debug)
   double* force_out[kMaxContacts];   // 3 * nslots or null (debug)
   int64_t block_off;                 // first node block of the job in the batch's block space

@@ -101,11 +101,13 @@ def boundary_kind(body: "Body") -> int:
 
 @dataclasses.dataclass
 class Contact:
-    """ContactHuang between bodies b1 and b2 with friction mu."""
+    """ContactHuang between bodies b1 and b2 with friction mu; reflected:
+    ContactHuang_ReflectedBoundary (the normal's wall components dropped)."""
 
     b1: int
     b2: int
     mu: float
+    reflected: bool = False
 
 
 @dataclasses.dataclass
@@ -192,6 +194,28 @@ def sliding_block(dim: int = 2, boundary: str = "CartesianFrictionalBox", mu: fl
     name = f"sliding_block_{dim}d_{boundary}"
     return Case(name=name, dim=dim, L=tuple([1.0] * dim), N=tuple([n_cells] * dim), dt=1e-4, steps=steps,
                 bodies=[body])
+
+
+def wall_collision(dim: int = 2, n_cells: int = 16, steps: int = 100, mu: float = 0.4,
+                   reflected: bool = True) -> Case:
+    """Two blocks resting on the floor of an n^dim grid on a 1 m box with
+    slip walls (CartesianSmoothBox), thrown at each other along x, with
+    ContactHuang (reflected: the ContactHuang_ReflectedBoundary variant)
+    between them: the contact nodes include floor nodes, where the reflected
+    variant drops the normal's floor component."""
+    h = tuple([1.0 / n_cells] * dim)
+    side = n_cells // 4
+    counts = tuple([2 * side] * dim)
+    lo1 = tuple([0.25] + [0.0] * (dim - 1))
+    lo2 = tuple([0.25 + side * h[0]] + [0.0] * (dim - 1))
+    v1 = tuple([1.0] + [0.0] * (dim - 1))
+    v2 = tuple([-1.0] + [0.0] * (dim - 1))
+    b1 = block_points(lo1, counts, h, 1000.0, v1, name="left", E=1e5, nu=0.3)
+    b2 = block_points(lo2, counts, h, 1000.0, v2, name="right", E=1e5, nu=0.3)
+    b1.boundary = b2.boundary = "CartesianSmoothBox"
+    name = f"wall_collision_{dim}d" + ("_reflected" if reflected else "")
+    return Case(name=name, dim=dim, L=tuple([1.0] * dim), N=tuple([n_cells] * dim), dt=1e-4, steps=steps,
+                bodies=[b1, b2], contacts=[Contact(0, 1, mu, reflected)])
 
 
 def two_body_collision_3d(n_cells: int = 128, steps: int = 1000, gravity=None, gap: Optional[float] = None,
@@ -389,7 +413,8 @@ def write_case(case: Case, directory: str, solver_class: str = "ExplicitUSL", po
                 lines += [f"    boundary-props = {{{_fmt(body.boundary_mu)}}}"]
         lines += ["}", ""]
     for c in case.contacts:
-        lines += ["contact", "{", '    name = "contact"', '    class = "ContactHuang"', f"    properties = {{{_fmt(c.mu)}}}",
+        cclass = "ContactHuang_ReflectedBoundary" if c.reflected else "ContactHuang"
+        lines += ["contact", "{", '    name = "contact"', f'    class = "{cclass}"', f"    properties = {{{_fmt(c.mu)}}}",
                   f'    str-properties = {{"{case.bodies[c.b1].name}","{case.bodies[c.b2].name}"}}', "}", ""]
     path = os.path.join(directory, f"{case.name}.cfg")
     with open(path, "w") as f:

@@ -42,7 +42,7 @@ class _BatchConfig(ctypes.Structure):
 
 
 class _ContactDesc(ctypes.Structure):
-    _fields_ = [("body1", ctypes.c_int), ("body2", ctypes.c_int), ("mu", ctypes.c_double)]
+    _fields_ = [("body1", ctypes.c_int), ("body2", ctypes.c_int), ("mu", ctypes.c_double), ("reflected", ctypes.c_int)]
 
 
 class _BodyDesc(ctypes.Structure):
@@ -78,6 +78,8 @@ def load() -> ctypes.CDLL:
     lib.mpmgpu_create.argtypes = [ctypes.POINTER(_Config), ctypes.POINTER(vp)]
     lib.mpmgpu_add_body.argtypes = [vp, ctypes.POINTER(_BodyDesc), ctypes.POINTER(ctypes.c_int)]
     lib.mpmgpu_add_contact.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.POINTER(ctypes.c_int)]
+    lib.mpmgpu_add_contact_reflected.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                                 ctypes.POINTER(ctypes.c_int)]
     lib.mpmgpu_set_gravity.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
     lib.mpmgpu_step.argtypes = [vp, ctypes.c_int]
     lib.mpmgpu_synchronize.argtypes = [vp]
@@ -180,7 +182,8 @@ class GPUExplicitUSL:
             self._check(self.lib.mpmgpu_add_body(self.h, ctypes.byref(desc), ctypes.byref(bid)))
         for c in case.contacts:
             cid = ctypes.c_int()
-            self._check(self.lib.mpmgpu_add_contact(self.h, c.b1, c.b2, c.mu, ctypes.byref(cid)))
+            add = self.lib.mpmgpu_add_contact_reflected if c.reflected else self.lib.mpmgpu_add_contact
+            self._check(add(self.h, c.b1, c.b2, c.mu, ctypes.byref(cid)))
         if case.gravity is not None:
             g = (ctypes.c_double * 3)(*(list(case.gravity) + [0.0] * (3 - len(case.gravity))))
             self._check(self.lib.mpmgpu_set_gravity(self.h, 1, g))
@@ -311,7 +314,7 @@ def job_desc(case: inputs.Case, steps: Optional[int] = None):
                               body.nu, inputs.boundary_kind(body), None, None, float(body.boundary_mu))
     contacts = (_ContactDesc * max(1, len(case.contacts)))()
     for i, c in enumerate(case.contacts):
-        contacts[i] = _ContactDesc(c.b1, c.b2, c.mu)
+        contacts[i] = _ContactDesc(c.b1, c.b2, c.mu, int(c.reflected))
     desc = _JobDesc()
     desc.grid = ctypes.pointer(cfg)
     desc.nbodies = len(case.bodies)

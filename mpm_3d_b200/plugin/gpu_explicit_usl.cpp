@@ -133,7 +133,11 @@ void GPUExplicitUSL::setUp(Job* job) {
     if (!ch) unsupported("contact class " + job->contacts[c]->object_name);
     const int b1 = gpu_body[ch->bodyIDs[0]], b2 = gpu_body[ch->bodyIDs[1]];
     if (b1 < 0 || b2 < 0) unsupported("contact between inactive bodies");
-    check(mpmgpu_add_contact(handle, b1, b2, ch->mu_f, nullptr), "mpmgpu_add_contact");
+    // ContactHuang_ReflectedBoundary derives from ContactHuang and differs in its normal
+    if (dynamic_cast<ContactHuang_ReflectedBoundary*>(ch))
+      check(mpmgpu_add_contact_reflected(handle, b1, b2, ch->mu_f, nullptr), "mpmgpu_add_contact_reflected");
+    else
+      check(mpmgpu_add_contact(handle, b1, b2, ch->mu_f, nullptr), "mpmgpu_add_contact");
   }
   // the driver has applied gravity to every point before the loop
   // (default_driver.cpp:58-60): take it from the points

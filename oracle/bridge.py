@@ -146,7 +146,7 @@ class RestatedJob(_JobBase):
         L.oc_create.argtypes = [ctypes.c_int, _dp, _ip, ctypes.c_double, ctypes.c_int, ctypes.c_int]
         L.oc_add_body.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp, _dp, _dp, _ip, ctypes.c_int,
                                   ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_double]
-        L.oc_add_contact.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_double]
+        L.oc_add_contact.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int]
         L.oc_set_gravity.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp]
         for fn in ("oc_step", "oc_num_nodes", "oc_get_point_field", "oc_get_node_field", "oc_get_contact_field",
                    "oc_map_size", "oc_grad_map_size", "oc_get_map", "oc_get_grad_map", "oc_build_map", "oc_destroy"):
@@ -168,7 +168,7 @@ class RestatedJob(_JobBase):
                           _ptr(arrs[4], _ip), int(body.material), body.E, body.nu, boundary_kind(body),
                           float(body.boundary_mu))
         for c in case.contacts:
-            L.oc_add_contact(self.h, c.b1, c.b2, c.mu)
+            L.oc_add_contact(self.h, c.b1, c.b2, c.mu, int(getattr(c, "reflected", False)))
         if case.gravity is not None:
             g = np.array(list(case.gravity) + [0.0] * (3 - len(case.gravity)), dtype=np.float64)
             L.oc_set_gravity(self.h, 1, _ptr(g))

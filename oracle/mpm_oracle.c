@@ -53,6 +53,7 @@ typedef struct {
 typedef struct {
   int b1, b2;
   double mu_f;
+  int reflected;          /* 1: ContactHuang_ReflectedBoundary */
   double *normal, *force; /* 3 per node */
 } oc_contact;
 
@@ -339,8 +340,31 @@ static void contact_generate(oc_job* J, oc_contact* C) {
     int i = B->G_i[k], j = B->G_j[k];
     for (int d = 0; d < J->dim; d++) C->normal[3 * (size_t)i + d] += B->G_v[3 * (size_t)k + d] * B->m[j];
   }
+  if (!C->reflected) {
+    for (int i = 0; i < N; i++) {
+      double* n = C->normal + 3 * (size_t)i;
+      double s = 0;
+      for (int d = 0; d < J->dim; d++) s += n[d] * n[d];
+      double inv = 1.0 / sqrt(s);
+      for (int d = 0; d < J->dim; d++) n[d] *= inv;
+    }
+    return;
+  }
+  /* ContactHuang_ReflectedBoundary::generateRules
+   * (contact_huang_reflected_boundary.cpp:90-114): at nodes where body 1 has
+   * mass, the components normal to a wall of the box (Lx from init, 66-74)
+   * are zeroed before the normalisation; other nodes keep the raw sum. */
+  double Lmax[3] = {0, 0, 0};
+  for (int i = 0; i < N; i++)
+    for (int pos = 0; pos < J->dim; pos++)
+      if (B->nx[3 * (size_t)i + pos] > Lmax[pos]) Lmax[pos] = B->nx[3 * (size_t)i + pos];
   for (int i = 0; i < N; i++) {
+    if (!(B->nm[i] > 0)) continue;
     double* n = C->normal + 3 * (size_t)i;
+    for (int pos = 0; pos < J->dim; pos++) {
+      double xv = B->nx[3 * (size_t)i + pos];
+      if (xv == 0 || xv == Lmax[pos]) n[pos] = 0;
+    }
     double s = 0;
     for (int d = 0; d < J->dim; d++) s += n[d] * n[d];
     double inv = 1.0 / sqrt(s);
@@ -720,13 +744,14 @@ int oc_add_body(void* hp, int n, const double* m, const double* v, const double*
   return J->nbodies - 1;
 }
 
-int oc_add_contact(void* hp, int b1, int b2, double mu_f) {
+int oc_add_contact(void* hp, int b1, int b2, double mu_f, int reflected) {
   oc_job* J = (oc_job*)hp;
   if (J->ncontacts >= OC_MAX_CONTACTS) return -1;
   oc_contact* C = &J->contacts[J->ncontacts];
   C->b1 = b1;
   C->b2 = b2;
   C->mu_f = mu_f;
+  C->reflected = reflected;
   C->normal = (double*)calloc(3 * (size_t)J->node_count, sizeof(double));
   C->force = (double*)calloc(3 * (size_t)J->node_count, sizeof(double));
   J->ncontacts++;

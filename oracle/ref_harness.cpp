@@ -174,6 +174,7 @@ Registry<Nodes>::Registry() {
 template <>
 Registry<Contact>::Registry() {
   object["ContactHuang"] = &make<Contact, ContactHuang>;
+  object["ContactHuang_ReflectedBoundary"] = &make<Contact, ContactHuang_ReflectedBoundary>;
 }
 template <>
 Registry<Material>::Registry() {

@@ -86,6 +86,8 @@ CASES = {
     "sliding_2d_frictional_box": (lambda: inputs.sliding_block(2, "CartesianFrictionalBox", mu=0.3, n_cells=16,
                                                                steps=60), 60),
     "sliding_3d_smooth_box": (lambda: inputs.sliding_block(3, "CartesianSmoothBox", n_cells=12, steps=30), 30),
+    "wall_collision_2d_reflected": (lambda: inputs.wall_collision(2, n_cells=16, steps=40), 40),
+    "wall_collision_3d_reflected": (lambda: inputs.wall_collision(3, n_cells=12, steps=20), 20),
     "sliding_3d_frictional_box": (lambda: inputs.sliding_block(3, "CartesianFrictionalBox", mu=0.3, n_cells=12,
                                                                steps=30), 30),
     "wall_exit_2d": (_wall_exit_2d, 25),

@@ -117,3 +117,21 @@ def test_restated_matches_reference_boundaries(dim, boundary):
             assert bits_equal(job.points(0, f), ref.points(0, f)), f"{boundary} step {s} point {f}"
         for f in NODE_FIELDS:
             assert bits_equal(job.nodes(0, f), ref.nodes(0, f)), f"{boundary} step {s} node {f}"
+
+
+@needs_ref
+@pytest.mark.parametrize("dim", [2, 3])
+def test_restated_matches_reference_reflected_contact(dim):
+    """Two blocks colliding on the floor with ContactHuang_ReflectedBoundary:
+    restatement == reference every step (points and contact forces)."""
+    case = inputs.wall_collision(dim, n_cells=16 if dim == 2 else 8, steps=15)
+    d = tempfile.mkdtemp()
+    ref = bridge.ReferenceJob(inputs.write_case(case, d))
+    job = bridge.RestatedJob(case)
+    for s in range(case.steps):
+        ref.step(1)
+        job.step(1)
+        for b in range(2):
+            for f in POINT_FIELDS:
+                assert bits_equal(job.points(b, f), ref.points(b, f)), f"step {s} body {b} point {f}"
+        assert bits_equal(job.contact(0, "force"), ref.contact(0, "force")), f"step {s} contact force"

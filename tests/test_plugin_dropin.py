@@ -37,6 +37,7 @@ CASES = {
     "sliding_2d_frictional_box": (lambda: inputs.sliding_block(2, "CartesianFrictionalBox", mu=0.3, n_cells=16,
                                                                steps=20), 20),
     "sliding_3d_smooth_box": (lambda: inputs.sliding_block(3, "CartesianSmoothBox", n_cells=12, steps=10), 10),
+    "wall_collision_2d_reflected": (lambda: inputs.wall_collision(2, n_cells=16, steps=20), 20),
 }
 
 
