@@ -94,6 +94,10 @@ typedef struct {
   const double* T;      /* 9n initial Cauchy stresses (row-major, symmetric)
                            or NULL (zero) */
   double boundary_mu;   /* CartesianFrictionalBox mu_f (boundary-props[0]) */
+  int material_kind;    /* 0: IsotropicLinearElasticity (isolin.cpp),
+                           1: CompressibleNeohookeanElasticity
+                           (compressible_neohookean_elasticity.cpp: F from
+                           the identity, neo-Hookean stress) */
 } mpmgpu_body_desc;
 
 typedef struct mpmgpu_handle mpmgpu_handle;

@@ -100,9 +100,10 @@ inline void make_geometry(const mpmgpu_config& cfg, Geom& g, MapConst& mc, BinGe
 }
 
 // IsotropicLinearElasticity constants, isolin.cpp:34-38.
-inline MaterialParams make_material(int has_material, double E, double nu) {
+inline MaterialParams make_material(int has_material, double E, double nu, int kind = 0) {
   MaterialParams m{};
   m.has_material = has_material;
+  m.kind = has_material ? kind : 0;
   if (has_material) {
     const double G = E / (2.0 * (1.0 + nu));
     const double K = E / (3.0 * (1.0 - 2 * nu));
@@ -348,13 +349,16 @@ class Batch : public BatchBase {
     const int64_t n = desc.n;
     HBody B;
     B.n = n;
-    MPM_TRY(stage_reserve((size_t)n * (18 * sizeof(PT) + 8) + 64 * 256));
+    MPM_TRY(stage_reserve((size_t)n * (21 * sizeof(PT) + 8) + 64 * 256));
     const size_t ns = (size_t)j->g.nslots;
+    if (desc.has_material && (desc.material_kind < 0 || desc.material_kind > 1))
+      return fail(MPMGPU_ERR_ARG, "unknown material kind");
+    const bool neo = desc.has_material && desc.material_kind == 1;
     // both point buffers and the nodal arrays of the body
     MPM_TRY(alloc_arena(
         [&](Arena& a) {
-          layout_points(a, B.P, n);
-          layout_points(a, B.Palt, n);
+          layout_points(a, B.P, n, neo);
+          layout_points(a, B.Palt, n, neo);
           if (det_) {
             carve(a, &B.Ar.m, ns);
             for (int d = 0; d < 3; d++) {
@@ -420,8 +424,14 @@ class Batch : public BatchBase {
       }
       MPM_TRY(upload(B.P.active, act));
       MPM_TRY(upload(B.P.pid, pid));
+      if (neo) {
+        // CompressibleNeohookeanElasticity::init: F = I (the other
+        // components are the arena's zeros)
+        std::vector<PT> one((size_t)n, PT(1));
+        for (int k = 0; k < 9; k += 4) MPM_TRY(upload(B.P.F[k], one));
+      }
     }
-    B.mat = make_material(desc.has_material, desc.E, desc.nu);
+    B.mat = make_material(desc.has_material, desc.E, desc.nu, desc.material_kind);
     B.has_boundary = desc.has_boundary;
     B.mu_f = desc.boundary_mu;
     MPM_TRY(finish_uploads());
@@ -981,7 +991,7 @@ class Batch : public BatchBase {
   // Point arrays hold n entries plus 8 of padding: the fused kernel's bulk
   // copies round their windows out to 16-byte boundaries and may read up to
   // 3 entries past the last point.
-  void layout_points(Arena& a, PointsT<PT>& P, int64_t n) {
+  void layout_points(Arena& a, PointsT<PT>& P, int64_t n, bool with_F) {
     P = PointsT<PT>{};
     P.n = n;
     const size_t na = (size_t)n + 8;
@@ -998,6 +1008,8 @@ class Batch : public BatchBase {
     carve(a, &P.pid, na);
     P.L = nullptr;
     if (keep_debug_ && !mixed()) carve(a, &P.L, (size_t)n * 9);
+    if (with_F)
+      for (int k = 0; k < 9; k++) carve(a, &P.F[k], na);
   }
 
   // Returns a job's arrays to the pool after the work already queued on the
@@ -1693,6 +1705,8 @@ class Batch : public BatchBase {
         MPM_TRY(snap_one(b.P.active, ni));
         MPM_TRY(snap_one(b.P.pid, ni));
         if (b.P.L) MPM_TRY(snap_one(b.P.L, (size_t)b.n * 9 * sizeof(double)));
+        if (b.P.F[0])
+          for (int k = 0; k < 9; k++) MPM_TRY(snap_one(b.P.F[k], np));
         MPM_TRY(snap_one(b.A.m, ns));
         for (int d = 0; d < 3; d++) {
           MPM_TRY(snap_one(b.A.mx[d], ns));

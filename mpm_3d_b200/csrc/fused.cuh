@@ -474,7 +474,15 @@ __device__ __forceinline__ void gather_update(const BodyCtx<PT>& c, int* err, un
   const R vol = sp[kFvol * ROW] * exp(dt * (gs.L[0][0] + gs.L[1][1] + gs.L[2][2]));
   sp[kFvol * ROW] = vol;
   P.vol[p] = vol;
-  if (c.mat.has_material) {
+  if (c.mat.has_material && c.mat.kind == 1) {
+    R s6[6];
+    neohookean_update<R>(P.F, p, gs.L, s6, (R)c.mat.G, (R)c.mat.lambda, dt);
+#pragma unroll
+    for (int k = 0; k < 6; k++) {
+      sp[(kFs + k) * ROW] = s6[k];
+      P.s[k][p] = s6[k];
+    }
+  } else if (c.mat.has_material) {
     R s6[6];
 #pragma unroll
     for (int k = 0; k < 6; k++) s6[k] = sp[(kFs + k) * ROW];

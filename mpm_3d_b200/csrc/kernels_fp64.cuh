@@ -360,6 +360,51 @@ __device__ __forceinline__ void jaumann_update(const R L[3][3], R* s6, R G, R la
   }
 }
 
+// CompressibleNeohookeanElasticity::calculateStress
+// (compressible_neohookean_elasticity.cpp:44-62) for one point: the
+// deformation gradient (global memory, row-major components F[0..8]) advances
+// as F += (L F) dt; with B = F F^T and J = sqrt(det B) the stress is
+// T = G/J (B - I) + lambda ln(J)/J I (lambda = K - 2G/3), returned as the 6
+// stored components (B is symmetric).
+template <typename R, typename PT>
+__device__ __forceinline__ void neohookean_update(PT* const* Fp, int64_t p, const R L[3][3], R* s6, R G, R lambda,
+                                                  R dt) {
+  R F[3][3];
+#pragma unroll
+  for (int a = 0; a < 3; a++)
+#pragma unroll
+    for (int b = 0; b < 3; b++) F[a][b] = (R)Fp[3 * a + b][p];
+  R LF[3][3];
+#pragma unroll
+  for (int a = 0; a < 3; a++)
+#pragma unroll
+    for (int b = 0; b < 3; b++) LF[a][b] = L[a][0] * F[0][b] + L[a][1] * F[1][b] + L[a][2] * F[2][b];
+#pragma unroll
+  for (int a = 0; a < 3; a++)
+#pragma unroll
+    for (int b = 0; b < 3; b++) {
+      F[a][b] = F[a][b] + LF[a][b] * dt;
+      Fp[3 * a + b][p] = (PT)F[a][b];
+    }
+  R B[3][3];
+#pragma unroll
+  for (int a = 0; a < 3; a++)
+#pragma unroll
+    for (int b = 0; b < 3; b++) B[a][b] = F[a][0] * F[b][0] + F[a][1] * F[b][1] + F[a][2] * F[b][2];
+  const R det = B[0][0] * (B[1][1] * B[2][2] - B[2][1] * B[1][2]) - B[0][1] * (B[1][0] * B[2][2] - B[2][0] * B[1][2]) +
+                B[0][2] * (B[1][0] * B[2][1] - B[2][0] * B[1][1]);
+  const R J = sqrt(det);
+  const R s1 = G / J;
+  const R s2 = lambda * log(J) / J;
+  const int ia[6] = {0, 1, 2, 0, 1, 0};
+  const int ib[6] = {0, 1, 2, 1, 2, 2};
+#pragma unroll
+  for (int c = 0; c < 6; c++) {
+    const int a = ia[c], b = ib[c];
+    s6[c] = s1 * (B[a][b] - (a == b ? R(1) : R(0))) + (a == b ? s2 : R(0));
+  }
+}
+
 // Order-independent nodal sums of the deterministic form (pre-rounded
 // two-level summation after Demmel and Nguyen, "Fast reproducible
 // floating-point summation", ARITH 2013). With M bounding every partial sum

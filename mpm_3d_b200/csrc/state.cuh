@@ -26,6 +26,8 @@ struct PointsT {
                      // move (inactive from the next map build on)
   int32_t* pid;      // original index of the point
   double* L;         // 9 per point when debug output is kept (FP64 form), else null
+  PT* F[9];          // CompressibleNeohookeanElasticity deformation gradient
+                     // (row-major components), else null
 };
 using PointsDev = PointsT<double>;
 
@@ -55,8 +57,9 @@ struct StepParams {
 
 struct MaterialParams {
   int has_material;
+  int kind;          // 0 IsotropicLinearElasticity, 1 CompressibleNeohookeanElasticity
   double G;
-  double lambda;
+  double lambda;     // K - 2G/3
 };
 
 // One job (the reference's Job: one grid, its bodies and contacts). Bodies

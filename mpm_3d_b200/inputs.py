@@ -68,6 +68,7 @@ class Body:
     E: float = 1e5
     nu: float = 0.3
     material: bool = True
+    material_class: str = "IsotropicLinearElasticity"   # or "CompressibleNeohookeanElasticity"
     # True or "CartesianBox", "CartesianSmoothBox", "CartesianFrictionalBox";
     # False: no boundary
     boundary: Union[bool, str] = True
@@ -79,6 +80,15 @@ class Body:
 
 
 BOUNDARY_CLASSES = ("CartesianBox", "CartesianSmoothBox", "CartesianFrictionalBox")
+MATERIAL_CLASSES = ("IsotropicLinearElasticity", "CompressibleNeohookeanElasticity")
+
+
+def material_kind(body: "Body") -> int:
+    """The C ABI's material code: 0 IsotropicLinearElasticity, 1
+    CompressibleNeohookeanElasticity."""
+    if body.material_class not in MATERIAL_CLASSES:
+        raise ValueError(f"unknown material class {body.material_class!r}")
+    return MATERIAL_CLASSES.index(body.material_class)
 
 
 def boundary_class(body: "Body") -> Optional[str]:
@@ -404,7 +414,7 @@ def write_case(case: Case, directory: str, solver_class: str = "ExplicitUSL", po
         lines += ["body", "{", '    class = "DefaultBody"', f'    name = "{body.name}"', f'    point-file = "{pfile}"',
                   f'    point-class = "{points_class}"', '    node-class = "DefaultNodes"']
         if body.material:
-            lines += ['    material-class = "IsotropicLinearElasticity"',
+            lines += [f'    material-class = "{body.material_class}"',
                       f"    material-props = {{{_fmt(body.E)},{_fmt(body.nu)}}}"]
         cls = boundary_class(body)
         if cls is not None:

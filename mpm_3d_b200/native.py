@@ -49,7 +49,8 @@ class _BodyDesc(ctypes.Structure):
     _fields_ = [("n", ctypes.c_int64), ("m", ctypes.c_void_p), ("v", ctypes.c_void_p), ("x", ctypes.c_void_p),
                 ("x_t", ctypes.c_void_p), ("active", ctypes.c_void_p), ("has_material", ctypes.c_int),
                 ("E", ctypes.c_double), ("nu", ctypes.c_double), ("has_boundary", ctypes.c_int),
-                ("u", ctypes.c_void_p), ("T", ctypes.c_void_p), ("boundary_mu", ctypes.c_double)]
+                ("u", ctypes.c_void_p), ("T", ctypes.c_void_p), ("boundary_mu", ctypes.c_double),
+                ("material_kind", ctypes.c_int)]
 
 
 class _JobDesc(ctypes.Structure):
@@ -177,7 +178,8 @@ class GPUExplicitUSL:
                         active=np.ascontiguousarray(body.active, np.int32))
             desc = _BodyDesc(body.n, _ptr(arrs["m"]).value, _ptr(arrs["v"]).value, _ptr(arrs["x"]).value,
                              _ptr(arrs["x_t"]).value, _ptr(arrs["active"]).value, int(body.material), body.E, body.nu,
-                             inputs.boundary_kind(body), None, None, float(body.boundary_mu))
+                             inputs.boundary_kind(body), None, None, float(body.boundary_mu),
+                             inputs.material_kind(body))
             bid = ctypes.c_int()
             self._check(self.lib.mpmgpu_add_body(self.h, ctypes.byref(desc), ctypes.byref(bid)))
         for c in case.contacts:
@@ -311,7 +313,8 @@ def job_desc(case: inputs.Case, steps: Optional[int] = None):
         keep.append(arrs)
         bodies[i] = _BodyDesc(body.n, _ptr(arrs["m"]).value, _ptr(arrs["v"]).value, _ptr(arrs["x"]).value,
                               _ptr(arrs["x_t"]).value, _ptr(arrs["active"]).value, int(body.material), body.E,
-                              body.nu, inputs.boundary_kind(body), None, None, float(body.boundary_mu))
+                              body.nu, inputs.boundary_kind(body), None, None, float(body.boundary_mu),
+                             inputs.material_kind(body))
     contacts = (_ContactDesc * max(1, len(case.contacts)))()
     for i, c in enumerate(case.contacts):
         contacts[i] = _ContactDesc(c.b1, c.b2, c.mu, int(c.reflected))

@@ -107,6 +107,8 @@ void GPUExplicitUSL::setUp(Job* job) {
       IsotropicLinearElasticity* mat = dynamic_cast<IsotropicLinearElasticity*>(body->material.get());
       if (!mat) unsupported("material class " + body->material->object_name);
       desc.has_material = 1;
+      // CompressibleNeohookeanElasticity derives from IsotropicLinearElasticity
+      desc.material_kind = dynamic_cast<CompressibleNeohookeanElasticity*>(mat) ? 1 : 0;
       desc.E = mat->E;
       desc.nu = mat->nu;
     }

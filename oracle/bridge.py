@@ -145,7 +145,7 @@ class RestatedJob(_JobBase):
         L.oc_create.restype = ctypes.c_void_p
         L.oc_create.argtypes = [ctypes.c_int, _dp, _ip, ctypes.c_double, ctypes.c_int, ctypes.c_int]
         L.oc_add_body.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp, _dp, _dp, _ip, ctypes.c_int,
-                                  ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_double]
+                                  ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_int]
         L.oc_add_contact.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int]
         L.oc_set_gravity.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp]
         for fn in ("oc_step", "oc_num_nodes", "oc_get_point_field", "oc_get_node_field", "oc_get_contact_field",
@@ -159,14 +159,14 @@ class RestatedJob(_JobBase):
         self.h = ctypes.c_void_p(h)
         self.case = case
         self._keep = []
-        from mpm_3d_b200.inputs import boundary_kind
+        from mpm_3d_b200.inputs import boundary_kind, material_kind
         for body in case.bodies:
             arrs = [np.ascontiguousarray(body.m, np.float64), np.ascontiguousarray(body.v, np.float64),
                     np.ascontiguousarray(body.x, np.float64), np.ascontiguousarray(body.x_t, np.float64),
                     np.ascontiguousarray(body.active, np.int32)]
             L.oc_add_body(self.h, body.n, _ptr(arrs[0]), _ptr(arrs[1]), _ptr(arrs[2]), _ptr(arrs[3]),
                           _ptr(arrs[4], _ip), int(body.material), body.E, body.nu, boundary_kind(body),
-                          float(body.boundary_mu))
+                          float(body.boundary_mu), material_kind(body))
         for c in case.contacts:
             L.oc_add_contact(self.h, c.b1, c.b2, c.mu, int(getattr(c, "reflected", False)))
         if case.gravity is not None:

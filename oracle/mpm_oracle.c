@@ -40,6 +40,8 @@ typedef struct {
   double *bc_force;      /* CartesianFrictionalBox bcNodalForce, 3 per node */
   double mu_f;           /* CartesianFrictionalBox friction */
   int has_material;
+  int material_kind;     /* 0 IsotropicLinearElasticity, 1 CompressibleNeohookeanElasticity */
+  double *F;             /* neo-Hookean deformation gradient, 9 per point (row-major) */
   int has_boundary;      /* 0 none, 1 CartesianBox, 2 CartesianSmoothBox, 3 CartesianFrictionalBox */
   double E, nu_, G, K, lambda;
   /* COO triplets of the last map build */
@@ -624,7 +626,41 @@ static void apply_gravity(oc_job* J) {
 
 /* IsotropicLinearElasticity::calculateStress, isolin.cpp:50-78, with the
  * MaterialTensor operators of mpm_tensor.hpp:964-1070. */
+/* CompressibleNeohookeanElasticity::calculateStress
+ * (compressible_neohookean_elasticity.cpp:44-62): F += (L F) dt, B = F F^T,
+ * J = sqrt(det B), T = G/J (B - I) + (K - 2G/3) ln(J)/J I, with the 3x3
+ * product and determinant of mpm_tensor.hpp (579-584, 1060-1070). */
+static void update_stress_neohookean(oc_job* J, oc_body* B) {
+  const double dt = J->dt;
+  static const double I[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+  for (int p = 0; p < B->n; p++) {
+    if (B->active[p] == 0) continue;
+    const double* L = B->L + 9 * (size_t)p;
+    double* F = B->F + 9 * (size_t)p;
+    double* T = B->T + 9 * (size_t)p;
+    double LF[9], Bm[9];
+    for (int a = 0; a < 3; a++)
+      for (int c = 0; c < 3; c++)
+        LF[3 * a + c] = L[3 * a + 0] * F[0 + c] + L[3 * a + 1] * F[3 + c] + L[3 * a + 2] * F[6 + c];
+    for (int k = 0; k < 9; k++) F[k] = F[k] + LF[k] * dt;
+    for (int a = 0; a < 3; a++)
+      for (int c = 0; c < 3; c++)
+        Bm[3 * a + c] = F[3 * a + 0] * F[3 * c + 0] + F[3 * a + 1] * F[3 * c + 1] + F[3 * a + 2] * F[3 * c + 2];
+    const double da = Bm[0] * (Bm[4] * Bm[8] - Bm[7] * Bm[5]);
+    const double db = Bm[1] * (Bm[3] * Bm[8] - Bm[6] * Bm[5]);
+    const double dc = Bm[2] * (Bm[3] * Bm[7] - Bm[6] * Bm[4]);
+    const double Jv = sqrt(da - db + dc);
+    const double s1 = B->G / Jv;
+    const double s2 = (B->K - 2.0 * B->G / 3.0) * log(Jv) / Jv;
+    for (int k = 0; k < 9; k++) T[k] = s1 * (Bm[k] - I[k]) + s2 * I[k];
+  }
+}
+
 static void update_stress(oc_job* J, oc_body* B) {
+  if (B->material_kind == 1) {
+    update_stress_neohookean(J, B);
+    return;
+  }
   double dt = J->dt;
   for (int p = 0; p < B->n; p++) {
     if (B->active[p] == 0) continue;
@@ -690,7 +726,8 @@ void* oc_create(int dim, const double* L, const int* N, double dt, int cpdi_spec
  * (default_points.cpp:35-57), DefaultNodes::init (default_nodes.cpp:29-63),
  * IsotropicLinearElasticity::init (isolin.cpp:34-38). */
 int oc_add_body(void* hp, int n, const double* m, const double* v, const double* x, const double* x_t,
-                const int* active, int has_material, double E, double nu, int has_boundary, double boundary_mu) {
+                const int* active, int has_material, double E, double nu, int has_boundary, double boundary_mu,
+                int material_kind) {
   oc_job* J = (oc_job*)hp;
   if (J->nbodies >= OC_MAX_BODIES) return -1;
   oc_body* B = &J->bodies[J->nbodies];
@@ -703,6 +740,8 @@ int oc_add_body(void* hp, int n, const double* m, const double* v, const double*
   B->mx_t = (double*)calloc(3 * (size_t)n, sizeof(double));
   B->b = (double*)calloc(3 * (size_t)n, sizeof(double));
   B->L = (double*)calloc(9 * (size_t)n, sizeof(double));
+  B->F = (double*)calloc(9 * (size_t)n, sizeof(double));
+  for (int p = 0; p < n; p++) B->F[9 * (size_t)p] = B->F[9 * (size_t)p + 4] = B->F[9 * (size_t)p + 8] = 1.0;
   B->T = (double*)calloc(9 * (size_t)n, sizeof(double));
   B->m = (double*)calloc((size_t)n, sizeof(double));
   B->v = (double*)calloc((size_t)n, sizeof(double));
@@ -731,6 +770,7 @@ int oc_add_body(void* hp, int n, const double* m, const double* v, const double*
   }
   for (size_t i = 0; i < N; i++) node_position(J, (int)i, B->nx + 3 * i);
   B->has_material = has_material;
+  B->material_kind = material_kind;
   B->has_boundary = has_boundary;
   B->mu_f = boundary_mu;
   B->E = E;
@@ -873,7 +913,7 @@ void oc_destroy(void* hp) {
   for (int b = 0; b < J->nbodies; b++) {
     oc_body* B = &J->bodies[b];
     free(B->x); free(B->u); free(B->x_t); free(B->mx_t); free(B->b);
-    free(B->L); free(B->T); free(B->m); free(B->v); free(B->v0);
+    free(B->L); free(B->F); free(B->T); free(B->m); free(B->v); free(B->v0);
     free(B->extent); free(B->active); free(B->nx); free(B->nu); free(B->nx_t);
     free(B->nmx_t); free(B->nf); free(B->ndiff); free(B->nm); free(B->bc_mask); free(B->bc_force);
     free(B->S_i); free(B->S_j); free(B->S_v); free(B->G_i); free(B->G_j); free(B->G_v);

@@ -179,6 +179,7 @@ Registry<Contact>::Registry() {
 template <>
 Registry<Material>::Registry() {
   object["IsotropicLinearElasticity"] = &make<Material, IsotropicLinearElasticity>;
+  object["CompressibleNeohookeanElasticity"] = &make<Material, CompressibleNeohookeanElasticity>;
 }
 template <>
 Registry<Boundary>::Registry() {

@@ -80,8 +80,19 @@ def _dense_cells_3d():
                        bodies=[body])
 
 
+def _neohookean(case):
+    for body in case.bodies:
+        body.material_class = "CompressibleNeohookeanElasticity"
+    case.name += "_neohookean"
+    return case
+
+
 CASES = {
     "dense_cells_3d": (_dense_cells_3d, 10),
+    "spinning_block_2d_neohookean": (lambda: _neohookean(_spinning_block_2d()), 60),
+    "collision_3d_neohookean": (lambda: _neohookean(inputs.two_body_collision_3d(16, steps=15, gap=0.01)), 15),
+    "sliding_3d_neohookean": (lambda: _neohookean(inputs.sliding_block(3, "CartesianSmoothBox", n_cells=12,
+                                                                       steps=30)), 30),
     "sliding_2d_smooth_box": (lambda: inputs.sliding_block(2, "CartesianSmoothBox", n_cells=16, steps=60), 60),
     "sliding_2d_frictional_box": (lambda: inputs.sliding_block(2, "CartesianFrictionalBox", mu=0.3, n_cells=16,
                                                                steps=60), 60),

@@ -135,3 +135,29 @@ def test_restated_matches_reference_reflected_contact(dim):
             for f in POINT_FIELDS:
                 assert bits_equal(job.points(b, f), ref.points(b, f)), f"step {s} body {b} point {f}"
         assert bits_equal(job.contact(0, "force"), ref.contact(0, "force")), f"step {s} contact force"
+
+
+def _neohookean(case):
+    for body in case.bodies:
+        body.material_class = "CompressibleNeohookeanElasticity"
+    case.name += "_neohookean"
+    return case
+
+
+@needs_ref
+@pytest.mark.parametrize("make", [lambda: _neohookean(inputs.block_drop_2d()),
+                                  lambda: _neohookean(inputs.two_body_collision_3d(8, steps=12, gap=0.02))],
+                         ids=["block_drop_2d", "collision_3d"])
+def test_restated_matches_reference_neohookean(make):
+    """CompressibleNeohookeanElasticity (deformation gradient, neo-Hookean
+    stress): restatement == reference every step."""
+    case = make()
+    d = tempfile.mkdtemp()
+    ref = bridge.ReferenceJob(inputs.write_case(case, d))
+    job = bridge.RestatedJob(case)
+    for s in range(12):
+        ref.step(1)
+        job.step(1)
+        for b in range(len(case.bodies)):
+            for f in POINT_FIELDS:
+                assert bits_equal(job.points(b, f), ref.points(b, f)), f"step {s} body {b} point {f}"

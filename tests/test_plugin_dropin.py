@@ -30,6 +30,13 @@ def test_plugin_configures_from_a_reference_config():
     assert job.nbodies == 1 and job.n_points(0) == 144
 
 
+def _neohookean(case):
+    for body in case.bodies:
+        body.material_class = "CompressibleNeohookeanElasticity"
+    case.name += "_neohookean"
+    return case
+
+
 CASES = {
     "block_drop_2d": (inputs.block_drop_2d, 30),
     "collision_2d": (lambda: inputs.two_body_collision_2d(20, steps=20), 20),
@@ -38,6 +45,7 @@ CASES = {
                                                                steps=20), 20),
     "sliding_3d_smooth_box": (lambda: inputs.sliding_block(3, "CartesianSmoothBox", n_cells=12, steps=10), 10),
     "wall_collision_2d_reflected": (lambda: inputs.wall_collision(2, n_cells=16, steps=20), 20),
+    "collision_3d_neohookean": (lambda: _neohookean(inputs.two_body_collision_3d(16, steps=8, gap=0.01)), 8),
 }
 
 
