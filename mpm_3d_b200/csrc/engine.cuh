@@ -424,12 +424,6 @@ class Batch : public BatchBase {
       }
       MPM_TRY(upload(B.P.active, act));
       MPM_TRY(upload(B.P.pid, pid));
-      if (neo) {
-        // CompressibleNeohookeanElasticity::init: F = I (the other
-        // components are the arena's zeros)
-        std::vector<PT> one((size_t)n, PT(1));
-        for (int k = 0; k < 9; k += 4) MPM_TRY(upload(B.P.F[k], one));
-      }
     }
     B.mat = make_material(desc.has_material, desc.E, desc.nu, desc.material_kind);
     B.has_boundary = desc.has_boundary;

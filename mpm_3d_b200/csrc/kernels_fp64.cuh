@@ -361,47 +361,54 @@ __device__ __forceinline__ void jaumann_update(const R L[3][3], R* s6, R G, R la
 }
 
 // CompressibleNeohookeanElasticity::calculateStress
-// (compressible_neohookean_elasticity.cpp:44-62) for one point: the
-// deformation gradient (global memory, row-major components F[0..8]) advances
-// as F += (L F) dt; with B = F F^T and J = sqrt(det B) the stress is
-// T = G/J (B - I) + lambda ln(J)/J I (lambda = K - 2G/3), returned as the 6
-// stored components (B is symmetric).
+// (compressible_neohookean_elasticity.cpp:44-62) for one point. The
+// reference advances F += (L F) dt and sets T = G/J (B - I) + lambda ln(J)/J I
+// with B = F F^T, J = sqrt(det B), lambda = K - 2G/3. Here the deformation
+// gradient is kept as H = F - I (global memory, row-major components
+// H[0..8]), so the same quantities come without the cancellation of B - I
+// and ln J near the identity (which costs FP32 most of its digits at small
+// strains): H += (L + L H) dt, B - I = H + H^T + H H^T,
+// J - 1 = det(I + H) - 1 = tr H + ((tr H)^2 - tr(H H))/2 + det H, and
+// ln J = log1p(J - 1). Returns the 6 stored stress components.
 template <typename R, typename PT>
-__device__ __forceinline__ void neohookean_update(PT* const* Fp, int64_t p, const R L[3][3], R* s6, R G, R lambda,
+__device__ __forceinline__ void neohookean_update(PT* const* Hp, int64_t p, const R L[3][3], R* s6, R G, R lambda,
                                                   R dt) {
-  R F[3][3];
+  R H[3][3];
 #pragma unroll
   for (int a = 0; a < 3; a++)
 #pragma unroll
-    for (int b = 0; b < 3; b++) F[a][b] = (R)Fp[3 * a + b][p];
-  R LF[3][3];
+    for (int b = 0; b < 3; b++) H[a][b] = (R)Hp[3 * a + b][p];
+  R LH[3][3];
 #pragma unroll
   for (int a = 0; a < 3; a++)
 #pragma unroll
-    for (int b = 0; b < 3; b++) LF[a][b] = L[a][0] * F[0][b] + L[a][1] * F[1][b] + L[a][2] * F[2][b];
+    for (int b = 0; b < 3; b++) LH[a][b] = L[a][0] * H[0][b] + L[a][1] * H[1][b] + L[a][2] * H[2][b];
 #pragma unroll
   for (int a = 0; a < 3; a++)
 #pragma unroll
     for (int b = 0; b < 3; b++) {
-      F[a][b] = F[a][b] + LF[a][b] * dt;
-      Fp[3 * a + b][p] = (PT)F[a][b];
+      H[a][b] = H[a][b] + (L[a][b] + LH[a][b]) * dt;
+      Hp[3 * a + b][p] = (PT)H[a][b];
     }
-  R B[3][3];
+  const R trH = H[0][0] + H[1][1] + H[2][2];
+  R trHH = R(0);
 #pragma unroll
   for (int a = 0; a < 3; a++)
 #pragma unroll
-    for (int b = 0; b < 3; b++) B[a][b] = F[a][0] * F[b][0] + F[a][1] * F[b][1] + F[a][2] * F[b][2];
-  const R det = B[0][0] * (B[1][1] * B[2][2] - B[2][1] * B[1][2]) - B[0][1] * (B[1][0] * B[2][2] - B[2][0] * B[1][2]) +
-                B[0][2] * (B[1][0] * B[2][1] - B[2][0] * B[1][1]);
-  const R J = sqrt(det);
+    for (int b = 0; b < 3; b++) trHH += H[a][b] * H[b][a];
+  const R detH = H[0][0] * (H[1][1] * H[2][2] - H[2][1] * H[1][2]) - H[0][1] * (H[1][0] * H[2][2] - H[2][0] * H[1][2]) +
+                 H[0][2] * (H[1][0] * H[2][1] - H[2][0] * H[1][1]);
+  const R Jm1 = trH + R(0.5) * (trH * trH - trHH) + detH;
+  const R J = R(1) + Jm1;
   const R s1 = G / J;
-  const R s2 = lambda * log(J) / J;
+  const R s2 = lambda * log1p(Jm1) / J;
   const int ia[6] = {0, 1, 2, 0, 1, 0};
   const int ib[6] = {0, 1, 2, 1, 2, 2};
 #pragma unroll
   for (int c = 0; c < 6; c++) {
     const int a = ia[c], b = ib[c];
-    s6[c] = s1 * (B[a][b] - (a == b ? R(1) : R(0))) + (a == b ? s2 : R(0));
+    const R bmi = H[a][b] + H[b][a] + (H[a][0] * H[b][0] + H[a][1] * H[b][1] + H[a][2] * H[b][2]);
+    s6[c] = s1 * bmi + (a == b ? s2 : R(0));
   }
 }
 

@@ -26,8 +26,9 @@ struct PointsT {
                      // move (inactive from the next map build on)
   int32_t* pid;      // original index of the point
   double* L;         // 9 per point when debug output is kept (FP64 form), else null
-  PT* F[9];          // CompressibleNeohookeanElasticity deformation gradient
-                     // (row-major components), else null
+  PT* F[9];          // CompressibleNeohookeanElasticity deformation gradient,
+                     // kept as F - I (row-major components; zero = identity,
+                     // CompressibleNeohookeanElasticity::init), else null
 };
 using PointsDev = PointsT<double>;
 

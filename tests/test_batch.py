@@ -164,3 +164,15 @@ def test_mixed_single_handle_within_1e4_of_fp64():
 def test_mixed_2d_single_handle():
     c = inputs.block_drop_2d()
     _compare(c, _solo(c, 200, mode="mixed"), _solo(c, 200), MIXED_TOL, "mixed 2D block drop")
+
+
+def test_mixed_neohookean_and_boundaries_within_1e4_of_fp64():
+    """The adjacent material and boundaries in the mixed form (FP32 point
+    state and deformation gradient, FP64 nodal sums): a neo-Hookean
+    collision and a block on a frictional floor, against FP64."""
+    coll = inputs.two_body_collision_3d(16, steps=20, gap=0.01)
+    for b in coll.bodies:
+        b.material_class = "CompressibleNeohookeanElasticity"
+    slide = inputs.sliding_block(3, "CartesianFrictionalBox", mu=0.3, n_cells=12, steps=20)
+    for c in (coll, slide):
+        _compare(c, _solo(c, c.steps, mode="mixed"), _solo(c, c.steps), MIXED_TOL, f"mixed {c.name}")
