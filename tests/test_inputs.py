@@ -57,3 +57,28 @@ def test_points_file_round_trip_is_exact():
     b = c.bodies[0]
     assert np.array_equal(m, b.m) and np.array_equal(v, b.v)
     assert np.array_equal(x, b.x) and np.array_equal(xt, b.x_t) and np.array_equal(act, b.active)
+
+
+def test_adjacent_classes_in_written_configs():
+    """The boundary, contact and material classes beyond the path's defaults
+    reach the .cfg the reference reads, with their properties."""
+    slide = inputs.sliding_block(2, "CartesianFrictionalBox", mu=0.25, n_cells=16, steps=5)
+    assert inputs.boundary_kind(slide.bodies[0]) == 3
+    assert slide.bodies[0].x[:, 1].min() > 0.0 and slide.bodies[0].x[:, 0].min() > 0.0
+    coll = inputs.wall_collision(3, n_cells=8, steps=5)
+    assert coll.contacts[0].reflected and [inputs.boundary_kind(b) for b in coll.bodies] == [2, 2]
+    coll.bodies[0].material_class = "CompressibleNeohookeanElasticity"
+    assert inputs.material_kind(coll.bodies[0]) == 1 and inputs.material_kind(coll.bodies[1]) == 0
+    d = tempfile.mkdtemp()
+    text = open(inputs.write_case(slide, d)).read()
+    assert 'boundary-class = "CartesianFrictionalBox"' in text and "boundary-props = {0.25" in text
+    text = open(inputs.write_case(coll, d)).read()
+    assert 'class = "ContactHuang_ReflectedBoundary"' in text
+    assert 'boundary-class = "CartesianSmoothBox"' in text
+    assert 'material-class = "CompressibleNeohookeanElasticity"' in text
+    assert 'material-class = "IsotropicLinearElasticity"' in text
+    plain = inputs.block_drop_2d()
+    assert inputs.boundary_kind(plain.bodies[0]) == 1
+    plain.bodies[0].boundary = False
+    assert inputs.boundary_kind(plain.bodies[0]) == 0
+    assert "boundary-class" not in open(inputs.write_case(plain, d)).read()
