@@ -7,7 +7,9 @@ steps plus the S / gradS triplets of the first map build. The reference tree
 has no golden vectors of its own for this path, so these outputs are the pin
 for the C restatement (oracle/mpm_oracle.c) and, through it, for the GPU path.
 
-    make -C oracle REF=/path/to/mpm_3d && python tests/golden/make_golden.py
+    make -C oracle REF=/path/to/mpm_3d && python tests/golden/make_golden.py [name ...]
+
+With names, only those fixtures are (re)written.
 """
 import os
 import sys
@@ -35,6 +37,10 @@ def golden_cases():
     explicit = inputs.two_body_collision_3d(16, steps=6, gap=0.01)
     explicit.contact_spec = 0
     explicit.name += "_explicit"
+    neohookean = inputs.two_body_collision_2d(20, steps=40)
+    for body in neohookean.bodies:
+        body.material_class = "CompressibleNeohookeanElasticity"
+    neohookean.name += "_neohookean"
     return {
         "block_drop_2d": (inputs.block_drop_2d(), [1, 10, 100]),
         "block_drop_2d_cpdi_off": (cpdi_off, [1, 20]),
@@ -42,6 +48,12 @@ def golden_cases():
         "collision_3d_touching": (inputs.two_body_collision_3d(16, steps=6, gap=0.01), [1, 6]),
         "collision_3d_explicit": (explicit, [6]),
         "column_collapse_s16": (inputs.column_collapse_3d(scale=16, steps=10), [10]),
+        # the classes beside the path's defaults: boundaries, reflected contact, material
+        "sliding_2d_frictional": (inputs.sliding_block(2, "CartesianFrictionalBox", mu=0.3, n_cells=16, steps=15),
+                                  [1, 15]),
+        "sliding_3d_smooth": (inputs.sliding_block(3, "CartesianSmoothBox", mu=0.3, n_cells=8, steps=15), [15]),
+        "wall_collision_2d_reflected": (inputs.wall_collision(2, n_cells=16, steps=15), [1, 15]),
+        "collision_2d_neohookean": (neohookean, [1, 40]),
     }
 
 
@@ -78,5 +90,7 @@ def run(name, case, snaps):
 
 
 if __name__ == "__main__":
+    wanted = set(sys.argv[1:])
     for name, (case, snaps) in golden_cases().items():
-        run(name, case, snaps)
+        if not wanted or name in wanted:
+            run(name, case, snaps)

@@ -56,6 +56,20 @@ def test_golden_cases_exercise_contact():
     gold = np.load(os.path.join(GOLDEN, "collision_3d_touching.npz"))
     force = gold["s6_c0_force"]
     assert (np.abs(force).sum(axis=1) > 0).sum() > 10
+    gold = np.load(os.path.join(GOLDEN, "wall_collision_2d_reflected.npz"))
+    assert (np.abs(gold["s15_c0_force"]).sum(axis=1) > 0).sum() > 0
+
+
+def test_golden_cases_exercise_their_classes():
+    """The fixtures of the adjacent classes are not trivially equal to the
+    defaults: friction slows the sliding block more than the slip wall, and
+    the neo-Hookean stress departs from the linear one."""
+    friction = np.load(os.path.join(GOLDEN, "sliding_2d_frictional.npz"))
+    first, last = friction["s1_b0_p_x_t"][:, 0], friction["s15_b0_p_x_t"][:, 0]
+    assert last.mean() < 0.9 * first.mean()
+    neo = np.load(os.path.join(GOLDEN, "collision_2d_neohookean.npz"))["s40_b0_p_T"]
+    lin = np.load(os.path.join(GOLDEN, "collision_2d.npz"))["s40_b0_p_T"]
+    assert np.abs(neo - lin).max() > 1e-3 * np.abs(lin).max()
 
 
 needs_ref = pytest.mark.skipif(not bridge.available("libmpmref_parity.so"),
