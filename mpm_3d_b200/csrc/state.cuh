@@ -9,9 +9,12 @@ namespace mpmb200 {
 
 // Points of one body, structure of arrays, in the point precision PT
 // (double for the FP64 form, float for the mixed form). The Cauchy stress is
-// stored as its 6 independent components (xx, yy, zz, xy, yz, xz): the
-// reference's update (isolin.cpp:62-74) keeps T exactly symmetric when it
-// starts symmetric, so the 9-component form carries no extra information.
+// stored as its 6 independent components (xx, yy, zz, xy, yz, xz). The
+// reference's update (isolin.cpp:62-74) keeps T symmetric up to rounding: W T
+// and T W are each other's negated transposes bit for bit, but their terms
+// are added to the symmetric part in a different order for (i,j) and (j,i),
+// so T_ij and T_ji can differ in the last bit. One stored value per pair is
+// within the FP64 parity tolerance of either.
 template <typename PT>
 struct PointsT {
   int64_t n;
