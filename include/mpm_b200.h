@@ -75,8 +75,8 @@ typedef struct {
 } mpmgpu_config;
 
 /* One DefaultBody: its points (DefaultPoints::readFromFile columns,
- * default_points.cpp:150-174), IsotropicLinearElasticity E and nu
- * (isolin.cpp:26-46) and its boundary: CartesianBox (cartesian_box.cpp),
+ * default_points.cpp:150-174), its material's E and nu (isolin.cpp:26-46)
+ * and further properties, and its boundary: CartesianBox (cartesian_box.cpp),
  * CartesianSmoothBox (cartesian_smooth_box.cpp) or CartesianFrictionalBox
  * (cartesian_frictional_box.cpp, friction mu_f from its fp64 property). */
 typedef struct {
@@ -97,7 +97,17 @@ typedef struct {
   int material_kind;    /* 0: IsotropicLinearElasticity (isolin.cpp),
                            1: CompressibleNeohookeanElasticity
                            (compressible_neohookean_elasticity.cpp: F from
-                           the identity, neo-Hookean stress) */
+                           the identity, neo-Hookean stress),
+                           2: Sand_SachithLocal (sand_sachithlocal.cpp:
+                           Jaumann trial stress, local mu(I) return,
+                           gammap and gammap_dot from zero) */
+  double material_props[6]; /* Sand_SachithLocal: grain diameter, mu_s,
+                           grains_rho, rho_critical, mu_2, I_0 as its init
+                           resolves them (sand_sachithlocal.cpp:57-103:
+                           mu_2 = mu_s and I_0 = 1 when the config gives
+                           six material-props) */
+  int material_flags;   /* bit 0: USE_DENSITY_FOR_PRESSURE (Sand_SachithLocal
+                           material-str-props) */
 } mpmgpu_body_desc;
 
 typedef struct mpmgpu_handle mpmgpu_handle;
@@ -115,7 +125,10 @@ typedef enum {
   MPMGPU_P_M = 7,      /* 1 */
   MPMGPU_P_V = 8,      /* 1 */
   MPMGPU_P_EXTENT = 9, /* 1 */
-  MPMGPU_P_ACTIVE = 10 /* 1 (as double) */
+  MPMGPU_P_ACTIVE = 10, /* 1 (as double) */
+  MPMGPU_P_GAMMAP = 11, /* 1, Sand_SachithLocal bodies: plastic shear
+                           strain (sand_sachithlocal.cpp:118-122) */
+  MPMGPU_P_GAMMAP_DOT = 12 /* 1, Sand_SachithLocal bodies: its rate */
 } mpmgpu_point_field;
 
 /* Node fields, as named in DefaultNodes::writeFrame

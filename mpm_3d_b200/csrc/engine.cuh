@@ -100,7 +100,11 @@ inline void make_geometry(const mpmgpu_config& cfg, Geom& g, MapConst& mc, BinGe
 }
 
 // IsotropicLinearElasticity constants, isolin.cpp:34-38.
-inline MaterialParams make_material(int has_material, double E, double nu, int kind = 0) {
+// props: a Sand_SachithLocal body's grain diameter, mu_s, grains_rho,
+// rho_critical, mu_2 and I_0 (kind 2 only); flags bit 0:
+// USE_DENSITY_FOR_PRESSURE.
+inline MaterialParams make_material(int has_material, double E, double nu, int kind = 0,
+                                    const double* props = nullptr, int flags = 0) {
   MaterialParams m{};
   m.has_material = has_material;
   m.kind = has_material ? kind : 0;
@@ -108,7 +112,17 @@ inline MaterialParams make_material(int has_material, double E, double nu, int k
     const double G = E / (2.0 * (1.0 + nu));
     const double K = E / (3.0 * (1.0 - 2 * nu));
     m.G = G;
+    m.K = K;
     m.lambda = K - 2.0 * G / 3.0;
+  }
+  if (m.kind == 2 && props) {
+    m.grains_d = props[0];
+    m.mu_s = props[1];
+    m.grains_rho = props[2];
+    m.rho_critical = props[3];
+    m.mu_2 = props[4];
+    m.i_0 = props[5];
+    m.use_density = flags & 1;
   }
   return m;
 }
@@ -351,14 +365,14 @@ class Batch : public BatchBase {
     B.n = n;
     MPM_TRY(stage_reserve((size_t)n * (21 * sizeof(PT) + 8) + 64 * 256));
     const size_t ns = (size_t)j->g.nslots;
-    if (desc.has_material && (desc.material_kind < 0 || desc.material_kind > 1))
+    if (desc.has_material && (desc.material_kind < 0 || desc.material_kind > 2))
       return fail(MPMGPU_ERR_ARG, "unknown material kind");
-    const bool neo = desc.has_material && desc.material_kind == 1;
+    const int nstate = material_state_arrays(desc.has_material, desc.material_kind);
     // both point buffers and the nodal arrays of the body
     MPM_TRY(alloc_arena(
         [&](Arena& a) {
-          layout_points(a, B.P, n, neo);
-          layout_points(a, B.Palt, n, neo);
+          layout_points(a, B.P, n, nstate);
+          layout_points(a, B.Palt, n, nstate);
           if (det_) {
             carve(a, &B.Ar.m, ns);
             for (int d = 0; d < 3; d++) {
@@ -425,7 +439,8 @@ class Batch : public BatchBase {
       MPM_TRY(upload(B.P.active, act));
       MPM_TRY(upload(B.P.pid, pid));
     }
-    B.mat = make_material(desc.has_material, desc.E, desc.nu, desc.material_kind);
+    B.mat = make_material(desc.has_material, desc.E, desc.nu, desc.material_kind, desc.material_props,
+                          desc.material_flags);
     B.has_boundary = desc.has_boundary;
     B.mu_f = desc.boundary_mu;
     MPM_TRY(finish_uploads());
@@ -600,6 +615,8 @@ class Batch : public BatchBase {
       return MPMGPU_OK;
     }
     if (field == MPMGPU_P_L && !B->P.L) return fail(MPMGPU_ERR_STATE, "L is kept only with keep_debug in the FP64 form");
+    if ((field == MPMGPU_P_GAMMAP || field == MPMGPU_P_GAMMAP_DOT) && B->mat.kind != 2)
+      return fail(MPMGPU_ERR_STATE, "gammap and gammap_dot belong to Sand_SachithLocal bodies");
     // the point ids and the arrays of the field, copied with one wait
     std::vector<std::pair<const void*, size_t>> items;
     items.emplace_back(B->P.pid, nz * sizeof(int32_t));
@@ -628,6 +645,8 @@ class Batch : public BatchBase {
       case MPMGPU_P_V: items.emplace_back(B->P.vol, np); break;
       case MPMGPU_P_EXTENT: items.emplace_back(B->P.ext, np); break;
       case MPMGPU_P_ACTIVE: items.emplace_back(B->P.active, nz * sizeof(int32_t)); break;
+      case MPMGPU_P_GAMMAP: items.emplace_back(B->P.ms[0], np); break;
+      case MPMGPU_P_GAMMAP_DOT: items.emplace_back(B->P.ms[1], np); break;
       default: return fail(MPMGPU_ERR_ARG, "unknown point field");
     }
     std::vector<const unsigned char*> h;
@@ -681,7 +700,9 @@ class Batch : public BatchBase {
       }
       case MPMGPU_P_M:
       case MPMGPU_P_V:
-      case MPMGPU_P_EXTENT: {
+      case MPMGPU_P_EXTENT:
+      case MPMGPU_P_GAMMAP:
+      case MPMGPU_P_GAMMAP_DOT: {
         const PT* a = arr(1);
         for (size_t i = 0; i < nz; i++) out[pid[i]] = (double)a[i];
         return MPMGPU_OK;
@@ -985,7 +1006,7 @@ class Batch : public BatchBase {
   // Point arrays hold n entries plus 8 of padding: the fused kernel's bulk
   // copies round their windows out to 16-byte boundaries and may read up to
   // 3 entries past the last point.
-  void layout_points(Arena& a, PointsT<PT>& P, int64_t n, bool with_F) {
+  void layout_points(Arena& a, PointsT<PT>& P, int64_t n, int nstate) {
     P = PointsT<PT>{};
     P.n = n;
     const size_t na = (size_t)n + 8;
@@ -1002,8 +1023,7 @@ class Batch : public BatchBase {
     carve(a, &P.pid, na);
     P.L = nullptr;
     if (keep_debug_ && !mixed()) carve(a, &P.L, (size_t)n * 9);
-    if (with_F)
-      for (int k = 0; k < 9; k++) carve(a, &P.F[k], na);
+    for (int k = 0; k < nstate; k++) carve(a, &P.ms[k], na);
   }
 
   // Returns a job's arrays to the pool after the work already queued on the
@@ -1699,8 +1719,8 @@ class Batch : public BatchBase {
         MPM_TRY(snap_one(b.P.active, ni));
         MPM_TRY(snap_one(b.P.pid, ni));
         if (b.P.L) MPM_TRY(snap_one(b.P.L, (size_t)b.n * 9 * sizeof(double)));
-        if (b.P.F[0])
-          for (int k = 0; k < 9; k++) MPM_TRY(snap_one(b.P.F[k], np));
+        for (int k = 0; k < 9; k++)
+          if (b.P.ms[k]) MPM_TRY(snap_one(b.P.ms[k], np));
         MPM_TRY(snap_one(b.A.m, ns));
         for (int d = 0; d < 3; d++) {
           MPM_TRY(snap_one(b.A.mx[d], ns));

@@ -476,7 +476,17 @@ __device__ __forceinline__ void gather_update(const BodyCtx<PT>& c, int* err, un
   P.vol[p] = vol;
   if (c.mat.has_material && c.mat.kind == 1) {
     R s6[6];
-    neohookean_update<R>(P.F, p, gs.L, s6, (R)c.mat.G, (R)c.mat.lambda, dt);
+    neohookean_update<R>(P.ms, p, gs.L, s6, (R)c.mat.G, (R)c.mat.lambda, dt);
+#pragma unroll
+    for (int k = 0; k < 6; k++) {
+      sp[(kFs + k) * ROW] = s6[k];
+      P.s[k][p] = s6[k];
+    }
+  } else if (c.mat.has_material && c.mat.kind == 2) {
+    R s6[6];
+#pragma unroll
+    for (int k = 0; k < 6; k++) s6[k] = sp[(kFs + k) * ROW];
+    sand_update<DIM, R>(P.ms, p, gs.L, s6, (R)sp[kFm * ROW], vol, c.mat, dt);
 #pragma unroll
     for (int k = 0; k < 6; k++) {
       sp[(kFs + k) * ROW] = s6[k];

@@ -412,6 +412,72 @@ __device__ __forceinline__ void neohookean_update(PT* const* Hp, int64_t p, cons
   }
 }
 
+// Sand_SachithLocal::calculateStress (sand_sachithlocal.cpp:140-215) for one
+// point, cohesion 0, on the 6 stored components. The trial stress s_tr is
+// the Jaumann update above; p_tr = -tr(s_tr)/3 (or K (rho/rho_c - 1) with
+// USE_DENSITY_FOR_PRESSURE), t0 = s_tr + p_tr I, tau_tr = |t0|/sqrt(2) with
+// |t0|^2 summed in the reference's row-major order. Below the critical
+// density, or at p_tr <= 0, the stress is zero and the shear rate is
+// tau_tr/(G dt). Inside the cone tau_tr <= mu_s p_tr the trial stress stays.
+// Otherwise tau is the smaller root of tau^2 - (S2 + tau_tr + alpha) tau +
+// S2 tau_tr + S0 alpha (S0 = mu_s p_tr, S2 = mu_2 p_tr, alpha = G I_0 dt
+// sqrt(p_tr/grains_rho)/grains_d), taken as in negative_root (44-53), and
+// T = (tau/tau_tr) t0 - p_tr I. A NaN p_tr leaves T as it was. gammap
+// (st[0]) advances by the shear rate times dt and gammap_dot (st[1]) takes
+// the rate. rho = m/V with V already updated this step (updateDensity runs
+// before the stress, explicit_usl.cpp:332-352).
+template <int DIM, typename R, typename PT>
+__device__ __forceinline__ void sand_update(PT* const* st, int64_t p, const R L[3][3], R* s6, R m, R vol,
+                                            const MaterialParams& mp, R dt) {
+  R t0[6];
+#pragma unroll
+  for (int k = 0; k < 6; k++) t0[k] = s6[k];
+  jaumann_update<DIM, R>(L, t0, (R)mp.G, (R)mp.lambda, dt);
+  R p_tr = -((t0[0] + t0[1]) + t0[2]) / R(3.0);
+#pragma unroll
+  for (int k = 0; k < 3; k++) t0[k] = t0[k] + p_tr;
+  // xx xy xz yx yy yz zx zy zz
+  R nn = t0[0] * t0[0];
+  nn += t0[3] * t0[3];
+  nn += t0[5] * t0[5];
+  nn += t0[3] * t0[3];
+  nn += t0[1] * t0[1];
+  nn += t0[4] * t0[4];
+  nn += t0[5] * t0[5];
+  nn += t0[4] * t0[4];
+  nn += t0[2] * t0[2];
+  const R tau_tr = sqrt(nn) / sqrt(R(2.0));
+  const R G = (R)mp.G;
+  const R rho = m / vol;
+  const R rho_c = (R)mp.rho_critical;
+  if (mp.use_density) p_tr = (R)mp.K * ((rho - rho_c) / rho_c);
+  R nup;
+  if (rho < rho_c || p_tr <= R(0)) {
+    nup = tau_tr / (G * dt);
+#pragma unroll
+    for (int k = 0; k < 6; k++) s6[k] = R(0);
+  } else if (p_tr > R(0)) {
+    const R S0 = (R)mp.mu_s * p_tr;
+    R tau = tau_tr, scale = R(1);
+    if (!(tau_tr <= S0)) {
+      const R S2 = (R)mp.mu_2 * p_tr;
+      const R alpha = G * (R)mp.i_0 * dt * sqrt(p_tr / (R)mp.grains_rho) / (R)mp.grains_d;
+      const R b = -(S2 + tau_tr + alpha);
+      const R c = S2 * tau_tr + S0 * alpha;
+      const R disc = sqrt(b * b - R(4) * c);
+      tau = b > R(0) ? (-b - disc) / R(2) : (R(2) * c) / (-b + disc);
+      scale = tau / tau_tr;
+    }
+    nup = ((tau_tr - tau) / G) / dt;
+#pragma unroll
+    for (int k = 0; k < 6; k++) s6[k] = scale * t0[k] - (k < 3 ? p_tr : R(0));
+  } else {
+    nup = R(0);
+  }
+  st[0][p] = (PT)((R)st[0][p] + nup * dt);
+  st[1][p] = (PT)nup;
+}
+
 // Order-independent nodal sums of the deterministic form (pre-rounded
 // two-level summation after Demmel and Nguyen, "Fast reproducible
 // floating-point summation", ARITH 2013). With M bounding every partial sum

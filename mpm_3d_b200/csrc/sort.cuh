@@ -332,8 +332,9 @@ __global__ void k_sort_scatter(const BatchHdr* hdr, const BodyCtx<PT>* bodies, c
     D.pid[pos] = S.pid[p];
     if (S.L != nullptr)
       for (int a = 0; a < 9; a++) D.L[9 * pos + a] = S.L[9 * p + a];
-    if (S.F[0] != nullptr)
-      for (int a = 0; a < 9; a++) D.F[a][pos] = S.F[a][p];
+#pragma unroll
+    for (int a = 0; a < 9; a++)
+      if (S.ms[a] != nullptr) D.ms[a][pos] = S.ms[a][p];
   }
 }
 

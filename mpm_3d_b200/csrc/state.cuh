@@ -29,9 +29,13 @@ struct PointsT {
                      // move (inactive from the next map build on)
   int32_t* pid;      // original index of the point
   double* L;         // 9 per point when debug output is kept (FP64 form), else null
-  PT* F[9];          // CompressibleNeohookeanElasticity deformation gradient,
-                     // kept as F - I (row-major components; zero = identity,
-                     // CompressibleNeohookeanElasticity::init), else null
+  // Per-point state of the material, zero at the start, else null:
+  // CompressibleNeohookeanElasticity keeps its deformation gradient as F - I
+  // (ms[0..8], row-major; zero = identity,
+  // CompressibleNeohookeanElasticity::init); Sand_SachithLocal its plastic
+  // shear strain gammap (ms[0]) and rate gammap_dot (ms[1])
+  // (sand_sachithlocal.cpp:98-101).
+  PT* ms[9];
 };
 using PointsDev = PointsT<double>;
 
@@ -61,10 +65,21 @@ struct StepParams {
 
 struct MaterialParams {
   int has_material;
-  int kind;          // 0 IsotropicLinearElasticity, 1 CompressibleNeohookeanElasticity
+  int kind;          // 0 IsotropicLinearElasticity, 1 CompressibleNeohookeanElasticity,
+                     // 2 Sand_SachithLocal
   double G;
   double lambda;     // K - 2G/3
+  double K;          // E / (3 (1 - 2 nu))
+  // Sand_SachithLocal properties (sand_sachithlocal.cpp:57-103)
+  double grains_d, mu_s, grains_rho, rho_critical, mu_2, i_0;
+  int use_density;   // USE_DENSITY_FOR_PRESSURE: pressure from the density
+  int pad_;
 };
+
+// Per-point material state arrays of each material kind (PointsT::ms).
+inline int material_state_arrays(int has_material, int kind) {
+  return !has_material ? 0 : (kind == 1 ? 9 : (kind == 2 ? 2 : 0));
+}
 
 // One job (the reference's Job: one grid, its bodies and contacts). Bodies
 // body0 .. body0+nb-1 of the body tables belong to it; contact body indices

@@ -68,7 +68,13 @@ class Body:
     E: float = 1e5
     nu: float = 0.3
     material: bool = True
-    material_class: str = "IsotropicLinearElasticity"   # or "CompressibleNeohookeanElasticity"
+    # "IsotropicLinearElasticity", "CompressibleNeohookeanElasticity" or
+    # "Sand_SachithLocal"
+    material_class: str = "IsotropicLinearElasticity"
+    # material-props after E and nu (Sand_SachithLocal: grain diameter, mu_s,
+    # grains_rho, rho_critical[, mu_2, I_0]) and material-str-props
+    material_props: Tuple[float, ...] = ()
+    material_str_props: Tuple[str, ...] = ()
     # True or "CartesianBox", "CartesianSmoothBox", "CartesianFrictionalBox";
     # False: no boundary
     boundary: Union[bool, str] = True
@@ -80,15 +86,29 @@ class Body:
 
 
 BOUNDARY_CLASSES = ("CartesianBox", "CartesianSmoothBox", "CartesianFrictionalBox")
-MATERIAL_CLASSES = ("IsotropicLinearElasticity", "CompressibleNeohookeanElasticity")
+MATERIAL_CLASSES = ("IsotropicLinearElasticity", "CompressibleNeohookeanElasticity", "Sand_SachithLocal")
+SAND_DENSITY_PRESSURE = "USE_DENSITY_FOR_PRESSURE"
 
 
 def material_kind(body: "Body") -> int:
     """The C ABI's material code: 0 IsotropicLinearElasticity, 1
-    CompressibleNeohookeanElasticity."""
+    CompressibleNeohookeanElasticity, 2 Sand_SachithLocal."""
     if body.material_class not in MATERIAL_CLASSES:
         raise ValueError(f"unknown material class {body.material_class!r}")
     return MATERIAL_CLASSES.index(body.material_class)
+
+
+def sand_params(body: "Body") -> Tuple[Tuple[float, ...], bool]:
+    """A Sand_SachithLocal body's properties as its init resolves them
+    (sand_sachithlocal.cpp:57-103): (grain diameter, mu_s, grains_rho,
+    rho_critical, mu_2, I_0), with mu_2 = mu_s and I_0 = 1 unless both are
+    given; and whether USE_DENSITY_FOR_PRESSURE is set."""
+    p = tuple(float(v) for v in body.material_props)
+    if len(p) < 4:
+        raise ValueError("Sand_SachithLocal needs E, nu, grain diameter, mu_s, grains_rho and rho_critical")
+    if len(p) < 6:
+        p = p[:4] + (p[1], 1.0)
+    return p[:6], SAND_DENSITY_PRESSURE in body.material_str_props
 
 
 def boundary_class(body: "Body") -> Optional[str]:
@@ -256,6 +276,29 @@ def two_body_collision_2d(n_cells: int = 20, steps: int = 200, gap: float = 0.02
                 steps=steps, bodies=[a, b], contacts=[Contact(0, 1, mu)])
 
 
+def sand_column(dim: int = 2, n_cells: int = 20, steps: int = 200, density_pressure: bool = False,
+                mu_2: Optional[float] = None) -> Case:
+    """A granular column collapsing under gravity on the floor of a 1 m box
+    (0.5 m deep in 3D), after the reference's own column-collapse examples
+    (examples/columncollapse2D, columncollapse3D): Sand_SachithLocal with
+    E = 1e7, nu = 0.3, grain diameter 0.01 m, mu_s = 0.577, grains_rho =
+    1650, rho_critical = 1000 (optionally mu_2 and I_0 = 0.278, and
+    USE_DENSITY_FOR_PRESSURE), density 1500, CartesianBox, dt = 1e-4. The
+    column is 0.2 m wide and 0.4 m tall at the centre of the floor."""
+    L = (1.0, 1.0) if dim == 2 else (1.0, 1.0, 0.5)
+    N = (n_cells, n_cells) if dim == 2 else (n_cells, n_cells, n_cells // 2)
+    h = tuple(L[i] / N[i] for i in range(dim))
+    size = (0.2, 0.4) if dim == 2 else (0.2, 0.2, 0.4)
+    lo = (0.4, 0.0) if dim == 2 else (0.4, 0.4, 0.0)
+    counts = tuple(int(round(size[i] / (h[i] / 2.0))) for i in range(dim))
+    body = block_points(lo, counts, h, 1500.0, (0.0,) * dim, name="column", E=1e7, nu=0.3)
+    body.material_class = "Sand_SachithLocal"
+    body.material_props = (0.01, 0.577, 1650.0, 1000.0) + (() if mu_2 is None else (mu_2, 0.278))
+    body.material_str_props = (SAND_DENSITY_PRESSURE,) if density_pressure else ()
+    name = f"sand_column_{dim}d" + ("_mu2" if mu_2 is not None else "") + ("_density" if density_pressure else "")
+    return Case(name=name, dim=dim, L=L, N=N, dt=1e-4, steps=steps, bodies=[body])
+
+
 def column_collapse_3d(scale: int = 1, seed: int = 1002, steps: int = 500) -> Case:
     """Column 0.5x0.5x0.75 m on the floor of a 2x2x1 m domain, rho=1500."""
     N = (256 // scale, 256 // scale, 128 // scale)
@@ -414,8 +457,11 @@ def write_case(case: Case, directory: str, solver_class: str = "ExplicitUSL", po
         lines += ["body", "{", '    class = "DefaultBody"', f'    name = "{body.name}"', f'    point-file = "{pfile}"',
                   f'    point-class = "{points_class}"', '    node-class = "DefaultNodes"']
         if body.material:
-            lines += [f'    material-class = "{body.material_class}"',
-                      f"    material-props = {{{_fmt(body.E)},{_fmt(body.nu)}}}"]
+            props = ",".join(_fmt(v) for v in (body.E, body.nu, *body.material_props))
+            lines += [f'    material-class = "{body.material_class}"', f"    material-props = {{{props}}}"]
+            if body.material_str_props:
+                sp = ",".join(f'"{v}"' for v in body.material_str_props)
+                lines += [f"    material-str-props = {{{sp}}}"]
         cls = boundary_class(body)
         if cls is not None:
             lines += [f'    boundary-class = "{cls}"']

@@ -20,7 +20,8 @@ LIB_PATH = os.environ.get("MPM_B200_LIB", os.path.join(HERE, "lib", "libmpm_b200
 
 MODES = {"fp64": 0, "fp64_deterministic": 1, "mixed": 2}
 POINT_FIELDS = {"x": (0, 3), "u": (1, 3), "x_t": (2, 3), "mx_t": (3, 3), "b": (4, 3), "L": (5, 9), "T": (6, 9),
-                "m": (7, 1), "v": (8, 1), "extent": (9, 1), "active": (10, 1)}
+                "m": (7, 1), "v": (8, 1), "extent": (9, 1), "active": (10, 1), "gammap": (11, 1),
+                "gammap_dot": (12, 1)}
 NODE_FIELDS = {"m": (0, 1), "mx_t": (1, 3), "f": (2, 3), "x_t": (3, 3), "u": (4, 3), "diff_x_t": (5, 3)}
 CONTACT_FIELDS = {"normal": (0, 3), "force": (1, 3)}
 
@@ -50,7 +51,24 @@ class _BodyDesc(ctypes.Structure):
                 ("x_t", ctypes.c_void_p), ("active", ctypes.c_void_p), ("has_material", ctypes.c_int),
                 ("E", ctypes.c_double), ("nu", ctypes.c_double), ("has_boundary", ctypes.c_int),
                 ("u", ctypes.c_void_p), ("T", ctypes.c_void_p), ("boundary_mu", ctypes.c_double),
-                ("material_kind", ctypes.c_int)]
+                ("material_kind", ctypes.c_int), ("material_props", ctypes.c_double * 6),
+                ("material_flags", ctypes.c_int)]
+
+
+def _body_desc(body: "inputs.Body"):
+    """mpmgpu_body_desc of a body, and the arrays it points at (keep them alive)."""
+    arrs = dict(m=np.ascontiguousarray(body.m, np.float64), v=np.ascontiguousarray(body.v, np.float64),
+                x=np.ascontiguousarray(body.x, np.float64), x_t=np.ascontiguousarray(body.x_t, np.float64),
+                active=np.ascontiguousarray(body.active, np.int32))
+    kind = inputs.material_kind(body)
+    desc = _BodyDesc(body.n, _ptr(arrs["m"]).value, _ptr(arrs["v"]).value, _ptr(arrs["x"]).value,
+                     _ptr(arrs["x_t"]).value, _ptr(arrs["active"]).value, int(body.material), body.E, body.nu,
+                     inputs.boundary_kind(body), None, None, float(body.boundary_mu), kind)
+    if body.material and kind == 2:
+        props, density = inputs.sand_params(body)
+        desc.material_props = (ctypes.c_double * 6)(*props)
+        desc.material_flags = int(density)
+    return desc, arrs
 
 
 class _JobDesc(ctypes.Structure):
@@ -173,13 +191,7 @@ class GPUExplicitUSL:
         self._check(self.lib.mpmgpu_create(ctypes.byref(cfg), ctypes.byref(h)), None)
         self.h = h
         for body in case.bodies:
-            arrs = dict(m=np.ascontiguousarray(body.m, np.float64), v=np.ascontiguousarray(body.v, np.float64),
-                        x=np.ascontiguousarray(body.x, np.float64), x_t=np.ascontiguousarray(body.x_t, np.float64),
-                        active=np.ascontiguousarray(body.active, np.int32))
-            desc = _BodyDesc(body.n, _ptr(arrs["m"]).value, _ptr(arrs["v"]).value, _ptr(arrs["x"]).value,
-                             _ptr(arrs["x_t"]).value, _ptr(arrs["active"]).value, int(body.material), body.E, body.nu,
-                             inputs.boundary_kind(body), None, None, float(body.boundary_mu),
-                             inputs.material_kind(body))
+            desc, arrs = _body_desc(body)
             bid = ctypes.c_int()
             self._check(self.lib.mpmgpu_add_body(self.h, ctypes.byref(desc), ctypes.byref(bid)))
         for c in case.contacts:
@@ -307,14 +319,8 @@ def job_desc(case: inputs.Case, steps: Optional[int] = None):
     cfg = _case_config(case)
     bodies = (_BodyDesc * len(case.bodies))()
     for i, body in enumerate(case.bodies):
-        arrs = dict(m=np.ascontiguousarray(body.m, np.float64), v=np.ascontiguousarray(body.v, np.float64),
-                    x=np.ascontiguousarray(body.x, np.float64), x_t=np.ascontiguousarray(body.x_t, np.float64),
-                    active=np.ascontiguousarray(body.active, np.int32))
+        bodies[i], arrs = _body_desc(body)
         keep.append(arrs)
-        bodies[i] = _BodyDesc(body.n, _ptr(arrs["m"]).value, _ptr(arrs["v"]).value, _ptr(arrs["x"]).value,
-                              _ptr(arrs["x_t"]).value, _ptr(arrs["active"]).value, int(body.material), body.E,
-                              body.nu, inputs.boundary_kind(body), None, None, float(body.boundary_mu),
-                             inputs.material_kind(body))
     contacts = (_ContactDesc * max(1, len(case.contacts)))()
     for i, c in enumerate(case.contacts):
         contacts[i] = _ContactDesc(c.b1, c.b2, c.mu, int(c.reflected))

@@ -104,13 +104,25 @@ void GPUExplicitUSL::setUp(Job* job) {
     desc.u = u.data();
     desc.T = T.data();
     if (body->activeMaterial) {
-      IsotropicLinearElasticity* mat = dynamic_cast<IsotropicLinearElasticity*>(body->material.get());
-      if (!mat) unsupported("material class " + body->material->object_name);
       desc.has_material = 1;
-      // CompressibleNeohookeanElasticity derives from IsotropicLinearElasticity
-      desc.material_kind = dynamic_cast<CompressibleNeohookeanElasticity*>(mat) ? 1 : 0;
-      desc.E = mat->E;
-      desc.nu = mat->nu;
+      if (Sand_SachithLocal* sand = dynamic_cast<Sand_SachithLocal*>(body->material.get())) {
+        // the properties as Sand_SachithLocal::init resolved them
+        // (sand_sachithlocal.cpp:57-103)
+        desc.material_kind = 2;
+        desc.E = sand->E;
+        desc.nu = sand->nu;
+        const double props[6] = {sand->grains_d, sand->MU_S, sand->GRAINS_RHO,
+                                 sand->RHO_CRITICAL, sand->MU_2, sand->I_0};
+        for (int k = 0; k < 6; k++) desc.material_props[k] = props[k];
+        desc.material_flags = sand->use_density_to_determine_pressure ? 1 : 0;
+      } else {
+        IsotropicLinearElasticity* mat = dynamic_cast<IsotropicLinearElasticity*>(body->material.get());
+        if (!mat) unsupported("material class " + body->material->object_name);
+        // CompressibleNeohookeanElasticity derives from IsotropicLinearElasticity
+        desc.material_kind = dynamic_cast<CompressibleNeohookeanElasticity*>(mat) ? 1 : 0;
+        desc.E = mat->E;
+        desc.nu = mat->nu;
+      }
     }
     if (body->activeBoundary) {
       Boundary* bc = body->boundary.get();
@@ -219,6 +231,16 @@ void GPUExplicitUSL::writeBack(Job* job) {
     for (int i = 0; i < n; i++) pts->v(i) = buf[i];
     check(mpmgpu_download_points(handle, id, MPMGPU_P_ACTIVE, buf.data()), "mpmgpu_download_points");
     for (int i = 0; i < n; i++) pts->active(i) = (int)buf[i];
+    Sand_SachithLocal* sand = job->bodies[b]->activeMaterial
+                                  ? dynamic_cast<Sand_SachithLocal*>(job->bodies[b]->material.get())
+                                  : nullptr;
+    if (sand) {
+      // the material's frame fields (Sand_SachithLocal::writeFrame)
+      check(mpmgpu_download_points(handle, id, MPMGPU_P_GAMMAP, buf.data()), "mpmgpu_download_points");
+      for (int i = 0; i < n; i++) sand->gammap(i) = buf[i];
+      check(mpmgpu_download_points(handle, id, MPMGPU_P_GAMMAP_DOT, buf.data()), "mpmgpu_download_points");
+      for (int i = 0; i < n; i++) sand->gammap_dot(i) = buf[i];
+    }
 
     const int nn = nds->x.size();
     std::vector<double> nb(3 * (size_t)nn);

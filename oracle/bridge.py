@@ -148,6 +148,7 @@ class RestatedJob(_JobBase):
                                   ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_int]
         L.oc_add_contact.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int]
         L.oc_set_gravity.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp]
+        L.oc_set_sand.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, ctypes.c_int, ctypes.c_int]
         for fn in ("oc_step", "oc_num_nodes", "oc_get_point_field", "oc_get_node_field", "oc_get_contact_field",
                    "oc_map_size", "oc_grad_map_size", "oc_get_map", "oc_get_grad_map", "oc_build_map", "oc_destroy"):
             getattr(L, fn).argtypes = None
@@ -159,14 +160,19 @@ class RestatedJob(_JobBase):
         self.h = ctypes.c_void_p(h)
         self.case = case
         self._keep = []
-        from mpm_3d_b200.inputs import boundary_kind, material_kind
-        for body in case.bodies:
+        from mpm_3d_b200.inputs import boundary_kind, material_kind, sand_params
+        for bi, body in enumerate(case.bodies):
             arrs = [np.ascontiguousarray(body.m, np.float64), np.ascontiguousarray(body.v, np.float64),
                     np.ascontiguousarray(body.x, np.float64), np.ascontiguousarray(body.x_t, np.float64),
                     np.ascontiguousarray(body.active, np.int32)]
             L.oc_add_body(self.h, body.n, _ptr(arrs[0]), _ptr(arrs[1]), _ptr(arrs[2]), _ptr(arrs[3]),
                           _ptr(arrs[4], _ip), int(body.material), body.E, body.nu, boundary_kind(body),
                           float(body.boundary_mu), material_kind(body))
+            if body.material and material_kind(body) == 2:
+                props, density = sand_params(body)
+                pa = np.array(props, dtype=np.float64)
+                if L.oc_set_sand(self.h, bi, _ptr(pa), len(props), int(density)) != 0:
+                    raise RuntimeError("oracle rejected the Sand_SachithLocal properties")
         for c in case.contacts:
             L.oc_add_contact(self.h, c.b1, c.b2, c.mu, int(getattr(c, "reflected", False)))
         if case.gravity is not None:

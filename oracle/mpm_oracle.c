@@ -40,8 +40,13 @@ typedef struct {
   double *bc_force;      /* CartesianFrictionalBox bcNodalForce, 3 per node */
   double mu_f;           /* CartesianFrictionalBox friction */
   int has_material;
-  int material_kind;     /* 0 IsotropicLinearElasticity, 1 CompressibleNeohookeanElasticity */
+  int material_kind;     /* 0 IsotropicLinearElasticity, 1 CompressibleNeohookeanElasticity,
+                            2 Sand_SachithLocal */
   double *F;             /* neo-Hookean deformation gradient, 9 per point (row-major) */
+  double *gammap, *gammap_dot; /* Sand_SachithLocal plastic shear strain and rate, 1 per point */
+  /* Sand_SachithLocal properties (sand_sachithlocal.cpp:57-103) */
+  double grains_d, mu_s, grains_rho, rho_critical, mu_2, i_0;
+  int use_density;       /* USE_DENSITY_FOR_PRESSURE */
   int has_boundary;      /* 0 none, 1 CartesianBox, 2 CartesianSmoothBox, 3 CartesianFrictionalBox */
   double E, nu_, G, K, lambda;
   /* COO triplets of the last map build */
@@ -656,9 +661,90 @@ static void update_stress_neohookean(oc_job* J, oc_body* B) {
   }
 }
 
+/* Sand_SachithLocal::negative_root (sand_sachithlocal.cpp:44-53): the
+ * smaller root of a x^2 + b x + c, in the form without cancellation. */
+static double sand_negative_root(double a, double b, double c) {
+  if (b > 0) return (-b - sqrt(b * b - 4 * a * c)) / (2 * a);
+  return (2 * c) / (-b + sqrt(b * b - 4 * a * c));
+}
+
+/* Sand_SachithLocal::calculateStress (sand_sachithlocal.cpp:140-215) with
+ * SPEC = UPDATE (explicit_usl.cpp:352) and cohesion c = 0: the Jaumann trial
+ * stress s_tr = T + dt (2G D + lambda tr(D) I + W T - T W), its pressure
+ * p_tr = -tr(s_tr)/3 (or K (rho/rho_c - 1) with USE_DENSITY_FOR_PRESSURE),
+ * deviator t0 = s_tr + p_tr I and tau_tr = |t0|/sqrt(2). Below the critical
+ * density or at p_tr <= 0 the stress is zero; inside the cone tau_tr <=
+ * mu_s p_tr it is the trial stress; otherwise tau is the smaller root of
+ * tau^2 - (S2 + tau_tr + alpha) tau + S2 tau_tr + S0 alpha and T = (tau /
+ * tau_tr) t0 - p_tr I. gammap += nup dt, gammap_dot = nup with nup the
+ * plastic shear rate. Tensor operations in the element order of
+ * mpm_tensor.hpp (trace 564-567, norm 570-576). */
+static void update_stress_sand(oc_job* J, oc_body* B) {
+  const double dt = J->dt;
+  const double c = 0;
+  static const double I[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+  for (int p = 0; p < B->n; p++) {
+    if (B->active[p] == 0) continue;
+    const double* L = B->L + 9 * (size_t)p;
+    double* T = B->T + 9 * (size_t)p;
+    double Lt[9], D[9], W[9];
+    for (int a = 0; a < 3; a++)
+      for (int k = 0; k < 3; k++) Lt[3 * a + k] = L[3 * k + a];
+    for (int k = 0; k < 9; k++) D[k] = 0.5 * (L[k] + Lt[k]);
+    for (int k = 0; k < 9; k++) W[k] = 0.5 * (L[k] - Lt[k]);
+    const double trD = D[0] + D[4] + D[8];
+    double WT[9], TW[9], tmp[9], s_tr[9], t0[9];
+    for (int a = 0; a < 3; a++)
+      for (int k = 0; k < 3; k++) {
+        WT[3 * a + k] = W[3 * a + 0] * T[0 + k] + W[3 * a + 1] * T[3 + k] + W[3 * a + 2] * T[6 + k];
+        TW[3 * a + k] = T[3 * a + 0] * W[0 + k] + T[3 * a + 1] * W[3 + k] + T[3 * a + 2] * W[6 + k];
+      }
+    const double twoG = 2 * B->G;
+    const double ltr = B->lambda * trD;
+    for (int k = 0; k < 9; k++) tmp[k] = ((twoG * D[k] + ltr * I[k]) + WT[k]) - TW[k];
+    for (int k = 0; k < 9; k++) s_tr[k] = T[k] + dt * tmp[k];
+    double p_tr = -(s_tr[0] + s_tr[4] + s_tr[8]) / 3.0;
+    for (int k = 0; k < 9; k++) t0[k] = s_tr[k] + p_tr * I[k];
+    double nn = 0;
+    for (int k = 0; k < 9; k++) nn += t0[k] * t0[k];
+    const double tau_tr = sqrt(nn) / sqrt(2.0);
+    if (B->use_density) p_tr = B->K * ((B->m[p] / B->v[p] - B->rho_critical) / B->rho_critical);
+    const int density_flag = (B->m[p] / B->v[p]) < B->rho_critical;
+    double nup_tau;
+    if (density_flag || p_tr <= c) {
+      nup_tau = tau_tr / (B->G * dt);
+      for (int k = 0; k < 9; k++) T[k] = 0.0;
+    } else if (p_tr > c) {
+      const double S0 = B->mu_s * p_tr;
+      double tau_tau, scale_factor;
+      if (tau_tr <= S0) {
+        tau_tau = tau_tr;
+        scale_factor = 1.0;
+      } else {
+        const double S2 = B->mu_2 * p_tr;
+        const double alpha = B->G * B->i_0 * dt * sqrt(p_tr / B->grains_rho) / B->grains_d;
+        const double Bq = -(S2 + tau_tr + alpha);
+        const double Hq = S2 * tau_tr + S0 * alpha;
+        tau_tau = sand_negative_root(1.0, Bq, Hq);
+        scale_factor = (tau_tau / tau_tr);
+      }
+      nup_tau = ((tau_tr - tau_tau) / B->G) / dt;
+      for (int k = 0; k < 9; k++) T[k] = scale_factor * t0[k] - p_tr * I[k];
+    } else {
+      nup_tau = 0; /* p_tr is NaN: T stays as it was */
+    }
+    B->gammap[p] += nup_tau * dt;
+    B->gammap_dot[p] = nup_tau;
+  }
+}
+
 static void update_stress(oc_job* J, oc_body* B) {
   if (B->material_kind == 1) {
     update_stress_neohookean(J, B);
+    return;
+  }
+  if (B->material_kind == 2) {
+    update_stress_sand(J, B);
     return;
   }
   double dt = J->dt;
@@ -743,6 +829,8 @@ int oc_add_body(void* hp, int n, const double* m, const double* v, const double*
   B->F = (double*)calloc(9 * (size_t)n, sizeof(double));
   for (int p = 0; p < n; p++) B->F[9 * (size_t)p] = B->F[9 * (size_t)p + 4] = B->F[9 * (size_t)p + 8] = 1.0;
   B->T = (double*)calloc(9 * (size_t)n, sizeof(double));
+  B->gammap = (double*)calloc((size_t)n, sizeof(double));
+  B->gammap_dot = (double*)calloc((size_t)n, sizeof(double));
   B->m = (double*)calloc((size_t)n, sizeof(double));
   B->v = (double*)calloc((size_t)n, sizeof(double));
   B->v0 = (double*)calloc((size_t)n, sizeof(double));
@@ -782,6 +870,27 @@ int oc_add_body(void* hp, int n, const double* m, const double* v, const double*
   J->nbodies++;
   apply_gravity(J); /* DefaultDriver::run applies gravity before its loop */
   return J->nbodies - 1;
+}
+
+/* Sets a Sand_SachithLocal body's properties after E and nu, in the order of
+ * its material-props (sand_sachithlocal.cpp:57-103): grain diameter, mu_s,
+ * grains_rho, rho_critical and, when nprops >= 6, mu_2 and I_0 (otherwise
+ * mu_2 = mu_s and I_0 = 1); use_density: the USE_DENSITY_FOR_PRESSURE
+ * str-property. Returns -1 for a body of another material or too few
+ * properties. */
+int oc_set_sand(void* hp, int b, const double* props, int nprops, int use_density) {
+  oc_job* J = (oc_job*)hp;
+  if (b < 0 || b >= J->nbodies || nprops < 4) return -1;
+  oc_body* B = &J->bodies[b];
+  if (B->material_kind != 2) return -1;
+  B->grains_d = props[0];
+  B->mu_s = props[1];
+  B->grains_rho = props[2];
+  B->rho_critical = props[3];
+  B->mu_2 = nprops >= 6 ? props[4] : B->mu_s;
+  B->i_0 = nprops >= 6 ? props[5] : 1;
+  B->use_density = use_density;
+  return 0;
 }
 
 int oc_add_contact(void* hp, int b1, int b2, double mu_f, int reflected) {
@@ -860,6 +969,8 @@ int oc_get_point_field(void* hp, int b, const char* name, double* out) {
   if (!strcmp(name, "v")) return memcpy(out, B->v, 8 * n), 1;
   if (!strcmp(name, "v0")) return memcpy(out, B->v0, 8 * n), 1;
   if (!strcmp(name, "extent")) return memcpy(out, B->extent, 8 * n), 1;
+  if (B->material_kind == 2 && !strcmp(name, "gammap")) return memcpy(out, B->gammap, 8 * n), 1;
+  if (B->material_kind == 2 && !strcmp(name, "gammap_dot")) return memcpy(out, B->gammap_dot, 8 * n), 1;
   if (!strcmp(name, "active")) {
     for (size_t p = 0; p < n; p++) out[p] = B->active[p];
     return 1;
@@ -913,7 +1024,7 @@ void oc_destroy(void* hp) {
   for (int b = 0; b < J->nbodies; b++) {
     oc_body* B = &J->bodies[b];
     free(B->x); free(B->u); free(B->x_t); free(B->mx_t); free(B->b);
-    free(B->L); free(B->F); free(B->T); free(B->m); free(B->v); free(B->v0);
+    free(B->L); free(B->F); free(B->T); free(B->gammap); free(B->gammap_dot); free(B->m); free(B->v); free(B->v0);
     free(B->extent); free(B->active); free(B->nx); free(B->nu); free(B->nx_t);
     free(B->nmx_t); free(B->nf); free(B->ndiff); free(B->nm); free(B->bc_mask); free(B->bc_force);
     free(B->S_i); free(B->S_j); free(B->S_v); free(B->G_i); free(B->G_j); free(B->G_v);

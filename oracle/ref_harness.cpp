@@ -180,6 +180,7 @@ template <>
 Registry<Material>::Registry() {
   object["IsotropicLinearElasticity"] = &make<Material, IsotropicLinearElasticity>;
   object["CompressibleNeohookeanElasticity"] = &make<Material, CompressibleNeohookeanElasticity>;
+  object["Sand_SachithLocal"] = &make<Material, Sand_SachithLocal>;
 }
 template <>
 Registry<Boundary>::Registry() {
@@ -276,7 +277,8 @@ int ref_num_points(void* hp, int b) { return static_cast<RefHandle*>(hp)->job.bo
 int ref_num_nodes(void* hp, int b) { return static_cast<RefHandle*>(hp)->job.bodies[b]->nodes->x.size(); }
 
 // Point fields: x, u, x_t, mx_t, b (3 per point); L, T (9 per point);
-// m, v, v0, extent, active (1 per point). Returns the number of doubles per
+// m, v, v0, extent, active, and gammap, gammap_dot of a Sand_SachithLocal
+// body (1 per point). Returns the number of doubles per
 // point, or -1 for an unknown name.
 int ref_get_point_field(void* hp, int b, const char* name, double* out) {
   RefHandle* h = static_cast<RefHandle*>(hp);
@@ -300,6 +302,14 @@ int ref_get_point_field(void* hp, int b, const char* name, double* out) {
     DefaultPoints* dp = dynamic_cast<DefaultPoints*>(p);
     if (dp == nullptr) return -1;
     copy_scalar(dp->extent, out);
+    return 1;
+  }
+  if (n == "gammap" || n == "gammap_dot") {
+    // Sand_SachithLocal's per-point plastic shear strain and its rate
+    // (the material's frame fields, sand_sachithlocal.cpp:118-122)
+    Sand_SachithLocal* sand = dynamic_cast<Sand_SachithLocal*>(h->job.bodies[b]->material.get());
+    if (sand == nullptr) return -1;
+    copy_scalar(n == "gammap" ? sand->gammap : sand->gammap_dot, out);
     return 1;
   }
   return -1;

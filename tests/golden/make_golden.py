@@ -54,7 +54,17 @@ def golden_cases():
         "sliding_3d_smooth": (inputs.sliding_block(3, "CartesianSmoothBox", mu=0.3, n_cells=8, steps=15), [15]),
         "wall_collision_2d_reflected": (inputs.wall_collision(2, n_cells=16, steps=15), [1, 15]),
         "collision_2d_neohookean": (neohookean, [1, 40]),
+        "sand_column_2d": (inputs.sand_column(2, steps=60), [1, 20, 60]),
+        "sand_column_2d_mu2_density": (inputs.sand_column(2, steps=12, density_pressure=True, mu_2=0.8), [12]),
     }
+
+
+def point_fields(body) -> list:
+    """The point fields a body's fixtures hold: the material's frame fields
+    beside the points' own."""
+    if body.material and body.material_class == "Sand_SachithLocal":
+        return POINT_FIELDS + ["gammap", "gammap_dot"]
+    return POINT_FIELDS
 
 
 def run(name, case, snaps):
@@ -76,7 +86,7 @@ def run(name, case, snaps):
         ref.step(s - done)
         done = s
         for b in range(len(case.bodies)):
-            for f in POINT_FIELDS:
+            for f in point_fields(case.bodies[b]):
                 out[f"s{s}_b{b}_p_{f}"] = ref.points(b, f)
             for f in NODE_FIELDS:
                 out[f"s{s}_b{b}_n_{f}"] = ref.nodes(b, f)

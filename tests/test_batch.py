@@ -176,3 +176,11 @@ def test_mixed_neohookean_and_boundaries_within_1e4_of_fp64():
     slide = inputs.sliding_block(3, "CartesianFrictionalBox", mu=0.3, n_cells=12, steps=20)
     for c in (coll, slide):
         _compare(c, _solo(c, c.steps, mode="mixed"), _solo(c, c.steps), MIXED_TOL, f"mixed {c.name}")
+
+
+def test_mixed_sand_within_1e4_of_fp64():
+    """Sand_SachithLocal in the mixed form (FP32 point state, stress and
+    plastic strain; FP64 nodal sums) against FP64: the 2D and 3D granular
+    columns, with their elastic, plastic-return and zero-stress points."""
+    for c in (inputs.sand_column(2, steps=80), inputs.sand_column(3, n_cells=12, steps=30)):
+        _compare(c, _solo(c, c.steps, mode="mixed"), _solo(c, c.steps), MIXED_TOL, f"mixed {c.name}")

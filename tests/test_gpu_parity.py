@@ -111,7 +111,19 @@ CASES = {
     "column_collapse_s16": (lambda: inputs.column_collapse_3d(scale=16, steps=15), 15),
     "collision_3d_zero_gravity": (lambda: inputs.two_body_collision_3d(16, steps=8, gap=0.01, gravity=(0.0, 0.0, 0.0)),
                                   8),
+    # Sand_SachithLocal: elastic, plastic-return and zero-stress points from
+    # the first tens of steps; with the pressure from the density the column
+    # dilates below the critical density from the 8th step on, where the
+    # stress switches off discontinuously, so that case stops before it
+    "sand_column_2d": (lambda: inputs.sand_column(2, steps=80), 80),
+    "sand_column_3d": (lambda: inputs.sand_column(3, n_cells=12, steps=30), 30),
+    "sand_column_2d_mu2_density": (lambda: inputs.sand_column(2, steps=6, density_pressure=True, mu_2=0.8), 6),
 }
+
+
+def _point_fields(body):
+    extra = ["gammap", "gammap_dot"] if body.material and body.material_class == "Sand_SachithLocal" else []
+    return POINT_FIELDS + extra
 
 
 @pytest.fixture(scope="module", autouse=True)
@@ -129,7 +141,7 @@ def _step_parity(name, sort_interval=0, mode="fp64"):
         ref.step(1)
         gpu.step(1)
         for b in range(len(case.bodies)):
-            for f in POINT_FIELDS:
+            for f in _point_fields(case.bodies[b]):
                 e = assert_close(gpu.points(b, f), ref.points(b, f), FP64_TOL, f"{name} step {s} body {b} point {f}",
                                  field_floor(case, f))
                 worst[f] = max(worst.get(f, 0.0), e)

@@ -12,7 +12,7 @@ import numpy as np
 import pytest
 
 import bridge
-from golden.make_golden import NODE_FIELDS, POINT_FIELDS, golden_cases
+from golden.make_golden import NODE_FIELDS, POINT_FIELDS, golden_cases, point_fields
 from mpm_3d_b200 import inputs
 from util import bits_equal
 
@@ -43,7 +43,7 @@ def test_restated_matches_golden(name):
         job.step(s - done)
         done = s
         for b in range(len(case.bodies)):
-            for f in POINT_FIELDS:
+            for f in point_fields(case.bodies[b]):
                 assert bits_equal(job.points(b, f), gold[f"s{s}_b{b}_p_{f}"]), f"{name} step {s} point {f}"
             for f in NODE_FIELDS:
                 assert bits_equal(job.nodes(b, f), gold[f"s{s}_b{b}_n_{f}"]), f"{name} step {s} node {f}"
@@ -175,3 +175,26 @@ def test_restated_matches_reference_neohookean(make):
         for b in range(len(case.bodies)):
             for f in POINT_FIELDS:
                 assert bits_equal(job.points(b, f), ref.points(b, f)), f"step {s} body {b} point {f}"
+
+
+@needs_ref
+@pytest.mark.parametrize("make,steps", [(lambda: inputs.sand_column(2, steps=300), 300),
+                                        (lambda: inputs.sand_column(2, steps=40, density_pressure=True, mu_2=0.8), 40),
+                                        (lambda: inputs.sand_column(3, n_cells=12, steps=40), 40)],
+                         ids=["column_2d", "column_2d_mu2_density", "column_3d"])
+def test_restated_matches_reference_sand(make, steps):
+    """Sand_SachithLocal (trial stress, local mu(I) return, zero stress below
+    the critical density or in tension, gammap): restatement == reference
+    every step. The density-pressure column dilates through the critical
+    density (its stress switches off) within these steps."""
+    case = make()
+    d = tempfile.mkdtemp()
+    ref = bridge.ReferenceJob(inputs.write_case(case, d))
+    job = bridge.RestatedJob(case)
+    for s in range(steps):
+        ref.step(1)
+        job.step(1)
+        for f in POINT_FIELDS + ["gammap", "gammap_dot"]:
+            assert bits_equal(job.points(0, f), ref.points(0, f)), f"step {s} point {f}"
+        for f in NODE_FIELDS:
+            assert bits_equal(job.nodes(0, f), ref.nodes(0, f)), f"step {s} node {f}"

@@ -28,6 +28,9 @@ def test_plugin_configures_from_a_reference_config():
     cfg = inputs.write_case(case, tempfile.mkdtemp(), solver_class="GPUExplicitUSL")
     job = bridge.ReferenceJob(cfg, build="gpu")
     assert job.nbodies == 1 and job.n_points(0) == 144
+    sand = inputs.sand_column(2, steps=5, density_pressure=True, mu_2=0.8)
+    job = bridge.ReferenceJob(inputs.write_case(sand, tempfile.mkdtemp(), solver_class="GPUExplicitUSL"), build="gpu")
+    assert job.points(0, "gammap").shape == (sand.bodies[0].n, 1)
 
 
 def _neohookean(case):
@@ -46,7 +49,13 @@ CASES = {
     "sliding_3d_smooth_box": (lambda: inputs.sliding_block(3, "CartesianSmoothBox", n_cells=12, steps=10), 10),
     "wall_collision_2d_reflected": (lambda: inputs.wall_collision(2, n_cells=16, steps=20), 20),
     "collision_3d_neohookean": (lambda: _neohookean(inputs.two_body_collision_3d(16, steps=8, gap=0.01)), 8),
+    "sand_column_2d": (lambda: inputs.sand_column(2, steps=30), 30),
 }
+
+
+def _material_fields(body):
+    # Sand_SachithLocal's frame fields, which the plugin writes back into the material
+    return ("gammap", "gammap_dot") if body.material_class == "Sand_SachithLocal" else ()
 
 
 @needs_gpu_harness
@@ -61,7 +70,7 @@ def test_dropin_matches_reference_solver(name):
         ref.step(1)
         gpu.step(1)
         for b in range(len(case.bodies)):
-            for f in ("x", "u", "x_t", "mx_t", "T", "L", "v", "active", "b"):
+            for f in ("x", "u", "x_t", "mx_t", "T", "L", "v", "active", "b") + _material_fields(case.bodies[b]):
                 assert_close(gpu.points(b, f), ref.points(b, f), FP64_TOL, f"{name} step {s} point {f}",
                              field_floor(case, f))
             for f in ("m", "mx_t", "f", "x_t", "u", "diff_x_t"):

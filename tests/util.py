@@ -50,8 +50,10 @@ def field_floor(case, field: str) -> float:
     """Physical scale of a field for ``rel_err``: the velocity scale is the
     largest initial speed (at least 1 m/s); the velocity-gradient scale is
     that speed over a cell; the stress scale is one step of elastic stress
-    at that gradient (E * dt * v / h)."""
+    at that gradient (E * dt * v / h); a plastic shear rate (gammap_dot)
+    has the gradient's scale and a plastic strain (gammap) one step of it."""
     v0 = max(1.0, max(float(np.abs(b.x_t).max()) for b in case.bodies))
     h = min(case.h)
     E = max(b.E for b in case.bodies)
-    return {"L": v0 / h, "T": E * case.dt * v0 / h, "x_t": v0, "u": h, "x": min(case.L)}.get(field, 0.0)
+    return {"L": v0 / h, "T": E * case.dt * v0 / h, "x_t": v0, "u": h, "x": min(case.L), "gammap_dot": v0 / h,
+            "gammap": case.dt * v0 / h}.get(field, 0.0)
