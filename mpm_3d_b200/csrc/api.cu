@@ -305,10 +305,8 @@ mpmgpu_status mpmgpu_batch_create(const mpmgpu_batch_config* cfg, mpmgpu_batch**
 
 mpmgpu_status mpmgpu_batch_footprint(const mpmgpu_batch* b, const mpmgpu_job_desc* job, int64_t* bytes) {
   if (!b || !job || !job->grid || !bytes || job->nbodies < 0 || job->nbodies > kMaxBodies) return MPMGPU_ERR_ARG;
-  std::vector<int64_t> n((size_t)job->nbodies);
-  for (int i = 0; i < job->nbodies; i++) n[(size_t)i] = job->bodies[i].n;
-  *bytes = job_footprint(*job->grid, b->cfg.mode == MPMGPU_MODE_MIXED, b->cfg.keep_debug != 0, job->nbodies,
-                         n.data(), job->ncontacts);
+  if (job->nbodies > 0 && !job->bodies) return MPMGPU_ERR_ARG;
+  *bytes = job_footprint(*job->grid, b->cfg.mode, b->cfg.keep_debug != 0, job->bodies, job->nbodies, job->ncontacts);
   return MPMGPU_OK;
 }
 

@@ -136,21 +136,26 @@ inline bool cap_available(int dim, bool mixed, int cap) {
   return cap == 512;
 }
 
-// Device bytes a job will hold: points (two buffers), nodal arrays, binning
-// and its share of the batch's scratch.
-inline int64_t job_footprint(const mpmgpu_config& cfg, bool mixed, bool keep_debug, int nbodies, const int64_t* npts,
-                             int ncontacts) {
+// Device bytes a job will hold: points (two buffers, with the material's
+// per-point state), nodal arrays (with the deterministic form's second
+// level), binning and its share of the batch's scratch.
+inline int64_t job_footprint(const mpmgpu_config& cfg, int mode, bool keep_debug, const mpmgpu_body_desc* bodies,
+                             int nbodies, int ncontacts) {
   Geom g;
   MapConst mc;
   BinGeom bg;
   make_geometry(cfg, g, mc, bg);
+  const bool mixed = mode == MPMGPU_MODE_MIXED;
   const int64_t ps = mixed ? 4 : 8;
   int64_t bytes = 0;
   for (int b = 0; b < nbodies; b++) {
-    const int64_t n = npts[b] + 8;
-    bytes += 2 * n * (18 * ps + 8) + 64 * 256;  // two point buffers (+ alignment of the arrays)
+    const int64_t n = bodies[b].n + 8;
+    const int nstate = material_state_arrays(bodies[b].has_material, bodies[b].material_kind);
+    // two point buffers (+ the 256-byte alignment of every array)
+    bytes += 2 * n * ((18 + nstate) * ps + 8) + 96 * 256;
     if (keep_debug && !mixed) bytes += 2 * n * 72;
     bytes += g.nslots * 8 * (7 + 6);            // accumulators + velocities
+    if (mode == MPMGPU_MODE_FP64_DETERMINISTIC) bytes += g.nslots * 8 * 7;
     bytes += n * 10;                             // sort key, rank, class rank
     bytes += ((int64_t)bg.nbins * bg.cells_per_bin + 1) * 12 + ((int64_t)bg.nbins + 2) * 4;
     bytes += ((int64_t)bg.nbins + n / 256 + 1) * 16;

@@ -62,17 +62,17 @@ class Server {
     return s;
   }
 
+  int mode() const { return mixed_ ? MPMGPU_MODE_MIXED : MPMGPU_MODE_FP64; }
+
   double clock() const {
     return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0_).count();
   }
 
   mpmgpu_status footprint(const mpmgpu_job_desc& d, int64_t* bytes) const {
     if (!d.grid || d.nbodies < 1 || !d.bodies || d.nbodies > kMaxBodies) return MPMGPU_ERR_ARG;
-    std::vector<int64_t> n((size_t)d.nbodies);
-    for (int b = 0; b < d.nbodies; b++) n[(size_t)b] = d.bodies[b].n;
     mpmgpu_config cfg = *d.grid;
     cfg.dim = batch_->dim();
-    *bytes = job_footprint(cfg, mixed_, keep_debug_, d.nbodies, n.data(), d.ncontacts);
+    *bytes = job_footprint(cfg, mode(), keep_debug_, d.bodies, d.nbodies, d.ncontacts);
     return MPMGPU_OK;
   }
 
@@ -83,12 +83,11 @@ class Server {
     if (!d.grid || d.nbodies < 1 || !d.bodies || d.nbodies > kMaxBodies || d.ncontacts < 0 ||
         (d.ncontacts > 0 && !d.contacts))
       return fail(MPMGPU_ERR_ARG, "invalid job description");
-    std::vector<int64_t> n((size_t)d.nbodies);
     int64_t pts = 0;
-    for (int b = 0; b < d.nbodies; b++) pts += (n[(size_t)b] = d.bodies[b].n);
+    for (int b = 0; b < d.nbodies; b++) pts += d.bodies[b].n;
     mpmgpu_config cfg = *d.grid;
     cfg.dim = batch_->dim();
-    const int64_t fp = job_footprint(cfg, mixed_, keep_debug_, d.nbodies, n.data(), d.ncontacts);
+    const int64_t fp = job_footprint(cfg, mode(), keep_debug_, d.bodies, d.nbodies, d.ncontacts);
     if (running_ > 0 && reserved_ + fp > budget_) return fail(MPMGPU_ERR_STATE, "request does not fit the memory budget now");
     int job = -1;
     mpmgpu_status st = batch_->new_job(cfg, d.steps, &job);
