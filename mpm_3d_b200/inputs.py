@@ -429,10 +429,12 @@ def read_points_file(path: str, dim: int) -> Tuple[np.ndarray, ...]:
 
 
 def write_case(case: Case, directory: str, solver_class: str = "ExplicitUSL", points_class: str = "DefaultPoints",
-               threads: Optional[int] = None, solver_extra: Sequence[int] = ()) -> str:
+               threads: Optional[int] = None, solver_extra: Sequence[int] = (),
+               point_int_props: Sequence[int] = ()) -> str:
     """Writes ``<name>.cfg`` and the ``.points`` files; returns the cfg path.
     ``solver_extra`` appends solver int-properties (the GPU solver's
-    write-back interval and form)."""
+    write-back interval and form); ``point_int_props`` are DefaultPoints'
+    int-properties ({1}: the point-element history, use_elem)."""
     os.makedirs(directory, exist_ok=True)
     lines = ["job", "{", f"    dt = {_fmt(case.dt)}", "    t = 0", f"    TYPE = {case.dim}"]
     if threads is not None:
@@ -456,6 +458,8 @@ def write_case(case: Case, directory: str, solver_class: str = "ExplicitUSL", po
         write_points_file(body, os.path.join(directory, pfile), case.dim)
         lines += ["body", "{", '    class = "DefaultBody"', f'    name = "{body.name}"', f'    point-file = "{pfile}"',
                   f'    point-class = "{points_class}"', '    node-class = "DefaultNodes"']
+        if point_int_props:
+            lines += ["    point-int-props = {" + ",".join(str(v) for v in point_int_props) + "}"]
         if body.material:
             props = ",".join(_fmt(v) for v in (body.E, body.nu, *body.material_props))
             lines += [f'    material-class = "{body.material_class}"', f"    material-props = {{{props}}}"]

@@ -198,3 +198,29 @@ def test_restated_matches_reference_sand(make, steps):
             assert bits_equal(job.points(0, f), ref.points(0, f)), f"step {s} point {f}"
         for f in NODE_FIELDS:
             assert bits_equal(job.nodes(0, f), ref.nodes(0, f)), f"step {s} node {f}"
+
+
+def _cpdi_off(case):
+    case.cpdi = 0
+    case.name += "_cpdi_off"
+    return case
+
+
+@needs_ref
+@pytest.mark.parametrize("make", [inputs.block_drop_2d, lambda: _cpdi_off(inputs.block_drop_2d()),
+                                  lambda: inputs.two_body_collision_3d(8, steps=12, gap=0.02)],
+                         ids=["block_drop_2d", "block_drop_2d_cpdi_off", "collision_3d"])
+def test_point_element_history_changes_nothing(make):
+    """DefaultPoints with use_elem (point-int-props {1}, default_points.cpp:86-95)
+    passes an element hint to the grid, which CartesianLinear ignores (the
+    Grid defaults fall back to the plain lookups, mpm_objects.hpp:263-274):
+    the reference with the option on equals the restatement bit for bit."""
+    case = make()
+    ref = bridge.ReferenceJob(inputs.write_case(case, tempfile.mkdtemp(), point_int_props=(1,)))
+    job = bridge.RestatedJob(case)
+    for s in range(12):
+        ref.step(1)
+        job.step(1)
+        for b in range(len(case.bodies)):
+            for f in POINT_FIELDS:
+                assert bits_equal(job.points(b, f), ref.points(b, f)), f"step {s} body {b} point {f}"

@@ -28,6 +28,8 @@ def test_plugin_configures_from_a_reference_config():
     cfg = inputs.write_case(case, tempfile.mkdtemp(), solver_class="GPUExplicitUSL")
     job = bridge.ReferenceJob(cfg, build="gpu")
     assert job.nbodies == 1 and job.n_points(0) == 144
+    cfg = inputs.write_case(case, tempfile.mkdtemp(), solver_class="GPUExplicitUSL", point_int_props=(1,))
+    assert bridge.ReferenceJob(cfg, build="gpu").n_points(0) == 144
     sand = inputs.sand_column(2, steps=5, density_pressure=True, mu_2=0.8)
     job = bridge.ReferenceJob(inputs.write_case(sand, tempfile.mkdtemp(), solver_class="GPUExplicitUSL"), build="gpu")
     assert job.points(0, "gammap").shape == (sand.bodies[0].n, 1)
