@@ -1,0 +1,342 @@
+// AsyncVTK: DefaultVTK's frames written by a background thread (see
+// async_vtk.hpp).
+#include "async_vtk.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <iomanip>
+#include <iostream>
+#include <sstream>
+
+#include "job.hpp"
+#include "mpm_tensorarray.hpp"
+#include "mpm_vectorarray.hpp"
+#include "parser.hpp"
+
+AsyncVTK::~AsyncVTK() {
+  {
+    std::lock_guard<std::mutex> lock(mu_);
+    stop_ = true;
+  }
+  cv_.notify_all();
+  if (writer_.joinable()) writer_.join();
+}
+
+// DefaultVTK::init (default_vtk.cpp:25-50): the same properties, the same
+// exit(0) on missing ones; int-properties[0] sets maxPending.
+void AsyncVTK::init(Job* job) {
+  if (str_props.size() < 3 || fp64_props.size() < 1) {
+    std::cout << str_props.size() << "\n";
+    fprintf(stderr, "%s:%s: Need at least 4 properties defined ({sampleRate}, {frameDirectory, outputDirectory, outputName}).\n",
+            __FILE__, __func__);
+    exit(0);
+  }
+  frameDirectory = Parser::makeDirectory(str_props[0]);
+  outputDirectory = Parser::makeDirectory(str_props[1]);
+  outputName = str_props[2];
+  sampleRate = fp64_props[0];
+  sampledFrames = 0;
+  if (!int_props.empty() && int_props[0] > 0) maxPending = int_props[0];
+  printf("Serializer properties (frameDirectory = %s, outputDirectory = %s, outputName = %s, sampleRate = %g, "
+         "maxPending = %d).\n",
+         frameDirectory.c_str(), outputDirectory.c_str(), outputName.c_str(), sampleRate, maxPending);
+  if (!writer_.joinable()) writer_ = std::thread(&AsyncVTK::writerLoop, this);
+  std::cout << "Serializer Initialized." << std::endl;
+}
+
+std::string AsyncVTK::saveState(Job* job) {
+  std::cerr << "NOT IMPLEMENTED! Oops." << std::endl;
+  return "error";
+}
+
+int AsyncVTK::loadState(Job* job, std::string fullpath) {
+  std::cerr << "NOT IMPLEMENTED! Oops." << std::endl;
+  return 0;
+}
+
+namespace {
+
+std::string frame_file(const char* prefix, const Body* body, int frame) {
+  std::stringstream ss;
+  ss << prefix << "." << body->id << "." << body->name << "." << std::setw(10) << std::setfill('0') << frame << ".vtk";
+  return ss.str();
+}
+
+std::vector<int> active_flags(const Eigen::VectorXi& a) {
+  std::vector<int> out((size_t)a.rows());
+  for (int i = 0; i < (int)a.rows(); i++) out[(size_t)i] = a(i);
+  return out;
+}
+
+}  // namespace
+
+// DefaultVTK::writeFrame (default_vtk.cpp:120-200): the frame condition, the
+// two files per body, the title lines (the node file's carries the frame
+// count, the point file's the frame index) and the order in which the
+// objects write. The objects' arrays are captured here and formatted by the
+// writer thread.
+int AsyncVTK::writeFrame(Job* job) {
+  if (!((job->t - job->t0) >= (sampledFrames / sampleRate) || sampledFrames == 0)) return 0;
+  sampledFrames += 1;
+  const int index = sampledFrames - 1;
+  std::vector<std::unique_ptr<Frame>> frame;
+  for (size_t b = 0; b < job->bodies.size(); b++) {
+    Body* body = job->bodies[b].get();
+    std::unique_ptr<Frame> f(new Frame());
+    const std::string pname = frameDirectory + frame_file("fpd", body, index);
+    const std::string nname = frameDirectory + frame_file("fnd", body, index);
+    f->pfile.open(pname, std::ios::trunc);
+    f->nfile.open(nname, std::ios::trunc);
+    f->plen = body->points->x.size();
+    f->nlen = body->nodes->x.size();
+    f->pactive = active_flags(body->points->active);
+    f->nactive = active_flags(body->nodes->active);
+    current_ = f.get();
+    if (f->pfile.is_open()) {
+      f->pfile << "# vtk DataFile Version 3.0\n";
+      f->pfile << "Frame: " << index << ", Time: " << job->t << "\n";
+      body->points->writeHeader(job, body, this, f->pfile, VTK);
+    } else {
+      std::cerr << "Could not open point frame: " << pname << " !" << std::endl;
+    }
+    if (f->nfile.is_open()) {
+      f->nfile << "# vtk DataFile Version 3.0\n";
+      f->nfile << "Frame: " << sampledFrames << ", Time: " << job->t << "\n";
+      job->grid->writeHeader(job, body, this, f->nfile, VTK);
+    } else {
+      std::cerr << "Could not open node frame: " << nname << " !" << std::endl;
+    }
+    if (job->activeBodies[b] != 0) {
+      body->points->writeFrame(job, body, this);
+      body->nodes->writeFrame(job, body, this);
+      if (body->activeMaterial != 0) body->material->writeFrame(job, body, this);
+      if (body->activeBoundary != 0) body->boundary->writeFrame(job, body, this);
+      job->grid->writeFrame(job, this);
+    }
+    for (size_t c = 0; c < job->contacts.size(); c++) job->contacts[c]->writeFrame(job, this);
+    current_ = nullptr;
+    frame.push_back(std::move(f));
+  }
+  std::unique_lock<std::mutex> lock(mu_);
+  cv_.wait(lock, [&] { return (int)queue_.size() + busy_ < std::max(maxPending, 1); });
+  queue_.push_back(std::move(frame));
+  lock.unlock();
+  cv_.notify_all();
+  return 1;
+}
+
+void AsyncVTK::flush() {
+  std::unique_lock<std::mutex> lock(mu_);
+  cv_.wait(lock, [&] { return queue_.empty() && busy_ == 0; });
+}
+
+// ---- capture (writeFrame's thread) ----
+
+void AsyncVTK::writeDefaultPointHeader(Job* job, Body* body, std::ofstream& pfile, int SPEC) {
+  if (!current_) return;
+  Block blk;
+  blk.kind = Block::kPointHeader;
+  blk.dim = body->points->x.DIM;
+  blk.count = body->points->x.size();
+  blk.values.assign(3 * (size_t)blk.count, 0.0);
+  for (int i = 0; i < blk.count; i++)
+    for (int pos = 0; pos < blk.dim && pos < 3; pos++) blk.values[3 * (size_t)i + pos] = body->points->x(i, pos);
+  current_->blocks.push_back(std::move(blk));
+}
+
+void AsyncVTK::writeDefaultNodeHeader(Job* job, Body* body, std::ofstream& nfile, int SPEC) {
+  if (!current_) return;
+  Block blk;
+  blk.kind = Block::kNodeHeader;
+  blk.dim = body->nodes->x.DIM;
+  blk.count = body->nodes->x.size();
+  blk.values.assign(3 * (size_t)blk.count, 0.0);
+  for (int i = 0; i < blk.count; i++)
+    for (int pos = 0; pos < blk.dim && pos < 3; pos++) blk.values[3 * (size_t)i + pos] = body->nodes->x(i, pos);
+  current_->blocks.push_back(std::move(blk));
+}
+
+void AsyncVTK::writeScalarArray(Eigen::VectorXd& scalarArray, std::string name) {
+  if (!current_) return;
+  Block blk;
+  blk.kind = Block::kScalar;
+  blk.name = name;
+  blk.count = (int)scalarArray.rows();
+  blk.values.resize((size_t)blk.count);
+  for (int i = 0; i < blk.count; i++) blk.values[(size_t)i] = scalarArray(i);
+  current_->blocks.push_back(std::move(blk));
+}
+
+void AsyncVTK::writeVectorArray(MPMVectorArray& vectorArray, std::string name) {
+  if (!current_) return;
+  Block blk;
+  blk.kind = Block::kVector;
+  blk.name = name;
+  blk.count = vectorArray.size();
+  blk.values.resize(3 * (size_t)blk.count);
+  for (int i = 0; i < blk.count; i++)
+    for (int pos = 0; pos < 3; pos++) blk.values[3 * (size_t)i + pos] = vectorArray(i, pos);
+  current_->blocks.push_back(std::move(blk));
+}
+
+void AsyncVTK::writeTensorArray(MPMTensorArray& tensorArray, std::string name) {
+  if (!current_) return;
+  Block blk;
+  blk.kind = Block::kTensor;
+  blk.name = name;
+  blk.count = tensorArray.size();
+  blk.values.resize(9 * (size_t)blk.count);
+  for (int i = 0; i < blk.count; i++)
+    for (int pos = 0; pos < 9; pos++) blk.values[9 * (size_t)i + pos] = tensorArray(i, pos);
+  current_->blocks.push_back(std::move(blk));
+}
+
+// ---- formatting (writer thread) ----
+
+void AsyncVTK::writerLoop() {
+  for (;;) {
+    std::vector<std::unique_ptr<Frame>> frame;
+    {
+      std::unique_lock<std::mutex> lock(mu_);
+      cv_.wait(lock, [&] { return stop_ || !queue_.empty(); });
+      if (queue_.empty()) return;
+      frame = std::move(queue_.front());
+      queue_.pop_front();
+      busy_++;
+    }
+    for (auto& f : frame) format(*f);
+    frame.clear();
+    {
+      std::lock_guard<std::mutex> lock(mu_);
+      busy_--;
+    }
+    cv_.notify_all();
+  }
+}
+
+namespace {
+
+// The rules of DefaultVTK's writers (default_vtk.cpp): the header writes a
+// position component when the axis exists, the entry is active (!= 0) and
+// the value finite; scalar and vector arrays write a value when the entry's
+// flag is exactly 1 and the value finite; a point tensor is written when the
+// point is active and all 9 components are finite, a node tensor (written
+// three times per node, as the reference does) when its components are
+// finite. Everything else is written as 0. Numbers use the stream's default
+// formatting.
+void header(std::ofstream& out, const AsyncVTK::Block& blk, const std::vector<int>& active) {
+  const int n = blk.count;
+  out << "ASCII\n";
+  out << "DATASET UNSTRUCTURED_GRID\n";
+  out << "POINTS " << n << " double\n";
+  for (int i = 0; i < n; i++) {
+    for (int pos = 0; pos < 3; pos++) {
+      const double v = blk.values[3 * (size_t)i + pos];
+      if (pos < blk.dim && active[(size_t)i] != 0 && std::isfinite(v))
+        out << v << " ";
+      else
+        out << "0 ";
+    }
+    out << "\n";
+  }
+  out << "CELLS " << n << " " << 2 * n << "\n";
+  for (int i = 0; i < n; i++) out << "1 " << i << "\n";
+  out << "CELL_TYPES " << n << "\n";
+  for (int i = 0; i < n; i++) out << "1\n";
+  out << "POINT_DATA " << n << "\n";
+}
+
+void scalars(std::ofstream& out, const AsyncVTK::Block& blk, const std::vector<int>& active) {
+  out << "SCALARS " << blk.name << " double 1\n";
+  out << "LOOKUP_TABLE default\n";
+  for (int i = 0; i < blk.count; i++) {
+    const double v = blk.values[(size_t)i];
+    if (active[(size_t)i] == 1 && std::isfinite(v))
+      out << v << "\n";
+    else
+      out << "0" << "\n";
+  }
+}
+
+void vectors(std::ofstream& out, const AsyncVTK::Block& blk, const std::vector<int>& active) {
+  out << "VECTORS " << blk.name << " double\n";
+  for (int i = 0; i < blk.count; i++) {
+    for (int pos = 0; pos < 3; pos++) {
+      const double v = blk.values[3 * (size_t)i + pos];
+      if (active[(size_t)i] == 1 && std::isfinite(v))
+        out << v << " ";
+      else
+        out << "0 ";
+    }
+    out << "\n";
+  }
+}
+
+void tensor_rows(std::ofstream& out, const double* t, bool write) {
+  if (!write) {
+    out << "0 0 0\n";
+    out << "0 0 0\n";
+    out << "0 0 0\n";
+    out << "\n";
+    return;
+  }
+  out << t[0] << " " << t[1] << " " << t[2] << "\n";
+  out << t[3] << " " << t[4] << " " << t[5] << "\n";
+  out << t[6] << " " << t[7] << " " << t[8] << "\n";
+  out << "\n";
+}
+
+bool all_finite(const double* t) {
+  for (int k = 0; k < 9; k++)
+    if (!std::isfinite(t[k])) return false;
+  return true;
+}
+
+void point_tensors(std::ofstream& out, const AsyncVTK::Block& blk, const std::vector<int>& active) {
+  out << "TENSORS " << blk.name << " double\n";
+  for (int i = 0; i < blk.count; i++) {
+    const double* t = blk.values.data() + 9 * (size_t)i;
+    tensor_rows(out, t, active[(size_t)i] != 0 && all_finite(t));
+  }
+}
+
+void node_tensors(std::ofstream& out, const AsyncVTK::Block& blk) {
+  out << "TENSORS " << blk.name << " double\n";
+  for (int i = 0; i < blk.count; i++) {
+    const double* t = blk.values.data() + 9 * (size_t)i;
+    const bool finite = all_finite(t);
+    for (int rep = 0; rep < 3; rep++) tensor_rows(out, t, finite);
+  }
+}
+
+}  // namespace
+
+void AsyncVTK::format(Frame& f) {
+  const bool p = f.pfile.is_open(), n = f.nfile.is_open();
+  for (const Block& blk : f.blocks) {
+    switch (blk.kind) {
+      case Block::kPointHeader:
+        if (p) header(f.pfile, blk, f.pactive);
+        break;
+      case Block::kNodeHeader:
+        if (n) header(f.nfile, blk, f.nactive);
+        break;
+      case Block::kScalar:
+        if (p && blk.count == f.plen) scalars(f.pfile, blk, f.pactive);
+        if (n && blk.count == f.nlen) scalars(f.nfile, blk, f.nactive);
+        break;
+      case Block::kVector:
+        if (p && blk.count == f.plen) vectors(f.pfile, blk, f.pactive);
+        if (n && blk.count == f.nlen) vectors(f.nfile, blk, f.nactive);
+        break;
+      case Block::kTensor:
+        if (p && blk.count == f.plen) point_tensors(f.pfile, blk, f.pactive);
+        if (n && blk.count == f.nlen) node_tensors(f.nfile, blk);
+        break;
+    }
+  }
+  f.pfile.close();
+  f.nfile.close();
+}

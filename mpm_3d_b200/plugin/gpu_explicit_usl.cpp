@@ -162,7 +162,7 @@ void GPUExplicitUSL::setUp(Job* job) {
   }
   check(mpmgpu_set_gravity(handle, 1, gravity), "mpmgpu_set_gravity");
   const std::string& sname = job->serializer->object_name;
-  if ((sname == "DefaultVTK" || sname == "MinimalVTK") && !job->serializer->fp64_props.empty())
+  if ((sname == "DefaultVTK" || sname == "MinimalVTK" || sname == "AsyncVTK") && !job->serializer->fp64_props.empty())
     sample_rate = job->serializer->fp64_props[0];
 }
 

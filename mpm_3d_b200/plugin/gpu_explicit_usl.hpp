@@ -10,13 +10,16 @@
 // driver, serializer) with the step on the GPU. int-properties mirror
 // ExplicitUSL::init (explicit_usl.cpp:25-44): {cpdi_spec, contact_spec}, plus
 // an optional third entry, the host write-back interval in steps (0 = write
-// back exactly when a DefaultVTK/MinimalVTK serializer is about to write a
-// frame, and every step for other serializers).
+// back exactly when a DefaultVTK, MinimalVTK or AsyncVTK serializer is about
+// to write a frame, and every step for other serializers).
 //
 // Supported objects on the path: CartesianLinear, DefaultBody with
-// DefaultPoints/DefaultNodes, IsotropicLinearElasticity, CartesianBox,
-// ContactHuang. Anything else is reported on stderr and the run stops with
-// exit(0), as the reference does for bad properties (cartesian.cpp:27-30).
+// DefaultPoints/DefaultNodes, IsotropicLinearElasticity,
+// CompressibleNeohookeanElasticity or Sand_SachithLocal, CartesianBox,
+// CartesianSmoothBox or CartesianFrictionalBox, ContactHuang or
+// ContactHuang_ReflectedBoundary. Anything else is reported on stderr and the
+// run stops with exit(0), as the reference does for bad properties
+// (cartesian.cpp:27-30).
 #ifndef MPM_B200_GPU_EXPLICIT_USL_HPP
 #define MPM_B200_GPU_EXPLICIT_USL_HPP
 

@@ -42,7 +42,10 @@
 #include "objects/materials/materials.hpp"
 #include "objects/nodes/nodes.hpp"
 #include "objects/points/points.hpp"
+#include "objects/serializers/serializers.hpp"
 #include "objects/solvers/solvers.hpp"
+
+#include "async_vtk.hpp"
 
 #ifdef MPM_WITH_GPU_PLUGIN
 // Drop-in check: the GPU solver plugin registered next to ExplicitUSL, as a
@@ -139,6 +142,11 @@ Registry<Serializer>::Registry() {
   object["DefaultVTK"] = &make<Serializer, NullSerializer>;
   object["MinimalVTK"] = &make<Serializer, NullSerializer>;
   object["NullSerializer"] = &make<Serializer, NullSerializer>;
+  // the reference's own DefaultVTK under a harness name (configs naming
+  // DefaultVTK keep the null serializer, so tests write no frames unless
+  // they ask), and the AsyncVTK plugin as a maintainer would register it
+  object["ReferenceDefaultVTK"] = &make<Serializer, DefaultVTK>;
+  object["AsyncVTK"] = &make<Serializer, AsyncVTK>;
 }
 template <>
 Registry<Driver>::Registry() {
@@ -263,6 +271,7 @@ int ref_step(void* hp, int n) {
   RefHandle* h = static_cast<RefHandle*>(hp);
   for (int s = 0; s < n; s++) {
     h->job.solver->step(&h->job);
+    h->job.serializer->writeFrame(&h->job);  // default_driver.cpp:65-79
     h->job.t += h->job.dt;
   }
   return 0;
