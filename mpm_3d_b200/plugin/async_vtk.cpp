@@ -15,6 +15,14 @@
 #include "mpm_vectorarray.hpp"
 #include "parser.hpp"
 
+AsyncVTK::AsyncVTK() {
+  object_name = "AsyncVTK";
+  mainpath = "";
+  // the streams the objects write into keep their text in memory
+  static_cast<std::ios&>(pcap_).rdbuf(&pbuf_);
+  static_cast<std::ios&>(ncap_).rdbuf(&nbuf_);
+}
+
 AsyncVTK::~AsyncVTK() {
   {
     std::lock_guard<std::mutex> lock(mu_);
@@ -75,39 +83,30 @@ std::vector<int> active_flags(const Eigen::VectorXi& a) {
 // DefaultVTK::writeFrame (default_vtk.cpp:120-200): the frame condition, the
 // two files per body, the title lines (the node file's carries the frame
 // count, the point file's the frame index) and the order in which the
-// objects write. The objects' arrays are captured here and formatted by the
-// writer thread.
+// objects write. Everything is captured here and written by the writer
+// thread.
 int AsyncVTK::writeFrame(Job* job) {
   if (!((job->t - job->t0) >= (sampledFrames / sampleRate) || sampledFrames == 0)) return 0;
   sampledFrames += 1;
   const int index = sampledFrames - 1;
+  if (headers_.size() < job->bodies.size()) headers_.resize(job->bodies.size());
   std::vector<std::unique_ptr<Frame>> frame;
   for (size_t b = 0; b < job->bodies.size(); b++) {
     Body* body = job->bodies[b].get();
     std::unique_ptr<Frame> f(new Frame());
-    const std::string pname = frameDirectory + frame_file("fpd", body, index);
-    const std::string nname = frameDirectory + frame_file("fnd", body, index);
-    f->pfile.open(pname, std::ios::trunc);
-    f->nfile.open(nname, std::ios::trunc);
+    f->ppath = frameDirectory + frame_file("fpd", body, index);
+    f->npath = frameDirectory + frame_file("fnd", body, index);
     f->plen = body->points->x.size();
     f->nlen = body->nodes->x.size();
     f->pactive = active_flags(body->points->active);
     f->nactive = active_flags(body->nodes->active);
     current_ = f.get();
-    if (f->pfile.is_open()) {
-      f->pfile << "# vtk DataFile Version 3.0\n";
-      f->pfile << "Frame: " << index << ", Time: " << job->t << "\n";
-      body->points->writeHeader(job, body, this, f->pfile, VTK);
-    } else {
-      std::cerr << "Could not open point frame: " << pname << " !" << std::endl;
-    }
-    if (f->nfile.is_open()) {
-      f->nfile << "# vtk DataFile Version 3.0\n";
-      f->nfile << "Frame: " << sampledFrames << ", Time: " << job->t << "\n";
-      job->grid->writeHeader(job, body, this, f->nfile, VTK);
-    } else {
-      std::cerr << "Could not open node frame: " << nname << " !" << std::endl;
-    }
+    pcap_ << "# vtk DataFile Version 3.0\n";
+    pcap_ << "Frame: " << index << ", Time: " << job->t << "\n";
+    body->points->writeHeader(job, body, this, pcap_, VTK);
+    ncap_ << "# vtk DataFile Version 3.0\n";
+    ncap_ << "Frame: " << sampledFrames << ", Time: " << job->t << "\n";
+    nodeHeader(job, body, b);
     if (job->activeBodies[b] != 0) {
       body->points->writeFrame(job, body, this);
       body->nodes->writeFrame(job, body, this);
@@ -116,6 +115,8 @@ int AsyncVTK::writeFrame(Job* job) {
       job->grid->writeFrame(job, this);
     }
     for (size_t c = 0; c < job->contacts.size(); c++) job->contacts[c]->writeFrame(job, this);
+    takeText(0);
+    takeText(1);
     current_ = nullptr;
     frame.push_back(std::move(f));
   }
@@ -127,6 +128,53 @@ int AsyncVTK::writeFrame(Job* job) {
   return 1;
 }
 
+// Moves the text collected for one file into the current frame, so that it
+// keeps its place among the captured blocks.
+void AsyncVTK::takeText(int file) {
+  std::stringbuf& buf = file == 0 ? pbuf_ : nbuf_;
+  std::string text = buf.str();
+  if (text.empty()) return;
+  buf.str(std::string());
+  Block blk;
+  blk.kind = Block::kText;
+  blk.file = file;
+  blk.text = std::make_shared<const std::string>(std::move(text));
+  current_->blocks.push_back(std::move(blk));
+}
+
+// The grid's node header (Grid::writeHeader, cartesian.cpp:459-520): reused
+// while the body's node positions and active flags are those it was written
+// from, else written again into memory and kept.
+void AsyncVTK::nodeHeader(Job* job, Body* body, size_t b) {
+  takeText(1);
+  HeaderCache& hc = headers_[b];
+  Nodes* nodes = body->nodes.get();
+  const int n = nodes->x.size();
+  std::vector<double> x(3 * (size_t)n);
+  for (int i = 0; i < n; i++)
+    for (int pos = 0; pos < 3; pos++) x[3 * (size_t)i + pos] = nodes->x(i, pos);
+  const std::vector<int>& active = current_->nactive;
+  if (hc.text && hc.x == x && hc.active == active) {
+    Block blk;
+    blk.kind = Block::kText;
+    blk.file = 1;
+    blk.text = hc.text;
+    current_->blocks.push_back(std::move(blk));
+    return;
+  }
+  headerCaptured_ = false;
+  const size_t before = current_->blocks.size();
+  job->grid->writeHeader(job, body, this, ncap_, VTK);
+  const bool plain = !headerCaptured_ && current_->blocks.size() == before;
+  takeText(1);
+  hc.text.reset();
+  if (plain && current_->blocks.size() == before + 1) {
+    hc.x = std::move(x);
+    hc.active = active;
+    hc.text = current_->blocks.back().text;
+  }
+}
+
 void AsyncVTK::flush() {
   std::unique_lock<std::mutex> lock(mu_);
   cv_.wait(lock, [&] { return queue_.empty() && busy_ == 0; });
@@ -136,6 +184,7 @@ void AsyncVTK::flush() {
 
 void AsyncVTK::writeDefaultPointHeader(Job* job, Body* body, std::ofstream& pfile, int SPEC) {
   if (!current_) return;
+  takeText(0);
   Block blk;
   blk.kind = Block::kPointHeader;
   blk.dim = body->points->x.DIM;
@@ -148,6 +197,8 @@ void AsyncVTK::writeDefaultPointHeader(Job* job, Body* body, std::ofstream& pfil
 
 void AsyncVTK::writeDefaultNodeHeader(Job* job, Body* body, std::ofstream& nfile, int SPEC) {
   if (!current_) return;
+  takeText(1);
+  headerCaptured_ = true;
   Block blk;
   blk.kind = Block::kNodeHeader;
   blk.dim = body->nodes->x.DIM;
@@ -160,6 +211,8 @@ void AsyncVTK::writeDefaultNodeHeader(Job* job, Body* body, std::ofstream& nfile
 
 void AsyncVTK::writeScalarArray(Eigen::VectorXd& scalarArray, std::string name) {
   if (!current_) return;
+  takeText(0);
+  takeText(1);
   Block blk;
   blk.kind = Block::kScalar;
   blk.name = name;
@@ -171,6 +224,8 @@ void AsyncVTK::writeScalarArray(Eigen::VectorXd& scalarArray, std::string name) 
 
 void AsyncVTK::writeVectorArray(MPMVectorArray& vectorArray, std::string name) {
   if (!current_) return;
+  takeText(0);
+  takeText(1);
   Block blk;
   blk.kind = Block::kVector;
   blk.name = name;
@@ -183,6 +238,8 @@ void AsyncVTK::writeVectorArray(MPMVectorArray& vectorArray, std::string name) {
 
 void AsyncVTK::writeTensorArray(MPMTensorArray& tensorArray, std::string name) {
   if (!current_) return;
+  takeText(0);
+  takeText(1);
   Block blk;
   blk.kind = Block::kTensor;
   blk.name = name;
@@ -314,29 +371,34 @@ void node_tensors(std::ofstream& out, const AsyncVTK::Block& blk) {
 }  // namespace
 
 void AsyncVTK::format(Frame& f) {
-  const bool p = f.pfile.is_open(), n = f.nfile.is_open();
+  std::ofstream pfile(f.ppath, std::ios::trunc), nfile(f.npath, std::ios::trunc);
+  const bool p = pfile.is_open(), n = nfile.is_open();
+  if (!p) std::cerr << "Could not open point frame: " << f.ppath << " !" << std::endl;
+  if (!n) std::cerr << "Could not open node frame: " << f.npath << " !" << std::endl;
   for (const Block& blk : f.blocks) {
     switch (blk.kind) {
+      case Block::kText:
+        if (blk.file == 0 && p) pfile << *blk.text;
+        if (blk.file == 1 && n) nfile << *blk.text;
+        break;
       case Block::kPointHeader:
-        if (p) header(f.pfile, blk, f.pactive);
+        if (p) header(pfile, blk, f.pactive);
         break;
       case Block::kNodeHeader:
-        if (n) header(f.nfile, blk, f.nactive);
+        if (n) header(nfile, blk, f.nactive);
         break;
       case Block::kScalar:
-        if (p && blk.count == f.plen) scalars(f.pfile, blk, f.pactive);
-        if (n && blk.count == f.nlen) scalars(f.nfile, blk, f.nactive);
+        if (p && blk.count == f.plen) scalars(pfile, blk, f.pactive);
+        if (n && blk.count == f.nlen) scalars(nfile, blk, f.nactive);
         break;
       case Block::kVector:
-        if (p && blk.count == f.plen) vectors(f.pfile, blk, f.pactive);
-        if (n && blk.count == f.nlen) vectors(f.nfile, blk, f.nactive);
+        if (p && blk.count == f.plen) vectors(pfile, blk, f.pactive);
+        if (n && blk.count == f.nlen) vectors(nfile, blk, f.nactive);
         break;
       case Block::kTensor:
-        if (p && blk.count == f.plen) point_tensors(f.pfile, blk, f.pactive);
-        if (n && blk.count == f.nlen) node_tensors(f.nfile, blk);
+        if (p && blk.count == f.plen) point_tensors(pfile, blk, f.pactive);
+        if (n && blk.count == f.nlen) node_tensors(nfile, blk);
         break;
     }
   }
-  f.pfile.close();
-  f.nfile.close();
 }

@@ -11,15 +11,18 @@
 // and it writes the same files with the same bytes: the frame condition and
 // file names of DefaultVTK::writeFrame (120-200), and the number formatting
 // and zero rules of its header and array writers (55-125, 204-330). At a
-// frame, writeFrame opens each body's point and node files and lets the
-// objects write as they do for DefaultVTK. Text an object writes straight
-// into a stream (the title lines, a grid's node header) goes there at once;
-// the default point and node headers and every array an object hands to
-// writeScalarArray / writeVectorArray / writeTensorArray are copied, with
-// the active flags they are written against, and formatted later by the
-// writer thread. maxPending (default 2) bounds the frames held in memory:
-// writeFrame waits while that many are queued. The destructor writes every
-// queued frame before it returns.
+// frame, writeFrame lets the objects write as they do for DefaultVTK, but
+// nothing reaches a file on that thread: text an object writes into the
+// stream it is given (the title lines, a grid's node header) is collected in
+// memory, and the default point and node headers and every array handed to
+// writeScalarArray / writeVectorArray / writeTensorArray are copied with the
+// active flags they are written against. A writer thread formats and writes
+// the frames in order. The grid's header text of a body is kept and reused
+// while the body's node positions and active flags are unchanged (a
+// CartesianLinear header is all positions and fixed connectivity).
+// maxPending (default 2) bounds the frames held in memory: writeFrame waits
+// while that many are queued. The destructor writes every queued frame
+// before it returns.
 #ifndef MPM_B200_ASYNC_VTK_HPP
 #define MPM_B200_ASYNC_VTK_HPP
 
@@ -28,6 +31,7 @@
 #include <fstream>
 #include <memory>
 #include <mutex>
+#include <sstream>
 #include <string>
 #include <thread>
 #include <vector>
@@ -36,10 +40,7 @@
 
 class AsyncVTK : public Serializer {
  public:
-  AsyncVTK() {
-    object_name = "AsyncVTK";
-    mainpath = "";
-  }
+  AsyncVTK();
   ~AsyncVTK() override;
 
   std::string frameDirectory, outputDirectory, outputName;
@@ -61,29 +62,45 @@ class AsyncVTK : public Serializer {
   // Blocks until every queued frame is on disk.
   void flush();
 
-  // One deferred piece of a frame file: a default header or a named array
-  // (width values per entry, entries in point or node order).
+  // One deferred piece of a frame file: text for one of the two files, a
+  // default header, or a named array (entries in point or node order).
   struct Block {
-    enum Kind { kPointHeader, kNodeHeader, kScalar, kVector, kTensor } kind;
+    enum Kind { kText, kPointHeader, kNodeHeader, kScalar, kVector, kTensor } kind;
+    int file = 0;                             // text: 0 point file, 1 node file
+    std::shared_ptr<const std::string> text;  // text
     std::string name;
     int dim = 0;                 // header: the position array's DIM
     int count = 0;               // entries
     std::vector<double> values;  // count * width
   };
 
-  // One body's frame: its two open files and what is still to be written.
+  // One body's frame: its two files and what is to be written into them.
   struct Frame {
-    std::ofstream pfile, nfile;
+    std::string ppath, npath;
     int plen = 0, nlen = 0;
     std::vector<int> pactive, nactive;  // the body's active flags at the frame
     std::vector<Block> blocks;          // in the order the objects wrote them
   };
 
  private:
+  // The grid header text of a body and the node state it was written from.
+  struct HeaderCache {
+    std::vector<double> x;
+    std::vector<int> active;
+    std::shared_ptr<const std::string> text;
+  };
+
+  void takeText(int file);
+  void nodeHeader(Job* job, Body* body, size_t b);
   void writerLoop();
   static void format(Frame& f);
 
   Frame* current_ = nullptr;  // the frame being captured (writeFrame's thread)
+  // streams handed to the objects; their text collects in memory
+  std::stringbuf pbuf_, nbuf_;
+  std::ofstream pcap_, ncap_;
+  bool headerCaptured_ = false;  // a default header was captured during a grid header call
+  std::vector<HeaderCache> headers_;
   std::mutex mu_;
   std::condition_variable cv_;
   std::deque<std::vector<std::unique_ptr<Frame>>> queue_;  // one entry per frame: its bodies' files
