@@ -399,6 +399,24 @@ mpmgpu_status mpmgpu_server_stats(const mpmgpu_server* s, int* running, int64_t*
 double mpmgpu_server_clock(const mpmgpu_server* s);
 mpmgpu_status mpmgpu_server_destroy(mpmgpu_server* s);
 
+/* ---- .points files ----
+ * Host-side reader of the DefaultPoints point files that the reference's
+ * configs name (DefaultPoints::readFromFile, default_points.cpp:104-193):
+ * a count line, then per point "m v x.. x_t.. active" separated by single
+ * spaces, split and converted as the reference does (Parser::splitString,
+ * std::stod). The lines are parsed on `threads` threads (0: all the host
+ * offers); no GPU is used. Arrays come back in mpmgpu_body_desc's layout
+ * (x and x_t AoS with stride 3, zero beyond dim), ready for
+ * mpmgpu_add_body. A missing file or a malformed line (wrong column count,
+ * a column that is not a number) gives MPMGPU_ERR_ARG and, where bad_line
+ * is not NULL, the 1-based line number (0 for the file itself); the
+ * reference prints an error there and keeps zeros for the remaining points.
+ * mpmgpu_points_file_count reads the count line; _read requires n to equal
+ * it. */
+mpmgpu_status mpmgpu_points_file_count(const char* path, int64_t* n);
+mpmgpu_status mpmgpu_points_file_read(const char* path, int dim, int64_t n, double* m, double* v, double* x,
+                                      double* x_t, int32_t* active, int threads, int64_t* bad_line);
+
 #ifdef __cplusplus
 }
 #endif

@@ -11,6 +11,7 @@
 
 #include "../../include/mpm_b200.h"
 #include "engine.cuh"
+#include "points_file.h"
 #include "server.cuh"
 
 using namespace mpmb200;
@@ -634,4 +635,21 @@ extern "C" mpmgpu_status mpmgpu_dump_map_noalloc(mpmgpu_handle* h, int body, int
   *count = total;
   if (total > capacity) return hfail(h, MPMGPU_ERR_ARG, "capacity below the triplet count");
   return MPMGPU_OK;
+}
+
+// ---- .points files (host only) ----
+
+mpmgpu_status mpmgpu_points_file_count(const char* path, int64_t* n) {
+  if (!path || !n) return MPMGPU_ERR_ARG;
+  return mpmb200::points_file_count(path, n).ok ? MPMGPU_OK : MPMGPU_ERR_ARG;
+}
+
+mpmgpu_status mpmgpu_points_file_read(const char* path, int dim, int64_t n, double* m, double* v, double* x,
+                                      double* x_t, int32_t* active, int threads, int64_t* bad_line) {
+  if (bad_line) *bad_line = 0;
+  if (!path || (dim != 2 && dim != 3) || n < 0 || (n > 0 && (!m || !v || !x || !x_t || !active)))
+    return MPMGPU_ERR_ARG;
+  const mpmb200::PointsFileResult r = mpmb200::points_file_read(path, dim, n, m, v, x, x_t, active, threads);
+  if (bad_line) *bad_line = r.bad_line;
+  return r.ok ? MPMGPU_OK : MPMGPU_ERR_ARG;
 }

@@ -156,12 +156,37 @@ def load() -> ctypes.CDLL:
     lib.mpmgpu_server_clock.restype = ctypes.c_double
     lib.mpmgpu_server_clock.argtypes = [vp]
     lib.mpmgpu_server_destroy.argtypes = [vp]
+    lib.mpmgpu_points_file_count.argtypes = [ctypes.c_char_p, i64p]
+    lib.mpmgpu_points_file_read.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int64, vp, vp, vp, vp, vp,
+                                            ctypes.c_int, i64p]
     _lib = lib
     return lib
 
 
 def _ptr(a: np.ndarray) -> ctypes.c_void_p:
     return ctypes.c_void_p(a.ctypes.data)
+
+
+def read_points_file(path: str, dim: int, threads: int = 0):
+    """Reads a DefaultPoints ``.points`` file with the library's parallel
+    reader (mpmgpu_points_file_read; host only, no GPU): returns (m, v,
+    x (n,3), x_t (n,3), active), parsed as DefaultPoints::readFromFile does."""
+    lib = load()
+    n = ctypes.c_int64()
+    st = lib.mpmgpu_points_file_count(path.encode(), ctypes.byref(n))
+    if st != 0:
+        raise MpmGpuError(f"{path}: no point count on the first line (status {st})")
+    m = np.zeros(n.value)
+    v = np.zeros(n.value)
+    x = np.zeros((n.value, 3))
+    xt = np.zeros((n.value, 3))
+    active = np.zeros(n.value, np.int32)
+    bad = ctypes.c_int64()
+    st = lib.mpmgpu_points_file_read(path.encode(), dim, n.value, _ptr(m), _ptr(v), _ptr(x), _ptr(xt), _ptr(active),
+                                     threads, ctypes.byref(bad))
+    if st != 0:
+        raise MpmGpuError(f"{path}: unable to read line {bad.value} (status {st})")
+    return m, v, x, xt, active
 
 
 class GPUExplicitUSL:
