@@ -3,6 +3,7 @@ import os
 import tempfile
 
 import numpy as np
+import pytest
 
 from mpm_3d_b200 import inputs
 
@@ -82,3 +83,31 @@ def test_adjacent_classes_in_written_configs():
     plain.bodies[0].boundary = False
     assert inputs.boundary_kind(plain.bodies[0]) == 0
     assert "boundary-class" not in open(inputs.write_case(plain, d)).read()
+
+
+def test_sand_properties_resolve_as_the_reference_init():
+    """Sand_SachithLocal::init (sand_sachithlocal.cpp:57-103): with six
+    material-props mu_2 = mu_s and I_0 = 1; with eight they are given."""
+    six = inputs.sand_column(2, steps=1)
+    props, density = inputs.sand_params(six.bodies[0])
+    assert props == (0.01, 0.577, 1650.0, 1000.0, 0.577, 1.0) and not density
+    eight = inputs.sand_column(2, steps=1, density_pressure=True, mu_2=0.8)
+    props, density = inputs.sand_params(eight.bodies[0])
+    assert props == (0.01, 0.577, 1650.0, 1000.0, 0.8, 0.278) and density
+    assert inputs.material_kind(eight.bodies[0]) == 2
+    bad = inputs.sand_column(2, steps=1)
+    bad.bodies[0].material_props = (0.01, 0.577)
+    with pytest.raises(ValueError):
+        inputs.sand_params(bad.bodies[0])
+
+
+def test_written_config_carries_material_point_and_serializer_settings(tmp_path):
+    case = inputs.sand_column(2, steps=1, density_pressure=True, mu_2=0.8)
+    text = open(inputs.write_case(case, str(tmp_path), point_int_props=(1,), serializer_class="AsyncVTK",
+                                  frame_dir="frames", sample_rate=250.0)).read()
+    assert 'material-class = "Sand_SachithLocal"' in text
+    assert "material-props = {10000000.0,0.3,0.01,0.577,1650.0,1000.0,0.8,0.278}" in text
+    assert 'material-str-props = {"USE_DENSITY_FOR_PRESSURE"}' in text
+    assert "point-int-props = {1}" in text
+    assert 'class = "AsyncVTK"' in text and "properties = {250.0}" in text
+    assert 'str-properties = {"frames","save","case"}' in text
