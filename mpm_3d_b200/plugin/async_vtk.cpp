@@ -120,6 +120,8 @@ int AsyncVTK::writeFrame(Job* job) {
     current_ = nullptr;
     frame.push_back(std::move(f));
   }
+  // a writer even when init was skipped, so that the wait below always ends
+  if (!writer_.joinable()) writer_ = std::thread(&AsyncVTK::writerLoop, this);
   std::unique_lock<std::mutex> lock(mu_);
   cv_.wait(lock, [&] { return (int)queue_.size() + busy_ < std::max(maxPending, 1); });
   queue_.push_back(std::move(frame));
