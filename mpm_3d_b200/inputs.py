@@ -431,19 +431,23 @@ def read_points_file(path: str, dim: int) -> Tuple[np.ndarray, ...]:
 def write_case(case: Case, directory: str, solver_class: str = "ExplicitUSL", points_class: str = "DefaultPoints",
                threads: Optional[int] = None, solver_extra: Sequence[int] = (),
                point_int_props: Sequence[int] = (), serializer_class: str = "DefaultVTK",
-               frame_dir: str = "output", sample_rate: float = 60.0) -> str:
+               frame_dir: str = "output", sample_rate: float = 60.0,
+               serializer_int_props: Sequence[int] = ()) -> str:
     """Writes ``<name>.cfg`` and the ``.points`` files; returns the cfg path.
     ``solver_extra`` appends solver int-properties (the GPU solver's
     write-back interval and form); ``point_int_props`` are DefaultPoints'
     int-properties ({1}: the point-element history, use_elem); the
     serializer writes frames to ``frame_dir`` at ``sample_rate`` per
-    simulated second."""
+    simulated second (``serializer_int_props``: its int-properties)."""
     os.makedirs(directory, exist_ok=True)
     lines = ["job", "{", f"    dt = {_fmt(case.dt)}", "    t = 0", f"    TYPE = {case.dim}"]
     if threads is not None:
         lines.append(f"    threads = {threads}")
     lines += ["}", "", "serializer", "{", f'    class = "{serializer_class}"', f"    properties = {{{_fmt(sample_rate)}}}",
-              f'    str-properties = {{"{frame_dir}","save","case"}}', "}", ""]
+              f'    str-properties = {{"{frame_dir}","save","case"}}']
+    if serializer_int_props:
+        lines += ["    int-properties = {" + ",".join(str(v) for v in serializer_int_props) + "}"]
+    lines += ["}", ""]
     stop = case.dt * case.steps
     if case.gravity is None:
         lines += ["driver", "{", '    class = "DefaultDriver"', f"    properties = {{{_fmt(stop)}}}", "}", ""]

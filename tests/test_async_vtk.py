@@ -40,12 +40,12 @@ CASES = {
 }
 
 
-def _frames(case, steps, serializer, every=5):
+def _frames(case, steps, serializer, every=5, int_props=()):
     d = tempfile.mkdtemp()
     frames = os.path.join(d, "frames")
     os.makedirs(frames)
     cfg = inputs.write_case(case, d, serializer_class=serializer, frame_dir=frames,
-                            sample_rate=1.0 / (every * case.dt))
+                            sample_rate=1.0 / (every * case.dt), serializer_int_props=int_props)
     job = bridge.ReferenceJob(cfg)
     job.step(steps)
     job.close()
@@ -75,3 +75,15 @@ def test_async_vtk_writes_the_reference_frames(name):
         assert "VECTORS contact_normal_" in nodes
     if case.bodies[0].material_class == "Sand_SachithLocal":
         assert "SCALARS gammap double 1" in sample
+
+
+@needs_ref
+def test_async_vtk_with_one_pending_frame_and_a_frame_every_step():
+    """maxPending = 1: writeFrame waits for the writer at every frame; the
+    files are still the reference's."""
+    case = inputs.two_body_collision_2d(20, steps=12)
+    ref = _frames(inputs.two_body_collision_2d(20, steps=12), 12, "ReferenceDefaultVTK", every=1)
+    got = _frames(case, 12, "AsyncVTK", every=1, int_props=(1,))
+    assert len(ref) >= 2 * 2 * 11 and sorted(got) == sorted(ref)
+    for fname in ref:
+        assert got[fname] == ref[fname], fname
