@@ -13,10 +13,13 @@ Workloads (seeded synthetic inputs, mpm_3d_b200.inputs):
   ensemble   (default) 512 independent 3D block drops (grids 16^3..96^3,
              16.75 M points, seed 1003) in one batch, mixed form (FP32 point
              state, FP64 nodal sums), one launch per stage replayed from a
-             CUDA graph, points per CTA chosen by the autotuner. Reported
-             beside it: the same batch in FP64, the plain FP64 path (one
-             handle per job, jobs one after another) and the mixed form's
-             error against FP64 on every 8th job.
+             CUDA graph, kernel form and points per CTA chosen by the
+             autotuner. Reported beside it: the same batch in FP64, the
+             plain FP64 path (one handle per job, jobs one after another),
+             the mixed form's error against FP64 on every 8th job after
+             its full 500 steps, the column collapse in plain FP64
+             (``column_fp64``, with its own roofline) and the full serving
+             stream (``serving_full``, 60 s of arrivals).
   blockdrop2d  the 2D block drop, 20x20 grid, 144 points, 2000 steps (CPU-sized)
   collision  two 0.25 m cubes colliding, 128^3 grid, 524,288 points, ContactHuang (FP64)
   column     column collapse, 256x256x128 grid, 3,145,728 points (FP64)
@@ -25,8 +28,8 @@ Workloads (seeded synthetic inputs, mpm_3d_b200.inputs):
              150 GB budget into one continuously batched mixed-form server;
              ``value`` is the particle-steps/s of the completed requests over
              the makespan, with p50/p99 time to completion. The ensemble
-             line carries the same figures for the first --serve-seconds of
-             the stream.
+             line carries the same figures for --serve-seconds of arrivals
+             (60 by default, the whole stream).
 
 With N > 1 (torchrun) every rank runs its own copy of the workload (the
 ensemble with seed 1003 + rank; the single jobs as replicas): no data
@@ -77,9 +80,9 @@ ENSEMBLE_JOBS = 512
 ENSEMBLE_SEED = 1003
 
 # DRAM bytes (read + write) per point of one k_g2p2g launch, from ncu
-# captures (profiles/k_g2p2g_ensemble96_mixed.md: the first 96 jobs of the
-# ensemble, scaled to a launch by its points; profiles/k_g2p2g_column_fp64.md:
-# the full column). None where no capture exists.
+# captures of the kernel (the ensemble's from a capture of its first 96 jobs,
+# scaled to a launch by its points; the column's at full size). None where no
+# capture exists.
 TRAFFIC_BYTES_PER_POINT = {("ensemble", "mixed"): 159.9, ("column", "fp64"): 305.3}
 
 
@@ -356,33 +359,47 @@ def roofline(points: int, steps: int, prof, active_ratio: float, mixed: bool, tr
             "bytes_per_point_step": bpp, "launch_ms": per_launch_ms, "points_per_launch": points_per_launch}
 
 
-def run_single(args, rank, world, local):
+def single_timed(case, form: str, steps: int, warmup: int, device: int, world: int = 1, traffic_key=None):
+    """One single-job handle: `warmup` steps, then `steps` steps timed with
+    CUDA events (L2 flushed between steps when the point state would fit
+    in it), a profiled pass for the fused kernel's launch time, and the
+    roofline of that kernel."""
     import torch
 
     from mpm_3d_b200.native import GPUExplicitUSL
 
+    n = case.n_points
+    flush_l2 = 148 * n < 2 * L2_BYTES
+    flush_buf = torch.empty(4 * L2_BYTES // 4, dtype=torch.float32, device="cuda") if flush_l2 else None
+    sim = GPUExplicitUSL(case, device=device, mode=form)
+    sim.step(warmup)
+    barrier(world)
+    step_ms, launches, clk = timed_steps(sim, steps, flush_buf)
+    barrier(world)
+    prof_steps = min(10, steps)
+    prof = profile_pass(sim, prof_steps)
+    active, _drift = sim.active_nodes()
+    active_ratio = active / max(1, n)
+    roof = roofline(n, prof_steps, prof, active_ratio, form == "mixed", traffic_key)
+    sim.close()
+    del flush_buf
+    return {"step_ms": step_ms, "launches": launches, "clocks": clk, "prof": prof, "prof_steps": prof_steps,
+            "active_ratio": active_ratio, "roofline": roof, "l2_flushed": flush_l2}
+
+
+def run_single(args, rank, world, local):
+    import torch
+
     torch.cuda.set_device(local)
     case = make_workload(args.workload)
     n = case.n_points
-    state_bytes = 148 * n
-    flush_l2 = state_bytes < 2 * L2_BYTES
-    flush_buf = torch.empty(4 * L2_BYTES // 4, dtype=torch.float32, device="cuda") if flush_l2 else None
-
-    sim = GPUExplicitUSL(case, device=local, mode=args.form)
-    sim.step(args.warmup)
-    barrier(world)
-    step_ms, launches, clk = timed_steps(sim, args.steps, flush_buf)
-    barrier(world)
+    r = single_timed(case, args.form, args.steps, args.warmup, local, world, (args.workload, args.form))
+    step_ms, launches, clk, prof, prof_steps = r["step_ms"], r["launches"], r["clocks"], r["prof"], r["prof_steps"]
+    flush_l2, active_ratio, roof = r["l2_flushed"], r["active_ratio"], r["roofline"]
     total_ms = sum(step_ms)
     total_ms_max = max_over_ranks(total_ms, world)
     points_all = sum_over_ranks(float(n), world)
     value = points_all * args.steps / (total_ms_max * 1e-3)
-    prof_steps = min(10, args.steps)
-    prof = profile_pass(sim, prof_steps)
-    active, _drift = sim.active_nodes()
-    active_ratio = active / max(1, n)
-    roof = roofline(n, prof_steps, prof, active_ratio, args.form == "mixed", (args.workload, args.form))
-    sim.close()
 
     e2e = run_e2e(case, args.steps, local, args.form) if rank == 0 and not args.no_e2e else None
     cpu = None
@@ -435,12 +452,51 @@ def run_batch(cases, mode: str, args, device: int, sample_ids):
     prof_steps = 3
     prof = profile_pass(b, prof_steps)
     active, drift = b.active_nodes()
-    fields = {i: {f: b.points(jobs[i], 0, f) for f in ("x", "x_t", "T")} for i in sample_ids}
     steps_done = b.state(jobs[0])[0]
     b.close()
     return {"step_ms": step_ms, "launches": launches, "clocks": clk, "prof": prof, "prof_steps": prof_steps,
-            "active": active, "drift": drift, "cap": cap, "sort_interval": si, "fields": fields,
+            "active": active, "drift": drift, "cap": cap, "sort_interval": si,
             "steps_done": steps_done}
+
+
+def mixed_error_full(cases, sample_ids, device: int):
+    """The mixed form's error against FP64 after every sampled job's full
+    step count: the sampled jobs run as one FP64 batch and one mixed batch
+    to their ends (outside any timed region) and x, x_t and the stress are
+    compared per job."""
+    from mpm_3d_b200.native import GPUBatch
+
+    sub = [cases[i] for i in sample_ids]
+    steps = max(c.steps for c in sub)
+    fields = {}
+    for mode in ("fp64", "mixed"):
+        b = GPUBatch(dim=3, mode=mode, device=device)
+        jobs = [b.add(c) for c in sub]
+        b.step(steps)
+        fields[mode] = [{f: b.points(j, 0, f) for f in ("x", "x_t", "T")} for j in jobs]
+        done = min(b.state(j)[0] for j in jobs)
+        b.close()
+    errs = {f: 0.0 for f in ("x", "x_t", "T")}
+    for k, c in enumerate(sub):
+        for f in errs:
+            errs[f] = max(errs[f], rel_err(fields["mixed"][k][f], fields["fp64"][k][f], field_floor(c, f)))
+    return {**errs, "jobs_compared": len(sub), "after_steps": done,
+            "norm": "max|mixed - fp64| / max(max|fp64|, field scale) per job, worst job"}
+
+
+def column_fp64_record(device: int, steps: int = 20, warmup: int = 5):
+    """The column collapse (3,145,728 points, 256x256x128 grid) in the plain
+    FP64 form on one handle: the configuration the FP64 roofline target is
+    stated on."""
+    case = make_workload("column")
+    r = single_timed(case, "fp64", steps, warmup, device, 1, ("column", "fp64"))
+    total_ms = sum(r["step_ms"])
+    return {"value": case.n_points * steps / (total_ms * 1e-3), "unit": UNIT, "ms_per_step": total_ms / steps,
+            "steps": steps, "warmup": warmup, "points": case.n_points, "grid": list(case.N), "form": "fp64",
+            "roofline": r["roofline"], "stage_ms_per_step": {k: v[1] / r["prof_steps"] for k, v in r["prof"].items()},
+            "gpu_launches": r["launches"], "clocks": r["clocks"],
+            "l2": "flushed between steps" if r["l2_flushed"] else "inputs larger than L2",
+            "active_nodes_per_point": round(r["active_ratio"], 4)}
 
 
 def plain_fp64(cases, steps: int, device: int):
@@ -488,14 +544,12 @@ def run_ensemble(args, rank, world, local):
     points_all = sum_over_ranks(float(n), world)
     value = points_all * args.steps / (total_ms_max * 1e-3)
     fp64_value = n * args.steps / (sum(fp64["step_ms"]) * 1e-3) if fp64 else None
-    # the mixed form's error against FP64 after the same steps, per field
-    errs = {f: (0.0 if fp64 else None) for f in ("x", "x_t", "T")}
-    for i in (sample_ids if fp64 else []):
-        for f in errs:
-            errs[f] = max(errs[f], rel_err(mixed["fields"][i][f], fp64["fields"][i][f], field_floor(cases[i], f)))
+    # the mixed form's error against FP64 after every sampled job's 500 steps
+    errs = mixed_error_full(cases, sample_ids, local) if fp64 else None
     active_ratio = mixed["active"] / max(1, n)
     roof = roofline(n, mixed["prof_steps"], mixed["prof"], active_ratio, True, ("ensemble", "mixed"))
     plain_value, plain_ms = plain_fp64(cases, args.plain_steps, local) if not args.no_plain else (None, None)
+    column = column_fp64_record(local) if not args.no_column else None
     serving = run_serving(args.serve_seconds, local, mixed["sort_interval"]) if args.serve_seconds > 0 else None
     # end to end: every job runs its own step count (the workload's 500
     # steps), as a user runs the ensemble
@@ -524,9 +578,9 @@ def run_ensemble(args, rank, world, local):
         "plain_fp64": {"value": plain_value, "unit": UNIT, "steps_per_job": args.plain_steps,
                        "how": "one mpmgpu_handle per job, jobs in sequence, CUDA events around each job's steps"},
         "vs_plain_fp64": (value / plain_value) if plain_value else None,
-        "mixed_rel_err_vs_fp64": {**errs, "jobs_compared": len(sample_ids), "after_steps": mixed["steps_done"],
-                                  "norm": "max|mixed - fp64| / max(max|fp64|, field scale) per job, worst job"},
-        "serving": serving,
+        "mixed_rel_err_vs_fp64": errs,
+        "column_fp64": column,
+        "serving_full": serving,
         "roofline": roof,
         "stage_ms_per_step": {k: v[1] / mixed["prof_steps"] for k, v in mixed["prof"].items()},
         "gpu_launches": mixed["launches"],
@@ -663,8 +717,9 @@ def main():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--jobs", type=int, default=0, help="ensemble: only the first JOBS jobs (profiling cases)")
     ap.add_argument("--only-mixed", action="store_true", help="ensemble: skip the FP64 batch")
-    ap.add_argument("--serve-seconds", type=float, default=-1.0,
-                    help="seconds of request arrivals of the serving stream (default 3 with the ensemble, 60 alone)")
+    ap.add_argument("--serve-seconds", type=float, default=60.0,
+                    help="seconds of request arrivals of the serving stream (0: none)")
+    ap.add_argument("--no-column", action="store_true", help="ensemble: skip the column FP64 record")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--ref-steps", type=int, default=4, help="steps of the CPU reference sample")
     ap.add_argument("--no-cpu", action="store_true")
@@ -672,8 +727,6 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    if args.serve_seconds < 0:
-        args.serve_seconds = 60.0 if args.workload == "serving" else 3.0
     if args.steps <= 0:
         args.steps = 100 if args.workload in ("ensemble", "serving") else make_workload(args.workload).steps
     rank, world, local = dist_setup(args.gpus)

@@ -2,7 +2,8 @@
  * mpm_b200: C ABI of the B200 (sm_100a) explicit MPM time step.
  *
  * This is the drop-in boundary for mpm_3d's ExplicitUSL solver. A host-side
- * Solver plugin owns one mpmgpu_handle per Job and maps
+ * Solver plugin (mpm_3d_b200/plugin/gpu_explicit_usl.cpp) owns one
+ * mpmgpu_handle per Job and maps
  * the reference objects onto these calls:
  *
  *   Solver::init / lazy first step   -> mpmgpu_create, mpmgpu_add_body,
@@ -202,9 +203,9 @@ mpmgpu_status mpmgpu_dump_map(mpmgpu_handle* h, int body, int32_t* node, int32_t
 
 /* No counterpart in the reference: an allocation-free form of
  * mpmgpu_dump_map for callers that cannot allocate device memory when they
- * need the map, e.g. code running while a CUDA stream is being captured into
- * a graph, a host framework that owns all device memory through its own
- * pool, or a real-time loop that forbids cudaMalloc/cudaFree after set-up.
+ * need the map, e.g. a host framework that owns all device memory through
+ * its own pool, or a real-time loop that forbids cudaMalloc/cudaFree after
+ * set-up.
  *
  * Writes the same triplets as mpmgpu_dump_map, in the same reference order,
  * into caller-provided DEVICE arrays: d_node[k], d_point[k] (int32),
@@ -217,11 +218,13 @@ mpmgpu_status mpmgpu_dump_map(mpmgpu_handle* h, int body, int32_t* node, int32_t
  * allocates nothing, but it serves at most 524,288 triplet slots: points x
  * 4^dim (8,192 points in 3D, 32,768 in 2D); larger bodies are rejected with
  * MPMGPU_ERR_ARG. The first call on a device looks up the array's device
- * address (cudaGetSymbolAddress); make that first call before any stream
- * capture. Every call reuses the same array: calls that overlap on the GPU
- * (from two handles or threads at once) race and must be serialised by the
- * caller. Returns after the triplets are written (synchronises the handle's
- * stream). */
+ * address (cudaGetSymbolAddress), and so does the first call after the
+ * device's context changed (a device reset). Every call reuses the same
+ * array: calls that overlap on the GPU (from two handles or threads at once)
+ * race and must be serialised by the caller. Returns after the triplets are
+ * written (synchronises the handle's stream); while the handle's stream is
+ * being captured into a CUDA graph the call queues nothing and returns
+ * MPMGPU_ERR_UNSUPPORTED, leaving the capture intact. */
 mpmgpu_status mpmgpu_dump_map_noalloc(mpmgpu_handle* h, int body, int32_t* d_node, int32_t* d_point, double* d_s,
                                       double* d_grad, int64_t capacity, int64_t* count);
 
@@ -239,6 +242,16 @@ void* mpmgpu_stream(const mpmgpu_handle* h);
  * the number of point visits that found a point outside its bin's staged
  * tile since creation (drift between re-binnings). Synchronises. */
 mpmgpu_status mpmgpu_active_nodes(mpmgpu_handle* h, int64_t* nodes, int64_t* drifted);
+
+/* No counterpart in the reference. Poll limit of the device-side waits of
+ * the fused kernel for the bulk copies of a work item (default 2^24 polls,
+ * far beyond the microseconds a copy takes). A wait that runs out does not
+ * hang the GPU: the kernel flags it, lets the copies in flight land and
+ * returns, and the next mpmgpu_synchronize reports MPMGPU_ERR_DEVICE. After
+ * that error the handle's simulation state is undefined (destroy it); the
+ * device and other handles stay usable. A small limit is a way to exercise
+ * that path without a fault. */
+mpmgpu_status mpmgpu_set_wait_limit(mpmgpu_handle* h, uint32_t polls);
 
 /* Per-stage device time accounting with CUDA events recorded on the
  * handle's stream around every launch of a stage. enable != 0 starts (and
@@ -352,12 +365,14 @@ mpmgpu_status mpmgpu_batch_destroy(mpmgpu_batch* b);
 /* ------------------------------------------------------------------------
  * Server: continuous batching of simulation requests.
  *
- * No counterpart in the reference. A server owns one batch and a device
- * memory budget. mpmgpu_server_submit admits a request (one job) at once if
- * its footprint (mpmgpu_batch_footprint) fits the budget left by the
- * requests still running, or while nothing runs; otherwise it returns
+ * No counterpart in the reference (its only run-time failure handling is
+ * exit(0) on SIGINT, include/signal_handler.hpp:15-31). A server owns one
+ * batch and a device memory budget. mpmgpu_server_submit admits a request
+ * (one job) at once if its footprint (mpmgpu_batch_footprint) fits the
+ * budget left by the requests still running; otherwise it returns
  * MPMGPU_ERR_STATE and the caller keeps the request queued and retries
- * after the next advance. Admitted requests join the running batch at the
+ * after the next advance. A request whose footprint exceeds the whole budget
+ * is rejected with MPMGPU_ERR_NOMEM (it could never run). Admitted requests join the running batch at the
  * next step boundary and step together with it; a request that has run its
  * steps has its final point state (x, u, x_t, T, v, active) copied to host
  * memory and its device memory released. Each request computes what it
@@ -383,7 +398,7 @@ mpmgpu_status mpmgpu_server_advance(mpmgpu_server* s, int steps);
 /* Ids of requests finished since the last poll (at most max_ids); returns
  * their number. */
 int mpmgpu_server_poll(mpmgpu_server* s, int* ids, int max_ids);
-/* State (1 running, 4 being copied out, 2 finished, 3 released),
+/* State (1 running, 4 being copied out, 2 finished, 3 released, 5 cancelled),
  * admission and completion times on mpmgpu_server_clock, points and steps
  * of a request. */
 mpmgpu_status mpmgpu_server_request(const mpmgpu_server* s, int id, int* state, double* t_admit, double* t_done,
@@ -391,6 +406,10 @@ mpmgpu_status mpmgpu_server_request(const mpmgpu_server* s, int id, int* state, 
 /* A finished request's final point field (MPMGPU_P_X, _U, _X_T, _T, _V or
  * _ACTIVE) of one body, in the layout of mpmgpu_download_points. */
 mpmgpu_status mpmgpu_server_result(mpmgpu_server* s, int id, int body, int field, double* out);
+/* Cancels a running request between advances: it leaves the batch at the
+ * next step boundary and its device memory and budget share are freed; the
+ * other requests are unaffected. MPMGPU_ERR_STATE if it is not running. */
+mpmgpu_status mpmgpu_server_cancel(mpmgpu_server* s, int id);
 /* Frees a finished request's host copy of its results. */
 mpmgpu_status mpmgpu_server_release(mpmgpu_server* s, int id);
 mpmgpu_status mpmgpu_server_stats(const mpmgpu_server* s, int* running, int64_t* reserved_bytes, int64_t* live_points,

@@ -193,6 +193,12 @@ mpmgpu_status mpmgpu_active_nodes(mpmgpu_handle* h, int64_t* nodes, int64_t* dri
   return h->b->active_nodes(nodes, drifted);
 }
 
+mpmgpu_status mpmgpu_set_wait_limit(mpmgpu_handle* h, uint32_t polls) {
+  if (!h) return MPMGPU_ERR_ARG;
+  h->b->set_wait_limit(polls);
+  return MPMGPU_OK;
+}
+
 mpmgpu_status mpmgpu_profile(mpmgpu_handle* h, int enable) {
   if (!h) return MPMGPU_ERR_ARG;
   return h->b->profile(enable);
@@ -414,7 +420,8 @@ mpmgpu_status mpmgpu_server_create(const mpmgpu_batch_config* cfg, int64_t budge
   if (!cfg || !out || budget_bytes <= 0) return MPMGPU_ERR_ARG;
   *out = nullptr;
   if (cfg->dim != 2 && cfg->dim != 3) return MPMGPU_ERR_UNSUPPORTED;
-  if (cfg->mode != MPMGPU_MODE_FP64 && cfg->mode != MPMGPU_MODE_MIXED) return MPMGPU_ERR_UNSUPPORTED;
+  if (cfg->mode != MPMGPU_MODE_FP64 && cfg->mode != MPMGPU_MODE_MIXED && cfg->mode != MPMGPU_MODE_FP64_DETERMINISTIC)
+    return MPMGPU_ERR_UNSUPPORTED;
   if (cfg->points_per_item != 0 && !cap_available(cfg->dim, cfg->mode == MPMGPU_MODE_MIXED, cfg->points_per_item))
     return MPMGPU_ERR_UNSUPPORTED;
   mpmgpu_status st = MPMGPU_OK;
@@ -428,7 +435,7 @@ mpmgpu_status mpmgpu_server_create(const mpmgpu_batch_config* cfg, int64_t budge
                       &msg);
   if (st != MPMGPU_OK) return st;
   auto srv = std::make_unique<mpmgpu_server>();
-  srv->s = std::make_unique<Server>(std::move(b), cfg->mode == MPMGPU_MODE_MIXED, cfg->keep_debug != 0, budget_bytes);
+  srv->s = std::make_unique<Server>(std::move(b), cfg->mode, cfg->keep_debug != 0, budget_bytes);
   *out = srv.release();
   return MPMGPU_OK;
 }
@@ -466,6 +473,11 @@ mpmgpu_status mpmgpu_server_result(mpmgpu_server* s, int id, int body, int field
   return s->s->result(id, body, field, out);
 }
 
+mpmgpu_status mpmgpu_server_cancel(mpmgpu_server* s, int id) {
+  if (!s) return MPMGPU_ERR_ARG;
+  return s->s->cancel(id);
+}
+
 mpmgpu_status mpmgpu_server_release(mpmgpu_server* s, int id) {
   if (!s) return MPMGPU_ERR_ARG;
   return s->s->release(id);
@@ -491,11 +503,12 @@ mpmgpu_status mpmgpu_server_destroy(mpmgpu_server* s) {
 // Allocation-free map export (mpmgpu_dump_map_noalloc).
 //
 // For callers that must not allocate device memory when they read the map
-// (graph capture, caller-owned memory pools, real-time loops): the slot
-// buffers that mpmgpu_dump_map takes from cudaMalloc live here in one static
-// device array, and the compaction to the reference's triplet order runs on
-// the device into the caller's arrays. Nothing is allocated on the host or
-// the device by the call.
+// (caller-owned memory pools, real-time loops): the slot buffers that
+// mpmgpu_dump_map takes from cudaMalloc live here in one static device
+// array, and the compaction to the reference's triplet order runs on the
+// device into the caller's arrays. Nothing is allocated on the host or the
+// device by the call. The call waits for its result (a stream
+// synchronisation), so it refuses to run on a stream under capture.
 // ---------------------------------------------------------------------------
 #include <mutex>
 
@@ -518,23 +531,49 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 constexpr int kNoAllocMaxDevices = 64;
 std::mutex g_noalloc_mutex;
 unsigned char* g_noalloc_base[kNoAllocMaxDevices] = {};
+void* g_noalloc_ctx[kNoAllocMaxDevices] = {};   // context the address belongs to
 
-// Device address of the scratch array on `device`, looked up once per device
-// with that device current (in host code the symbol is only a stand-in).
+// The current driver context of the calling thread (cuCtxGetCurrent, taken
+// through the runtime's driver entry point: the library does not link the
+// driver library itself). Null if it cannot be queried.
+void* current_context() {
+  using CtxGet = int (*)(void**);
+  static CtxGet fn = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      f = nullptr;
+    return reinterpret_cast<CtxGet>(f);
+  }();
+  void* ctx = nullptr;
+  if (fn == nullptr || fn(&ctx) != 0) return nullptr;
+  return ctx;
+}
+
+// Device address of the scratch array on `device`, looked up with that
+// device current (in host code the symbol is only a stand-in) the first time
+// and again whenever the device's context has changed since (after a device
+// reset the module is loaded anew and the array may move).
 mpmgpu_status noalloc_scratch(mpmgpu_handle* h, int device, unsigned char** out) {
   if (device < 0 || device >= kNoAllocMaxDevices) return hfail(h, MPMGPU_ERR_ARG, "device ordinal out of range");
   std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-  if (g_noalloc_base[device] == nullptr) {
-    int current = 0;
-    CUDA_TRY(h, cudaGetDevice(&current));
-    if (current != device) CUDA_TRY(h, cudaSetDevice(device));
+  int current = 0;
+  CUDA_TRY(h, cudaGetDevice(&current));
+  if (current != device) CUDA_TRY(h, cudaSetDevice(device));
+  void* ctx = current_context();
+  cudaError_t e = cudaSuccess;
+  if (g_noalloc_base[device] == nullptr || ctx != g_noalloc_ctx[device]) {
     void* p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (current != device) CUDA_TRY(h, cudaSetDevice(current));
-    if (e != cudaSuccess)
-      return hfail(h, MPMGPU_ERR_CUDA, std::string("cudaGetSymbolAddress(map scratch): ") + cudaGetErrorString(e));
-    g_noalloc_base[device] = static_cast<unsigned char*>(p);
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e == cudaSuccess) {
+      g_noalloc_base[device] = static_cast<unsigned char*>(p);
+      g_noalloc_ctx[device] = ctx;
+    }
   }
+  if (current != device) CUDA_TRY(h, cudaSetDevice(current));
+  if (e != cudaSuccess)
+    return hfail(h, MPMGPU_ERR_CUDA, std::string("cudaGetSymbolAddress(map scratch): ") + cudaGetErrorString(e));
   *out = g_noalloc_base[device];
   return MPMGPU_OK;
 }
@@ -601,6 +640,17 @@ extern "C" mpmgpu_status mpmgpu_dump_map_noalloc(mpmgpu_handle* h, int body, int
                  "mpmgpu_dump_map_noalloc: body has " + std::to_string(P.n) + " points x " + std::to_string(per_point) +
                      " triplet slots = " + std::to_string(nslots) + " slots, above the static scratch limit of " +
                      std::to_string(kNoAllocSlots));
+  cudaStream_t st = h->b->stream();
+  {
+    // the call ends with a wait for its result, which a stream under capture
+    // cannot do; refuse before queuing anything, so the caller's capture
+    // stays valid
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    CUDA_TRY(h, cudaStreamIsCapturing(st, &cs));
+    if (cs != cudaStreamCaptureStatusNone)
+      return hfail(h, MPMGPU_ERR_UNSUPPORTED,
+                   "mpmgpu_dump_map_noalloc waits for its result and cannot run while the handle's stream is captured");
+  }
   unsigned char* base = nullptr;
   TRY(noalloc_scratch(h, h->cfg.device, &base));
   int32_t* node = reinterpret_cast<int32_t*>(base + kNoAllocOffNode);
@@ -608,7 +658,6 @@ extern "C" mpmgpu_status mpmgpu_dump_map_noalloc(mpmgpu_handle* h, int body, int
   int32_t* blk = reinterpret_cast<int32_t*>(base + kNoAllocOffBlk);
   double* s = reinterpret_cast<double*>(base + kNoAllocOffS);
   double* grad = reinterpret_cast<double*>(base + kNoAllocOffGrad);
-  cudaStream_t st = h->b->stream();
   // every slot read below is written first by this call: nothing carries over
   if (P.n > 0) {
     if (g.dim == 3)

@@ -49,10 +49,15 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   return done != 0;
 }
 
+// Default poll limit of a bounded wait (a bulk copy lands within a few
+// microseconds; 2^24 polls are far longer).
+constexpr uint32_t kWaitPolls = 1u << 24;
+
 // Waits for the barrier phase with an iteration limit; on timeout sets
 // kErrWaitTimeout in *err and returns false.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, int* err) {
-  for (uint32_t it = 0; it < (1u << 24); it++)
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, int* err,
+                                                  uint32_t limit = kWaitPolls) {
+  for (uint32_t it = 0; it < limit; it++)
     if (mbar_try_wait(bar, parity)) return true;
   atomicOr(err, kErrWaitTimeout);
   return false;

@@ -23,6 +23,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -30,6 +31,7 @@
 
 #include "../../include/mpm_b200.h"
 #include "fused.cuh"
+#include "fused_lean.cuh"
 #include "kernels_fp64.cuh"
 #include "sort.cuh"
 
@@ -205,6 +207,9 @@ class BatchBase {
   virtual mpmgpu_status profile(int enable) = 0;
   virtual mpmgpu_status profile_read(int stage, int64_t* launches, double* ms) = 0;
   virtual mpmgpu_status autotune(int steps, int* best_cap) = 0;
+  // Poll limit of the fused kernels' waits for bulk copies (kWaitPolls by
+  // default); a wait that runs out makes the step report MPMGPU_ERR_DEVICE.
+  virtual void set_wait_limit(uint32_t polls) = 0;
   virtual int64_t memory_in_use() const = 0;
   virtual void counts(int* live_jobs, int64_t* live_points) const = 0;
   virtual int points_per_item() const = 0;
@@ -280,6 +285,8 @@ class Batch : public BatchBase {
       uint64_t keep = UINT64_MAX;
       MPM_CUDA_TRY(cudaMemPoolSetAttribute(pool_, cudaMemPoolAttrReleaseThreshold, &keep));
     }
+    if (const char* e = getenv("MPM_B200_LEAN")) lean_ = e[0] == '1' && dim_ == 3 && !det_;
+    if (lean_) cap_ = kLeanCap;
     if (cap_ == 0) cap_ = default_cap();
     if (!cap_available(dim_, mixed(), cap_) || (det_ && cap_ != default_cap()))
       return fail(MPMGPU_ERR_ARG, "points_per_item " + std::to_string(cap_) + " not available for this form");
@@ -536,6 +543,7 @@ class Batch : public BatchBase {
     if (flag & kErrWideSpan) return fail(MPMGPU_ERR_DEVICE, "point corners span more than two cells (extent > cell size)");
     if (flag & kErrElemAlias) return fail(MPMGPU_ERR_DEVICE, "point within rounding of the upper domain face");
     if (flag & kErrWaitTimeout) return fail(MPMGPU_ERR_DEVICE, "a bulk copy did not complete within the wait limit");
+    if (flag & kErrItemCap) return fail(MPMGPU_ERR_DEVICE, "a work item holds more points than the kernel takes");
     return MPMGPU_OK;
   }
 
@@ -910,6 +918,7 @@ class Batch : public BatchBase {
     const int caps[3] = {256, 512, 1024};
     for (int ci = 0; ci < 3 && st == MPMGPU_OK; ci++) {
       if (!cap_available(dim_, mixed(), caps[ci]) || (det_ && caps[ci] != default_cap())) continue;
+      if (lean_ && caps[ci] != kLeanCap) continue;
       cap_ = caps[ci];
       float ms = 0.0f;
       st = trial(steps, 1 << 30, &ms);
@@ -942,6 +951,11 @@ class Batch : public BatchBase {
   }
 
   int sort_interval() const override { return sort_interval_; }
+
+  void set_wait_limit(uint32_t polls) override {
+    wait_polls_ = polls;
+    drop_graphs();   // the limit travels in the launch arguments
+  }
 
  private:
   // ---- allocation helpers ----
@@ -1114,6 +1128,7 @@ class Batch : public BatchBase {
     if (flag & kErrWideSpan) return fail(MPMGPU_ERR_DEVICE, "point corners span more than two cells (extent > cell size)");
     if (flag & kErrElemAlias) return fail(MPMGPU_ERR_DEVICE, "point within rounding of the upper domain face");
     if (flag & kErrWaitTimeout) return fail(MPMGPU_ERR_DEVICE, "a bulk copy did not complete within the wait limit");
+    if (flag & kErrItemCap) return fail(MPMGPU_ERR_DEVICE, "a work item holds more points than the kernel takes");
     return MPMGPU_OK;
   }
 
@@ -1366,7 +1381,11 @@ class Batch : public BatchBase {
     ctx_host_ = ctx;
     single_mode_ = ctx.size() <= 4;
     any_plain_ = any_normal_ = false;
-    for (const auto& c : ctx) (c.needs_normal ? any_normal_ : any_plain_) = true;
+    all_elastic_ = true;
+    for (const auto& c : ctx) {
+      (c.needs_normal ? any_normal_ : any_plain_) = true;
+      if (c.mat.has_material && c.mat.kind != 0) all_elastic_ = false;
+    }
     drop_graphs();   // one-body launches carry the table entries in their arguments
     // block -> job slot map: only the ranges of joining jobs change
     for (auto& j : jobs_) {
@@ -1484,6 +1503,7 @@ class Batch : public BatchBase {
     fl.prime_pass = prime_pass;
     fl.phases = phases;
     fl.bounds = bounds_;
+    fl.wait_polls = wait_polls_;
     constexpr size_t smem = fused_smem_bytes<DIM, PT, CAP, NORMAL, DET>();
     auto kern = k_g2p2g<DIM, PT, CAP, NORMAL, SINGLE, DET>;
     // resident CTAs per SM, looked up once per kernel (before any capture)
@@ -1522,7 +1542,66 @@ class Batch : public BatchBase {
     return MPMGPU_OK;
   }
 
+  template <bool NORMAL, bool SINGLE, int MAT>
+  mpmgpu_status launch_lean_k(int prime_pass, int phases, int one_body) {
+    FusedLaunch<PT> fl{};
+    if (SINGLE) fl.one = ctx_host_[(size_t)one_body];
+    fl.one_body = SINGLE ? one_body : -1;
+    fl.bodies = ctx_d_;
+    fl.item_off = item_off_d_;
+    fl.nwork_body = nwork_body_;
+    fl.work_end_body = work_end_body_;
+    fl.flat_body = flat_body_;
+    fl.flat_item = flat_item_;
+    fl.nbodies_cap = (int)ctx_host_.size();
+    fl.work_bin = work_bin_;
+    fl.work_start = work_start_;
+    fl.work_end = work_end_;
+    fl.nwork = nwork_;
+    fl.err = err_;
+    fl.drift = drift_;
+    fl.prime_pass = prime_pass;
+    fl.phases = phases;
+    fl.bounds = nullptr;
+    fl.wait_polls = wait_polls_;
+    constexpr size_t smem = lean_smem_bytes<3, PT, NORMAL>();
+    auto kern = k_g2p2g_lean<3, PT, NORMAL, SINGLE, MAT>;
+    int& per_sm = lean_per_sm_[(NORMAL ? 4 : 0) + (SINGLE ? 2 : 0) + (MAT == 0 ? 1 : 0)];
+    if (per_sm == 0) {
+      MPM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      MPM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kLeanThreads, smem));
+      if (per_sm < 1) return fail(MPMGPU_ERR_CUDA, "fused kernel does not fit on an SM");
+    }
+    StageTimer timer(this, kStageFused);
+    kern<<<per_sm * sm_count_, kLeanThreads, smem, stream_>>>(fl);
+    return check_launch("k_g2p2g_lean");
+  }
+
+  template <bool NORMAL, bool SINGLE>
+  mpmgpu_status launch_lean_m(int prime_pass, int phases, int one_body, bool elastic) {
+    if (elastic) return launch_lean_k<NORMAL, SINGLE, 0>(prime_pass, phases, one_body);
+    return launch_lean_k<NORMAL, SINGLE, -1>(prime_pass, phases, one_body);
+  }
+
+  mpmgpu_status launch_lean(int prime_pass, int phases) {
+    if (single_mode_) {
+      for (size_t b = 0; b < ctx_host_.size(); b++) {
+        if (prime_pass && !ctx_host_[b].prime) continue;
+        const bool el = !ctx_host_[b].mat.has_material || ctx_host_[b].mat.kind == 0;
+        if (ctx_host_[b].needs_normal)
+          MPM_TRY((launch_lean_m<true, true>(prime_pass, phases, (int)b, el)));
+        else
+          MPM_TRY((launch_lean_m<false, true>(prime_pass, phases, (int)b, el)));
+      }
+      return MPMGPU_OK;
+    }
+    if (any_plain_) MPM_TRY((launch_lean_m<false, false>(prime_pass, phases, -1, all_elastic_)));
+    if (any_normal_) MPM_TRY((launch_lean_m<true, false>(prime_pass, phases, -1, all_elastic_)));
+    return MPMGPU_OK;
+  }
+
   mpmgpu_status launch_fused(int prime_pass, int phases) {
+    if (lean_ && dim_ == 3 && !det_) return launch_lean(prime_pass, phases);
     if constexpr (sizeof(PT) == 8) {
       if (det_) {
         // the deterministic form: 256 points per item in 3D (two tile levels)
@@ -1789,6 +1868,10 @@ class Batch : public BatchBase {
   std::vector<BodyCtx<PT>> ctx_host_;   // host copy of the body table
   bool single_mode_ = false;
   bool any_plain_ = false, any_normal_ = false;
+  bool all_elastic_ = true;              // every body IsotropicLinearElasticity (or no material)
+  bool lean_ = false;                    // the one-point-per-thread kernel (fused_lean.cuh)
+  uint32_t wait_polls_ = kWaitPolls;     // poll limit of the fused kernels' first waits
+  int lean_per_sm_[8] = {};
   int flip_ = 0;                        // point buffers swapped an odd number of times
   cudaStream_t stream_ = nullptr;
   std::vector<HJob> jobs_;

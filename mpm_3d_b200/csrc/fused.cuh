@@ -64,6 +64,10 @@ struct FusedLaunch {
   int prime_pass;   // 1: only bodies still to prime, scatter only
   int phases;       // 1: gather + point update, 2: map + scatter, 3: both
   const unsigned long long* bounds;  // deterministic form: 4 per body (k_det_bounds)
+  // poll limit of the waits for a work item's bulk copies; a wait that runs
+  // out flags kErrWaitTimeout and its CTA returns (after the copies in
+  // flight have landed, waited for with the default limit)
+  uint32_t wait_polls;
 };
 
 // Staged point arrays: x0..2 v0..2 u0..2 s0..5 vol m ext, then active.
@@ -892,7 +896,7 @@ __global__ void __launch_bounds__(fused_threads<PT, CAP>(), fused_min_ctas<PT, C
         mbar_arrive_expect_tx(bar_ctx + (slot ^ 1), kCtxBytes);
         bulk_copy_g2s(slot_ctx(slot ^ 1), fl.bodies + fl.flat_body[w + gridDim.x], kCtxBytes, bar_ctx + (slot ^ 1));
       }
-      const bool got = mbar_wait_bounded(bar_ctx + slot, (uint32_t)((k >> 1) & 1), fl.err);
+      const bool got = mbar_wait_bounded(bar_ctx + slot, (uint32_t)((k >> 1) & 1), fl.err, fl.wait_polls);
       if (__syncthreads_or(got ? 0 : 1)) {
         // let the copies in flight land before leaving
         if (threadIdx.x == 0) {
@@ -1014,7 +1018,7 @@ __global__ void __launch_bounds__(fused_threads<PT, CAP>(), fused_min_ctas<PT, C
         for (int t = threadIdx.x; t < TN; t += blockDim.x) touched[t] = 0;
       }
     }
-    const bool arrived = mbar_wait_bounded(bar, parity, fl.err);
+    const bool arrived = mbar_wait_bounded(bar, parity, fl.err, fl.wait_polls);
     // one decision for the whole CTA (also the barrier after the tile loads)
     if (__syncthreads_or(arrived ? 0 : 1)) {
       if (!arrived) mbar_wait_bounded(bar, parity, fl.err);  // let copies in flight land before leaving

@@ -1,0 +1,339 @@
+// Lean form of the fused gather + point update + scatter kernel: one point
+// per thread and no staged copy of the point arrays.
+//
+// A CTA of kLeanThreads threads works on one work item at a time (at most
+// kLeanThreads points of one bin of one body):
+//   0. every thread issues the global loads of its own point (coalesced:
+//      consecutive threads, consecutive points) while the CTA stages the
+//      nodal velocities of the bin's node tile and clears a separate FP64
+//      accumulator tile;
+//   1. one barrier; then each thread takes its point through gather, state
+//      update (movePoints, calculateStrainRate, updateDensity,
+//      updateStress), map build at the new position and scatter into the
+//      accumulator tile, with no barrier between the phases;
+//   2. one barrier; the touched tile nodes are added into the global
+//      accumulators (one global atomic per node and value).
+// Shared memory holds only the two tiles (about 41 KB in FP64, 31 KB in the
+// mixed form), so residency is set by registers. The material is a template
+// parameter (MAT >= 0 compiles one constitutive model; -1 dispatches at run
+// time), which keeps the other models' state out of the register budget.
+// The arithmetic of every phase is the one of the staged kernel (fused.cuh),
+// so both kernels give the same results.
+#pragma once
+
+#include "fused.cuh"
+
+namespace mpmb200 {
+
+constexpr int kLeanThreads = 256;
+constexpr int kLeanCap = kLeanThreads;   // points per work item
+
+// Resident CTAs per SM the register budget is sized for.
+template <typename PT>
+__host__ __device__ constexpr int lean_min_ctas() {
+  return sizeof(PT) == 4 ? 4 : 3;
+}
+
+// Shared memory: mbarriers | table entry slots [2] | velocity tile
+// [2 DIM][TN] in the point precision | accumulator tile [NACC][TN] FP64 |
+// touched [TN].
+template <int DIM, typename PT>
+__host__ __device__ constexpr size_t lean_off_tvel() {
+  return kOffCtx + 2 * ctx_bytes<PT>();
+}
+template <int DIM, typename PT>
+__host__ __device__ constexpr size_t lean_off_tacc() {
+  return (lean_off_tvel<DIM, PT>() + sizeof(PT) * 2 * DIM * fused_tile_nodes<DIM, fused_bin<DIM>()>() + 15) / 16 * 16;
+}
+template <int DIM, typename PT, bool NORMAL>
+__host__ __device__ constexpr size_t lean_off_touched() {
+  return lean_off_tacc<DIM, PT>() + sizeof(double) * fused_nacc(NORMAL) * fused_tile_nodes<DIM, fused_bin<DIM>()>();
+}
+template <int DIM, typename PT, bool NORMAL>
+__host__ __device__ constexpr size_t lean_smem_bytes() {
+  return lean_off_touched<DIM, PT, NORMAL>() + fused_tile_nodes<DIM, fused_bin<DIM>()>();
+}
+
+// Stress update of one point for material MAT (-1: the body's kind at run
+// time). s6 holds the stress before the step on entry, after it on exit.
+template <int DIM, int MAT, typename R, typename PT>
+__device__ __forceinline__ void lean_stress(const BodyCtx<PT>& c, int64_t p, const R L[3][3], R* s6, R m, R vol,
+                                            R dt) {
+  const PointsT<PT>& P = c.P;
+  const int kind = MAT >= 0 ? MAT : c.mat.kind;
+  if (kind == 1) {
+    neohookean_update<R>(P.ms, p, L, s6, (R)c.mat.G, (R)c.mat.lambda, dt);
+  } else if (kind == 2) {
+    sand_update<DIM, R>(P.ms, p, L, s6, m, vol, c.mat, dt);
+  } else {
+    jaumann_update<DIM, R>(L, s6, (R)c.mat.G, (R)c.mat.lambda, dt);
+  }
+}
+
+// One point through both phases. `a` is its active state (1 active, 2 left
+// the domain at the last move). The arithmetic follows gather_update and
+// map_scatter of the staged kernel.
+template <int DIM, int T, int TN, bool NORMAL, int MAT, typename PT>
+__device__ __forceinline__ void lean_point(const BodyCtx<PT>& c, int* err, unsigned long long* drift, int64_t p,
+                                           int a, const int* o, const PT* tvel, const double* vref, double* tacc,
+                                           uint8_t* touched, int do_g2p, bool do_p2g, int stepping) {
+  using R = PT;
+  const PointsT<PT>& P = c.P;
+  const R dt = (R)c.sp.dt;
+  const R ext = P.ext[p];
+  R x[3] = {R(0), R(0), R(0)}, u[3] = {R(0), R(0), R(0)};
+#pragma unroll
+  for (int d = 0; d < DIM; d++) {
+    x[d] = P.x[d][p];
+    if (sizeof(PT) == 4 || do_g2p) u[d] = P.u[d][p];
+  }
+  R v[3] = {R(0), R(0), R(0)}, s6[6], vol;
+  if (do_g2p) {
+    if (a == 2) {
+      // left the domain at the last move; generateMap deactivates it now
+      P.active[p] = 0;
+      return;
+    }
+    R xc[3] = {R(0), R(0), R(0)};
+#pragma unroll
+    for (int d = 0; d < DIM; d++) xc[d] = sizeof(PT) == 8 ? x[d] : x[d] + u[d];
+    GatherSum<R> gs;
+    {
+      PointMapT<R> pm;
+      const int st = build_map<DIM>(c.g, c.mc, c.sp.cpdi, xc, ext, pm, err);
+      if (st > 0) {
+        const bool in = window_in_tile<DIM>(pm, o, T);
+        const unsigned am = __activemask();
+        const unsigned inm = __ballot_sync(am, in);
+        if (in)
+          gs = gather_box_any<DIM, T, TN>(pm, o, tvel, __reduce_or_sync(inm, span_bits<DIM>(pm)));
+        else
+          gs = gather_general<DIM, T, TN>(c, drift, pm, o, tvel, vref);
+        if constexpr (sizeof(PT) == 4) {
+#pragma unroll
+          for (int d = 0; d < DIM; d++) gs.du[d] += (R)vref[d];
+        }
+      }
+    }
+    // movePoints (explicit_usl.cpp:279-292)
+#pragma unroll
+    for (int d = 0; d < DIM; d++) {
+      const R dx = dt * gs.du[d];
+      v[d] = P.v[d][p] + gs.dv[d];
+      u[d] = u[d] + dx;
+      if constexpr (sizeof(PT) == 8) {
+        x[d] = x[d] + dx;
+        P.x[d][p] = x[d];
+      }
+      P.v[d][p] = v[d];
+      P.u[d][p] = u[d];
+    }
+    vol = P.vol[p] * exp(dt * (gs.L[0][0] + gs.L[1][1] + gs.L[2][2]));
+    P.vol[p] = vol;
+#pragma unroll
+    for (int k = 0; k < 6; k++) s6[k] = P.s[k][p];
+    if (c.mat.has_material) {
+      lean_stress<DIM, MAT, R>(c, p, gs.L, s6, MAT == 2 || MAT < 0 ? P.m[p] : R(0), vol, dt);
+#pragma unroll
+      for (int k = 0; k < 6; k++) P.s[k][p] = s6[k];
+    }
+    if (P.L != nullptr) {
+#pragma unroll
+      for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) P.L[9 * p + 3 * i + j] = (double)gs.L[i][j];
+    }
+  } else {
+#pragma unroll
+    for (int d = 0; d < DIM; d++) v[d] = P.v[d][p];
+#pragma unroll
+    for (int k = 0; k < 6; k++) s6[k] = P.s[k][p];
+    vol = P.vol[p];
+  }
+  if (!do_p2g || a != 1) return;
+  // map build and scatter at the new position (mapPointsToNodes,
+  // explicit_usl.cpp:112-164; contact normal, contact_huang.cpp:91)
+  R xn[3] = {R(0), R(0), R(0)};
+#pragma unroll
+  for (int d = 0; d < DIM; d++) xn[d] = sizeof(PT) == 8 ? x[d] : x[d] + u[d];
+  PointMapT<R> pm;
+  const int st = build_map<DIM>(c.g, c.mc, c.sp.cpdi, xn, ext, pm, err);
+  if (st < 0) {
+    // outside the domain: inactive from the next map build on
+    // (default_points.cpp:217-219); before the first step, at once
+    P.active[p] = stepping ? 2 : 0;
+    return;
+  }
+  if (st == 0) return;
+  ScatterSrc<R> q;
+  q.m = P.m[p];
+#pragma unroll
+  for (int d = 0; d < 3; d++) q.mv[d] = d < DIM ? q.m * v[d] : R(0);
+  R vs[6];
+#pragma unroll
+  for (int k = 0; k < 6; k++) vs[k] = (DIM == 3 || k == 0 || k == 1 || k == 3) ? s6[k] * vol : R(0);
+  const R V3[3][3] = {{vs[0], vs[3], vs[5]}, {vs[3], vs[1], vs[4]}, {vs[5], vs[4], vs[2]}};
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int j = 0; j < 3; j++) q.V3[i][j] = V3[i][j];
+  const bool in = window_in_tile<DIM>(pm, o, T);
+  const unsigned am = __activemask();
+  const unsigned inm = __ballot_sync(am, in);
+  if (in)
+    scatter_box_any<DIM, T, TN, NORMAL, false>(pm, o, q, tacc, touched, nullptr,
+                                              __reduce_or_sync(inm, span_bits<DIM>(pm)));
+  else
+    scatter_general<DIM, T, TN, NORMAL, false>(c, drift, pm, o, q, tacc, touched, nullptr);
+}
+
+template <int DIM, typename PT, bool NORMAL, bool SINGLE, int MAT>
+__global__ void __launch_bounds__(kLeanThreads, lean_min_ctas<PT>())
+    k_g2p2g_lean(const __grid_constant__ FusedLaunch<PT> fl) {
+  constexpr int B = fused_bin<DIM>();
+  constexpr int T = B + 3;
+  constexpr int TN = fused_tile_nodes<DIM, B>();
+  constexpr int NACC = fused_nacc(NORMAL);
+  constexpr uint32_t kCtxBytes = (uint32_t)ctx_bytes<PT>();
+  extern __shared__ __align__(128) unsigned char smem[];
+  uint64_t* bar_ctx = reinterpret_cast<uint64_t*>(smem + 8);   // table entry slots 0, 1
+  auto slot_ctx = [&](int i) { return reinterpret_cast<BodyCtx<PT>*>(smem + kOffCtx + (size_t)i * kCtxBytes); };
+  PT* tvel = reinterpret_cast<PT*>(smem + lean_off_tvel<DIM, PT>());
+  double* tacc = reinterpret_cast<double*>(smem + lean_off_tacc<DIM, PT>());
+  uint8_t* touched = smem + lean_off_touched<DIM, PT, NORMAL>();
+
+  if (!SINGLE) {
+    if (threadIdx.x == 0) {
+      mbar_init(bar_ctx, 1);
+      mbar_init(bar_ctx + 1, 1);
+      mbar_init_fence();
+    }
+    __syncthreads();
+  }
+  const int nwork = SINGLE ? fl.nwork_body[fl.one_body] : *fl.nwork;
+  // launches over every body: the table entry of each work item arrives by
+  // a bulk copy issued one item ahead (slot k & 1 for the CTA's k-th item)
+  if (!SINGLE && threadIdx.x == 0 && (int)blockIdx.x < nwork) {
+    mbar_arrive_expect_tx(bar_ctx, kCtxBytes);
+    bulk_copy_g2s(slot_ctx(0), fl.bodies + fl.flat_body[blockIdx.x], kCtxBytes, bar_ctx);
+  }
+  int k = 0;
+  for (int w = blockIdx.x; w < nwork; w += gridDim.x, k++) {
+    int item;
+    if (SINGLE) {
+      item = fl.item_off[fl.one_body] + w;
+    } else {
+      item = fl.flat_item[w];
+      const int slot = k & 1;
+      const bool ahead = w + (int)gridDim.x < nwork;
+      if (threadIdx.x == 0 && ahead) {
+        // the other slot was last read by the previous item (all threads
+        // passed its closing barrier)
+        fence_async_shared();
+        mbar_arrive_expect_tx(bar_ctx + (slot ^ 1), kCtxBytes);
+        bulk_copy_g2s(slot_ctx(slot ^ 1), fl.bodies + fl.flat_body[w + gridDim.x], kCtxBytes, bar_ctx + (slot ^ 1));
+      }
+      const bool got = mbar_wait_bounded(bar_ctx + slot, (uint32_t)((k >> 1) & 1), fl.err, fl.wait_polls);
+      if (__syncthreads_or(got ? 0 : 1)) {
+        // let the copies in flight land before leaving
+        if (threadIdx.x == 0) {
+          if (!got) mbar_wait_bounded(bar_ctx + slot, (uint32_t)((k >> 1) & 1), fl.err);
+          if (ahead) mbar_wait_bounded(bar_ctx + (slot ^ 1), (uint32_t)(((k + 1) >> 1) & 1), fl.err);
+        }
+        return;
+      }
+    }
+    const BodyCtx<PT>& c = SINGLE ? fl.one : *slot_ctx(k & 1);
+    if (!SINGLE) {
+      // items of the other kind (contact normal or not) belong to the other launch
+      if ((c.needs_normal != 0) != NORMAL) {
+        __syncthreads();
+        continue;
+      }
+    }
+    const int prime = c.prime;
+    if (fl.prime_pass && !prime) {
+      __syncthreads();   // every thread has read the staged entry
+      continue;
+    }
+    const int do_g2p = (prime || !(fl.phases & 1)) ? 0 : 1;
+    const bool do_p2g = (fl.phases & 2) != 0;
+    const PointsT<PT>& P = c.P;
+    const Geom& g = c.g;
+    const int bin = fl.work_bin[item];
+    const int64_t pstart = fl.work_start[item];
+    const int n = fl.work_end[item] - (int)pstart;
+    if (n > kLeanCap && threadIdx.x == 0) atomicOr(fl.err, kErrItemCap);   // the work list was cut for another size
+    const int j = threadIdx.x;
+    const int64_t p = pstart + j;
+    const int a = j < n ? P.active[p] : 0;
+    int o[3] = {0, 0, 0};
+    {
+      const int bx = bin % c.bg.nbx;
+      const int r = bin / c.bg.nbx;
+      o[0] = bx * B - 1;
+      o[1] = (r % c.bg.nby) * B - 1;
+      o[2] = DIM == 3 ? (r / c.bg.nby) * B - 1 : 0;
+    }
+    // reference velocity of the mixed form: the item's first point (any
+    // value is exact; one close to the item's velocities keeps the
+    // differences small)
+    double vref[3] = {0.0, 0.0, 0.0};
+    if (do_g2p) {
+      if constexpr (sizeof(PT) == 4) {
+#pragma unroll
+        for (int d = 0; d < DIM; d++) vref[d] = (double)P.v[d][pstart];
+      }
+      // nodal velocities of the tile: each thread issues the loads of up to
+      // two nodes before its first shared-memory store
+      constexpr int ITER = (TN + kLeanThreads - 1) / kLeanThreads;
+      constexpr int CH = ITER > 2 ? 2 : ITER;
+#pragma unroll 1
+      for (int it0 = 0; it0 < ITER; it0 += CH) {
+        double vv[CH][2 * DIM];
+        int tt[CH];
+#pragma unroll
+        for (int ic = 0; ic < CH; ic++) {
+          const int t = (int)threadIdx.x + (it0 + ic) * kLeanThreads;
+          tt[ic] = -1;
+          int tx, ty, tz;
+          if (t >= TN || !TileLayout<DIM, T>::node(t, tx, ty, tz)) continue;
+          const int i = o[0] + tx, jj = o[1] + ty, kk = o[2] + tz;
+          if (i < 0 || jj < 0 || kk < 0 || i >= g.nn[0] || jj >= g.nn[1] || kk >= g.nn[2]) continue;
+          const int64_t s = node_slot(g, i, jj, kk);
+          tt[ic] = t;
+#pragma unroll
+          for (int d = 0; d < DIM; d++) {
+            vv[ic][d] = c.V.vt[d][s];
+            vv[ic][DIM + d] = c.V.dv[d][s];
+          }
+        }
+#pragma unroll
+        for (int ic = 0; ic < CH; ic++) {
+          const int t = tt[ic];
+          if (t < 0) continue;
+#pragma unroll
+          for (int d = 0; d < DIM; d++) {
+            tvel[d * TN + t] = (PT)(vv[ic][d] - vref[d]);
+            tvel[(3 + d) * TN + t] = (PT)vv[ic][DIM + d];
+          }
+        }
+      }
+    }
+    if (do_p2g) {
+      for (int t = threadIdx.x; t < NACC * TN; t += kLeanThreads) tacc[t] = 0.0;
+      for (int t = threadIdx.x; t < TN; t += kLeanThreads) touched[t] = 0;
+    }
+    __syncthreads();
+    if (a != 0)
+      lean_point<DIM, T, TN, NORMAL, MAT>(c, fl.err, fl.drift, p, a, o, tvel, vref, tacc, touched, do_g2p, do_p2g,
+                                          prime ? 0 : 1);
+    if (do_p2g) {
+      __syncthreads();
+      flush_tile<DIM, T, TN, NORMAL, false>(c, g, o, tacc, touched);
+    }
+    __syncthreads();
+  }
+}
+
+}  // namespace mpmb200

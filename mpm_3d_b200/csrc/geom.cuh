@@ -13,6 +13,7 @@ constexpr int kMaxContacts = 8;
 // Device error flags (bit mask in one int).
 constexpr int kErrWideSpan = 1;     // corner spread wider than one cell
 constexpr int kErrElemAlias = 2;    // floor(x/L*N) == N for x < L (reference UB)
+constexpr int kErrItemCap = 8;      // a work item larger than the kernel's points per item
 
 // Uniform Cartesian grid (CartesianLinear, src/objects/grids/cartesian.cpp)
 // and its node storage. Nodes are stored block-linear: blocks of

@@ -36,7 +36,7 @@ class Server {
   };
   struct Request {
     int job = -1;
-    int state = 0;  // 1 running, 4 copying out, 2 done, 3 released
+    int state = 0;  // 1 running, 4 copying out, 2 done, 3 released, 5 cancelled
     int64_t footprint = 0;
     int64_t points = 0;
     int64_t steps = 0;
@@ -44,8 +44,8 @@ class Server {
     std::vector<Result> bodies;
   };
 
-  Server(std::unique_ptr<BatchBase> b, bool mixed, bool keep_debug, int64_t budget)
-      : batch_(std::move(b)), mixed_(mixed), keep_debug_(keep_debug), budget_(budget),
+  Server(std::unique_ptr<BatchBase> b, int mode, bool keep_debug, int64_t budget)
+      : batch_(std::move(b)), mode_(mode), keep_debug_(keep_debug), budget_(budget),
         t0_(std::chrono::steady_clock::now()) {}
 
   ~Server() {
@@ -62,7 +62,7 @@ class Server {
     return s;
   }
 
-  int mode() const { return mixed_ ? MPMGPU_MODE_MIXED : MPMGPU_MODE_FP64; }
+  int mode() const { return mode_; }
 
   double clock() const {
     return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0_).count();
@@ -76,9 +76,9 @@ class Server {
     return MPMGPU_OK;
   }
 
-  // Admits the request if its footprint fits the budget now (or nothing is
-  // running, so that a request larger than the budget still runs alone).
-  // MPMGPU_ERR_STATE: does not fit now, retry later.
+  // Admits the request if its footprint fits the budget left now.
+  // MPMGPU_ERR_STATE: does not fit now, retry later. MPMGPU_ERR_NOMEM: the
+  // footprint exceeds the whole budget, so the request can never run.
   mpmgpu_status submit(const mpmgpu_job_desc& d, int* id) {
     if (!d.grid || d.nbodies < 1 || !d.bodies || d.nbodies > kMaxBodies || d.ncontacts < 0 ||
         (d.ncontacts > 0 && !d.contacts))
@@ -88,7 +88,10 @@ class Server {
     mpmgpu_config cfg = *d.grid;
     cfg.dim = batch_->dim();
     const int64_t fp = job_footprint(cfg, mode(), keep_debug_, d.bodies, d.nbodies, d.ncontacts);
-    if (running_ > 0 && reserved_ + fp > budget_) return fail(MPMGPU_ERR_STATE, "request does not fit the memory budget now");
+    if (fp > budget_)
+      return fail(MPMGPU_ERR_NOMEM, "request footprint of " + std::to_string(fp) + " bytes exceeds the whole budget of " +
+                                        std::to_string(budget_) + " bytes");
+    if (reserved_ + fp > budget_) return fail(MPMGPU_ERR_STATE, "request does not fit the memory budget now");
     int job = -1;
     mpmgpu_status st = batch_->new_job(cfg, d.steps, &job);
     for (int b = 0; b < d.nbodies && st == MPMGPU_OK; b++) st = batch_->add_body(job, d.bodies[b], nullptr);
@@ -180,6 +183,24 @@ class Server {
       default: return fail(MPMGPU_ERR_UNSUPPORTED, "the server keeps x, u, x_t, T, v and active");
     }
     std::copy(src->begin(), src->end(), out);
+    return MPMGPU_OK;
+  }
+
+  // Cancels a running request between advances: its job leaves the batch at
+  // the next step boundary (the steps already queued finish with it, in
+  // stream order), its device memory returns to the pool and its footprint
+  // to the budget. The other requests' results do not change: every job
+  // steps on its own nodes and points.
+  mpmgpu_status cancel(int id) {
+    if (id < 0 || id >= (int)reqs_.size()) return fail(MPMGPU_ERR_ARG, "no such request");
+    Request& r = reqs_[(size_t)id];
+    if (r.state != 1) return fail(MPMGPU_ERR_STATE, "request is not running");
+    mpmgpu_status st = batch_->remove_job(r.job);
+    if (st != MPMGPU_OK) return fail(st, batch_->last_error);
+    r.state = 5;
+    r.t_done = clock();
+    running_--;
+    reserved_ -= r.footprint;
     return MPMGPU_OK;
   }
 
@@ -303,7 +324,7 @@ class Server {
   }
 
   std::unique_ptr<BatchBase> batch_;
-  bool mixed_;
+  int mode_;
   bool keep_debug_;
   int64_t budget_;
   std::chrono::steady_clock::time_point t0_;

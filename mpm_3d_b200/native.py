@@ -113,6 +113,7 @@ def load() -> ctypes.CDLL:
     lib.mpmgpu_stream.restype = vp
     lib.mpmgpu_stream.argtypes = [vp]
     lib.mpmgpu_profile.argtypes = [vp, ctypes.c_int]
+    lib.mpmgpu_set_wait_limit.argtypes = [vp, ctypes.c_uint32]
     lib.mpmgpu_profile_read.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_double)]
     lib.mpmgpu_destroy.argtypes = [vp]
     i64p = ctypes.POINTER(ctypes.c_int64)
@@ -152,6 +153,7 @@ def load() -> ctypes.CDLL:
                                           ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double), i64p, i64p]
     lib.mpmgpu_server_result.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp]
     lib.mpmgpu_server_release.argtypes = [vp, ctypes.c_int]
+    lib.mpmgpu_server_cancel.argtypes = [vp, ctypes.c_int]
     lib.mpmgpu_server_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_int), i64p, i64p, i64p]
     lib.mpmgpu_server_clock.restype = ctypes.c_double
     lib.mpmgpu_server_clock.argtypes = [vp]
@@ -262,6 +264,11 @@ class GPUExplicitUSL:
         return int(self.lib.mpmgpu_stream(self.h) or 0)
 
     STAGES = {"g2p2g": 0, "grid": 1, "compact": 2, "rebin": 3}
+
+    def set_wait_limit(self, polls: int):
+        """Poll limit of the fused kernel's waits for bulk copies (2^24 by
+        default); a wait that runs out makes the next synchronize raise."""
+        self._check(self.lib.mpmgpu_set_wait_limit(self.h, polls))
 
     def active_nodes(self) -> Tuple[int, int]:
         """(nodes with mass in the last step, per body; drifted point visits)."""
@@ -487,6 +494,7 @@ class GPUBatch:
         return int(self.lib.mpmgpu_batch_launch_count(self.h))
 
 
+STATUS_NOMEM = 3
 STATUS_STATE = 5
 
 
@@ -536,6 +544,8 @@ class GPUServer:
         st = self.lib.mpmgpu_server_submit(self.h, ctypes.byref(desc), ctypes.byref(rid))
         if st == STATUS_STATE:
             return None
+        if st == STATUS_NOMEM:
+            return -1   # larger than the whole budget: can never run
         self._check(st)
         self.cases[rid.value] = case
         return rid.value
@@ -566,6 +576,12 @@ class GPUServer:
 
     def release(self, rid: int):
         self._check(self.lib.mpmgpu_server_release(self.h, rid))
+        self.cases.pop(rid, None)
+
+    def cancel(self, rid: int):
+        """Cancels a running request (it leaves the batch at the next step
+        boundary; the other requests are unaffected)."""
+        self._check(self.lib.mpmgpu_server_cancel(self.h, rid))
         self.cases.pop(rid, None)
 
     def stats(self) -> Dict[str, int]:

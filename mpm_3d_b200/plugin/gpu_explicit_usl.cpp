@@ -1,6 +1,7 @@
 // GPUExplicitUSL: mpm_3d Solver plugin over the C ABI of include/mpm_b200.h.
-// Compiled inside the reference tree; it uses only the
-// reference's public object interface.
+// Compiled together with the reference's sources (registered as
+// REGISTER(Solver, GPUExplicitUSL)); it uses only the reference's public
+// object interface.
 #include "gpu_explicit_usl.hpp"
 
 #include <cmath>

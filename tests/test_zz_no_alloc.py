@@ -1,16 +1,18 @@
 """The allocation-free map export, mpmgpu_dump_map_noalloc.
 
-Callers that cannot allocate device memory at the point of the call (code
-running under CUDA graph capture, frameworks that own all device memory
-through their own pools, real-time loops that forbid cudaMalloc after
-set-up) read the S / gradS triplets through this entry point: it keeps its
-scratch in a static device array of the library and writes into device
-arrays the caller already owns. This test owns those arrays (allocated here
-with torch), calls the entry point through the C ABI twice in a row (at the
-initial positions and after some steps, so the second call reuses scratch
-the first call left behind), and checks each result against the allocating
-entry point mpmgpu_dump_map, bit for bit. It also checks that a body above
-the static scratch limit is rejected with an error instead of being served.
+Callers that cannot allocate device memory at the point of the call
+(frameworks that own all device memory through their own pools, real-time
+loops that forbid cudaMalloc after set-up) read the S / gradS triplets
+through this entry point: it keeps its scratch in a static device array of
+the library and writes into device arrays the caller already owns. This test
+owns those arrays (allocated here with torch), calls the entry point through
+the C ABI twice in a row (at the initial positions and after some steps, so
+the second call reuses scratch the first call left behind), and checks each
+result against the allocating entry point mpmgpu_dump_map, bit for bit, and
+that the second call leaves the device's free memory unchanged. It also
+checks that a body above the static scratch limit is rejected with an error
+instead of being served, and that a call while the handle's stream is being
+captured into a CUDA graph is refused without breaking the capture.
 
 The file name makes pytest collect it last, so a run that stops at the first
 failure has already run every other test.
@@ -67,4 +69,50 @@ def test_noalloc_map_rejects_bodies_above_the_scratch_limit():
     bufs = _device_buffers(torch, 16)
     with pytest.raises(MpmGpuError, match="static scratch limit"):
         _noalloc_map(sim, 0, bufs, 16)
+    sim.close()
+
+
+def test_noalloc_map_allocates_no_device_memory():
+    torch = pytest.importorskip("torch")
+    # 8,000 points per body: 512,000 slots, just under the scratch limit, so
+    # that slot buffers taken from cudaMalloc (about 18 MB) would show
+    case = inputs.two_body_collision_3d(40, steps=2, gap=0.01)
+    sim = GPUExplicitUSL(case)
+    capacity = max(b.n for b in case.bodies) * 64
+    assert capacity <= 1 << 19
+    bufs = _device_buffers(torch, capacity)
+    want = sim.map(0)
+    first = _noalloc_map(sim, 0, bufs, capacity)
+    torch.cuda.synchronize()
+    free_before = torch.cuda.mem_get_info()[0]
+    node, pt, s_, g = bufs
+    n = sim.map_noalloc(0, node.data_ptr(), pt.data_ptr(), s_.data_ptr(), g.data_ptr(), capacity)
+    torch.cuda.synchronize()
+    free_after = torch.cuda.mem_get_info()[0]
+    assert free_after == free_before
+    assert n == len(want[0]) == len(first[0])
+    assert np.array_equal(node[:n].cpu().numpy(), want[0]) and bits_equal(s_[:n].cpu().numpy(), want[2])
+    sim.close()
+
+
+def test_noalloc_map_refuses_a_captured_stream():
+    torch = pytest.importorskip("torch")
+    case = inputs.two_body_collision_3d(16, steps=2, gap=0.01)
+    sim = GPUExplicitUSL(case)
+    capacity = max(b.n for b in case.bodies) * 64
+    bufs = _device_buffers(torch, capacity)
+    want = _noalloc_map(sim, 0, bufs, capacity)
+    stream = torch.cuda.ExternalStream(sim.stream())
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.stream(stream):
+        graph.capture_begin()
+        try:
+            with pytest.raises(MpmGpuError, match="captured"):
+                _noalloc_map(sim, 0, bufs, capacity)
+        finally:
+            graph.capture_end()   # the capture is still valid: it ends without an error
+    del graph
+    # and the handle still serves the call once the capture is over
+    got = _noalloc_map(sim, 0, bufs, capacity)
+    assert np.array_equal(got[0], want[0]) and bits_equal(got[2], want[2])
     sim.close()
