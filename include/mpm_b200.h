@@ -9,9 +9,10 @@
  *   Solver::init / lazy first step   -> mpmgpu_create, mpmgpu_add_body,
  *                                       mpmgpu_add_contact, mpmgpu_set_gravity
  *   Solver::step                     -> mpmgpu_step
- *   frame output / end of run        -> mpmgpu_download_points,
- *                                       mpmgpu_download_nodes,
- *                                       mpmgpu_download_contact
+ *   frame output / end of run        -> mpmgpu_frame_begin, mpmgpu_frame_points,
+ *                                       mpmgpu_frame_nodes, mpmgpu_frame_contact
+ *                                       (or mpmgpu_download_points / _nodes /
+ *                                       _contact, one field at a time)
  *   Job teardown                     -> mpmgpu_destroy
  *
  * All pointers passed in are HOST pointers unless a function says otherwise;
@@ -190,6 +191,22 @@ mpmgpu_status mpmgpu_synchronize(mpmgpu_handle* h);
 mpmgpu_status mpmgpu_download_points(mpmgpu_handle* h, int body, int field, double* out);
 mpmgpu_status mpmgpu_download_nodes(mpmgpu_handle* h, int body, int field, double* out);
 mpmgpu_status mpmgpu_download_contact(mpmgpu_handle* h, int contact, int field, double* out);
+
+/* The write-back behind a frame (DefaultPoints::writeFrame,
+ * default_points.cpp:341-368; DefaultNodes::writeFrame,
+ * default_nodes.cpp:68-82; the contact arrays of ContactHuang::writeFrame,
+ * contact_huang.cpp:202-206) in two halves. mpmgpu_frame_begin queues, behind
+ * the steps queued so far, copies of every body's point, node and contact
+ * fields into pinned host memory, and returns without waiting; steps queued
+ * after it run while the copies are converted. mpmgpu_frame_points / _nodes
+ * / _contact then give one field in the layout of the mpmgpu_download_*
+ * call of the same name, as it stood at mpmgpu_frame_begin (the first of
+ * them waits for the copies). A frame stays readable until the next
+ * mpmgpu_frame_begin. */
+mpmgpu_status mpmgpu_frame_begin(mpmgpu_handle* h);
+mpmgpu_status mpmgpu_frame_points(mpmgpu_handle* h, int body, int field, double* out);
+mpmgpu_status mpmgpu_frame_nodes(mpmgpu_handle* h, int body, int field, double* out);
+mpmgpu_status mpmgpu_frame_contact(mpmgpu_handle* h, int contact, int field, double* out);
 
 /* Rebuilds the S / gradS maps of body b for the current positions (the
  * first stage of ExplicitUSL::step, DefaultPoints::generateMap,

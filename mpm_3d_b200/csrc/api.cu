@@ -224,6 +224,26 @@ mpmgpu_status mpmgpu_download_contact(mpmgpu_handle* h, int contact, int field, 
   return h->b->download_contact(h->job, contact, field, out);
 }
 
+mpmgpu_status mpmgpu_frame_begin(mpmgpu_handle* h) {
+  if (!h) return MPMGPU_ERR_ARG;
+  return h->b->frame_begin(h->job);
+}
+
+mpmgpu_status mpmgpu_frame_points(mpmgpu_handle* h, int body, int field, double* out) {
+  if (!h || !out) return MPMGPU_ERR_ARG;
+  return h->b->frame_points(h->job, body, field, out);
+}
+
+mpmgpu_status mpmgpu_frame_nodes(mpmgpu_handle* h, int body, int field, double* out) {
+  if (!h || !out) return MPMGPU_ERR_ARG;
+  return h->b->frame_nodes(h->job, body, field, out);
+}
+
+mpmgpu_status mpmgpu_frame_contact(mpmgpu_handle* h, int contact, int field, double* out) {
+  if (!h || !out) return MPMGPU_ERR_ARG;
+  return h->b->frame_contact(h->job, contact, field, out);
+}
+
 mpmgpu_status mpmgpu_dump_map(mpmgpu_handle* h, int body, int32_t* node, int32_t* point, double* s_val, double* grad,
                               int64_t* count) {
   if (!h || !count) return MPMGPU_ERR_ARG;

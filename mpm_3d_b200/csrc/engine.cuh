@@ -26,6 +26,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <memory>
+#include <set>
 #include <string>
 #include <vector>
 
@@ -203,6 +204,16 @@ class BatchBase {
                                double* active) const = 0;
   virtual mpmgpu_status download_nodes(int job, int body, int field, double* out) = 0;
   virtual mpmgpu_status download_contact(int job, int contact, int field, double* out) = 0;
+  // Frames: every body's point, node and contact fields of a job copied to
+  // pinned host memory behind the work queued so far, without waiting
+  // (frame_begin); frame_points / _nodes / _contact wait for those copies
+  // (once) and convert one field to the reference layout, while later work
+  // queued on the stream runs. A frame stays readable until the next
+  // frame_begin.
+  virtual mpmgpu_status frame_begin(int job) = 0;
+  virtual mpmgpu_status frame_points(int job, int body, int field, double* out) = 0;
+  virtual mpmgpu_status frame_nodes(int job, int body, int field, double* out) = 0;
+  virtual mpmgpu_status frame_contact(int job, int contact, int field, double* out) = 0;
   virtual mpmgpu_status sizes(int job, int body, int64_t* n_points, int64_t* n_nodes) const = 0;
   virtual mpmgpu_status profile(int enable) = 0;
   virtual mpmgpu_status profile_read(int stage, int64_t* launches, double* ms) = 0;
@@ -285,10 +296,13 @@ class Batch : public BatchBase {
       uint64_t keep = UINT64_MAX;
       MPM_CUDA_TRY(cudaMemPoolSetAttribute(pool_, cudaMemPoolAttrReleaseThreshold, &keep));
     }
-    if (const char* e = getenv("MPM_B200_LEAN")) lean_ = e[0] == '1' && dim_ == 3 && !det_;
-    if (lean_) cap_ = kLeanCap;
+    if (const char* e = getenv("MPM_B200_LEAN")) {
+      const int v = atoi(e);
+      lean_nt_ = (dim_ == 3 && !det_ && lean_size_ok(v)) ? v : 0;
+    }
+    if (lean_nt_ > 0) cap_ = lean_nt_;
     if (cap_ == 0) cap_ = default_cap();
-    if (!cap_available(dim_, mixed(), cap_) || (det_ && cap_ != default_cap()))
+    if ((lean_nt_ == 0 && !cap_available(dim_, mixed(), cap_)) || (det_ && cap_ != default_cap()))
       return fail(MPMGPU_ERR_ARG, "points_per_item " + std::to_string(cap_) + " not available for this form");
     if (det_ && mixed()) return fail(MPMGPU_ERR_UNSUPPORTED, "the deterministic form is FP64");
     MPM_TRY(alloc_raw(&hdr_, 1, scratch_allocs_));
@@ -317,6 +331,8 @@ class Batch : public BatchBase {
     if (pool_) cudaMemPoolDestroy(pool_);
     if (stage_) cudaFreeHost(stage_);
     if (dl_stage_) cudaFreeHost(dl_stage_);
+    if (frame_stage_) cudaFreeHost(frame_stage_);
+    if (frame_ev_) cudaEventDestroy(frame_ev_);
     if (upload_ev_) cudaEventDestroy(upload_ev_);
     if (copy_stream_) cudaStreamDestroy(copy_stream_);
     if (stream_) cudaStreamDestroy(stream_);
@@ -614,121 +630,307 @@ class Batch : public BatchBase {
 
   // ---- downloads (reference layout, original point order) ----
 
-  mpmgpu_status download_points(int job, int body, int field, double* out) override {
-    HJob* j;
-    HBody* B;
-    MPM_TRY(readable_body(job, body, &j, &B));
-    const int64_t n = B->n;
-    const size_t nz = (size_t)n;
-    const int D = dim_;
-    if (field == MPMGPU_P_B) {
-      MPM_TRY(synchronize());
-      for (int64_t i = 0; i < n; i++)
-        for (int d = 0; d < 3; d++) out[3 * i + d] = j->sp.grav[d];
-      return MPMGPU_OK;
+  // Host views of one body's point arrays (copies in pinned memory), from
+  // which fields are converted to the reference's layout and point order.
+  struct PointView {
+    int64_t n = 0;
+    const int32_t* pid = nullptr;
+    const int32_t* active = nullptr;
+    const PT* x[3] = {};
+    const PT* u[3] = {};
+    const PT* v[3] = {};
+    const PT* s[6] = {};
+    const PT* vol = nullptr;
+    const PT* m = nullptr;
+    const PT* ext = nullptr;
+    const PT* ms[2] = {};
+    const double* L = nullptr;
+  };
+
+  static bool point_field_known(int field) {
+    switch (field) {
+      case MPMGPU_P_X: case MPMGPU_P_U: case MPMGPU_P_X_T: case MPMGPU_P_MX_T: case MPMGPU_P_L: case MPMGPU_P_T:
+      case MPMGPU_P_M: case MPMGPU_P_V: case MPMGPU_P_EXTENT: case MPMGPU_P_ACTIVE: case MPMGPU_P_GAMMAP:
+      case MPMGPU_P_GAMMAP_DOT:
+        return true;
     }
-    if (field == MPMGPU_P_L && !B->P.L) return fail(MPMGPU_ERR_STATE, "L is kept only with keep_debug in the FP64 form");
-    if ((field == MPMGPU_P_GAMMAP || field == MPMGPU_P_GAMMAP_DOT) && B->mat.kind != 2)
-      return fail(MPMGPU_ERR_STATE, "gammap and gammap_dot belong to Sand_SachithLocal bodies");
-    // the point ids and the arrays of the field, copied with one wait
-    std::vector<std::pair<const void*, size_t>> items;
-    items.emplace_back(B->P.pid, nz * sizeof(int32_t));
-    const size_t np = nz * sizeof(PT);
+    return false;
+  }
+
+  // The device arrays a point field is converted from (the point ids
+  // first): add(source, bytes, slot of the view that receives its copy).
+  template <typename F>
+  void point_field_arrays(const HBody& B, int field, PointView& v, F&& add) const {
+    const size_t nz = (size_t)B.n, np = nz * sizeof(PT);
+    const int D = dim_;
+    auto slot = [](auto& p) { return reinterpret_cast<const void**>(&p); };
+    add(B.P.pid, nz * sizeof(int32_t), slot(v.pid));
     switch (field) {
       case MPMGPU_P_X:
-        for (int d = 0; d < D; d++) items.emplace_back(B->P.x[d], np);
+        for (int d = 0; d < D; d++) add(B.P.x[d], np, slot(v.x[d]));
         if constexpr (sizeof(PT) == 4)
-          for (int d = 0; d < D; d++) items.emplace_back(B->P.u[d], np);
+          for (int d = 0; d < D; d++) add(B.P.u[d], np, slot(v.u[d]));
         break;
       case MPMGPU_P_U:
-        for (int d = 0; d < D; d++) items.emplace_back(B->P.u[d], np);
+        for (int d = 0; d < D; d++) add(B.P.u[d], np, slot(v.u[d]));
         break;
       case MPMGPU_P_X_T:
-        for (int d = 0; d < D; d++) items.emplace_back(B->P.v[d], np);
+        for (int d = 0; d < D; d++) add(B.P.v[d], np, slot(v.v[d]));
         break;
       case MPMGPU_P_MX_T:
-        for (int d = 0; d < D; d++) items.emplace_back(B->P.v[d], np);
-        items.emplace_back(B->P.m, np);
+        for (int d = 0; d < D; d++) add(B.P.v[d], np, slot(v.v[d]));
+        add(B.P.m, np, slot(v.m));
         break;
-      case MPMGPU_P_L: items.emplace_back(B->P.L, nz * 9 * sizeof(double)); break;
+      case MPMGPU_P_L: add(B.P.L, nz * 9 * sizeof(double), slot(v.L)); break;
       case MPMGPU_P_T:
-        for (int c = 0; c < 6; c++) items.emplace_back(B->P.s[c], np);
+        for (int c = 0; c < 6; c++) add(B.P.s[c], np, slot(v.s[c]));
         break;
-      case MPMGPU_P_M: items.emplace_back(B->P.m, np); break;
-      case MPMGPU_P_V: items.emplace_back(B->P.vol, np); break;
-      case MPMGPU_P_EXTENT: items.emplace_back(B->P.ext, np); break;
-      case MPMGPU_P_ACTIVE: items.emplace_back(B->P.active, nz * sizeof(int32_t)); break;
-      case MPMGPU_P_GAMMAP: items.emplace_back(B->P.ms[0], np); break;
-      case MPMGPU_P_GAMMAP_DOT: items.emplace_back(B->P.ms[1], np); break;
-      default: return fail(MPMGPU_ERR_ARG, "unknown point field");
+      case MPMGPU_P_M: add(B.P.m, np, slot(v.m)); break;
+      case MPMGPU_P_V: add(B.P.vol, np, slot(v.vol)); break;
+      case MPMGPU_P_EXTENT: add(B.P.ext, np, slot(v.ext)); break;
+      case MPMGPU_P_ACTIVE: add(B.P.active, nz * sizeof(int32_t), slot(v.active)); break;
+      case MPMGPU_P_GAMMAP: add(B.P.ms[0], np, slot(v.ms[0])); break;
+      case MPMGPU_P_GAMMAP_DOT: add(B.P.ms[1], np, slot(v.ms[1])); break;
     }
-    std::vector<const unsigned char*> h;
-    MPM_TRY(fetch(items, h));
-    const int32_t* pid = reinterpret_cast<const int32_t*>(h[0]);
-    auto arr = [&](size_t k) { return reinterpret_cast<const PT*>(h[k]); };
-    auto vec3 = [&](size_t first) {
+  }
+
+  // One point field from host views, in the layout of mpmgpu_download_points
+  // and the reference's point order (pid).
+  void points_to_ref(const PointView& v, int field, double* out) const {
+    const int64_t n = v.n;
+    const size_t nz = (size_t)n;
+    const int D = dim_;
+    const int32_t* pid = v.pid;
+    auto vec3 = [&](const PT* const* a) {
       for (int64_t i = 0; i < 3 * n; i++) out[i] = 0.0;
-      for (int d = 0; d < D; d++) {
-        const PT* a = arr(first + (size_t)d);
-        for (size_t i = 0; i < nz; i++) out[3 * (int64_t)pid[i] + d] = (double)a[i];
-      }
+      for (int d = 0; d < D; d++)
+        for (size_t i = 0; i < nz; i++) out[3 * (int64_t)pid[i] + d] = (double)a[d][i];
+    };
+    auto scalar = [&](const PT* a) {
+      for (size_t i = 0; i < nz; i++) out[pid[i]] = (double)a[i];
     };
     switch (field) {
       case MPMGPU_P_X:
         if constexpr (sizeof(PT) == 4) {
           // the mixed form keeps x0 in the x arrays: x = x0 + u (in FP32)
           for (int64_t i = 0; i < 3 * n; i++) out[i] = 0.0;
-          for (int d = 0; d < D; d++) {
-            const PT* x0 = arr(1 + (size_t)d);
-            const PT* u = arr(1 + (size_t)(D + d));
-            for (size_t i = 0; i < nz; i++) out[3 * (int64_t)pid[i] + d] = (double)(x0[i] + u[i]);
-          }
+          for (int d = 0; d < D; d++)
+            for (size_t i = 0; i < nz; i++) out[3 * (int64_t)pid[i] + d] = (double)(v.x[d][i] + v.u[d][i]);
         } else {
-          vec3(1);
+          vec3(v.x);
         }
-        return MPMGPU_OK;
-      case MPMGPU_P_U:
-      case MPMGPU_P_X_T: vec3(1); return MPMGPU_OK;
-      case MPMGPU_P_MX_T: {
-        vec3(1);
-        const PT* m = arr(1 + (size_t)D);
+        return;
+      case MPMGPU_P_U: vec3(v.u); return;
+      case MPMGPU_P_X_T: vec3(v.v); return;
+      case MPMGPU_P_MX_T:
+        vec3(v.v);
         // movePoints: mx_t = m * x_t (explicit_usl.cpp:295-297)
         for (size_t i = 0; i < nz; i++) {
           const int64_t q = pid[i];
-          for (int d = 0; d < D; d++) out[3 * q + d] = (double)m[i] * out[3 * q + d];
+          for (int d = 0; d < D; d++) out[3 * q + d] = (double)v.m[i] * out[3 * q + d];
         }
-        return MPMGPU_OK;
-      }
-      case MPMGPU_P_L: {
-        const double* L = reinterpret_cast<const double*>(h[1]);
+        return;
+      case MPMGPU_P_L:
         for (size_t i = 0; i < nz; i++)
-          for (int k = 0; k < 9; k++) out[9 * (int64_t)pid[i] + k] = L[9 * i + (size_t)k];
-        return MPMGPU_OK;
-      }
+          for (int k = 0; k < 9; k++) out[9 * (int64_t)pid[i] + k] = v.L[9 * i + (size_t)k];
+        return;
       case MPMGPU_P_T: {
         static const int idx[9] = {0, 3, 5, 3, 1, 4, 5, 4, 2};
         for (size_t i = 0; i < nz; i++)
-          for (int k = 0; k < 9; k++) out[9 * (int64_t)pid[i] + k] = (double)arr(1 + (size_t)idx[k])[i];
-        return MPMGPU_OK;
+          for (int k = 0; k < 9; k++) out[9 * (int64_t)pid[i] + k] = (double)v.s[idx[k]][i];
+        return;
       }
-      case MPMGPU_P_M:
-      case MPMGPU_P_V:
-      case MPMGPU_P_EXTENT:
-      case MPMGPU_P_GAMMAP:
-      case MPMGPU_P_GAMMAP_DOT: {
-        const PT* a = arr(1);
-        for (size_t i = 0; i < nz; i++) out[pid[i]] = (double)a[i];
-        return MPMGPU_OK;
-      }
-      case MPMGPU_P_ACTIVE: {
-        const int32_t* a = reinterpret_cast<const int32_t*>(h[1]);
+      case MPMGPU_P_M: scalar(v.m); return;
+      case MPMGPU_P_V: scalar(v.vol); return;
+      case MPMGPU_P_EXTENT: scalar(v.ext); return;
+      case MPMGPU_P_GAMMAP: scalar(v.ms[0]); return;
+      case MPMGPU_P_GAMMAP_DOT: scalar(v.ms[1]); return;
+      case MPMGPU_P_ACTIVE:
         // 2 = left the domain at the last move: still active until the next
         // map build deactivates it, as in the reference
-        for (size_t i = 0; i < nz; i++) out[pid[i]] = a[i] != 0 ? 1.0 : 0.0;
-        return MPMGPU_OK;
+        for (size_t i = 0; i < nz; i++) out[pid[i]] = v.active[i] != 0 ? 1.0 : 0.0;
+        return;
+    }
+  }
+
+  mpmgpu_status point_field_check(const HBody& B, int field) {
+    if (!point_field_known(field)) return fail(MPMGPU_ERR_ARG, "unknown point field");
+    if (field == MPMGPU_P_L && !B.P.L) return fail(MPMGPU_ERR_STATE, "L is kept only with keep_debug in the FP64 form");
+    if ((field == MPMGPU_P_GAMMAP || field == MPMGPU_P_GAMMAP_DOT) && B.mat.kind != 2)
+      return fail(MPMGPU_ERR_STATE, "gammap and gammap_dot belong to Sand_SachithLocal bodies");
+    return MPMGPU_OK;
+  }
+
+  mpmgpu_status download_points(int job, int body, int field, double* out) override {
+    HJob* j;
+    HBody* B;
+    MPM_TRY(readable_body(job, body, &j, &B));
+    const int64_t n = B->n;
+    if (field == MPMGPU_P_B) {
+      MPM_TRY(synchronize());
+      for (int64_t i = 0; i < n; i++)
+        for (int d = 0; d < 3; d++) out[3 * i + d] = j->sp.grav[d];
+      return MPMGPU_OK;
+    }
+    MPM_TRY(point_field_check(*B, field));
+    // the point ids and the arrays of the field, copied with one wait
+    PointView pv;
+    pv.n = n;
+    std::vector<std::pair<const void*, size_t>> items;
+    std::vector<const void**> slots;
+    point_field_arrays(*B, field, pv, [&](const void* src, size_t bytes, const void** slot) {
+      items.emplace_back(src, bytes);
+      slots.push_back(slot);
+    });
+    std::vector<const unsigned char*> h;
+    MPM_TRY(fetch(items, h));
+    for (size_t k = 0; k < slots.size(); k++) *slots[k] = h[k];
+    points_to_ref(pv, field, out);
+    return MPMGPU_OK;
+  }
+
+  // ---- frames ----
+
+  mpmgpu_status frame_begin(int job) override {
+    HJob* j;
+    MPM_TRY(live_job(job, &j));
+    MPM_TRY(frame_wait());   // the previous frame's buffer is reused
+    struct Copy {
+      const void* src;
+      size_t bytes;
+      const void** slot;
+    };
+    std::vector<Copy> cp;
+    std::set<const void**> seen;
+    auto add = [&](const void* src, size_t bytes, const void** slot) {
+      if (src != nullptr && seen.insert(slot).second) cp.push_back({src, bytes, slot});
+    };
+    auto slot = [](auto& p) { return reinterpret_cast<const void**>(&p); };
+    Frame f;
+    f.job = job;
+    f.primed = j->primed && j->block_off >= 0;
+    f.dt = j->sp.dt;
+    f.g = j->g;
+    for (int d = 0; d < 3; d++) f.grav[d] = j->sp.grav[d];
+    f.pts.assign(j->bodies.size(), PointView{});
+    f.nodes.assign(j->bodies.size(), NodeView{});
+    f.contact.assign((size_t)j->nc, {nullptr, nullptr});
+    add(err_, sizeof(int), slot(f.err));
+    static const int fields[] = {MPMGPU_P_X, MPMGPU_P_U, MPMGPU_P_X_T, MPMGPU_P_MX_T, MPMGPU_P_T,
+                                 MPMGPU_P_V, MPMGPU_P_M, MPMGPU_P_EXTENT, MPMGPU_P_ACTIVE, MPMGPU_P_L,
+                                 MPMGPU_P_GAMMAP, MPMGPU_P_GAMMAP_DOT};
+    const size_t ns = (size_t)j->g.nslots * sizeof(double);
+    for (size_t b = 0; b < j->bodies.size(); b++) {
+      const HBody& B = j->bodies[b];
+      f.pts[b].n = B.n;
+      for (int field : fields) {
+        if (field == MPMGPU_P_L && !B.P.L) continue;
+        if ((field == MPMGPU_P_GAMMAP || field == MPMGPU_P_GAMMAP_DOT) && B.mat.kind != 2) continue;
+        point_field_arrays(B, field, f.pts[b], add);
+      }
+      if (!f.primed) continue;
+      NodeView& nv = f.nodes[b];
+      add(was_active_ + j->block_off, (size_t)j->g.nblocks, slot(nv.act));
+      add(B.snap.m, ns, slot(nv.m));
+      for (int d = 0; d < dim_; d++) {
+        add(B.snap.mx[d], ns, slot(nv.mx[d]));
+        add(B.snap.f[d], ns, slot(nv.f[d]));
+        add(B.V.vt[d], ns, slot(nv.vt[d]));
+        add(B.V.dv[d], ns, slot(nv.dv[d]));
       }
     }
-    return fail(MPMGPU_ERR_ARG, "unknown point field");
+    if (j->block_off >= 0 && !f.primed) add(was_active_ + j->block_off, (size_t)j->g.nblocks, slot(f.act));
+    for (int c = 0; c < j->nc; c++) {
+      add(j->normal_out[c], 3 * ns, slot(f.contact[(size_t)c].first));
+      add(j->force_out[c], 3 * ns, slot(f.contact[(size_t)c].second));
+    }
+    size_t total = 0;
+    for (const Copy& c : cp) total += (c.bytes + 255) / 256 * 256;
+    if (total > frame_cap_) {
+      MPM_CUDA_TRY(cudaStreamSynchronize(stream_));
+      if (frame_stage_) cudaFreeHost(frame_stage_);
+      frame_stage_ = nullptr;
+      frame_cap_ = 0;
+      const size_t cap = std::max<size_t>(total, (size_t)16 << 20);
+      MPM_CUDA_TRY(cudaHostAlloc(&frame_stage_, cap, cudaHostAllocDefault));
+      frame_cap_ = cap;
+    }
+    if (!frame_ev_) MPM_CUDA_TRY(cudaEventCreateWithFlags(&frame_ev_, cudaEventDisableTiming));
+    unsigned char* base = static_cast<unsigned char*>(frame_stage_);
+    size_t off = 0;
+    for (const Copy& c : cp) {
+      if (c.bytes > 0) MPM_CUDA_TRY(cudaMemcpyAsync(base + off, c.src, c.bytes, cudaMemcpyDeviceToHost, stream_));
+      *c.slot = base + off;
+      off += (c.bytes + 255) / 256 * 256;
+    }
+    MPM_CUDA_TRY(cudaEventRecord(frame_ev_, stream_));
+    f.pending = true;
+    frame_ = std::move(f);
+    return MPMGPU_OK;
+  }
+
+  mpmgpu_status frame_points(int job, int body, int field, double* out) override {
+    HBody* B;
+    MPM_TRY(frame_body(job, body, &B));
+    if (field == MPMGPU_P_B) {
+      for (int64_t i = 0; i < frame_.pts[(size_t)body].n; i++)
+        for (int d = 0; d < 3; d++) out[3 * i + d] = frame_.grav[d];
+      return MPMGPU_OK;
+    }
+    MPM_TRY(point_field_check(*B, field));
+    MPM_TRY(frame_wait());
+    points_to_ref(frame_.pts[(size_t)body], field, out);
+    return MPMGPU_OK;
+  }
+
+  mpmgpu_status frame_nodes(int job, int body, int field, double* out) override {
+    HBody* B;
+    MPM_TRY(frame_body(job, body, &B));
+    const Geom& g = frame_.g;
+    const int D = dim_;
+    const bool dbg = B->snap.m != nullptr;
+    const bool vec = field != MPMGPU_N_M;
+    if ((field == MPMGPU_N_M || field == MPMGPU_N_MX_T || field == MPMGPU_N_F) && !dbg)
+      return fail(MPMGPU_ERR_STATE, "nodal m, mx_t and f are kept only with keep_debug");
+    if (field < MPMGPU_N_M || field > MPMGPU_N_DIFF_X_T) return fail(MPMGPU_ERR_ARG, "unknown node field");
+    MPM_TRY(frame_wait());
+    if (!frame_.primed) {
+      for (int64_t i = 0; i < g.nnodes * (vec ? 3 : 1); i++) out[i] = 0.0;
+      return MPMGPU_OK;
+    }
+    const NodeView& nv = frame_.nodes[(size_t)body];
+    switch (field) {
+      case MPMGPU_N_M: nodes_host_to_ref(g, nv.act, &nv.m, 1, 1, out); break;
+      case MPMGPU_N_MX_T: nodes_host_to_ref(g, nv.act, nv.mx, D, 3, out); break;
+      case MPMGPU_N_F: nodes_host_to_ref(g, nv.act, nv.f, D, 3, out); break;
+      case MPMGPU_N_X_T: nodes_host_to_ref(g, nv.act, nv.vt, D, 3, out); break;
+      case MPMGPU_N_DIFF_X_T: nodes_host_to_ref(g, nv.act, nv.dv, D, 3, out); break;
+      case MPMGPU_N_U:
+        nodes_host_to_ref(g, nv.act, nv.vt, D, 3, out);
+        // moveGrid: u = dt * x_t (explicit_usl.cpp:252)
+        for (int64_t i = 0; i < 3 * g.nnodes; i++) out[i] = frame_.dt * out[i];
+        break;
+    }
+    return MPMGPU_OK;
+  }
+
+  mpmgpu_status frame_contact(int job, int contact, int field, double* out) override {
+    if (job != frame_.job) return fail(MPMGPU_ERR_STATE, "no frame of this job was begun");
+    if (contact < 0 || contact >= (int)frame_.contact.size()) return fail(MPMGPU_ERR_ARG, "no such contact");
+    if (!keep_debug_) return fail(MPMGPU_ERR_STATE, "contact fields are kept only with keep_debug");
+    if (field != MPMGPU_C_NORMAL && field != MPMGPU_C_FORCE) return fail(MPMGPU_ERR_ARG, "unknown contact field");
+    MPM_TRY(frame_wait());
+    const Geom& g = frame_.g;
+    const auto& cv = frame_.contact[(size_t)contact];
+    const double* src = field == MPMGPU_C_NORMAL ? cv.first : cv.second;
+    const uint8_t* act = frame_.primed ? frame_.nodes[0].act : frame_.act;
+    std::vector<uint8_t> none;
+    if (act == nullptr) {
+      none.assign((size_t)g.nblocks, 0);
+      act = none.data();
+    }
+    contact_host_to_ref(g, frame_.primed, act, src, field == MPMGPU_C_NORMAL, out);
+    return MPMGPU_OK;
   }
 
   size_t snapshot_bytes(int64_t n) const override { return (size_t)n * (16 * sizeof(PT) + 2 * sizeof(int32_t)); }
@@ -823,20 +1025,7 @@ class Batch : public BatchBase {
     MPM_TRY(download(tmp, src, 3 * (size_t)g.nslots));
     std::vector<uint8_t> act((size_t)g.nblocks, 0);
     if (j.block_off >= 0) MPM_TRY(download(act, was_active_ + j.block_off, (size_t)g.nblocks));
-    const double nan = std::nan("");
-    for (int k = 0; k < g.nn[2]; k++)
-      for (int jj = 0; jj < g.nn[1]; jj++)
-        for (int i = 0; i < g.nn[0]; i++) {
-          const int64_t id = i + (int64_t)g.nn[0] * (jj + (int64_t)g.nn[1] * k);
-          const int64_t s = node_slot(g, i, jj, k);
-          const bool on = j.primed && act[(size_t)node_block(g, i, jj, k)] != 0;
-          for (int d = 0; d < 3; d++) {
-            double v = tmp[(size_t)(3 * s + d)];
-            // the reference normalises every node's normal; a zero normal gives 0 * (1/0)
-            if (!on) v = (field == MPMGPU_C_NORMAL) ? (d < g.dim ? nan : 0.0) : 0.0;
-            out[3 * id + d] = v;
-          }
-        }
+    contact_host_to_ref(g, j.primed, act.data(), tmp.data(), field == MPMGPU_C_NORMAL, out);
     return MPMGPU_OK;
   }
 
@@ -918,7 +1107,7 @@ class Batch : public BatchBase {
     const int caps[3] = {256, 512, 1024};
     for (int ci = 0; ci < 3 && st == MPMGPU_OK; ci++) {
       if (!cap_available(dim_, mixed(), caps[ci]) || (det_ && caps[ci] != default_cap())) continue;
-      if (lean_ && caps[ci] != kLeanCap) continue;
+      if (lean_nt_ > 0 && caps[ci] != lean_nt_) continue;
       cap_ = caps[ci];
       float ms = 0.0f;
       st = trial(steps, 1 << 30, &ms);
@@ -1164,25 +1353,56 @@ class Batch : public BatchBase {
 
   int default_cap() const { return det_ && dim_ == 3 ? 256 : 512; }
 
+  // Converts block-linear nodal arrays (comps SoA components, host copies)
+  // to reference node order; nodes of blocks that were not active in the
+  // last step read 0.
+  static void nodes_host_to_ref(const Geom& g, const uint8_t* act, const double* const* arr, int comps, int width,
+                                double* out) {
+    for (int64_t i = 0; i < g.nnodes * width; i++) out[i] = 0.0;
+    for (int d = 0; d < comps; d++)
+      for (int k = 0; k < g.nn[2]; k++)
+        for (int jj = 0; jj < g.nn[1]; jj++)
+          for (int i = 0; i < g.nn[0]; i++) {
+            const int64_t id = i + (int64_t)g.nn[0] * (jj + (int64_t)g.nn[1] * k);
+            const bool on = act[(size_t)node_block(g, i, jj, k)] != 0;
+            out[id * width + d] = on ? arr[d][(size_t)node_slot(g, i, jj, k)] : 0.0;
+          }
+  }
+
   // Copies a block-linear nodal array (comps SoA components) to reference
   // node order; nodes of blocks that were not active in the last step read 0.
   mpmgpu_status nodes_to_ref(HJob& j, double* const* arr, int comps, int width, double* out) {
     const Geom& g = j.g;
     std::vector<uint8_t> act;
     MPM_TRY(download(act, was_active_ + j.block_off, (size_t)g.nblocks));
-    for (int64_t i = 0; i < g.nnodes * width; i++) out[i] = 0.0;
-    std::vector<double> tmp;
+    std::vector<std::vector<double>> tmp((size_t)comps);
+    const double* host[3] = {};
     for (int d = 0; d < comps; d++) {
-      MPM_TRY(download(tmp, arr[d], (size_t)g.nslots));
-      for (int k = 0; k < g.nn[2]; k++)
-        for (int jj = 0; jj < g.nn[1]; jj++)
-          for (int i = 0; i < g.nn[0]; i++) {
-            const int64_t id = i + (int64_t)g.nn[0] * (jj + (int64_t)g.nn[1] * k);
-            const bool on = act[(size_t)node_block(g, i, jj, k)] != 0;
-            out[id * width + d] = on ? tmp[(size_t)node_slot(g, i, jj, k)] : 0.0;
-          }
+      MPM_TRY(download(tmp[(size_t)d], arr[d], (size_t)g.nslots));
+      host[d] = tmp[(size_t)d].data();
     }
+    nodes_host_to_ref(g, act.data(), host, comps, width, out);
     return MPMGPU_OK;
+  }
+
+  // Converts a contact's per-node output (3 per slot, host copy) to
+  // reference node order.
+  static void contact_host_to_ref(const Geom& g, bool primed, const uint8_t* act, const double* src, bool normal,
+                                  double* out) {
+    const double nan = std::nan("");
+    for (int k = 0; k < g.nn[2]; k++)
+      for (int jj = 0; jj < g.nn[1]; jj++)
+        for (int i = 0; i < g.nn[0]; i++) {
+          const int64_t id = i + (int64_t)g.nn[0] * (jj + (int64_t)g.nn[1] * k);
+          const int64_t s = node_slot(g, i, jj, k);
+          const bool on = primed && act[(size_t)node_block(g, i, jj, k)] != 0;
+          for (int d = 0; d < 3; d++) {
+            double v = src[(size_t)(3 * s + d)];
+            // the reference normalises every node's normal; a zero normal gives 0 * (1/0)
+            if (!on) v = normal ? (d < g.dim ? nan : 0.0) : 0.0;
+            out[3 * id + d] = v;
+          }
+        }
   }
 
   // ---- block space (first-fit ranges, stable for a job's lifetime) ----
@@ -1339,7 +1559,7 @@ class Batch : public BatchBase {
         bins += j.bg.nbins + 1;
         cells += (int64_t)j.bg.nbins * j.bg.cells_per_bin + 1;
         item_off.push_back((int32_t)items);
-        items += j.bg.nbins + b.n / 256 + 1;
+        items += j.bg.nbins + b.n / kMinItemCap + 1;   // ceil(count / cap) summed over bins
         point_end.push_back(points);
         bin_end.push_back(bins);
         ctx.push_back(c);
@@ -1542,7 +1762,7 @@ class Batch : public BatchBase {
     return MPMGPU_OK;
   }
 
-  template <bool NORMAL, bool SINGLE, int MAT>
+  template <int NT, bool NORMAL, bool SINGLE, int MAT>
   mpmgpu_status launch_lean_k(int prime_pass, int phases, int one_body) {
     FusedLaunch<PT> fl{};
     if (SINGLE) fl.one = ctx_host_[(size_t)one_body];
@@ -1565,22 +1785,26 @@ class Batch : public BatchBase {
     fl.bounds = nullptr;
     fl.wait_polls = wait_polls_;
     constexpr size_t smem = lean_smem_bytes<3, PT, NORMAL>();
-    auto kern = k_g2p2g_lean<3, PT, NORMAL, SINGLE, MAT>;
-    int& per_sm = lean_per_sm_[(NORMAL ? 4 : 0) + (SINGLE ? 2 : 0) + (MAT == 0 ? 1 : 0)];
+    auto kern = k_g2p2g_lean<3, PT, NT, NORMAL, SINGLE, MAT>;
+    int& per_sm = lean_per_sm_[(NT == 128 ? 8 : 0) + (NORMAL ? 4 : 0) + (SINGLE ? 2 : 0) + (MAT == 0 ? 1 : 0)];
     if (per_sm == 0) {
       MPM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      MPM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kLeanThreads, smem));
+      MPM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, smem));
       if (per_sm < 1) return fail(MPMGPU_ERR_CUDA, "fused kernel does not fit on an SM");
     }
     StageTimer timer(this, kStageFused);
-    kern<<<per_sm * sm_count_, kLeanThreads, smem, stream_>>>(fl);
+    kern<<<per_sm * sm_count_, NT, smem, stream_>>>(fl);
     return check_launch("k_g2p2g_lean");
   }
 
   template <bool NORMAL, bool SINGLE>
   mpmgpu_status launch_lean_m(int prime_pass, int phases, int one_body, bool elastic) {
-    if (elastic) return launch_lean_k<NORMAL, SINGLE, 0>(prime_pass, phases, one_body);
-    return launch_lean_k<NORMAL, SINGLE, -1>(prime_pass, phases, one_body);
+    if (lean_nt_ == 128) {
+      if (elastic) return launch_lean_k<128, NORMAL, SINGLE, 0>(prime_pass, phases, one_body);
+      return launch_lean_k<128, NORMAL, SINGLE, -1>(prime_pass, phases, one_body);
+    }
+    if (elastic) return launch_lean_k<256, NORMAL, SINGLE, 0>(prime_pass, phases, one_body);
+    return launch_lean_k<256, NORMAL, SINGLE, -1>(prime_pass, phases, one_body);
   }
 
   mpmgpu_status launch_lean(int prime_pass, int phases) {
@@ -1601,7 +1825,7 @@ class Batch : public BatchBase {
   }
 
   mpmgpu_status launch_fused(int prime_pass, int phases) {
-    if (lean_ && dim_ == 3 && !det_) return launch_lean(prime_pass, phases);
+    if (lean_nt_ > 0) return launch_lean(prime_pass, phases);
     if constexpr (sizeof(PT) == 8) {
       if (det_) {
         // the deterministic form: 256 points per item in 3D (two tile levels)
@@ -1868,10 +2092,55 @@ class Batch : public BatchBase {
   std::vector<BodyCtx<PT>> ctx_host_;   // host copy of the body table
   bool single_mode_ = false;
   bool any_plain_ = false, any_normal_ = false;
+  // the frame in flight or last taken (frame_begin)
+  struct NodeView {
+    const uint8_t* act = nullptr;   // the job's node blocks active in the frame's step
+    const double* m = nullptr;
+    const double* mx[3] = {};
+    const double* f[3] = {};
+    const double* vt[3] = {};
+    const double* dv[3] = {};
+  };
+  struct Frame {
+    int job = -1;
+    bool pending = false;
+    bool primed = false;
+    double dt = 0.0;
+    double grav[3] = {0.0, 0.0, 0.0};
+    Geom g{};
+    std::vector<PointView> pts;
+    std::vector<NodeView> nodes;
+    std::vector<std::pair<const double*, const double*>> contact;   // normal, force
+    const uint8_t* act = nullptr;   // node blocks of an unprimed job (all inactive)
+    const int* err = nullptr;
+  } frame_;
+  void* frame_stage_ = nullptr;
+  size_t frame_cap_ = 0;
+  cudaEvent_t frame_ev_ = nullptr;
+
+  mpmgpu_status frame_wait() {
+    if (!frame_.pending) return MPMGPU_OK;
+    frame_.pending = false;
+    MPM_CUDA_TRY(cudaEventSynchronize(frame_ev_));
+    const int flag = *frame_.err;
+    if (flag & kErrWideSpan) return fail(MPMGPU_ERR_DEVICE, "point corners span more than two cells (extent > cell size)");
+    if (flag & kErrElemAlias) return fail(MPMGPU_ERR_DEVICE, "point within rounding of the upper domain face");
+    if (flag & kErrWaitTimeout) return fail(MPMGPU_ERR_DEVICE, "a bulk copy did not complete within the wait limit");
+    if (flag & kErrItemCap) return fail(MPMGPU_ERR_DEVICE, "a work item holds more points than the kernel takes");
+    return MPMGPU_OK;
+  }
+
+  mpmgpu_status frame_body(int job, int body, HBody** B) {
+    if (job != frame_.job) return fail(MPMGPU_ERR_STATE, "no frame of this job was begun");
+    HJob* j;
+    MPM_TRY(readable_body(job, body, &j, B));
+    if (body >= (int)frame_.pts.size()) return fail(MPMGPU_ERR_ARG, "no such body in the frame");
+    return MPMGPU_OK;
+  }
   bool all_elastic_ = true;              // every body IsotropicLinearElasticity (or no material)
-  bool lean_ = false;                    // the one-point-per-thread kernel (fused_lean.cuh)
+  int lean_nt_ = 0;                      // > 0: the one-point-per-thread kernel with CTAs of that size
   uint32_t wait_polls_ = kWaitPolls;     // poll limit of the fused kernels' first waits
-  int lean_per_sm_[8] = {};
+  int lean_per_sm_[16] = {};
   int flip_ = 0;                        // point buffers swapped an odd number of times
   cudaStream_t stream_ = nullptr;
   std::vector<HJob> jobs_;

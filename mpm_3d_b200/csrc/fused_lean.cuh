@@ -1,8 +1,8 @@
 // Lean form of the fused gather + point update + scatter kernel: one point
 // per thread and no staged copy of the point arrays.
 //
-// A CTA of kLeanThreads threads works on one work item at a time (at most
-// kLeanThreads points of one bin of one body):
+// A CTA of NT threads works on one work item at a time (at most NT points
+// of one bin of one body):
 //   0. every thread issues the global loads of its own point (coalesced:
 //      consecutive threads, consecutive points) while the CTA stages the
 //      nodal velocities of the bin's node tile and clears a separate FP64
@@ -25,13 +25,15 @@
 
 namespace mpmb200 {
 
-constexpr int kLeanThreads = 256;
-constexpr int kLeanCap = kLeanThreads;   // points per work item
+// Threads per CTA (= points per work item) of the two sizes the autotuner
+// chooses from: 256, or 128 for batches whose bins hold few points (a CTA
+// idles the threads its item does not fill).
+__host__ __device__ constexpr bool lean_size_ok(int nt) { return nt == 128 || nt == 256; }
 
 // Resident CTAs per SM the register budget is sized for.
-template <typename PT>
+template <typename PT, int NT>
 __host__ __device__ constexpr int lean_min_ctas() {
-  return sizeof(PT) == 4 ? 4 : 3;
+  return (sizeof(PT) == 4 ? 3 : 2) * (256 / NT);
 }
 
 // Shared memory: mbarriers | table entry slots [2] | velocity tile
@@ -187,8 +189,8 @@ __device__ __forceinline__ void lean_point(const BodyCtx<PT>& c, int* err, unsig
     scatter_general<DIM, T, TN, NORMAL, false>(c, drift, pm, o, q, tacc, touched, nullptr);
 }
 
-template <int DIM, typename PT, bool NORMAL, bool SINGLE, int MAT>
-__global__ void __launch_bounds__(kLeanThreads, lean_min_ctas<PT>())
+template <int DIM, typename PT, int NT, bool NORMAL, bool SINGLE, int MAT>
+__global__ void __launch_bounds__(NT, lean_min_ctas<PT, NT>())
     k_g2p2g_lean(const __grid_constant__ FusedLaunch<PT> fl) {
   constexpr int B = fused_bin<DIM>();
   constexpr int T = B + 3;
@@ -263,7 +265,7 @@ __global__ void __launch_bounds__(kLeanThreads, lean_min_ctas<PT>())
     const int bin = fl.work_bin[item];
     const int64_t pstart = fl.work_start[item];
     const int n = fl.work_end[item] - (int)pstart;
-    if (n > kLeanCap && threadIdx.x == 0) atomicOr(fl.err, kErrItemCap);   // the work list was cut for another size
+    if (n > NT && threadIdx.x == 0) atomicOr(fl.err, kErrItemCap);   // the work list was cut for another size
     const int j = threadIdx.x;
     const int64_t p = pstart + j;
     const int a = j < n ? P.active[p] : 0;
@@ -286,7 +288,7 @@ __global__ void __launch_bounds__(kLeanThreads, lean_min_ctas<PT>())
       }
       // nodal velocities of the tile: each thread issues the loads of up to
       // two nodes before its first shared-memory store
-      constexpr int ITER = (TN + kLeanThreads - 1) / kLeanThreads;
+      constexpr int ITER = (TN + NT - 1) / NT;
       constexpr int CH = ITER > 2 ? 2 : ITER;
 #pragma unroll 1
       for (int it0 = 0; it0 < ITER; it0 += CH) {
@@ -294,7 +296,7 @@ __global__ void __launch_bounds__(kLeanThreads, lean_min_ctas<PT>())
         int tt[CH];
 #pragma unroll
         for (int ic = 0; ic < CH; ic++) {
-          const int t = (int)threadIdx.x + (it0 + ic) * kLeanThreads;
+          const int t = (int)threadIdx.x + (it0 + ic) * NT;
           tt[ic] = -1;
           int tx, ty, tz;
           if (t >= TN || !TileLayout<DIM, T>::node(t, tx, ty, tz)) continue;
@@ -321,8 +323,8 @@ __global__ void __launch_bounds__(kLeanThreads, lean_min_ctas<PT>())
       }
     }
     if (do_p2g) {
-      for (int t = threadIdx.x; t < NACC * TN; t += kLeanThreads) tacc[t] = 0.0;
-      for (int t = threadIdx.x; t < TN; t += kLeanThreads) touched[t] = 0;
+      for (int t = threadIdx.x; t < NACC * TN; t += NT) tacc[t] = 0.0;
+      for (int t = threadIdx.x; t < TN; t += NT) touched[t] = 0;
     }
     __syncthreads();
     if (a != 0)

@@ -225,6 +225,8 @@ __global__ void k_scan_small(int32_t* v, int n, int32_t* total) {
 // scans its chunk in place and writes the chunk total; k_scan_small scans
 // the totals; k_scan_add adds them back.
 constexpr int kScanChunk = 1024;
+// Smallest points-per-item any fused kernel uses (work item capacity).
+constexpr int kMinItemCap = 128;
 
 __device__ __forceinline__ int block_exclusive_scan_1024(int x, int* total) {
   __shared__ int32_t warp_sums[32];

@@ -102,8 +102,10 @@ def load() -> ctypes.CDLL:
     lib.mpmgpu_set_gravity.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
     lib.mpmgpu_step.argtypes = [vp, ctypes.c_int]
     lib.mpmgpu_synchronize.argtypes = [vp]
-    for fn in ("mpmgpu_download_points", "mpmgpu_download_nodes", "mpmgpu_download_contact"):
+    for fn in ("mpmgpu_download_points", "mpmgpu_download_nodes", "mpmgpu_download_contact", "mpmgpu_frame_points",
+               "mpmgpu_frame_nodes", "mpmgpu_frame_contact"):
         getattr(lib, fn).argtypes = [vp, ctypes.c_int, ctypes.c_int, vp]
+    lib.mpmgpu_frame_begin.argtypes = [vp]
     lib.mpmgpu_dump_map.argtypes = [vp, ctypes.c_int, vp, vp, vp, vp, ctypes.POINTER(ctypes.c_int64)]
     lib.mpmgpu_dump_map_noalloc.argtypes = [vp, ctypes.c_int, vp, vp, vp, vp, ctypes.c_int64,
                                             ctypes.POINTER(ctypes.c_int64)]
@@ -307,6 +309,30 @@ class GPUExplicitUSL:
         fid, w = CONTACT_FIELDS[name]
         out = np.zeros((self.n_nodes, w))
         self._check(self.lib.mpmgpu_download_contact(self.h, c, fid, _ptr(out)))
+        return out
+
+    def frame_begin(self):
+        """Queues copies of every field behind the steps queued so far
+        (returns at once); frame_points / frame_nodes / frame_contact read
+        them as they stood then."""
+        self._check(self.lib.mpmgpu_frame_begin(self.h))
+
+    def frame_points(self, b: int, name: str) -> np.ndarray:
+        fid, w = POINT_FIELDS[name]
+        out = np.zeros((self.case.bodies[b].n, w))
+        self._check(self.lib.mpmgpu_frame_points(self.h, b, fid, _ptr(out)))
+        return out
+
+    def frame_nodes(self, b: int, name: str) -> np.ndarray:
+        fid, w = NODE_FIELDS[name]
+        out = np.zeros((self.n_nodes, w))
+        self._check(self.lib.mpmgpu_frame_nodes(self.h, b, fid, _ptr(out)))
+        return out
+
+    def frame_contact(self, c: int, name: str) -> np.ndarray:
+        fid, w = CONTACT_FIELDS[name]
+        out = np.zeros((self.n_nodes, w))
+        self._check(self.lib.mpmgpu_frame_contact(self.h, c, fid, _ptr(out)))
         return out
 
     def map(self, b: int) -> Tuple[np.ndarray, np.ndarray, np.ndarray, np.ndarray]:

@@ -4,10 +4,14 @@
 // object interface.
 #include "gpu_explicit_usl.hpp"
 
+#include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <functional>
 #include <iostream>
+#include <thread>
 #include <vector>
 
 #include "objects/bodies/bodies.hpp"
@@ -44,12 +48,13 @@ void GPUExplicitUSL::init(Job* job) {
   if (int_props.size() >= 2) contact_spec = int_props[1];
   if (int_props.size() >= 3) writeback_interval = int_props[2];
   if (int_props.size() >= 4) mode = int_props[3];
+  if (int_props.size() >= 5) overlap = int_props[4];
   if (mode < 0 || mode > 2) {
     std::cerr << "GPUExplicitUSL: form " << mode << " is not 0 (FP64), 1 (deterministic) or 2 (mixed)." << std::endl;
     exit(0);
   }
-  printf("Solver properties (cpdi_spec = %i, contact_spec = %i, writeback = %i, form = %i).\n", cpdi_spec,
-         contact_spec, writeback_interval, mode);
+  printf("Solver properties (cpdi_spec = %i, contact_spec = %i, writeback = %i, form = %i, overlap = %i).\n",
+         cpdi_spec, contact_spec, writeback_interval, mode, overlap);
   std::cout << "Solver Initialized." << std::endl;
 }
 
@@ -183,7 +188,10 @@ bool GPUExplicitUSL::frameDue(Job* job) {
 // ExplicitUSL::step (explicit_usl.cpp:48-87) on the GPU.
 void GPUExplicitUSL::step(Job* job) {
   if (!handle) setUp(job);
-  check(mpmgpu_step(handle, 1), "mpmgpu_step");
+  if (queued_ahead)
+    queued_ahead = false;   // queued behind the last frame's copies
+  else
+    check(mpmgpu_step(handle, 1), "mpmgpu_step");
   steps++;
   // explicit_usl.cpp:80-81: the driver sets the next step's body force
   job->driver->generateGravity(job);
@@ -201,77 +209,145 @@ void GPUExplicitUSL::step(Job* job) {
   if (frameDue(job)) writeBack(job);
 }
 
+namespace {
+
+// Runs the tasks on up to `threads` host threads.
+void run_tasks(std::vector<std::function<void()>>& tasks, unsigned threads) {
+  std::atomic<size_t> next{0};
+  auto worker = [&]() {
+    for (size_t k = next++; k < tasks.size(); k = next++) tasks[k]();
+  };
+  std::vector<std::thread> pool;
+  for (unsigned t = 1; t < threads && t < tasks.size(); t++) pool.emplace_back(worker);
+  worker();
+  for (auto& t : pool) t.join();
+}
+
+}  // namespace
+
+// The host arrays the serializer reads at a frame (DefaultPoints::writeFrame,
+// default_points.cpp:341-368; DefaultNodes::writeFrame,
+// default_nodes.cpp:68-82; ContactHuang's contact arrays,
+// contact_huang.cpp:202-206). The copies are queued behind the step that
+// just ran; with overlap on, the driver's next step is queued behind them
+// (DefaultDriver::run calls step, then writeFrame, then advances t,
+// default_driver.cpp:62-83, so that step comes next; its gravity is already
+// set), and the fields are converted to the reference layout on host threads
+// while the GPU runs it.
 void GPUExplicitUSL::writeBack(Job* job) {
-  check(mpmgpu_synchronize(handle), "mpmgpu_synchronize");
-  for (size_t b = 0; b < job->bodies.size(); b++) {
-    const int id = gpu_body[b];
-    if (id < 0) continue;
-    Points* pts = job->bodies[b]->points.get();
-    Nodes* nds = job->bodies[b]->nodes.get();
-    const int n = pts->x.size();
-    std::vector<double> buf(9 * (size_t)n);
-    auto vec3 = [&](int field, KinematicVectorArray& arr) {
-      check(mpmgpu_download_points(handle, id, field, buf.data()), "mpmgpu_download_points");
-      for (int i = 0; i < n; i++)
-        for (int j = 0; j < 3; j++) arr(i, j) = buf[3 * i + j];
+  check(mpmgpu_frame_begin(handle), "mpmgpu_frame_begin");
+  if (overlap) {
+    check(mpmgpu_step(handle, 1), "mpmgpu_step");
+    queued_ahead = true;
+  }
+  // the first field waits for the copies; the rest convert in parallel
+  std::vector<std::function<void()>> tasks;
+  std::vector<std::vector<double>> bufs;
+  bufs.reserve(64);
+  auto buffer = [&](size_t n) -> double* {
+    bufs.emplace_back(n);
+    return bufs.back().data();
+  };
+  bool waited = false;
+  auto point_task = [&](int id, int field, int n, int width, std::function<void(const double*)> store) {
+    double* b = buffer((size_t)n * width);
+    auto run = [this, id, field, b, store]() {
+      check(mpmgpu_frame_points(handle, id, field, b), "mpmgpu_frame_points");
+      store(b);
     };
-    vec3(MPMGPU_P_X, pts->x);
-    vec3(MPMGPU_P_U, pts->u);
-    vec3(MPMGPU_P_X_T, pts->x_t);
-    vec3(MPMGPU_P_MX_T, pts->mx_t);
+    if (!waited) {
+      run();
+      waited = true;
+    } else {
+      tasks.push_back(run);
+    }
+  };
+  for (size_t bi = 0; bi < job->bodies.size(); bi++) {
+    const int id = gpu_body[bi];
+    if (id < 0) continue;
+    Points* pts = job->bodies[bi]->points.get();
+    Nodes* nds = job->bodies[bi]->nodes.get();
+    const int n = pts->x.size();
+    auto vec3 = [n](KinematicVectorArray& arr) {
+      return [n, &arr](const double* b) {
+        for (int i = 0; i < n; i++)
+          for (int j = 0; j < 3; j++) arr(i, j) = b[3 * i + j];
+      };
+    };
+    point_task(id, MPMGPU_P_X, n, 3, vec3(pts->x));
+    point_task(id, MPMGPU_P_U, n, 3, vec3(pts->u));
+    point_task(id, MPMGPU_P_X_T, n, 3, vec3(pts->x_t));
+    point_task(id, MPMGPU_P_MX_T, n, 3, vec3(pts->mx_t));
     if (mode != MPMGPU_MODE_MIXED) {
       // the velocity gradient is kept on the device in the FP64 forms only
-      check(mpmgpu_download_points(handle, id, MPMGPU_P_L, buf.data()), "mpmgpu_download_points");
-      for (int i = 0; i < n; i++)
-        for (int k = 0; k < 9; k++) pts->L[i][k] = buf[9 * i + k];
+      point_task(id, MPMGPU_P_L, n, 9, [n, pts](const double* b) {
+        for (int i = 0; i < n; i++)
+          for (int k = 0; k < 9; k++) pts->L[i][k] = b[9 * i + k];
+      });
     }
-    check(mpmgpu_download_points(handle, id, MPMGPU_P_T, buf.data()), "mpmgpu_download_points");
-    for (int i = 0; i < n; i++)
-      for (int k = 0; k < 9; k++) pts->T[i][k] = buf[9 * i + k];
-    check(mpmgpu_download_points(handle, id, MPMGPU_P_V, buf.data()), "mpmgpu_download_points");
-    for (int i = 0; i < n; i++) pts->v(i) = buf[i];
-    check(mpmgpu_download_points(handle, id, MPMGPU_P_ACTIVE, buf.data()), "mpmgpu_download_points");
-    for (int i = 0; i < n; i++) pts->active(i) = (int)buf[i];
-    Sand_SachithLocal* sand = job->bodies[b]->activeMaterial
-                                  ? dynamic_cast<Sand_SachithLocal*>(job->bodies[b]->material.get())
+    point_task(id, MPMGPU_P_T, n, 9, [n, pts](const double* b) {
+      for (int i = 0; i < n; i++)
+        for (int k = 0; k < 9; k++) pts->T[i][k] = b[9 * i + k];
+    });
+    point_task(id, MPMGPU_P_V, n, 1, [n, pts](const double* b) {
+      for (int i = 0; i < n; i++) pts->v(i) = b[i];
+    });
+    point_task(id, MPMGPU_P_ACTIVE, n, 1, [n, pts](const double* b) {
+      for (int i = 0; i < n; i++) pts->active(i) = (int)b[i];
+    });
+    Sand_SachithLocal* sand = job->bodies[bi]->activeMaterial
+                                  ? dynamic_cast<Sand_SachithLocal*>(job->bodies[bi]->material.get())
                                   : nullptr;
     if (sand) {
       // the material's frame fields (Sand_SachithLocal::writeFrame)
-      check(mpmgpu_download_points(handle, id, MPMGPU_P_GAMMAP, buf.data()), "mpmgpu_download_points");
-      for (int i = 0; i < n; i++) sand->gammap(i) = buf[i];
-      check(mpmgpu_download_points(handle, id, MPMGPU_P_GAMMAP_DOT, buf.data()), "mpmgpu_download_points");
-      for (int i = 0; i < n; i++) sand->gammap_dot(i) = buf[i];
+      point_task(id, MPMGPU_P_GAMMAP, n, 1, [n, sand](const double* b) {
+        for (int i = 0; i < n; i++) sand->gammap(i) = b[i];
+      });
+      point_task(id, MPMGPU_P_GAMMAP_DOT, n, 1, [n, sand](const double* b) {
+        for (int i = 0; i < n; i++) sand->gammap_dot(i) = b[i];
+      });
     }
-
     const int nn = nds->x.size();
-    std::vector<double> nb(3 * (size_t)nn);
-    auto nvec3 = [&](int field, KinematicVectorArray& arr) {
-      check(mpmgpu_download_nodes(handle, id, field, nb.data()), "mpmgpu_download_nodes");
-      for (int i = 0; i < nn; i++)
-        for (int j = 0; j < 3; j++) arr(i, j) = nb[3 * i + j];
+    auto node_task = [&, id, nn](int field, int width, std::function<void(const double*)> store) {
+      double* b = buffer((size_t)nn * width);
+      tasks.push_back([this, id, field, b, store]() {
+        check(mpmgpu_frame_nodes(handle, id, field, b), "mpmgpu_frame_nodes");
+        store(b);
+      });
     };
-    check(mpmgpu_download_nodes(handle, id, MPMGPU_N_M, nb.data()), "mpmgpu_download_nodes");
-    for (int i = 0; i < nn; i++) nds->m(i) = nb[i];
-    nvec3(MPMGPU_N_MX_T, nds->mx_t);
-    nvec3(MPMGPU_N_F, nds->f);
-    nvec3(MPMGPU_N_X_T, nds->x_t);
-    nvec3(MPMGPU_N_U, nds->u);
-    nvec3(MPMGPU_N_DIFF_X_T, nds->diff_x_t);
+    auto nvec3 = [nn](KinematicVectorArray& arr) {
+      return [nn, &arr](const double* b) {
+        for (int i = 0; i < nn; i++)
+          for (int j = 0; j < 3; j++) arr(i, j) = b[3 * i + j];
+      };
+    };
+    node_task(MPMGPU_N_M, 1, [nn, nds](const double* b) {
+      for (int i = 0; i < nn; i++) nds->m(i) = b[i];
+    });
+    node_task(MPMGPU_N_MX_T, 3, nvec3(nds->mx_t));
+    node_task(MPMGPU_N_F, 3, nvec3(nds->f));
+    node_task(MPMGPU_N_X_T, 3, nvec3(nds->x_t));
+    node_task(MPMGPU_N_U, 3, nvec3(nds->u));
+    node_task(MPMGPU_N_DIFF_X_T, 3, nvec3(nds->diff_x_t));
   }
   int gc = 0;
   for (size_t c = 0; c < job->contacts.size(); c++) {
     if (job->activeContacts[c] == 0) continue;
     ContactHuang* ch = dynamic_cast<ContactHuang*>(job->contacts[c].get());
     const int nn = ch->contact_normal.size();
-    std::vector<double> nb(3 * (size_t)nn);
-    check(mpmgpu_download_contact(handle, gc, MPMGPU_C_NORMAL, nb.data()), "mpmgpu_download_contact");
-    for (int i = 0; i < nn; i++)
-      for (int j = 0; j < 3; j++) ch->contact_normal(i, j) = nb[3 * i + j];
-    check(mpmgpu_download_contact(handle, gc, MPMGPU_C_FORCE, nb.data()), "mpmgpu_download_contact");
-    for (int i = 0; i < nn; i++)
-      for (int j = 0; j < 3; j++) ch->contact_force(i, j) = nb[3 * i + j];
+    for (int field : {MPMGPU_C_NORMAL, MPMGPU_C_FORCE}) {
+      KinematicVectorArray& arr = field == MPMGPU_C_NORMAL ? ch->contact_normal : ch->contact_force;
+      double* b = buffer(3 * (size_t)nn);
+      tasks.push_back([this, gc, field, b, nn, &arr]() {
+        check(mpmgpu_frame_contact(handle, gc, field, b), "mpmgpu_frame_contact");
+        for (int i = 0; i < nn; i++)
+          for (int j = 0; j < 3; j++) arr(i, j) = b[3 * i + j];
+      });
+    }
     gc++;
   }
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  run_tasks(tasks, std::min(hw, 8u));
 }
 
 // As ExplicitUSL (explicit_usl.cpp:91-99): not implemented in the reference.

@@ -9,9 +9,13 @@
 // runs the same Job (grid, bodies, points, materials, boundaries, contacts,
 // driver, serializer) with the step on the GPU. int-properties mirror
 // ExplicitUSL::init (explicit_usl.cpp:25-44): {cpdi_spec, contact_spec}, plus
-// an optional third entry, the host write-back interval in steps (0 = write
-// back exactly when a DefaultVTK, MinimalVTK or AsyncVTK serializer is about
-// to write a frame, and every step for other serializers).
+// optional entries: the host write-back interval in steps (0 = write back
+// exactly when a DefaultVTK, MinimalVTK or AsyncVTK serializer is about to
+// write a frame, and every step for other serializers), the form (0 FP64,
+// 1 deterministic FP64, 2 mixed) and the overlap switch (1, the default:
+// at a frame the driver's next step is queued on the GPU before the frame is
+// converted on the host, so that the two run at the same time; 0: the step
+// is queued when the driver asks for it).
 //
 // Supported objects on the path: CartesianLinear, DefaultBody with
 // DefaultPoints/DefaultNodes, IsotropicLinearElasticity,
@@ -38,6 +42,7 @@ class GPUExplicitUSL : public Solver {
   int contact_spec = Contact::IMPLICIT;
   int writeback_interval = 0;
   int mode = 0;  // mpmgpu_mode: 0 FP64, 1 deterministic FP64, 2 mixed
+  int overlap = 1;
 
   void init(Job* job) override;
   void step(Job* job) override;
@@ -57,6 +62,7 @@ class GPUExplicitUSL : public Solver {
   double gravity[3] = {0.0, 0.0, 0.0};
   long steps = 0;
   long frames = 0;             // frames the serializer has written (mirrors DefaultVTK)
+  bool queued_ahead = false;   // the next step was queued at the last frame
   double sample_rate = 0.0;    // DefaultVTK properties[0], 0 if unknown
 };
 
