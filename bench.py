@@ -649,9 +649,8 @@ def run_e2e_batch(cases, steps: int, device: int, cap: int, sort_interval: int):
     t2 = time.perf_counter()
     phases["steps_s"] = t2 - t1
     d2h = 0
-    for j in jobs:
-        for f in ("x", "x_t", "T"):
-            d2h += b.points(j, 0, f).nbytes
+    for f in ("x", "x_t", "T"):
+        d2h += sum(o.nbytes for o in b.points_many(jobs, 0, f))
     t3 = time.perf_counter()
     phases["download_s"] = t3 - t2
     b.close()

@@ -270,6 +270,29 @@ mpmgpu_status mpmgpu_active_nodes(mpmgpu_handle* h, int64_t* nodes, int64_t* dri
  * that path without a fault. */
 mpmgpu_status mpmgpu_set_wait_limit(mpmgpu_handle* h, uint32_t polls);
 
+/* No counterpart in the reference. Forms of the fused gather / update /
+ * scatter kernel; every form computes the same step (the parity tests run
+ * each). */
+typedef enum {
+  /* point arrays of a work item staged in shared memory, the gather and
+   * scatter phases apart: 256 or 512 points per item (3D FP64), 256, 512 or
+   * 1024 (3D mixed), 512 (2D); the only form of 2D jobs and of the
+   * deterministic form */
+  MPMGPU_KERNEL_STAGED = 0,
+  /* one point per thread from gather to scatter, point state read from
+   * global memory: 128 or 256 points per item (3D) */
+  MPMGPU_KERNEL_POINT_PER_THREAD = 1,
+  /* as above, with the item's point arrays staged by bulk copies */
+  MPMGPU_KERNEL_POINT_PER_THREAD_STAGED = 2
+} mpmgpu_kernel_form;
+
+/* Selects the fused kernel's form and points per work item (default: one
+ * point per thread with 256 points in 3D outside the deterministic form,
+ * else staged with 512); MPMGPU_ERR_ARG if the pair is not available for
+ * the handle. Takes effect at the next step. */
+mpmgpu_status mpmgpu_set_kernel(mpmgpu_handle* h, int form, int points_per_item);
+mpmgpu_status mpmgpu_kernel(const mpmgpu_handle* h, int* form, int* points_per_item);
+
 /* Per-stage device time accounting with CUDA events recorded on the
  * handle's stream around every launch of a stage. enable != 0 starts (and
  * resets) it, 0 stops it. Stages: 0 fused gather/scatter kernel, 1 grid
@@ -302,9 +325,13 @@ typedef struct {
   int mode;            /* MPMGPU_MODE_FP64 or MPMGPU_MODE_MIXED */
   int device;          /* CUDA device ordinal */
   int sort_interval;   /* steps between re-binnings (0 = default 32) */
-  int points_per_item; /* points per CTA work item: 0 = default (512);
-                          3D: 256 or 512 (FP64), 256, 512 or 1024 (mixed);
-                          see mpmgpu_batch_autotune */
+  int points_per_item; /* points per CTA work item: 0 = default (3D,
+                          not deterministic: 256 on the one-point-per-thread
+                          kernel; else 512 on the staged kernel); 128 or 256
+                          run on the one-point-per-thread kernel where it
+                          applies, other sizes on the staged kernel (3D: 256
+                          or 512 in FP64, 256, 512 or 1024 mixed); see
+                          mpmgpu_set_kernel and mpmgpu_batch_autotune */
   int no_graph;        /* 1: launch stage by stage instead of graph replay */
   int keep_debug;      /* as mpmgpu_config.keep_debug */
 } mpmgpu_batch_config;
@@ -350,6 +377,12 @@ mpmgpu_status mpmgpu_batch_sizes(const mpmgpu_batch* b, int job, int body, int64
 
 /* As mpmgpu_download_points, for body `body` of job `job`. */
 mpmgpu_status mpmgpu_batch_download_points(mpmgpu_batch* b, int job, int body, int field, double* out);
+/* No counterpart in the reference. One point field of body `body` of each
+ * of `count` jobs, outs[k] receiving jobs[k]'s (layout of
+ * mpmgpu_download_points): the copies are queued together with one wait and
+ * converted to the reference's order on up to `threads` host threads. */
+mpmgpu_status mpmgpu_batch_download_points_many(mpmgpu_batch* b, int count, const int* jobs, int body, int field,
+                                                double* const* outs, int threads);
 
 /* Frees the job's device memory; it leaves the batch at the next step. */
 mpmgpu_status mpmgpu_batch_remove_job(mpmgpu_batch* b, int job);
@@ -358,12 +391,18 @@ mpmgpu_status mpmgpu_batch_remove_job(mpmgpu_batch* b, int job);
 mpmgpu_status mpmgpu_batch_counts(const mpmgpu_batch* b, int* live_jobs, int64_t* live_points, int64_t* bytes_in_use);
 
 /* Tunes the launch shape on the current jobs: times `steps` steps for every
- * available points-per-item choice, then 32 steps for each re-binning
- * interval (4, 8, 16, 32), restoring the jobs' state after each trial, and
- * keeps the fastest of each. The jobs' state after the call is the state
- * before it. */
+ * available kernel form and points-per-item choice (staged 256, 512, 1024;
+ * one point per thread 128, 256; one point per thread with staged point
+ * arrays 256), then 32 steps for each re-binning interval (4, 8, 16, 32),
+ * restoring the jobs' state after each trial, and keeps the fastest of
+ * each. The jobs' state after the call is the state before it. */
 mpmgpu_status mpmgpu_batch_autotune(mpmgpu_batch* b, int steps, int* points_per_item);
 int mpmgpu_batch_points_per_item(const mpmgpu_batch* b);
+/* The fused kernel's form (mpmgpu_kernel_form) in use. */
+int mpmgpu_batch_kernel_form(const mpmgpu_batch* b);
+/* Selects the fused kernel's form and points per work item (as
+ * mpmgpu_set_kernel); the jobs are re-binned before the next step. */
+mpmgpu_status mpmgpu_batch_set_kernel(mpmgpu_batch* b, int form, int points_per_item);
 int mpmgpu_batch_sort_interval(const mpmgpu_batch* b);
 
 /* As mpmgpu_active_nodes, over every job of the batch. */
@@ -398,8 +437,7 @@ mpmgpu_status mpmgpu_batch_destroy(mpmgpu_batch* b);
 
 typedef struct mpmgpu_server mpmgpu_server;
 
-/* cfg->points_per_item = 0 selects 256 for the 3D mixed form (many small
- * jobs run fastest with small work items) and the batch default otherwise. */
+/* cfg->points_per_item = 0 selects the batch default. */
 mpmgpu_status mpmgpu_server_create(const mpmgpu_batch_config* cfg, int64_t budget_bytes, mpmgpu_server** out);
 const char* mpmgpu_server_last_error(const mpmgpu_server* s);
 /* Device bytes the request will reserve from the budget while it runs. */

@@ -193,6 +193,18 @@ mpmgpu_status mpmgpu_active_nodes(mpmgpu_handle* h, int64_t* nodes, int64_t* dri
   return h->b->active_nodes(nodes, drifted);
 }
 
+mpmgpu_status mpmgpu_set_kernel(mpmgpu_handle* h, int form, int points_per_item) {
+  if (!h) return MPMGPU_ERR_ARG;
+  return h->b->set_kernel(form, points_per_item);
+}
+
+mpmgpu_status mpmgpu_kernel(const mpmgpu_handle* h, int* form, int* points_per_item) {
+  if (!h) return MPMGPU_ERR_ARG;
+  if (form) *form = h->b->kernel_form();
+  if (points_per_item) *points_per_item = h->b->points_per_item();
+  return MPMGPU_OK;
+}
+
 mpmgpu_status mpmgpu_set_wait_limit(mpmgpu_handle* h, uint32_t polls) {
   if (!h) return MPMGPU_ERR_ARG;
   h->b->set_wait_limit(polls);
@@ -317,7 +329,10 @@ mpmgpu_status mpmgpu_batch_create(const mpmgpu_batch_config* cfg, mpmgpu_batch**
   if (cfg->mode != MPMGPU_MODE_FP64 && cfg->mode != MPMGPU_MODE_MIXED && cfg->mode != MPMGPU_MODE_FP64_DETERMINISTIC)
     return MPMGPU_ERR_UNSUPPORTED;
   if (cfg->sort_interval < 0 || cfg->points_per_item < 0) return MPMGPU_ERR_ARG;
-  if (cfg->points_per_item != 0 && !cap_available(cfg->dim, cfg->mode == MPMGPU_MODE_MIXED, cfg->points_per_item))
+  if (cfg->points_per_item != 0 &&
+      !form_available(cfg->dim, cfg->mode == MPMGPU_MODE_MIXED, cfg->mode == MPMGPU_MODE_FP64_DETERMINISTIC,
+                      kFormLean, cfg->points_per_item) &&
+      !cap_available(cfg->dim, cfg->mode == MPMGPU_MODE_MIXED, cfg->points_per_item))
     return MPMGPU_ERR_UNSUPPORTED;
   auto b = std::make_unique<mpmgpu_batch>();
   b->cfg = *cfg;
@@ -387,6 +402,12 @@ mpmgpu_status mpmgpu_batch_download_points(mpmgpu_batch* b, int job, int body, i
   return b->b->download_points(job, body, field, out);
 }
 
+mpmgpu_status mpmgpu_batch_download_points_many(mpmgpu_batch* b, int count, const int* jobs, int body, int field,
+                                                double* const* outs, int threads) {
+  if (!b) return MPMGPU_ERR_ARG;
+  return b->b->download_points_many(count, jobs, body, field, outs, threads);
+}
+
 mpmgpu_status mpmgpu_batch_remove_job(mpmgpu_batch* b, int job) {
   if (!b) return MPMGPU_ERR_ARG;
   return b->b->remove_job(job);
@@ -415,6 +436,12 @@ mpmgpu_status mpmgpu_batch_profile_read(mpmgpu_batch* b, int stage, int64_t* lau
 }
 
 int mpmgpu_batch_points_per_item(const mpmgpu_batch* b) { return b ? b->b->points_per_item() : 0; }
+int mpmgpu_batch_kernel_form(const mpmgpu_batch* b) { return b ? b->b->kernel_form() : -1; }
+
+mpmgpu_status mpmgpu_batch_set_kernel(mpmgpu_batch* b, int form, int points_per_item) {
+  if (!b) return MPMGPU_ERR_ARG;
+  return b->b->set_kernel(form, points_per_item);
+}
 
 int mpmgpu_batch_sort_interval(const mpmgpu_batch* b) { return b ? b->b->sort_interval() : 0; }
 
@@ -442,15 +469,16 @@ mpmgpu_status mpmgpu_server_create(const mpmgpu_batch_config* cfg, int64_t budge
   if (cfg->dim != 2 && cfg->dim != 3) return MPMGPU_ERR_UNSUPPORTED;
   if (cfg->mode != MPMGPU_MODE_FP64 && cfg->mode != MPMGPU_MODE_MIXED && cfg->mode != MPMGPU_MODE_FP64_DETERMINISTIC)
     return MPMGPU_ERR_UNSUPPORTED;
-  if (cfg->points_per_item != 0 && !cap_available(cfg->dim, cfg->mode == MPMGPU_MODE_MIXED, cfg->points_per_item))
+  if (cfg->points_per_item != 0 &&
+      !form_available(cfg->dim, cfg->mode == MPMGPU_MODE_MIXED, cfg->mode == MPMGPU_MODE_FP64_DETERMINISTIC,
+                      kFormLean, cfg->points_per_item) &&
+      !cap_available(cfg->dim, cfg->mode == MPMGPU_MODE_MIXED, cfg->points_per_item))
     return MPMGPU_ERR_UNSUPPORTED;
   mpmgpu_status st = MPMGPU_OK;
   std::string msg;
-  // a stream of requests is a batch of many small jobs: in 3D the mixed form
-  // runs them fastest with 256-point work items (the autotuner's choice on
-  // the block-drop ensemble), unless the caller picks the size
-  const int cap = cfg->points_per_item != 0 ? cfg->points_per_item
-                                            : (cfg->dim == 3 && cfg->mode == MPMGPU_MODE_MIXED ? 256 : 0);
+  // the batch's default kernel (in 3D one point per thread, 256 points per
+  // work item), unless the caller picks the size
+  const int cap = cfg->points_per_item;
   auto b = make_batch(cfg->dim, cfg->mode, cfg->device, cfg->sort_interval, cap, !cfg->no_graph, cfg->keep_debug, &st,
                       &msg);
   if (st != MPMGPU_OK) return st;

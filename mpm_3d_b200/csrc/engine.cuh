@@ -27,6 +27,7 @@
 #include <cstring>
 #include <memory>
 #include <set>
+#include <thread>
 #include <string>
 #include <vector>
 
@@ -133,10 +134,24 @@ inline MaterialParams make_material(int has_material, double E, double nu, int k
 // Extent of a point, default_points.cpp:49-57 (computed once, never updated).
 inline double point_extent(int dim, double vol) { return dim == 2 ? 0.5 * std::sqrt(vol) : 0.5 * std::cbrt(vol); }
 
-// Particles per work item (CTA) available for each dimension and precision.
+// Particles per work item (CTA) of the staged kernel available for each
+// dimension and precision.
 inline bool cap_available(int dim, bool mixed, int cap) {
   if (dim == 3) return mixed ? (cap == 256 || cap == 512 || cap == 1024) : (cap == 256 || cap == 512);
   return cap == 512;
+}
+
+// Forms of the fused kernel (mpmgpu_set_kernel): the staged kernel
+// (fused.cuh: point arrays staged in shared memory, gather and scatter
+// phases apart, up to 1024 points per CTA), the one-point-per-thread kernel
+// (fused_lean.cuh, 3D, not the deterministic form), and the latter with its
+// items' point arrays staged by bulk copies.
+enum { kFormStaged = 0, kFormLean = 1, kFormLeanStaged = 2 };
+
+inline bool form_available(int dim, bool mixed, bool det, int form, int cap) {
+  if (form == kFormStaged) return cap_available(dim, mixed, cap);
+  if (form == kFormLean || form == kFormLeanStaged) return dim == 3 && !det && lean_size_ok(cap);
+  return false;
 }
 
 // Device bytes a job will hold: points (two buffers, with the material's
@@ -192,6 +207,10 @@ class BatchBase {
   virtual mpmgpu_status remove_job(int job) = 0;
   virtual mpmgpu_status job_state(int job, int64_t* done, int64_t* left) const = 0;
   virtual mpmgpu_status download_points(int job, int body, int field, double* out) = 0;
+  // One point field of one body of each of `count` jobs, copied with one
+  // wait and converted on up to `threads` host threads.
+  virtual mpmgpu_status download_points_many(int count, const int* jobs, int body, int field, double* const* outs,
+                                             int threads) = 0;
   // Raw point state of a body copied to host memory in stream order, i.e.
   // as it stands after the work queued so far (without waiting): x, u, x_t
   // (3 arrays each), stress (6) and V in the point precision, then active
@@ -225,6 +244,12 @@ class BatchBase {
   virtual void counts(int* live_jobs, int64_t* live_points) const = 0;
   virtual int points_per_item() const = 0;
   virtual int sort_interval() const = 0;
+  // Form of the fused kernel (kFormStaged, kFormLean, kFormLeanStaged) and
+  // its points per work item; chosen at creation (the one-point-per-thread
+  // kernel with 256 points in 3D, the staged kernel otherwise), by the
+  // autotuner, or by set_kernel.
+  virtual int kernel_form() const = 0;
+  virtual mpmgpu_status set_kernel(int form, int cap) = 0;
   virtual mpmgpu_status active_nodes(int64_t* nodes, int64_t* drifted) = 0;
   // FP64 map export support (single-job handle)
   virtual mpmgpu_status body_points_fp64(int job, int body, PointsDev* P, Geom* g, int* cpdi) = 0;
@@ -296,13 +321,11 @@ class Batch : public BatchBase {
       uint64_t keep = UINT64_MAX;
       MPM_CUDA_TRY(cudaMemPoolSetAttribute(pool_, cudaMemPoolAttrReleaseThreshold, &keep));
     }
-    if (const char* e = getenv("MPM_B200_LEAN")) {
-      const int v = atoi(e);
-      lean_nt_ = (dim_ == 3 && !det_ && lean_size_ok(v)) ? v : 0;
-    }
-    if (lean_nt_ > 0) cap_ = lean_nt_;
-    if (cap_ == 0) cap_ = default_cap();
-    if ((lean_nt_ == 0 && !cap_available(dim_, mixed(), cap_)) || (det_ && cap_ != default_cap()))
+    // a requested item size is served by the one-point-per-thread kernel
+    // where it has that size, else by the staged kernel
+    if (cap_ == 0) cap_ = (dim_ == 3 && !det_) ? kDefaultLeanCap : default_cap();
+    form_ = form_available(dim_, mixed(), det_, kFormLean, cap_) ? kFormLean : kFormStaged;
+    if (!form_available(dim_, mixed(), det_, form_, cap_) || (det_ && cap_ != default_cap()))
       return fail(MPMGPU_ERR_ARG, "points_per_item " + std::to_string(cap_) + " not available for this form");
     if (det_ && mixed()) return fail(MPMGPU_ERR_UNSUPPORTED, "the deterministic form is FP64");
     MPM_TRY(alloc_raw(&hdr_, 1, scratch_allocs_));
@@ -789,6 +812,40 @@ class Batch : public BatchBase {
     return MPMGPU_OK;
   }
 
+  mpmgpu_status download_points_many(int count, const int* jobs, int body, int field, double* const* outs,
+                                     int threads) override {
+    if (count < 0 || (count > 0 && (!jobs || !outs))) return fail(MPMGPU_ERR_ARG, "job list missing");
+    if (field == MPMGPU_P_B) {
+      for (int k = 0; k < count; k++) MPM_TRY(download_points(jobs[k], body, field, outs[k]));
+      return MPMGPU_OK;
+    }
+    std::vector<PointView> views((size_t)count);
+    std::vector<std::pair<const void*, size_t>> items;
+    std::vector<std::pair<size_t, const void**>> slots;   // (view, slot)
+    for (int k = 0; k < count; k++) {
+      HJob* j;
+      HBody* B;
+      MPM_TRY(readable_body(jobs[k], body, &j, &B));
+      MPM_TRY(point_field_check(*B, field));
+      views[(size_t)k].n = B->n;
+      point_field_arrays(*B, field, views[(size_t)k], [&](const void* src, size_t bytes, const void** slot) {
+        items.emplace_back(src, bytes);
+        slots.emplace_back((size_t)k, slot);
+      });
+    }
+    std::vector<const unsigned char*> h;
+    MPM_TRY(fetch(items, h));
+    for (size_t i = 0; i < slots.size(); i++) *slots[i].second = h[i];
+    const int nt = std::max(1, std::min(threads, count));
+    std::vector<std::thread> pool;
+    for (int t = 0; t < nt; t++)
+      pool.emplace_back([&, t]() {
+        for (int k = t; k < count; k += nt) points_to_ref(views[(size_t)k], field, outs[k]);
+      });
+    for (auto& th : pool) th.join();
+    return MPMGPU_OK;
+  }
+
   // ---- frames ----
 
   mpmgpu_status frame_begin(int job) override {
@@ -1102,21 +1159,27 @@ class Batch : public BatchBase {
       return snapshot_restore();
     };
     mpmgpu_status st = MPMGPU_OK;
-    int best_c = original_cap, best_si = original_si;
+    const int original_form = form_;
+    int best_c = original_cap, best_f = original_form, best_si = original_si;
     float best_ms = 1e30f;
-    const int caps[3] = {256, 512, 1024};
-    for (int ci = 0; ci < 3 && st == MPMGPU_OK; ci++) {
-      if (!cap_available(dim_, mixed(), caps[ci]) || (det_ && caps[ci] != default_cap())) continue;
-      if (lean_nt_ > 0 && caps[ci] != lean_nt_) continue;
-      cap_ = caps[ci];
+    // kernel form and points per item
+    const int cand[6][2] = {{kFormStaged, 256}, {kFormStaged, 512},   {kFormStaged, 1024},
+                            {kFormLean, 128},   {kFormLean, 256},     {kFormLeanStaged, 256}};
+    for (int ci = 0; ci < 6 && st == MPMGPU_OK; ci++) {
+      const int f = cand[ci][0], c = cand[ci][1];
+      if (!form_available(dim_, mixed(), det_, f, c) || (det_ && c != default_cap())) continue;
+      form_ = f;
+      cap_ = c;
       float ms = 0.0f;
       st = trial(steps, 1 << 30, &ms);
       if (st == MPMGPU_OK && ms < best_ms) {
         best_ms = ms;
-        best_c = caps[ci];
+        best_c = c;
+        best_f = f;
       }
     }
     cap_ = best_c;
+    form_ = best_f;
     best_ms = 1e30f;
     const int intervals[4] = {4, 8, 16, 32};
     for (int k = 0; k < 4 && st == MPMGPU_OK; k++) {
@@ -1130,6 +1193,7 @@ class Batch : public BatchBase {
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     cap_ = (st == MPMGPU_OK) ? best_c : original_cap;
+    form_ = (st == MPMGPU_OK) ? best_f : original_form;
     sort_interval_ = (st == MPMGPU_OK) ? best_si : original_si;
     drop_graphs();
     snapshot_free();
@@ -1140,6 +1204,20 @@ class Batch : public BatchBase {
   }
 
   int sort_interval() const override { return sort_interval_; }
+  int kernel_form() const override { return form_; }
+
+  mpmgpu_status set_kernel(int form, int cap) override {
+    if (!form_available(dim_, mixed(), det_, form, cap) || (det_ && cap != default_cap()))
+      return fail(MPMGPU_ERR_ARG, "kernel form " + std::to_string(form) + " with " + std::to_string(cap) +
+                                      " points per item is not available for this batch");
+    if (form == form_ && cap == cap_) return MPMGPU_OK;
+    form_ = form;
+    cap_ = cap;
+    drop_graphs();
+    // the work items depend on the item size: re-bin before the next step
+    membership_dirty_ = true;
+    return MPMGPU_OK;
+  }
 
   void set_wait_limit(uint32_t polls) override {
     wait_polls_ = polls;
@@ -1762,7 +1840,7 @@ class Batch : public BatchBase {
     return MPMGPU_OK;
   }
 
-  template <int NT, bool NORMAL, bool SINGLE, int MAT>
+  template <int NT, bool NORMAL, bool SINGLE, int MAT, bool STAGE>
   mpmgpu_status launch_lean_k(int prime_pass, int phases, int one_body) {
     FusedLaunch<PT> fl{};
     if (SINGLE) fl.one = ctx_host_[(size_t)one_body];
@@ -1784,9 +1862,10 @@ class Batch : public BatchBase {
     fl.phases = phases;
     fl.bounds = nullptr;
     fl.wait_polls = wait_polls_;
-    constexpr size_t smem = lean_smem_bytes<3, PT, NORMAL>();
-    auto kern = k_g2p2g_lean<3, PT, NT, NORMAL, SINGLE, MAT>;
-    int& per_sm = lean_per_sm_[(NT == 128 ? 8 : 0) + (NORMAL ? 4 : 0) + (SINGLE ? 2 : 0) + (MAT == 0 ? 1 : 0)];
+    constexpr size_t smem = lean_smem_bytes<3, PT, NT, NORMAL, STAGE>();
+    auto kern = k_g2p2g_lean<3, PT, NT, NORMAL, SINGLE, MAT, STAGE>;
+    int& per_sm =
+        lean_per_sm_[(STAGE ? 16 : 0) + (NT == 128 ? 8 : 0) + (NORMAL ? 4 : 0) + (SINGLE ? 2 : 0) + (MAT == 0 ? 1 : 0)];
     if (per_sm == 0) {
       MPM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
       MPM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, smem));
@@ -1797,14 +1876,21 @@ class Batch : public BatchBase {
     return check_launch("k_g2p2g_lean");
   }
 
+  template <int NT, bool NORMAL, bool SINGLE, bool STAGE>
+  mpmgpu_status launch_lean_s(int prime_pass, int phases, int one_body, bool elastic) {
+    if (elastic) return launch_lean_k<NT, NORMAL, SINGLE, 0, STAGE>(prime_pass, phases, one_body);
+    return launch_lean_k<NT, NORMAL, SINGLE, -1, STAGE>(prime_pass, phases, one_body);
+  }
+
   template <bool NORMAL, bool SINGLE>
   mpmgpu_status launch_lean_m(int prime_pass, int phases, int one_body, bool elastic) {
-    if (lean_nt_ == 128) {
-      if (elastic) return launch_lean_k<128, NORMAL, SINGLE, 0>(prime_pass, phases, one_body);
-      return launch_lean_k<128, NORMAL, SINGLE, -1>(prime_pass, phases, one_body);
+    const bool stage = form_ == kFormLeanStaged;
+    if (cap_ == 128) {
+      if (stage) return launch_lean_s<128, NORMAL, SINGLE, true>(prime_pass, phases, one_body, elastic);
+      return launch_lean_s<128, NORMAL, SINGLE, false>(prime_pass, phases, one_body, elastic);
     }
-    if (elastic) return launch_lean_k<256, NORMAL, SINGLE, 0>(prime_pass, phases, one_body);
-    return launch_lean_k<256, NORMAL, SINGLE, -1>(prime_pass, phases, one_body);
+    if (stage) return launch_lean_s<256, NORMAL, SINGLE, true>(prime_pass, phases, one_body, elastic);
+    return launch_lean_s<256, NORMAL, SINGLE, false>(prime_pass, phases, one_body, elastic);
   }
 
   mpmgpu_status launch_lean(int prime_pass, int phases) {
@@ -1825,7 +1911,7 @@ class Batch : public BatchBase {
   }
 
   mpmgpu_status launch_fused(int prime_pass, int phases) {
-    if (lean_nt_ > 0) return launch_lean(prime_pass, phases);
+    if (form_ != kFormStaged) return launch_lean(prime_pass, phases);
     if constexpr (sizeof(PT) == 8) {
       if (det_) {
         // the deterministic form: 256 points per item in 3D (two tile levels)
@@ -2138,9 +2224,9 @@ class Batch : public BatchBase {
     return MPMGPU_OK;
   }
   bool all_elastic_ = true;              // every body IsotropicLinearElasticity (or no material)
-  int lean_nt_ = 0;                      // > 0: the one-point-per-thread kernel with CTAs of that size
+  int form_ = kFormStaged;               // form of the fused kernel (cap_: its points per item)
   uint32_t wait_polls_ = kWaitPolls;     // poll limit of the fused kernels' first waits
-  int lean_per_sm_[16] = {};
+  int lean_per_sm_[32] = {};
   int flip_ = 0;                        // point buffers swapped an odd number of times
   cudaStream_t stream_ = nullptr;
   std::vector<HJob> jobs_;

@@ -135,9 +135,19 @@ __device__ __forceinline__ int axis_element_fast(const Geom& g, const MapConst& 
 // (axis_element_fast). Triplet-exact values come from exact_map.cuh.
 // Returns -1 outside the domain (caller deactivates), 0 without triplets,
 // 1 otherwise.
+// The gradient scale of the corner-sampled map, 1 / ((cp/2) extent): it
+// depends only on the point's extent, so a caller that builds two maps of
+// one point computes it once and passes it in.
+__device__ __forceinline__ double map_grad_scale(const Geom& g, double extent) {
+  return 1.0 / ((g.cp * 0.5) * extent);
+}
+__device__ __forceinline__ float map_grad_scale(const Geom& g, float extent) {
+  return 1.0f / (((float)g.cp * 0.5f) * extent);
+}
+
 template <int DIM>
 __device__ __forceinline__ int build_map_fast(const Geom& g, const MapConst& mc, int cpdi_spec, const double* x,
-                                              double extent, PointMap& pm, int* err) {
+                                              double extent, PointMap& pm, int* err, double sG) {
   if (!in_domain<DIM>(g, x)) return -1;
   int cpdi = cpdi_spec;
   const double a = 0.5 * extent;
@@ -194,7 +204,7 @@ __device__ __forceinline__ int build_map_fast(const Geom& g, const MapConst& mc,
       }
     }
     pm.sS = 1.0 / (double)g.cp;
-    pm.sG = 1.0 / ((g.cp * 0.5) * extent);
+    pm.sG = sG;
     return 1;
   }
 #pragma unroll
@@ -236,7 +246,7 @@ __device__ __forceinline__ int axis_element_f32(const Geom& g, const MapConst& m
 
 template <int DIM>
 __device__ __forceinline__ int build_map_f32(const Geom& g, const MapConst& mc, int cpdi_spec, const float* x,
-                                             float extent, PointMapT<float>& pm, int* err) {
+                                             float extent, PointMapT<float>& pm, int* err, float sG) {
 #pragma unroll
   for (int d = 0; d < DIM; d++)
     if (!(x[d] <= mc.Lf[d] && x[d] >= 0.0f)) return -1;
@@ -289,7 +299,7 @@ __device__ __forceinline__ int build_map_f32(const Geom& g, const MapConst& mc, 
       }
     }
     pm.sS = 1.0f / (float)g.cp;
-    pm.sG = 1.0f / (((float)g.cp * 0.5f) * extent);
+    pm.sG = sG;
     return 1;
   }
 #pragma unroll
@@ -319,12 +329,22 @@ __device__ __forceinline__ int build_map_f32(const Geom& g, const MapConst& mc, 
 template <int DIM>
 __device__ __forceinline__ int build_map(const Geom& g, const MapConst& mc, int cpdi, const double* x, double ext,
                                          PointMapT<double>& pm, int* err) {
-  return build_map_fast<DIM>(g, mc, cpdi, x, ext, pm, err);
+  return build_map_fast<DIM>(g, mc, cpdi, x, ext, pm, err, map_grad_scale(g, ext));
+}
+template <int DIM>
+__device__ __forceinline__ int build_map(const Geom& g, const MapConst& mc, int cpdi, const double* x, double ext,
+                                         PointMapT<double>& pm, int* err, double sG) {
+  return build_map_fast<DIM>(g, mc, cpdi, x, ext, pm, err, sG);
 }
 template <int DIM>
 __device__ __forceinline__ int build_map(const Geom& g, const MapConst& mc, int cpdi, const float* x, float ext,
                                          PointMapT<float>& pm, int* err) {
-  return build_map_f32<DIM>(g, mc, cpdi, x, ext, pm, err);
+  return build_map_f32<DIM>(g, mc, cpdi, x, ext, pm, err, map_grad_scale(g, ext));
+}
+template <int DIM>
+__device__ __forceinline__ int build_map(const Geom& g, const MapConst& mc, int cpdi, const float* x, float ext,
+                                         PointMapT<float>& pm, int* err, float sG) {
+  return build_map_f32<DIM>(g, mc, cpdi, x, ext, pm, err, sG);
 }
 
 }  // namespace mpmb200

@@ -19,6 +19,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.environ.get("MPM_B200_LIB", os.path.join(HERE, "lib", "libmpm_b200.so"))
 
 MODES = {"fp64": 0, "fp64_deterministic": 1, "mixed": 2}
+# forms of the fused kernel (mpmgpu_kernel_form)
+KERNELS = {"staged": 0, "point_per_thread": 1, "point_per_thread_staged": 2}
+KERNEL_NAMES = {v: k for k, v in KERNELS.items()}
 POINT_FIELDS = {"x": (0, 3), "u": (1, 3), "x_t": (2, 3), "mx_t": (3, 3), "b": (4, 3), "L": (5, 9), "T": (6, 9),
                 "m": (7, 1), "v": (8, 1), "extent": (9, 1), "active": (10, 1), "gammap": (11, 1),
                 "gammap_dot": (12, 1)}
@@ -116,6 +119,10 @@ def load() -> ctypes.CDLL:
     lib.mpmgpu_stream.argtypes = [vp]
     lib.mpmgpu_profile.argtypes = [vp, ctypes.c_int]
     lib.mpmgpu_set_wait_limit.argtypes = [vp, ctypes.c_uint32]
+    lib.mpmgpu_set_kernel.argtypes = [vp, ctypes.c_int, ctypes.c_int]
+    lib.mpmgpu_kernel.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
+    lib.mpmgpu_batch_set_kernel.argtypes = [vp, ctypes.c_int, ctypes.c_int]
+    lib.mpmgpu_batch_kernel_form.argtypes = [vp]
     lib.mpmgpu_profile_read.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_double)]
     lib.mpmgpu_destroy.argtypes = [vp]
     i64p = ctypes.POINTER(ctypes.c_int64)
@@ -129,6 +136,8 @@ def load() -> ctypes.CDLL:
     lib.mpmgpu_batch_job_state.argtypes = [vp, ctypes.c_int, i64p, i64p]
     lib.mpmgpu_batch_sizes.argtypes = [vp, ctypes.c_int, ctypes.c_int, i64p, i64p]
     lib.mpmgpu_batch_download_points.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp]
+    lib.mpmgpu_batch_download_points_many.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.c_int,
+                                                      ctypes.c_int, ctypes.POINTER(ctypes.c_void_p), ctypes.c_int]
     lib.mpmgpu_batch_remove_job.argtypes = [vp, ctypes.c_int]
     lib.mpmgpu_batch_counts.argtypes = [vp, ctypes.POINTER(ctypes.c_int), i64p, i64p]
     lib.mpmgpu_batch_autotune.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
@@ -201,7 +210,7 @@ class GPUExplicitUSL:
     """
 
     def __init__(self, case: inputs.Case, mode: str = "fp64", keep_debug: bool = False, device: int = 0,
-                 sort_interval: int = 0):
+                 sort_interval: int = 0, kernel: Optional[Tuple[str, int]] = None):
         self.lib = load()
         self.case = case
         cfg = _Config()
@@ -230,6 +239,8 @@ class GPUExplicitUSL:
         if case.gravity is not None:
             g = (ctypes.c_double * 3)(*(list(case.gravity) + [0.0] * (3 - len(case.gravity))))
             self._check(self.lib.mpmgpu_set_gravity(self.h, 1, g))
+        if kernel is not None:
+            self.set_kernel(*kernel)
         n_nodes = ctypes.c_int64()
         self._check(self.lib.mpmgpu_sizes(self.h, 0, None, ctypes.byref(n_nodes)))
         self.n_nodes = n_nodes.value
@@ -266,6 +277,16 @@ class GPUExplicitUSL:
         return int(self.lib.mpmgpu_stream(self.h) or 0)
 
     STAGES = {"g2p2g": 0, "grid": 1, "compact": 2, "rebin": 3}
+
+    def set_kernel(self, form: str, points_per_item: int):
+        """Selects the fused kernel's form (KERNELS) and points per work item."""
+        self._check(self.lib.mpmgpu_set_kernel(self.h, KERNELS[form], points_per_item))
+
+    def kernel(self) -> Tuple[str, int]:
+        f = ctypes.c_int()
+        c = ctypes.c_int()
+        self._check(self.lib.mpmgpu_kernel(self.h, ctypes.byref(f), ctypes.byref(c)))
+        return KERNEL_NAMES[f.value], c.value
 
     def set_wait_limit(self, polls: int):
         """Poll limit of the fused kernel's waits for bulk copies (2^24 by
@@ -406,7 +427,8 @@ class GPUBatch:
     """
 
     def __init__(self, dim: int = 3, mode: str = "mixed", device: int = 0, sort_interval: int = 0,
-                 points_per_item: int = 0, graph: bool = True, keep_debug: bool = False):
+                 points_per_item: int = 0, graph: bool = True, keep_debug: bool = False,
+                 kernel: Optional[Tuple[str, int]] = None):
         self.lib = load()
         cfg = _BatchConfig(dim, MODES[mode], device, sort_interval, points_per_item, 0 if graph else 1,
                            int(keep_debug))
@@ -417,6 +439,8 @@ class GPUBatch:
         self.h = h
         self.dim = dim
         self.cases: Dict[int, inputs.Case] = {}
+        if kernel is not None:
+            self.set_kernel(*kernel)
 
     def _check(self, status: int):
         if status != 0:
@@ -469,6 +493,17 @@ class GPUBatch:
         self._check(self.lib.mpmgpu_batch_download_points(self.h, job, b, fid, _ptr(out)))
         return out
 
+    def points_many(self, jobs, b: int, name: str, threads: int = 0):
+        """One point field of body b of several jobs, copied with one wait
+        and converted on host threads (all host threads by default)."""
+        fid, w = POINT_FIELDS[name]
+        outs = [np.zeros((self.cases[j].bodies[b].n, w)) for j in jobs]
+        ids = (ctypes.c_int * len(jobs))(*jobs)
+        ptrs = (ctypes.c_void_p * len(jobs))(*[o.ctypes.data for o in outs])
+        self._check(self.lib.mpmgpu_batch_download_points_many(self.h, len(jobs), ids, b, fid, ptrs,
+                                                               threads or (os.cpu_count() or 1)))
+        return outs
+
     def remove(self, job: int):
         self._check(self.lib.mpmgpu_batch_remove_job(self.h, job))
         self.cases.pop(job, None)
@@ -488,6 +523,13 @@ class GPUBatch:
 
     def points_per_item(self) -> int:
         return int(self.lib.mpmgpu_batch_points_per_item(self.h))
+
+    def kernel_form(self) -> str:
+        return KERNEL_NAMES[int(self.lib.mpmgpu_batch_kernel_form(self.h))]
+
+    def set_kernel(self, form: str, points_per_item: int):
+        """Selects the fused kernel's form (KERNELS) and points per work item."""
+        self._check(self.lib.mpmgpu_batch_set_kernel(self.h, KERNELS[form], points_per_item))
 
     def sort_interval(self) -> int:
         return int(self.lib.mpmgpu_batch_sort_interval(self.h))
