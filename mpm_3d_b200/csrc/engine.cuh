@@ -33,6 +33,7 @@
 
 #include "../../include/mpm_b200.h"
 #include "fused.cuh"
+#include "frame.cuh"
 #include "fused_lean.cuh"
 #include "kernels_fp64.cuh"
 #include "sort.cuh"
@@ -355,6 +356,7 @@ class Batch : public BatchBase {
     if (stage_) cudaFreeHost(stage_);
     if (dl_stage_) cudaFreeHost(dl_stage_);
     if (frame_stage_) cudaFreeHost(frame_stage_);
+    if (frame_dev_) cudaFree(frame_dev_);
     if (frame_ev_) cudaEventDestroy(frame_ev_);
     if (upload_ev_) cudaEventDestroy(upload_ev_);
     if (copy_stream_) cudaStreamDestroy(copy_stream_);
@@ -851,76 +853,109 @@ class Batch : public BatchBase {
   mpmgpu_status frame_begin(int job) override {
     HJob* j;
     MPM_TRY(live_job(job, &j));
-    MPM_TRY(frame_wait());   // the previous frame's buffer is reused
-    struct Copy {
-      const void* src;
-      size_t bytes;
-      const void** slot;
-    };
-    std::vector<Copy> cp;
-    std::set<const void**> seen;
-    auto add = [&](const void* src, size_t bytes, const void** slot) {
-      if (src != nullptr && seen.insert(slot).second) cp.push_back({src, bytes, slot});
-    };
-    auto slot = [](auto& p) { return reinterpret_cast<const void**>(&p); };
+    MPM_TRY(frame_wait());   // the previous frame's buffers are reused
     Frame f;
     f.job = job;
     f.primed = j->primed && j->block_off >= 0;
-    f.dt = j->sp.dt;
-    f.g = j->g;
+    f.nnodes = j->g.nnodes;
     for (int d = 0; d < 3; d++) f.grav[d] = j->sp.grav[d];
-    f.pts.assign(j->bodies.size(), PointView{});
-    f.nodes.assign(j->bodies.size(), NodeView{});
-    f.contact.assign((size_t)j->nc, {nullptr, nullptr});
-    add(err_, sizeof(int), slot(f.err));
-    static const int fields[] = {MPMGPU_P_X, MPMGPU_P_U, MPMGPU_P_X_T, MPMGPU_P_MX_T, MPMGPU_P_T,
-                                 MPMGPU_P_V, MPMGPU_P_M, MPMGPU_P_EXTENT, MPMGPU_P_ACTIVE, MPMGPU_P_L,
-                                 MPMGPU_P_GAMMAP, MPMGPU_P_GAMMAP_DOT};
-    const size_t ns = (size_t)j->g.nslots * sizeof(double);
+    // layout of the frame: per body its point fields, then its node fields;
+    // then the contacts
+    int64_t off = 0;
+    auto take = [&](int64_t n) {
+      const int64_t o = off;
+      off += (n + 31) / 32 * 32;   // 256-byte aligned fields
+      return o;
+    };
+    const int64_t nn = j->g.nnodes;
+    for (const HBody& B : j->bodies) {
+      FramePointLayout pl;
+      const int64_t n = B.n;
+      pl.x = take(3 * n);
+      pl.u = take(3 * n);
+      pl.xt = take(3 * n);
+      pl.mxt = take(3 * n);
+      pl.T = take(9 * n);
+      pl.v = take(n);
+      pl.m = take(n);
+      pl.ext = take(n);
+      pl.active = take(n);
+      pl.L = B.P.L ? take(9 * n) : -1;
+      const bool sand = B.mat.has_material && B.mat.kind == 2 && B.P.ms[0] != nullptr;
+      pl.gammap = sand ? take(n) : -1;
+      pl.gammap_dot = sand ? take(n) : -1;
+      f.pts.push_back(pl);
+      f.npts.push_back(n);
+      FrameNodeLayout nl;
+      const bool dbg = B.snap.m != nullptr;
+      nl.m = dbg ? take(nn) : -1;
+      nl.mxt = dbg ? take(3 * nn) : -1;
+      nl.f = dbg ? take(3 * nn) : -1;
+      nl.xt = take(3 * nn);
+      nl.u = take(3 * nn);
+      nl.dxt = take(3 * nn);
+      f.nodes.push_back(nl);
+    }
+    for (int c = 0; c < j->nc; c++) {
+      const bool kept = j->normal_out[c] != nullptr && j->force_out[c] != nullptr;
+      f.contact.push_back({kept ? take(3 * nn) : -1, kept ? take(3 * nn) : -1});
+    }
+    const size_t bytes = (size_t)off * sizeof(double) + 256;   // + the error flag
+    if (bytes > frame_dev_cap_ || bytes > frame_cap_) {
+      MPM_CUDA_TRY(cudaStreamSynchronize(stream_));
+      if (bytes > frame_dev_cap_) {
+        if (frame_dev_) cudaFree(frame_dev_);
+        frame_dev_ = nullptr;
+        frame_dev_cap_ = 0;
+        const cudaError_t e = cudaMalloc(&frame_dev_, bytes);
+        if (e != cudaSuccess) return fail(MPMGPU_ERR_NOMEM, std::string("frame staging: ") + cudaGetErrorString(e));
+        frame_dev_cap_ = bytes;
+      }
+      if (bytes > frame_cap_) {
+        if (frame_stage_) cudaFreeHost(frame_stage_);
+        frame_stage_ = nullptr;
+        frame_cap_ = 0;
+        MPM_CUDA_TRY(cudaHostAlloc(&frame_stage_, bytes, cudaHostAllocDefault));
+        frame_cap_ = bytes;
+      }
+    }
+    double* out = reinterpret_cast<double*>(frame_dev_);
+    const uint8_t* act = j->block_off >= 0 ? was_active_ + j->block_off : nullptr;
+    const int blocks = sm_count_ * 8;
     for (size_t b = 0; b < j->bodies.size(); b++) {
       const HBody& B = j->bodies[b];
-      f.pts[b].n = B.n;
-      for (int field : fields) {
-        if (field == MPMGPU_P_L && !B.P.L) continue;
-        if ((field == MPMGPU_P_GAMMAP || field == MPMGPU_P_GAMMAP_DOT) && B.mat.kind != 2) continue;
-        point_field_arrays(B, field, f.pts[b], add);
+      if (B.n > 0) {
+        k_frame_points<PT><<<blocks, 256, 0, stream_>>>(B.P, dim_, f.pts[b], out);
+        MPM_TRY(check_launch("k_frame_points"));
       }
-      if (!f.primed) continue;
-      NodeView& nv = f.nodes[b];
-      add(was_active_ + j->block_off, (size_t)j->g.nblocks, slot(nv.act));
-      add(B.snap.m, ns, slot(nv.m));
-      for (int d = 0; d < dim_; d++) {
-        add(B.snap.mx[d], ns, slot(nv.mx[d]));
-        add(B.snap.f[d], ns, slot(nv.f[d]));
-        add(B.V.vt[d], ns, slot(nv.vt[d]));
-        add(B.V.dv[d], ns, slot(nv.dv[d]));
+      if (f.primed) {
+        k_frame_nodes<<<blocks, 256, 0, stream_>>>(j->g, j->sp.dt, act, B.snap, B.V, f.nodes[b], out);
+        MPM_TRY(check_launch("k_frame_nodes"));
+      } else {
+        const FrameNodeLayout& nl = f.nodes[b];
+        const int64_t first = nl.m >= 0 ? nl.m : nl.xt;
+        const int64_t last = nl.dxt + 3 * nn;
+        MPM_CUDA_TRY(cudaMemsetAsync(out + first, 0, (size_t)(last - first) * sizeof(double), stream_));
       }
     }
-    if (j->block_off >= 0 && !f.primed) add(was_active_ + j->block_off, (size_t)j->g.nblocks, slot(f.act));
     for (int c = 0; c < j->nc; c++) {
-      add(j->normal_out[c], 3 * ns, slot(f.contact[(size_t)c].first));
-      add(j->force_out[c], 3 * ns, slot(f.contact[(size_t)c].second));
+      if (f.contact[(size_t)c].first < 0) continue;
+      k_frame_contact<<<blocks, 256, 0, stream_>>>(j->g, f.primed ? 1 : 0, act, j->normal_out[c], 1,
+                                                   out + f.contact[(size_t)c].first);
+      k_frame_contact<<<blocks, 256, 0, stream_>>>(j->g, f.primed ? 1 : 0, act, j->force_out[c], 0,
+                                                   out + f.contact[(size_t)c].second);
+      MPM_TRY(check_launch("k_frame_contact"));
     }
-    size_t total = 0;
-    for (const Copy& c : cp) total += (c.bytes + 255) / 256 * 256;
-    if (total > frame_cap_) {
-      MPM_CUDA_TRY(cudaStreamSynchronize(stream_));
-      if (frame_stage_) cudaFreeHost(frame_stage_);
-      frame_stage_ = nullptr;
-      frame_cap_ = 0;
-      const size_t cap = std::max<size_t>(total, (size_t)16 << 20);
-      MPM_CUDA_TRY(cudaHostAlloc(&frame_stage_, cap, cudaHostAllocDefault));
-      frame_cap_ = cap;
-    }
+    unsigned char* host = static_cast<unsigned char*>(frame_stage_);
+    MPM_CUDA_TRY(cudaMemcpyAsync(host + (size_t)off * sizeof(double), err_, sizeof(int), cudaMemcpyDeviceToHost,
+                                 stream_));
+    if (off > 0)
+      MPM_CUDA_TRY(
+          cudaMemcpyAsync(host, frame_dev_, (size_t)off * sizeof(double), cudaMemcpyDeviceToHost, stream_));
     if (!frame_ev_) MPM_CUDA_TRY(cudaEventCreateWithFlags(&frame_ev_, cudaEventDisableTiming));
-    unsigned char* base = static_cast<unsigned char*>(frame_stage_);
-    size_t off = 0;
-    for (const Copy& c : cp) {
-      if (c.bytes > 0) MPM_CUDA_TRY(cudaMemcpyAsync(base + off, c.src, c.bytes, cudaMemcpyDeviceToHost, stream_));
-      *c.slot = base + off;
-      off += (c.bytes + 255) / 256 * 256;
-    }
     MPM_CUDA_TRY(cudaEventRecord(frame_ev_, stream_));
+    f.data = reinterpret_cast<const double*>(host);
+    f.err = reinterpret_cast<const int*>(host + (size_t)off * sizeof(double));
     f.pending = true;
     frame_ = std::move(f);
     return MPMGPU_OK;
@@ -929,64 +964,64 @@ class Batch : public BatchBase {
   mpmgpu_status frame_points(int job, int body, int field, double* out) override {
     HBody* B;
     MPM_TRY(frame_body(job, body, &B));
+    const int64_t n = frame_.npts[(size_t)body];
     if (field == MPMGPU_P_B) {
-      for (int64_t i = 0; i < frame_.pts[(size_t)body].n; i++)
+      for (int64_t i = 0; i < n; i++)
         for (int d = 0; d < 3; d++) out[3 * i + d] = frame_.grav[d];
       return MPMGPU_OK;
     }
     MPM_TRY(point_field_check(*B, field));
+    const FramePointLayout& pl = frame_.pts[(size_t)body];
+    int64_t o = -1, w = 1;
+    switch (field) {
+      case MPMGPU_P_X: o = pl.x; w = 3; break;
+      case MPMGPU_P_U: o = pl.u; w = 3; break;
+      case MPMGPU_P_X_T: o = pl.xt; w = 3; break;
+      case MPMGPU_P_MX_T: o = pl.mxt; w = 3; break;
+      case MPMGPU_P_T: o = pl.T; w = 9; break;
+      case MPMGPU_P_L: o = pl.L; w = 9; break;
+      case MPMGPU_P_V: o = pl.v; break;
+      case MPMGPU_P_M: o = pl.m; break;
+      case MPMGPU_P_EXTENT: o = pl.ext; break;
+      case MPMGPU_P_ACTIVE: o = pl.active; break;
+      case MPMGPU_P_GAMMAP: o = pl.gammap; break;
+      case MPMGPU_P_GAMMAP_DOT: o = pl.gammap_dot; break;
+    }
+    if (o < 0) return fail(MPMGPU_ERR_STATE, "field not in the frame");
     MPM_TRY(frame_wait());
-    points_to_ref(frame_.pts[(size_t)body], field, out);
+    std::memcpy(out, frame_.data + o, (size_t)(n * w) * sizeof(double));
     return MPMGPU_OK;
   }
 
   mpmgpu_status frame_nodes(int job, int body, int field, double* out) override {
     HBody* B;
     MPM_TRY(frame_body(job, body, &B));
-    const Geom& g = frame_.g;
-    const int D = dim_;
-    const bool dbg = B->snap.m != nullptr;
-    const bool vec = field != MPMGPU_N_M;
-    if ((field == MPMGPU_N_M || field == MPMGPU_N_MX_T || field == MPMGPU_N_F) && !dbg)
-      return fail(MPMGPU_ERR_STATE, "nodal m, mx_t and f are kept only with keep_debug");
-    if (field < MPMGPU_N_M || field > MPMGPU_N_DIFF_X_T) return fail(MPMGPU_ERR_ARG, "unknown node field");
-    MPM_TRY(frame_wait());
-    if (!frame_.primed) {
-      for (int64_t i = 0; i < g.nnodes * (vec ? 3 : 1); i++) out[i] = 0.0;
-      return MPMGPU_OK;
-    }
-    const NodeView& nv = frame_.nodes[(size_t)body];
+    const FrameNodeLayout& nl = frame_.nodes[(size_t)body];
+    int64_t o = -1, w = 3;
     switch (field) {
-      case MPMGPU_N_M: nodes_host_to_ref(g, nv.act, &nv.m, 1, 1, out); break;
-      case MPMGPU_N_MX_T: nodes_host_to_ref(g, nv.act, nv.mx, D, 3, out); break;
-      case MPMGPU_N_F: nodes_host_to_ref(g, nv.act, nv.f, D, 3, out); break;
-      case MPMGPU_N_X_T: nodes_host_to_ref(g, nv.act, nv.vt, D, 3, out); break;
-      case MPMGPU_N_DIFF_X_T: nodes_host_to_ref(g, nv.act, nv.dv, D, 3, out); break;
-      case MPMGPU_N_U:
-        nodes_host_to_ref(g, nv.act, nv.vt, D, 3, out);
-        // moveGrid: u = dt * x_t (explicit_usl.cpp:252)
-        for (int64_t i = 0; i < 3 * g.nnodes; i++) out[i] = frame_.dt * out[i];
-        break;
+      case MPMGPU_N_M: o = nl.m; w = 1; break;
+      case MPMGPU_N_MX_T: o = nl.mxt; break;
+      case MPMGPU_N_F: o = nl.f; break;
+      case MPMGPU_N_X_T: o = nl.xt; break;
+      case MPMGPU_N_U: o = nl.u; break;
+      case MPMGPU_N_DIFF_X_T: o = nl.dxt; break;
+      default: return fail(MPMGPU_ERR_ARG, "unknown node field");
     }
+    if (o < 0) return fail(MPMGPU_ERR_STATE, "nodal m, mx_t and f are kept only with keep_debug");
+    MPM_TRY(frame_wait());
+    std::memcpy(out, frame_.data + o, (size_t)(frame_.nnodes * w) * sizeof(double));
     return MPMGPU_OK;
   }
 
   mpmgpu_status frame_contact(int job, int contact, int field, double* out) override {
     if (job != frame_.job) return fail(MPMGPU_ERR_STATE, "no frame of this job was begun");
     if (contact < 0 || contact >= (int)frame_.contact.size()) return fail(MPMGPU_ERR_ARG, "no such contact");
-    if (!keep_debug_) return fail(MPMGPU_ERR_STATE, "contact fields are kept only with keep_debug");
     if (field != MPMGPU_C_NORMAL && field != MPMGPU_C_FORCE) return fail(MPMGPU_ERR_ARG, "unknown contact field");
+    const auto& cl = frame_.contact[(size_t)contact];
+    const int64_t o = field == MPMGPU_C_NORMAL ? cl.first : cl.second;
+    if (o < 0) return fail(MPMGPU_ERR_STATE, "contact fields are kept only with keep_debug");
     MPM_TRY(frame_wait());
-    const Geom& g = frame_.g;
-    const auto& cv = frame_.contact[(size_t)contact];
-    const double* src = field == MPMGPU_C_NORMAL ? cv.first : cv.second;
-    const uint8_t* act = frame_.primed ? frame_.nodes[0].act : frame_.act;
-    std::vector<uint8_t> none;
-    if (act == nullptr) {
-      none.assign((size_t)g.nblocks, 0);
-      act = none.data();
-    }
-    contact_host_to_ref(g, frame_.primed, act, src, field == MPMGPU_C_NORMAL, out);
+    std::memcpy(out, frame_.data + o, (size_t)(3 * frame_.nnodes) * sizeof(double));
     return MPMGPU_OK;
   }
 
@@ -2178,30 +2213,25 @@ class Batch : public BatchBase {
   std::vector<BodyCtx<PT>> ctx_host_;   // host copy of the body table
   bool single_mode_ = false;
   bool any_plain_ = false, any_normal_ = false;
-  // the frame in flight or last taken (frame_begin)
-  struct NodeView {
-    const uint8_t* act = nullptr;   // the job's node blocks active in the frame's step
-    const double* m = nullptr;
-    const double* mx[3] = {};
-    const double* f[3] = {};
-    const double* vt[3] = {};
-    const double* dv[3] = {};
-  };
+  // the frame in flight or last taken (frame_begin): field offsets (in
+  // doubles) in its pinned copy
   struct Frame {
     int job = -1;
     bool pending = false;
     bool primed = false;
-    double dt = 0.0;
+    int64_t nnodes = 0;
     double grav[3] = {0.0, 0.0, 0.0};
-    Geom g{};
-    std::vector<PointView> pts;
-    std::vector<NodeView> nodes;
-    std::vector<std::pair<const double*, const double*>> contact;   // normal, force
-    const uint8_t* act = nullptr;   // node blocks of an unprimed job (all inactive)
+    std::vector<FramePointLayout> pts;
+    std::vector<int64_t> npts;
+    std::vector<FrameNodeLayout> nodes;
+    std::vector<std::pair<int64_t, int64_t>> contact;   // normal, force
+    const double* data = nullptr;
     const int* err = nullptr;
   } frame_;
-  void* frame_stage_ = nullptr;
+  void* frame_stage_ = nullptr;   // pinned host copy
   size_t frame_cap_ = 0;
+  void* frame_dev_ = nullptr;     // device staging in the reference layout
+  size_t frame_dev_cap_ = 0;
   cudaEvent_t frame_ev_ = nullptr;
 
   mpmgpu_status frame_wait() {

@@ -228,39 +228,38 @@ void run_tasks(std::vector<std::function<void()>>& tasks, unsigned threads) {
 // The host arrays the serializer reads at a frame (DefaultPoints::writeFrame,
 // default_points.cpp:341-368; DefaultNodes::writeFrame,
 // default_nodes.cpp:68-82; ContactHuang's contact arrays,
-// contact_huang.cpp:202-206). The copies are queued behind the step that
-// just ran; with overlap on, the driver's next step is queued behind them
-// (DefaultDriver::run calls step, then writeFrame, then advances t,
-// default_driver.cpp:62-83, so that step comes next; its gravity is already
-// set), and the fields are converted to the reference layout on host threads
-// while the GPU runs it.
+// contact_huang.cpp:202-206). The device writes every field in the
+// reference's layout and order into one buffer and copies it to pinned host
+// memory behind the step that just ran; with overlap on, the driver's next
+// step is queued behind the copies (DefaultDriver::run calls step, then
+// writeFrame, then advances t, default_driver.cpp:62-83, so that step comes
+// next; its gravity is already set). The fields are then copied straight
+// into the reference arrays' buffers (3 doubles per vector, 9 per tensor,
+// mpm_vectorarray.hpp:29, mpm_tensorarray.hpp:31) on host threads while the
+// GPU runs that step.
 void GPUExplicitUSL::writeBack(Job* job) {
   check(mpmgpu_frame_begin(handle), "mpmgpu_frame_begin");
   if (overlap) {
     check(mpmgpu_step(handle, 1), "mpmgpu_step");
     queued_ahead = true;
   }
-  // the first field waits for the copies; the rest convert in parallel
   std::vector<std::function<void()>> tasks;
-  std::vector<std::vector<double>> bufs;
-  bufs.reserve(64);
-  auto buffer = [&](size_t n) -> double* {
-    bufs.emplace_back(n);
-    return bufs.back().data();
-  };
+  std::vector<std::vector<double>> bufs;   // fields whose reference storage is not double
   bool waited = false;
-  auto point_task = [&](int id, int field, int n, int width, std::function<void(const double*)> store) {
-    double* b = buffer((size_t)n * width);
-    auto run = [this, id, field, b, store]() {
-      check(mpmgpu_frame_points(handle, id, field, b), "mpmgpu_frame_points");
-      store(b);
-    };
+  // the first copy waits for the frame; the rest run in parallel
+  auto add = [&](std::function<void()> run) {
     if (!waited) {
       run();
       waited = true;
     } else {
-      tasks.push_back(run);
+      tasks.push_back(std::move(run));
     }
+  };
+  auto point_field = [&](int id, int field, double* dst) {
+    add([this, id, field, dst]() { check(mpmgpu_frame_points(handle, id, field, dst), "mpmgpu_frame_points"); });
+  };
+  auto node_field = [&](int id, int field, double* dst) {
+    add([this, id, field, dst]() { check(mpmgpu_frame_nodes(handle, id, field, dst), "mpmgpu_frame_nodes"); });
   };
   for (size_t bi = 0; bi < job->bodies.size(); bi++) {
     const int id = gpu_body[bi];
@@ -268,82 +267,43 @@ void GPUExplicitUSL::writeBack(Job* job) {
     Points* pts = job->bodies[bi]->points.get();
     Nodes* nds = job->bodies[bi]->nodes.get();
     const int n = pts->x.size();
-    auto vec3 = [n](KinematicVectorArray& arr) {
-      return [n, &arr](const double* b) {
-        for (int i = 0; i < n; i++)
-          for (int j = 0; j < 3; j++) arr(i, j) = b[3 * i + j];
-      };
-    };
-    point_task(id, MPMGPU_P_X, n, 3, vec3(pts->x));
-    point_task(id, MPMGPU_P_U, n, 3, vec3(pts->u));
-    point_task(id, MPMGPU_P_X_T, n, 3, vec3(pts->x_t));
-    point_task(id, MPMGPU_P_MX_T, n, 3, vec3(pts->mx_t));
-    if (mode != MPMGPU_MODE_MIXED) {
-      // the velocity gradient is kept on the device in the FP64 forms only
-      point_task(id, MPMGPU_P_L, n, 9, [n, pts](const double* b) {
-        for (int i = 0; i < n; i++)
-          for (int k = 0; k < 9; k++) pts->L[i][k] = b[9 * i + k];
-      });
-    }
-    point_task(id, MPMGPU_P_T, n, 9, [n, pts](const double* b) {
-      for (int i = 0; i < n; i++)
-        for (int k = 0; k < 9; k++) pts->T[i][k] = b[9 * i + k];
-    });
-    point_task(id, MPMGPU_P_V, n, 1, [n, pts](const double* b) {
-      for (int i = 0; i < n; i++) pts->v(i) = b[i];
-    });
-    point_task(id, MPMGPU_P_ACTIVE, n, 1, [n, pts](const double* b) {
-      for (int i = 0; i < n; i++) pts->active(i) = (int)b[i];
+    point_field(id, MPMGPU_P_X, pts->x.data());
+    point_field(id, MPMGPU_P_U, pts->u.data());
+    point_field(id, MPMGPU_P_X_T, pts->x_t.data());
+    point_field(id, MPMGPU_P_MX_T, pts->mx_t.data());
+    // the velocity gradient is kept on the device in the FP64 forms only
+    if (mode != MPMGPU_MODE_MIXED) point_field(id, MPMGPU_P_L, pts->L.data());
+    point_field(id, MPMGPU_P_T, pts->T.data());
+    point_field(id, MPMGPU_P_V, pts->v.data());
+    bufs.emplace_back((size_t)n);
+    double* ab = bufs.back().data();
+    add([this, id, n, ab, pts]() {
+      check(mpmgpu_frame_points(handle, id, MPMGPU_P_ACTIVE, ab), "mpmgpu_frame_points");
+      for (int i = 0; i < n; i++) pts->active(i) = (int)ab[i];
     });
     Sand_SachithLocal* sand = job->bodies[bi]->activeMaterial
                                   ? dynamic_cast<Sand_SachithLocal*>(job->bodies[bi]->material.get())
                                   : nullptr;
     if (sand) {
       // the material's frame fields (Sand_SachithLocal::writeFrame)
-      point_task(id, MPMGPU_P_GAMMAP, n, 1, [n, sand](const double* b) {
-        for (int i = 0; i < n; i++) sand->gammap(i) = b[i];
-      });
-      point_task(id, MPMGPU_P_GAMMAP_DOT, n, 1, [n, sand](const double* b) {
-        for (int i = 0; i < n; i++) sand->gammap_dot(i) = b[i];
-      });
+      point_field(id, MPMGPU_P_GAMMAP, sand->gammap.data());
+      point_field(id, MPMGPU_P_GAMMAP_DOT, sand->gammap_dot.data());
     }
-    const int nn = nds->x.size();
-    auto node_task = [&, id, nn](int field, int width, std::function<void(const double*)> store) {
-      double* b = buffer((size_t)nn * width);
-      tasks.push_back([this, id, field, b, store]() {
-        check(mpmgpu_frame_nodes(handle, id, field, b), "mpmgpu_frame_nodes");
-        store(b);
-      });
-    };
-    auto nvec3 = [nn](KinematicVectorArray& arr) {
-      return [nn, &arr](const double* b) {
-        for (int i = 0; i < nn; i++)
-          for (int j = 0; j < 3; j++) arr(i, j) = b[3 * i + j];
-      };
-    };
-    node_task(MPMGPU_N_M, 1, [nn, nds](const double* b) {
-      for (int i = 0; i < nn; i++) nds->m(i) = b[i];
-    });
-    node_task(MPMGPU_N_MX_T, 3, nvec3(nds->mx_t));
-    node_task(MPMGPU_N_F, 3, nvec3(nds->f));
-    node_task(MPMGPU_N_X_T, 3, nvec3(nds->x_t));
-    node_task(MPMGPU_N_U, 3, nvec3(nds->u));
-    node_task(MPMGPU_N_DIFF_X_T, 3, nvec3(nds->diff_x_t));
+    node_field(id, MPMGPU_N_M, nds->m.data());
+    node_field(id, MPMGPU_N_MX_T, nds->mx_t.data());
+    node_field(id, MPMGPU_N_F, nds->f.data());
+    node_field(id, MPMGPU_N_X_T, nds->x_t.data());
+    node_field(id, MPMGPU_N_U, nds->u.data());
+    node_field(id, MPMGPU_N_DIFF_X_T, nds->diff_x_t.data());
   }
   int gc = 0;
   for (size_t c = 0; c < job->contacts.size(); c++) {
     if (job->activeContacts[c] == 0) continue;
     ContactHuang* ch = dynamic_cast<ContactHuang*>(job->contacts[c].get());
-    const int nn = ch->contact_normal.size();
-    for (int field : {MPMGPU_C_NORMAL, MPMGPU_C_FORCE}) {
-      KinematicVectorArray& arr = field == MPMGPU_C_NORMAL ? ch->contact_normal : ch->contact_force;
-      double* b = buffer(3 * (size_t)nn);
-      tasks.push_back([this, gc, field, b, nn, &arr]() {
-        check(mpmgpu_frame_contact(handle, gc, field, b), "mpmgpu_frame_contact");
-        for (int i = 0; i < nn; i++)
-          for (int j = 0; j < 3; j++) arr(i, j) = b[3 * i + j];
-      });
-    }
+    double* nrm = ch->contact_normal.data();
+    double* frc = ch->contact_force.data();
+    add([this, gc, nrm]() { check(mpmgpu_frame_contact(handle, gc, MPMGPU_C_NORMAL, nrm), "mpmgpu_frame_contact"); });
+    add([this, gc, frc]() { check(mpmgpu_frame_contact(handle, gc, MPMGPU_C_FORCE, frc), "mpmgpu_frame_contact"); });
     gc++;
   }
   const unsigned hw = std::max(1u, std::thread::hardware_concurrency());

@@ -107,3 +107,21 @@ def test_malformed_lines_are_reported(mutate, line):
         f.writelines(mutate(lines))
     with pytest.raises(MpmGpuError, match=f"line {line} "):
         read_points_file(files[0], 2)
+
+
+def test_2d_lines_with_three_coordinates_are_malformed_as_in_the_reference():
+    """DefaultPoints::readFromFile accepts 1 + 1 + DIM + DIM + 1 or
+    1 + 1 + GRID_DIM + GRID_DIM + 1 columns (default_points.cpp:150-176); for
+    the job types of this path (TYPE 2 and 3, job.hpp:58-71) DIM equals
+    GRID_DIM, so a 2D file takes 7 columns only, and a 9-column line ends the
+    reference's reading with an error, as it ends this reader's."""
+    case = inputs.block_drop_2d()
+    _, files = _write(case)
+    with open(files[0]) as f:
+        lines = f.readlines()
+    parts = lines[3].split()
+    lines[3] = " ".join(parts[:4] + ["0"] + parts[4:6] + ["0"] + parts[6:]) + "\n"   # x, y, 0, vx, vy, 0
+    with open(files[0], "w") as f:
+        f.writelines(lines)
+    with pytest.raises(MpmGpuError, match="line 4 "):
+        read_points_file(files[0], 2)
