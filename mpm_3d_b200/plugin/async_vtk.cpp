@@ -9,6 +9,9 @@
 #include <iomanip>
 #include <iostream>
 #include <sstream>
+#include <string>
+#include <thread>
+#include <vector>
 
 #include "job.hpp"
 #include "mpm_tensorarray.hpp"
@@ -277,74 +280,122 @@ void AsyncVTK::writerLoop() {
 
 namespace {
 
+// Text of the frames. DefaultVTK streams each number with the stream's
+// default formatting, which is printf's %g at the stream's precision, 6
+// (num_put), in the C locale; snprintf with "%.6g" gives the same
+// characters. Large arrays are formatted in chunks on several threads and
+// written in order.
+void put_num(std::string& s, double v) {
+  char buf[32];
+  const int k = std::snprintf(buf, sizeof(buf), "%.6g", v);
+  s.append(buf, (size_t)k);
+}
+
+void put_int(std::string& s, long v) {
+  char buf[24];
+  const int k = std::snprintf(buf, sizeof(buf), "%ld", v);
+  s.append(buf, (size_t)k);
+}
+
+// Formats entries [0, n) with `one(text, i)` into `out`, on up to 8 threads
+// for large arrays (chunks written in entry order).
+template <typename F>
+void emit(std::ofstream& out, int n, F one) {
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const int chunks = n < 65536 ? 1 : (int)std::min(hw, 8u);
+  std::vector<std::string> text((size_t)chunks);
+  auto run = [&](int c) {
+    const int b = (int)((int64_t)n * c / chunks), e = (int)((int64_t)n * (c + 1) / chunks);
+    std::string& t = text[(size_t)c];
+    t.reserve((size_t)(e - b) * 16);
+    for (int i = b; i < e; i++) one(t, i);
+  };
+  std::vector<std::thread> pool;
+  for (int c = 1; c < chunks; c++) pool.emplace_back(run, c);
+  run(0);
+  for (auto& th : pool) th.join();
+  for (const std::string& t : text) out.write(t.data(), (std::streamsize)t.size());
+}
+
 // The rules of DefaultVTK's writers (default_vtk.cpp): the header writes a
 // position component when the axis exists, the entry is active (!= 0) and
 // the value finite; scalar and vector arrays write a value when the entry's
 // flag is exactly 1 and the value finite; a point tensor is written when the
 // point is active and all 9 components are finite, a node tensor (written
 // three times per node, as the reference does) when its components are
-// finite. Everything else is written as 0. Numbers use the stream's default
-// formatting.
+// finite. Everything else is written as 0.
 void header(std::ofstream& out, const AsyncVTK::Block& blk, const std::vector<int>& active) {
   const int n = blk.count;
   out << "ASCII\n";
   out << "DATASET UNSTRUCTURED_GRID\n";
   out << "POINTS " << n << " double\n";
-  for (int i = 0; i < n; i++) {
+  emit(out, n, [&](std::string& t, int i) {
     for (int pos = 0; pos < 3; pos++) {
       const double v = blk.values[3 * (size_t)i + pos];
-      if (pos < blk.dim && active[(size_t)i] != 0 && std::isfinite(v))
-        out << v << " ";
-      else
-        out << "0 ";
+      if (pos < blk.dim && active[(size_t)i] != 0 && std::isfinite(v)) {
+        put_num(t, v);
+        t += ' ';
+      } else {
+        t += "0 ";
+      }
     }
-    out << "\n";
-  }
+    t += '\n';
+  });
   out << "CELLS " << n << " " << 2 * n << "\n";
-  for (int i = 0; i < n; i++) out << "1 " << i << "\n";
+  emit(out, n, [&](std::string& t, int i) {
+    t += "1 ";
+    put_int(t, i);
+    t += '\n';
+  });
   out << "CELL_TYPES " << n << "\n";
-  for (int i = 0; i < n; i++) out << "1\n";
+  emit(out, n, [&](std::string& t, int) { t += "1\n"; });
   out << "POINT_DATA " << n << "\n";
 }
 
 void scalars(std::ofstream& out, const AsyncVTK::Block& blk, const std::vector<int>& active) {
   out << "SCALARS " << blk.name << " double 1\n";
   out << "LOOKUP_TABLE default\n";
-  for (int i = 0; i < blk.count; i++) {
+  emit(out, blk.count, [&](std::string& t, int i) {
     const double v = blk.values[(size_t)i];
-    if (active[(size_t)i] == 1 && std::isfinite(v))
-      out << v << "\n";
-    else
-      out << "0" << "\n";
-  }
+    if (active[(size_t)i] == 1 && std::isfinite(v)) {
+      put_num(t, v);
+      t += '\n';
+    } else {
+      t += "0\n";
+    }
+  });
 }
 
 void vectors(std::ofstream& out, const AsyncVTK::Block& blk, const std::vector<int>& active) {
   out << "VECTORS " << blk.name << " double\n";
-  for (int i = 0; i < blk.count; i++) {
+  emit(out, blk.count, [&](std::string& t, int i) {
     for (int pos = 0; pos < 3; pos++) {
       const double v = blk.values[3 * (size_t)i + pos];
-      if (active[(size_t)i] == 1 && std::isfinite(v))
-        out << v << " ";
-      else
-        out << "0 ";
+      if (active[(size_t)i] == 1 && std::isfinite(v)) {
+        put_num(t, v);
+        t += ' ';
+      } else {
+        t += "0 ";
+      }
     }
-    out << "\n";
-  }
+    t += '\n';
+  });
 }
 
-void tensor_rows(std::ofstream& out, const double* t, bool write) {
+void tensor_rows(std::string& t, const double* v, bool write) {
   if (!write) {
-    out << "0 0 0\n";
-    out << "0 0 0\n";
-    out << "0 0 0\n";
-    out << "\n";
+    t += "0 0 0\n0 0 0\n0 0 0\n\n";
     return;
   }
-  out << t[0] << " " << t[1] << " " << t[2] << "\n";
-  out << t[3] << " " << t[4] << " " << t[5] << "\n";
-  out << t[6] << " " << t[7] << " " << t[8] << "\n";
-  out << "\n";
+  for (int r = 0; r < 3; r++) {
+    put_num(t, v[3 * r]);
+    t += ' ';
+    put_num(t, v[3 * r + 1]);
+    t += ' ';
+    put_num(t, v[3 * r + 2]);
+    t += '\n';
+  }
+  t += '\n';
 }
 
 bool all_finite(const double* t) {
@@ -355,19 +406,19 @@ bool all_finite(const double* t) {
 
 void point_tensors(std::ofstream& out, const AsyncVTK::Block& blk, const std::vector<int>& active) {
   out << "TENSORS " << blk.name << " double\n";
-  for (int i = 0; i < blk.count; i++) {
-    const double* t = blk.values.data() + 9 * (size_t)i;
-    tensor_rows(out, t, active[(size_t)i] != 0 && all_finite(t));
-  }
+  emit(out, blk.count, [&](std::string& t, int i) {
+    const double* v = blk.values.data() + 9 * (size_t)i;
+    tensor_rows(t, v, active[(size_t)i] != 0 && all_finite(v));
+  });
 }
 
 void node_tensors(std::ofstream& out, const AsyncVTK::Block& blk) {
   out << "TENSORS " << blk.name << " double\n";
-  for (int i = 0; i < blk.count; i++) {
-    const double* t = blk.values.data() + 9 * (size_t)i;
-    const bool finite = all_finite(t);
-    for (int rep = 0; rep < 3; rep++) tensor_rows(out, t, finite);
-  }
+  emit(out, blk.count, [&](std::string& t, int i) {
+    const double* v = blk.values.data() + 9 * (size_t)i;
+    const bool finite = all_finite(v);
+    for (int rep = 0; rep < 3; rep++) tensor_rows(t, v, finite);
+  });
 }
 
 }  // namespace

@@ -37,6 +37,9 @@ CASES = {
     "collision_3d_touching": (lambda: inputs.two_body_collision_3d(8, steps=10, gap=0.02), 10),
     "sand_column_2d": (lambda: inputs.sand_column(2, steps=20), 20),
     "wall_exit_2d": (_wall_exit_2d, 25),
+    # 49,152 points on 139,425 nodes: arrays large enough to be formatted in
+    # chunks on several threads
+    "column_3d_s4": (lambda: inputs.column_collapse_3d(scale=4, steps=10), 10),
 }
 
 
