@@ -279,11 +279,11 @@ typedef enum {
    * 1024 (3D mixed), 512 (2D); the only form of 2D jobs and of the
    * deterministic form */
   MPMGPU_KERNEL_STAGED = 0,
-  /* one point per thread from gather to scatter, point state read from
-   * global memory: 128 or 256 points per item (3D) */
-  MPMGPU_KERNEL_POINT_PER_THREAD = 1,
-  /* as above, with the item's point arrays staged by bulk copies */
-  MPMGPU_KERNEL_POINT_PER_THREAD_STAGED = 2
+  /* each thread takes its points from gather to scatter, point state read
+   * from global memory: 128 points per item (CTAs of 128 threads), 256
+   * (256 threads) or 512 (256 threads, two points each); 3D, not the
+   * deterministic form */
+  MPMGPU_KERNEL_POINT_PER_THREAD = 1
 } mpmgpu_kernel_form;
 
 /* Selects the fused kernel's form and points per work item (default: one
@@ -326,11 +326,11 @@ typedef struct {
   int device;          /* CUDA device ordinal */
   int sort_interval;   /* steps between re-binnings (0 = default 32) */
   int points_per_item; /* points per CTA work item: 0 = default (3D,
-                          not deterministic: 256 on the one-point-per-thread
-                          kernel; else 512 on the staged kernel); 128 or 256
-                          run on the one-point-per-thread kernel where it
-                          applies, other sizes on the staged kernel (3D: 256
-                          or 512 in FP64, 256, 512 or 1024 mixed); see
+                          not deterministic: 256 on the point-per-thread
+                          kernel; else 512 on the staged kernel); 128, 256
+                          or 512 run on the point-per-thread kernel where
+                          it applies, other sizes on the staged kernel
+                          (1024 in the 3D mixed form, 512 in 2D); see
                           mpmgpu_set_kernel and mpmgpu_batch_autotune */
   int no_graph;        /* 1: launch stage by stage instead of graph replay */
   int keep_debug;      /* as mpmgpu_config.keep_debug */
@@ -392,8 +392,8 @@ mpmgpu_status mpmgpu_batch_counts(const mpmgpu_batch* b, int* live_jobs, int64_t
 
 /* Tunes the launch shape on the current jobs: times `steps` steps for every
  * available kernel form and points-per-item choice (staged 256, 512, 1024;
- * one point per thread 128, 256; one point per thread with staged point
- * arrays 256), then 32 steps for each re-binning interval (4, 8, 16, 32),
+ * point per thread 128, 256, 512), then 32 steps for each re-binning
+ * interval (4, 8, 16, 32),
  * restoring the jobs' state after each trial, and keeps the fastest of
  * each. The jobs' state after the call is the state before it. */
 mpmgpu_status mpmgpu_batch_autotune(mpmgpu_batch* b, int steps, int* points_per_item);

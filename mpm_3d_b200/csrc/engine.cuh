@@ -144,14 +144,13 @@ inline bool cap_available(int dim, bool mixed, int cap) {
 
 // Forms of the fused kernel (mpmgpu_set_kernel): the staged kernel
 // (fused.cuh: point arrays staged in shared memory, gather and scatter
-// phases apart, up to 1024 points per CTA), the one-point-per-thread kernel
-// (fused_lean.cuh, 3D, not the deterministic form), and the latter with its
-// items' point arrays staged by bulk copies.
-enum { kFormStaged = 0, kFormLean = 1, kFormLeanStaged = 2 };
+// phases apart, up to 1024 points per CTA) and the point-per-thread kernel
+// (fused_lean.cuh, 3D, not the deterministic form).
+enum { kFormStaged = 0, kFormLean = 1 };
 
 inline bool form_available(int dim, bool mixed, bool det, int form, int cap) {
   if (form == kFormStaged) return cap_available(dim, mixed, cap);
-  if (form == kFormLean || form == kFormLeanStaged) return dim == 3 && !det && lean_size_ok(cap);
+  if (form == kFormLean) return dim == 3 && !det && lean_size_ok(cap);
   return false;
 }
 
@@ -245,8 +244,8 @@ class BatchBase {
   virtual void counts(int* live_jobs, int64_t* live_points) const = 0;
   virtual int points_per_item() const = 0;
   virtual int sort_interval() const = 0;
-  // Form of the fused kernel (kFormStaged, kFormLean, kFormLeanStaged) and
-  // its points per work item; chosen at creation (the one-point-per-thread
+  // Form of the fused kernel (kFormStaged, kFormLean) and
+  // its points per work item; chosen at creation (the point-per-thread
   // kernel with 256 points in 3D, the staged kernel otherwise), by the
   // autotuner, or by set_kernel.
   virtual int kernel_form() const = 0;
@@ -322,7 +321,7 @@ class Batch : public BatchBase {
       uint64_t keep = UINT64_MAX;
       MPM_CUDA_TRY(cudaMemPoolSetAttribute(pool_, cudaMemPoolAttrReleaseThreshold, &keep));
     }
-    // a requested item size is served by the one-point-per-thread kernel
+    // a requested item size is served by the point-per-thread kernel
     // where it has that size, else by the staged kernel
     if (cap_ == 0) cap_ = (dim_ == 3 && !det_) ? kDefaultLeanCap : default_cap();
     form_ = form_available(dim_, mixed(), det_, kFormLean, cap_) ? kFormLean : kFormStaged;
@@ -1198,8 +1197,8 @@ class Batch : public BatchBase {
     int best_c = original_cap, best_f = original_form, best_si = original_si;
     float best_ms = 1e30f;
     // kernel form and points per item
-    const int cand[6][2] = {{kFormStaged, 256}, {kFormStaged, 512},   {kFormStaged, 1024},
-                            {kFormLean, 128},   {kFormLean, 256},     {kFormLeanStaged, 256}};
+    const int cand[6][2] = {{kFormStaged, 256}, {kFormStaged, 512}, {kFormStaged, 1024},
+                            {kFormLean, 128},   {kFormLean, 256},   {kFormLean, 512}};
     for (int ci = 0; ci < 6 && st == MPMGPU_OK; ci++) {
       const int f = cand[ci][0], c = cand[ci][1];
       if (!form_available(dim_, mixed(), det_, f, c) || (det_ && c != default_cap())) continue;
@@ -1875,7 +1874,7 @@ class Batch : public BatchBase {
     return MPMGPU_OK;
   }
 
-  template <int NT, bool NORMAL, bool SINGLE, int MAT, bool STAGE>
+  template <int NT, int PPT, bool NORMAL, bool SINGLE, int MAT>
   mpmgpu_status launch_lean_k(int prime_pass, int phases, int one_body) {
     FusedLaunch<PT> fl{};
     if (SINGLE) fl.one = ctx_host_[(size_t)one_body];
@@ -1897,10 +1896,10 @@ class Batch : public BatchBase {
     fl.phases = phases;
     fl.bounds = nullptr;
     fl.wait_polls = wait_polls_;
-    constexpr size_t smem = lean_smem_bytes<3, PT, NT, NORMAL, STAGE>();
-    auto kern = k_g2p2g_lean<3, PT, NT, NORMAL, SINGLE, MAT, STAGE>;
+    constexpr size_t smem = lean_smem_bytes<3, PT, NORMAL>();
+    auto kern = k_g2p2g_lean<3, PT, NT, PPT, NORMAL, SINGLE, MAT>;
     int& per_sm =
-        lean_per_sm_[(STAGE ? 16 : 0) + (NT == 128 ? 8 : 0) + (NORMAL ? 4 : 0) + (SINGLE ? 2 : 0) + (MAT == 0 ? 1 : 0)];
+        lean_per_sm_[(PPT == 2 ? 16 : 0) + (NT == 128 ? 8 : 0) + (NORMAL ? 4 : 0) + (SINGLE ? 2 : 0) + (MAT == 0 ? 1 : 0)];
     if (per_sm == 0) {
       MPM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
       MPM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, smem));
@@ -1911,21 +1910,19 @@ class Batch : public BatchBase {
     return check_launch("k_g2p2g_lean");
   }
 
-  template <int NT, bool NORMAL, bool SINGLE, bool STAGE>
+  template <int NT, int PPT, bool NORMAL, bool SINGLE>
   mpmgpu_status launch_lean_s(int prime_pass, int phases, int one_body, bool elastic) {
-    if (elastic) return launch_lean_k<NT, NORMAL, SINGLE, 0, STAGE>(prime_pass, phases, one_body);
-    return launch_lean_k<NT, NORMAL, SINGLE, -1, STAGE>(prime_pass, phases, one_body);
+    if (elastic) return launch_lean_k<NT, PPT, NORMAL, SINGLE, 0>(prime_pass, phases, one_body);
+    return launch_lean_k<NT, PPT, NORMAL, SINGLE, -1>(prime_pass, phases, one_body);
   }
 
+  // points per item: 128 (CTAs of 128 threads), 256 (256 threads) or 512
+  // (256 threads, two points each)
   template <bool NORMAL, bool SINGLE>
   mpmgpu_status launch_lean_m(int prime_pass, int phases, int one_body, bool elastic) {
-    const bool stage = form_ == kFormLeanStaged;
-    if (cap_ == 128) {
-      if (stage) return launch_lean_s<128, NORMAL, SINGLE, true>(prime_pass, phases, one_body, elastic);
-      return launch_lean_s<128, NORMAL, SINGLE, false>(prime_pass, phases, one_body, elastic);
-    }
-    if (stage) return launch_lean_s<256, NORMAL, SINGLE, true>(prime_pass, phases, one_body, elastic);
-    return launch_lean_s<256, NORMAL, SINGLE, false>(prime_pass, phases, one_body, elastic);
+    if (cap_ == 128) return launch_lean_s<128, 1, NORMAL, SINGLE>(prime_pass, phases, one_body, elastic);
+    if (cap_ == 512) return launch_lean_s<256, 2, NORMAL, SINGLE>(prime_pass, phases, one_body, elastic);
+    return launch_lean_s<256, 1, NORMAL, SINGLE>(prime_pass, phases, one_body, elastic);
   }
 
   mpmgpu_status launch_lean(int prime_pass, int phases) {

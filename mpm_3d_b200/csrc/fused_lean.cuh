@@ -1,34 +1,37 @@
-// Lean form of the fused gather + point update + scatter kernel: one point
-// per thread and no staged copy of the point arrays.
+// Lean form of the fused gather + point update + scatter kernel: each thread
+// takes its points from gather to scatter, with no staged copy of the point
+// arrays.
 //
-// A CTA of NT threads works on one work item at a time (at most NT points
-// of one bin of one body):
-//   0. every thread issues the global loads of its own point (coalesced:
-//      consecutive threads, consecutive points) while the CTA stages the
-//      nodal velocities of the bin's node tile and clears a separate FP64
-//      accumulator tile;
-//   1. one barrier; then each thread takes its point through gather, state
-//      update (movePoints, calculateStrainRate, updateDensity,
+// A CTA of NT threads works on one work item at a time (at most PPT * NT
+// points of one bin of one body, PPT points per thread):
+//   0. the CTA stages the nodal velocities of the bin's node tile and clears
+//      a separate FP64 accumulator tile;
+//   1. one barrier; then each thread takes its points (global loads,
+//      coalesced: consecutive threads, consecutive points) through gather,
+//      state update (movePoints, calculateStrainRate, updateDensity,
 //      updateStress), map build at the new position and scatter into the
 //      accumulator tile, with no barrier between the phases;
 //   2. one barrier; the touched tile nodes are added into the global
 //      accumulators (one global atomic per node and value).
 // Shared memory holds only the two tiles (about 41 KB in FP64, 31 KB in the
-// mixed form), so residency is set by registers. The material is a template
-// parameter (MAT >= 0 compiles one constitutive model; -1 dispatches at run
-// time), which keeps the other models' state out of the register budget.
-// The arithmetic of every phase is the one of the staged kernel (fused.cuh),
-// so both kernels give the same results.
+// mixed form), so residency is set by registers: the register budget (80 per
+// thread in FP64, 64 in the mixed form) leaves room for 24 or 32 resident
+// warps per SM, and was measured faster than 128 registers without spills
+// at 16 warps. The material is a template parameter (MAT >= 0 compiles one
+// constitutive model; -1 dispatches at run time), which keeps the other
+// models' state out of the register budget. The arithmetic of every phase is
+// the one of the staged kernel (fused.cuh), so both kernels give the same
+// results up to the order of the nodal sums.
 #pragma once
 
 #include "fused.cuh"
 
 namespace mpmb200 {
 
-// Threads per CTA (= points per work item) of the two sizes the autotuner
-// chooses from: 256, or 128 for batches whose bins hold few points (a CTA
-// idles the threads its item does not fill).
-__host__ __device__ constexpr bool lean_size_ok(int nt) { return nt == 128 || nt == 256; }
+// Points per work item the autotuner chooses from: 128 (CTAs of 128
+// threads), 256 (256 threads) and 512 (256 threads, two points each: one
+// tile load, clear and flush for a whole 4x4x4 bin of 8 points per cell).
+__host__ __device__ constexpr bool lean_size_ok(int cap) { return cap == 128 || cap == 256 || cap == 512; }
 constexpr int kDefaultLeanCap = 256;
 
 // Resident CTAs per SM the register budget is sized for: 80 registers per
@@ -39,56 +42,25 @@ __host__ __device__ constexpr int lean_min_ctas() {
   return (sizeof(PT) == 4 ? 4 : 3) * (256 / NT);
 }
 
-// Shared memory: mbarriers (point arrays, table entry slots 0 and 1) |
-// table entry slots [2] | with STAGE: the item's point arrays [kNF][NT + 8]
-// and active flags [NT + 8] | velocity tile [2 DIM][TN] in the point
-// precision | accumulator tile [NACC][TN] FP64 | touched [TN].
-template <typename PT, int NT, bool STAGE>
-__host__ __device__ constexpr size_t lean_off_pts() {
+// Shared memory: mbarriers (table entry slots 0 and 1) | table entry slots
+// [2] | velocity tile [2 DIM][TN] in the point precision | accumulator tile
+// [NACC][TN] FP64 | touched [TN].
+template <int DIM, typename PT>
+__host__ __device__ constexpr size_t lean_off_tvel() {
   return kOffCtx + 2 * ctx_bytes<PT>();
 }
-template <typename PT, int NT, bool STAGE>
-__host__ __device__ constexpr size_t lean_off_act() {
-  return lean_off_pts<PT, NT, STAGE>() + (STAGE ? (sizeof(PT) * kNF * cap_row<NT>() + 15) / 16 * 16 : 0);
-}
-template <int DIM, typename PT, int NT, bool STAGE>
-__host__ __device__ constexpr size_t lean_off_tvel() {
-  return lean_off_act<PT, NT, STAGE>() + (STAGE ? (sizeof(int32_t) * cap_row<NT>() + 15) / 16 * 16 : 0);
-}
-template <int DIM, typename PT, int NT, bool STAGE>
+template <int DIM, typename PT>
 __host__ __device__ constexpr size_t lean_off_tacc() {
-  return (lean_off_tvel<DIM, PT, NT, STAGE>() + sizeof(PT) * 2 * DIM * fused_tile_nodes<DIM, fused_bin<DIM>()>() + 15) /
-         16 * 16;
+  return (lean_off_tvel<DIM, PT>() + sizeof(PT) * 2 * DIM * fused_tile_nodes<DIM, fused_bin<DIM>()>() + 15) / 16 * 16;
 }
-template <int DIM, typename PT, int NT, bool NORMAL, bool STAGE>
+template <int DIM, typename PT, bool NORMAL>
 __host__ __device__ constexpr size_t lean_off_touched() {
-  return lean_off_tacc<DIM, PT, NT, STAGE>() +
-         sizeof(double) * fused_nacc(NORMAL) * fused_tile_nodes<DIM, fused_bin<DIM>()>();
+  return lean_off_tacc<DIM, PT>() + sizeof(double) * fused_nacc(NORMAL) * fused_tile_nodes<DIM, fused_bin<DIM>()>();
 }
-template <int DIM, typename PT, int NT, bool NORMAL, bool STAGE>
+template <int DIM, typename PT, bool NORMAL>
 __host__ __device__ constexpr size_t lean_smem_bytes() {
-  return lean_off_touched<DIM, PT, NT, NORMAL, STAGE>() + fused_tile_nodes<DIM, fused_bin<DIM>()>();
+  return lean_off_touched<DIM, PT, NORMAL>() + fused_tile_nodes<DIM, fused_bin<DIM>()>();
 }
-
-// Reads of one point's state: from its column of the staged arrays (stride
-// ROW) when the item was staged, else from global memory.
-template <typename PT, int ROW, bool STAGE>
-struct PointSrc {
-  const PointsT<PT>& P;
-  int64_t p;
-  const PT* sp;
-  __device__ __forceinline__ PT get(int f, const PT* g) const {
-    if constexpr (STAGE) return sp[f * ROW];
-    else return g[p];
-  }
-  __device__ __forceinline__ PT ext() const { return get(kFext, P.ext); }
-  __device__ __forceinline__ PT x(int d) const { return get(kFx + d, P.x[d]); }
-  __device__ __forceinline__ PT u(int d) const { return get(kFu + d, P.u[d]); }
-  __device__ __forceinline__ PT v(int d) const { return get(kFv + d, P.v[d]); }
-  __device__ __forceinline__ PT s(int k) const { return get(kFs + k, P.s[k]); }
-  __device__ __forceinline__ PT vol() const { return get(kFvol, P.vol); }
-  __device__ __forceinline__ PT m() const { return get(kFm, P.m); }
-};
 
 // Stress update of one point for material MAT (-1: the body's kind at run
 // time). s6 holds the stress before the step on entry, after it on exit.
@@ -109,21 +81,20 @@ __device__ __forceinline__ void lean_stress(const BodyCtx<PT>& c, int64_t p, con
 // One point through both phases. `a` is its active state (1 active, 2 left
 // the domain at the last move). The arithmetic follows gather_update and
 // map_scatter of the staged kernel.
-template <int DIM, int T, int TN, bool NORMAL, int MAT, typename PT, int ROW, bool STAGE>
+template <int DIM, int T, int TN, bool NORMAL, int MAT, typename PT>
 __device__ __forceinline__ void lean_point(const BodyCtx<PT>& c, int* err, unsigned long long* drift, int64_t p,
-                                           const PointSrc<PT, ROW, STAGE>& src, int a, const int* o, const PT* tvel,
-                                           const double* vref, double* tacc, uint8_t* touched, int do_g2p,
-                                           bool do_p2g, int stepping) {
+                                           int a, const int* o, const PT* tvel, const double* vref, double* tacc,
+                                           uint8_t* touched, int do_g2p, bool do_p2g, int stepping) {
   using R = PT;
   const PointsT<PT>& P = c.P;
   const R dt = (R)c.sp.dt;
-  const R ext = src.ext();
+  const R ext = P.ext[p];
   const R sG = map_grad_scale(c.g, ext);   // the same for both of the point's maps
   R x[3] = {R(0), R(0), R(0)}, u[3] = {R(0), R(0), R(0)};
 #pragma unroll
   for (int d = 0; d < DIM; d++) {
-    x[d] = src.x(d);
-    if (sizeof(PT) == 4 || do_g2p) u[d] = src.u(d);
+    x[d] = P.x[d][p];
+    if (sizeof(PT) == 4 || do_g2p) u[d] = P.u[d][p];
   }
   R v[3] = {R(0), R(0), R(0)}, s6[6], vol;
   if (do_g2p) {
@@ -157,7 +128,7 @@ __device__ __forceinline__ void lean_point(const BodyCtx<PT>& c, int* err, unsig
 #pragma unroll
     for (int d = 0; d < DIM; d++) {
       const R dx = dt * gs.du[d];
-      v[d] = src.v(d) + gs.dv[d];
+      v[d] = P.v[d][p] + gs.dv[d];
       u[d] = u[d] + dx;
       if constexpr (sizeof(PT) == 8) {
         x[d] = x[d] + dx;
@@ -166,12 +137,12 @@ __device__ __forceinline__ void lean_point(const BodyCtx<PT>& c, int* err, unsig
       P.v[d][p] = v[d];
       P.u[d][p] = u[d];
     }
-    vol = src.vol() * exp(dt * (gs.L[0][0] + gs.L[1][1] + gs.L[2][2]));
+    vol = P.vol[p] * exp(dt * (gs.L[0][0] + gs.L[1][1] + gs.L[2][2]));
     P.vol[p] = vol;
 #pragma unroll
-    for (int k = 0; k < 6; k++) s6[k] = src.s(k);
+    for (int k = 0; k < 6; k++) s6[k] = P.s[k][p];
     if (c.mat.has_material) {
-      lean_stress<DIM, MAT, R>(c, p, gs.L, s6, MAT == 2 || MAT < 0 ? src.m() : R(0), vol, dt);
+      lean_stress<DIM, MAT, R>(c, p, gs.L, s6, MAT == 2 || MAT < 0 ? P.m[p] : R(0), vol, dt);
 #pragma unroll
       for (int k = 0; k < 6; k++) P.s[k][p] = s6[k];
     }
@@ -183,10 +154,10 @@ __device__ __forceinline__ void lean_point(const BodyCtx<PT>& c, int* err, unsig
     }
   } else {
 #pragma unroll
-    for (int d = 0; d < DIM; d++) v[d] = src.v(d);
+    for (int d = 0; d < DIM; d++) v[d] = P.v[d][p];
 #pragma unroll
-    for (int k = 0; k < 6; k++) s6[k] = src.s(k);
-    vol = src.vol();
+    for (int k = 0; k < 6; k++) s6[k] = P.s[k][p];
+    vol = P.vol[p];
   }
   if (!do_p2g || a != 1) return;
   // map build and scatter at the new position (mapPointsToNodes,
@@ -204,7 +175,7 @@ __device__ __forceinline__ void lean_point(const BodyCtx<PT>& c, int* err, unsig
   }
   if (st == 0) return;
   ScatterSrc<R> q;
-  q.m = src.m();
+  q.m = P.m[p];
 #pragma unroll
   for (int d = 0; d < 3; d++) q.mv[d] = d < DIM ? q.m * v[d] : R(0);
   R vs[6];
@@ -225,36 +196,29 @@ __device__ __forceinline__ void lean_point(const BodyCtx<PT>& c, int* err, unsig
     scatter_general<DIM, T, TN, NORMAL, false>(c, drift, pm, o, q, tacc, touched, nullptr);
 }
 
-template <int DIM, typename PT, int NT, bool NORMAL, bool SINGLE, int MAT, bool STAGE>
+template <int DIM, typename PT, int NT, int PPT, bool NORMAL, bool SINGLE, int MAT>
 __global__ void __launch_bounds__(NT, lean_min_ctas<PT, NT>())
     k_g2p2g_lean(const __grid_constant__ FusedLaunch<PT> fl) {
   constexpr int B = fused_bin<DIM>();
   constexpr int T = B + 3;
   constexpr int TN = fused_tile_nodes<DIM, B>();
   constexpr int NACC = fused_nacc(NORMAL);
-  constexpr int ROW = cap_row<NT>();
-  constexpr int AL = 16 / (int)sizeof(PT);   // elements per 16 bytes
   constexpr uint32_t kCtxBytes = (uint32_t)ctx_bytes<PT>();
   extern __shared__ __align__(128) unsigned char smem[];
-  uint64_t* bar = reinterpret_cast<uint64_t*>(smem);            // staged point arrays
   uint64_t* bar_ctx = reinterpret_cast<uint64_t*>(smem + 8);   // table entry slots 0, 1
   auto slot_ctx = [&](int i) { return reinterpret_cast<BodyCtx<PT>*>(smem + kOffCtx + (size_t)i * kCtxBytes); };
-  PT* pts = reinterpret_cast<PT*>(smem + lean_off_pts<PT, NT, STAGE>());
-  int32_t* act = reinterpret_cast<int32_t*>(smem + lean_off_act<PT, NT, STAGE>());
-  PT* tvel = reinterpret_cast<PT*>(smem + lean_off_tvel<DIM, PT, NT, STAGE>());
-  double* tacc = reinterpret_cast<double*>(smem + lean_off_tacc<DIM, PT, NT, STAGE>());
-  uint8_t* touched = smem + lean_off_touched<DIM, PT, NT, NORMAL, STAGE>();
+  PT* tvel = reinterpret_cast<PT*>(smem + lean_off_tvel<DIM, PT>());
+  double* tacc = reinterpret_cast<double*>(smem + lean_off_tacc<DIM, PT>());
+  uint8_t* touched = smem + lean_off_touched<DIM, PT, NORMAL>();
 
-  if (!SINGLE || STAGE) {
+  if (!SINGLE) {
     if (threadIdx.x == 0) {
-      mbar_init(bar, 1);
       mbar_init(bar_ctx, 1);
       mbar_init(bar_ctx + 1, 1);
       mbar_init_fence();
     }
     __syncthreads();
   }
-  uint32_t parity = 0;
   const int nwork = SINGLE ? fl.nwork_body[fl.one_body] : *fl.nwork;
   // launches over every body: the table entry of each work item arrives by
   // a bulk copy issued one item ahead (slot k & 1 for the CTA's k-th item)
@@ -308,27 +272,14 @@ __global__ void __launch_bounds__(NT, lean_min_ctas<PT, NT>())
     const int bin = fl.work_bin[item];
     const int64_t pstart = fl.work_start[item];
     const int n = fl.work_end[item] - (int)pstart;
-    if (n > NT && threadIdx.x == 0) atomicOr(fl.err, kErrItemCap);   // the work list was cut for another size
-    const int j = threadIdx.x;
-    const int64_t p = pstart + j;
-    // with STAGE, the item's point arrays arrive by bulk copies (one thread
-    // issues them, completed on an mbarrier) while the tile is staged; their
-    // windows start on 16-byte boundaries and are rounded up to 16 bytes
-    const int64_t sp0 = pstart & ~(int64_t)(AL - 1), s4 = pstart & ~(int64_t)3;
-    const int offp = (int)(pstart - sp0), off4 = (int)(pstart - s4);
-    if constexpr (STAGE) {
-      if (threadIdx.x == 0) {
-        const int np = (offp + n + AL - 1) & ~(AL - 1), n4 = (off4 + n + 3) & ~3;
-        const PT* src[kNF] = {P.x[0], P.x[1], P.x[2], P.v[0], P.v[1], P.v[2], P.u[0], P.u[1], P.u[2],
-                              P.s[0], P.s[1], P.s[2], P.s[3], P.s[4], P.s[5], P.vol, P.m, P.ext};
-        fence_async_shared();
-        mbar_arrive_expect_tx(bar, (uint32_t)(kNF * np * sizeof(PT) + n4 * 4));
-#pragma unroll 1
-        for (int f = 0; f < kNF; f++) bulk_copy_g2s(pts + f * ROW, src[f] + sp0, (uint32_t)(np * sizeof(PT)), bar);
-        bulk_copy_g2s(act, P.active + s4, (uint32_t)(n4 * 4), bar);
-      }
+    if (n > PPT * NT && threadIdx.x == 0) atomicOr(fl.err, kErrItemCap);   // the work list was cut for another size
+    // activity of the thread's points (coalesced loads issued before the tile work)
+    int a[PPT];
+#pragma unroll
+    for (int r = 0; r < PPT; r++) {
+      const int j = (int)threadIdx.x + r * NT;
+      a[r] = j < n ? P.active[pstart + j] : 0;
     }
-    const int a_direct = (!STAGE && j < n) ? P.active[p] : 0;
     int o[3] = {0, 0, 0};
     {
       const int bx = bin % c.bg.nbx;
@@ -386,22 +337,12 @@ __global__ void __launch_bounds__(NT, lean_min_ctas<PT, NT>())
       for (int t = threadIdx.x; t < NACC * TN; t += NT) tacc[t] = 0.0;
       for (int t = threadIdx.x; t < TN; t += NT) touched[t] = 0;
     }
-    if constexpr (STAGE) {
-      const bool arrived = mbar_wait_bounded(bar, parity, fl.err, fl.wait_polls);
-      // one decision for the whole CTA (also the barrier after the tile loads)
-      if (__syncthreads_or(arrived ? 0 : 1)) {
-        if (!arrived) mbar_wait_bounded(bar, parity, fl.err);  // let copies in flight land before leaving
-        return;
-      }
-      parity ^= 1u;
-    } else {
-      __syncthreads();
-    }
-    const int a = STAGE ? (j < n ? act[off4 + j] : 0) : a_direct;
-    if (a != 0) {
-      const PointSrc<PT, ROW, STAGE> src{P, p, pts + offp + j};
-      lean_point<DIM, T, TN, NORMAL, MAT>(c, fl.err, fl.drift, p, src, a, o, tvel, vref, tacc, touched, do_g2p,
-                                          do_p2g, prime ? 0 : 1);
+    __syncthreads();
+#pragma unroll 1
+    for (int r = 0; r < PPT; r++) {
+      if (a[r] != 0)
+        lean_point<DIM, T, TN, NORMAL, MAT>(c, fl.err, fl.drift, pstart + threadIdx.x + r * NT, a[r], o, tvel, vref,
+                                            tacc, touched, do_g2p, do_p2g, prime ? 0 : 1);
     }
     if (do_p2g) {
       __syncthreads();

@@ -20,7 +20,7 @@ LIB_PATH = os.environ.get("MPM_B200_LIB", os.path.join(HERE, "lib", "libmpm_b200
 
 MODES = {"fp64": 0, "fp64_deterministic": 1, "mixed": 2}
 # forms of the fused kernel (mpmgpu_kernel_form)
-KERNELS = {"staged": 0, "point_per_thread": 1, "point_per_thread_staged": 2}
+KERNELS = {"staged": 0, "point_per_thread": 1}
 KERNEL_NAMES = {v: k for k, v in KERNELS.items()}
 POINT_FIELDS = {"x": (0, 3), "u": (1, 3), "x_t": (2, 3), "mx_t": (3, 3), "b": (4, 3), "L": (5, 9), "T": (6, 9),
                 "m": (7, 1), "v": (8, 1), "extent": (9, 1), "active": (10, 1), "gammap": (11, 1),

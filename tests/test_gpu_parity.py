@@ -165,7 +165,7 @@ def test_step_parity(name):
 
 
 CASES_3D = sorted(n for n in CASES if "3d" in n)
-KERNEL_FORMS = [("staged", 512), ("staged", 256), ("point_per_thread", 128), ("point_per_thread_staged", 256)]
+KERNEL_FORMS = [("staged", 512), ("staged", 256), ("point_per_thread", 128), ("point_per_thread", 512)]
 
 
 @pytest.mark.parametrize("kernel", KERNEL_FORMS, ids=lambda k: f"{k[0]}{k[1]}")

@@ -10,7 +10,11 @@ names, the same lines of text outside the arrays (titles, headers, array
 names, connectivity), and in every array the same numbers up to the
 printing of 6 significant digits on top of the FP64 parity tolerance (a
 value the two runs differ in by a rounding can print with its last digit
-one apart).
+one apart). As in the parity tests, the tolerance of a field that can be
+pure round-off (the velocity gradient and stress of a body in free fall) is
+taken relative to its physical scale (util.field_floor), and the contact
+normal, which at nodes of one body normalises round-off, is compared in
+its layout only (the parity tests compare it where both bodies have mass).
 """
 import os
 import re
@@ -21,6 +25,7 @@ import pytest
 
 import bridge
 from mpm_3d_b200 import inputs
+from util import field_floor
 
 pytestmark = pytest.mark.gpu
 
@@ -60,7 +65,12 @@ def _sections(lines):
     return secs
 
 
-def _compare(fname, ref, got, tol=1e-10, digits=1e-5):
+# physical scale of the arrays a frame holds, by name (util.field_floor)
+FLOOR_FIELD = {"velocity_gradient": "L", "cauchy_stress": "T", "pressure": "T", "velocity": "x_t",
+               "diff_velocity": "x_t", "displacement": "u", "gammap": "gammap", "gammap_dot": "gammap_dot"}
+
+
+def _compare(fname, ref, got, case, tol=1e-10, digits=1e-5):
     rs, gs = _sections(ref), _sections(got)
     assert [h for h, _ in rs] == [h for h, _ in gs], f"{fname}: section headers differ"
     for (h, rd), (_, gd) in zip(rs, gs):
@@ -74,7 +84,13 @@ def _compare(fname, ref, got, tol=1e-10, digits=1e-5):
             assert rd == gd, f"{fname} {h}: text differs"
             continue
         assert a.shape == b.shape, f"{fname} {h}: token counts differ"
+        parts = h.split()
+        name = parts[1] if len(parts) > 1 and parts[0] in ("SCALARS", "VECTORS", "TENSORS") else ""
+        if name.startswith("contact_normal"):
+            continue
         scale = float(np.abs(a).max()) if a.size else 0.0
+        if name in FLOOR_FIELD:
+            scale = max(scale, field_floor(case, FLOOR_FIELD[name]))
         bound = tol * scale + digits * np.maximum(np.abs(a), np.abs(b))
         bad = np.abs(a - b) > bound
         assert not bad.any(), (f"{fname} {h}: {int(bad.sum())} values differ, e.g. {a[bad][:3]} vs {b[bad][:3]}")
@@ -97,4 +113,4 @@ def test_gpu_solver_with_async_vtk_writes_the_reference_frames(name):
     assert len(ref) == 2 * len(case.bodies) * -(-steps // every)
     assert sorted(got) == sorted(ref)
     for fname in ref:
-        _compare(fname, ref[fname], got[fname])
+        _compare(fname, ref[fname], got[fname], case)
