@@ -98,13 +98,20 @@ def make_workload(name: str, rank: int = 0):
     raise SystemExit(f"unknown workload {name}")
 
 
+# The mixed form keeps the initial position in the x arrays and derives
+# x = x0 + u, so it does not write x: 12 bytes per point-step of the
+# algorithmic figure that it never moves, left out of its count.
+MIXED_X_WRITE_SKIPPED = 12.0
+
+
 def bytes_per_point_step(active_nodes_per_point: float, mixed: bool = False) -> float:
     """Algorithmic bytes per particle-step. FP64 form: point state read
     (x, v, m, V, sigma(6), u, extent, active = 148 B) and written (x, v, V,
     sigma, u = 128 B); mixed form: the same fields in FP32 (76 B read, 64 B
-    written). Plus the grid term 112 B per active node per body (m,
-    momentum, force accumulated and read once, FP64 in both forms)."""
-    return (140.0 if mixed else 276.0) + 112.0 * active_nodes_per_point
+    written), less the x write it does not do (12 B). Plus the grid term
+    112 B per active node per body (m, momentum, force accumulated and read
+    once, FP64 in both forms)."""
+    return (140.0 - MIXED_X_WRITE_SKIPPED if mixed else 276.0) + 112.0 * active_nodes_per_point
 
 
 def field_floor(case, field: str) -> float:
@@ -224,14 +231,18 @@ def sum_over_ranks(value: float, world: int) -> float:
 
 
 def cpu_reference_run(case, steps: int, warmup: int, threads: int):
-    """Times the reference's ThreadPoolExplicitUSL (own sources, timing
-    build) on `threads` host threads: returns seconds per step."""
+    """Times the reference's solver (own sources, timing build) on `threads`
+    host threads: ThreadPoolExplicitUSL with ThreadPoolPoints, or the serial
+    ExplicitUSL for threads == 1. Returns seconds per step."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import bridge
 
     d = tempfile.mkdtemp()
-    cfg = inputs.write_case(case, d, solver_class="ThreadPoolExplicitUSL", points_class="ThreadPoolPoints",
-                            threads=threads)
+    if threads == 1:
+        cfg = inputs.write_case(case, d)
+    else:
+        cfg = inputs.write_case(case, d, solver_class="ThreadPoolExplicitUSL", points_class="ThreadPoolPoints",
+                                threads=threads)
     with quiet_stdout():  # the reference reports its set-up on stdout
         job = bridge.ReferenceJob(cfg, build="timing")
         job.step(warmup)
@@ -446,6 +457,7 @@ def run_batch(cases, mode: str, args, device: int, sample_ids):
     b = GPUBatch(dim=3, mode=mode, device=device)
     jobs = [b.add(c) for c in cases]
     cap = b.autotune(steps=8)
+    kernel = b.kernel_form()
     si = b.sort_interval()
     b.step(args.warmup)
     step_ms, launches, clk = timed_steps(b, args.steps)
@@ -455,7 +467,7 @@ def run_batch(cases, mode: str, args, device: int, sample_ids):
     steps_done = b.state(jobs[0])[0]
     b.close()
     return {"step_ms": step_ms, "launches": launches, "clocks": clk, "prof": prof, "prof_steps": prof_steps,
-            "active": active, "drift": drift, "cap": cap, "sort_interval": si,
+            "active": active, "drift": drift, "cap": cap, "kernel": kernel, "sort_interval": si,
             "steps_done": steps_done}
 
 
@@ -553,12 +565,14 @@ def run_ensemble(args, rank, world, local):
     serving = run_serving(args.serve_seconds, local, mixed["sort_interval"]) if args.serve_seconds > 0 else None
     # end to end: every job runs its own step count (the workload's 500
     # steps), as a user runs the ensemble
-    e2e = (run_e2e_batch(cases, max(c.steps for c in cases), local, mixed["cap"], mixed["sort_interval"])
+    e2e = (run_e2e_batch(cases, max(c.steps for c in cases), local, (mixed["kernel"], mixed["cap"]),
+                         mixed["sort_interval"])
            if rank == 0 and not args.no_e2e else None)
     cpu = None
     if rank == 0 and not args.no_cpu:
         try:
             cpu = cpu_ensemble_sample(cases, args.ref_steps)
+            cpu["thread_variants"] = cpu_thread_variants(cases)
         except Exception as exc:  # the oracle build may be absent
             cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": f"unavailable: {exc}"}
     if rank != 0:
@@ -570,10 +584,11 @@ def run_ensemble(args, rank, world, local):
         "config": {"workload": f"ensemble{ENSEMBLE_JOBS}" + (f"[:{args.jobs}]" if args.jobs > 0 else ""),
                    "jobs": len(cases), "points": n,
                    "grids": "N^3, N log-uniform in [16,96]", "form": "mixed (FP32 points, FP64 nodal sums)",
-                   "points_per_item": mixed["cap"], "sort_interval": mixed["sort_interval"], "graph": True,
+                   "kernel": mixed["kernel"], "points_per_item": mixed["cap"],
+                   "sort_interval": mixed["sort_interval"], "graph": True,
                    "parallelism": f"independent{world}",
                    "l2": "inputs larger than L2", "active_nodes_per_point": round(active_ratio, 4)},
-        "batched_fp64": ({"value": fp64_value, "unit": UNIT, "points_per_item": fp64["cap"],
+        "batched_fp64": ({"value": fp64_value, "unit": UNIT, "kernel": fp64["kernel"], "points_per_item": fp64["cap"],
                           "sort_interval": fp64["sort_interval"]} if fp64 else None),
         "plain_fp64": {"value": plain_value, "unit": UNIT, "steps_per_job": args.plain_steps,
                        "how": "one mpmgpu_handle per job, jobs in sequence, CUDA events around each job's steps"},
@@ -628,7 +643,7 @@ def run_serving_workload(args, rank, world, local):
     print(json.dumps(line), flush=True)
 
 
-def run_e2e_batch(cases, steps: int, device: int, cap: int, sort_interval: int):
+def run_e2e_batch(cases, steps: int, device: int, kernel, sort_interval: int):
     """The ensemble through the C ABI from host buffers: batch creation and
     upload of every job, `steps` steps (each job stops at its own count),
     download of every point's x, x_t and stress, teardown, all on the wall
@@ -640,7 +655,7 @@ def run_e2e_batch(cases, steps: int, device: int, cap: int, sort_interval: int):
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     phases = {}
-    b = GPUBatch(dim=3, mode="mixed", device=device, points_per_item=cap, sort_interval=sort_interval)
+    b = GPUBatch(dim=3, mode="mixed", device=device, sort_interval=sort_interval, kernel=kernel)
     jobs = [b.add(c) for c in cases]
     t1 = time.perf_counter()
     phases["create_upload_s"] = t1 - t0
@@ -660,6 +675,23 @@ def run_e2e_batch(cases, steps: int, device: int, cap: int, sort_interval: int):
     h2d = sum(b_.n * (8 + 8 + 24 + 24 + 4) for c in cases for b_ in c.bodies)
     return {"value": psteps / dt, "unit": UNIT, "h2d_bytes_per_step": h2d // steps, "d2h_bytes_per_step": d2h // steps,
             "steps": steps, "seconds": dt, "phases": {k: round(v, 3) for k, v in phases.items()}}
+
+
+def cpu_thread_variants(cases, steps: int = 2):
+    """The reference's solver on 4 of the ensemble's jobs (every 128th) with
+    one thread (the serial ExplicitUSL) and with all host threads but one
+    (ThreadPoolExplicitUSL's main thread busy-waits on its workers,
+    threadpool_explicit_usl.cpp:327-343)."""
+    cores = os.cpu_count() or 1
+    ids = list(range(0, len(cases), max(1, len(cases) // 4)))[:4]
+    out = {}
+    for t in sorted({1, max(1, cores - 1)}):
+        sec = sum(cpu_reference_run(cases[i], steps, 1, t) * steps for i in ids)
+        pts = sum(cases[i].n_points * steps for i in ids)
+        out[f"threads_{t}"] = pts / sec
+    out.update({"unit": UNIT, "jobs": ids, "steps": steps,
+                "solver": "ExplicitUSL (1 thread), ThreadPoolExplicitUSL+ThreadPoolPoints (more)"})
+    return out
 
 
 def cpu_ensemble_sample(cases, steps: int, warmup: int = 1):
