@@ -370,7 +370,8 @@ def roofline(points: int, steps: int, prof, active_ratio: float, mixed: bool, tr
             "bytes_per_point_step": bpp, "launch_ms": per_launch_ms, "points_per_launch": points_per_launch}
 
 
-def single_timed(case, form: str, steps: int, warmup: int, device: int, world: int = 1, traffic_key=None):
+def single_timed(case, form: str, steps: int, warmup: int, device: int, world: int = 1, traffic_key=None,
+                 kernel=None):
     """One single-job handle: `warmup` steps, then `steps` steps timed with
     CUDA events (L2 flushed between steps when the point state would fit
     in it), a profiled pass for the fused kernel's launch time, and the
@@ -382,7 +383,7 @@ def single_timed(case, form: str, steps: int, warmup: int, device: int, world: i
     n = case.n_points
     flush_l2 = 148 * n < 2 * L2_BYTES
     flush_buf = torch.empty(4 * L2_BYTES // 4, dtype=torch.float32, device="cuda") if flush_l2 else None
-    sim = GPUExplicitUSL(case, device=device, mode=form)
+    sim = GPUExplicitUSL(case, device=device, mode=form, kernel=kernel)
     sim.step(warmup)
     barrier(world)
     step_ms, launches, clk = timed_steps(sim, steps, flush_buf)
@@ -392,10 +393,11 @@ def single_timed(case, form: str, steps: int, warmup: int, device: int, world: i
     active, _drift = sim.active_nodes()
     active_ratio = active / max(1, n)
     roof = roofline(n, prof_steps, prof, active_ratio, form == "mixed", traffic_key)
+    used = sim.kernel()
     sim.close()
     del flush_buf
     return {"step_ms": step_ms, "launches": launches, "clocks": clk, "prof": prof, "prof_steps": prof_steps,
-            "active_ratio": active_ratio, "roofline": roof, "l2_flushed": flush_l2}
+            "active_ratio": active_ratio, "roofline": roof, "l2_flushed": flush_l2, "kernel": used}
 
 
 def run_single(args, rank, world, local):
@@ -404,7 +406,7 @@ def run_single(args, rank, world, local):
     torch.cuda.set_device(local)
     case = make_workload(args.workload)
     n = case.n_points
-    r = single_timed(case, args.form, args.steps, args.warmup, local, world, (args.workload, args.form))
+    r = single_timed(case, args.form, args.steps, args.warmup, local, world, (args.workload, args.form), args.kernel)
     step_ms, launches, clk, prof, prof_steps = r["step_ms"], r["launches"], r["clocks"], r["prof"], r["prof_steps"]
     flush_l2, active_ratio, roof = r["l2_flushed"], r["active_ratio"], r["roofline"]
     total_ms = sum(step_ms)
@@ -431,7 +433,8 @@ def run_single(args, rank, world, local):
         "ms_per_step": total_ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32+f64" if args.form == "mixed" else "f64", "data": "synthetic (seeded mpm_3d_b200.inputs)",
         "config": {"workload": args.workload, "points": n, "bodies": len(case.bodies), "grid": list(case.N),
-                   "dt": case.dt, "form": args.form, "parallelism": f"replicas{world}",
+                   "dt": case.dt, "form": args.form, "kernel": r["kernel"][0], "points_per_item": r["kernel"][1],
+                   "parallelism": f"replicas{world}",
                    "l2": "flushed between steps" if flush_l2 else "inputs larger than L2",
                    "active_nodes_per_point": round(active_ratio, 4)},
         "roofline": roof,
@@ -454,9 +457,14 @@ def run_batch(cases, mode: str, args, device: int, sample_ids):
     sampled jobs."""
     from mpm_3d_b200.native import GPUBatch
 
-    b = GPUBatch(dim=3, mode=mode, device=device)
-    jobs = [b.add(c) for c in cases]
-    cap = b.autotune(steps=8)
+    if args.kernel is None:
+        b = GPUBatch(dim=3, mode=mode, device=device)
+        jobs = [b.add(c) for c in cases]
+        cap = b.autotune(steps=8)
+    else:
+        b = GPUBatch(dim=3, mode=mode, device=device, sort_interval=args.sort_interval, kernel=args.kernel)
+        jobs = [b.add(c) for c in cases]
+        cap = b.points_per_item()
     kernel = b.kernel_form()
     si = b.sort_interval()
     b.step(args.warmup)
@@ -562,7 +570,8 @@ def run_ensemble(args, rank, world, local):
     roof = roofline(n, mixed["prof_steps"], mixed["prof"], active_ratio, True, ("ensemble", "mixed"))
     plain_value, plain_ms = plain_fp64(cases, args.plain_steps, local) if not args.no_plain else (None, None)
     column = column_fp64_record(local) if not args.no_column else None
-    serving = run_serving(args.serve_seconds, local, mixed["sort_interval"]) if args.serve_seconds > 0 else None
+    serving = (run_serving(args.serve_seconds, local, mixed["sort_interval"], policy=args.policy)
+               if args.serve_seconds > 0 else None)
     # end to end: every job runs its own step count (the workload's 500
     # steps), as a user runs the ensemble
     e2e = (run_e2e_batch(cases, max(c.steps for c in cases), local, (mixed["kernel"], mixed["cap"]),
@@ -606,15 +615,16 @@ def run_ensemble(args, rank, world, local):
     print(json.dumps(line), flush=True)
 
 
-def run_serving(seconds: float, device: int, sort_interval: int = 8, round_steps: int = 20):
+def run_serving(seconds: float, device: int, sort_interval: int = 8, round_steps: int = 20, policy: str = "fifo"):
     """The serving stream for `seconds` of arrivals (seed 1004) until every
-    request has completed; p50/p99 time to completion and throughput."""
+    request has completed, admitted by `policy`; p50/p99 time to completion
+    and throughput."""
     from mpm_3d_b200.native import GPUServer
     from mpm_3d_b200.serving import run_stream
 
     specs = inputs.serving_stream(rate=100.0, duration=seconds, seed=1004)
     srv = GPUServer(budget_bytes=150 * 10**9, mode="mixed", device=device, sort_interval=sort_interval)
-    rep = run_stream(srv, specs, round_steps=round_steps)
+    rep = run_stream(srv, specs, round_steps=round_steps, policy=policy)
     srv.close()
     out = rep.summary()
     out.update({"arrivals_s": seconds, "rate_per_s": 100.0, "budget_bytes": 150 * 10**9, "round_steps": round_steps,
@@ -626,7 +636,7 @@ def run_serving_workload(args, rank, world, local):
     import torch
 
     torch.cuda.set_device(local)
-    rep = run_serving(args.serve_seconds, local)
+    rep = run_serving(args.serve_seconds, local, policy=args.policy)
     rep_max = max_over_ranks(rep["makespan_s"], world)
     steps_all = sum_over_ranks(float(rep["particle_steps"]), world)
     if rank != 0:
@@ -636,7 +646,8 @@ def run_serving_workload(args, rank, world, local):
         "warmup": 0, "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32+f64", "data": "synthetic (mpm_3d_b200.inputs.serving_stream, seed 1004)",
         "config": {"workload": "serving", "arrivals_s": args.serve_seconds, "rate_per_s": 100.0,
-                   "budget_bytes": 150 * 10**9, "form": "mixed", "parallelism": f"independent{world}"},
+                   "budget_bytes": 150 * 10**9, "form": "mixed", "policy": args.policy,
+                   "parallelism": f"independent{world}"},
         "serving": rep,
         "gpu_launches": None,
     }
@@ -736,6 +747,18 @@ def run_e2e(case, steps: int, device: int, form: str = "fp64"):
             "d2h_bytes_per_step": d2h // steps, "steps": steps, "seconds": dt}
 
 
+def parse_kernel(spec: str):
+    """'FORM/POINTS' -> (form, points per work item); '' -> None."""
+    if not spec:
+        return None
+    form, _, cap = spec.partition("/")
+    from mpm_3d_b200.native import KERNELS
+
+    if form not in KERNELS or not cap.isdigit():
+        raise SystemExit(f"--kernel wants FORM/POINTS with FORM one of {sorted(KERNELS)}")
+    return form, int(cap)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -755,7 +778,13 @@ def main():
     ap.add_argument("--ref-steps", type=int, default=4, help="steps of the CPU reference sample")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--kernel", default="", metavar="FORM/POINTS",
+                    help="fix the fused kernel's form and points per work item (e.g. point_per_thread/256) "
+                         "instead of the default (single jobs) or the autotuner's choice (batches)")
+    ap.add_argument("--sort-interval", type=int, default=8, help="re-binning interval of a batch with --kernel")
+    ap.add_argument("--policy", default="fifo", choices=["fifo", "fit"], help="admission policy of the serving stream")
     args = ap.parse_args()
+    args.kernel = parse_kernel(args.kernel)
     if args.warmup < 3:
         args.warmup = 3
     if args.steps <= 0:

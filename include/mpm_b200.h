@@ -287,11 +287,18 @@ typedef enum {
 } mpmgpu_kernel_form;
 
 /* Selects the fused kernel's form and points per work item (default: one
- * point per thread with 256 points in 3D outside the deterministic form,
+ * point per thread with 512 points in 3D outside the deterministic form,
  * else staged with 512); MPMGPU_ERR_ARG if the pair is not available for
  * the handle. Takes effect at the next step. */
 mpmgpu_status mpmgpu_set_kernel(mpmgpu_handle* h, int form, int points_per_item);
 mpmgpu_status mpmgpu_kernel(const mpmgpu_handle* h, int* form, int* points_per_item);
+/* No counterpart in the reference. Tunes the handle's launch shape on its
+ * own bodies as mpmgpu_batch_autotune does (every available kernel form and
+ * points-per-item choice for `steps` steps, then the re-binning interval),
+ * keeps the fastest and reports it in *form and *points_per_item (either
+ * may be null). The simulation's state after the call is the state before
+ * it. */
+mpmgpu_status mpmgpu_autotune(mpmgpu_handle* h, int steps, int* form, int* points_per_item);
 
 /* Per-stage device time accounting with CUDA events recorded on the
  * handle's stream around every launch of a stage. enable != 0 starts (and
@@ -326,7 +333,7 @@ typedef struct {
   int device;          /* CUDA device ordinal */
   int sort_interval;   /* steps between re-binnings (0 = default 32) */
   int points_per_item; /* points per CTA work item: 0 = default (3D,
-                          not deterministic: 256 on the point-per-thread
+                          not deterministic: 512 on the point-per-thread
                           kernel; else 512 on the staged kernel); 128, 256
                           or 512 run on the point-per-thread kernel where
                           it applies, other sizes on the staged kernel

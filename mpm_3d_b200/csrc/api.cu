@@ -205,6 +205,18 @@ mpmgpu_status mpmgpu_kernel(const mpmgpu_handle* h, int* form, int* points_per_i
   return MPMGPU_OK;
 }
 
+mpmgpu_status mpmgpu_autotune(mpmgpu_handle* h, int steps, int* form, int* points_per_item) {
+  if (!h || steps < 1) return MPMGPU_ERR_ARG;
+  int64_t n = 0;
+  TRY(h->b->sizes(h->job, 0, &n, nullptr) == MPMGPU_OK ? MPMGPU_OK : hfail(h, MPMGPU_ERR_STATE, "no bodies"));
+  TRY(start(h));
+  int cap = 0;
+  TRY(h->b->autotune(steps, &cap));
+  if (form) *form = h->b->kernel_form();
+  if (points_per_item) *points_per_item = cap;
+  return MPMGPU_OK;
+}
+
 mpmgpu_status mpmgpu_set_wait_limit(mpmgpu_handle* h, uint32_t polls) {
   if (!h) return MPMGPU_ERR_ARG;
   h->b->set_wait_limit(polls);

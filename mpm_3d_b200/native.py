@@ -104,6 +104,7 @@ def load() -> ctypes.CDLL:
                                                  ctypes.POINTER(ctypes.c_int)]
     lib.mpmgpu_set_gravity.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
     lib.mpmgpu_step.argtypes = [vp, ctypes.c_int]
+    lib.mpmgpu_autotune.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
     lib.mpmgpu_synchronize.argtypes = [vp]
     for fn in ("mpmgpu_download_points", "mpmgpu_download_nodes", "mpmgpu_download_contact", "mpmgpu_frame_points",
                "mpmgpu_frame_nodes", "mpmgpu_frame_contact"):
@@ -281,6 +282,15 @@ class GPUExplicitUSL:
     def set_kernel(self, form: str, points_per_item: int):
         """Selects the fused kernel's form (KERNELS) and points per work item."""
         self._check(self.lib.mpmgpu_set_kernel(self.h, KERNELS[form], points_per_item))
+
+    def autotune(self, steps: int = 5) -> Tuple[str, int]:
+        """Times every available kernel form and points-per-item choice on
+        this handle's bodies, then the re-binning interval, and keeps the
+        fastest (the state after the call is the state before it)."""
+        f = ctypes.c_int()
+        c = ctypes.c_int()
+        self._check(self.lib.mpmgpu_autotune(self.h, steps, ctypes.byref(f), ctypes.byref(c)))
+        return KERNEL_NAMES[f.value], c.value
 
     def kernel(self) -> Tuple[str, int]:
         f = ctypes.c_int()

@@ -131,11 +131,15 @@ def restated_lib():
     bridge.build_restated()
 
 
-def _step_parity(name, sort_interval=0, mode="fp64", kernel=None):
+def _step_parity(name, sort_interval=0, mode="fp64", kernel=None, autotune=False):
     make, steps = CASES[name]
     case = make()
     ref = bridge.RestatedJob(case)
     gpu = GPUExplicitUSL(case, keep_debug=True, sort_interval=sort_interval, mode=mode, kernel=kernel)
+    if autotune:
+        # the trials run from snapshots: the state after tuning is the state before it
+        form, cap = gpu.autotune(steps=2)
+        assert gpu.kernel() == (form, cap)
     worst = {}
     for s in range(steps):
         ref.step(1)
@@ -165,16 +169,23 @@ def test_step_parity(name):
 
 
 CASES_3D = sorted(n for n in CASES if "3d" in n)
-KERNEL_FORMS = [("staged", 512), ("staged", 256), ("point_per_thread", 128), ("point_per_thread", 512)]
+KERNEL_FORMS = [("staged", 512), ("staged", 256), ("point_per_thread", 128), ("point_per_thread", 256)]
 
 
 @pytest.mark.parametrize("kernel", KERNEL_FORMS, ids=lambda k: f"{k[0]}{k[1]}")
 @pytest.mark.parametrize("name", CASES_3D)
 def test_step_parity_kernel_forms(name, kernel):
-    """3D jobs run on the one-point-per-thread kernel with 256 points per
+    """3D jobs run on the one-point-per-thread kernel with 512 points per
     item by default (test_step_parity); every other kernel form and size
     must meet the same parity."""
     _step_parity(name, kernel=kernel)
+
+
+@pytest.mark.parametrize("name", ["collision_3d_touching", "spinning_block_2d"])
+def test_step_parity_after_autotune(name):
+    """mpmgpu_autotune on a single handle: whatever it keeps, the steps after
+    it meet the parity from the unchanged initial state."""
+    _step_parity(name, autotune=True)
 
 
 @pytest.mark.parametrize("name", ["collision_3d_touching", "wall_exit_2d", "spinning_block_2d", "dense_cells_3d"])
