@@ -83,7 +83,7 @@ ENSEMBLE_SEED = 1003
 # captures of the kernel (the ensemble's from a capture of its first 96 jobs,
 # scaled to a launch by its points; the column's at full size). None where no
 # capture exists.
-TRAFFIC_BYTES_PER_POINT = {("ensemble", "mixed"): 159.9, ("column", "fp64"): 305.3}
+TRAFFIC_BYTES_PER_POINT = {("ensemble", "mixed"): 179.8, ("column", "fp64"): 388.4}
 
 
 def make_workload(name: str, rank: int = 0):
@@ -98,20 +98,15 @@ def make_workload(name: str, rank: int = 0):
     raise SystemExit(f"unknown workload {name}")
 
 
-# The mixed form keeps the initial position in the x arrays and derives
-# x = x0 + u, so it does not write x: 12 bytes per point-step of the
-# algorithmic figure that it never moves, left out of its count.
-MIXED_X_WRITE_SKIPPED = 12.0
-
-
 def bytes_per_point_step(active_nodes_per_point: float, mixed: bool = False) -> float:
     """Algorithmic bytes per particle-step. FP64 form: point state read
     (x, v, m, V, sigma(6), u, extent, active = 148 B) and written (x, v, V,
-    sigma, u = 128 B); mixed form: the same fields in FP32 (76 B read, 64 B
-    written), less the x write it does not do (12 B). Plus the grid term
-    112 B per active node per body (m, momentum, force accumulated and read
-    once, FP64 in both forms)."""
-    return (140.0 - MIXED_X_WRITE_SKIPPED if mixed else 276.0) + 112.0 * active_nodes_per_point
+    sigma, u = 128 B). Mixed form: x, x_t and m as two FP32 words (8 B per
+    value), the other fields in FP32: read x 24, x_t 24, m 8, V 4, sigma 24,
+    u 12, extent 4, active 4 = 104 B; written x, x_t, V, sigma, u = 88 B.
+    Plus the grid term 112 B per active node per body (m, momentum, force
+    accumulated and read once, FP64 in both forms)."""
+    return (192.0 if mixed else 276.0) + 112.0 * active_nodes_per_point
 
 
 def field_floor(case, field: str) -> float:
@@ -479,29 +474,51 @@ def run_batch(cases, mode: str, args, device: int, sample_ids):
             "steps_done": steps_done}
 
 
-def mixed_error_full(cases, sample_ids, device: int):
-    """The mixed form's error against FP64 after every sampled job's full
-    step count: the sampled jobs run as one FP64 batch and one mixed batch
-    to their ends (outside any timed region) and x, x_t and the stress are
-    compared per job."""
-    from mpm_3d_b200.native import GPUBatch
+REL_ERR_BOUND = 1e-4
+
+
+def form_errors_full(cases, sample_ids, device: int):
+    """Errors of the batched forms after every sampled job's full step count
+    (outside any timed region): the sampled jobs run as one FP64 batch and
+    one mixed batch, and each as a single deterministic-FP64 handle, to
+    their ends; x, x_t and the stress are compared per job. `mixed` is the
+    mixed form against the FP64 batch; `fp64` is the FP64 batch against the
+    deterministic form, i.e. how far two FP64 summation orders drift apart
+    on these dynamics (the amplification of round-off)."""
+    from mpm_3d_b200.native import GPUBatch, GPUExplicitUSL
 
     sub = [cases[i] for i in sample_ids]
     steps = max(c.steps for c in sub)
+    keys = ("x", "x_t", "T")
     fields = {}
     for mode in ("fp64", "mixed"):
         b = GPUBatch(dim=3, mode=mode, device=device)
         jobs = [b.add(c) for c in sub]
         b.step(steps)
-        fields[mode] = [{f: b.points(j, 0, f) for f in ("x", "x_t", "T")} for j in jobs]
+        fields[mode] = [{f: b.points(j, 0, f) for f in keys} for j in jobs]
         done = min(b.state(j)[0] for j in jobs)
         b.close()
-    errs = {f: 0.0 for f in ("x", "x_t", "T")}
-    for k, c in enumerate(sub):
-        for f in errs:
-            errs[f] = max(errs[f], rel_err(fields["mixed"][k][f], fields["fp64"][k][f], field_floor(c, f)))
-    return {**errs, "jobs_compared": len(sub), "after_steps": done,
-            "norm": "max|mixed - fp64| / max(max|fp64|, field scale) per job, worst job"}
+    fields["det"] = []
+    for c in sub:
+        sim = GPUExplicitUSL(c, device=device, mode="fp64_deterministic")
+        sim.step(c.steps)
+        fields["det"].append({f: sim.points(0, f) for f in keys})
+        sim.close()
+
+    def summary(got, ref):
+        worst = {f: 0.0 for f in keys}
+        failing = []
+        for k, c in enumerate(sub):
+            e = {f: rel_err(fields[got][k][f], fields[ref][k][f], field_floor(c, f)) for f in keys}
+            for f in keys:
+                worst[f] = max(worst[f], e[f])
+            if max(e.values()) > REL_ERR_BOUND:
+                failing.append(sample_ids[k])
+        return {**worst, "jobs_compared": len(sub), "jobs_within_bound": len(sub) - len(failing),
+                "jobs_over_bound": failing, "bound": REL_ERR_BOUND, "after_steps": done,
+                "norm": "max|a - b| / max(max|b|, field scale) per job and field; worst job"}
+
+    return {"mixed": summary("mixed", "fp64"), "fp64": summary("fp64", "det")}
 
 
 def column_fp64_record(device: int, steps: int = 20, warmup: int = 5):
@@ -547,6 +564,11 @@ def plain_fp64(cases, steps: int, device: int):
 
 
 def run_ensemble(args, rank, world, local):
+    """The ensemble in both batched forms. The line's `value` is the fastest
+    batched form whose results stay within REL_ERR_BOUND of FP64 on every
+    compared job after its full step count (the metric's condition): the
+    mixed form when it holds, else the FP64 batch; the other form is
+    reported beside it with its errors."""
     import torch
 
     torch.cuda.set_device(local)
@@ -559,23 +581,32 @@ def run_ensemble(args, rank, world, local):
     fp64 = run_batch(cases, "fp64", args, local, sample_ids) if not args.only_mixed else None
     mixed = run_batch(cases, "mixed", args, local, sample_ids)
     barrier(world)
-    total_ms = sum(mixed["step_ms"])
+    # the forms' errors after every sampled job's 500 steps
+    errs = form_errors_full(cases, sample_ids, local) if fp64 else None
+    mixed_ok = errs is None or errs["mixed"]["jobs_within_bound"] == errs["mixed"]["jobs_compared"]
+    head_mode = "mixed" if mixed_ok else "fp64"
+    head = mixed if mixed_ok else fp64
+    total_ms = sum(head["step_ms"])
     total_ms_max = max_over_ranks(total_ms, world)
     points_all = sum_over_ranks(float(n), world)
     value = points_all * args.steps / (total_ms_max * 1e-3)
-    fp64_value = n * args.steps / (sum(fp64["step_ms"]) * 1e-3) if fp64 else None
-    # the mixed form's error against FP64 after every sampled job's 500 steps
-    errs = mixed_error_full(cases, sample_ids, local) if fp64 else None
-    active_ratio = mixed["active"] / max(1, n)
-    roof = roofline(n, mixed["prof_steps"], mixed["prof"], active_ratio, True, ("ensemble", "mixed"))
+
+    def form_value(r):
+        return n * args.steps / (sum(r["step_ms"]) * 1e-3)
+
+    def form_roof(r, mode):
+        return roofline(n, r["prof_steps"], r["prof"], r["active"] / max(1, n), mode == "mixed", ("ensemble", mode))
+
+    active_ratio = head["active"] / max(1, n)
+    roof = form_roof(head, head_mode)
     plain_value, plain_ms = plain_fp64(cases, args.plain_steps, local) if not args.no_plain else (None, None)
     column = column_fp64_record(local) if not args.no_column else None
     serving = (run_serving(args.serve_seconds, local, mixed["sort_interval"], policy=args.policy)
                if args.serve_seconds > 0 else None)
     # end to end: every job runs its own step count (the workload's 500
-    # steps), as a user runs the ensemble
-    e2e = (run_e2e_batch(cases, max(c.steps for c in cases), local, (mixed["kernel"], mixed["cap"]),
-                         mixed["sort_interval"])
+    # steps), as a user runs the ensemble, in the headline's form
+    e2e = (run_e2e_batch(cases, max(c.steps for c in cases), local, (head["kernel"], head["cap"]),
+                         head["sort_interval"], head_mode)
            if rank == 0 and not args.no_e2e else None)
     cpu = None
     if rank == 0 and not args.no_cpu:
@@ -586,29 +617,43 @@ def run_ensemble(args, rank, world, local):
             cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": f"unavailable: {exc}"}
     if rank != 0:
         return
+
+    def form_record(r, mode):
+        if r is None:
+            return None
+        return {"value": form_value(r), "unit": UNIT, "ms_per_step": sum(r["step_ms"]) / args.steps,
+                "kernel": r["kernel"], "points_per_item": r["cap"], "sort_interval": r["sort_interval"],
+                "roofline": form_roof(r, mode),
+                "rel_err": errs[mode] if errs else None,
+                "rel_err_against": "the FP64 batch" if mode == "mixed" else "deterministic FP64 (single handles)"}
+
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": total_ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32+f64", "data": f"synthetic (mpm_3d_b200.inputs.block_drop_ensemble, seed {ENSEMBLE_SEED}+rank)",
+        "dtype": "f32+f64" if head_mode == "mixed" else "f64",
+        "data": f"synthetic (mpm_3d_b200.inputs.block_drop_ensemble, seed {ENSEMBLE_SEED}+rank)",
         "config": {"workload": f"ensemble{ENSEMBLE_JOBS}" + (f"[:{args.jobs}]" if args.jobs > 0 else ""),
                    "jobs": len(cases), "points": n,
-                   "grids": "N^3, N log-uniform in [16,96]", "form": "mixed (FP32 points, FP64 nodal sums)",
-                   "kernel": mixed["kernel"], "points_per_item": mixed["cap"],
-                   "sort_interval": mixed["sort_interval"], "graph": True,
+                   "grids": "N^3, N log-uniform in [16,96]",
+                   "form": ("mixed (FP32 points, FP64 nodal sums)" if head_mode == "mixed" else "FP64"),
+                   "form_rule": f"fastest batched form within {REL_ERR_BOUND:g} of FP64 on every compared job "
+                                "after 500 steps",
+                   "kernel": head["kernel"], "points_per_item": head["cap"],
+                   "sort_interval": head["sort_interval"], "graph": True,
                    "parallelism": f"independent{world}",
                    "l2": "inputs larger than L2", "active_nodes_per_point": round(active_ratio, 4)},
-        "batched_fp64": ({"value": fp64_value, "unit": UNIT, "kernel": fp64["kernel"], "points_per_item": fp64["cap"],
-                          "sort_interval": fp64["sort_interval"]} if fp64 else None),
+        "batched_fp64": form_record(fp64, "fp64"),
+        "batched_mixed": form_record(mixed, "mixed"),
         "plain_fp64": {"value": plain_value, "unit": UNIT, "steps_per_job": args.plain_steps,
                        "how": "one mpmgpu_handle per job, jobs in sequence, CUDA events around each job's steps"},
         "vs_plain_fp64": (value / plain_value) if plain_value else None,
-        "mixed_rel_err_vs_fp64": errs,
+        "mixed_rel_err_vs_fp64": errs["mixed"] if errs else None,
         "column_fp64": column,
         "serving_full": serving,
         "roofline": roof,
-        "stage_ms_per_step": {k: v[1] / mixed["prof_steps"] for k, v in mixed["prof"].items()},
-        "gpu_launches": mixed["launches"],
-        "clocks": mixed["clocks"],
+        "stage_ms_per_step": {k: v[1] / head["prof_steps"] for k, v in head["prof"].items()},
+        "gpu_launches": head["launches"],
+        "clocks": head["clocks"],
         "e2e": e2e,
         "cpu_baseline": cpu,
     }
@@ -654,7 +699,7 @@ def run_serving_workload(args, rank, world, local):
     print(json.dumps(line), flush=True)
 
 
-def run_e2e_batch(cases, steps: int, device: int, kernel, sort_interval: int):
+def run_e2e_batch(cases, steps: int, device: int, kernel, sort_interval: int, mode: str = "mixed"):
     """The ensemble through the C ABI from host buffers: batch creation and
     upload of every job, `steps` steps (each job stops at its own count),
     download of every point's x, x_t and stress, teardown, all on the wall
@@ -666,7 +711,7 @@ def run_e2e_batch(cases, steps: int, device: int, kernel, sort_interval: int):
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     phases = {}
-    b = GPUBatch(dim=3, mode="mixed", device=device, sort_interval=sort_interval, kernel=kernel)
+    b = GPUBatch(dim=3, mode=mode, device=device, sort_interval=sort_interval, kernel=kernel)
     jobs = [b.add(c) for c in cases]
     t1 = time.perf_counter()
     phases["create_upload_s"] = t1 - t0

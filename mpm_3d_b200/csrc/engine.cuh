@@ -76,9 +76,6 @@ inline void make_geometry(const mpmgpu_config& cfg, Geom& g, MapConst& mc, BinGe
     } else {
       g.nn[d] = 1;
     }
-    mc.Lf[d] = (float)g.L[d];
-    mc.hf[d] = (float)g.h[d];
-    mc.NLf[d] = (float)mc.NL[d];
     mc.invhf[d] = (float)mc.invh[d];
   }
   if (cfg.dim == 3) {
@@ -169,8 +166,10 @@ inline int64_t job_footprint(const mpmgpu_config& cfg, int mode, bool keep_debug
   for (int b = 0; b < nbodies; b++) {
     const int64_t n = bodies[b].n + 8;
     const int nstate = material_state_arrays(bodies[b].has_material, bodies[b].material_kind);
-    // two point buffers (+ the 256-byte alignment of every array)
-    bytes += 2 * n * ((18 + nstate) * ps + 8) + 96 * 256;
+    // two point buffers (+ the 256-byte alignment of every array); the
+    // mixed form adds the low words of x, x_t and m
+    const int nlow = mixed ? 7 : 0;
+    bytes += 2 * n * ((18 + nstate + nlow) * ps + 8) + (96 + 2 * nlow) * 256;
     if (keep_debug && !mixed) bytes += 2 * n * 72;
     bytes += g.nslots * 8 * (7 + 6);            // accumulators + velocities
     if (mode == MPMGPU_MODE_FP64_DETERMINISTIC) bytes += g.nslots * 8 * 7;
@@ -213,8 +212,9 @@ class BatchBase {
                                              int threads) = 0;
   // Raw point state of a body copied to host memory in stream order, i.e.
   // as it stands after the work queued so far (without waiting): x, u, x_t
-  // (3 arrays each), stress (6) and V in the point precision, then active
-  // and pid (int32). `host` is pinned and holds snapshot_bytes(n).
+  // (3 arrays each), stress (6) and V in the point precision (and the mixed
+  // form's low words of x and x_t), then active and pid (int32). `host` is
+  // pinned and holds snapshot_bytes(n).
   virtual size_t snapshot_bytes(int64_t n) const = 0;
   virtual mpmgpu_status snapshot_body(int job, int body, void* host) = 0;
   // The fields of a completed snapshot in reference point order, as
@@ -415,7 +415,7 @@ class Batch : public BatchBase {
     const int64_t n = desc.n;
     HBody B;
     B.n = n;
-    MPM_TRY(stage_reserve((size_t)n * (21 * sizeof(PT) + 8) + 64 * 256));
+    MPM_TRY(stage_reserve((size_t)n * (28 * sizeof(PT) + 8) + 64 * 256));
     const size_t ns = (size_t)j->g.nslots;
     if (desc.has_material && (desc.material_kind < 0 || desc.material_kind > 2))
       return fail(MPMGPU_ERR_ARG, "unknown material kind");
@@ -453,19 +453,32 @@ class Batch : public BatchBase {
       auto col = [&](const double* aos, int w, int d) {
         for (int64_t i = 0; i < n; i++) tmp[(size_t)i] = (PT)aos[i * w + d];
       };
+      // the mixed form's low words of x, x_t and m (hi + lo = the value)
+      auto col_lo = [&](const double* aos, int w, int d) {
+        for (int64_t i = 0; i < n; i++) {
+          float hi, lo;
+          split_two_word(aos[i * w + d], hi, lo);
+          tmp[(size_t)i] = (PT)lo;
+        }
+      };
       for (int d = 0; d < D; d++) {
         col(desc.x, 3, d);
-        if constexpr (sizeof(PT) == 4) {
-          // the mixed form stores x0 = x - u and uses x = x0 + u
-          if (desc.u)
-            for (int64_t i = 0; i < n; i++) tmp[(size_t)i] = (PT)(desc.x[3 * i + d] - desc.u[3 * i + d]);
-        }
         MPM_TRY(upload(B.P.x[d], tmp));
         col(desc.x_t, 3, d);
         MPM_TRY(upload(B.P.v[d], tmp));
+        if constexpr (sizeof(PT) == 4) {
+          col_lo(desc.x, 3, d);
+          MPM_TRY(upload(B.P.xl[d], tmp));
+          col_lo(desc.x_t, 3, d);
+          MPM_TRY(upload(B.P.vl[d], tmp));
+        }
       }
       col(desc.m, 1, 0);
       MPM_TRY(upload(B.P.m, tmp));
+      if constexpr (sizeof(PT) == 4) {
+        col_lo(desc.m, 1, 0);
+        MPM_TRY(upload(B.P.ml, tmp));
+      }
       col(desc.v, 1, 0);
       MPM_TRY(upload(B.P.vol, tmp));
       for (int64_t i = 0; i < n; i++) tmp[(size_t)i] = (PT)point_extent(D, desc.v[i]);
@@ -669,6 +682,10 @@ class Batch : public BatchBase {
     const PT* ext = nullptr;
     const PT* ms[2] = {};
     const double* L = nullptr;
+    // low words of the mixed form (null in the FP64 form)
+    const PT* xl[3] = {};
+    const PT* vl[3] = {};
+    const PT* ml = nullptr;
   };
 
   static bool point_field_known(int field) {
@@ -689,27 +706,37 @@ class Batch : public BatchBase {
     const int D = dim_;
     auto slot = [](auto& p) { return reinterpret_cast<const void**>(&p); };
     add(B.P.pid, nz * sizeof(int32_t), slot(v.pid));
+    const bool two = B.P.ml != nullptr;   // the mixed form's low words
     switch (field) {
       case MPMGPU_P_X:
         for (int d = 0; d < D; d++) add(B.P.x[d], np, slot(v.x[d]));
-        if constexpr (sizeof(PT) == 4)
-          for (int d = 0; d < D; d++) add(B.P.u[d], np, slot(v.u[d]));
+        if (two)
+          for (int d = 0; d < D; d++) add(B.P.xl[d], np, slot(v.xl[d]));
         break;
       case MPMGPU_P_U:
         for (int d = 0; d < D; d++) add(B.P.u[d], np, slot(v.u[d]));
         break;
       case MPMGPU_P_X_T:
         for (int d = 0; d < D; d++) add(B.P.v[d], np, slot(v.v[d]));
+        if (two)
+          for (int d = 0; d < D; d++) add(B.P.vl[d], np, slot(v.vl[d]));
         break;
       case MPMGPU_P_MX_T:
         for (int d = 0; d < D; d++) add(B.P.v[d], np, slot(v.v[d]));
         add(B.P.m, np, slot(v.m));
+        if (two) {
+          for (int d = 0; d < D; d++) add(B.P.vl[d], np, slot(v.vl[d]));
+          add(B.P.ml, np, slot(v.ml));
+        }
         break;
       case MPMGPU_P_L: add(B.P.L, nz * 9 * sizeof(double), slot(v.L)); break;
       case MPMGPU_P_T:
         for (int c = 0; c < 6; c++) add(B.P.s[c], np, slot(v.s[c]));
         break;
-      case MPMGPU_P_M: add(B.P.m, np, slot(v.m)); break;
+      case MPMGPU_P_M:
+        add(B.P.m, np, slot(v.m));
+        if (two) add(B.P.ml, np, slot(v.ml));
+        break;
       case MPMGPU_P_V: add(B.P.vol, np, slot(v.vol)); break;
       case MPMGPU_P_EXTENT: add(B.P.ext, np, slot(v.ext)); break;
       case MPMGPU_P_ACTIVE: add(B.P.active, nz * sizeof(int32_t), slot(v.active)); break;
@@ -725,33 +752,27 @@ class Batch : public BatchBase {
     const size_t nz = (size_t)n;
     const int D = dim_;
     const int32_t* pid = v.pid;
-    auto vec3 = [&](const PT* const* a) {
+    // lo: the mixed form's low words (hi + lo), else null
+    auto vec3 = [&](const PT* const* a, const PT* const* lo = nullptr) {
       for (int64_t i = 0; i < 3 * n; i++) out[i] = 0.0;
       for (int d = 0; d < D; d++)
-        for (size_t i = 0; i < nz; i++) out[3 * (int64_t)pid[i] + d] = (double)a[d][i];
+        for (size_t i = 0; i < nz; i++)
+          out[3 * (int64_t)pid[i] + d] = two_word(a[d], lo ? lo[d] : nullptr, (int64_t)i);
     };
-    auto scalar = [&](const PT* a) {
-      for (size_t i = 0; i < nz; i++) out[pid[i]] = (double)a[i];
+    auto scalar = [&](const PT* a, const PT* lo = nullptr) {
+      for (size_t i = 0; i < nz; i++) out[pid[i]] = two_word(a, lo, (int64_t)i);
     };
     switch (field) {
-      case MPMGPU_P_X:
-        if constexpr (sizeof(PT) == 4) {
-          // the mixed form keeps x0 in the x arrays: x = x0 + u (in FP32)
-          for (int64_t i = 0; i < 3 * n; i++) out[i] = 0.0;
-          for (int d = 0; d < D; d++)
-            for (size_t i = 0; i < nz; i++) out[3 * (int64_t)pid[i] + d] = (double)(v.x[d][i] + v.u[d][i]);
-        } else {
-          vec3(v.x);
-        }
-        return;
+      case MPMGPU_P_X: vec3(v.x, v.xl[0] ? v.xl : nullptr); return;
       case MPMGPU_P_U: vec3(v.u); return;
-      case MPMGPU_P_X_T: vec3(v.v); return;
+      case MPMGPU_P_X_T: vec3(v.v, v.vl[0] ? v.vl : nullptr); return;
       case MPMGPU_P_MX_T:
-        vec3(v.v);
+        vec3(v.v, v.vl[0] ? v.vl : nullptr);
         // movePoints: mx_t = m * x_t (explicit_usl.cpp:295-297)
         for (size_t i = 0; i < nz; i++) {
           const int64_t q = pid[i];
-          for (int d = 0; d < D; d++) out[3 * q + d] = (double)v.m[i] * out[3 * q + d];
+          const double m = two_word(v.m, v.ml, (int64_t)i);
+          for (int d = 0; d < D; d++) out[3 * q + d] = m * out[3 * q + d];
         }
         return;
       case MPMGPU_P_L:
@@ -764,7 +785,7 @@ class Batch : public BatchBase {
           for (int k = 0; k < 9; k++) out[9 * (int64_t)pid[i] + k] = (double)v.s[idx[k]][i];
         return;
       }
-      case MPMGPU_P_M: scalar(v.m); return;
+      case MPMGPU_P_M: scalar(v.m, v.ml); return;
       case MPMGPU_P_V: scalar(v.vol); return;
       case MPMGPU_P_EXTENT: scalar(v.ext); return;
       case MPMGPU_P_GAMMAP: scalar(v.ms[0]); return;
@@ -1024,7 +1045,14 @@ class Batch : public BatchBase {
     return MPMGPU_OK;
   }
 
-  size_t snapshot_bytes(int64_t n) const override { return (size_t)n * (16 * sizeof(PT) + 2 * sizeof(int32_t)); }
+  // Point arrays of a snapshot: x, u, x_t (3 each), the stress (6), V, and
+  // in the mixed form the low words of x and x_t (3 each); then active and
+  // the point ids.
+  int snapshot_arrays() const { return mixed() ? 22 : 16; }
+
+  size_t snapshot_bytes(int64_t n) const override {
+    return (size_t)n * ((size_t)snapshot_arrays() * sizeof(PT) + 2 * sizeof(int32_t));
+  }
 
   mpmgpu_status snapshot_body(int job, int body, void* host) override {
     HJob* j;
@@ -1033,14 +1061,16 @@ class Batch : public BatchBase {
     const size_t n = (size_t)B->n;
     if (n == 0) return MPMGPU_OK;
     PT* h = static_cast<PT*>(host);
-    const PT* src[16] = {B->P.x[0], B->P.x[1], B->P.x[2], B->P.u[0], B->P.u[1], B->P.u[2], B->P.v[0], B->P.v[1],
-                         B->P.v[2], B->P.s[0], B->P.s[1], B->P.s[2], B->P.s[3], B->P.s[4], B->P.s[5], B->P.vol};
-    for (int a = 0; a < 16; a++) {
-      // x, u and x_t exist for the grid's axes only
-      if (a < 9 && a % 3 >= dim_) continue;
+    const PT* src[22] = {B->P.x[0],  B->P.x[1],  B->P.x[2],  B->P.u[0],  B->P.u[1],  B->P.u[2],  B->P.v[0],  B->P.v[1],
+                         B->P.v[2],  B->P.s[0],  B->P.s[1],  B->P.s[2],  B->P.s[3],  B->P.s[4],  B->P.s[5],  B->P.vol,
+                         B->P.xl[0], B->P.xl[1], B->P.xl[2], B->P.vl[0], B->P.vl[1], B->P.vl[2]};
+    const int na = snapshot_arrays();
+    for (int a = 0; a < na; a++) {
+      // x, u, x_t and the low words exist for the grid's axes only
+      if ((a < 9 || a >= 16) && (a < 16 ? a % 3 : (a - 16) % 3) >= dim_) continue;
       MPM_CUDA_TRY(cudaMemcpyAsync(h + a * n, src[a], n * sizeof(PT), cudaMemcpyDeviceToHost, stream_));
     }
-    int32_t* hi = reinterpret_cast<int32_t*>(h + 16 * n);
+    int32_t* hi = reinterpret_cast<int32_t*>(h + (size_t)na * n);
     MPM_CUDA_TRY(cudaMemcpyAsync(hi, B->P.active, n * sizeof(int32_t), cudaMemcpyDeviceToHost, stream_));
     MPM_CUDA_TRY(cudaMemcpyAsync(hi + n, B->P.pid, n * sizeof(int32_t), cudaMemcpyDeviceToHost, stream_));
     return MPMGPU_OK;
@@ -1050,18 +1080,17 @@ class Batch : public BatchBase {
                        double* active) const override {
     const size_t n = (size_t)n64;
     const PT* h = static_cast<const PT*>(host);
-    const int32_t* act = reinterpret_cast<const int32_t*>(h + 16 * n);
+    const int na = snapshot_arrays();
+    const int32_t* act = reinterpret_cast<const int32_t*>(h + (size_t)na * n);
     const int32_t* pid = act + n;
     static const int idx[9] = {0, 3, 5, 3, 1, 4, 5, 4, 2};
     for (size_t i = 0; i < n; i++) {
       const size_t q = (size_t)pid[i];
       for (int d = 0; d < 3; d++) {
         const bool on = d < dim_;
-        // the mixed form keeps x0 in the x arrays: x = x0 + u (in FP32)
-        const PT xv = on ? (sizeof(PT) == 4 ? (PT)(h[d * n + i] + h[(3 + d) * n + i]) : h[d * n + i]) : PT(0);
-        x[3 * q + d] = on ? (double)xv : 0.0;
+        x[3 * q + d] = on ? two_word(h + d * n, mixed() ? h + (16 + d) * n : nullptr, (int64_t)i) : 0.0;
         u[3 * q + d] = on ? (double)h[(3 + d) * n + i] : 0.0;
-        x_t[3 * q + d] = on ? (double)h[(6 + d) * n + i] : 0.0;
+        x_t[3 * q + d] = on ? two_word(h + (6 + d) * n, mixed() ? h + (19 + d) * n : nullptr, (int64_t)i) : 0.0;
       }
       for (int k = 0; k < 9; k++) T[9 * q + k] = (double)h[(9 + idx[k]) * n + i];
       v[q] = (double)h[15 * n + i];
@@ -1344,6 +1373,13 @@ class Batch : public BatchBase {
     P.L = nullptr;
     if (keep_debug_ && !mixed()) carve(a, &P.L, (size_t)n * 9);
     for (int k = 0; k < nstate; k++) carve(a, &P.ms[k], na);
+    if (mixed()) {
+      for (int d = 0; d < 3; d++) {
+        carve(a, &P.xl[d], na);
+        carve(a, &P.vl[d], na);
+      }
+      carve(a, &P.ml, na);
+    }
   }
 
   // Returns a job's arrays to the pool after the work already queued on the
@@ -2147,6 +2183,11 @@ class Batch : public BatchBase {
         if (b.P.L) MPM_TRY(snap_one(b.P.L, (size_t)b.n * 9 * sizeof(double)));
         for (int k = 0; k < 9; k++)
           if (b.P.ms[k]) MPM_TRY(snap_one(b.P.ms[k], np));
+        for (int d = 0; d < 3; d++) {
+          MPM_TRY(snap_one(b.P.xl[d], np));
+          MPM_TRY(snap_one(b.P.vl[d], np));
+        }
+        MPM_TRY(snap_one(b.P.ml, np));
         MPM_TRY(snap_one(b.A.m, ns));
         for (int d = 0; d < 3; d++) {
           MPM_TRY(snap_one(b.A.mx[d], ns));

@@ -26,21 +26,22 @@ __global__ void k_frame_points(PointsT<PT> P, int dim, FramePointLayout o, doubl
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < P.n; p += stride) {
     const int64_t q = P.pid[p];
+    // the mixed form's x, x_t and m are two-word values (hi + lo)
+    const double m = two_word(P.m, P.ml, p);
     for (int d = 0; d < 3; d++) {
       const bool on = d < dim;
-      // the mixed form keeps the initial position in the x arrays: x = x0 + u
-      const double x = on ? (sizeof(PT) == 4 ? (double)(P.x[d][p] + P.u[d][p]) : (double)P.x[d][p]) : 0.0;
-      const double xt = on ? (double)P.v[d][p] : 0.0;
+      const double x = on ? two_word(P.x[d], P.xl[d], p) : 0.0;
+      const double xt = on ? two_word(P.v[d], P.vl[d], p) : 0.0;
       out[o.x + 3 * q + d] = x;
       out[o.u + 3 * q + d] = on ? (double)P.u[d][p] : 0.0;
       out[o.xt + 3 * q + d] = xt;
       // movePoints: mx_t = m * x_t (explicit_usl.cpp:295-297)
-      out[o.mxt + 3 * q + d] = (double)P.m[p] * xt;
+      out[o.mxt + 3 * q + d] = m * xt;
     }
     const int idx[9] = {0, 3, 5, 3, 1, 4, 5, 4, 2};   // row-major 3x3 from xx yy zz xy yz xz
     for (int k = 0; k < 9; k++) out[o.T + 9 * q + k] = (double)P.s[idx[k]][p];
     out[o.v + q] = (double)P.vol[p];
-    out[o.m + q] = (double)P.m[p];
+    out[o.m + q] = m;
     out[o.ext + q] = (double)P.ext[p];
     // 2 = left the domain at the last move: active until the next map build
     out[o.active + q] = P.active[p] != 0 ? 1.0 : 0.0;

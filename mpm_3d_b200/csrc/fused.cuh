@@ -405,17 +405,29 @@ __device__ __forceinline__ GatherSum<R> gather_general(const BodyCtx<PT>& c, uns
   return gs;
 }
 
-// Position of a staged point. The FP64 form stores x and updates it as the
-// reference does (x += S^T u). The mixed form stores the initial position
-// x0 in the x arrays and derives x = x0 + u from the displacement u, which
-// the reference updates by the same increment (explicit_usl.cpp:279-280),
-// so x0 + u is x in exact arithmetic; in FP32 it avoids accumulating a
-// rounding of x at every step (x is large next to its increments, u is
-// not), and x0 is never written.
+// A staged point's position (k = kFx) or velocity (k = kFv) component in
+// double: the FP64 form's value, or the mixed form's two-word value, its
+// high word from the staged copy and its low word from global memory.
 template <typename PT, int ROW>
-__device__ __forceinline__ PT staged_pos(const PT* sp, int d) {
-  if constexpr (sizeof(PT) == 8) return sp[(kFx + d) * ROW];
-  else return sp[(kFx + d) * ROW] + sp[(kFu + d) * ROW];
+__device__ __forceinline__ double staged_two(const PT* sp, const PointsT<PT>& P, int64_t p, int k, int d) {
+  if constexpr (sizeof(PT) == 8) return sp[(k + d) * ROW];
+  else return (double)sp[(k + d) * ROW] + (double)(k == kFx ? P.xl[d][p] : P.vl[d][p]);
+}
+
+// Stores a position or velocity component (the mixed form splits it into
+// its two words).
+template <typename PT, int ROW>
+__device__ __forceinline__ void store_two(PT* sp, const PointsT<PT>& P, int64_t p, int k, int d, double v) {
+  if constexpr (sizeof(PT) == 8) {
+    sp[(k + d) * ROW] = v;
+    (k == kFx ? P.x[d] : P.v[d])[p] = v;
+  } else {
+    float hi, lo;
+    split_two_word(v, hi, lo);
+    sp[(k + d) * ROW] = hi;
+    (k == kFx ? P.x[d] : P.v[d])[p] = hi;
+    (k == kFx ? P.xl[d] : P.vl[d])[p] = lo;
+  }
 }
 
 // Phase 1 for one point: gather, movePoints / calculateStrainRate /
@@ -435,9 +447,9 @@ __device__ __forceinline__ void gather_update(const BodyCtx<PT>& c, int* err, un
   using R = PT;
   const PointsT<PT>& P = c.P;
   const R dt = (R)c.sp.dt;
-  R x[3] = {R(0), R(0), R(0)};
+  double x[3] = {0.0, 0.0, 0.0};
 #pragma unroll
-  for (int d = 0; d < DIM; d++) x[d] = staged_pos<PT, ROW>(sp, d);
+  for (int d = 0; d < DIM; d++) x[d] = staged_two<PT, ROW>(sp, P, p, kFx, d);
   PointMapT<R> pm;
   const int st = build_map<DIM>(c.g, c.mc, c.sp.cpdi, x, sp[kFext * ROW], pm, err);
   GatherSum<R> gs;
@@ -459,20 +471,15 @@ __device__ __forceinline__ void gather_update(const BodyCtx<PT>& c, int* err, un
     }
   }
   // movePoints: u_node = dt * x_t_node; x += S^T u, u += S^T u,
-  // x_t += S^T diff_x_t (explicit_usl.cpp:279-292)
+  // x_t += S^T diff_x_t (explicit_usl.cpp:279-292); the mixed form adds
+  // the increments to its two-word x and x_t in FP64
 #pragma unroll
   for (int d = 0; d < DIM; d++) {
     const R dx = dt * gs.du[d];
-    const R vn = sp[(kFv + d) * ROW] + gs.dv[d];
     const R un = sp[(kFu + d) * ROW] + dx;
-    if constexpr (sizeof(PT) == 8) {
-      const R xn = x[d] + dx;
-      sp[(kFx + d) * ROW] = xn;
-      P.x[d][p] = xn;
-    }
-    sp[(kFv + d) * ROW] = vn;
+    store_two<PT, ROW>(sp, P, p, kFx, d, x[d] + (double)dx);
+    store_two<PT, ROW>(sp, P, p, kFv, d, staged_two<PT, ROW>(sp, P, p, kFv, d) + (double)gs.dv[d]);
     sp[(kFu + d) * ROW] = un;
-    P.v[d][p] = vn;
     P.u[d][p] = un;
   }
   const R vol = sp[kFvol * ROW] * exp(dt * (gs.L[0][0] + gs.L[1][1] + gs.L[2][2]));
@@ -516,11 +523,14 @@ __device__ __forceinline__ void gather_update(const BodyCtx<PT>& c, int* err, un
 }
 
 // Values a point adds to one tile node, in the order m, mx[0..DIM),
-// f[0..DIM), normal[0..DIM); tile_field gives each one's tile row.
+// f[0..DIM), normal[0..DIM); tile_field gives each one's tile row. They
+// are FP64 (the tile's type): the mixed form forms the mass and momentum
+// contributions in FP64 from its two-word mass and velocity, and its force
+// and normal contributions in FP32.
 template <int DIM, bool NORMAL, typename R>
 struct NodeVals {
   static constexpr int K = 1 + 2 * DIM + (NORMAL ? DIM : 0);
-  R v[K];
+  double v[K];
 };
 
 template <int DIM>
@@ -540,20 +550,21 @@ __device__ __forceinline__ void tile_add_node(double* tacc, int t, const NodeVal
       // deterministic form: two exactly summed levels (second tile behind the first)
       const int cls = i == 0 ? 0 : (i <= DIM ? 1 : (i <= 2 * DIM ? 2 : 3));
       double q0, q1;
-      presplit((double)nv.v[i], ks[cls], q0, q1);
+      presplit(nv.v[i], ks[cls], q0, q1);
       atomicAdd(tacc + tile_field<DIM>(i) * TN + t, q0);
       atomicAdd(tacc + (10 + tile_field<DIM>(i)) * TN + t, q1);
     } else {
-      atomicAdd(tacc + tile_field<DIM>(i) * TN + t, (double)nv.v[i]);
+      atomicAdd(tacc + tile_field<DIM>(i) * TN + t, nv.v[i]);
     }
   }
 }
 
-// Per-point scatter sources: m, m x_t and V sigma (symmetric 3x3).
+// Per-point scatter sources: m, m x_t (FP64 in both forms: the mixed form's
+// are its two-word values) and V sigma (symmetric 3x3, point precision).
 template <typename R>
 struct ScatterSrc {
-  R m;
-  R mv[3];
+  double m;
+  double mv[3];
   R V3[3][3];
 };
 
@@ -571,11 +582,13 @@ __device__ __forceinline__ void scatter_box(const PointMapT<R>& pm, const int* o
   // the map's scales go into the point's sources once (sS on m and m x_t,
   // sG on V sigma and on m for the normal), the node loop uses the
   // unscaled axis factors
-  const R sm = pm.sS * q.m, gm = pm.sG * q.m;
-  R smv[3], sV[3][3];
+  const double sm = (double)pm.sS * q.m;
+  const R gm = pm.sG * (R)q.m;
+  double smv[3];
+  R sV[3][3];
 #pragma unroll
   for (int a = 0; a < 3; a++) {
-    smv[a] = pm.sS * q.mv[a];
+    smv[a] = (double)pm.sS * q.mv[a];
 #pragma unroll
     for (int b = 0; b < 3; b++) sV[a][b] = pm.sG * q.V3[a][b];
   }
@@ -590,11 +603,12 @@ __device__ __forceinline__ void scatter_box(const PointMapT<R>& pm, const int* o
       const R W12 = pm.ax[1].W[k1] * wz;
       const R G1W2 = pm.ax[1].G[k1] * wz;
       const R W1G2 = pm.ax[1].W[k1] * gz;
-      const R mrow = sm * W12;
-      R mvrow[3], A[3], Bf[3];
+      const double mrow = sm * (double)W12;
+      double mvrow[3];
+      R A[3], Bf[3];
 #pragma unroll
       for (int d = 0; d < DIM; d++) {
-        mvrow[d] = smv[d] * W12;
+        mvrow[d] = smv[d] * (double)W12;
         A[d] = sV[d][0] * W12;
         Bf[d] = sV[d][1] * G1W2;
         if (DIM == 3) Bf[d] += sV[d][2] * W1G2;
@@ -606,16 +620,16 @@ __device__ __forceinline__ void scatter_box(const PointMapT<R>& pm, const int* o
         touched[t] = 1;
         const R w0 = pm.ax[0].W[k0], g0 = pm.ax[0].G[k0];
         NodeVals<DIM, NORMAL, R> nv;
-        nv.v[0] = w0 * mrow;
+        nv.v[0] = (double)w0 * mrow;
 #pragma unroll
         for (int d = 0; d < DIM; d++) {
-          nv.v[1 + d] = w0 * mvrow[d];
-          nv.v[1 + DIM + d] = -(g0 * A[d] + w0 * Bf[d]);
+          nv.v[1 + d] = (double)w0 * mvrow[d];
+          nv.v[1 + DIM + d] = (double)(-(g0 * A[d] + w0 * Bf[d]));
         }
         if constexpr (NORMAL) {
           const R gr[3] = {g0 * W12, w0 * G1W2, w0 * W1G2};
 #pragma unroll
-          for (int d = 0; d < DIM; d++) nv.v[1 + 2 * DIM + d] = gr[d] * gm;
+          for (int d = 0; d < DIM; d++) nv.v[1 + 2 * DIM + d] = (double)(gr[d] * gm);
         }
         tile_add_node<DIM, NORMAL, TN, DET>(tacc, t, nv, ks);
       }
@@ -634,11 +648,13 @@ __device__ __forceinline__ void scatter_rolled(const PointMapT<R>& pm, const int
   const bool third0 = pm.ax[0].span == 3, third1 = pm.ax[1].span == 3, third2 = DIM == 3 && pm.ax[2].span == 3;
   const int K1 = 2 + ((mask >> 1) & 1), K2 = DIM == 3 ? 2 + ((mask >> 2) & 1) : 1;
   const bool wide0 = (mask & 1) != 0;
-  const R sm = pm.sS * q.m, gm = pm.sG * q.m;
-  R smv[3], sV[3][3];
+  const double sm = (double)pm.sS * q.m;
+  const R gm = pm.sG * (R)q.m;
+  double smv[3];
+  R sV[3][3];
 #pragma unroll
   for (int a = 0; a < 3; a++) {
-    smv[a] = pm.sS * q.mv[a];
+    smv[a] = (double)pm.sS * q.mv[a];
 #pragma unroll
     for (int b = 0; b < 3; b++) sV[a][b] = pm.sG * q.V3[a][b];
   }
@@ -655,11 +671,12 @@ __device__ __forceinline__ void scatter_rolled(const PointMapT<R>& pm, const int
       const R W12 = w1 * wz;
       const R G1W2 = sel3(pm.ax[1].G, k1) * wz;
       const R W1G2 = w1 * gz;
-      const R mrow = sm * W12;
-      R mvrow[3], A[3], Bf[3];
+      const double mrow = sm * (double)W12;
+      double mvrow[3];
+      R A[3], Bf[3];
 #pragma unroll
       for (int d = 0; d < DIM; d++) {
-        mvrow[d] = smv[d] * W12;
+        mvrow[d] = smv[d] * (double)W12;
         A[d] = sV[d][0] * W12;
         Bf[d] = sV[d][1] * G1W2;
         if (DIM == 3) Bf[d] += sV[d][2] * W1G2;
@@ -672,16 +689,16 @@ __device__ __forceinline__ void scatter_rolled(const PointMapT<R>& pm, const int
         touched[t] = 1;
         const R w0 = pm.ax[0].W[k0], g0 = pm.ax[0].G[k0];
         NodeVals<DIM, NORMAL, R> nv;
-        nv.v[0] = w0 * mrow;
+        nv.v[0] = (double)w0 * mrow;
 #pragma unroll
         for (int d = 0; d < DIM; d++) {
-          nv.v[1 + d] = w0 * mvrow[d];
-          nv.v[1 + DIM + d] = -(g0 * A[d] + w0 * Bf[d]);
+          nv.v[1 + d] = (double)w0 * mvrow[d];
+          nv.v[1 + DIM + d] = (double)(-(g0 * A[d] + w0 * Bf[d]));
         }
         if constexpr (NORMAL) {
           const R gr[3] = {g0 * W12, w0 * G1W2, w0 * W1G2};
 #pragma unroll
-          for (int d = 0; d < DIM; d++) nv.v[1 + 2 * DIM + d] = gr[d] * gm;
+          for (int d = 0; d < DIM; d++) nv.v[1 + 2 * DIM + d] = (double)(gr[d] * gm);
         }
         tile_add_node<DIM, NORMAL, TN, DET>(tacc, t, nv, ks);
       }
@@ -721,14 +738,14 @@ __device__ __forceinline__ void scatter_general(const BodyCtx<PT>& c, unsigned l
     const R gw0 = sG * pm.ax[0].W[k0];
     const R gr[3] = {sG * pm.ax[0].G[k0] * W12, gw0 * (g1 * wz), gw0 * (w1 * gz)};
     NodeVals<DIM, NORMAL, R> nv;
-    nv.v[0] = S * q.m;
+    nv.v[0] = (double)S * q.m;
 #pragma unroll
     for (int d = 0; d < DIM; d++) {
-      nv.v[1 + d] = S * q.mv[d];
+      nv.v[1 + d] = (double)S * q.mv[d];
       R fi = q.V3[d][0] * gr[0] + q.V3[d][1] * gr[1];
       if (DIM == 3) fi += q.V3[d][2] * gr[2];
-      nv.v[1 + DIM + d] = -fi;
-      if constexpr (NORMAL) nv.v[1 + 2 * DIM + d] = gr[d] * q.m;
+      nv.v[1 + DIM + d] = (double)(-fi);
+      if constexpr (NORMAL) nv.v[1 + 2 * DIM + d] = (double)(gr[d] * (R)q.m);
     }
     if (in_tile) {
       const int t = txy + k0 + TL::RL * k1 + TL::zoff(bz + k2);
@@ -747,12 +764,12 @@ __device__ __forceinline__ void scatter_general(const BodyCtx<PT>& c, unsigned l
           atomicAdd(a0 + s, v);
         }
       };
-      gadd(c.A.m, c.Ar.m, 0, (double)nv.v[0]);
+      gadd(c.A.m, c.Ar.m, 0, nv.v[0]);
 #pragma unroll
       for (int d = 0; d < DIM; d++) {
-        gadd(c.A.mx[d], c.Ar.mx[d], 1, (double)nv.v[1 + d]);
-        gadd(c.A.f[d], c.Ar.f[d], 2, (double)nv.v[1 + DIM + d]);
-        if constexpr (NORMAL) gadd(c.A.nrm[d], c.Ar.nrm[d], 3, (double)nv.v[1 + 2 * DIM + d]);
+        gadd(c.A.mx[d], c.Ar.mx[d], 1, nv.v[1 + d]);
+        gadd(c.A.f[d], c.Ar.f[d], 2, nv.v[1 + DIM + d]);
+        if constexpr (NORMAL) gadd(c.A.nrm[d], c.Ar.nrm[d], 3, nv.v[1 + 2 * DIM + d]);
       }
     }
   });
@@ -766,9 +783,9 @@ __device__ __forceinline__ void map_scatter(const BodyCtx<PT>& c, int* err, unsi
                                             const PT* sp, const int* o, int stepping, double* tacc, uint8_t* touched,
                                             const Split2* ks) {
   using R = PT;
-  R x[3] = {R(0), R(0), R(0)};
+  double x[3] = {0.0, 0.0, 0.0};
 #pragma unroll
-  for (int d = 0; d < DIM; d++) x[d] = staged_pos<PT, ROW>(sp, d);
+  for (int d = 0; d < DIM; d++) x[d] = staged_two<PT, ROW>(sp, c.P, p, kFx, d);
   PointMapT<R> pm;
   const int st = build_map<DIM>(c.g, c.mc, c.sp.cpdi, x, sp[kFext * ROW], pm, err);
   if (st < 0) {
@@ -779,10 +796,11 @@ __device__ __forceinline__ void map_scatter(const BodyCtx<PT>& c, int* err, unsi
   }
   if (st == 0) return;
   ScatterSrc<R> q;
-  q.m = sp[kFm * ROW];
+  // the mixed form's two-word mass and velocity (momentum in FP64)
+  q.m = sizeof(PT) == 8 ? (double)sp[kFm * ROW] : two_word(c.P.m, c.P.ml, p);
   const R vol = sp[kFvol * ROW];
 #pragma unroll
-  for (int d = 0; d < 3; d++) q.mv[d] = d < DIM ? q.m * sp[(kFv + d) * ROW] : R(0);
+  for (int d = 0; d < 3; d++) q.mv[d] = d < DIM ? q.m * staged_two<PT, ROW>(sp, c.P, p, kFv, d) : 0.0;
   // V * sigma as a symmetric 3x3 (stored xx yy zz xy yz xz)
   R vs[6];
 #pragma unroll

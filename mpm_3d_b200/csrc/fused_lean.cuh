@@ -77,6 +77,32 @@ __device__ __forceinline__ void prefetch_point_l2(const PointsT<PT>& P, int64_t 
                          P.s[0], P.s[1], P.s[2], P.s[3], P.s[4], P.s[5], P.vol, P.m, P.ext};
 #pragma unroll
   for (int f = 0; f < kNF; f++) prefetch_l2(arrs[f] + q);
+  if constexpr (sizeof(PT) == 4) {
+    const PT* lows[7] = {P.xl[0], P.xl[1], P.xl[2], P.vl[0], P.vl[1], P.vl[2], P.ml};
+#pragma unroll
+    for (int f = 0; f < 7; f++) prefetch_l2(lows[f] + q);
+  }
+}
+
+// A position, velocity or mass in double: the FP64 form's value, or the
+// mixed form's two words (hi + lo).
+template <typename PT>
+__device__ __forceinline__ double lean_two(const PT* hi, const PT* lo, int64_t p) {
+  if constexpr (sizeof(PT) == 8) return hi[p];
+  else return (double)hi[p] + (double)lo[p];
+}
+
+// Stores a position or velocity (the mixed form splits it into its two words).
+template <typename PT>
+__device__ __forceinline__ void lean_store_two(PT* hi, PT* lo, int64_t p, double v) {
+  if constexpr (sizeof(PT) == 8) {
+    hi[p] = v;
+  } else {
+    float h, l;
+    split_two_word(v, h, l);
+    hi[p] = h;
+    lo[p] = l;
+  }
 }
 
 // Stress update of one point for material MAT (-1: the body's kind at run
@@ -107,26 +133,26 @@ __device__ __forceinline__ void lean_point(const BodyCtx<PT>& c, int* err, unsig
   const R dt = (R)c.sp.dt;
   const R ext = P.ext[p];
   const R sG = map_grad_scale(c.g, ext);   // the same for both of the point's maps
-  R x[3] = {R(0), R(0), R(0)}, u[3] = {R(0), R(0), R(0)};
+  // position in double (the mixed form's two words); velocity in the point
+  // precision for the scatter's sources, vd its double value
+  double x[3] = {0.0, 0.0, 0.0}, vd[3] = {0.0, 0.0, 0.0};
+  R u[3] = {R(0), R(0), R(0)};
 #pragma unroll
   for (int d = 0; d < DIM; d++) {
-    x[d] = P.x[d][p];
-    if (sizeof(PT) == 4 || do_g2p) u[d] = P.u[d][p];
+    x[d] = lean_two(P.x[d], P.xl[d], p);
+    if (do_g2p) u[d] = P.u[d][p];
   }
-  R v[3] = {R(0), R(0), R(0)}, s6[6], vol;
+  R s6[6], vol;
   if (do_g2p) {
     if (a == 2) {
       // left the domain at the last move; generateMap deactivates it now
       P.active[p] = 0;
       return;
     }
-    R xc[3] = {R(0), R(0), R(0)};
-#pragma unroll
-    for (int d = 0; d < DIM; d++) xc[d] = sizeof(PT) == 8 ? x[d] : x[d] + u[d];
     GatherSum<R> gs;
     {
       PointMapT<R> pm;
-      const int st = build_map<DIM>(c.g, c.mc, c.sp.cpdi, xc, ext, pm, err, sG);
+      const int st = build_map<DIM>(c.g, c.mc, c.sp.cpdi, x, ext, pm, err, sG);
       if (st > 0) {
         const bool in = window_in_tile<DIM>(pm, o, T);
         const unsigned am = __activemask();
@@ -141,17 +167,16 @@ __device__ __forceinline__ void lean_point(const BodyCtx<PT>& c, int* err, unsig
         }
       }
     }
-    // movePoints (explicit_usl.cpp:279-292)
+    // movePoints (explicit_usl.cpp:279-292); the mixed form adds the
+    // increments to its two-word x and x_t in FP64
 #pragma unroll
     for (int d = 0; d < DIM; d++) {
       const R dx = dt * gs.du[d];
-      v[d] = P.v[d][p] + gs.dv[d];
+      x[d] = x[d] + (double)dx;
+      vd[d] = lean_two(P.v[d], P.vl[d], p) + (double)gs.dv[d];
       u[d] = u[d] + dx;
-      if constexpr (sizeof(PT) == 8) {
-        x[d] = x[d] + dx;
-        P.x[d][p] = x[d];
-      }
-      P.v[d][p] = v[d];
+      lean_store_two(P.x[d], P.xl[d], p, x[d]);
+      lean_store_two(P.v[d], P.vl[d], p, vd[d]);
       P.u[d][p] = u[d];
     }
     vol = P.vol[p] * exp(dt * (gs.L[0][0] + gs.L[1][1] + gs.L[2][2]));
@@ -171,7 +196,7 @@ __device__ __forceinline__ void lean_point(const BodyCtx<PT>& c, int* err, unsig
     }
   } else {
 #pragma unroll
-    for (int d = 0; d < DIM; d++) v[d] = P.v[d][p];
+    for (int d = 0; d < DIM; d++) vd[d] = lean_two(P.v[d], P.vl[d], p);
 #pragma unroll
     for (int k = 0; k < 6; k++) s6[k] = P.s[k][p];
     vol = P.vol[p];
@@ -179,11 +204,8 @@ __device__ __forceinline__ void lean_point(const BodyCtx<PT>& c, int* err, unsig
   if (!do_p2g || a != 1) return;
   // map build and scatter at the new position (mapPointsToNodes,
   // explicit_usl.cpp:112-164; contact normal, contact_huang.cpp:91)
-  R xn[3] = {R(0), R(0), R(0)};
-#pragma unroll
-  for (int d = 0; d < DIM; d++) xn[d] = sizeof(PT) == 8 ? x[d] : x[d] + u[d];
   PointMapT<R> pm;
-  const int st = build_map<DIM>(c.g, c.mc, c.sp.cpdi, xn, ext, pm, err, sG);
+  const int st = build_map<DIM>(c.g, c.mc, c.sp.cpdi, x, ext, pm, err, sG);
   if (st < 0) {
     // outside the domain: inactive from the next map build on
     // (default_points.cpp:217-219); before the first step, at once
@@ -192,9 +214,9 @@ __device__ __forceinline__ void lean_point(const BodyCtx<PT>& c, int* err, unsig
   }
   if (st == 0) return;
   ScatterSrc<R> q;
-  q.m = P.m[p];
+  q.m = lean_two(P.m, P.ml, p);
 #pragma unroll
-  for (int d = 0; d < 3; d++) q.mv[d] = d < DIM ? q.m * v[d] : R(0);
+  for (int d = 0; d < 3; d++) q.mv[d] = d < DIM ? q.m * vd[d] : 0.0;
   R vs[6];
 #pragma unroll
   for (int k = 0; k < 6; k++) vs[k] = (DIM == 3 || k == 0 || k == 1 || k == 3) ? s6[k] * vol : R(0);

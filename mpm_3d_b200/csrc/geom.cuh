@@ -109,10 +109,7 @@ __device__ __forceinline__ int axis_element(const Geom& g, int d, double c) {
 struct MapConst {
   double NL[3];    // N / L: element index scale
   double invh[3];  // 1 / h
-  float Lf[3];     // single-precision copies for the mixed form
-  float hf[3];
-  float NLf[3];
-  float invhf[3];
+  float invhf[3];  // 1 / h in single precision (the mixed form's point-sampled gradients)
 };
 
 // Element index floor(x / L * N) without a division: the product x * (N/L)
@@ -234,25 +231,20 @@ __device__ __forceinline__ int build_map_fast(const Geom& g, const MapConst& mc,
   return 1;
 }
 
-// Single-precision map of the mixed form: the same decisions as
-// build_map_fast in float arithmetic. The element index comes from
-// floor(x * N/L) clamped into the grid (no exact fallback: the mixed form
-// is compared with the FP64 form by tolerance, not bit for bit).
-__device__ __forceinline__ int axis_element_f32(const Geom& g, const MapConst& mc, int d, float c) {
-  int e = (int)floorf(c * mc.NLf[d]);
-  e = e < 0 ? 0 : e;
-  return e >= g.N[d] ? g.N[d] - 1 : e;
-}
-
+// Map of the mixed form: the decisions of build_map_fast on the point's
+// double position (the two-word value), so that its connectivity is the
+// FP64 form's; each corner's offset from its element's first node is taken
+// in double and rounded once, and the hat values and their sums are FP32
+// arithmetic on it. (Offsets formed in FP32, x - h e with x ~ 1 and h ~
+// 1/64, would keep only the bits of x below h: an error of about 4e-6 of a
+// hat value per step.)
 template <int DIM>
-__device__ __forceinline__ int build_map_f32(const Geom& g, const MapConst& mc, int cpdi_spec, const float* x,
+__device__ __forceinline__ int build_map_f32(const Geom& g, const MapConst& mc, int cpdi_spec, const double* x,
                                              float extent, PointMapT<float>& pm, int* err, float sG) {
-#pragma unroll
-  for (int d = 0; d < DIM; d++)
-    if (!(x[d] <= mc.Lf[d] && x[d] >= 0.0f)) return -1;
+  if (!in_domain<DIM>(g, x)) return -1;
   int cpdi = cpdi_spec;
-  const float a = 0.5f * extent;
-  float clo[3], chi[3];
+  const double a = 0.5 * (double)extent;
+  double clo[3], chi[3];
 #pragma unroll
   for (int d = 0; d < DIM; d++) {
     clo[d] = x[d] - a;
@@ -261,24 +253,28 @@ __device__ __forceinline__ int build_map_f32(const Geom& g, const MapConst& mc, 
   if (cpdi == 1) {
 #pragma unroll
     for (int d = 0; d < DIM; d++)
-      if (!(clo[d] <= mc.Lf[d] && clo[d] >= 0.0f) || !(chi[d] <= mc.Lf[d] && chi[d] >= 0.0f)) cpdi = 0;
+      if (!(clo[d] <= g.L[d] && clo[d] >= 0.0) || !(chi[d] <= g.L[d] && chi[d] >= 0.0)) cpdi = 0;
   }
   if (cpdi == 1) {
 #pragma unroll
     for (int d = 0; d < DIM; d++) {
       AxisMapT<float>& A = pm.ax[d];
-      const int elo = axis_element_f32(g, mc, d, clo[d]);
-      const bool hi_ok = chi[d] < mc.Lf[d];
-      const int ehi = hi_ok ? axis_element_f32(g, mc, d, chi[d]) : elo;
+      const int elo = axis_element_fast(g, mc, d, clo[d]);
+      const bool hi_ok = chi[d] < g.L[d];
+      const int ehi = hi_ok ? axis_element_fast(g, mc, d, chi[d]) : elo;
+      if (elo >= g.N[d] || (hi_ok && ehi >= g.N[d])) {
+        atomicOr(err, kErrElemAlias);
+        return 0;
+      }
       const int delta = ehi - elo;
       if (delta > 1 || delta < 0) atomicOr(err, kErrWideSpan);
       A.base = elo;
       A.span = 2 + (hi_ok && delta == 1 ? 1 : 0);
-      const float rl = (clo[d] - mc.hf[d] * (float)elo) * mc.invhf[d];
+      const float rl = (float)((clo[d] - g.h[d] * (double)elo) * mc.invh[d]);
       const float wl0 = 1.0f - fabsf(rl), wl1 = 1.0f - fabsf(rl - 1.0f);
       float wh0 = 0.0f, wh1 = 0.0f;
       if (hi_ok) {
-        const float rh = (chi[d] - mc.hf[d] * (float)ehi) * mc.invhf[d];
+        const float rh = (float)((chi[d] - g.h[d] * (double)ehi) * mc.invh[d]);
         wh0 = 1.0f - fabsf(rh);
         wh1 = 1.0f - fabsf(rh - 1.0f);
       }
@@ -304,16 +300,20 @@ __device__ __forceinline__ int build_map_f32(const Geom& g, const MapConst& mc, 
   }
 #pragma unroll
   for (int d = 0; d < DIM; d++)
-    if (!(x[d] < mc.Lf[d] && x[d] >= 0.0f)) return 0;
+    if (!(x[d] < g.L[d] && x[d] >= 0.0)) return 0;
 #pragma unroll
   for (int d = 0; d < DIM; d++) {
     AxisMapT<float>& A = pm.ax[d];
-    const int e = axis_element_f32(g, mc, d, x[d]);
+    const int e = axis_element_fast(g, mc, d, x[d]);
+    if (e >= g.N[d]) {
+      atomicOr(err, kErrElemAlias);
+      return 0;
+    }
     A.base = e;
     A.span = 2;
 #pragma unroll
     for (int o = 0; o < 2; o++) {
-      const float r = (x[d] - mc.hf[d] * (float)(e + o)) * mc.invhf[d];
+      const float r = (float)((x[d] - g.h[d] * (double)(e + o)) * mc.invh[d]);
       A.W[o] = 1.0f - fabsf(r);
       A.G[o] = (fabsf(r) >= 1.0f) ? 0.0f : -(r / fabsf(r)) * mc.invhf[d];
     }
@@ -337,12 +337,12 @@ __device__ __forceinline__ int build_map(const Geom& g, const MapConst& mc, int 
   return build_map_fast<DIM>(g, mc, cpdi, x, ext, pm, err, sG);
 }
 template <int DIM>
-__device__ __forceinline__ int build_map(const Geom& g, const MapConst& mc, int cpdi, const float* x, float ext,
+__device__ __forceinline__ int build_map(const Geom& g, const MapConst& mc, int cpdi, const double* x, float ext,
                                          PointMapT<float>& pm, int* err) {
   return build_map_f32<DIM>(g, mc, cpdi, x, ext, pm, err, map_grad_scale(g, ext));
 }
 template <int DIM>
-__device__ __forceinline__ int build_map(const Geom& g, const MapConst& mc, int cpdi, const float* x, float ext,
+__device__ __forceinline__ int build_map(const Geom& g, const MapConst& mc, int cpdi, const double* x, float ext,
                                          PointMapT<float>& pm, int* err, float sG) {
   return build_map_f32<DIM>(g, mc, cpdi, x, ext, pm, err, sG);
 }

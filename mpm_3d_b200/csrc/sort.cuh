@@ -140,13 +140,9 @@ __global__ void k_sort_count(const BatchHdr* hdr, const BodyCtx<PT>* bodies, con
     if (B.P.active[p] == 0) {
       k = B.bg.nbins * B.bg.cells_per_bin;
     } else {
-      PT xp[3] = {PT(0), PT(0), PT(0)};
+      double xp[3] = {0.0, 0.0, 0.0};
 #pragma unroll
-      for (int d = 0; d < DIM; d++) {
-        // the mixed form keeps x0 in the x arrays and x = x0 + u
-        if constexpr (sizeof(PT) == 8) xp[d] = B.P.x[d][p];
-        else xp[d] = B.P.x[d][p] + B.P.u[d][p];
-      }
+      for (int d = 0; d < DIM; d++) xp[d] = two_word(B.P.x[d], B.P.xl[d], p);   // the mixed form: hi + lo
       int c[3] = {0, 0, 0};
       const int cls = point_cell<DIM>(B.g, xp, 0.5 * (double)B.P.ext[p], c);
       int b, l;
@@ -337,6 +333,14 @@ __global__ void k_sort_scatter(const BatchHdr* hdr, const BodyCtx<PT>* bodies, c
 #pragma unroll
     for (int a = 0; a < 9; a++)
       if (S.ms[a] != nullptr) D.ms[a][pos] = S.ms[a][p];
+    if (S.ml != nullptr) {
+#pragma unroll
+      for (int d = 0; d < 3; d++) {
+        D.xl[d][pos] = S.xl[d][p];
+        D.vl[d][pos] = S.vl[d][p];
+      }
+      D.ml[pos] = S.ml[p];
+    }
   }
 }
 

@@ -36,8 +36,31 @@ struct PointsT {
   // shear strain gammap (ms[0]) and rate gammap_dot (ms[1])
   // (sand_sachithlocal.cpp:98-101).
   PT* ms[9];
+  // Mixed form only (null in the FP64 form): the low words of the
+  // position, velocity and mass, whose values are hi + lo summed in double
+  // (two FP32 words, 48 significant bits; the high words are x, v and m).
+  // The dynamics of soft bodies amplify a perturbation of the state by up
+  // to 1e5 over a few hundred steps, so storing x or x_t rounded to FP32
+  // (relative error 6e-8 per step) moves a trajectory by up to 1e-2 of its
+  // scale, while the stress, volume and displacement in one FP32 word stay
+  // well inside the mixed form's 1e-4 bound.
+  PT* xl[3];
+  PT* vl[3];
+  PT* ml;
 };
 using PointsDev = PointsT<double>;
+
+// A two-word value (hi + lo in double; the FP64 form has no low word).
+template <typename PT>
+__host__ __device__ __forceinline__ double two_word(const PT* hi, const PT* lo, int64_t i) {
+  return lo != nullptr ? (double)hi[i] + (double)lo[i] : (double)hi[i];
+}
+
+// Splits a double into a two-word FP32 value: hi = fl(v), lo = fl(v - hi).
+__host__ __device__ __forceinline__ void split_two_word(double v, float& hi, float& lo) {
+  hi = (float)v;
+  lo = (float)(v - (double)hi);
+}
 
 // Nodal accumulators of one body (the values mapPointsToNodes builds,
 // explicit_usl.cpp:112-164): mass, momentum and force.
