@@ -488,7 +488,7 @@ mpmgpu_status mpmgpu_server_create(const mpmgpu_batch_config* cfg, int64_t budge
     return MPMGPU_ERR_UNSUPPORTED;
   mpmgpu_status st = MPMGPU_OK;
   std::string msg;
-  // the batch's default kernel (in 3D point per thread, 256 points per
+  // the batch's default kernel (in 3D point per thread, 512 points per
   // work item), unless the caller picks the size
   const int cap = cfg->points_per_item;
   auto b = make_batch(cfg->dim, cfg->mode, cfg->device, cfg->sort_interval, cap, !cfg->no_graph, cfg->keep_debug, &st,

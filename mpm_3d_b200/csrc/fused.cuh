@@ -507,7 +507,7 @@ __device__ __forceinline__ void gather_update(const BodyCtx<PT>& c, int* err, un
     R s6[6];
 #pragma unroll
     for (int k = 0; k < 6; k++) s6[k] = sp[(kFs + k) * ROW];
-    jaumann_update<DIM, R>(gs.L, s6, (R)c.mat.G, (R)c.mat.lambda, dt);
+    jaumann_point<DIM, R>(gs.L, s6, c.mat, c.sp.dt);
 #pragma unroll
     for (int k = 0; k < 6; k++) {
       sp[(kFs + k) * ROW] = s6[k];

@@ -117,7 +117,7 @@ __device__ __forceinline__ void lean_stress(const BodyCtx<PT>& c, int64_t p, con
   } else if (kind == 2) {
     sand_update<DIM, R>(P.ms, p, L, s6, m, vol, c.mat, dt);
   } else {
-    jaumann_update<DIM, R>(L, s6, (R)c.mat.G, (R)c.mat.lambda, dt);
+    jaumann_point<DIM, R>(L, s6, c.mat, c.sp.dt);
   }
 }
 
