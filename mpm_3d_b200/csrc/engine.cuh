@@ -246,7 +246,7 @@ class BatchBase {
   virtual int sort_interval() const = 0;
   // Form of the fused kernel (kFormStaged, kFormLean) and
   // its points per work item; chosen at creation (the point-per-thread
-  // kernel with 256 points in 3D, the staged kernel otherwise), by the
+  // kernel with 512 points in 3D, the staged kernel otherwise), by the
   // autotuner, or by set_kernel.
   virtual int kernel_form() const = 0;
   virtual mpmgpu_status set_kernel(int form, int cap) = 0;
@@ -449,60 +449,52 @@ class Batch : public BatchBase {
         },
         B.allocs, j->bytes));
     if (n > 0) {
-      std::vector<PT> tmp((size_t)n);
-      auto col = [&](const double* aos, int w, int d) {
-        for (int64_t i = 0; i < n; i++) tmp[(size_t)i] = (PT)aos[i * w + d];
+      // each array is written straight into the pinned staging buffer (on
+      // several host threads for large bodies) and copied on the copy stream
+      auto col = [&](PT* dst, const double* aos, int w, int d) {
+        return upload_fill(dst, n, [=](PT* h, int64_t a, int64_t b) {
+          for (int64_t i = a; i < b; i++) h[i] = (PT)aos[i * w + d];
+        });
       };
       // the mixed form's low words of x, x_t and m (hi + lo = the value)
-      auto col_lo = [&](const double* aos, int w, int d) {
-        for (int64_t i = 0; i < n; i++) {
-          float hi, lo;
-          split_two_word(aos[i * w + d], hi, lo);
-          tmp[(size_t)i] = (PT)lo;
-        }
+      auto col_lo = [&](PT* dst, const double* aos, int w, int d) {
+        return upload_fill(dst, n, [=](PT* h, int64_t a, int64_t b) {
+          for (int64_t i = a; i < b; i++) {
+            float hi, lo;
+            split_two_word(aos[i * w + d], hi, lo);
+            h[i] = (PT)lo;
+          }
+        });
       };
       for (int d = 0; d < D; d++) {
-        col(desc.x, 3, d);
-        MPM_TRY(upload(B.P.x[d], tmp));
-        col(desc.x_t, 3, d);
-        MPM_TRY(upload(B.P.v[d], tmp));
+        MPM_TRY(col(B.P.x[d], desc.x, 3, d));
+        MPM_TRY(col(B.P.v[d], desc.x_t, 3, d));
         if constexpr (sizeof(PT) == 4) {
-          col_lo(desc.x, 3, d);
-          MPM_TRY(upload(B.P.xl[d], tmp));
-          col_lo(desc.x_t, 3, d);
-          MPM_TRY(upload(B.P.vl[d], tmp));
+          MPM_TRY(col_lo(B.P.xl[d], desc.x, 3, d));
+          MPM_TRY(col_lo(B.P.vl[d], desc.x_t, 3, d));
         }
       }
-      col(desc.m, 1, 0);
-      MPM_TRY(upload(B.P.m, tmp));
-      if constexpr (sizeof(PT) == 4) {
-        col_lo(desc.m, 1, 0);
-        MPM_TRY(upload(B.P.ml, tmp));
-      }
-      col(desc.v, 1, 0);
-      MPM_TRY(upload(B.P.vol, tmp));
-      for (int64_t i = 0; i < n; i++) tmp[(size_t)i] = (PT)point_extent(D, desc.v[i]);
-      MPM_TRY(upload(B.P.ext, tmp));
+      MPM_TRY(col(B.P.m, desc.m, 1, 0));
+      if constexpr (sizeof(PT) == 4) MPM_TRY(col_lo(B.P.ml, desc.m, 1, 0));
+      MPM_TRY(col(B.P.vol, desc.v, 1, 0));
+      const double* vol0 = desc.v;
+      MPM_TRY(upload_fill(B.P.ext, n, [=](PT* h, int64_t a, int64_t b) {
+        for (int64_t i = a; i < b; i++) h[i] = (PT)point_extent(D, vol0[i]);
+      }));
       if (desc.u)
-        for (int d = 0; d < D; d++) {
-          col(desc.u, 3, d);
-          MPM_TRY(upload(B.P.u[d], tmp));
-        }
+        for (int d = 0; d < D; d++) MPM_TRY(col(B.P.u[d], desc.u, 3, d));
       if (desc.T) {
         // stored as xx yy zz xy yz xz (row-major 9 -> symmetric 6)
         static const int idx[6] = {0, 4, 8, 1, 5, 2};
-        for (int c = 0; c < 6; c++) {
-          col(desc.T, 9, idx[c]);
-          MPM_TRY(upload(B.P.s[c], tmp));
-        }
+        for (int c = 0; c < 6; c++) MPM_TRY(col(B.P.s[c], desc.T, 9, idx[c]));
       }
-      std::vector<int32_t> act((size_t)n, 1), pid((size_t)n);
-      for (int64_t i = 0; i < n; i++) {
-        if (desc.active) act[(size_t)i] = desc.active[i] != 0 ? 1 : 0;
-        pid[(size_t)i] = (int32_t)i;
-      }
-      MPM_TRY(upload(B.P.active, act));
-      MPM_TRY(upload(B.P.pid, pid));
+      const int32_t* act0 = desc.active;
+      MPM_TRY(upload_fill(B.P.active, n, [=](int32_t* h, int64_t a, int64_t b) {
+        for (int64_t i = a; i < b; i++) h[i] = act0 ? (act0[i] != 0 ? 1 : 0) : 1;
+      }));
+      MPM_TRY(upload_fill(B.P.pid, n, [](int32_t* h, int64_t a, int64_t b) {
+        for (int64_t i = a; i < b; i++) h[i] = (int32_t)i;
+      }));
     }
     B.mat = make_material(desc.has_material, desc.E, desc.nu, desc.material_kind, desc.material_props,
                           desc.material_flags);
@@ -1402,25 +1394,50 @@ class Batch : public BatchBase {
     if (bytes <= stage_cap_) return MPMGPU_OK;
     if (stage_) cudaFreeHost(stage_);
     stage_ = nullptr;
+    // at least twice the old size: pinning pages is slow (about as slow as
+    // the upload itself), so a batch that grows job by job reallocates only
+    // a few times
+    const size_t cap = std::max<size_t>(std::max<size_t>(bytes, 2 * stage_cap_), (size_t)64 << 20);
     stage_cap_ = 0;
-    const size_t cap = std::max<size_t>(bytes, (size_t)64 << 20);
     MPM_CUDA_TRY(cudaHostAlloc(&stage_, cap, cudaHostAllocDefault));
     stage_cap_ = cap;
     return MPMGPU_OK;
   }
 
-  template <typename T>
-  mpmgpu_status upload(T* dst, const std::vector<T>& src) {
-    if (src.empty()) return MPMGPU_OK;
-    const size_t bytes = src.size() * sizeof(T);
+  // Runs body(a, b) over [0, n) in chunks on up to 8 host threads (one
+  // thread below 2^18 entries).
+  template <typename F>
+  static void host_parallel(int64_t n, F&& body) {
+    const int64_t per = (int64_t)1 << 18;
+    const int hw = std::max(1, (int)std::thread::hardware_concurrency());
+    const int nt = (int)std::min<int64_t>(std::min(8, hw), (n + per - 1) / per);
+    if (nt <= 1) {
+      body((int64_t)0, n);
+      return;
+    }
+    std::vector<std::thread> pool;
+    for (int t = 1; t < nt; t++) pool.emplace_back([&body, n, nt, t]() { body(n * t / nt, n * (t + 1) / nt); });
+    body((int64_t)0, n / nt);
+    for (auto& th : pool) th.join();
+  }
+
+  // Uploads n entries of a device array on the copy stream: fill(h, a, b)
+  // writes entries a..b-1 of the host image straight into the pinned
+  // staging buffer (reserved by stage_reserve), or into a pageable buffer
+  // copied synchronously when the reservation is exceeded.
+  template <typename T, typename F>
+  mpmgpu_status upload_fill(T* dst, int64_t n, F&& fill) {
+    if (n <= 0) return MPMGPU_OK;
+    const size_t bytes = (size_t)n * sizeof(T);
     if (stage_used_ + bytes > stage_cap_) {
-      // more than reserved: this copy goes through the pageable path
-      MPM_CUDA_TRY(cudaMemcpyAsync(dst, src.data(), bytes, cudaMemcpyHostToDevice, copy_stream_));
+      std::vector<T> tmp((size_t)n);
+      host_parallel(n, [&](int64_t a, int64_t b) { fill(tmp.data(), a, b); });
+      MPM_CUDA_TRY(cudaMemcpyAsync(dst, tmp.data(), bytes, cudaMemcpyHostToDevice, copy_stream_));
       MPM_CUDA_TRY(cudaStreamSynchronize(copy_stream_));
       return MPMGPU_OK;
     }
-    unsigned char* h = static_cast<unsigned char*>(stage_) + stage_used_;
-    std::memcpy(h, src.data(), bytes);
+    T* h = reinterpret_cast<T*>(static_cast<unsigned char*>(stage_) + stage_used_);
+    host_parallel(n, [&](int64_t a, int64_t b) { fill(h, a, b); });
     stage_used_ += (bytes + 255) / 256 * 256;
     MPM_CUDA_TRY(cudaMemcpyAsync(dst, h, bytes, cudaMemcpyHostToDevice, copy_stream_));
     return MPMGPU_OK;
@@ -1445,8 +1462,10 @@ class Batch : public BatchBase {
       MPM_CUDA_TRY(cudaStreamSynchronize(stream_));
       if (dl_stage_) cudaFreeHost(dl_stage_);
       dl_stage_ = nullptr;
+      // twice the request: the next, larger download of the same jobs (the
+      // stress after the positions) then fits without pinning pages again
+      const size_t cap = std::max<size_t>(2 * total, (size_t)16 << 20);
       dl_cap_ = 0;
-      const size_t cap = std::max<size_t>(total, (size_t)16 << 20);
       MPM_CUDA_TRY(cudaHostAlloc(&dl_stage_, cap, cudaHostAllocDefault));
       dl_cap_ = cap;
     }
