@@ -50,11 +50,15 @@ typedef enum {
 typedef enum {
   /* FP64 throughout; nodal sums use atomics (order varies run to run). */
   MPMGPU_MODE_FP64 = 0,
-  /* FP64 throughout; nodal sums in a fixed order: bit-reproducible
-   * (not available in this build: MPMGPU_ERR_UNSUPPORTED). */
+  /* FP64 throughout; nodal sums exact in any order (two-level pre-rounded
+   * contributions): bit-reproducible run to run, across re-binning
+   * intervals and batch mixes. */
   MPMGPU_MODE_FP64_DETERMINISTIC = 1,
-  /* FP32 particle state, shape functions and stress; FP64 nodal mass,
-   * momentum and force sums, nodal division and contact projection. */
+  /* FP32 particle state (position, velocity and mass as two FP32 words,
+   * hi + lo), shape functions and stress; the stress update, the mass and
+   * momentum contributions and the position and velocity updates in FP64
+   * arithmetic; FP64 nodal mass, momentum and force sums, nodal division
+   * and contact projection. */
   MPMGPU_MODE_MIXED = 2
 } mpmgpu_mode;
 
