@@ -836,29 +836,53 @@ class Batch : public BatchBase {
     std::vector<PointView> views((size_t)count);
     std::vector<std::pair<const void*, size_t>> items;
     std::vector<std::pair<size_t, const void**>> slots;   // (view, slot)
+    std::vector<size_t> first_item((size_t)count + 1, 0);
     for (int k = 0; k < count; k++) {
       HJob* j;
       HBody* B;
       MPM_TRY(readable_body(jobs[k], body, &j, &B));
       MPM_TRY(point_field_check(*B, field));
       views[(size_t)k].n = B->n;
+      first_item[(size_t)k] = items.size();
       point_field_arrays(*B, field, views[(size_t)k], [&](const void* src, size_t bytes, const void** slot) {
         items.emplace_back(src, bytes);
         slots.emplace_back((size_t)k, slot);
       });
     }
-    std::vector<const unsigned char*> h;
-    MPM_TRY(fetch(items, h));
-    for (size_t i = 0; i < slots.size(); i++) *slots[i].second = h[i];
-    const int nt = std::max(1, std::min(threads, count));
-    std::vector<std::thread> pool;
-    for (int t = 0; t < nt; t++)
-      pool.emplace_back([&, t]() {
-        for (int k = t; k < count; k += nt) points_to_ref(views[(size_t)k], field, outs[k]);
-      });
-    for (auto& th : pool) th.join();
+    first_item[(size_t)count] = items.size();
+    // jobs in groups of at most kFetchGroupBytes staged bytes: one copy and
+    // wait per group, then the group's conversion on host threads (a bounded
+    // pinned buffer instead of one the size of the whole field)
+    int k0 = 0;
+    while (k0 < count) {
+      int k1 = k0;
+      size_t bytes = 0;
+      while (k1 < count) {
+        size_t b = 0;
+        for (size_t i = first_item[(size_t)k1]; i < first_item[(size_t)k1 + 1]; i++) b += (items[i].second + 255) / 256 * 256;
+        if (k1 > k0 && bytes + b > kFetchGroupBytes) break;
+        bytes += b;
+        k1++;
+      }
+      const size_t i0 = first_item[(size_t)k0], i1 = first_item[(size_t)k1];
+      std::vector<std::pair<const void*, size_t>> group(items.begin() + (std::ptrdiff_t)i0,
+                                                        items.begin() + (std::ptrdiff_t)i1);
+      std::vector<const unsigned char*> h;
+      MPM_TRY(fetch(group, h));
+      for (size_t i = i0; i < i1; i++) *slots[i].second = h[i - i0];
+      const int ng = k1 - k0;
+      const int nt = std::max(1, std::min(threads, ng));
+      std::vector<std::thread> pool;
+      for (int t = 0; t < nt; t++)
+        pool.emplace_back([&, t]() {
+          for (int k = k0 + t; k < k1; k += nt) points_to_ref(views[(size_t)k], field, outs[k]);
+        });
+      for (auto& th : pool) th.join();
+      k0 = k1;
+    }
     return MPMGPU_OK;
   }
+  static constexpr size_t kFetchGroupBytes = (size_t)192 << 20;
 
   // ---- frames ----
 
