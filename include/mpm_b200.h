@@ -292,10 +292,8 @@ typedef enum {
 
 /* Selects the fused kernel's form and points per work item (default: one
  * point per thread with 512 points in 3D outside the deterministic form,
- * except that an FP64 3D handle with contacts starts, at its first step,
- * on the staged form with 512, measured faster there; else staged with
- * 512); MPMGPU_ERR_ARG if the pair is not available for the handle. Takes
- * effect at the next step. */
+ * else staged with 512); MPMGPU_ERR_ARG if the pair is not available for
+ * the handle. Takes effect at the next step. */
 mpmgpu_status mpmgpu_set_kernel(mpmgpu_handle* h, int form, int points_per_item);
 mpmgpu_status mpmgpu_kernel(const mpmgpu_handle* h, int* form, int* points_per_item);
 /* No counterpart in the reference. Tunes the handle's launch shape on its

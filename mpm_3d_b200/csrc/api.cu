@@ -23,8 +23,6 @@ struct mpmgpu_handle {
   bool started = false;
   int64_t extra_launches = 0;  // map exports (outside the engine)
   std::string last_error;
-  int contacts = 0;              // contact pairs added
-  bool kernel_chosen = false;    // mpmgpu_set_kernel or mpmgpu_autotune was called
 };
 
 struct mpmgpu_batch {
@@ -94,13 +92,6 @@ std::unique_ptr<BatchBase> make_batch(int dim, int mode, int device, int sort_in
 
 mpmgpu_status start(mpmgpu_handle* h) {
   if (h->started) return MPMGPU_OK;
-  // default kernel of an FP64 3D handle with contact: the staged form
-  // (measured on the two-body collision, 524,288 points: 0.140 ms per
-  // fused launch against 0.148 for the point-per-thread form at 256 points
-  // per item and 0.157 at 512); without contact, or in the mixed form, the
-  // point-per-thread form is the faster
-  if (!h->kernel_chosen && h->contacts > 0 && h->cfg.dim == 3 && h->cfg.mode == MPMGPU_MODE_FP64)
-    TRY(h->b->set_kernel(kFormStaged, 512));
   TRY(h->b->admit(h->job));
   h->started = true;
   return MPMGPU_OK;
@@ -161,17 +152,13 @@ mpmgpu_status mpmgpu_add_body(mpmgpu_handle* h, const mpmgpu_body_desc* desc, in
 mpmgpu_status mpmgpu_add_contact(mpmgpu_handle* h, int body1, int body2, double mu_f, int* contact_id) {
   if (!h) return MPMGPU_ERR_ARG;
   if (h->started) return hfail(h, MPMGPU_ERR_STATE, "contacts must be added before the first step");
-  TRY(h->b->add_contact(h->job, body1, body2, mu_f, contact_id));
-  h->contacts++;
-  return MPMGPU_OK;
+  return h->b->add_contact(h->job, body1, body2, mu_f, contact_id);
 }
 
 mpmgpu_status mpmgpu_add_contact_reflected(mpmgpu_handle* h, int body1, int body2, double mu_f, int* contact_id) {
   if (!h) return MPMGPU_ERR_ARG;
   if (h->started) return hfail(h, MPMGPU_ERR_STATE, "contacts must be added before the first step");
-  TRY(h->b->add_contact(h->job, body1, body2, mu_f, contact_id, 1));
-  h->contacts++;
-  return MPMGPU_OK;
+  return h->b->add_contact(h->job, body1, body2, mu_f, contact_id, 1);
 }
 
 mpmgpu_status mpmgpu_set_gravity(mpmgpu_handle* h, int use_vector, const double g[3]) {
@@ -208,9 +195,7 @@ mpmgpu_status mpmgpu_active_nodes(mpmgpu_handle* h, int64_t* nodes, int64_t* dri
 
 mpmgpu_status mpmgpu_set_kernel(mpmgpu_handle* h, int form, int points_per_item) {
   if (!h) return MPMGPU_ERR_ARG;
-  TRY(h->b->set_kernel(form, points_per_item));
-  h->kernel_chosen = true;
-  return MPMGPU_OK;
+  return h->b->set_kernel(form, points_per_item);
 }
 
 mpmgpu_status mpmgpu_kernel(const mpmgpu_handle* h, int* form, int* points_per_item) {
@@ -227,7 +212,6 @@ mpmgpu_status mpmgpu_autotune(mpmgpu_handle* h, int steps, int* form, int* point
   TRY(start(h));
   int cap = 0;
   TRY(h->b->autotune(steps, &cap));
-  h->kernel_chosen = true;
   if (form) *form = h->b->kernel_form();
   if (points_per_item) *points_per_item = cap;
   return MPMGPU_OK;
