@@ -11,15 +11,16 @@ download of the final point state, all inside the timed region).
 
 Workloads (seeded synthetic inputs, mpm_3d_b200.inputs):
   ensemble   (default) 512 independent 3D block drops (grids 16^3..96^3,
-             16.75 M points, seed 1003) in one batch, mixed form (FP32 point
-             state, FP64 nodal sums), one launch per stage replayed from a
-             CUDA graph, kernel form and points per CTA chosen by the
-             autotuner. Reported beside it: the same batch in FP64, the
-             plain FP64 path (one handle per job, jobs one after another),
-             the mixed form's error against FP64 on every 8th job after
-             its full 500 steps, the column collapse in plain FP64
-             (``column_fp64``, with its own roofline) and the full serving
-             stream (``serving_full``, 60 s of arrivals).
+             16.75 M points, seed 1003) in one batch per form (FP64; mixed:
+             FP32 point state with two-word x, x_t and m, FP64 nodal sums),
+             one launch per stage replayed from a CUDA graph, kernel form
+             and points per CTA chosen by the autotuner. ``value`` is the
+             fastest batched form within 1e-4 of FP64 on every compared job
+             (every 8th) after its full 500 steps; both forms are reported
+             with their errors, beside the plain FP64 path (one handle per
+             job, jobs one after another), the column collapse in plain
+             FP64 (``column_fp64``, with its own roofline) and the full
+             serving stream (``serving_full``, 60 s of arrivals).
   blockdrop2d  the 2D block drop, 20x20 grid, 144 points, 2000 steps (CPU-sized)
   collision  two 0.25 m cubes colliding, 128^3 grid, 524,288 points, ContactHuang (FP64)
   column     column collapse, 256x256x128 grid, 3,145,728 points (FP64)

@@ -569,8 +569,9 @@ struct ScatterSrc {
 };
 
 // Scatter over a box of K0 x K1 (x K2) nodes inside the tile (as
-// gather_box). The nodal force -V sigma . grad S is evaluated per row of the
-// box as -(G0 A + W0 B) with A, B the row factors of the separable gradient.
+// gather_box). The nodal force -V sigma . grad S is formed per node from the
+// node's gradient (measured 2 % faster on the column than row factors
+// -(G0 A + W0 B) precomputed per box row, which hold 6 more values).
 template <int DIM, int T, int TN, bool NORMAL, bool DET, int K0, int K1, int K2, typename R>
 __device__ __forceinline__ void scatter_box(const PointMapT<R>& pm, const int* o, const ScatterSrc<R>& q,
                                             double* tacc, uint8_t* touched, const Split2* ks) {
@@ -603,31 +604,22 @@ __device__ __forceinline__ void scatter_box(const PointMapT<R>& pm, const int* o
       const R W12 = pm.ax[1].W[k1] * wz;
       const R G1W2 = pm.ax[1].G[k1] * wz;
       const R W1G2 = pm.ax[1].W[k1] * gz;
-      const double mrow = sm * (double)W12;
-      double mvrow[3];
-      R A[3], Bf[3];
-#pragma unroll
-      for (int d = 0; d < DIM; d++) {
-        mvrow[d] = smv[d] * (double)W12;
-        A[d] = sV[d][0] * W12;
-        Bf[d] = sV[d][1] * G1W2;
-        if (DIM == 3) Bf[d] += sV[d][2] * W1G2;
-      }
 #pragma unroll
       for (int k0 = 0; k0 < K0; k0++) {
         if (k0 == 2 && !third0) continue;
         const int t = txy + k0 + TL::RL * k1 + TL::zoff(bz + k2);
         touched[t] = 1;
         const R w0 = pm.ax[0].W[k0], g0 = pm.ax[0].G[k0];
+        const R S = w0 * W12, gr0 = g0 * W12, gr1 = w0 * G1W2, gr2 = w0 * W1G2;
         NodeVals<DIM, NORMAL, R> nv;
-        nv.v[0] = (double)w0 * mrow;
+        nv.v[0] = (double)S * sm;
 #pragma unroll
         for (int d = 0; d < DIM; d++) {
-          nv.v[1 + d] = (double)w0 * mvrow[d];
-          nv.v[1 + DIM + d] = (double)(-(g0 * A[d] + w0 * Bf[d]));
+          nv.v[1 + d] = (double)S * smv[d];
+          nv.v[1 + DIM + d] = (double)(-(sV[d][0] * gr0 + sV[d][1] * gr1 + (DIM == 3 ? sV[d][2] * gr2 : R(0))));
         }
         if constexpr (NORMAL) {
-          const R gr[3] = {g0 * W12, w0 * G1W2, w0 * W1G2};
+          const R gr[3] = {gr0, gr1, gr2};
 #pragma unroll
           for (int d = 0; d < DIM; d++) nv.v[1 + 2 * DIM + d] = (double)(gr[d] * gm);
         }
