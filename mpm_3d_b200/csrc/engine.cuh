@@ -27,6 +27,7 @@
 #include <cstring>
 #include <memory>
 #include <set>
+#include <mutex>
 #include <thread>
 #include <string>
 #include <vector>
@@ -183,6 +184,86 @@ inline int64_t job_footprint(const mpmgpu_config& cfg, int mode, bool keep_debug
   return bytes;
 }
 
+// Process-wide device memory pools, one per device: batches allocate their
+// jobs' arrays from it in stream order, and a closed batch's memory stays
+// reserved for the next batch (mapping and unmapping device pages is what
+// makes a batch slow to create and to close). A closing batch trims the
+// pool to kPoolKeepBytes.
+constexpr size_t kPoolKeepBytes = (size_t)48 << 30;
+
+inline cudaError_t shared_pool(int device, cudaMemPool_t* out) {
+  static std::mutex m;
+  static cudaMemPool_t pools[64] = {};
+  if (device < 0 || device >= 64) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lock(m);
+  if (!pools[device]) {
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    cudaMemPool_t pool = nullptr;
+    cudaError_t e = cudaMemPoolCreate(&pool, &props);
+    if (e != cudaSuccess) return e;
+    uint64_t keep = UINT64_MAX;
+    e = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    if (e != cudaSuccess) return e;
+    pools[device] = pool;
+  }
+  *out = pools[device];
+  return cudaSuccess;
+}
+
+// Process-wide cache of pinned host buffers (staging of uploads, downloads
+// and frames): pinning and unpinning pages costs about as much as the copy
+// itself, so a closed batch's buffers serve the next one. At most
+// kPinnedKeepBytes stay cached.
+constexpr size_t kPinnedKeepBytes = (size_t)4 << 30;
+
+struct PinnedCache {
+  std::mutex m;
+  std::vector<std::pair<void*, size_t>> free;
+  size_t held = 0;
+};
+inline PinnedCache& pinned_cache() {
+  static PinnedCache c;
+  return c;
+}
+// A pinned buffer of at least `bytes` (its size in *cap).
+inline cudaError_t pinned_take(size_t bytes, void** out, size_t* cap) {
+  PinnedCache& c = pinned_cache();
+  {
+    std::lock_guard<std::mutex> lock(c.m);
+    size_t best = c.free.size();
+    for (size_t i = 0; i < c.free.size(); i++)
+      if (c.free[i].second >= bytes && (best == c.free.size() || c.free[i].second < c.free[best].second)) best = i;
+    if (best < c.free.size()) {
+      *out = c.free[best].first;
+      *cap = c.free[best].second;
+      c.held -= c.free[best].second;
+      c.free.erase(c.free.begin() + (std::ptrdiff_t)best);
+      return cudaSuccess;
+    }
+  }
+  *cap = bytes;
+  return cudaHostAlloc(out, bytes, cudaHostAllocDefault);
+}
+inline void pinned_give(void* p, size_t cap) {
+  if (!p) return;
+  PinnedCache& c = pinned_cache();
+  std::lock_guard<std::mutex> lock(c.m);
+  c.free.emplace_back(p, cap);
+  c.held += cap;
+  while (c.held > kPinnedKeepBytes && !c.free.empty()) {
+    // drop the smallest first: large buffers are the expensive ones to pin
+    size_t small = 0;
+    for (size_t i = 1; i < c.free.size(); i++)
+      if (c.free[i].second < c.free[small].second) small = i;
+    cudaFreeHost(c.free[small].first);
+    c.held -= c.free[small].second;
+    c.free.erase(c.free.begin() + (std::ptrdiff_t)small);
+  }
+}
+
 // Type-independent interface of a batch (the C ABI holds this).
 class BatchBase {
  public:
@@ -310,17 +391,10 @@ class Batch : public BatchBase {
     MPM_CUDA_TRY(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
     MPM_CUDA_TRY(cudaStreamCreateWithFlags(&copy_stream_, cudaStreamNonBlocking));
     MPM_CUDA_TRY(cudaEventCreateWithFlags(&upload_ev_, cudaEventDisableTiming));
-    {
-      // jobs' arrays come from a stream-ordered pool that keeps freed memory
-      // for the next job (no device-wide synchronisation per job)
-      cudaMemPoolProps props{};
-      props.allocType = cudaMemAllocationTypePinned;
-      props.location.type = cudaMemLocationTypeDevice;
-      props.location.id = device_;
-      MPM_CUDA_TRY(cudaMemPoolCreate(&pool_, &props));
-      uint64_t keep = UINT64_MAX;
-      MPM_CUDA_TRY(cudaMemPoolSetAttribute(pool_, cudaMemPoolAttrReleaseThreshold, &keep));
-    }
+    // jobs' arrays come from the device's stream-ordered pool, which keeps
+    // freed memory for the next job and the next batch (no device-wide
+    // synchronisation per job)
+    MPM_CUDA_TRY(shared_pool(device_, &pool_));
     // a requested item size is served by the point-per-thread kernel
     // where it has that size, else by the staged kernel
     if (cap_ == 0) cap_ = (dim_ == 3 && !det_) ? kDefaultLeanCap : default_cap();
@@ -351,10 +425,10 @@ class Batch : public BatchBase {
     if (stream_) cudaStreamSynchronize(stream_);
     for (void* p : scratch_allocs_) cudaFree(p);
     for (void* p : cap_allocs_) cudaFree(p);
-    if (pool_) cudaMemPoolDestroy(pool_);
-    if (stage_) cudaFreeHost(stage_);
-    if (dl_stage_) cudaFreeHost(dl_stage_);
-    if (frame_stage_) cudaFreeHost(frame_stage_);
+    if (pool_) cudaMemPoolTrimTo(pool_, kPoolKeepBytes);
+    pinned_give(stage_, stage_cap_);
+    pinned_give(dl_stage_, dl_cap_);
+    pinned_give(frame_stage_, frame_cap_);
     if (frame_dev_) cudaFree(frame_dev_);
     if (frame_ev_) cudaEventDestroy(frame_ev_);
     if (upload_ev_) cudaEventDestroy(upload_ev_);
@@ -948,11 +1022,12 @@ class Batch : public BatchBase {
         frame_dev_cap_ = bytes;
       }
       if (bytes > frame_cap_) {
-        if (frame_stage_) cudaFreeHost(frame_stage_);
+        pinned_give(frame_stage_, frame_cap_);
         frame_stage_ = nullptr;
         frame_cap_ = 0;
-        MPM_CUDA_TRY(cudaHostAlloc(&frame_stage_, bytes, cudaHostAllocDefault));
-        frame_cap_ = bytes;
+        size_t cap = 0;
+        MPM_CUDA_TRY(pinned_take(bytes, &frame_stage_, &cap));
+        frame_cap_ = cap;
       }
     }
     double* out = reinterpret_cast<double*>(frame_dev_);
@@ -1416,14 +1491,15 @@ class Batch : public BatchBase {
     MPM_CUDA_TRY(cudaStreamSynchronize(copy_stream_));  // the staging buffer is free again
     stage_used_ = 0;
     if (bytes <= stage_cap_) return MPMGPU_OK;
-    if (stage_) cudaFreeHost(stage_);
+    pinned_give(stage_, stage_cap_);
     stage_ = nullptr;
     // at least twice the old size: pinning pages is slow (about as slow as
     // the upload itself), so a batch that grows job by job reallocates only
     // a few times
-    const size_t cap = std::max<size_t>(std::max<size_t>(bytes, 2 * stage_cap_), (size_t)64 << 20);
+    const size_t want = std::max<size_t>(std::max<size_t>(bytes, 2 * stage_cap_), (size_t)64 << 20);
     stage_cap_ = 0;
-    MPM_CUDA_TRY(cudaHostAlloc(&stage_, cap, cudaHostAllocDefault));
+    size_t cap = 0;
+    MPM_CUDA_TRY(pinned_take(want, &stage_, &cap));
     stage_cap_ = cap;
     return MPMGPU_OK;
   }
@@ -1484,13 +1560,14 @@ class Batch : public BatchBase {
     for (auto& it : items) total += (it.second + 255) / 256 * 256;
     if (total > dl_cap_) {
       MPM_CUDA_TRY(cudaStreamSynchronize(stream_));
-      if (dl_stage_) cudaFreeHost(dl_stage_);
+      pinned_give(dl_stage_, dl_cap_);
       dl_stage_ = nullptr;
       // twice the request: the next, larger download of the same jobs (the
       // stress after the positions) then fits without pinning pages again
-      const size_t cap = std::max<size_t>(2 * total, (size_t)16 << 20);
+      const size_t want = std::max<size_t>(2 * total, (size_t)16 << 20);
       dl_cap_ = 0;
-      MPM_CUDA_TRY(cudaHostAlloc(&dl_stage_, cap, cudaHostAllocDefault));
+      size_t cap = 0;
+      MPM_CUDA_TRY(pinned_take(want, &dl_stage_, &cap));
       dl_cap_ = cap;
     }
     unsigned char* base = static_cast<unsigned char*>(dl_stage_);

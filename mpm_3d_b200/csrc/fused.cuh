@@ -663,16 +663,6 @@ __device__ __forceinline__ void scatter_rolled(const PointMapT<R>& pm, const int
       const R W12 = w1 * wz;
       const R G1W2 = sel3(pm.ax[1].G, k1) * wz;
       const R W1G2 = w1 * gz;
-      const double mrow = sm * (double)W12;
-      double mvrow[3];
-      R A[3], Bf[3];
-#pragma unroll
-      for (int d = 0; d < DIM; d++) {
-        mvrow[d] = smv[d] * (double)W12;
-        A[d] = sV[d][0] * W12;
-        Bf[d] = sV[d][1] * G1W2;
-        if (DIM == 3) Bf[d] += sV[d][2] * W1G2;
-      }
       const int trow = txy + TL::RL * k1 + zo;
 #pragma unroll
       for (int k0 = 0; k0 < 3; k0++) {
@@ -680,15 +670,16 @@ __device__ __forceinline__ void scatter_rolled(const PointMapT<R>& pm, const int
         const int t = trow + k0;
         touched[t] = 1;
         const R w0 = pm.ax[0].W[k0], g0 = pm.ax[0].G[k0];
+        const R S = w0 * W12, gr0 = g0 * W12, gr1 = w0 * G1W2, gr2 = w0 * W1G2;
         NodeVals<DIM, NORMAL, R> nv;
-        nv.v[0] = (double)w0 * mrow;
+        nv.v[0] = (double)S * sm;
 #pragma unroll
         for (int d = 0; d < DIM; d++) {
-          nv.v[1 + d] = (double)w0 * mvrow[d];
-          nv.v[1 + DIM + d] = (double)(-(g0 * A[d] + w0 * Bf[d]));
+          nv.v[1 + d] = (double)S * smv[d];
+          nv.v[1 + DIM + d] = (double)(-(sV[d][0] * gr0 + sV[d][1] * gr1 + (DIM == 3 ? sV[d][2] * gr2 : R(0))));
         }
         if constexpr (NORMAL) {
-          const R gr[3] = {g0 * W12, w0 * G1W2, w0 * W1G2};
+          const R gr[3] = {gr0, gr1, gr2};
 #pragma unroll
           for (int d = 0; d < DIM; d++) nv.v[1 + 2 * DIM + d] = (double)(gr[d] * gm);
         }
