@@ -312,6 +312,10 @@ mpmgpu_status mpmgpu_profile(mpmgpu_handle* h, int enable);
 /* Waits for the stream, then reports launches and total milliseconds of a stage. */
 mpmgpu_status mpmgpu_profile_read(mpmgpu_handle* h, int stage, int64_t* launches, double* total_ms);
 
+/* Releases the handle. Its job memory returns to the process's pool for
+ * the device, which keeps up to 48 GB reserved for later handles and
+ * batches (the rest is returned to the device); pinned staging buffers are
+ * kept for reuse likewise (up to 4 GB). */
 mpmgpu_status mpmgpu_destroy(mpmgpu_handle* h);
 
 /* ------------------------------------------------------------------------
@@ -427,6 +431,7 @@ mpmgpu_status mpmgpu_batch_profile_read(mpmgpu_batch* b, int stage, int64_t* lau
 void* mpmgpu_batch_stream(const mpmgpu_batch* b);
 /* Kernel launches issued (a graph replay counts its kernels). */
 int64_t mpmgpu_batch_launch_count(const mpmgpu_batch* b);
+/* Releases the batch (memory as mpmgpu_destroy). */
 mpmgpu_status mpmgpu_batch_destroy(mpmgpu_batch* b);
 
 /* ------------------------------------------------------------------------
