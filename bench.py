@@ -84,7 +84,7 @@ ENSEMBLE_SEED = 1003
 # captures of the kernel (the ensemble's from a capture of its first 96 jobs,
 # scaled to a launch by its points; the column's at full size). None where no
 # capture exists.
-TRAFFIC_BYTES_PER_POINT = {("ensemble", "mixed"): 267.8, ("ensemble", "fp64"): 396.7, ("column", "fp64"): 388.4}
+TRAFFIC_BYTES_PER_POINT = {("ensemble", "mixed"): 300.4, ("ensemble", "fp64"): 348.1, ("column", "fp64"): 349.5}
 
 
 def make_workload(name: str, rank: int = 0):
