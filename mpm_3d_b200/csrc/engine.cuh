@@ -406,6 +406,7 @@ class Batch : public BatchBase {
     MPM_TRY(alloc_raw(&count_, 1, scratch_allocs_));
     MPM_TRY(alloc_raw(&err_, 1, scratch_allocs_));
     MPM_TRY(alloc_raw(&drift_, 1, scratch_allocs_));
+    MPM_TRY(alloc_raw(&queue_, 2, scratch_allocs_));
     MPM_TRY(alloc_raw(&nwork_, 1, scratch_allocs_));
     MPM_TRY(alloc_raw(&active_nodes_, 1, scratch_allocs_));
     return MPMGPU_OK;
@@ -1992,6 +1993,7 @@ class Batch : public BatchBase {
     fl.phases = phases;
     fl.bounds = bounds_;
     fl.wait_polls = wait_polls_;
+    fl.queue = queue_;
     constexpr size_t smem = fused_smem_bytes<DIM, PT, CAP, NORMAL, DET>();
     auto kern = k_g2p2g<DIM, PT, CAP, NORMAL, SINGLE, DET>;
     // resident CTAs per SM, looked up once per kernel (before any capture)
@@ -2052,6 +2054,7 @@ class Batch : public BatchBase {
     fl.phases = phases;
     fl.bounds = nullptr;
     fl.wait_polls = wait_polls_;
+    fl.queue = queue_;
     constexpr size_t smem = lean_smem_bytes<3, PT, NORMAL>();
     auto kern = k_g2p2g_lean<3, PT, NT, PPT, NORMAL, SINGLE, MAT>;
     int& per_sm =
@@ -2438,6 +2441,7 @@ class Batch : public BatchBase {
   unsigned long long* count_ = nullptr;
   int* err_ = nullptr;
   unsigned long long* drift_ = nullptr;
+  int* queue_ = nullptr;   // the fused kernels' work queue (claim_item), zero between launches
   int32_t* nwork_ = nullptr;
   unsigned long long* active_nodes_ = nullptr;
   InstDev* insts_d_ = nullptr;

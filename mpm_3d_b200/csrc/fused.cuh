@@ -68,7 +68,30 @@ struct FusedLaunch {
   // out flags kErrWaitTimeout and its CTA returns (after the copies in
   // flight have landed, waited for with the default limit)
   uint32_t wait_polls;
+  // work queue of the launch (two counters, zero between launches; see
+  // claim_item)
+  int* queue;
 };
+
+// Dynamic distribution of a launch's work items. A CTA's first item is its
+// blockIdx.x; each later one is claimed from the launch's counter (items
+// gridDim.x, gridDim.x + 1, ... in claim order), so that CTAs that drew
+// small items take more of them: items differ in size by up to 8x where bins
+// are cut by body surfaces, and a fixed stride left the slowest CTA with
+// 5-17 % more than the mean of the work. queue[0] counts the claims,
+// queue[1] the CTAs that finished; the last CTA to finish zeroes both, so
+// the next launch on the stream (every kernel of an engine runs on its one
+// stream) starts from zero.
+__device__ __forceinline__ int claim_item(int* queue) { return (int)gridDim.x + atomicAdd(queue, 1); }
+
+// Called once per CTA by thread 0 after its last claim (every exit path).
+__device__ __forceinline__ void queue_done(int* queue) {
+  __threadfence();   // this CTA's claims precede its count of finished CTAs
+  if (atomicAdd(queue + 1, 1) == (int)gridDim.x - 1) {
+    atomicExch(queue, 0);
+    atomicExch(queue + 1, 0);
+  }
+}
 
 // Staged point arrays: x0..2 v0..2 u0..2 s0..5 vol m ext, then active.
 constexpr int kFx = 0, kFv = 3, kFu = 6, kFs = 9, kFvol = 15, kFm = 16, kFext = 17, kNF = 18;
@@ -879,8 +902,29 @@ __global__ void __launch_bounds__(fused_threads<PT, CAP>(), fused_min_ctas<PT, C
     mbar_arrive_expect_tx(bar_ctx, kCtxBytes);
     bulk_copy_g2s(slot_ctx(0), fl.bodies + fl.flat_body[blockIdx.x], kCtxBytes, bar_ctx);
   }
+  // the CTA's next item (claim_item), slot k & 1 for its k-th item: written
+  // by thread 0 before a barrier of the item, read by every thread after the
+  // item's last barrier
+  __shared__ int next_item[2];
   int k = 0;
-  for (int w = blockIdx.x; w < nwork; w += gridDim.x, k++) {
+  for (int w = blockIdx.x; w < nwork; w = next_item[k & 1], k++) {
+    // thread 0 claims the next item now and publishes it (and, over the
+    // table, starts the copy of its entry) before the item's first barrier
+    const int wn = threadIdx.x == 0 ? claim_item(fl.queue) : 0;
+    bool ahead = false;   // thread 0: the next entry's copy is in flight
+    auto publish_next = [&]() {
+      if (threadIdx.x != 0) return;
+      next_item[k & 1] = wn;
+      if (!SINGLE && wn < nwork) {
+        // the other slot was last read by the previous item (all threads
+        // passed its closing barrier)
+        const int other = (k & 1) ^ 1;
+        fence_async_shared();
+        mbar_arrive_expect_tx(bar_ctx + other, kCtxBytes);
+        bulk_copy_g2s(slot_ctx(other), fl.bodies + fl.flat_body[wn], kCtxBytes, bar_ctx + other);
+        ahead = true;
+      }
+    };
     int item, body_of_item;
     if (SINGLE) {
       body_of_item = fl.one_body;
@@ -889,20 +933,13 @@ __global__ void __launch_bounds__(fused_threads<PT, CAP>(), fused_min_ctas<PT, C
       body_of_item = fl.flat_body[w];
       item = fl.flat_item[w];
       const int slot = k & 1;
-      const bool ahead = w + (int)gridDim.x < nwork;
-      if (threadIdx.x == 0 && ahead) {
-        // the other slot was last read by the previous item (all threads
-        // passed its closing barrier)
-        fence_async_shared();
-        mbar_arrive_expect_tx(bar_ctx + (slot ^ 1), kCtxBytes);
-        bulk_copy_g2s(slot_ctx(slot ^ 1), fl.bodies + fl.flat_body[w + gridDim.x], kCtxBytes, bar_ctx + (slot ^ 1));
-      }
       const bool got = mbar_wait_bounded(bar_ctx + slot, (uint32_t)((k >> 1) & 1), fl.err, fl.wait_polls);
       if (__syncthreads_or(got ? 0 : 1)) {
-        // let the copies in flight land before leaving
+        // let the copy in flight land before leaving (the next entry's copy
+        // is not issued yet)
         if (threadIdx.x == 0) {
           if (!got) mbar_wait_bounded(bar_ctx + slot, (uint32_t)((k >> 1) & 1), fl.err);
-          if (ahead) mbar_wait_bounded(bar_ctx + (slot ^ 1), (uint32_t)(((k + 1) >> 1) & 1), fl.err);
+          queue_done(fl.queue);
         }
         return;
       }
@@ -911,12 +948,14 @@ __global__ void __launch_bounds__(fused_threads<PT, CAP>(), fused_min_ctas<PT, C
     if (!SINGLE) {
       // items of the other kind (contact normal or not) belong to the other launch
       if ((c.needs_normal != 0) != NORMAL) {
+        publish_next();
         __syncthreads();
         continue;
       }
     }
     const int prime = c.prime;
     if (fl.prime_pass && !prime) {
+      publish_next();
       __syncthreads();   // every thread has read the staged entry
       continue;
     }
@@ -1019,10 +1058,16 @@ __global__ void __launch_bounds__(fused_threads<PT, CAP>(), fused_min_ctas<PT, C
         for (int t = threadIdx.x; t < TN; t += blockDim.x) touched[t] = 0;
       }
     }
+    publish_next();
     const bool arrived = mbar_wait_bounded(bar, parity, fl.err, fl.wait_polls);
     // one decision for the whole CTA (also the barrier after the tile loads)
     if (__syncthreads_or(arrived ? 0 : 1)) {
-      if (!arrived) mbar_wait_bounded(bar, parity, fl.err);  // let copies in flight land before leaving
+      // let copies in flight land before leaving
+      if (!arrived) mbar_wait_bounded(bar, parity, fl.err);
+      if (threadIdx.x == 0) {
+        if (ahead) mbar_wait_bounded(bar_ctx + ((k & 1) ^ 1), (uint32_t)(((k + 1) >> 1) & 1), fl.err);
+        queue_done(fl.queue);
+      }
       return;
     }
     parity ^= 1u;
@@ -1094,6 +1139,7 @@ __global__ void __launch_bounds__(fused_threads<PT, CAP>(), fused_min_ctas<PT, C
     }
     __syncthreads();
   }
+  if (threadIdx.x == 0) queue_done(fl.queue);
 }
 
 }  // namespace mpmb200

@@ -265,28 +265,41 @@ __global__ void __launch_bounds__(NT, lean_min_ctas<PT, NT>())
     mbar_arrive_expect_tx(bar_ctx, kCtxBytes);
     bulk_copy_g2s(slot_ctx(0), fl.bodies + fl.flat_body[blockIdx.x], kCtxBytes, bar_ctx);
   }
+  // the CTA's next item, slot k & 1 for its k-th item: written by thread 0
+  // before a barrier of the item, read by every thread after the item's
+  // last barrier (the slot is written again two items later)
+  __shared__ int next_item[2];
   int k = 0;
-  for (int w = blockIdx.x; w < nwork; w += gridDim.x, k++) {
+  for (int w = blockIdx.x; w < nwork; w = next_item[k & 1], k++) {
+    // thread 0 claims the next item now and publishes it (and, over the
+    // table, starts the copy of its entry) before the item's first barrier,
+    // so that the claim's latency overlaps the tile loads
+    const int wn = threadIdx.x == 0 ? claim_item(fl.queue) : 0;
+    auto publish_next = [&]() {
+      if (threadIdx.x != 0) return;
+      next_item[k & 1] = wn;
+      if (!SINGLE && wn < nwork) {
+        // the other slot was last read by the previous item (all threads
+        // passed its closing barrier)
+        const int other = (k & 1) ^ 1;
+        fence_async_shared();
+        mbar_arrive_expect_tx(bar_ctx + other, kCtxBytes);
+        bulk_copy_g2s(slot_ctx(other), fl.bodies + fl.flat_body[wn], kCtxBytes, bar_ctx + other);
+      }
+    };
     int item;
     if (SINGLE) {
       item = fl.item_off[fl.one_body] + w;
     } else {
       item = fl.flat_item[w];
       const int slot = k & 1;
-      const bool ahead = w + (int)gridDim.x < nwork;
-      if (threadIdx.x == 0 && ahead) {
-        // the other slot was last read by the previous item (all threads
-        // passed its closing barrier)
-        fence_async_shared();
-        mbar_arrive_expect_tx(bar_ctx + (slot ^ 1), kCtxBytes);
-        bulk_copy_g2s(slot_ctx(slot ^ 1), fl.bodies + fl.flat_body[w + gridDim.x], kCtxBytes, bar_ctx + (slot ^ 1));
-      }
       const bool got = mbar_wait_bounded(bar_ctx + slot, (uint32_t)((k >> 1) & 1), fl.err, fl.wait_polls);
       if (__syncthreads_or(got ? 0 : 1)) {
-        // let the copies in flight land before leaving
+        // let the copy in flight land before leaving (the next entry's copy
+        // is not issued yet)
         if (threadIdx.x == 0) {
           if (!got) mbar_wait_bounded(bar_ctx + slot, (uint32_t)((k >> 1) & 1), fl.err);
-          if (ahead) mbar_wait_bounded(bar_ctx + (slot ^ 1), (uint32_t)(((k + 1) >> 1) & 1), fl.err);
+          queue_done(fl.queue);
         }
         return;
       }
@@ -295,12 +308,14 @@ __global__ void __launch_bounds__(NT, lean_min_ctas<PT, NT>())
     if (!SINGLE) {
       // items of the other kind (contact normal or not) belong to the other launch
       if ((c.needs_normal != 0) != NORMAL) {
+        publish_next();
         __syncthreads();
         continue;
       }
     }
     const int prime = c.prime;
     if (fl.prime_pass && !prime) {
+      publish_next();
       __syncthreads();   // every thread has read the staged entry
       continue;
     }
@@ -377,6 +392,7 @@ __global__ void __launch_bounds__(NT, lean_min_ctas<PT, NT>())
       for (int t = threadIdx.x; t < NACC * TN; t += NT) tacc[t] = 0.0;
       for (int t = threadIdx.x; t < TN; t += NT) touched[t] = 0;
     }
+    publish_next();
     __syncthreads();
 #pragma unroll 1
     for (int r = 0; r < PPT; r++) {
@@ -390,6 +406,7 @@ __global__ void __launch_bounds__(NT, lean_min_ctas<PT, NT>())
     }
     __syncthreads();
   }
+  if (threadIdx.x == 0) queue_done(fl.queue);
 }
 
 }  // namespace mpmb200
