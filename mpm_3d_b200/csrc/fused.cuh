@@ -73,15 +73,21 @@ struct FusedLaunch {
   int* queue;
 };
 
-// Dynamic distribution of a launch's work items. A CTA's first item is its
-// blockIdx.x; each later one is claimed from the launch's counter (items
-// gridDim.x, gridDim.x + 1, ... in claim order), so that CTAs that drew
-// small items take more of them: items differ in size by up to 8x where bins
-// are cut by body surfaces, and a fixed stride left the slowest CTA with
-// 5-17 % more than the mean of the work. queue[0] counts the claims,
-// queue[1] the CTAs that finished; the last CTA to finish zeroes both, so
-// the next launch on the stream (every kernel of an engine runs on its one
-// stream) starts from zero.
+// Dynamic distribution of the work items of a launch over the body table. A
+// CTA's first item is its blockIdx.x; each later one is claimed from the
+// launch's counter (items gridDim.x, gridDim.x + 1, ... in claim order), so
+// that CTAs that drew small items take more of them: items differ in size by
+// up to 8x where bins are cut by body surfaces, and a fixed stride left the
+// slowest CTA with 5-17 % more than the mean of the work (measured 4 % and
+// 7 % off the ensemble's FP64 and mixed kernels). A claim is made when the
+// CTA starts its current item, one item ahead, to hide its latency. A
+// one-body launch keeps the fixed stride: its items are few per CTA (one or
+// two on a 0.5 M-point body), where claims made one item ahead crowd the
+// last round onto fewer SMs than the stride does (measured 11 % slower on a
+// two-body collision). queue[0] counts the claims, queue[1] the CTAs that
+// finished; the last CTA to finish zeroes both, so the next launch on the
+// stream (every kernel of an engine runs on its one stream) starts from
+// zero.
 __device__ __forceinline__ int claim_item(int* queue) { return (int)gridDim.x + atomicAdd(queue, 1); }
 
 // Called once per CTA by thread 0 after its last claim (every exit path).
@@ -907,15 +913,15 @@ __global__ void __launch_bounds__(fused_threads<PT, CAP>(), fused_min_ctas<PT, C
   // item's last barrier
   __shared__ int next_item[2];
   int k = 0;
-  for (int w = blockIdx.x; w < nwork; w = next_item[k & 1], k++) {
+  for (int w = blockIdx.x; w < nwork; w = SINGLE ? w + (int)gridDim.x : next_item[k & 1], k++) {
     // thread 0 claims the next item now and publishes it (and, over the
     // table, starts the copy of its entry) before the item's first barrier
-    const int wn = threadIdx.x == 0 ? claim_item(fl.queue) : 0;
+    const int wn = !SINGLE && threadIdx.x == 0 ? claim_item(fl.queue) : 0;
     bool ahead = false;   // thread 0: the next entry's copy is in flight
     auto publish_next = [&]() {
-      if (threadIdx.x != 0) return;
+      if (SINGLE || threadIdx.x != 0) return;
       next_item[k & 1] = wn;
-      if (!SINGLE && wn < nwork) {
+      if (wn < nwork) {
         // the other slot was last read by the previous item (all threads
         // passed its closing barrier)
         const int other = (k & 1) ^ 1;
@@ -1066,7 +1072,7 @@ __global__ void __launch_bounds__(fused_threads<PT, CAP>(), fused_min_ctas<PT, C
       if (!arrived) mbar_wait_bounded(bar, parity, fl.err);
       if (threadIdx.x == 0) {
         if (ahead) mbar_wait_bounded(bar_ctx + ((k & 1) ^ 1), (uint32_t)(((k + 1) >> 1) & 1), fl.err);
-        queue_done(fl.queue);
+        if (!SINGLE) queue_done(fl.queue);
       }
       return;
     }
@@ -1139,7 +1145,7 @@ __global__ void __launch_bounds__(fused_threads<PT, CAP>(), fused_min_ctas<PT, C
     }
     __syncthreads();
   }
-  if (threadIdx.x == 0) queue_done(fl.queue);
+  if (!SINGLE && threadIdx.x == 0) queue_done(fl.queue);
 }
 
 }  // namespace mpmb200

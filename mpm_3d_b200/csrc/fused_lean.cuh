@@ -270,15 +270,15 @@ __global__ void __launch_bounds__(NT, lean_min_ctas<PT, NT>())
   // last barrier (the slot is written again two items later)
   __shared__ int next_item[2];
   int k = 0;
-  for (int w = blockIdx.x; w < nwork; w = next_item[k & 1], k++) {
+  for (int w = blockIdx.x; w < nwork; w = SINGLE ? w + (int)gridDim.x : next_item[k & 1], k++) {
     // thread 0 claims the next item now and publishes it (and, over the
     // table, starts the copy of its entry) before the item's first barrier,
     // so that the claim's latency overlaps the tile loads
-    const int wn = threadIdx.x == 0 ? claim_item(fl.queue) : 0;
+    const int wn = !SINGLE && threadIdx.x == 0 ? claim_item(fl.queue) : 0;
     auto publish_next = [&]() {
-      if (threadIdx.x != 0) return;
+      if (SINGLE || threadIdx.x != 0) return;
       next_item[k & 1] = wn;
-      if (!SINGLE && wn < nwork) {
+      if (wn < nwork) {
         // the other slot was last read by the previous item (all threads
         // passed its closing barrier)
         const int other = (k & 1) ^ 1;
@@ -406,7 +406,7 @@ __global__ void __launch_bounds__(NT, lean_min_ctas<PT, NT>())
     }
     __syncthreads();
   }
-  if (threadIdx.x == 0) queue_done(fl.queue);
+  if (!SINGLE && threadIdx.x == 0) queue_done(fl.queue);
 }
 
 }  // namespace mpmb200
