@@ -465,7 +465,9 @@ def run_batch(cases, mode: str, args, device: int, sample_ids):
     si = b.sort_interval()
     b.step(args.warmup)
     step_ms, launches, clk = timed_steps(b, args.steps)
-    prof_steps = 3
+    # one whole re-binning interval, so that the per-stage times carry one
+    # re-binning per sort_interval steps, as the timed steps do
+    prof_steps = max(3, si)
     prof = profile_pass(b, prof_steps)
     active, drift = b.active_nodes()
     steps_done = b.state(jobs[0])[0]

@@ -93,6 +93,12 @@ inline bool parse_points(const std::vector<char>& buf, const std::vector<size_t>
                          int64_t last, double* m, double* v, double* x, double* x_t, int32_t* active,
                          int64_t* bad) {
   const size_t size = buf.size() - 1;
+  // DefaultPoints::readFromFile (default_points.cpp:152-175) takes lines of
+  // 2 + 2 job->DIM + 1 or of 2 + 2 GRID_DIM + 1 columns. For the job types
+  // this path runs, JOB_2D and JOB_3D, job->DIM equals the grid's dimension
+  // (Job::assignJobType, job.hpp:58-70), so both widths are 3 + 2 dim; the
+  // 2D out-of-plane and axisymmetric types (job->DIM 3 over a 2D grid) are
+  // refused by the solver plugin.
   const int cols = 3 + 2 * dim;
   const char* text = buf.data();
   std::vector<std::pair<const char*, const char*>> tok;
