@@ -391,6 +391,11 @@ class Batch : public BatchBase {
     MPM_CUDA_TRY(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
     MPM_CUDA_TRY(cudaStreamCreateWithFlags(&copy_stream_, cudaStreamNonBlocking));
     MPM_CUDA_TRY(cudaEventCreateWithFlags(&upload_ev_, cudaEventDisableTiming));
+    MPM_CUDA_TRY(cudaEventCreateWithFlags(&fork_ev_, cudaEventDisableTiming));
+    for (int i = 0; i < kSideStreams; i++) {
+      MPM_CUDA_TRY(cudaStreamCreateWithFlags(&side_[i], cudaStreamNonBlocking));
+      MPM_CUDA_TRY(cudaEventCreateWithFlags(&join_ev_[i], cudaEventDisableTiming));
+    }
     // jobs' arrays come from the device's stream-ordered pool, which keeps
     // freed memory for the next job and the next batch (no device-wide
     // synchronisation per job)
@@ -433,6 +438,12 @@ class Batch : public BatchBase {
     if (frame_dev_) cudaFree(frame_dev_);
     if (frame_ev_) cudaEventDestroy(frame_ev_);
     if (upload_ev_) cudaEventDestroy(upload_ev_);
+    if (fork_ev_) cudaEventDestroy(fork_ev_);
+    for (int i = 0; i < kSideStreams; i++) {
+      if (side_[i]) cudaStreamSynchronize(side_[i]);
+      if (side_[i]) cudaStreamDestroy(side_[i]);
+      if (join_ev_[i]) cudaEventDestroy(join_ev_[i]);
+    }
     if (copy_stream_) cudaStreamDestroy(copy_stream_);
     if (stream_) cudaStreamDestroy(stream_);
   }
@@ -1972,7 +1983,7 @@ class Batch : public BatchBase {
   int stride_blocks(int threads) const { return sm_count_ * (2048 / threads); }
 
   template <int DIM, int CAP, bool NORMAL, bool SINGLE, bool DET>
-  mpmgpu_status launch_fused_k(int prime_pass, int phases, int one_body) {
+  mpmgpu_status launch_fused_k(int prime_pass, int phases, int one_body, cudaStream_t st) {
     FusedLaunch<PT> fl{};
     if (SINGLE) fl.one = ctx_host_[(size_t)one_body];
     fl.one_body = SINGLE ? one_body : -1;
@@ -2006,7 +2017,7 @@ class Batch : public BatchBase {
     }
     const int blocks = per_sm * sm_count_;
     StageTimer timer(this, kStageFused);
-    kern<<<blocks, fused_threads<PT, CAP>(), smem, stream_>>>(fl);
+    kern<<<blocks, fused_threads<PT, CAP>(), smem, st>>>(fl);
     return check_launch("k_g2p2g");
   }
 
@@ -2017,23 +2028,19 @@ class Batch : public BatchBase {
   mpmgpu_status launch_fused_t(int prime_pass, int phases) {
     if constexpr (CAP == 512) {
       if (single_mode_) {
-        for (size_t b = 0; b < ctx_host_.size(); b++) {
-          if (prime_pass && !ctx_host_[b].prime) continue;
-          if (ctx_host_[b].needs_normal)
-            MPM_TRY((launch_fused_k<DIM, CAP, true, true, DET>(prime_pass, phases, (int)b)));
-          else
-            MPM_TRY((launch_fused_k<DIM, CAP, false, true, DET>(prime_pass, phases, (int)b)));
-        }
-        return MPMGPU_OK;
+        return one_body_launches(prime_pass, [&](int b, cudaStream_t st) {
+          if (ctx_host_[(size_t)b].needs_normal) return launch_fused_k<DIM, CAP, true, true, DET>(prime_pass, phases, b, st);
+          return launch_fused_k<DIM, CAP, false, true, DET>(prime_pass, phases, b, st);
+        });
       }
     }
-    if (any_plain_) MPM_TRY((launch_fused_k<DIM, CAP, false, false, DET>(prime_pass, phases, -1)));
-    if (any_normal_) MPM_TRY((launch_fused_k<DIM, CAP, true, false, DET>(prime_pass, phases, -1)));
+    if (any_plain_) MPM_TRY((launch_fused_k<DIM, CAP, false, false, DET>(prime_pass, phases, -1, stream_)));
+    if (any_normal_) MPM_TRY((launch_fused_k<DIM, CAP, true, false, DET>(prime_pass, phases, -1, stream_)));
     return MPMGPU_OK;
   }
 
   template <int NT, int PPT, bool NORMAL, bool SINGLE, int MAT>
-  mpmgpu_status launch_lean_k(int prime_pass, int phases, int one_body) {
+  mpmgpu_status launch_lean_k(int prime_pass, int phases, int one_body, cudaStream_t st) {
     FusedLaunch<PT> fl{};
     if (SINGLE) fl.one = ctx_host_[(size_t)one_body];
     fl.one_body = SINGLE ? one_body : -1;
@@ -2065,39 +2072,73 @@ class Batch : public BatchBase {
       if (per_sm < 1) return fail(MPMGPU_ERR_CUDA, "fused kernel does not fit on an SM");
     }
     StageTimer timer(this, kStageFused);
-    kern<<<per_sm * sm_count_, NT, smem, stream_>>>(fl);
+    kern<<<per_sm * sm_count_, NT, smem, st>>>(fl);
     return check_launch("k_g2p2g_lean");
   }
 
   template <int NT, int PPT, bool NORMAL, bool SINGLE>
-  mpmgpu_status launch_lean_s(int prime_pass, int phases, int one_body, bool elastic) {
-    if (elastic) return launch_lean_k<NT, PPT, NORMAL, SINGLE, 0>(prime_pass, phases, one_body);
-    return launch_lean_k<NT, PPT, NORMAL, SINGLE, -1>(prime_pass, phases, one_body);
+  mpmgpu_status launch_lean_s(int prime_pass, int phases, int one_body, bool elastic, cudaStream_t st) {
+    if (elastic) return launch_lean_k<NT, PPT, NORMAL, SINGLE, 0>(prime_pass, phases, one_body, st);
+    return launch_lean_k<NT, PPT, NORMAL, SINGLE, -1>(prime_pass, phases, one_body, st);
   }
 
   // points per item: 128 (CTAs of 128 threads), 256 (256 threads) or 512
   // (256 threads, two points each)
   template <bool NORMAL, bool SINGLE>
-  mpmgpu_status launch_lean_m(int prime_pass, int phases, int one_body, bool elastic) {
-    if (cap_ == 128) return launch_lean_s<128, 1, NORMAL, SINGLE>(prime_pass, phases, one_body, elastic);
-    if (cap_ == 512) return launch_lean_s<256, 2, NORMAL, SINGLE>(prime_pass, phases, one_body, elastic);
-    return launch_lean_s<256, 1, NORMAL, SINGLE>(prime_pass, phases, one_body, elastic);
+  mpmgpu_status launch_lean_m(int prime_pass, int phases, int one_body, bool elastic, cudaStream_t st) {
+    if (cap_ == 128) return launch_lean_s<128, 1, NORMAL, SINGLE>(prime_pass, phases, one_body, elastic, st);
+    if (cap_ == 512) return launch_lean_s<256, 2, NORMAL, SINGLE>(prime_pass, phases, one_body, elastic, st);
+    return launch_lean_s<256, 1, NORMAL, SINGLE>(prime_pass, phases, one_body, elastic, st);
+  }
+
+  // The one-body launches of a stage, body by body (bodies still to prime
+  // only, in a priming pass). The bodies are independent here (each gathers
+  // from and scatters into its own nodal arrays), so the second to fourth
+  // body's launch runs on a side stream forked from the step's stream and
+  // joined back into it: its CTAs fill the SMs that the previous launch's
+  // last round of items leaves idle (a 0.26 M-point body is 512 items for
+  // 444 CTAs). A captured step graph holds the launches as parallel
+  // branches. Profiled steps launch on the step's stream only, so that each
+  // launch's stage time is its own.
+  template <typename F>
+  mpmgpu_status one_body_launches(int prime_pass, F&& launch_body) {
+    int todo[kSideStreams + 1];
+    int nt = 0;
+    for (size_t b = 0; b < ctx_host_.size(); b++) {
+      if (prime_pass && !ctx_host_[b].prime) continue;
+      if (nt == kSideStreams + 1) return fail(MPMGPU_ERR_UNSUPPORTED, "too many bodies for one-body launches");
+      todo[nt++] = (int)b;
+    }
+    const bool fork = !profiling_ && nt > 1;
+    if (fork) MPM_CUDA_TRY(cudaEventRecord(fork_ev_, stream_));
+    for (int i = 0; i < nt; i++) {
+      cudaStream_t st = stream_;
+      if (fork && i > 0) {
+        st = side_[i - 1];
+        MPM_CUDA_TRY(cudaStreamWaitEvent(st, fork_ev_, 0));
+      }
+      const mpmgpu_status r = launch_body(todo[i], st);
+      if (fork && i > 0) MPM_CUDA_TRY(cudaEventRecord(join_ev_[i - 1], st));
+      if (r != MPMGPU_OK) {
+        for (int k = 1; fork && k <= i; k++) cudaStreamWaitEvent(stream_, join_ev_[k - 1], 0);
+        return r;
+      }
+    }
+    for (int i = 1; fork && i < nt; i++) MPM_CUDA_TRY(cudaStreamWaitEvent(stream_, join_ev_[i - 1], 0));
+    return MPMGPU_OK;
   }
 
   mpmgpu_status launch_lean(int prime_pass, int phases) {
     if (single_mode_) {
-      for (size_t b = 0; b < ctx_host_.size(); b++) {
-        if (prime_pass && !ctx_host_[b].prime) continue;
-        const bool el = !ctx_host_[b].mat.has_material || ctx_host_[b].mat.kind == 0;
-        if (ctx_host_[b].needs_normal)
-          MPM_TRY((launch_lean_m<true, true>(prime_pass, phases, (int)b, el)));
-        else
-          MPM_TRY((launch_lean_m<false, true>(prime_pass, phases, (int)b, el)));
-      }
-      return MPMGPU_OK;
+      return one_body_launches(prime_pass, [&](int b, cudaStream_t st) {
+        const BodyCtx<PT>& c = ctx_host_[(size_t)b];
+        const bool el = !c.mat.has_material || c.mat.kind == 0;
+        if (c.needs_normal) return launch_lean_m<true, true>(prime_pass, phases, b, el, st);
+        return launch_lean_m<false, true>(prime_pass, phases, b, el, st);
+      });
     }
-    if (any_plain_) MPM_TRY((launch_lean_m<false, false>(prime_pass, phases, -1, all_elastic_)));
-    if (any_normal_) MPM_TRY((launch_lean_m<true, false>(prime_pass, phases, -1, all_elastic_)));
+    if (any_plain_) MPM_TRY((launch_lean_m<false, false>(prime_pass, phases, -1, all_elastic_, stream_)));
+    if (any_normal_) MPM_TRY((launch_lean_m<true, false>(prime_pass, phases, -1, all_elastic_, stream_)));
     return MPMGPU_OK;
   }
 
@@ -2368,6 +2409,11 @@ class Batch : public BatchBase {
   int fused_per_sm_[24] = {};
   cudaStream_t copy_stream_ = nullptr;
   cudaEvent_t upload_ev_ = nullptr;
+  // one-body launches of the second to fourth body (one_body_launches)
+  static constexpr int kSideStreams = 3;
+  cudaStream_t side_[kSideStreams] = {};
+  cudaEvent_t fork_ev_ = nullptr;
+  cudaEvent_t join_ev_[kSideStreams] = {};
   cudaMemPool_t pool_ = nullptr;
   void* stage_ = nullptr;
   size_t stage_cap_ = 0, stage_used_ = 0;
