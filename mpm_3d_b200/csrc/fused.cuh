@@ -85,9 +85,9 @@ struct FusedLaunch {
 // two on a 0.5 M-point body), where claims made one item ahead crowd the
 // last round onto fewer SMs than the stride does (measured 11 % slower on a
 // two-body collision). queue[0] counts the claims, queue[1] the CTAs that
-// finished; the last CTA to finish zeroes both, so the next launch on the
-// stream (every kernel of an engine runs on its one stream) starts from
-// zero.
+// finished; the last CTA to finish zeroes both, so the next launch over the
+// table starts from zero (an engine issues those launches one after the
+// other on its step stream; only one-body launches use side streams).
 __device__ __forceinline__ int claim_item(int* queue) { return (int)gridDim.x + atomicAdd(queue, 1); }
 
 // Called once per CTA by thread 0 after its last claim (every exit path).
