@@ -84,7 +84,8 @@ ENSEMBLE_SEED = 1003
 # captures of the kernel (the ensemble's from a capture of its first 96 jobs,
 # scaled to a launch by its points; the column's at full size). None where no
 # capture exists.
-TRAFFIC_BYTES_PER_POINT = {("ensemble", "mixed"): 289.2, ("ensemble", "fp64"): 341.2, ("column", "fp64"): 349.5}
+TRAFFIC_BYTES_PER_POINT = {("ensemble", "mixed"): 289.2, ("ensemble", "fp64"): 341.2, ("column", "fp64"): 349.5,
+                           ("column", "mixed"): 271.7}
 
 
 def make_workload(name: str, rank: int = 0):
