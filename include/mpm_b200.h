@@ -255,8 +255,11 @@ mpmgpu_status mpmgpu_sizes(const mpmgpu_handle* h, int body, int64_t* n_points, 
 /* Number of kernel launches issued since creation (for launch accounting). */
 int64_t mpmgpu_launch_count(const mpmgpu_handle* h);
 
-/* The CUDA stream (cudaStream_t) all of the handle's work is queued on, so
- * a caller can record its own events around mpmgpu_step. */
+/* The CUDA stream (cudaStream_t) all of the handle's work is ordered on, so
+ * a caller can record its own events around mpmgpu_step. (With two to four
+ * bodies, a step runs the bodies' fused kernels on side streams forked from
+ * this stream and joined back into it before the step's next kernel, so
+ * events and waits on this stream see the whole step.) */
 void* mpmgpu_stream(const mpmgpu_handle* h);
 
 /* Nodes with mass (counted per body) in the last step's grid update, and
