@@ -1879,7 +1879,7 @@ class Batch : public BatchBase {
     MPM_TRY(grow(&flat_item_, &cap_items_fi_, std::max<int64_t>(items, 1), 0));
     for (size_t b = 0; b < ctx.size(); b++) ctx[b].flags = flags_ + insts[(size_t)ctx[b].inst].block_off;
     ctx_host_ = ctx;
-    single_mode_ = ctx.size() <= 4;
+    single_mode_ = ctx.size() <= (size_t)kSideStreams + 1;   // one launch per body, concurrent (one_body_launches)
     any_plain_ = any_normal_ = false;
     all_elastic_ = true;
     for (const auto& c : ctx) {
